@@ -1,0 +1,337 @@
+"""Benchmark of the progressive path tracer on the flagship workload.
+
+Workload: the two-level-BVH, full-Disney-BSDF scene at 1920x1080 with 8 bounces (a displaced
+81,920-triangle icosphere instanced 64x, 32 analytic primitives, a 2048x1024 RGBE sky with
+importance sampling), seed 1.  One step = one progressive frame: one camera path per pixel
+(2,073,600 paths) through the renderer's C ABI, like one Renderer.render(frame) of tracer.js.
+The metric is paths/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N>1 runs under torchrun, one process per GPU; every rank renders the same view with its own
+seed (independent sample streams of one progressive image, no data-path collective), and the
+job's value is all ranks' paths over the slowest rank's device time.  `--impl reference` times
+the CPU restatement of the reference's shaders on this host's cores on the same workload (the
+reference's WGSL cannot run here: it needs a WebGPU device and no graphics stack exists).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WIDTH, HEIGHT, BOUNCES, SPP = 1920, 1080, 8, 64
+METRIC = "paths/s (1920x1080, 8 bounces)"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+# Algorithmic bytes per counted unit (counters of wgpt_read_counters):
+BYTES_PER_UNIT = {
+    3: 32,    # BVH node popped (two 16-byte vectors)
+    4: 32,    # child AABB tested
+    5: 48,    # triangle tested (v0, v1, v2)
+    6: 96,    # TLAS object visited (matrix + header)
+    7: 144,   # shading event (material record)
+    9: 4,     # environment CDF probe
+    10: 8,    # sky texel read (rgba16f)
+    11: 32,   # hit attributes of the winning primitive (normals)
+}
+PIXEL_BYTES = 16 + 16 + 4   # accumulation read + write, rgba8 store
+
+
+def algorithmic_bytes(counters: np.ndarray, pixels: int) -> float:
+    return float(sum(int(counters[k]) * b for k, b in BYTES_PER_UNIT.items()) + pixels * PIXEL_BYTES)
+
+
+def load_peaks() -> tuple[dict, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(n_gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def build_workload(seed: int = 1):
+    from webgpuraytracer_b200 import scene as sc
+    from webgpuraytracer_b200 import synth
+    s = synth.flagship_scene(seed, WIDTH, HEIGHT, BOUNCES)
+    return s, sc.pack_scene_data(s)
+
+
+def cpu_sample(scene, packed, frames: int, min_seconds: float, max_frames: int, rows: int | None = None):
+    """Times the CPU restatement on all host cores: whole 1080p frames (or the first `rows` rows)
+    one sample per pixel, until min_seconds have passed or max_frames were rendered."""
+    import oracle
+    from webgpuraytracer_b200 import scene as sc
+    scene.camera.update_rays2()
+    params = sc.pack_params(scene, packed, WIDTH, HEIGHT, 0, 1)
+    os_ = oracle.OracleScene(packed)
+    h = rows or HEIGHT
+    acc = np.zeros((HEIGHT, WIDTH, 4), np.float32)
+    out = np.zeros((HEIGHT, WIDTH, 4), np.uint8)
+    threads = os.cpu_count() or 1
+    done = 0
+    t0 = time.perf_counter()
+    while done < max_frames and (done < frames or time.perf_counter() - t0 < min_seconds):
+        oracle.render(os_, params, done, 1, (0, 0, WIDTH, h), acc, out, threads)
+        done += 1
+    dt = time.perf_counter() - t0
+    return WIDTH * h * done / dt, threads, f"{done} x {WIDTH}x{h} frame(s) at 1 spp, {dt:.1f} s"
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement of the reference's shaders on every host core."""
+    rank, world, _ = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0
+    if rank != 0:
+        return 0
+    scene, packed = build_workload()
+    import oracle
+    from webgpuraytracer_b200 import scene as sc
+    scene.camera.update_rays2()
+    params = sc.pack_params(scene, packed, WIDTH, HEIGHT, 0, 1)
+    os_ = oracle.OracleScene(packed)
+    acc = np.zeros((HEIGHT, WIDTH, 4), np.float32)
+    out = np.zeros((HEIGHT, WIDTH, 4), np.uint8)
+    threads = os.cpu_count() or 1
+    rows = 34   # one step = a 1920x34 band of the frame at 1 spp (65,280 paths)
+    for i in range(args.warmup):
+        oracle.render(os_, params, i, 1, (0, (i * rows) % (HEIGHT - rows), WIDTH, rows), acc, out, threads)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        y = (i * rows) % (HEIGHT - rows)
+        oracle.render(os_, params, i, 1, (0, y, WIDTH, rows), acc, out, threads)
+    dt = time.perf_counter() - t0
+    paths = WIDTH * rows * args.steps
+    value = paths / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scene generator)",
+        "config": {"workload": "flagship 1920x1080, 8 bounces, 64 instances x 81,920-tri BLAS + 32 prims, 2048x1024 RGBE env",
+                   "step": f"{WIDTH}x{rows} band at 1 spp", "l2": "not applicable (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "paths/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} bands of {WIDTH}x{rows} at 1 spp"},
+        "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's WGSL needs a WebGPU device; no graphics stack exists on this box, so the "
+                "reference arm is the CPU restatement of shader.wgsl (OpenMP over pixels)",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    rank, world, local = dist_setup(args.gpus)
+    import torch
+    from webgpuraytracer_b200 import renderer as rd
+    from webgpuraytracer_b200 import scene as sc
+
+    torch.cuda.set_device(local)
+    scene, packed = build_workload()
+    r = rd.Renderer(WIDTH, HEIGHT, device=local, seed_fn=lambda: 1 + rank)
+    r.set_scene(scene, packed=packed)
+    stream = torch.cuda.ExternalStream(r.stream_handle(), device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
+    scene.camera.update_rays2()
+
+    def params_for(frame):
+        return sc.pack_params(scene, packed, WIDTH, HEIGHT, frame, 1 + rank)
+
+    def launch(frame):
+        p = params_for(frame)
+        r._check(r.L.wgpt_set_params(r.ctx, rd.ptr(p)), "set_params")
+        r._check(r.L.wgpt_render(r.ctx, frame, 1, 0, 0, WIDTH, HEIGHT), "render")
+
+    # warm-up
+    for i in range(args.warmup):
+        launch(i)
+    r.synchronize()
+    # device-resident timing: one event pair per step, L2 flushed between steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(i))
+            starts[i].record(stream)
+        launch(args.warmup + i)
+        with torch.cuda.stream(stream):
+            ends[i].record(stream)
+    r.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    dev_s = sum(step_ms) / 1e3
+    dev_s_max = max_over_ranks(dev_s, world)
+    paths = WIDTH * HEIGHT * args.steps * world
+    value = paths / dev_s_max
+
+    # end-to-end through the C ABI with host buffers: params in, rgba8 image out, every step
+    out_host = torch.empty((HEIGHT, WIDTH, 4), dtype=torch.uint8, pin_memory=True)
+    e2e_steps = max(1, min(args.steps, 16))
+    barrier(world)
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        launch(args.warmup + args.steps + i)
+        r._check(r.L.wgpt_read_output(r.ctx, out_host.data_ptr()), "read_output")
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = WIDTH * HEIGHT * e2e_steps * world / e2e_s
+
+    # work counters of the timed frames (a separate counting pass, outside the timed region)
+    r.set_counting(True)
+    for i in range(args.steps):
+        launch(args.warmup + i)
+    cnt = r.read_counters()
+    r.set_counting(False)
+    launches = args.steps
+    bytes_per_launch = algorithmic_bytes(cnt, WIDTH * HEIGHT * args.steps) / launches
+    avg_launch_s = dev_s / launches
+    peaks, peak_kind = load_peaks()
+    achieved = bytes_per_launch / avg_launch_s / 1e9
+    rays = int(cnt[1] + cnt[2])
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_sample(scene, packed, 1, args.cpu_seconds, 8)
+        cpu = {"value": v, "unit": "paths/s", "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_s_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+            "config": {"workload": "flagship 1920x1080, 8 bounces, 64 instances x 81,920-tri BLAS + 32 prims, "
+                                   "2048x1024 RGBE env with importance sampling",
+                       "step": "one progressive frame: 1 path per pixel (2,073,600 paths)",
+                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"},
+            "rays_per_s": rays * world / dev_s_max,
+            "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": 112,
+                    "d2h_bytes_per_step": WIDTH * HEIGHT * 4},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback 6.65 TB/s",
+                         "kernel": "k_render", "algorithmic_bytes_per_launch": bytes_per_launch},
+            "counters_per_step": {"paths": int(cnt[0]) // args.steps, "ext_rays": int(cnt[1]) // args.steps,
+                                  "shadow_rays": int(cnt[2]) // args.steps, "nodes": int(cnt[3]) // args.steps,
+                                  "tri_tests": int(cnt[5]) // args.steps},
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    r.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,157 @@
+/*
+ * wgpt -- C ABI of the B200 progressive path tracer, a drop-in for the WebGPU device, buffers and
+ * dispatch loop of DragonFireGames/WebGPURaytracer's Renderer / Denoiser (tracer.js).
+ *
+ * Buffers are accepted in the reference's own packed layouts (see wgpt_layout.h).  All functions
+ * return WGPT_OK (0) or an error code; wgpt_last_error() gives a message.  No function aborts.
+ * The library owns all device memory; callers own every host pointer they pass.  One context is
+ * used by one thread at a time.  Work is queued on the context's CUDA stream; functions that
+ * hand data back to the host synchronise that stream first.
+ */
+#ifndef WGPT_H
+#define WGPT_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "wgpt_layout.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WGPT_ABI_VERSION 1
+
+enum wgpt_status {
+  WGPT_OK = 0,
+  WGPT_E_INVALID = 1,     /* bad argument (null pointer, zero size, out-of-range section) */
+  WGPT_E_LAYOUT = 2,      /* a buffer's size or an index inside it breaks the layout contract */
+  WGPT_E_CUDA = 3,        /* a CUDA runtime call failed */
+  WGPT_E_NOMEM = 4,       /* device allocation failed */
+  WGPT_E_STATE = 5,       /* call out of order (no scene, no size, no G-buffer) */
+  WGPT_E_UNSUPPORTED = 6, /* textures / parallax maps (not part of this build) */
+  WGPT_E_REBUILD = 7,     /* wgpt_update_scene: the new data does not fit, upload again */
+  WGPT_E_DEVICE = 8       /* a kernel reported an error (traversal stack overflow) */
+};
+
+typedef struct wgpt_ctx wgpt_ctx;
+
+typedef struct wgpt_buffer {
+  const void* ptr;
+  size_t bytes;
+} wgpt_buffer;
+
+/* Scene buffers of Renderer.setScene (tracer.js:1955-2102); binding numbers of shader.wgsl. */
+typedef struct wgpt_scene_desc {
+  wgpt_buffer materials;    /* binding 3,  wgpt_material[]      (144 B) */
+  wgpt_buffer objects;      /* binding 4,  wgpt_object[]        (96 B)  */
+  wgpt_buffer tlas;         /* binding 5,  wgpt_bvh_node[]      (32 B)  */
+  wgpt_buffer meshes;       /* binding 6,  list meshes, packed at 96 B and read at 80 B */
+  wgpt_buffer bvh;          /* binding 7,  wgpt_bvh_node[]      (32 B)  */
+  wgpt_buffer triangles;    /* binding 8,  wgpt_triangle[]      (128 B) */
+  wgpt_buffer planes;       /* binding 9,  wgpt_plane[]         (32 B)  */
+  wgpt_buffer lights;       /* binding 10, wgpt_light[]         (80 B)  */
+  wgpt_buffer sky_cdf;      /* binding 15, float[] (buildHDRCDF, tracer.js:135-204) */
+  const uint16_t* sky_rgba16f; /* binding 13, sky_width*sky_height texels of 4 IEEE halves */
+  uint32_t sky_width;
+  uint32_t sky_height;
+  int32_t bounce_limit;     /* override constant 0 (BOUNCE_LIMIT) */
+  uint32_t feature_flags;   /* override constants 1..11 as WGPT_HAS_* bits */
+} wgpt_scene_desc;
+
+/* Renderer constructor + init() (tracer.js:1720-1770): binds CUDA device `device`. */
+int wgpt_create(int device, wgpt_ctx** out);
+int wgpt_destroy(wgpt_ctx* ctx);
+const char* wgpt_last_error(const wgpt_ctx* ctx);
+int wgpt_abi_version(void);
+
+/* setScene buffer creation + writeBuffer (tracer.js:2015-2036) and the pipeline constants
+   (tracer.js:2062-2082).  Validates strides, indices and tree structure (WGPT_E_LAYOUT). */
+int wgpt_upload_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc);
+
+/* The upload checks alone, on the host (no device needed): 0 or the status wgpt_upload_scene
+   would return; msg (nullable) receives the reason. */
+int wgpt_validate_scene(const wgpt_scene_desc* desc, char* msg, size_t msg_len);
+
+/* updateObjects fast path (tracer.js:2132-2164): rewrites objects, tlas, planes, meshes and
+   materials in place when they fit and the flags are unchanged, else WGPT_E_REBUILD. */
+int wgpt_update_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc);
+
+/* resize (tracer.js:2166-2205): accumulation (16 B/px), rgba8 output and, with want_gbuf, the
+   48 B/px G-buffer; all zero-filled. */
+int wgpt_resize(wgpt_ctx* ctx, uint32_t width, uint32_t height, int want_gbuf);
+
+/* updateUniforms (tracer.js:2207-2240): the 112-byte SceneParams, taken verbatim (the seed is
+   the caller's; the reference draws it with Math.random). */
+int wgpt_set_params(wgpt_ctx* ctx, const void* scene_params_112);
+
+/* render / renderSection (tracer.js:2242-2309): `reps` samples of main over the section, sample
+   k using sample_number = first_frame + k.  Queued on the context stream (asynchronous). */
+int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sec_x, uint32_t sec_y,
+                uint32_t sec_w, uint32_t sec_h);
+
+/* setScene(scene, true) + render(): one dispatch of gbuf_main (shader.wgsl:2510-2603) into the
+   G-buffer and the debug quadrant image. */
+int wgpt_render_gbuffer(wgpt_ctx* ctx, uint32_t sec_x, uint32_t sec_y, uint32_t sec_w, uint32_t sec_h);
+
+/* Denoiser.execute (tracer.js:2583-2637): prepass, `passes` a-trous passes with the given step
+   widths (the reference as run uses 2^(passes-1) for every pass, see denoiser quirk notes), and
+   composite into the rgba8 output.  uniforms_48: wgpt_denoise_uniforms (width/height must match
+   the context size; step_width and passes are taken from `steps`/`passes`). */
+int wgpt_denoise(wgpt_ctx* ctx, const void* uniforms_48, const uint32_t* steps, uint32_t passes);
+
+/* renderPreview blit (tracer.js:2365-2389, scale.wgsl): bilinear resample of the output image
+   (its top-left ratio_x/ratio_y part) into a dst_w x dst_h canvas image owned by the context. */
+int wgpt_resample(wgpt_ctx* ctx, uint32_t dst_w, uint32_t dst_h, float ratio_x, float ratio_y);
+
+/* Waits for queued work; returns WGPT_E_DEVICE if a kernel flagged an error. */
+int wgpt_synchronize(wgpt_ctx* ctx);
+
+/* Readback / write-back of the context images (SaveRender, gui.js:1622; checkpoint/resume). */
+int wgpt_read_accum(wgpt_ctx* ctx, float* dst_rgba32f);
+int wgpt_write_accum(wgpt_ctx* ctx, const float* src_rgba32f);
+int wgpt_read_output(wgpt_ctx* ctx, uint8_t* dst_rgba8);
+int wgpt_read_gbuffer(wgpt_ctx* ctx, void* dst_48B_per_px);
+int wgpt_write_gbuffer(wgpt_ctx* ctx, const void* src_48B_per_px);
+int wgpt_read_denoised(wgpt_ctx* ctx, float* filtered_rgba32f, float* composited_rgba32f);
+int wgpt_read_canvas(wgpt_ctx* ctx, uint8_t* dst_rgba8, uint32_t dst_w, uint32_t dst_h);
+
+/* Closest hit of caller rays (trace_scene, shader.wgsl:754-774) for parity tests: rays are n x
+   (origin, direction) floats; outputs object index, material index, global triangle index
+   (-1 unless a mesh triangle), t, world normal (3 floats). Host pointers. */
+int wgpt_trace_rays(wgpt_ctx* ctx, const float* rays, uint32_t n, int32_t* o_idx, int32_t* m_idx,
+                    int32_t* prim, float* t, float* normal);
+
+/* Work counters of the renders queued while counting is on, 16 x u64: 0 paths, 1 extension rays,
+   2 shadow rays, 3 BVH nodes popped, 4 child AABB tests, 5 triangle tests, 6 TLAS objects
+   visited, 7 shading events, 8 environment NEE samples, 9 CDF probes, 10 sky texel reads,
+   11 hit-attribute evaluations, 12-15 reserved (zero). */
+int wgpt_set_counting(wgpt_ctx* ctx, int on);
+int wgpt_read_counters(wgpt_ctx* ctx, uint64_t* dst16);
+
+/* The context's cudaStream_t (as void*) for callers that time or order work around it. */
+void* wgpt_stream(wgpt_ctx* ctx);
+
+/* Host-side builders of the scene buffers (tracer.js host math, native): */
+/* ModelData.generateBVH (tracer.js:1025-1118): binned-SAH BLAS over n triangles given as
+   n x 24 floats (v0 v1 v2 n0 n1 n2 as xyz, uv0 uv1 uv2 as xy).  Writes up to 2n-1 nodes and n
+   triangles in flattened order; *n_nodes receives the node count. */
+int wgpt_build_blas(const float* tris24, uint32_t n, wgpt_bvh_node* nodes_out, uint32_t* n_nodes,
+                    wgpt_triangle* tris_out);
+/* SceneBVHBuilder (tracer.js:1509-1619): median-split TLAS over n object AABBs (n x 6 floats,
+   min xyz then max xyz).  Writes up to 2n-1 nodes; *n_nodes receives the count. */
+int wgpt_build_tlas(const float* aabbs6, uint32_t n, wgpt_bvh_node* nodes_out, uint32_t* n_nodes);
+/* HDRTexture.buildHDRCDF (tracer.js:135-204) over w x h rgba16f texels: writes (h+1) + h(w+1)
+   floats and the total weight (sky_total_lum). */
+int wgpt_build_env_cdf(const uint16_t* rgba16f, uint32_t w, uint32_t h, float exposure, float* cdf_out,
+                       double* total_weight);
+/* parseHdr (lib/parse-hdr.js:125-211) + HDRTexture.updateData (tracer.js:76-87): decodes a
+   Radiance RLE RGBE file into w x h rgba16f texels (exposure applied, clamp 65519). Call with
+   rgba16f == NULL to query w and h. */
+int wgpt_decode_rgbe(const uint8_t* file, size_t bytes, float exposure, uint16_t* rgba16f, uint32_t* w,
+                     uint32_t* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WGPT_H */

@@ -1,0 +1,308 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU restatement of the shaders.
+
+The kernels and the oracle evaluate the same operations in the same order with correctly rounded
+IEEE binary32 arithmetic and the same built-in functions, so the expected agreement is exact:
+closest-hit ids, hit distances, normals, per-pixel accumulation and the rgba8 images are
+compared bit for bit.  The tolerances stated by the path's contract (hit t within 1e-5 relative,
+a-trous output within 1e-5 relative) are asserted as well, so a failure reports both.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from webgpuraytracer_b200 import renderer as rd
+from webgpuraytracer_b200 import scene as sc
+from webgpuraytracer_b200 import synth
+from webgpuraytracer_b200._lib import WgptError
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small():
+    s = synth.small_scene(1, 256, 256, 4)
+    return s, sc.pack_scene_data(s)
+
+
+@pytest.fixture(scope="module")
+def flagship():
+    s = synth.flagship_scene(1, 1920, 1080, 8)
+    return s, sc.pack_scene_data(s)
+
+
+def _renderer(scene, packed, w, h, gbuf=False):
+    r = rd.Renderer(w, h)
+    r.set_scene(scene, isgbuf=gbuf, packed=packed)
+    return r
+
+
+def _params(scene, packed, w, h, frame=0, seed=1, section=(0, 0)):
+    scene.camera.aspect = w / h
+    scene.camera.update_rays2()
+    return sc.pack_params(scene, packed, w, h, frame, seed, section)
+
+
+def _oracle_render(packed, params, w, h, first, reps, section=None, counters=None):
+    acc = np.zeros((h, w, 4), np.float32)
+    out = np.zeros((h, w, 4), np.uint8)
+    rc = oracle.render(oracle.OracleScene(packed), params, first, reps, section or (0, 0, w, h), acc, out,
+                       oracle.default_threads(), counters)
+    assert rc == 0
+    return acc, out
+
+
+def _gpu_render(r, params, first, reps, section=None):
+    w, h = r.width, r.height
+    r._check(r.L.wgpt_set_params(r.ctx, rd.ptr(params)), "set_params")
+    sx, sy, sw, sh = section or (0, 0, w, h)
+    r._check(r.L.wgpt_render(r.ctx, first, reps, sx, sy, sw, sh), "render")
+    r.synchronize()
+    return r.read_accum(), r.read_output()
+
+
+def _assert_same(a, b, what):
+    bad = ~((a == b) | (np.isnan(a) & np.isnan(b)))
+    n = int(bad.sum())
+    assert n == 0, f"{what}: {n} of {a.size} values differ; first at {np.argwhere(bad)[:5].tolist()}"
+
+
+def _camera_rays(scene, w, h, n, rng):
+    cam = scene.camera
+    cam.update_rays2()
+    u = rng.random(n)
+    v = rng.random(n)
+    r00, r10, r01, r11 = (np.asarray(x, np.float64) for x in (cam.ray00, cam.ray10, cam.ray01, cam.ray11))
+    d = (r00 * (1 - u[:, None]) + r10 * u[:, None]) * v[:, None] + (r01 * (1 - u[:, None]) + r11 * u[:, None]) * (1 - v[:, None])
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    o = np.repeat(np.asarray(cam.position, np.float64)[None], n, 0)
+    return np.concatenate([o, d], 1).astype(np.float32)
+
+
+def _random_rays(n, rng, box=12.0):
+    o = rng.uniform(-box, box, (n, 3))
+    o[:, 1] = rng.uniform(0.0, 6.0, n)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return np.concatenate([o, d], 1).astype(np.float32)
+
+
+def test_closest_hits_bitexact(flagship):
+    """Closest-hit object/triangle ids, t and normals on camera rays and rays from inside the
+    scene (two-level BVH, spheres, cylinders, tori)."""
+    scene, packed = flagship
+    rng = np.random.default_rng(3)
+    rays = np.concatenate([_camera_rays(scene, 1920, 1080, 40000, rng), _random_rays(40000, rng)])
+    r = _renderer(scene, packed, 64, 64)
+    go, gm, gp, gt, gn = r.trace_rays(rays)
+    oo, om, op, ot, on = oracle.trace_closest(oracle.OracleScene(packed), rays, oracle.default_threads())
+    hit = om >= 0
+    assert hit.mean() > 0.3 and (op >= 0).sum() > 1000, "the ray set must exercise meshes and analytic hits"
+    _assert_same(go, oo, "object index")
+    _assert_same(gm, om, "material index")
+    _assert_same(gp, op, "triangle index")
+    np.testing.assert_allclose(gt[hit], ot[hit], rtol=1e-5, atol=0)
+    _assert_same(gt, ot, "hit t")
+    _assert_same(gn[hit], on[hit], "normal")
+    r.close()
+
+
+def test_small_config_bitexact(small):
+    """256x256, 16 spp, 4 bounces, seed 1: the full small configuration."""
+    scene, packed = small
+    params = _params(scene, packed, 256, 256)
+    acc_o, out_o = _oracle_render(packed, params, 256, 256, 0, 16)
+    r = _renderer(scene, packed, 256, 256)
+    acc_g, out_g = _gpu_render(r, params, 0, 16)
+    _assert_same(acc_g, acc_o, "accumulation")
+    _assert_same(out_g, out_o, "rgba8 output")
+    r.close()
+
+
+def test_flagship_crop_bitexact(flagship):
+    """A 160x120 section of the 1920x1080 frame at 2 spp: meshes, Disney BSDF, env NEE, media."""
+    scene, packed = flagship
+    w, h = 1920, 1080
+    params = _params(scene, packed, w, h, section=(880, 420))
+    sec = (880, 420, 160, 120)
+    acc_o, out_o = _oracle_render(packed, params, w, h, 5, 2, sec)
+    r = _renderer(scene, packed, w, h)
+    acc_g, out_g = _gpu_render(r, params, 5, 2, sec)
+    ys, xs = slice(420, 540), slice(880, 1040)
+    _assert_same(acc_g[ys, xs], acc_o[ys, xs], "accumulation")
+    _assert_same(out_g[ys, xs], out_o[ys, xs], "rgba8 output")
+    assert np.all(acc_g[:420] == 0), "pixels outside the section must stay untouched"
+    r.close()
+
+
+def test_tiles_and_reps_match_one_dispatch(small):
+    """Tiled rendering (render(tsize, reps)) equals one full-frame dispatch with the same frames."""
+    scene, packed = small
+    scene.camera.aspect = 1.0
+    r = _renderer(scene, packed, 256, 256)
+    r.render(tsize=96, reps=3)
+    tiled = r.read_accum()
+    r.resize()
+    params = _params(scene, packed, 256, 256)
+    full, _ = _gpu_render(r, params, 0, 3)
+    _assert_same(tiled, full, "tiled vs full")
+    r.close()
+
+
+def test_counters_match_oracle(flagship):
+    """The device's work counters equal the oracle's instrumented traversal (the roofline
+    numerator)."""
+    scene, packed = flagship
+    w, h = 1920, 1080
+    params = _params(scene, packed, w, h)
+    sec = (600, 300, 128, 96)
+    cnt_o = np.zeros(16, np.uint64)
+    _oracle_render(packed, params, w, h, 0, 1, sec, cnt_o)
+    r = _renderer(scene, packed, w, h)
+    r.set_counting(True)
+    _gpu_render(r, params, 0, 1, sec)
+    cnt_g = r.read_counters()
+    assert cnt_g[0] == 128 * 96
+    np.testing.assert_array_equal(cnt_g[:11], cnt_o[:11])
+    r.close()
+
+
+def test_gbuffer_bitexact(small, flagship):
+    for (scene, packed), (w, h) in ((small, (256, 256)), (flagship, (480, 270))):
+        params = _params(scene, packed, w, h)
+        g_o = np.zeros((h, w, 12), np.float32)
+        img_o = np.zeros((h, w, 4), np.uint8)
+        assert oracle.gbuffer(oracle.OracleScene(packed), params, (0, 0, w, h), g_o, img_o, oracle.default_threads()) == 0
+        r = _renderer(scene, packed, w, h, gbuf=True)
+        r._check(r.L.wgpt_set_params(r.ctx, rd.ptr(params)), "set_params")
+        r._check(r.L.wgpt_render_gbuffer(r.ctx, 0, 0, w, h), "gbuffer")
+        r.synchronize()
+        _assert_same(r.read_gbuffer(), g_o, "gbuffer")
+        _assert_same(r.read_output(), img_o, "gbuffer debug image")
+        r.close()
+
+
+@pytest.mark.parametrize("mode", ["intended", "as_run"])
+def test_denoise_bitexact(small, mode):
+    """prepass + 5 a-trous passes + composite on a 4-spp render of the small scene family, both
+    step schedules; exact and within the 1e-5 relative bar."""
+    scene, packed = small
+    w, h = 480, 270
+    scene.camera.aspect = w / h
+    r = _renderer(scene, packed, w, h, gbuf=True)
+    r.render_gbuffer()
+    r.render(tsize=256, reps=4)
+    color = r.read_accum()
+    gbuf = r.read_gbuffer()
+    u = rd.denoise_uniforms(w, h, passes=5)
+    steps = rd.step_schedule(5, mode)
+    f_o, c_o, o_o = oracle.denoise(color, gbuf, u, steps, oracle.default_threads())
+    r._check(r.L.wgpt_denoise(r.ctx, rd.ptr(u), rd.ptr(steps), 5), "denoise")
+    r.synchronize()
+    f_g = np.empty_like(f_o)
+    c_g = np.empty_like(c_o)
+    r._check(r.L.wgpt_read_denoised(r.ctx, rd.ptr(f_g), rd.ptr(c_g)), "read_denoised")
+    np.testing.assert_allclose(f_g, f_o, rtol=1e-5, atol=1e-7)
+    _assert_same(f_g, f_o, "filtered")
+    _assert_same(c_g, c_o, "composited")
+    _assert_same(r.read_output(), o_o, "rgba8")
+    r.close()
+
+
+def test_denoise_1080p_config(small):
+    """The a-trous configuration at full size: 1920x1080, 4 spp, 5 passes (1,2,4,8,16)."""
+    scene, packed = small
+    w, h = 1920, 1080
+    scene.camera.aspect = w / h
+    r = _renderer(scene, packed, w, h, gbuf=True)
+    r.render_gbuffer()
+    r.render(tsize=1024, reps=4)
+    color, gbuf = r.read_accum(), r.read_gbuffer()
+    u = rd.denoise_uniforms(w, h, passes=5)
+    steps = rd.step_schedule(5, "intended")
+    f_o, c_o, o_o = oracle.denoise(color, gbuf, u, steps, oracle.default_threads())
+    r._check(r.L.wgpt_denoise(r.ctx, rd.ptr(u), rd.ptr(steps), 5), "denoise")
+    r.synchronize()
+    f_g = np.empty_like(f_o)
+    c_g = np.empty_like(c_o)
+    r._check(r.L.wgpt_read_denoised(r.ctx, rd.ptr(f_g), rd.ptr(c_g)), "read_denoised")
+    rel = np.abs(f_g - f_o) / np.maximum(np.abs(f_o), 1e-30)
+    assert float(rel.max()) <= 1e-5
+    _assert_same(c_g, c_o, "composited")
+    _assert_same(r.read_output(), o_o, "rgba8")
+    r.close()
+
+
+def test_resample_bitexact(small):
+    scene, packed = small
+    scene.camera.aspect = 1.0
+    r = _renderer(scene, packed, 256, 256)
+    r.render(tsize=256, reps=2)
+    src = r.read_output()
+    for (dw, dh, rx, ry) in ((256, 256, 0.5, 0.5), (300, 170, 1.0, 1.0), (1000, 900, 0.37, 0.81)):
+        dst_g = r.resample(dw, dh, float(np.float32(rx)), float(np.float32(ry)))
+        dst_o = oracle.resample(src, dw, dh, float(np.float32(rx)), float(np.float32(ry)))
+        _assert_same(dst_g, dst_o, f"resample {dw}x{dh}")
+    r.close()
+
+
+def test_preview_path(small):
+    """renderPreview: reduced-size sample into the canvas buffers, then the blit."""
+    scene, packed = small
+    scene.camera.aspect = 1.0
+    r = _renderer(scene, packed, 256, 256)
+    canvas = r.render_preview(100)
+    pw = ph = 100
+    params = sc.pack_params(scene, packed, pw, ph, 0, 1, (0, 0))
+    acc_o, out_o = _oracle_render(packed, params, pw, ph, 0, 1)
+    src = np.zeros((256, 256, 4), np.uint8)
+    src[:ph, :pw] = out_o
+    dst_o = oracle.resample(src, 256, 256, float(np.float32(pw / 256)), float(np.float32(ph / 256)))
+    _assert_same(canvas, dst_o, "preview canvas")
+    r.close()
+
+
+def _light_scene():
+    s = synth.small_scene(4, 128, 128, 6)
+    lamp = sc.Material("lamp", [1, 0.9, 0.8], 1.0, emittance=[1, 0.9, 0.7], emissionIntensity=6.0)
+    a = s.add(sc.Sphere("lamp0", lamp, 1.5, 3.0, 1.0, 0.6))
+    a.enableNEE = True
+    b = s.add(sc.Cube("lamp1", lamp, -3.0, 2.0, -2.0, -2.2, 2.5, -1.4))
+    b.enableNEE = True
+    t = s.add(sc.Torus("torus", sc.Material("t", [0.7, 0.5, 0.3], 0.3, metallic=0.5), 1.0, 0.3))
+    t.set_position(0.0, -1.0, 0.0)
+    c = sc.Cylinder("cyl", sc.Material("c", [0.3, 0.6, 0.3], 0.6, clearcoat=0.8, sheen=0.5), 0.4)
+    c.position = sc.gm.vec3(2.5, -2.0, 2.0)
+    c.scale = sc.gm.vec3(0.7, 1.5, 0.7)
+    c.rotate(0.4, 1, 0, 0.3)
+    s.add(c)
+    return s
+
+
+def test_lights_and_all_primitives_bitexact():
+    """Explicit light sampling (reservoir over sphere and box lights, MIS on implicit hits) with
+    spheres, cubes, tori, cylinders and the plane."""
+    s = _light_scene()
+    packed = sc.pack_scene_data(s)
+    assert packed.flags & rd.sc.HAS_LIGHTS
+    params = _params(s, packed, 128, 128)
+    acc_o, out_o = _oracle_render(packed, params, 128, 128, 0, 8)
+    r = _renderer(s, packed, 128, 128)
+    acc_g, out_g = _gpu_render(r, params, 0, 8)
+    _assert_same(acc_g, acc_o, "accumulation")
+    _assert_same(out_g, out_o, "rgba8")
+    r.close()
+
+
+def test_upload_rejects_bad_layout(small):
+    scene, packed = small
+    bad = sc.PackedScene(**{**packed.__dict__})
+    tl = packed.tlas.copy().view(np.uint32).reshape(-1, 8)
+    tl[0, 7] = 10_000           # right child of the root far out of range
+    bad.tlas = tl.view(np.uint8).reshape(-1).copy()
+    r = rd.Renderer(16, 16)
+    with pytest.raises(WgptError) as ei:
+        r.set_scene(scene, packed=bad)
+    assert ei.value.code == 2
+    r.close()

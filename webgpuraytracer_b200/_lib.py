@@ -1,0 +1,122 @@
+"""ctypes binding of libwgpt.so (include/wgpt.h).
+
+The library is the product: there is no CPU fallback.  If it is missing or cannot be loaded the
+import raises, naming the build step (webgpuraytracer_b200.build.build()).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libwgpt.so"
+
+WGPT_OK = 0
+STATUS_NAMES = {
+    0: "WGPT_OK", 1: "WGPT_E_INVALID", 2: "WGPT_E_LAYOUT", 3: "WGPT_E_CUDA", 4: "WGPT_E_NOMEM",
+    5: "WGPT_E_STATE", 6: "WGPT_E_UNSUPPORTED", 7: "WGPT_E_REBUILD", 8: "WGPT_E_DEVICE",
+}
+
+# feature flags (pipeline override constants 1..11, shader.wgsl:1-12)
+HAS_SPHERES = 1 << 0
+HAS_CUBES = 1 << 1
+HAS_PLANES = 1 << 2
+HAS_CYLINDERS = 1 << 3
+HAS_TORI = 1 << 4
+HAS_MESHES = 1 << 5
+HAS_LIST_MESHES = 1 << 6
+HAS_HEIGHTMAPS = 1 << 7
+HAS_LIGHTS = 1 << 8
+HAS_SKYBOX = 1 << 9
+MIS_SKYBOX = 1 << 10
+
+
+class Buffer(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("bytes", C.c_size_t)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("materials", Buffer), ("objects", Buffer), ("tlas", Buffer), ("meshes", Buffer), ("bvh", Buffer),
+        ("triangles", Buffer), ("planes", Buffer), ("lights", Buffer), ("sky_cdf", Buffer),
+        ("sky_rgba16f", C.c_void_p), ("sky_width", C.c_uint32), ("sky_height", C.c_uint32),
+        ("bounce_limit", C.c_int32), ("feature_flags", C.c_uint32),
+    ]
+
+
+class WgptError(RuntimeError):
+    def __init__(self, code: int, what: str, msg: str = ""):
+        self.code = code
+        super().__init__(f"{what}: {STATUS_NAMES.get(code, code)}" + (f" ({msg})" if msg else ""))
+
+
+_P = C.c_void_p
+_U32 = C.c_uint32
+_I32 = C.c_int32
+_F = C.c_float
+
+EXPORTS = {
+    "wgpt_abi_version": ([], C.c_int),
+    "wgpt_create": ([C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "wgpt_destroy": ([_P], C.c_int),
+    "wgpt_last_error": ([_P], C.c_char_p),
+    "wgpt_validate_scene": ([C.POINTER(SceneDesc), C.c_char_p, C.c_size_t], C.c_int),
+    "wgpt_upload_scene": ([_P, C.POINTER(SceneDesc)], C.c_int),
+    "wgpt_update_scene": ([_P, C.POINTER(SceneDesc)], C.c_int),
+    "wgpt_resize": ([_P, _U32, _U32, C.c_int], C.c_int),
+    "wgpt_set_params": ([_P, _P], C.c_int),
+    "wgpt_render": ([_P, _U32, _U32, _U32, _U32, _U32, _U32], C.c_int),
+    "wgpt_render_gbuffer": ([_P, _U32, _U32, _U32, _U32], C.c_int),
+    "wgpt_denoise": ([_P, _P, _P, _U32], C.c_int),
+    "wgpt_resample": ([_P, _U32, _U32, _F, _F], C.c_int),
+    "wgpt_synchronize": ([_P], C.c_int),
+    "wgpt_read_accum": ([_P, _P], C.c_int),
+    "wgpt_write_accum": ([_P, _P], C.c_int),
+    "wgpt_read_output": ([_P, _P], C.c_int),
+    "wgpt_read_gbuffer": ([_P, _P], C.c_int),
+    "wgpt_write_gbuffer": ([_P, _P], C.c_int),
+    "wgpt_read_denoised": ([_P, _P, _P], C.c_int),
+    "wgpt_read_canvas": ([_P, _P, _U32, _U32], C.c_int),
+    "wgpt_trace_rays": ([_P, _P, _U32, _P, _P, _P, _P, _P], C.c_int),
+    "wgpt_set_counting": ([_P, C.c_int], C.c_int),
+    "wgpt_read_counters": ([_P, _P], C.c_int),
+    "wgpt_stream": ([_P], C.c_void_p),
+    "wgpt_build_blas": ([_P, _U32, _P, C.POINTER(_U32), _P], C.c_int),
+    "wgpt_build_tlas": ([_P, _U32, _P, C.POINTER(_U32)], C.c_int),
+    "wgpt_build_env_cdf": ([_P, _U32, _U32, _F, _P, C.POINTER(C.c_double)], C.c_int),
+    "wgpt_decode_rgbe": ([_P, C.c_size_t, _F, _P, C.POINTER(_U32), C.POINTER(_U32)], C.c_int),
+}
+
+_lib: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    """Loads libwgpt.so once and declares every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with webgpuraytracer_b200.build.build()")
+    handle = C.CDLL(str(LIB_PATH))
+    for name, (argtypes, restype) in EXPORTS.items():
+        fn = getattr(handle, name)
+        fn.argtypes = argtypes
+        fn.restype = restype
+    _lib = handle
+    return handle
+
+
+def ptr(a) -> int | None:
+    """Address of a contiguous numpy array (or None)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays passed to the library must be C-contiguous"
+    return a.ctypes.data
+
+
+def check(rc: int, what: str, ctx=None) -> None:
+    if rc != WGPT_OK:
+        msg = ""
+        if ctx is not None:
+            raw = lib().wgpt_last_error(ctx)
+            msg = raw.decode() if raw else ""
+        raise WgptError(rc, what, msg)

@@ -1,0 +1,588 @@
+// C ABI of the renderer (include/wgpt.h): context, scene upload with layout validation, image
+// buffers, and the render / G-buffer / denoise / resample entry points.  Each call maps to one
+// step of tracer.js's Renderer or Denoiser (cited per function in wgpt.h).
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+#include <string>
+#include <vector>
+#include <set>
+#include <utility>
+
+#include "../../include/wgpt.h"
+#include "wgpt_internal.h"
+
+struct wgpt_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // scene buffers: 0 materials, 1 objects, 2 tlas, 3 meshes, 4 bvh, 5 triangles, 6 planes,
+  // 7 lights, 8 sky_cdf, 9 sky texels
+  void* d_buf[10] = {nullptr};
+  size_t cap[10] = {0};
+  size_t bytes[10] = {0};
+  wgpt::DeviceScene ds{};
+  bool has_scene = false;
+  // images
+  uint32_t w = 0, h = 0;
+  float* accum = nullptr;
+  uint8_t* out = nullptr;
+  float* gbuf = nullptr;
+  // denoiser
+  float* dn_a = nullptr;
+  float* dn_b = nullptr;
+  float* dn_guide = nullptr;
+  float* dn_comp = nullptr;
+  const float* dn_final = nullptr;
+  // preview canvas
+  uint8_t* canvas = nullptr;
+  uint32_t cw = 0, ch = 0;
+  // params, status, counters
+  wgpt_scene_params params{};
+  bool has_params = false;
+  uint32_t* d_status = nullptr;
+  unsigned long long* d_counters = nullptr;
+  bool counting = false;
+};
+
+namespace {
+
+int fail(wgpt_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(wgpt_ctx* c, cudaError_t e, const char* what) {
+  return fail(c, e == cudaErrorMemoryAllocation ? WGPT_E_NOMEM : WGPT_E_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+  } while (0)
+
+void dfree(void*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+template <typename T>
+void dfree_t(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+const uint32_t kStride[10] = {WGPT_STRIDE_MATERIAL, WGPT_STRIDE_OBJECT, WGPT_STRIDE_NODE, WGPT_STRIDE_MESH_READ,
+                              WGPT_STRIDE_NODE, WGPT_STRIDE_TRIANGLE, WGPT_STRIDE_PLANE, WGPT_STRIDE_LIGHT, 4, 8};
+const char* kName[10] = {"materials", "objects", "tlas", "meshes", "bvh", "triangles", "planes", "lights",
+                         "sky_cdf", "sky"};
+
+struct HostScene {
+  const wgpt_material* mats; uint32_t n_mats;
+  const wgpt_object* objs; uint32_t n_objs;
+  const wgpt_bvh_node* tlas; uint32_t n_tlas;
+  const uint8_t* meshes; uint32_t n_meshes;
+  const wgpt_bvh_node* bvh; uint32_t n_bvh;
+  const wgpt_triangle* tris; uint32_t n_tris;
+  const wgpt_plane* planes; uint32_t n_planes;
+  const wgpt_light* lights; uint32_t n_lights;
+};
+
+constexpr uint32_t kMaxDepth = 62;   // traversal stacks hold 64 entries (shader.wgsl:17)
+
+// A BVH in the reference's DFS layout: left child = index + 1, right child = base + next
+// (strictly after the left child), leaves reference [item_base + next, + count).  Returns an
+// empty string when every reachable node and item is in range and the depth fits the stack.
+std::string check_tree(const wgpt_bvh_node* nodes, uint32_t n_nodes, uint32_t root, uint32_t base,
+                       uint32_t item_base, uint32_t n_items, const char* what) {
+  if (root >= n_nodes) return std::string(what) + ": root node out of range";
+  std::vector<std::pair<uint32_t, uint32_t>> st;
+  st.push_back({root, 0u});
+  char buf[256];
+  while (!st.empty()) {
+    auto [i, d] = st.back();
+    st.pop_back();
+    if (d > kMaxDepth) { snprintf(buf, sizeof buf, "%s: tree deeper than %u levels", what, kMaxDepth); return buf; }
+    const wgpt_bvh_node& nd = nodes[i];
+    if (nd.num_triangles > 0u) {
+      uint64_t start = (uint64_t)item_base + nd.next;
+      if (start + nd.num_triangles > n_items) {
+        snprintf(buf, sizeof buf, "%s: leaf %u references items [%llu, %llu) beyond %u", what, i,
+                 (unsigned long long)start, (unsigned long long)(start + nd.num_triangles), n_items);
+        return buf;
+      }
+    } else {
+      uint64_t l = (uint64_t)i + 1u, r = (uint64_t)base + nd.next;
+      if (l >= n_nodes || r >= n_nodes || r <= i) {
+        snprintf(buf, sizeof buf, "%s: inner node %u has children %llu/%llu outside (%u, %u)", what, i,
+                 (unsigned long long)l, (unsigned long long)r, i, n_nodes);
+        return buf;
+      }
+      st.push_back({(uint32_t)l, d + 1});
+      st.push_back({(uint32_t)r, d + 1});
+    }
+  }
+  return "";
+}
+
+std::string validate(const HostScene& s, uint32_t flags, std::set<std::pair<uint32_t, uint32_t>>& checked) {
+  char buf[256];
+  const uint32_t tlas_flags = WGPT_HAS_SPHERES | WGPT_HAS_CUBES | WGPT_HAS_CYLINDERS | WGPT_HAS_TORI | WGPT_HAS_MESHES;
+  if (s.n_mats == 0) return "materials: at least one material record is required";
+  for (uint32_t i = 0; i < s.n_mats; ++i) {
+    const wgpt_material& m = s.mats[i];
+    if (m.emissive_idx >= 0 || m.albedo_idx >= 0 || m.normal_idx >= 0 || m.height_idx >= 0 ||
+        m.roughness_idx >= 0 || m.metallic_idx >= 0) {
+      snprintf(buf, sizeof buf, "materials[%u]: texture indices are not supported by this build", i);
+      return std::string("U") + buf;
+    }
+  }
+  auto mat_ok = [&](int32_t m) { return m >= -1 && m < (int32_t)s.n_mats; };
+  auto blas_ok = [&](uint32_t node_offset, uint32_t tri_offset, const char* what) -> std::string {
+    if (checked.count({node_offset, tri_offset})) return "";
+    std::string e = check_tree(s.bvh, s.n_bvh, node_offset, node_offset, tri_offset, s.n_tris, what);
+    if (e.empty()) checked.insert({node_offset, tri_offset});
+    return e;
+  };
+  if (flags & tlas_flags) {
+    if (s.n_tlas == 0) return "tlas: empty while object flags are set";
+    std::string e = check_tree(s.tlas, s.n_tlas, 0, 0, 0, s.n_objs, "tlas");
+    if (!e.empty()) return e;
+    for (uint32_t i = 0; i < s.n_objs; ++i) {
+      const wgpt_object& o = s.objs[i];
+      if (!mat_ok(o.material_idx)) { snprintf(buf, sizeof buf, "objects[%u]: material %d out of range", i, o.material_idx); return buf; }
+      if ((flags & WGPT_HAS_LIGHTS) && o.light_idx >= (int32_t)s.n_lights) {
+        snprintf(buf, sizeof buf, "objects[%u]: light %d out of range", i, o.light_idx); return buf;
+      }
+      if (o.object_type == 0 && (flags & WGPT_HAS_MESHES)) {
+        uint32_t no, to;
+        memcpy(&no, &o.param0, 4); memcpy(&to, &o.param1, 4);
+        e = blas_ok(no, to, "bvh");
+        if (!e.empty()) { snprintf(buf, sizeof buf, "objects[%u]: ", i); return buf + e; }
+        if (o.material_idx < 0) { snprintf(buf, sizeof buf, "objects[%u]: mesh without material", i); return buf; }
+      }
+    }
+  }
+  if (flags & WGPT_HAS_LIST_MESHES) {
+    for (uint32_t i = 0; i < s.n_meshes; ++i) {
+      wgpt_mesh_instance mi;
+      memcpy(&mi, s.meshes + (size_t)i * WGPT_STRIDE_MESH_READ, sizeof mi);
+      if (!mat_ok(mi.material_idx)) { snprintf(buf, sizeof buf, "meshes[%u] (80-byte read stride): material %d out of range", i, mi.material_idx); return buf; }
+      std::string e = blas_ok(mi.node_offset, mi.tri_offset, "bvh");
+      if (!e.empty()) { snprintf(buf, sizeof buf, "meshes[%u] (80-byte read stride): ", i); return buf + e; }
+    }
+  }
+  if (flags & WGPT_HAS_PLANES) {
+    for (uint32_t i = 0; i < s.n_planes; ++i)
+      if (!mat_ok(s.planes[i].material_idx)) { snprintf(buf, sizeof buf, "planes[%u]: material out of range", i); return buf; }
+  }
+  if (flags & WGPT_HAS_LIGHTS) {
+    for (uint32_t i = 0; i < s.n_lights; ++i) {
+      int32_t oi = s.lights[i].obj_idx;
+      if (oi >= (int32_t)s.n_objs) { snprintf(buf, sizeof buf, "lights[%u]: object %d out of range", i, oi); return buf; }
+      if (oi >= 0 && s.objs[oi].material_idx < 0) { snprintf(buf, sizeof buf, "lights[%u]: object without material", i); return buf; }
+    }
+  }
+  return "";
+}
+
+int upload_buffers(wgpt_ctx* ctx, const wgpt_scene_desc* d, bool in_place_only) {
+  const wgpt_buffer* src[9] = {&d->materials, &d->objects, &d->tlas, &d->meshes, &d->bvh,
+                               &d->triangles, &d->planes, &d->lights, &d->sky_cdf};
+  size_t sky_bytes = (size_t)d->sky_width * d->sky_height * 8;
+  for (int k = 0; k < 10; ++k) {
+    const void* p = k < 9 ? src[k]->ptr : (const void*)d->sky_rgba16f;
+    size_t n = k < 9 ? src[k]->bytes : sky_bytes;
+    if (n == 0 || p == nullptr) {
+      // empty arrays are bound as one zeroed element (tracer.js:1789, makeBuf minimum sizes)
+      n = kStride[k];
+      p = nullptr;
+    }
+    if (in_place_only) {
+      if (n > ctx->cap[k]) return fail(ctx, WGPT_E_REBUILD, std::string(kName[k]) + ": does not fit the existing buffer");
+    } else if (n > ctx->cap[k]) {
+      dfree(ctx->d_buf[k]);
+      size_t alloc = (n + 255) & ~(size_t)255;
+      CK(cudaMalloc(&ctx->d_buf[k], alloc), "cudaMalloc scene buffer");
+      ctx->cap[k] = alloc;
+    }
+    if (p) {
+      CK(cudaMemcpyAsync(ctx->d_buf[k], p, n, cudaMemcpyHostToDevice, ctx->stream), "upload scene buffer");
+    } else {
+      CK(cudaMemsetAsync(ctx->d_buf[k], 0, n, ctx->stream), "zero scene buffer");
+    }
+    ctx->bytes[k] = n;
+  }
+  // the sources are pageable host memory: the copies above have completed on return, but keep
+  // the contract explicit for callers that free them right after.
+  CK(cudaStreamSynchronize(ctx->stream), "scene upload");
+  return WGPT_OK;
+}
+
+int check_desc(wgpt_ctx* ctx, const wgpt_scene_desc* d, HostScene& hs) {
+  if (!d) return fail(ctx, WGPT_E_INVALID, "scene descriptor is null");
+  const wgpt_buffer* b[9] = {&d->materials, &d->objects, &d->tlas, &d->meshes, &d->bvh,
+                             &d->triangles, &d->planes, &d->lights, &d->sky_cdf};
+  for (int k = 0; k < 9; ++k) {
+    if (b[k]->bytes && !b[k]->ptr) return fail(ctx, WGPT_E_INVALID, std::string(kName[k]) + ": null pointer with nonzero size");
+    uint32_t stride = kStride[k];
+    if (k != 3 && k != 8 && b[k]->bytes % stride != 0)
+      return fail(ctx, WGPT_E_LAYOUT, std::string(kName[k]) + ": size is not a multiple of its record size");
+  }
+  if (d->bounce_limit < 0) return fail(ctx, WGPT_E_INVALID, "bounce_limit must be >= 0");
+  if (d->feature_flags & WGPT_HAS_HEIGHTMAPS) return fail(ctx, WGPT_E_UNSUPPORTED, "HAS_HEIGHTMAPS (parallax maps) is not supported by this build");
+  if (d->feature_flags & ~0x7ffu) return fail(ctx, WGPT_E_INVALID, "unknown feature flag bits");
+  if ((d->feature_flags & WGPT_HAS_SKYBOX) && (!d->sky_rgba16f || d->sky_width == 0 || d->sky_height == 0))
+    return fail(ctx, WGPT_E_INVALID, "sky texture missing while HAS_SKYBOX is set");
+  auto cnt = [&](int k) { return (uint32_t)(b[k]->bytes / kStride[k]); };
+  hs.mats = (const wgpt_material*)b[0]->ptr; hs.n_mats = cnt(0);
+  hs.objs = (const wgpt_object*)b[1]->ptr; hs.n_objs = cnt(1);
+  hs.tlas = (const wgpt_bvh_node*)b[2]->ptr; hs.n_tlas = cnt(2);
+  hs.meshes = (const uint8_t*)b[3]->ptr; hs.n_meshes = cnt(3);
+  hs.bvh = (const wgpt_bvh_node*)b[4]->ptr; hs.n_bvh = cnt(4);
+  hs.tris = (const wgpt_triangle*)b[5]->ptr; hs.n_tris = cnt(5);
+  hs.planes = (const wgpt_plane*)b[6]->ptr; hs.n_planes = cnt(6);
+  hs.lights = (const wgpt_light*)b[7]->ptr; hs.n_lights = cnt(7);
+  std::set<std::pair<uint32_t, uint32_t>> checked;
+  std::string e = validate(hs, d->feature_flags, checked);
+  if (!e.empty()) {
+    if (e[0] == 'U') return fail(ctx, WGPT_E_UNSUPPORTED, e.substr(1));
+    return fail(ctx, WGPT_E_LAYOUT, e);
+  }
+  return WGPT_OK;
+}
+
+void fill_device_scene(wgpt_ctx* ctx, const wgpt_scene_desc* d) {
+  auto cnt = [&](int k) { return (uint32_t)(ctx->bytes[k] / kStride[k]); };
+  wgpt::DeviceScene& s = ctx->ds;
+  s.mats = ctx->d_buf[0]; s.n_mats = cnt(0);
+  s.objs = ctx->d_buf[1]; s.n_objs = cnt(1);
+  s.tlas = ctx->d_buf[2]; s.n_tlas = cnt(2);
+  s.meshes = ctx->d_buf[3]; s.n_meshes = d->meshes.bytes ? (uint32_t)(d->meshes.bytes / WGPT_STRIDE_MESH_READ) : 1u;
+  s.bvh = ctx->d_buf[4]; s.n_bvh = cnt(4);
+  s.tris = ctx->d_buf[5]; s.n_tris = cnt(5);
+  s.planes = ctx->d_buf[6]; s.n_planes = cnt(6);
+  s.lights = ctx->d_buf[7]; s.n_lights = cnt(7);
+  s.cdf = ctx->d_buf[8]; s.n_cdf = cnt(8);
+  s.sky = ctx->d_buf[9];
+  s.sky_w = d->sky_rgba16f ? d->sky_width : 1u;
+  s.sky_h = d->sky_rgba16f ? d->sky_height : 1u;
+  s.bounce_limit = d->bounce_limit;
+  s.flags = d->feature_flags;
+}
+
+int check_section(wgpt_ctx* ctx, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh) {
+  if (ctx->w == 0) return fail(ctx, WGPT_E_STATE, "no image size: call wgpt_resize first");
+  if (!ctx->has_params) return fail(ctx, WGPT_E_STATE, "no scene params: call wgpt_set_params first");
+  // params.width/height may be smaller than the context (renderPreview renders a reduced image
+  // into the canvas-sized buffers); the accumulation is indexed with params.width, the rgba8
+  // image with the context width (the storage texture's row pitch).
+  if (ctx->params.width == 0 || ctx->params.height == 0 || ctx->params.width > ctx->w || ctx->params.height > ctx->h)
+    return fail(ctx, WGPT_E_INVALID, "params width/height must be nonzero and within the context size");
+  if (sw == 0 || sh == 0 || (uint64_t)sx + sw > ctx->params.width || (uint64_t)sy + sh > ctx->params.height)
+    return fail(ctx, WGPT_E_INVALID, "section outside the image");
+  return WGPT_OK;
+}
+
+int check_env(wgpt_ctx* ctx) {
+  const wgpt_scene_params& p = ctx->params;
+  if ((ctx->ds.flags & WGPT_HAS_SKYBOX) && (ctx->ds.flags & WGPT_MIS_SKYBOX)) {
+    if (p.sky_width == 0 || p.sky_height == 0) return fail(ctx, WGPT_E_INVALID, "params sky_width/sky_height are zero");
+    uint64_t last = (uint64_t)p.sky_cdf_index + (uint64_t)(p.sky_height - 1) * (p.sky_width + 1) + p.sky_width - 1;
+    if (p.sky_height > ctx->ds.n_cdf || last >= ctx->ds.n_cdf)
+      return fail(ctx, WGPT_E_LAYOUT, "sky_cdf is smaller than the params' sky_width/sky_height/sky_cdf_index imply");
+  }
+  return WGPT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wgpt_abi_version(void) { return WGPT_ABI_VERSION; }
+
+int wgpt_create(int device, wgpt_ctx** out) {
+  if (!out) return WGPT_E_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return WGPT_E_CUDA;
+  if (device < 0 || device >= n) return WGPT_E_INVALID;
+  wgpt_ctx* ctx = new wgpt_ctx();
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counters, 16 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_counters, 0, 16 * sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    wgpt_destroy(ctx);
+    return WGPT_E_CUDA;
+  }
+  *out = ctx;
+  return WGPT_OK;
+}
+
+int wgpt_destroy(wgpt_ctx* ctx) {
+  if (!ctx) return WGPT_E_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (int k = 0; k < 10; ++k) dfree(ctx->d_buf[k]);
+  dfree_t(ctx->accum); dfree_t(ctx->out); dfree_t(ctx->gbuf);
+  dfree_t(ctx->dn_a); dfree_t(ctx->dn_b); dfree_t(ctx->dn_guide); dfree_t(ctx->dn_comp);
+  dfree_t(ctx->canvas); dfree_t(ctx->d_status); dfree_t(ctx->d_counters);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return WGPT_OK;
+}
+
+const char* wgpt_last_error(const wgpt_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void* wgpt_stream(wgpt_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int wgpt_validate_scene(const wgpt_scene_desc* desc, char* msg, size_t msg_len) {
+  wgpt_ctx tmp;   // host-only: no device state is touched
+  HostScene hs;
+  int rc = check_desc(&tmp, desc, hs);
+  if (msg && msg_len) {
+    snprintf(msg, msg_len, "%s", tmp.err.c_str());
+  }
+  return rc;
+}
+
+int wgpt_upload_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
+  if (!ctx) return WGPT_E_INVALID;
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  HostScene hs;
+  int rc = check_desc(ctx, desc, hs);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->stream), "drain before upload");
+  rc = upload_buffers(ctx, desc, false);
+  if (rc) return rc;
+  fill_device_scene(ctx, desc);
+  ctx->has_scene = true;
+  return WGPT_OK;
+}
+
+int wgpt_update_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (desc && (desc->feature_flags != ctx->ds.flags || desc->bounce_limit != ctx->ds.bounce_limit))
+    return fail(ctx, WGPT_E_REBUILD, "pipeline constants changed: full upload required");
+  HostScene hs;
+  int rc = check_desc(ctx, desc, hs);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->stream), "drain before update");
+  rc = upload_buffers(ctx, desc, true);
+  if (rc) return rc;
+  fill_device_scene(ctx, desc);
+  return WGPT_OK;
+}
+
+int wgpt_resize(wgpt_ctx* ctx, uint32_t width, uint32_t height, int want_gbuf) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (width == 0 || height == 0 || (uint64_t)width * height > (1ull << 28)) return fail(ctx, WGPT_E_INVALID, "bad image size");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "drain before resize");
+  size_t npix = (size_t)width * height;
+  bool same = width == ctx->w && height == ctx->h;
+  if (!same) {
+    dfree_t(ctx->accum); dfree_t(ctx->out); dfree_t(ctx->gbuf);
+    dfree_t(ctx->dn_a); dfree_t(ctx->dn_b); dfree_t(ctx->dn_guide); dfree_t(ctx->dn_comp);
+    ctx->dn_final = nullptr;
+    ctx->w = ctx->h = 0;
+    CK(cudaMalloc(&ctx->accum, npix * 16), "cudaMalloc accum");
+    CK(cudaMalloc(&ctx->out, npix * 4), "cudaMalloc output");
+  }
+  if (want_gbuf && !ctx->gbuf) CK(cudaMalloc(&ctx->gbuf, npix * 48), "cudaMalloc gbuffer");
+  CK(cudaMemsetAsync(ctx->accum, 0, npix * 16, ctx->stream), "clear accum");
+  CK(cudaMemsetAsync(ctx->out, 0, npix * 4, ctx->stream), "clear output");
+  if (want_gbuf) CK(cudaMemsetAsync(ctx->gbuf, 0, npix * 48, ctx->stream), "clear gbuffer");
+  ctx->w = width; ctx->h = height;
+  CK(cudaStreamSynchronize(ctx->stream), "resize");
+  return WGPT_OK;
+}
+
+int wgpt_set_params(wgpt_ctx* ctx, const void* p) {
+  if (!ctx || !p) return WGPT_E_INVALID;
+  memcpy(&ctx->params, p, sizeof(wgpt_scene_params));
+  ctx->has_params = true;
+  return WGPT_OK;
+}
+
+int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
+  int rc = check_section(ctx, sx, sy, sw, sh);
+  if (rc) return rc;
+  rc = check_env(ctx);
+  if (rc) return rc;
+  if (reps == 0) return WGPT_OK;
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::launch_render(ctx->ds, ctx->params, first_frame, reps, sx, sy, sw, sh, ctx->accum, ctx->out, ctx->w,
+                         ctx->d_status, ctx->counting ? ctx->d_counters : nullptr, ctx->stream),
+     "render launch");
+  return WGPT_OK;
+}
+
+int wgpt_render_gbuffer(wgpt_ctx* ctx, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
+  int rc = check_section(ctx, sx, sy, sw, sh);
+  if (rc) return rc;
+  if (!ctx->gbuf) return fail(ctx, WGPT_E_STATE, "no G-buffer: resize with want_gbuf");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::launch_gbuffer(ctx->ds, ctx->params, sx, sy, sw, sh, ctx->gbuf, ctx->out, ctx->w, ctx->d_status,
+                          ctx->stream),
+     "gbuffer launch");
+  return WGPT_OK;
+}
+
+int wgpt_denoise(wgpt_ctx* ctx, const void* uniforms, const uint32_t* steps, uint32_t passes) {
+  if (!ctx || !uniforms || (passes && !steps)) return WGPT_E_INVALID;
+  if (ctx->w == 0) return fail(ctx, WGPT_E_STATE, "no image size");
+  if (!ctx->gbuf) return fail(ctx, WGPT_E_STATE, "no G-buffer: resize with want_gbuf and render it");
+  wgpt_denoise_uniforms u;
+  memcpy(&u, uniforms, sizeof u);
+  if (u.width != ctx->w || u.height != ctx->h) return fail(ctx, WGPT_E_INVALID, "uniform width/height differ from the context size");
+  if (passes > 64) return fail(ctx, WGPT_E_INVALID, "more than 64 passes");
+  for (uint32_t i = 0; i < passes; ++i)
+    if (steps[i] == 0 || steps[i] > (1u << 20)) return fail(ctx, WGPT_E_INVALID, "step width out of range");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  size_t npix = (size_t)ctx->w * ctx->h;
+  if (!ctx->dn_a) {
+    CK(cudaMalloc(&ctx->dn_a, npix * 16), "cudaMalloc denoise A");
+    CK(cudaMalloc(&ctx->dn_b, npix * 16), "cudaMalloc denoise B");
+    CK(cudaMalloc(&ctx->dn_guide, npix * 48), "cudaMalloc denoise guide");
+    CK(cudaMalloc(&ctx->dn_comp, npix * 16), "cudaMalloc denoise composite");
+  }
+  CK(wgpt::launch_denoise(ctx->accum, ctx->gbuf, u, steps, passes, ctx->dn_a, ctx->dn_b, ctx->dn_guide, ctx->dn_comp,
+                          ctx->out, &ctx->dn_final, ctx->stream),
+     "denoise launch");
+  return WGPT_OK;
+}
+
+int wgpt_resample(wgpt_ctx* ctx, uint32_t dst_w, uint32_t dst_h, float rx, float ry) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (ctx->w == 0) return fail(ctx, WGPT_E_STATE, "no image size");
+  if (dst_w == 0 || dst_h == 0 || (uint64_t)dst_w * dst_h > (1ull << 28)) return fail(ctx, WGPT_E_INVALID, "bad canvas size");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (dst_w != ctx->cw || dst_h != ctx->ch) {
+    CK(cudaStreamSynchronize(ctx->stream), "drain before canvas resize");
+    dfree_t(ctx->canvas);
+    CK(cudaMalloc(&ctx->canvas, (size_t)dst_w * dst_h * 4), "cudaMalloc canvas");
+    ctx->cw = dst_w; ctx->ch = dst_h;
+  }
+  CK(wgpt::launch_resample(ctx->out, ctx->w, ctx->h, ctx->canvas, dst_w, dst_h, rx, ry, ctx->stream), "resample launch");
+  return WGPT_OK;
+}
+
+int wgpt_synchronize(wgpt_ctx* ctx) {
+  if (!ctx) return WGPT_E_INVALID;
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "stream synchronize");
+  uint32_t st = 0;
+  CK(cudaMemcpy(&st, ctx->d_status, sizeof st, cudaMemcpyDeviceToHost), "status readback");
+  if (st) {
+    CK(cudaMemset(ctx->d_status, 0, sizeof st), "status reset");
+    return fail(ctx, WGPT_E_DEVICE, "a kernel overflowed its 64-entry traversal stack");
+  }
+  return WGPT_OK;
+}
+
+static int readback(wgpt_ctx* ctx, void* dst, const void* src, size_t n, const char* what) {
+  if (!ctx || !dst) return WGPT_E_INVALID;
+  if (!src) return fail(ctx, WGPT_E_STATE, std::string(what) + ": nothing to read");
+  int rc = wgpt_synchronize(ctx);
+  if (rc) return rc;
+  CK(cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost), what);
+  return WGPT_OK;
+}
+
+int wgpt_read_accum(wgpt_ctx* ctx, float* dst) {
+  if (!ctx) return WGPT_E_INVALID;
+  return readback(ctx, dst, ctx->accum, (size_t)ctx->w * ctx->h * 16, "read accum");
+}
+int wgpt_read_output(wgpt_ctx* ctx, uint8_t* dst) {
+  if (!ctx) return WGPT_E_INVALID;
+  return readback(ctx, dst, ctx->out, (size_t)ctx->w * ctx->h * 4, "read output");
+}
+int wgpt_read_gbuffer(wgpt_ctx* ctx, void* dst) {
+  if (!ctx) return WGPT_E_INVALID;
+  return readback(ctx, dst, ctx->gbuf, (size_t)ctx->w * ctx->h * 48, "read gbuffer");
+}
+int wgpt_read_denoised(wgpt_ctx* ctx, float* filtered, float* composited) {
+  if (!ctx) return WGPT_E_INVALID;
+  size_t n = (size_t)ctx->w * ctx->h * 16;
+  int rc = WGPT_OK;
+  if (filtered) rc = readback(ctx, filtered, ctx->dn_final, n, "read denoised");
+  if (!rc && composited) rc = readback(ctx, composited, ctx->dn_final ? ctx->dn_comp : nullptr, n, "read composited");
+  return rc;
+}
+int wgpt_read_canvas(wgpt_ctx* ctx, uint8_t* dst, uint32_t dst_w, uint32_t dst_h) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (dst_w != ctx->cw || dst_h != ctx->ch) return fail(ctx, WGPT_E_INVALID, "canvas size mismatch");
+  return readback(ctx, dst, ctx->canvas, (size_t)dst_w * dst_h * 4, "read canvas");
+}
+
+int wgpt_write_accum(wgpt_ctx* ctx, const float* src) {
+  if (!ctx || !src) return WGPT_E_INVALID;
+  if (!ctx->accum) return fail(ctx, WGPT_E_STATE, "no image size");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "drain");
+  CK(cudaMemcpy(ctx->accum, src, (size_t)ctx->w * ctx->h * 16, cudaMemcpyHostToDevice), "write accum");
+  return WGPT_OK;
+}
+int wgpt_write_gbuffer(wgpt_ctx* ctx, const void* src) {
+  if (!ctx || !src) return WGPT_E_INVALID;
+  if (!ctx->gbuf) return fail(ctx, WGPT_E_STATE, "no G-buffer");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "drain");
+  CK(cudaMemcpy(ctx->gbuf, src, (size_t)ctx->w * ctx->h * 48, cudaMemcpyHostToDevice), "write gbuffer");
+  return WGPT_OK;
+}
+
+int wgpt_trace_rays(wgpt_ctx* ctx, const float* rays, uint32_t n, int32_t* o_idx, int32_t* m_idx, int32_t* prim,
+                    float* t, float* normal) {
+  if (!ctx || !rays || !o_idx || !m_idx || !prim || !t || !normal) return WGPT_E_INVALID;
+  if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
+  if (n == 0) return WGPT_OK;
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  void* d = nullptr;
+  size_t per = 6 * 4 + 4 + 4 + 4 + 4 + 12;
+  CK(cudaMalloc(&d, (size_t)n * per), "cudaMalloc rays");
+  float* d_rays = (float*)d;
+  int32_t* d_o = (int32_t*)(d_rays + (size_t)n * 6);
+  int32_t* d_m = d_o + n;
+  int32_t* d_p = d_m + n;
+  float* d_t = (float*)(d_p + n);
+  float* d_n = d_t + n;
+  cudaError_t e = cudaMemcpyAsync(d_rays, rays, (size_t)n * 24, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = wgpt::launch_trace_rays(ctx->ds, d_rays, n, d_o, d_m, d_p, d_t, d_n, ctx->d_status, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(o_idx, d_o, (size_t)n * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(m_idx, d_m, (size_t)n * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(prim, d_p, (size_t)n * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(t, d_t, (size_t)n * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(normal, d_n, (size_t)n * 12, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "trace rays");
+  return wgpt_synchronize(ctx);
+}
+
+int wgpt_set_counting(wgpt_ctx* ctx, int on) {
+  if (!ctx) return WGPT_E_INVALID;
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (on && !ctx->counting) CK(cudaMemsetAsync(ctx->d_counters, 0, 16 * sizeof(unsigned long long), ctx->stream), "reset counters");
+  ctx->counting = on != 0;
+  return WGPT_OK;
+}
+
+int wgpt_read_counters(wgpt_ctx* ctx, uint64_t* dst) {
+  if (!ctx) return WGPT_E_INVALID;
+  return readback(ctx, dst, ctx->d_counters, 16 * sizeof(unsigned long long), "read counters");
+}
+
+}  // extern "C"

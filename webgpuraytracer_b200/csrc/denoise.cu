@@ -1,0 +1,210 @@
+// Edge-aware a-trous denoiser (denoiser.wgsl) and the preview resample blit (scale.wgsl).
+//   k_prepass    3x3 luminance median, NaN/Inf sanitising, tonemap, albedo demodulation
+//                (denoiser.wgsl:55-112); also writes the per-pixel guide record that every
+//                a-trous pass reads instead of re-deriving it from the G-buffer 25 times;
+//   k_atrous     one 5x5 B3-spline a-trous pass with colour/normal/depth/albedo/material edge
+//                stops (denoiser.wgsl:117-189);
+//   k_composite  remodulation and the rgba8 store (denoiser.wgsl:194-213);
+//   k_resample   bilinear resample of an rgba8 image (scale.wgsl:6-35).
+// The guide record holds, per pixel, values the reference computes identically for every tap:
+// normal (3), normal length, depth mapped by d/(d+3), tonemapped albedo (3),
+// and (transmission, roughness, metallic) -- 12 floats, so the per-tap arithmetic is unchanged.
+#include <stdint.h>
+#include <cuda_runtime.h>
+#include "wgsl_builtins.h"
+#include "wgpt_internal.h"
+
+using namespace wb;
+
+namespace {
+
+__device__ __forceinline__ v3 tonemap_dn(v3 c, float exposure) {
+  v3 color = c * exposure;
+  color = color / (color + mk3s(0.3f));
+  return vpow(color, 0.4545f);
+}
+__device__ __forceinline__ float lum_dn(float4 c) { return dot(mk3(c.x, c.y, c.z), mk3(0.299f, 0.587f, 0.114f)); }
+
+struct GuidePix { float4 a, b, c; };   // (n.xyz, |n|) (dmap, alb.rgb) (trans, rough, metal, -)
+
+__global__ void __launch_bounds__(256)
+k_prepass(const float4* __restrict__ color, const float* __restrict__ gbuf, wgpt_denoise_uniforms u,
+          float4* __restrict__ out, float4* __restrict__ guide) {
+  int x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 16 + (threadIdx.x >> 4);
+  int W = (int)u.width, H = (int)u.height;
+  if (x >= W || y >= H) return;
+  size_t idx = (size_t)y * W + x;
+  float4 center;
+  if (u.flags & 1u) {
+    float4 cols[9]; float lums[9];
+    int k = 0;
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++) {
+#pragma unroll
+      for (int dx = -1; dx <= 1; dx++) {
+        int cx = min(max(x + dx, 0), W - 1), cy = min(max(y + dy, 0), H - 1);
+        cols[k] = __ldg(color + (size_t)cy * W + cx);
+        lums[k] = lum_dn(cols[k]);
+        k++;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+#pragma unroll
+      for (int j = i + 1; j < 9; j++) {
+        if (lums[j] < lums[i]) {
+          float tl = lums[i]; lums[i] = lums[j]; lums[j] = tl;
+          float4 tc = cols[i]; cols[i] = cols[j]; cols[j] = tc;
+        }
+      }
+    }
+    center = cols[4];
+  } else {
+    center = color[idx];
+  }
+  bool valid = (center.x >= 0.0f && center.y >= 0.0f && center.z >= 0.0f) &&
+               (center.x <= 10000.0f && center.y <= 10000.0f && center.z <= 10000.0f);
+  if (!valid) center = make_float4(0.0f, 0.0f, 0.0f, center.w);
+  v3 mapped = tonemap_dn(mk3(center.x, center.y, center.z), u.exposure);
+  const float* g = gbuf + idx * 12;
+  v3 n = mk3(g[0], g[1], g[2]);
+  float nlen = length(n);
+  bool is_sky = nlen < 0.1f;
+  v3 alb_map = tonemap_dn(mk3(g[4], g[5], g[6]), u.exposure);
+  if ((u.flags & 2u) && !is_sky) {
+    v3 ma = vmax(alb_map, mk3s(0.001f));
+    mapped = mapped / ma;
+    mapped = vmin(vmax(mapped, mk3s(0.0f)), mk3s(10.0f));
+  }
+  out[idx] = make_float4(mapped.x, mapped.y, mapped.z, center.w);
+  float dist = g[11];
+  GuidePix gp;
+  gp.a = make_float4(n.x, n.y, n.z, nlen);
+  gp.b = make_float4(dist / (dist + 3.0f), alb_map.x, alb_map.y, alb_map.z);
+  gp.c = make_float4(g[10], g[3], g[7], 0.0f);
+  guide[idx * 3 + 0] = gp.a; guide[idx * 3 + 1] = gp.b; guide[idx * 3 + 2] = gp.c;
+}
+
+__global__ void __launch_bounds__(256)
+k_atrous(const float4* __restrict__ in, const float4* __restrict__ guide, wgpt_denoise_uniforms u, int step,
+         float4* __restrict__ out) {
+  int x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 16 + (threadIdx.x >> 4);
+  int W = (int)u.width, H = (int)u.height;
+  if (x >= W || y >= H) return;
+  size_t ci = (size_t)y * W + x;
+  float4 cc = __ldg(in + ci);
+  float4 ga = __ldg(guide + ci * 3), gb = __ldg(guide + ci * 3 + 1), gc = __ldg(guide + ci * 3 + 2);
+  v3 c_n = mk3(ga.x, ga.y, ga.z);
+  bool c_nflag = ga.w > 0.1f;
+  float preserve = (1.0f - gc.y) * wmax(gc.z, gc.x);
+  float attenuation = mix(1.0f, 0.0f, preserve * u.glossy_protect);
+  const float sc = u.sigma_color * u.sigma_color + 1e-5f;
+  const float sd = u.sigma_depth * u.sigma_depth + 1e-5f;
+  const float sa = u.sigma_albedo * u.sigma_albedo + 1e-5f;
+  const float sm = u.sigma_material * u.sigma_material + 1e-5f;
+  const float kern[5] = {0.0625f, 0.25f, 0.375f, 0.25f, 0.0625f};
+  float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float sum_w = 0.0f;
+#pragma unroll
+  for (int dy = -2; dy <= 2; dy++) {
+    int sy = min(max(y + dy * step, 0), H - 1);
+#pragma unroll
+    for (int dx = -2; dx <= 2; dx++) {
+      int sx = min(max(x + dx * step, 0), W - 1);
+      size_t si = (size_t)sy * W + sx;
+      float4 s = __ldg(in + si);
+      float4 sa4 = __ldg(guide + si * 3), sb4 = __ldg(guide + si * 3 + 1), sc4 = __ldg(guide + si * 3 + 2);
+      float h = kern[dx + 2] * kern[dy + 2];
+      v3 c_diff = mk3(cc.x, cc.y, cc.z) - mk3(s.x, s.y, s.z);
+      float w_color = exp_(-dot(c_diff, c_diff) / sc);
+      float w_normal = 1.0f;
+      if (c_nflag || sa4.w > 0.1f) {
+        float n_dot = wmax(0.0f, dot(c_n, mk3(sa4.x, sa4.y, sa4.z)));
+        w_normal = pow_(n_dot, u.sigma_normal);
+      }
+      float d_diff = gb.x - sb4.x;
+      float w_depth = exp_(-(d_diff * d_diff) / sd);
+      v3 a_diff = mk3(gb.y, gb.z, gb.w) - mk3(sb4.y, sb4.z, sb4.w);
+      float w_albedo = exp_(-dot(a_diff, a_diff) / sa);
+      v3 m_diff = mk3(gc.x, gc.y, gc.z) - mk3(sc4.x, sc4.y, sc4.z);
+      float w_material = exp_(-dot(m_diff, m_diff) / sm);
+      float weight = h * w_color * w_normal * w_depth * w_albedo * w_material;
+      if (dx != 0 || dy != 0) weight *= attenuation;
+      sum.x = sum.x + s.x * weight; sum.y = sum.y + s.y * weight;
+      sum.z = sum.z + s.z * weight; sum.w = sum.w + s.w * weight;
+      sum_w += weight;
+    }
+  }
+  float d = sum_w + 1e-5f;
+  out[ci] = make_float4(sum.x / d, sum.y / d, sum.z / d, sum.w / d);
+}
+
+__global__ void __launch_bounds__(256)
+k_composite(const float4* __restrict__ in, const float4* __restrict__ guide, wgpt_denoise_uniforms u,
+            float4* __restrict__ composited, uchar4* __restrict__ out) {
+  int x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 16 + (threadIdx.x >> 4);
+  int W = (int)u.width, H = (int)u.height;
+  if (x >= W || y >= H) return;
+  size_t idx = (size_t)y * W + x;
+  float4 c = in[idx];
+  float4 ga = guide[idx * 3], gb = guide[idx * 3 + 1];
+  bool is_sky = ga.w < 0.1f;
+  if ((u.flags & 2u) && !is_sky) {
+    v3 ma = vmax(mk3(gb.y, gb.z, gb.w), mk3s(0.001f));
+    c = make_float4(c.x * ma.x, c.y * ma.y, c.z * ma.z, c.w);
+  }
+  if (composited) composited[idx] = c;
+  out[idx] = make_uchar4((unsigned char)unorm8(c.x), (unsigned char)unorm8(c.y), (unsigned char)unorm8(c.z),
+                         (unsigned char)unorm8(c.w));
+}
+
+__global__ void __launch_bounds__(256)
+k_resample(const uchar4* __restrict__ src, uint32_t sw, uint32_t sh, uchar4* __restrict__ dst, uint32_t dw,
+           uint32_t dh, float rx, float ry) {
+  uint32_t x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 16 + (threadIdx.x >> 4);
+  if (x >= dw || y >= dh) return;
+  float ux = (float)x / (float)dw, uy = (float)y / (float)dh;
+  float spx = ux * rx * (float)sw - 0.5f, spy = uy * ry * (float)sh - 0.5f;
+  float fx = fract(spx), fy = fract(spy);
+  int bx = (int)floorf(spx), by = (int)floorf(spy);
+  int mx = (int)sw - 1, my = (int)sh - 1;
+  auto tl = [&](int tx, int ty) {
+    tx = min(max(tx, 0), mx); ty = min(max(ty, 0), my);
+    uchar4 t = __ldg(src + (size_t)ty * sw + tx);
+    return mk4((float)t.x / 255.0f, (float)t.y / 255.0f, (float)t.z / 255.0f, (float)t.w / 255.0f);
+  };
+  v4 t00 = tl(bx, by), t10 = tl(bx + 1, by), t01 = tl(bx, by + 1), t11 = tl(bx + 1, by + 1);
+  v4 col = vmix4(vmix4(t00, t10, fx), vmix4(t01, t11, fx), fy);
+  dst[(size_t)y * dw + x] = make_uchar4((unsigned char)unorm8(col.x), (unsigned char)unorm8(col.y),
+                                        (unsigned char)unorm8(col.z), 255);
+}
+
+}  // namespace
+
+namespace wgpt {
+
+static inline dim3 grid16(uint32_t w, uint32_t h) { return dim3((w + 15) / 16, (h + 15) / 16); }
+
+cudaError_t launch_denoise(const float* color, const float* gbuf, const wgpt_denoise_uniforms& u,
+                           const uint32_t* steps, uint32_t passes, float* buf_a, float* buf_b, float* guide,
+                           float* composited, uint8_t* out, const float** final_buf, cudaStream_t st) {
+  dim3 g = grid16(u.width, u.height);
+  k_prepass<<<g, 256, 0, st>>>((const float4*)color, gbuf, u, (float4*)buf_a, (float4*)guide);
+  float* in = buf_a;
+  float* ob = buf_b;
+  for (uint32_t i = 0; i < passes; ++i) {
+    k_atrous<<<g, 256, 0, st>>>((const float4*)in, (const float4*)guide, u, (int)steps[i], (float4*)ob);
+    float* t = in; in = ob; ob = t;
+  }
+  k_composite<<<g, 256, 0, st>>>((const float4*)in, (const float4*)guide, u, (float4*)composited, (uchar4*)out);
+  if (final_buf) *final_buf = in;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_resample(const uint8_t* src, uint32_t sw, uint32_t sh, uint8_t* dst, uint32_t dw, uint32_t dh,
+                            float rx, float ry, cudaStream_t st) {
+  k_resample<<<grid16(dw, dh), 256, 0, st>>>((const uchar4*)src, sw, sh, (uchar4*)dst, dw, dh, rx, ry);
+  return cudaGetLastError();
+}
+
+}  // namespace wgpt

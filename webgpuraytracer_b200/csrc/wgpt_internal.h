@@ -1,0 +1,39 @@
+// Internal interfaces between the C ABI (api.cu) and the kernel translation units.
+#pragma once
+#include <stdint.h>
+#include <cuda_runtime.h>
+#include "../../include/wgpt_layout.h"
+
+namespace wgpt {
+
+// Device copies of the scene buffers, in the reference's packed layouts.
+struct DeviceScene {
+  const void* mats; uint32_t n_mats;
+  const void* objs; uint32_t n_objs;
+  const void* tlas; uint32_t n_tlas;
+  const void* meshes; uint32_t n_meshes;   // count at the 80-byte read stride
+  const void* bvh; uint32_t n_bvh;
+  const void* tris; uint32_t n_tris;
+  const void* planes; uint32_t n_planes;
+  const void* lights; uint32_t n_lights;
+  const void* sky; uint32_t sky_w, sky_h;
+  const void* cdf; uint32_t n_cdf;
+  int32_t bounce_limit;
+  uint32_t flags;
+};
+
+cudaError_t launch_render(const DeviceScene& d, const wgpt_scene_params& q, uint32_t first_frame, uint32_t reps,
+                          uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh, float* accum, uint8_t* out,
+                          uint32_t out_pitch, uint32_t* status, unsigned long long* counters, cudaStream_t st);
+cudaError_t launch_gbuffer(const DeviceScene& d, const wgpt_scene_params& q, uint32_t sx, uint32_t sy, uint32_t sw,
+                           uint32_t sh, float* gbuf, uint8_t* out, uint32_t out_pitch, uint32_t* status,
+                           cudaStream_t st);
+cudaError_t launch_trace_rays(const DeviceScene& d, const float* rays, uint32_t n, int32_t* o_idx, int32_t* m_idx,
+                              int32_t* prim, float* t, float* normal, uint32_t* status, cudaStream_t st);
+cudaError_t launch_denoise(const float* color, const float* gbuf, const wgpt_denoise_uniforms& u,
+                           const uint32_t* steps, uint32_t passes, float* buf_a, float* buf_b, float* guide,
+                           float* composited, uint8_t* out, const float** final_buf, cudaStream_t st);
+cudaError_t launch_resample(const uint8_t* src, uint32_t sw, uint32_t sh, uint8_t* dst, uint32_t dw, uint32_t dh,
+                            float rx, float ry, cudaStream_t st);
+
+}  // namespace wgpt

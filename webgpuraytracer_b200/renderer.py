@@ -1,0 +1,264 @@
+"""Renderer and Denoiser over libwgpt.so, mirroring tracer.js's classes of the same names.
+
+    Renderer.set_scene      setScene       (tracer.js:1955-2102)
+    Renderer.update_objects updateObjects  (tracer.js:2132-2164)
+    Renderer.resize         resize         (tracer.js:2166-2205)
+    Renderer.update_uniforms updateUniforms (tracer.js:2207-2240)
+    Renderer.render         render         (tracer.js:2242-2297), tile by tile
+    Renderer.render_preview renderPreview  (tracer.js:2334-2392), with the scale.wgsl blit
+    Denoiser.execute        execute        (tracer.js:2583-2637)
+
+Device work goes through the C ABI only; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import scene as sc
+from ._lib import SceneDesc, Buffer, check, lib, ptr
+
+
+def _buf(a: np.ndarray | None) -> Buffer:
+    if a is None or a.size == 0:
+        return Buffer(None, 0)
+    return Buffer(ptr(a), a.nbytes)
+
+
+def scene_desc(p: sc.PackedScene) -> SceneDesc:
+    d = SceneDesc()
+    d.materials = _buf(p.materials)
+    d.objects = _buf(p.objects)
+    d.tlas = _buf(p.tlas)
+    d.meshes = _buf(p.meshes)
+    d.bvh = _buf(p.bvh)
+    d.triangles = _buf(p.triangles)
+    d.planes = _buf(p.planes)
+    d.lights = _buf(p.lights)
+    d.sky_cdf = _buf(p.sky_cdf)
+    d.sky_rgba16f = ptr(p.sky)
+    d.sky_width = p.sky_width
+    d.sky_height = p.sky_height
+    d.bounce_limit = p.bounce_limit
+    d.feature_flags = p.flags
+    return d
+
+
+class Renderer:
+    def __init__(self, width: int, height: int, device: int = 0, seed_fn=None):
+        self.width, self.height = int(width), int(height)
+        self.L = lib()
+        h = C.c_void_p()
+        check(self.L.wgpt_create(device, C.byref(h)), "wgpt_create")
+        self.ctx = h
+        self.scene: sc.Scene | None = None
+        self.packed: sc.PackedScene | None = None
+        self.frame = 0
+        self.isgbuf = False
+        # the reference draws a fresh Math.random() seed per dispatch; tests pin it
+        self.seed_fn = seed_fn or (lambda: 1)
+        self.section = (0, 0, self.width, self.height)
+
+    # -- lifetime
+    def close(self):
+        if self.ctx:
+            self.L.wgpt_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        check(rc, what, self.ctx)
+
+    # -- scene
+    def set_scene(self, scene: sc.Scene, isgbuf: bool = False, packed: sc.PackedScene | None = None):
+        self.scene = scene
+        self.isgbuf = isgbuf
+        self.packed = packed if packed is not None else sc.pack_scene_data(scene)
+        self._desc = scene_desc(self.packed)
+        self._check(self.L.wgpt_upload_scene(self.ctx, C.byref(self._desc)), "upload_scene")
+        self.resize()
+
+    def update_objects(self):
+        """Fast path when everything fits and the flags are unchanged, else a full set_scene."""
+        packed = sc.pack_scene_data(self.scene)
+        desc = scene_desc(packed)
+        rc = self.L.wgpt_update_scene(self.ctx, C.byref(desc))
+        if rc == 7:   # WGPT_E_REBUILD
+            self.set_scene(self.scene, self.isgbuf, packed)
+            return
+        self._check(rc, "update_scene")
+        self.packed, self._desc = packed, desc
+
+    def resize(self, width: int | None = None, height: int | None = None):
+        if width is not None:
+            self.width, self.height = int(width), int(height)
+        self._check(self.L.wgpt_resize(self.ctx, self.width, self.height, 1 if self.isgbuf else 0), "resize")
+        self.reset()
+
+    def reset(self):
+        self.frame = 0
+
+    # -- dispatch
+    def update_uniforms(self, frame: int | None = None, section=(0, 0)):
+        cam = self.scene.camera
+        cam.update_rays2()
+        params = sc.pack_params(self.scene, self.packed, self.width, self.height,
+                                self.frame if frame is None else frame, self.seed_fn(), section)
+        self._params = params
+        self._check(self.L.wgpt_set_params(self.ctx, ptr(params)), "set_params")
+        return params
+
+    def render_section(self, first_frame: int, reps: int, x: int, y: int, w: int, h: int):
+        self.update_uniforms(first_frame, (x, y))
+        self._check(self.L.wgpt_render(self.ctx, first_frame, reps, x, y, w, h), "render")
+
+    def render(self, tsize: int = 256, reps: int = 1, sync: bool = True):
+        """Tiled progressive render: every tile gets `reps` samples (frames frame..frame+reps-1)."""
+        start = self.frame
+        tiles_x = math.ceil(self.width / tsize)
+        tiles_y = math.ceil(self.height / tsize)
+        for ty in range(tiles_y):
+            for tx in range(tiles_x):
+                left, top = tx * tsize, ty * tsize
+                w = min(tsize, self.width - left)
+                h = min(tsize, self.height - top)
+                self.section = (left, top, w, h)
+                self.render_section(start, reps, left, top, w, h)
+        if sync:
+            self.synchronize()
+        self.frame = start + reps
+
+    def render_gbuffer(self):
+        self.update_uniforms(self.frame, (0, 0))
+        self._check(self.L.wgpt_render_gbuffer(self.ctx, 0, 0, self.width, self.height), "render_gbuffer")
+        self.synchronize()
+
+    def render_preview(self, preview_size: float) -> np.ndarray:
+        """renderPreview (tracer.js:2334-2392) at a given preview size: one sample of the reduced
+        pWidth x pHeight image into the canvas-sized buffers, then the scale.wgsl blit to the
+        canvas.  Returns the canvas image (rgba8)."""
+        cw, ch = self.width, self.height
+        maxsize = math.floor(preview_size)
+        scale = min(maxsize / cw, maxsize / ch)
+        pw, ph = int(math.floor(cw * scale)), int(math.floor(ch * scale))
+        self.scene.camera.update_rays2()
+        params = sc.pack_params(self.scene, self.packed, pw, ph, self.frame, self.seed_fn(), (0, 0))
+        self._params = params
+        self._check(self.L.wgpt_set_params(self.ctx, ptr(params)), "set_params")
+        self._check(self.L.wgpt_render(self.ctx, self.frame, 1, 0, 0, pw, ph), "render")
+        rx = float(np.float32(pw / cw))
+        ry = float(np.float32(ph / ch))
+        canvas = self.resample(cw, ch, rx, ry)
+        self.frame += 1
+        return canvas
+
+    def synchronize(self):
+        self._check(self.L.wgpt_synchronize(self.ctx), "synchronize")
+
+    # -- readback
+    def read_accum(self) -> np.ndarray:
+        a = np.empty((self.height, self.width, 4), dtype=np.float32)
+        self._check(self.L.wgpt_read_accum(self.ctx, ptr(a)), "read_accum")
+        return a
+
+    def write_accum(self, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        self._check(self.L.wgpt_write_accum(self.ctx, ptr(a)), "write_accum")
+
+    def read_output(self) -> np.ndarray:
+        a = np.empty((self.height, self.width, 4), dtype=np.uint8)
+        self._check(self.L.wgpt_read_output(self.ctx, ptr(a)), "read_output")
+        return a
+
+    def read_gbuffer(self) -> np.ndarray:
+        a = np.empty((self.height, self.width, 12), dtype=np.float32)
+        self._check(self.L.wgpt_read_gbuffer(self.ctx, ptr(a)), "read_gbuffer")
+        return a
+
+    def write_gbuffer(self, g: np.ndarray):
+        g = np.ascontiguousarray(g, dtype=np.float32)
+        self._check(self.L.wgpt_write_gbuffer(self.ctx, ptr(g)), "write_gbuffer")
+
+    def trace_rays(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        n = rays.shape[0]
+        o = np.empty(n, np.int32)
+        m = np.empty(n, np.int32)
+        p = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        nn = np.empty((n, 3), np.float32)
+        self._check(self.L.wgpt_trace_rays(self.ctx, ptr(rays), n, ptr(o), ptr(m), ptr(p), ptr(t), ptr(nn)),
+                    "trace_rays")
+        return o, m, p, t, nn
+
+    def set_counting(self, on: bool):
+        self._check(self.L.wgpt_set_counting(self.ctx, 1 if on else 0), "set_counting")
+
+    def read_counters(self) -> np.ndarray:
+        a = np.zeros(16, dtype=np.uint64)
+        self._check(self.L.wgpt_read_counters(self.ctx, ptr(a)), "read_counters")
+        return a
+
+    def stream_handle(self) -> int:
+        return int(self.L.wgpt_stream(self.ctx) or 0)
+
+    def resample(self, dst_w: int, dst_h: int, rx: float, ry: float) -> np.ndarray:
+        self._check(self.L.wgpt_resample(self.ctx, dst_w, dst_h, rx, ry), "resample")
+        out = np.empty((dst_h, dst_w, 4), dtype=np.uint8)
+        self._check(self.L.wgpt_read_canvas(self.ctx, ptr(out), dst_w, dst_h), "read_canvas")
+        return out
+
+
+def denoise_uniforms(width, height, passes=4, sigma_color=0.30, sigma_normal=128.0, sigma_depth=0.2,
+                     sigma_albedo=0.07, sigma_material=0.07, glossy_protect=0.75, exposure=1.0,
+                     use_median=True, use_demodulate=True, step_width=1) -> np.ndarray:
+    """Denoiser.updateUniforms (tracer.js:2560-2581) with the constructor defaults (2424-2435)."""
+    u = np.zeros(12, dtype=np.uint32)
+    f = u.view(np.float32)
+    u[0], u[1], u[2], u[3] = width, height, step_width, passes
+    f[4], f[5], f[6], f[7], f[8], f[9], f[10] = (sigma_color, sigma_normal, sigma_depth, sigma_albedo,
+                                                 sigma_material, glossy_protect, exposure)
+    u[11] = (1 if use_median else 0) | (2 if use_demodulate else 0)
+    return u.view(np.uint8).copy()
+
+
+def step_schedule(passes: int, mode: str = "intended") -> np.ndarray:
+    """Step widths per a-trous pass.  "intended": 1, 2, 4, ... (tracer.js:2603 computes 1 << i);
+    "as_run": every pass sees 2^(passes-1), because all queue.writeBuffer calls land before the
+    single submit (tracer.js:2605 + 2636)."""
+    if mode == "intended":
+        return np.array([1 << i for i in range(passes)], dtype=np.uint32)
+    if mode == "as_run":
+        return np.full(passes, 1 << (passes - 1) if passes else 1, dtype=np.uint32)
+    raise ValueError(mode)
+
+
+class Denoiser:
+    """tracer.js:2418-2638"""
+
+    def __init__(self, renderer: Renderer, passes: int = 4, mode: str = "intended", **params):
+        self.r = renderer
+        self.passes = passes
+        self.mode = mode
+        self.params = params
+        self.exposure = renderer.scene.camera.exposure if renderer.scene else 1.0
+
+    def execute(self):
+        u = denoise_uniforms(self.r.width, self.r.height, self.passes, exposure=self.exposure, **self.params)
+        steps = step_schedule(self.passes, self.mode)
+        self.r._check(self.r.L.wgpt_denoise(self.r.ctx, ptr(u), ptr(steps), self.passes), "denoise")
+        self.r.synchronize()
+
+    def read(self):
+        n = self.r.width * self.r.height
+        filt = np.empty((self.r.height, self.r.width, 4), dtype=np.float32)
+        comp = np.empty((self.r.height, self.r.width, 4), dtype=np.float32)
+        self.r._check(self.r.L.wgpt_read_denoised(self.r.ctx, ptr(filt), ptr(comp)), "read_denoised")
+        return filt, comp, self.r.read_output()

@@ -141,13 +141,13 @@ int wgpt_build_blas(const float* tris24, uint32_t n, wgpt_bvh_node* nodes_out, u
    min xyz then max xyz).  Writes up to 2n-1 nodes; *n_nodes receives the count. */
 int wgpt_build_tlas(const float* aabbs6, uint32_t n, wgpt_bvh_node* nodes_out, uint32_t* n_nodes);
 /* HDRTexture.buildHDRCDF (tracer.js:135-204) over w x h rgba16f texels: writes (h+1) + h(w+1)
-   floats and the total weight (sky_total_lum). */
-int wgpt_build_env_cdf(const uint16_t* rgba16f, uint32_t w, uint32_t h, float exposure, float* cdf_out,
+   floats and the total weight (sky_total_lum).  exposure is a JavaScript number (double). */
+int wgpt_build_env_cdf(const uint16_t* rgba16f, uint32_t w, uint32_t h, double exposure, float* cdf_out,
                        double* total_weight);
 /* parseHdr (lib/parse-hdr.js:125-211) + HDRTexture.updateData (tracer.js:76-87): decodes a
    Radiance RLE RGBE file into w x h rgba16f texels (exposure applied, clamp 65519). Call with
    rgba16f == NULL to query w and h. */
-int wgpt_decode_rgbe(const uint8_t* file, size_t bytes, float exposure, uint16_t* rgba16f, uint32_t* w,
+int wgpt_decode_rgbe(const uint8_t* file, size_t bytes, double exposure, uint16_t* rgba16f, uint32_t* w,
                      uint32_t* h);
 
 #ifdef __cplusplus

@@ -98,7 +98,7 @@ def test_closest_hits_bitexact(flagship):
     go, gm, gp, gt, gn = r.trace_rays(rays)
     oo, om, op, ot, on = oracle.trace_closest(oracle.OracleScene(packed), rays, oracle.default_threads())
     hit = om >= 0
-    assert hit.mean() > 0.3 and (op >= 0).sum() > 1000, "the ray set must exercise meshes and analytic hits"
+    assert hit.mean() > 0.15 and (op >= 0).sum() > 1000, "the ray set must exercise meshes and analytic hits"
     _assert_same(go, oo, "object index")
     _assert_same(gm, om, "material index")
     _assert_same(gp, op, "triangle index")

@@ -1,0 +1,219 @@
+"""The native scene builders of libwgpt.so against their Python restatements (oracle/host_oracle.py)
+and against the properties the traversal relies on."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import host_oracle as ho
+from webgpuraytracer_b200 import glmat as gm
+from webgpuraytracer_b200 import scene as sc
+from webgpuraytracer_b200 import synth
+from webgpuraytracer_b200._lib import check, lib, ptr
+
+
+def native_blas(t24):
+    n = len(t24)
+    nodes = np.zeros((2 * n - 1, 32), np.uint8)
+    tris = np.zeros((n, 128), np.uint8)
+    cnt = C.c_uint32(0)
+    check(lib().wgpt_build_blas(ptr(np.ascontiguousarray(t24, np.float32)), n, ptr(nodes), C.byref(cnt), ptr(tris)), "blas")
+    return nodes[: cnt.value].reshape(-1), tris
+
+
+def _mesh_tris(sub, seed):
+    verts, faces = synth.icosphere(sub)
+    rng = np.random.default_rng(seed)
+    verts = verts * (1 + 0.1 * rng.uniform(-1, 1, (len(verts), 1)))
+    md = sc.ModelData("m", verts.astype(np.float32), verts.astype(np.float32),
+                      np.zeros((len(verts), 2), np.float32), faces)
+    return md.triangles24()
+
+
+@pytest.mark.parametrize("t24", [
+    _mesh_tris(2, 1),                                                  # 320 triangles
+    _mesh_tris(3, 2),                                                  # 1280 triangles
+    np.random.default_rng(5).uniform(-1, 1, (300, 24)).astype(np.float32),   # triangle soup
+    np.tile(np.random.default_rng(6).uniform(-1, 1, (1, 24)), (40, 1)).astype(np.float32),  # identical triangles
+    np.concatenate([np.zeros((50, 9)), np.random.default_rng(7).uniform(0, 1, (50, 15))], 1).astype(np.float32),  # degenerate
+    np.random.default_rng(8).uniform(-1, 1, (2, 24)).astype(np.float32),
+])
+def test_blas_matches_restatement(t24):
+    nodes, tris = native_blas(t24)
+    ref_nodes, order = ho.blas_build(t24)
+    np.testing.assert_array_equal(nodes, ho.nodes_to_bytes(ref_nodes))
+    flat = tris.view(np.float32).reshape(-1, 32)
+    want = t24[order]
+    np.testing.assert_array_equal(flat[:, [0, 1, 2, 4, 5, 6, 8, 9, 10]], want[:, :9])
+    np.testing.assert_array_equal(flat[:, [12, 13, 14, 16, 17, 18, 20, 21, 22]], want[:, 9:18])
+    np.testing.assert_array_equal(flat[:, 24:30], want[:, 18:24])
+
+
+def test_blas_structure_full_size():
+    """81,920-triangle mesh: every triangle in exactly one leaf, children inside parents, DFS
+    layout (left = index + 1, right > left)."""
+    md = synth.flagship_mesh(6)
+    nodes = md.nodes.view(np.uint32).reshape(-1, 8)
+    f = md.nodes.view(np.float32).reshape(-1, 8)
+    n_tri = len(md.flat_triangles)
+    assert n_tri == 81920
+    leaves = nodes[:, 3] > 0
+    covered = np.zeros(n_tri, np.int64)
+    for i in np.nonzero(leaves)[0]:
+        covered[nodes[i, 7]:nodes[i, 7] + nodes[i, 3]] += 1
+    assert np.all(covered == 1)
+    inner = np.nonzero(~leaves)[0]
+    right = nodes[inner, 7]
+    assert np.all(right > inner + 1) and np.all(right < len(nodes))
+    for child in (inner + 1, right):
+        assert np.all(f[child, 0:3] >= f[inner, 0:3]) and np.all(f[child, 4:7] <= f[inner, 4:7])
+    tv = md.flat_triangles.view(np.float32).reshape(-1, 32)
+    for i in np.nonzero(leaves)[0][:2000]:
+        s, c = nodes[i, 7], nodes[i, 3]
+        v = tv[s:s + c][:, [0, 1, 2, 4, 5, 6, 8, 9, 10]].reshape(-1, 3)
+        assert np.all(v >= f[i, 0:3]) and np.all(v <= f[i, 4:7])
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 7, 64, 96, 200])
+def test_tlas_matches_restatement(n):
+    rng = np.random.default_rng(n)
+    lo = rng.uniform(-10, 10, (n, 3)).astype(np.float32)
+    hi = (lo + rng.uniform(0.1, 3, (n, 3))).astype(np.float32)
+    if n >= 7:
+        lo[3] = lo[1]
+        hi[3] = hi[1]       # tied centres exercise the stable sort
+    aabbs = np.ascontiguousarray(np.concatenate([lo, hi], 1), np.float32)
+    nodes = np.zeros((2 * n - 1, 32), np.uint8)
+    cnt = C.c_uint32(0)
+    check(lib().wgpt_build_tlas(ptr(aabbs), n, ptr(nodes), C.byref(cnt)), "tlas")
+    np.testing.assert_array_equal(nodes[: cnt.value].reshape(-1), ho.tlas_build(aabbs))
+
+
+def test_tlas_deep_leaf_quirk():
+    """Below depth 20 the median split stops and a leaf keeps every remaining object while
+    pointing at the first one's index (tracer.js:1553-1556)."""
+    n = 3_000_000 // 1000  # small n never reaches depth 21
+    aabbs = np.zeros((n, 6), np.float32)
+    aabbs[:, 3:] = 1
+    nodes = np.zeros((2 * n - 1, 32), np.uint8)
+    cnt = C.c_uint32(0)
+    check(lib().wgpt_build_tlas(ptr(aabbs), n, ptr(nodes), C.byref(cnt)), "tlas")
+    u = nodes[: cnt.value].view(np.uint32).reshape(-1, 8)
+    assert u[u[:, 3] > 0, 3].max() == 1
+
+
+def native_cdf(data16, w, h, exposure):
+    cdf = np.zeros((h + 1) + h * (w + 1), np.float32)
+    tot = C.c_double(0)
+    check(lib().wgpt_build_env_cdf(ptr(data16), w, h, exposure, ptr(cdf), C.byref(tot)), "cdf")
+    return cdf, tot.value
+
+
+@pytest.mark.parametrize("w,h,exposure", [(1, 1, 1.0), (16, 8, 1.0), (64, 32, 2.5), (7, 13, 0.3)])
+def test_env_cdf_matches_restatement(w, h, exposure):
+    rng = np.random.default_rng(w * h)
+    img = np.ones((h, w, 4))
+    img[..., :3] = np.minimum(rng.exponential(1.0, (h, w, 3)) * np.where(rng.random((h, w, 1)) < 0.02, 5e4, 1.0), 6e4)
+    data16 = np.ascontiguousarray(img.astype(np.float16).view(np.uint16).reshape(-1))
+    cdf, tot = native_cdf(data16, w, h, exposure)
+    ref, idx, rtot = ho.env_cdf(data16, w, h, exposure)
+    np.testing.assert_array_equal(cdf, ref)
+    assert tot == rtot and idx == h + 1
+    assert np.all(np.diff(cdf[: h + 1]) >= 0) and abs(float(cdf[h]) - 1.0) < 1e-6
+
+
+def test_env_cdf_black_rows_are_uniform():
+    w, h = 8, 4
+    data16 = np.zeros(w * h * 4, np.uint16)
+    cdf, tot = native_cdf(data16, w, h, 1.0)
+    assert tot == 0.0
+    np.testing.assert_array_equal(cdf[1:h + 1], np.float32(np.arange(1, h + 1) / h))
+
+
+def native_decode(b, exposure=1.0):
+    L = lib()
+    buf = np.frombuffer(b, np.uint8)
+    w, h = C.c_uint32(0), C.c_uint32(0)
+    check(L.wgpt_decode_rgbe(ptr(buf), buf.size, exposure, None, C.byref(w), C.byref(h)), "decode")
+    out = np.zeros(w.value * h.value * 4, np.uint16)
+    check(L.wgpt_decode_rgbe(ptr(buf), buf.size, exposure, ptr(out), C.byref(w), C.byref(h)), "decode")
+    return out, w.value, h.value
+
+
+def test_rgbe_decode_matches_restatement():
+    img = synth.procedural_sky(128, 64)
+    b = synth.encode_rgbe(img)
+    out, w, h = native_decode(b, 1.0)
+    ref, rw, rh = ho.decode_rgbe(b, 1.0)
+    assert (w, h) == (rw, rh) == (128, 64)
+    np.testing.assert_array_equal(out, ref)
+    dec = out.view(np.float16).astype(np.float32).reshape(h, w, 4)[..., :3]
+    # RGBE keeps ~8 bits of mantissa; parse-hdr divides by 255 (no +0.5), so it reads low
+    assert np.all(dec <= img * 1.01 + 1e-6) and np.all(dec >= img * 0.98 - 1e-3)
+    assert abs(float(dec.max()) - float(img.max())) / float(img.max()) < 0.01
+
+
+def test_flagship_sky_has_the_sun():
+    sky = synth.procedural_sky()
+    assert sky.shape == (1024, 2048, 3) and sky.max() == np.float32(5e4)
+    tex = synth.flagship_sky()
+    v = tex.data.view(np.float16).astype(np.float32).reshape(1024, 2048, 4)
+    assert 4.9e4 < v.max() < 5.1e4 and tex.width == 2048 and tex.height == 1024
+
+
+def test_rgbe_decode_clamps_like_update_data():
+    img = np.full((2, 4, 3), 1e6, np.float32)
+    out, w, h = native_decode(synth.encode_rgbe(img), 1.0)
+    vals = out.view(np.float16).astype(np.float32).reshape(h, w, 4)
+    assert np.all(vals[..., :3] == 65504.0) and np.all(vals[..., 3] == 1.0)
+
+
+def test_rgbe_decode_reference_asset():
+    """The reference ships a 2048x1024 sky; decode it both ways where the file is present."""
+    p = Path("/root/reference/assets/noon_sky.hdr")
+    if not p.exists():
+        pytest.skip("reference assets are not present on this host")
+    b = p.read_bytes()
+    out, w, h = native_decode(b)
+    ref, rw, rh = ho.decode_rgbe(b)
+    assert (w, h) == (rw, rh)
+    np.testing.assert_array_equal(out, ref)
+
+
+def test_rgbe_rejects_flat_header():
+    with pytest.raises(Exception):
+        native_decode(b"#?RADIANCE\n\n-Y 2 +X 2\n" + bytes(16))
+
+
+def test_glmatrix_known_answers():
+    q = gm.quat_set_axis_angle(gm.vec3_normalize([1, 2, 3]), 0.7)
+    m = gm.mat4_from_rts(q, [1, -2, 3], [0.5, 2.0, 1.5])
+    inv = gm.mat4_invert(m)
+    prod = m.reshape(4, 4).T.astype(np.float64) @ inv.reshape(4, 4).T.astype(np.float64)
+    np.testing.assert_allclose(prod, np.eye(4), atol=2e-6)
+    assert m.dtype == np.float32 and inv.dtype == np.float32
+    np.testing.assert_array_equal(gm.quat_rotation_to([0, 1, 0], [0, 1, 0]), [0, 0, 0, 1])
+    n = gm.vec3_transform_quat([0, 1, 0], gm.quat_rotation_to([0, 1, 0], gm.vec3_normalize([1, 1, 0])))
+    np.testing.assert_allclose(n, np.float32([0.70710677, 0.70710677, 0]), atol=1e-7)
+
+
+def test_packed_layout_offsets():
+    """Material, object and plane records land at the WGSL struct offsets."""
+    s = synth.small_scene(1, 32, 32, 4)
+    p = sc.pack_scene_data(s)
+    mats = p.materials.view(np.float32).reshape(-1, 36)
+    ints = p.materials.view(np.int32).reshape(-1, 36)
+    m0 = s.get_materials()[0]
+    np.testing.assert_array_equal(mats[0, 0:3], np.float32([c ** 2.2 for c in m0.color]))
+    assert np.all(ints[:, 23:29] == -1)          # emissive..metallic texture indices
+    assert np.all(mats[:, 30:32] == 1.0)   # uv_scale
+    obj = p.objects.view(np.int32).reshape(-1, 24)
+    assert list(obj[:, 18]) == [1] * 5 + [2] * 2  # object_type at byte 72
+    of = p.objects.view(np.float32).reshape(-1, 24)
+    np.testing.assert_array_equal(of[0, 20:23], s.objects[0].position)   # world_position at 80
+    pl = p.planes.view(np.float32).reshape(-1, 8)
+    np.testing.assert_allclose(pl[0, 0:3], [0, 1, 0])
+    assert p.flags & sc.HAS_SKYBOX and not p.flags & sc.MIS_SKYBOX

@@ -82,8 +82,8 @@ EXPORTS = {
     "wgpt_stream": ([_P], C.c_void_p),
     "wgpt_build_blas": ([_P, _U32, _P, C.POINTER(_U32), _P], C.c_int),
     "wgpt_build_tlas": ([_P, _U32, _P, C.POINTER(_U32)], C.c_int),
-    "wgpt_build_env_cdf": ([_P, _U32, _U32, _F, _P, C.POINTER(C.c_double)], C.c_int),
-    "wgpt_decode_rgbe": ([_P, C.c_size_t, _F, _P, C.POINTER(_U32), C.POINTER(_U32)], C.c_int),
+    "wgpt_build_env_cdf": ([_P, _U32, _U32, C.c_double, _P, C.POINTER(C.c_double)], C.c_int),
+    "wgpt_decode_rgbe": ([_P, C.c_size_t, C.c_double, _P, C.POINTER(_U32), C.POINTER(_U32)], C.c_int),
 }
 
 _lib: C.CDLL | None = None

@@ -251,7 +251,7 @@ int wgpt_build_tlas(const float* aabbs6, uint32_t n, wgpt_bvh_node* nodes_out, u
   return WGPT_OK;
 }
 
-int wgpt_build_env_cdf(const uint16_t* data, uint32_t width, uint32_t height, float exposure_f, float* cdf,
+int wgpt_build_env_cdf(const uint16_t* data, uint32_t width, uint32_t height, double exposure_f, float* cdf,
                        double* total_weight) {
   if (!data || !cdf || width == 0 || height == 0) return WGPT_E_INVALID;
   const double exposure = exposure_f;
@@ -292,7 +292,7 @@ int wgpt_build_env_cdf(const uint16_t* data, uint32_t width, uint32_t height, fl
   return WGPT_OK;
 }
 
-int wgpt_decode_rgbe(const uint8_t* buf, size_t len, float exposure_f, uint16_t* out, uint32_t* w_out, uint32_t* h_out) {
+int wgpt_decode_rgbe(const uint8_t* buf, size_t len, double exposure_f, uint16_t* out, uint32_t* w_out, uint32_t* h_out) {
   if (!buf || !w_out || !h_out) return WGPT_E_INVALID;
   size_t off = 0;
   auto read_line = [&]() {

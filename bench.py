@@ -35,7 +35,8 @@ WIDTH, HEIGHT, BOUNCES, SPP = 1920, 1080, 8, 64
 METRIC = "paths/s (1920x1080, 8 bounces)"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
-# Algorithmic bytes per counted unit (counters of wgpt_read_counters):
+# Algorithmic bytes per counted unit (counter slots of wgpt_read_counters): what the reference's
+# algorithm must read or write per unit of work, independent of how it is laid out.
 BYTES_PER_UNIT = {
     3: 32,    # BVH node popped (two 16-byte vectors)
     4: 32,    # child AABB tested
@@ -47,10 +48,22 @@ BYTES_PER_UNIT = {
     11: 32,   # hit attributes of the winning primitive (normals)
 }
 PIXEL_BYTES = 16 + 16 + 4   # accumulation read + write, rgba8 store
+STAGES = ["raygen_or_megakernel", "extend (closest hit)", "shade", "resolve (shadow rays + accumulate)"]
+KERNELS = ["k_wf_raygen", "k_wf_extend", "k_wf_shade", "k_wf_resolve"]
 
 
 def algorithmic_bytes(counters: np.ndarray, pixels: int) -> float:
     return float(sum(int(counters[k]) * b for k, b in BYTES_PER_UNIT.items()) + pixels * PIXEL_BYTES)
+
+
+def stage_bytes(stage_counters: np.ndarray, pixels: int, megakernel: bool) -> list[float]:
+    """Algorithmic bytes per stage; the accumulation traffic belongs to the stage that writes it."""
+    out = []
+    for st in range(4):
+        c = stage_counters[st]
+        px = pixels if (st == 3 or (st == 0 and megakernel)) else 0
+        out.append(algorithmic_bytes(c, px))
+    return out
 
 
 def load_peaks() -> tuple[dict, str]:
@@ -214,6 +227,7 @@ def run_ours(args):
     scene, packed = build_workload()
     r = rd.Renderer(WIDTH, HEIGHT, device=local, seed_fn=lambda: 1 + rank)
     r.set_scene(scene, packed=packed)
+    r._check(r.L.wgpt_set_render_mode(r.ctx, 0 if args.mode == "wavefront" else 1), "render mode")
     stream = torch.cuda.ExternalStream(r.stream_handle(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
     scene.camera.update_rays2()
@@ -230,7 +244,9 @@ def run_ours(args):
     for i in range(args.warmup):
         launch(i)
     r.synchronize()
-    # device-resident timing: one event pair per step, L2 flushed between steps
+    # device-resident timing: one event pair per step, L2 flushed between steps; the library
+    # records an event pair around every stage launch on the same stream
+    r._check(r.L.wgpt_set_stage_timing(r.ctx, 1), "stage timing")
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     sampler = ClockSampler(local)
@@ -249,6 +265,10 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier(world)
     clocks = sampler.stop()
+    stage_ms = np.zeros(4, np.float64)
+    stage_launches = np.zeros(4, np.uint32)
+    r._check(r.L.wgpt_read_stage_times(r.ctx, rd.ptr(stage_ms), rd.ptr(stage_launches)), "stage times")
+    r._check(r.L.wgpt_set_stage_timing(r.ctx, 0), "stage timing")
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     dev_s = sum(step_ms) / 1e3
     dev_s_max = max_over_ranks(dev_s, world)
@@ -271,13 +291,26 @@ def run_ours(args):
     for i in range(args.steps):
         launch(args.warmup + i)
     cnt = r.read_counters()
+    stage_cnt = np.zeros(64, np.uint64)
+    r._check(r.L.wgpt_read_stage_counters(r.ctx, rd.ptr(stage_cnt)), "stage counters")
+    stage_cnt = stage_cnt.reshape(4, 16)
     r.set_counting(False)
-    launches = args.steps
-    bytes_per_launch = algorithmic_bytes(cnt, WIDTH * HEIGHT * args.steps) / launches
-    avg_launch_s = dev_s / launches
+    mega = args.mode == "megakernel"
+    sbytes = stage_bytes(stage_cnt, WIDTH * HEIGHT * args.steps, mega)
+    dom = int(np.argmax(stage_ms))
+    launches = int(stage_launches.sum())
+    bytes_per_launch = sbytes[dom] / max(1, int(stage_launches[dom]))
+    avg_launch_s = stage_ms[dom] / 1e3 / max(1, int(stage_launches[dom]))
     peaks, peak_kind = load_peaks()
     achieved = bytes_per_launch / avg_launch_s / 1e9
     rays = int(cnt[1] + cnt[2])
+    stages = {}
+    for st in range(4):
+        if stage_launches[st]:
+            t = stage_ms[st] / 1e3
+            stages[("k_render" if mega else KERNELS[st])] = {
+                "launches": int(stage_launches[st]), "ms_total": float(stage_ms[st]),
+                "share": float(stage_ms[st] / stage_ms.sum()), "algorithmic_GBps": sbytes[st] / t / 1e9 if t else None}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -292,16 +325,20 @@ def run_ours(args):
             "config": {"workload": "flagship 1920x1080, 8 bounces, 64 instances x 81,920-tri BLAS + 32 prims, "
                                    "2048x1024 RGBE env with importance sampling",
                        "step": "one progressive frame: 1 path per pixel (2,073,600 paths)",
-                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"},
+                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}",
+                       "render_mode": args.mode},
             "rays_per_s": rays * world / dev_s_max,
             "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": 112,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 4},
             "gpu_launches": launches,
+            "stages": stages,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
-                         "kernel": "k_render", "algorithmic_bytes_per_launch": bytes_per_launch},
+                         "kernel": "k_render" if mega else KERNELS[dom],
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "note": "scene (~80 MB) is L2-resident; traversal is latency/divergence bound"},
             "counters_per_step": {"paths": int(cnt[0]) // args.steps, "ext_rays": int(cnt[1]) // args.steps,
                                   "shadow_rays": int(cnt[2]) // args.steps, "nodes": int(cnt[3]) // args.steps,
                                   "tri_tests": int(cnt[5]) // args.steps},
@@ -325,6 +362,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["wavefront", "megakernel"], default="wavefront")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -89,6 +89,14 @@ int wgpt_set_params(wgpt_ctx* ctx, const void* scene_params_112);
 int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sec_x, uint32_t sec_y,
                 uint32_t sec_w, uint32_t sec_h);
 
+/* How wgpt_render runs a sample: WGPT_MODE_WAVEFRONT (default) splits each bounce into closest-
+   hit, shading and shadow/accumulate kernels over compacted path queues (path state in a
+   context-owned buffer of about 440 bytes per pixel); WGPT_MODE_MEGAKERNEL runs one thread per
+   path through all bounces, like the reference's single compute entry point.  Both produce
+   identical results. */
+enum { WGPT_MODE_WAVEFRONT = 0, WGPT_MODE_MEGAKERNEL = 1 };
+int wgpt_set_render_mode(wgpt_ctx* ctx, int mode);
+
 /* setScene(scene, true) + render(): one dispatch of gbuf_main (shader.wgsl:2510-2603) into the
    G-buffer and the debug quadrant image. */
 int wgpt_render_gbuffer(wgpt_ctx* ctx, uint32_t sec_x, uint32_t sec_y, uint32_t sec_w, uint32_t sec_h);
@@ -127,6 +135,15 @@ int wgpt_trace_rays(wgpt_ctx* ctx, const float* rays, uint32_t n, int32_t* o_idx
    11 hit-attribute evaluations, 12-15 reserved (zero). */
 int wgpt_set_counting(wgpt_ctx* ctx, int on);
 int wgpt_read_counters(wgpt_ctx* ctx, uint64_t* dst16);
+
+/* The same counters split by stage (4 x 16 u64: 0 ray generation or the single kernel,
+   1 closest hit, 2 shading, 3 shadow rays and accumulation). */
+int wgpt_read_stage_counters(wgpt_ctx* ctx, uint64_t* dst64);
+
+/* CUDA-event timing of every stage launch queued while timing is on; wgpt_read_stage_times
+   returns the summed milliseconds and launch counts per stage (as above) and restarts. */
+int wgpt_set_stage_timing(wgpt_ctx* ctx, int on);
+int wgpt_read_stage_times(wgpt_ctx* ctx, double* ms4, uint32_t* launches4);
 
 /* The context's cudaStream_t (as void*) for callers that time or order work around it. */
 void* wgpt_stream(wgpt_ctx* ctx);

@@ -306,3 +306,20 @@ def test_upload_rejects_bad_layout(small):
         r.set_scene(scene, packed=bad)
     assert ei.value.code == 2
     r.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_both_render_modes_match_oracle(flagship, mode):
+    """The wavefront (0) and single-kernel (1) forms of main agree with the oracle bit for bit."""
+    scene, packed = flagship
+    w, h = 1920, 1080
+    params = _params(scene, packed, w, h, section=(300, 500))
+    sec = (300, 500, 200, 96)
+    acc_o, out_o = _oracle_render(packed, params, w, h, 11, 2, sec)
+    r = _renderer(scene, packed, w, h)
+    r._check(r.L.wgpt_set_render_mode(r.ctx, mode), "mode")
+    acc_g, out_g = _gpu_render(r, params, 11, 2, sec)
+    ys, xs = slice(500, 596), slice(300, 500)
+    _assert_same(acc_g[ys, xs], acc_o[ys, xs], f"accumulation (mode {mode})")
+    _assert_same(out_g[ys, xs], out_o[ys, xs], f"rgba8 (mode {mode})")
+    r.close()

@@ -16,6 +16,9 @@ STATUS_NAMES = {
     5: "WGPT_E_STATE", 6: "WGPT_E_UNSUPPORTED", 7: "WGPT_E_REBUILD", 8: "WGPT_E_DEVICE",
 }
 
+MODE_WAVEFRONT = 0
+MODE_MEGAKERNEL = 1
+
 # feature flags (pipeline override constants 1..11, shader.wgsl:1-12)
 HAS_SPHERES = 1 << 0
 HAS_CUBES = 1 << 1
@@ -77,8 +80,12 @@ EXPORTS = {
     "wgpt_read_denoised": ([_P, _P, _P], C.c_int),
     "wgpt_read_canvas": ([_P, _P, _U32, _U32], C.c_int),
     "wgpt_trace_rays": ([_P, _P, _U32, _P, _P, _P, _P, _P], C.c_int),
+    "wgpt_set_render_mode": ([_P, C.c_int], C.c_int),
     "wgpt_set_counting": ([_P, C.c_int], C.c_int),
     "wgpt_read_counters": ([_P, _P], C.c_int),
+    "wgpt_read_stage_counters": ([_P, _P], C.c_int),
+    "wgpt_set_stage_timing": ([_P, C.c_int], C.c_int),
+    "wgpt_read_stage_times": ([_P, _P, _P], C.c_int),
     "wgpt_stream": ([_P], C.c_void_p),
     "wgpt_build_blas": ([_P, _U32, _P, C.POINTER(_U32), _P], C.c_int),
     "wgpt_build_tlas": ([_P, _U32, _P, C.POINTER(_U32)], C.c_int),

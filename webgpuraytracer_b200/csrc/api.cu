@@ -43,6 +43,12 @@ struct wgpt_ctx {
   uint32_t* d_status = nullptr;
   unsigned long long* d_counters = nullptr;
   bool counting = false;
+  // wavefront path state (scratch sized for the whole image)
+  int mode = WGPT_MODE_WAVEFRONT;
+  wgpt::StageTimer* timer = nullptr;
+  bool timing = false;
+  void* wf_scratch = nullptr;
+  uint32_t wf_capacity = 0;
 };
 
 namespace {
@@ -314,8 +320,8 @@ int wgpt_create(int device, wgpt_ctx** out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counters, 16 * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMemset(ctx->d_counters, 0, 16 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counters, 64 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_counters, 0, 64 * sizeof(unsigned long long));
   if (e != cudaSuccess) {
     wgpt_destroy(ctx);
     return WGPT_E_CUDA;
@@ -331,7 +337,12 @@ int wgpt_destroy(wgpt_ctx* ctx) {
   for (int k = 0; k < 10; ++k) dfree(ctx->d_buf[k]);
   dfree_t(ctx->accum); dfree_t(ctx->out); dfree_t(ctx->gbuf);
   dfree_t(ctx->dn_a); dfree_t(ctx->dn_b); dfree_t(ctx->dn_guide); dfree_t(ctx->dn_comp);
-  dfree_t(ctx->canvas); dfree_t(ctx->d_status); dfree_t(ctx->d_counters);
+  dfree_t(ctx->canvas); dfree_t(ctx->d_status); dfree_t(ctx->d_counters); dfree(ctx->wf_scratch);
+  if (ctx->timer) {
+    if (ctx->timer->ready)
+      for (int i = 0; i < wgpt::StageTimer::kMaxEvents; ++i) cudaEventDestroy(ctx->timer->ev[i]);
+    delete ctx->timer;
+  }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return WGPT_OK;
@@ -421,9 +432,27 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
   if (rc) return rc;
   if (reps == 0) return WGPT_OK;
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-  CK(wgpt::launch_render(ctx->ds, ctx->params, first_frame, reps, sx, sy, sw, sh, ctx->accum, ctx->out, ctx->w,
-                         ctx->d_status, ctx->counting ? ctx->d_counters : nullptr, ctx->stream),
-     "render launch");
+  unsigned long long* cnt = ctx->counting ? ctx->d_counters : nullptr;
+  wgpt::StageTimer* tm = ctx->timing ? ctx->timer : nullptr;
+  if (ctx->mode == WGPT_MODE_MEGAKERNEL) {
+    if (tm) tm->begin(0, ctx->stream);
+    CK(wgpt::launch_render(ctx->ds, ctx->params, first_frame, reps, sx, sy, sw, sh, ctx->accum, ctx->out, ctx->w,
+                           ctx->d_status, cnt, ctx->stream),
+       "render launch");
+    if (tm) tm->end(0, ctx->stream);
+    return WGPT_OK;
+  }
+  uint32_t need = ctx->w * ctx->h;
+  if (ctx->wf_capacity < need) {
+    CK(cudaStreamSynchronize(ctx->stream), "drain before path-state allocation");
+    dfree(ctx->wf_scratch);
+    ctx->wf_capacity = 0;
+    CK(cudaMalloc(&ctx->wf_scratch, wgpt::wavefront_scratch_bytes(need)), "cudaMalloc path state");
+    ctx->wf_capacity = need;
+  }
+  CK(wgpt::launch_render_wavefront(ctx->ds, ctx->params, first_frame, reps, sx, sy, sw, sh, ctx->accum, ctx->out,
+                                   ctx->w, ctx->wf_scratch, ctx->wf_capacity, ctx->d_status, cnt, ctx->stream, tm),
+     "wavefront render launch");
   return WGPT_OK;
 }
 
@@ -572,17 +601,63 @@ int wgpt_trace_rays(wgpt_ctx* ctx, const float* rays, uint32_t n, int32_t* o_idx
   return wgpt_synchronize(ctx);
 }
 
+int wgpt_set_render_mode(wgpt_ctx* ctx, int mode) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (mode != WGPT_MODE_WAVEFRONT && mode != WGPT_MODE_MEGAKERNEL) return fail(ctx, WGPT_E_INVALID, "unknown render mode");
+  ctx->mode = mode;
+  return WGPT_OK;
+}
+
 int wgpt_set_counting(wgpt_ctx* ctx, int on) {
   if (!ctx) return WGPT_E_INVALID;
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-  if (on && !ctx->counting) CK(cudaMemsetAsync(ctx->d_counters, 0, 16 * sizeof(unsigned long long), ctx->stream), "reset counters");
+  if (on && !ctx->counting) CK(cudaMemsetAsync(ctx->d_counters, 0, 64 * sizeof(unsigned long long), ctx->stream), "reset counters");
   ctx->counting = on != 0;
   return WGPT_OK;
 }
 
 int wgpt_read_counters(wgpt_ctx* ctx, uint64_t* dst) {
+  if (!ctx || !dst) return WGPT_E_INVALID;
+  uint64_t all[64];
+  int rc = readback(ctx, all, ctx->d_counters, sizeof all, "read counters");
+  if (rc) return rc;
+  for (int k = 0; k < 16; ++k) dst[k] = all[k] + all[16 + k] + all[32 + k] + all[48 + k];
+  return WGPT_OK;
+}
+
+int wgpt_read_stage_counters(wgpt_ctx* ctx, uint64_t* dst64) {
   if (!ctx) return WGPT_E_INVALID;
-  return readback(ctx, dst, ctx->d_counters, 16 * sizeof(unsigned long long), "read counters");
+  return readback(ctx, dst64, ctx->d_counters, 64 * sizeof(unsigned long long), "read stage counters");
+}
+
+int wgpt_set_stage_timing(wgpt_ctx* ctx, int on) {
+  if (!ctx) return WGPT_E_INVALID;
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (on && !ctx->timer) {
+    ctx->timer = new wgpt::StageTimer();
+    for (int i = 0; i < wgpt::StageTimer::kMaxEvents; ++i) CK(cudaEventCreate(&ctx->timer->ev[i]), "cudaEventCreate");
+    ctx->timer->ready = true;
+  }
+  if (ctx->timer) ctx->timer->used = 0;
+  ctx->timing = on != 0;
+  return WGPT_OK;
+}
+
+int wgpt_read_stage_times(wgpt_ctx* ctx, double* ms4, uint32_t* launches4) {
+  if (!ctx || !ms4 || !launches4) return WGPT_E_INVALID;
+  for (int k = 0; k < 4; ++k) { ms4[k] = 0; launches4[k] = 0; }
+  if (!ctx->timer) return WGPT_OK;
+  int rc = wgpt_synchronize(ctx);
+  if (rc) return rc;
+  for (int i = 0; i + 1 < ctx->timer->used; i += 2) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->timer->ev[i], ctx->timer->ev[i + 1]), "cudaEventElapsedTime");
+    int stg = ctx->timer->stage_of[i / 2];
+    ms4[stg] += ms;
+    launches4[stg] += 1;
+  }
+  ctx->timer->used = 0;
+  return WGPT_OK;
 }
 
 }  // extern "C"

@@ -72,13 +72,13 @@ struct Counters {
   __device__ __forceinline__ void add(int k, uint32_t n = 1) { if (COUNT) v[k] += n; }
 };
 
-__device__ __forceinline__ bool HAS(const DScene& s, uint32_t f) { return (s.flags & f) != 0u; }
-__device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
-__device__ __forceinline__ v3 f3(float4 a) { return mk3(a.x, a.y, a.z); }
-__device__ __forceinline__ int32_t bi(float f) { return __float_as_int(f); }
-__device__ __forceinline__ uint32_t bu(float f) { return __float_as_uint(f); }
+static __device__ __forceinline__ bool HAS(const DScene& s, uint32_t f) { return (s.flags & f) != 0u; }
+static __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
+static __device__ __forceinline__ v3 f3(float4 a) { return mk3(a.x, a.y, a.z); }
+static __device__ __forceinline__ int32_t bi(float f) { return __float_as_int(f); }
+static __device__ __forceinline__ uint32_t bu(float f) { return __float_as_uint(f); }
 
-__device__ __forceinline__ m4 load_m4(const float4* p) {
+static __device__ __forceinline__ m4 load_m4(const float4* p) {
   m4 m;
   float4 a = ld4(p), b = ld4(p + 1), c = ld4(p + 2), d = ld4(p + 3);
   m.c[0] = mk4(a.x, a.y, a.z, a.w); m.c[1] = mk4(b.x, b.y, b.z, b.w);
@@ -92,7 +92,7 @@ struct DMat {
       sheen_tint, clearcoat, clearcoat_gloss, clearcoat_ior, transmission, concentration;
   v3 subsurface_tint; float subsurface; v3 emittance;
 };
-__device__ __forceinline__ DMat load_mat(const DScene& s, int32_t i) {
+static __device__ __forceinline__ DMat load_mat(const DScene& s, int32_t i) {
   const float4* p = s.mats + (size_t)i * 9;
   float4 a = ld4(p), b = ld4(p + 1), c = ld4(p + 2), d = ld4(p + 3), e = ld4(p + 4), f = ld4(p + 5);
   DMat m;
@@ -104,12 +104,12 @@ __device__ __forceinline__ DMat load_mat(const DScene& s, int32_t i) {
   m.emittance = mk3(f.x, f.y, f.z);
   return m;
 }
-__device__ __forceinline__ v3 load_mat_emittance(const DScene& s, int32_t i) {
+static __device__ __forceinline__ v3 load_mat_emittance(const DScene& s, int32_t i) {
   return f3(ld4(s.mats + (size_t)i * 9 + 5));
 }
 
 // ------------------------------------------------------------------------ sky and env CDF
-__device__ __forceinline__ v4 sky_texel(const DScene& s, int x, int y) {
+static __device__ __forceinline__ v4 sky_texel(const DScene& s, int x, int y) {
   uint2 t = __ldg(s.sky + (size_t)y * s.sky_w + x);
   __half2 lo = *reinterpret_cast<__half2*>(&t.x);
   __half2 hi = *reinterpret_cast<__half2*>(&t.y);
@@ -118,7 +118,7 @@ __device__ __forceinline__ v4 sky_texel(const DScene& s, int x, int y) {
 }
 // Linear filter with clamp-to-edge addressing, in FP32.
 template <bool COUNT>
-__device__ v3 sky_bilinear(const DScene& s, v2 uv, Counters<COUNT>& cn) {
+static __device__ v3 sky_bilinear(const DScene& s, v2 uv, Counters<COUNT>& cn) {
   cn.add(C_SKY_TEXELS, 4);
   float fx = uv.x * (float)s.sky_w - 0.5f;
   float fy = uv.y * (float)s.sky_h - 0.5f;
@@ -135,7 +135,7 @@ __device__ v3 sky_bilinear(const DScene& s, v2 uv, Counters<COUNT>& cn) {
 
 // shader.wgsl:176-188
 template <bool COUNT>
-__device__ v3 sample_sky(const DScene& s, v3 dir, Counters<COUNT>& cn) {
+static __device__ v3 sample_sky(const DScene& s, v3 dir, Counters<COUNT>& cn) {
   float phi = atan2_(dir.z, dir.x);
   float theta = asin_(clamp(dir.y, -1.0f, 1.0f));
   return sky_bilinear(s, mk2(0.5f + phi / TWO_PI, 0.5f - theta / PI), cn);
@@ -143,7 +143,7 @@ __device__ v3 sample_sky(const DScene& s, v3 dir, Counters<COUNT>& cn) {
 
 // shader.wgsl:192-206
 template <bool COUNT>
-__device__ __forceinline__ uint32_t binary_search_cdf(const DScene& s, uint32_t offset, uint32_t size, float targ, Counters<COUNT>& cn) {
+static __device__ __forceinline__ uint32_t binary_search_cdf(const DScene& s, uint32_t offset, uint32_t size, float targ, Counters<COUNT>& cn) {
   uint32_t low = 0u, high = size;
   while (low < high) {
     uint32_t mid = low + (high - low) / 2u;
@@ -156,7 +156,7 @@ __device__ __forceinline__ uint32_t binary_search_cdf(const DScene& s, uint32_t 
 
 // shader.wgsl:208-229
 template <bool COUNT>
-__device__ float get_sky_pdf(const DScene& s, const DParams& p, v3 dir, Counters<COUNT>& cn) {
+static __device__ float get_sky_pdf(const DScene& s, const DParams& p, v3 dir, Counters<COUNT>& cn) {
   float phi = atan2_(dir.z, dir.x);
   float theta = acos_(clamp(dir.y, -1.0f, 1.0f));
   float u = (phi + PI) / (2.0f * PI);
@@ -172,7 +172,7 @@ struct LightSample { v3 dir; v3 color; float dist; float pdf; };
 
 // shader.wgsl:231-254
 template <bool COUNT>
-__device__ LightSample sample_env_cdf(const DScene& s, const DParams& p, float ux, float uy, Counters<COUNT>& cn) {
+static __device__ LightSample sample_env_cdf(const DScene& s, const DParams& p, float ux, float uy, Counters<COUNT>& cn) {
   LightSample samp;
   uint32_t v_idx = binary_search_cdf(s, 0u, p.sky_height, uy, cn);
   uint32_t row_offset = p.sky_cdf_index + (v_idx * (p.sky_width + 1u));
@@ -202,7 +202,7 @@ struct HitRec {
 
 // shader.wgsl:256-265.  IEEE fminf/fmaxf: the sign of a zero result can differ from WGSL's
 // min/max, but every consumer only compares the result, where +0 == -0.
-__device__ __forceinline__ float intersect_aabb(v3 o, v3 inv, float4 lo, float4 hi) {
+static __device__ __forceinline__ float intersect_aabb(v3 o, v3 inv, float4 lo, float4 hi) {
   float t0x = (lo.x - o.x) * inv.x, t0y = (lo.y - o.y) * inv.y, t0z = (lo.z - o.z) * inv.z;
   float t1x = (hi.x - o.x) * inv.x, t1y = (hi.y - o.y) * inv.y, t1z = (hi.z - o.z) * inv.z;
   float t_near = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
@@ -212,7 +212,7 @@ __device__ __forceinline__ float intersect_aabb(v3 o, v3 inv, float4 lo, float4 
 }
 
 // shader.wgsl:267-288 (hit distance and barycentrics only)
-__device__ __forceinline__ bool intersect_triangle(const Ray& r, float4 a, float4 b, float4 c, float* t_out, float* u_out, float* v_out) {
+static __device__ __forceinline__ bool intersect_triangle(const Ray& r, float4 a, float4 b, float4 c, float* t_out, float* u_out, float* v_out) {
   v3 v0 = f3(a);
   v3 edge1 = f3(b) - v0;
   v3 edge2 = f3(c) - v0;
@@ -232,7 +232,7 @@ __device__ __forceinline__ bool intersect_triangle(const Ray& r, float4 a, float
 }
 
 // shader.wgsl:290-300
-__device__ __forceinline__ float hit_unit_sphere(const Ray& r) {
+static __device__ __forceinline__ float hit_unit_sphere(const Ray& r) {
   float a = dot(r.direction, r.direction);
   float half_b = dot(r.origin, r.direction);
   float cc = dot(r.origin, r.origin) - 1.0f;
@@ -245,7 +245,7 @@ __device__ __forceinline__ float hit_unit_sphere(const Ray& r) {
 }
 
 // shader.wgsl:302-312
-__device__ __forceinline__ float hit_unit_cube(const Ray& r) {
+static __device__ __forceinline__ float hit_unit_cube(const Ray& r) {
   v3 inv = 1.0f / r.direction;
   float t0x = (-1.0f - r.origin.x) * inv.x, t0y = (-1.0f - r.origin.y) * inv.y, t0z = (-1.0f - r.origin.z) * inv.z;
   float t1x = (1.0f - r.origin.x) * inv.x, t1y = (1.0f - r.origin.y) * inv.y, t1z = (1.0f - r.origin.z) * inv.z;
@@ -256,7 +256,7 @@ __device__ __forceinline__ float hit_unit_cube(const Ray& r) {
 }
 
 // shader.wgsl:323-379
-__device__ bool hit_cylinder(const Ray& r, float r0, float r1, float* t_out, v3* n_out) {
+static __device__ bool hit_cylinder(const Ray& r, float r0, float r1, float* t_out, v3* n_out) {
   float h = 1.0f;
   float dr = r1 - r0;
   float k = dr / h;
@@ -303,7 +303,7 @@ __device__ bool hit_cylinder(const Ray& r, float r0, float r1, float* t_out, v3*
 }
 
 // shader.wgsl:381-471
-__device__ float hit_torus(const Ray& r, float Ra, float ra) {
+static __device__ float hit_torus(const Ray& r, float Ra, float ra) {
   float po = 1.0f;
   float Ra2 = Ra * Ra;
   float ra2 = ra * ra;
@@ -372,13 +372,13 @@ __device__ float hit_torus(const Ray& r, float Ra, float ra) {
 }
 
 // Local-space ray of an object (m * (o,1), m * (d,0)).
-__device__ __forceinline__ Ray to_local(const m4& m, const Ray& r) {
+static __device__ __forceinline__ Ray to_local(const m4& m, const Ray& r) {
   Ray l; l.origin = mul_point(m, r.origin); l.direction = mul_dir(m, r.direction); return l;
 }
 
 // Object record fields used by traversal: inverse matrix rows and the fourth/fifth vectors.
 struct ObjHdr { int32_t material_idx, light_idx, type; float param0; v3 world_position; float param1; };
-__device__ __forceinline__ ObjHdr load_obj_hdr(const DScene& s, uint32_t i) {
+static __device__ __forceinline__ ObjHdr load_obj_hdr(const DScene& s, uint32_t i) {
   float4 a = ld4(s.objs + (size_t)i * 6 + 4), b = ld4(s.objs + (size_t)i * 6 + 5);
   ObjHdr h;
   h.material_idx = bi(a.x); h.light_idx = bi(a.y); h.type = bi(a.z); h.param0 = a.w;
@@ -388,7 +388,7 @@ __device__ __forceinline__ ObjHdr load_obj_hdr(const DScene& s, uint32_t i) {
 
 // BLAS closest hit: shader.wgsl:473-542.  Updates hit if a closer triangle is found.
 template <bool COUNT>
-__device__ __forceinline__ void trace_mesh(const DScene& s, const Ray& rw, const m4& inv_m, uint32_t node_offset,
+static __device__ __forceinline__ void trace_mesh(const DScene& s, const Ray& rw, const m4& inv_m, uint32_t node_offset,
                                            uint32_t tri_offset, int32_t material_idx, int32_t idx, int32_t kind,
                                            int32_t aux, HitRec& hit, uint32_t& err, Counters<COUNT>& cn) {
   Ray rl = to_local(inv_m, rw);
@@ -444,7 +444,7 @@ __device__ __forceinline__ void trace_mesh(const DScene& s, const Ray& rw, const
 // Analytic TLAS objects: shader.wgsl:544-692 (hit distance only; attributes are deferred).
 // Returns true when the reference would accept the candidate at world distance *t_out before the
 // comparison with the current closest hit.
-__device__ __forceinline__ bool analytic_t(const m4& inv, const ObjHdr& h, const Ray& rw, float* t_out) {
+static __device__ __forceinline__ bool analytic_t(const m4& inv, const ObjHdr& h, const Ray& rw, float* t_out) {
   Ray rl = to_local(inv, rw);
   if (h.type == 1) { float t = hit_unit_sphere(rl); *t_out = t; return t > 0.001f; }
   if (h.type == 2) { float t = hit_unit_cube(rl); *t_out = t; return t > 0.001f; }
@@ -462,7 +462,7 @@ __device__ __forceinline__ bool analytic_t(const m4& inv, const ObjHdr& h, const
 
 // shader.wgsl:694-752 (+ trace_scene planes and list meshes, :754-774)
 template <bool COUNT>
-__device__ HitRec trace_scene(const DScene& s, const Ray& ray, uint32_t& err, Counters<COUNT>& cn) {
+static __device__ HitRec trace_scene(const DScene& s, const Ray& ray, uint32_t& err, Counters<COUNT>& cn) {
   cn.add(C_RAYS_EXT);
   HitRec hit;
   hit.t = 1e10f; hit.m_idx = -1; hit.o_idx = -1; hit.kind = 0; hit.id = -1; hit.aux = -1; hit.bu = 0.0f; hit.bv = 0.0f;
@@ -541,7 +541,7 @@ __device__ HitRec trace_scene(const DScene& s, const Ray& ray, uint32_t& err, Co
 }
 
 // World-space normal of the winning primitive (the hit_n the reference leaves in SurfaceHit).
-__device__ v3 hit_normal(const DScene& s, const Ray& rw, const HitRec& hit) {
+static __device__ v3 hit_normal(const DScene& s, const Ray& rw, const HitRec& hit) {
   if (hit.kind == 1) return f3(ld4(s.planes + (size_t)hit.id * 2));
   if (hit.kind == 2 || hit.kind == 4) {
     m4 inv = hit.kind == 2 ? load_m4(s.objs + (size_t)hit.o_idx * 6) : load_m4(s.meshes + (size_t)hit.aux * 5);
@@ -591,7 +591,7 @@ __device__ v3 hit_normal(const DScene& s, const Ray& rw, const HitRec& hit) {
 // shadow test reduces to "is anything hit in (0.001, target_dist)" with the reference's interval
 // rules per primitive.
 template <bool COUNT>
-__device__ bool mesh_occludes(const DScene& s, const Ray& rw, const m4& inv_m, uint32_t node_offset,
+static __device__ bool mesh_occludes(const DScene& s, const Ray& rw, const m4& inv_m, uint32_t node_offset,
                               uint32_t tri_offset, float target_dist, uint32_t& err, Counters<COUNT>& cn) {
   Ray rl = to_local(inv_m, rw);
   v3 inv_dir = 1.0f / rl.direction;
@@ -641,7 +641,7 @@ __device__ bool mesh_occludes(const DScene& s, const Ray& rw, const m4& inv_m, u
 }
 
 // shader.wgsl:1019-1034
-__device__ float solve_cubic_real(float a, float b, float cc) {
+static __device__ float solve_cubic_real(float a, float b, float cc) {
   float q = (a * a - 3.0f * b) / 9.0f;
   float r = (2.0f * a * a * a - 9.0f * a * b + 27.0f * cc) / 54.0f;
   float r2 = r * r;
@@ -657,7 +657,7 @@ __device__ float solve_cubic_real(float a, float b, float cc) {
 }
 
 // shader.wgsl:1037-1087
-__device__ void solve_quartic_real(float a, float b, float cc, float d, float roots[4]) {
+static __device__ void solve_quartic_real(float a, float b, float cc, float d, float roots[4]) {
   roots[0] = roots[1] = roots[2] = roots[3] = -1.0f;
   float a2 = a * a;
   float y = solve_cubic_real(-b, a * cc - 4.0f * d, 4.0f * b * d - a2 * d - cc * cc);
@@ -696,7 +696,7 @@ __device__ void solve_quartic_real(float a, float b, float cc, float d, float ro
 
 // Analytic shadow tests: shader.wgsl:874-905 (sphere), 926-956 (cube), 964-1016 (cylinder),
 // 1096-1132 (torus).
-__device__ bool analytic_occludes(const m4& inv, const ObjHdr& h, const Ray& rw, float target_dist) {
+static __device__ bool analytic_occludes(const m4& inv, const ObjHdr& h, const Ray& rw, float target_dist) {
   Ray lr = to_local(inv, rw);
   if (h.type == 1) {
     float a = dot(lr.direction, lr.direction);
@@ -774,7 +774,7 @@ __device__ bool analytic_occludes(const m4& inv, const ObjHdr& h, const Ray& rw,
 
 // shader.wgsl:1206-1229: true if the shadow ray is blocked.
 template <bool COUNT>
-__device__ bool scene_occluded(const DScene& s, const Ray& ray, int32_t target_idx, float target_dist, uint32_t& err, Counters<COUNT>& cn) {
+static __device__ bool scene_occluded(const DScene& s, const Ray& ray, int32_t target_idx, float target_dist, uint32_t& err, Counters<COUNT>& cn) {
   cn.add(C_RAYS_SHADOW);
   if (HAS(s, WGPT_HAS_PLANES)) {
     for (uint32_t i = 0; i < s.n_planes; i++) {
@@ -846,22 +846,22 @@ __device__ bool scene_occluded(const DScene& s, const Ray& ray, int32_t target_i
 // ------------------------------------------------------------------------ BSDF
 struct Medium { float ior; v3 sigma; v3 emission; };
 struct MediumStack { Medium media[4]; int32_t count; };
-__device__ __forceinline__ Medium air() { Medium m; m.ior = 1.0f; m.sigma = mk3s(0.0f); m.emission = mk3s(0.0f); return m; }
-__device__ __forceinline__ Medium peek_medium(const MediumStack& st) { return st.count > 0 ? st.media[st.count - 1] : air(); }
-__device__ __forceinline__ float peek_ior(const MediumStack& st) { return st.count > 0 ? st.media[st.count - 1].ior : 1.0f; }
-__device__ __forceinline__ float peek_outer_ior(const MediumStack& st) { return st.count > 1 ? st.media[st.count - 2].ior : 1.0f; }
-__device__ __forceinline__ void push_medium(MediumStack& st, const Medium& m) { if (st.count < 4) { st.media[st.count] = m; st.count += 1; } }
-__device__ __forceinline__ void pop_medium(MediumStack& st) { if (st.count > 0) st.count -= 1; }
+static __device__ __forceinline__ Medium air() { Medium m; m.ior = 1.0f; m.sigma = mk3s(0.0f); m.emission = mk3s(0.0f); return m; }
+static __device__ __forceinline__ Medium peek_medium(const MediumStack& st) { return st.count > 0 ? st.media[st.count - 1] : air(); }
+static __device__ __forceinline__ float peek_ior(const MediumStack& st) { return st.count > 0 ? st.media[st.count - 1].ior : 1.0f; }
+static __device__ __forceinline__ float peek_outer_ior(const MediumStack& st) { return st.count > 1 ? st.media[st.count - 2].ior : 1.0f; }
+static __device__ __forceinline__ void push_medium(MediumStack& st, const Medium& m) { if (st.count < 4) { st.media[st.count] = m; st.count += 1; } }
+static __device__ __forceinline__ void pop_medium(MediumStack& st) { if (st.count > 0) st.count -= 1; }
 
 struct SurfCtx { v3 normal; v3 albedo; float roughness, metallic; v3 emittance; };
 
 // shader.wgsl:1700-1704
-__device__ __forceinline__ float D_GGX(float NdotH, float alpha2) {
+static __device__ __forceinline__ float D_GGX(float NdotH, float alpha2) {
   float denom = (NdotH * NdotH * (alpha2 - 1.0f) + 1.0f);
   return alpha2 / (PI * denom * denom + 1e-10f);
 }
 // shader.wgsl:1721-1733
-__device__ __forceinline__ float fresnel_dielectric(float cosThetaI, float etai, float etat) {
+static __device__ __forceinline__ float fresnel_dielectric(float cosThetaI, float etai, float etat) {
   float cosi = clamp(absf(cosThetaI), 0.0f, 1.0f);
   float sint = (etai / etat) * sqrtf(wmax(0.0f, 1.0f - cosi * cosi));
   if (sint >= 1.0f) return 1.0f;
@@ -871,22 +871,22 @@ __device__ __forceinline__ float fresnel_dielectric(float cosThetaI, float etai,
   return (Rs * Rs + Rp * Rp) / 2.0f;
 }
 // shader.wgsl:1787-1803
-__device__ __forceinline__ float G_Smith_GGX_div_NV(float NdotV, float NdotL, float alpha2) {
+static __device__ __forceinline__ float G_Smith_GGX_div_NV(float NdotV, float NdotL, float alpha2) {
   float sqrt_v = sqrtf(wmax(0.0f, alpha2 + NdotV * NdotV * (1.0f - alpha2)));
   float sqrt_l = sqrtf(wmax(0.0f, alpha2 + NdotL * NdotL * (1.0f - alpha2)));
   return (2.0f * NdotL) / (NdotL * sqrt_v + NdotV * sqrt_l + 1e-10f);
 }
-__device__ __forceinline__ float G_Smith_GGX_Uncorrelated_div_NV(float NdotV, float NdotL, float alpha2) {
+static __device__ __forceinline__ float G_Smith_GGX_Uncorrelated_div_NV(float NdotV, float NdotL, float alpha2) {
   float lambda_v = NdotV + sqrtf(wmax(0.0f, alpha2 + NdotV * NdotV * (1.0f - alpha2)));
   float lambda_l = NdotL + sqrtf(wmax(0.0f, alpha2 + NdotL * NdotL * (1.0f - alpha2)));
   return (4.0f * NdotL) / (lambda_v * lambda_l + 1e-7f);
 }
-__device__ __forceinline__ float G1_GGX_div_NV(float NdotV, float alpha2) {
+static __device__ __forceinline__ float G1_GGX_div_NV(float NdotV, float alpha2) {
   return 2.0f / (NdotV + sqrtf(wmax(0.0f, alpha2 + (1.0f - alpha2) * NdotV * NdotV)) + 1e-7f);
 }
 
 // eval_surface and pdf_surface of shader.wgsl:1831-2047 evaluated together.
-__device__ void bsdf_eval_pdf(v3 V, v3 L, const DMat& mat, const SurfCtx& ctx, const MediumStack& stack, v3* f_out, float* pdf_out) {
+static __device__ void bsdf_eval_pdf(v3 V, v3 L, const DMat& mat, const SurfCtx& ctx, const MediumStack& stack, v3* f_out, float* pdf_out) {
   bool entering = dot(ctx.normal, V) > 0.0f;
   v3 n_orient = entering ? ctx.normal : -ctx.normal;
   float dotNV = dot(n_orient, V);
@@ -1004,7 +1004,7 @@ __device__ void bsdf_eval_pdf(v3 V, v3 L, const DMat& mat, const SurfCtx& ctx, c
 }
 
 // shader.wgsl:1806-1829
-__device__ v3 ImportanceSampleVNDF_GGX(float xi0, float xi1, v3 V, v3 N, float alpha_ggx) {
+static __device__ v3 ImportanceSampleVNDF_GGX(float xi0, float xi1, v3 V, v3 N, float alpha_ggx) {
   v3 up = absf(N.y) > 0.999f ? mk3(0.0f, 0.0f, 1.0f) : mk3(0.0f, 1.0f, 0.0f);
   v3 T = normalize(cross(up, N));
   v3 B = cross(N, T);
@@ -1025,7 +1025,7 @@ __device__ v3 ImportanceSampleVNDF_GGX(float xi0, float xi1, v3 V, v3 N, float a
 }
 
 // shader.wgsl:1751-1763
-__device__ v3 ImportanceSampleCosine(float xi0, float xi1, v3 N) {
+static __device__ v3 ImportanceSampleCosine(float xi0, float xi1, v3 N) {
   float phi = TWO_PI * xi0;
   float cosTheta = sqrtf(clamp(xi1, 0.0f, 1.0f));
   float sinTheta = sqrtf(wmax(0.0f, 1.0f - xi1));
@@ -1037,7 +1037,7 @@ __device__ v3 ImportanceSampleCosine(float xi0, float xi1, v3 N) {
 }
 
 // shader.wgsl:1648-1659
-__device__ __forceinline__ float mis_weight(float pdf_a, float pdf_b) {
+static __device__ __forceinline__ float mis_weight(float pdf_a, float pdf_b) {
   if (pdf_a <= 0.0f) return 0.0f;
   float max_pdf = wmax(pdf_a, pdf_b);
   float a = pdf_a / max_pdf;
@@ -1050,7 +1050,7 @@ __device__ __forceinline__ float mis_weight(float pdf_a, float pdf_b) {
 }
 
 // shader.wgsl:2177-2189
-__device__ __forceinline__ v3 clamp_firefly(v3 rad, int bounce) {
+static __device__ __forceinline__ v3 clamp_firefly(v3 rad, int bounce) {
   if (bounce == 0) return rad;
   float lum = dot(rad, mk3(0.2126f, 0.7152f, 0.0722f));
   if (lum > 20.0f) return rad * (20.0f / lum);
@@ -1059,7 +1059,7 @@ __device__ __forceinline__ v3 clamp_firefly(v3 rad, int bounce) {
 
 // ------------------------------------------------------------------------ analytic lights
 // shader.wgsl:1459-1464
-__device__ __forceinline__ m3 build_tangent_space(v3 N) {
+static __device__ __forceinline__ m3 build_tangent_space(v3 N) {
   v3 a = absf(N.y) > 0.99999f ? mk3(0.0f, 0.0f, 1.0f) : mk3(0.0f, 1.0f, 0.0f);
   v3 T = normalize(cross(N, a));
   v3 B = cross(T, N);
@@ -1067,7 +1067,7 @@ __device__ __forceinline__ m3 build_tangent_space(v3 N) {
 }
 
 struct DLight { int32_t obj_idx; float area, power, scale; m4 matrix; };
-__device__ __forceinline__ DLight load_light(const DScene& s, uint32_t i) {
+static __device__ __forceinline__ DLight load_light(const DScene& s, uint32_t i) {
   const float4* p = s.lights + (size_t)i * 5;
   float4 a = ld4(p);
   DLight l; l.obj_idx = bi(a.x); l.area = a.y; l.power = a.z; l.scale = a.w;
@@ -1076,7 +1076,7 @@ __device__ __forceinline__ DLight load_light(const DScene& s, uint32_t i) {
 }
 
 struct BoxAreas { v3 v1, v2, v3_, cen; float s1, s2, s3, a1, a2, a3, total; };
-__device__ BoxAreas box_areas(const DLight& light, v3 hit_pos) {
+static __device__ BoxAreas box_areas(const DLight& light, v3 hit_pos) {
   BoxAreas b;
   b.v1 = xyz(light.matrix.c[0]); b.v2 = xyz(light.matrix.c[1]); b.v3_ = xyz(light.matrix.c[2]); b.cen = xyz(light.matrix.c[3]);
   v3 d = b.cen - hit_pos;
@@ -1091,7 +1091,7 @@ __device__ BoxAreas box_areas(const DLight& light, v3 hit_pos) {
 }
 
 // shader.wgsl:1473-1499
-__device__ float light_sphere_pdf(const DLight& light, v3 light_pos, v3 hit_pos, v3 dir) {
+static __device__ float light_sphere_pdf(const DLight& light, v3 light_pos, v3 hit_pos, v3 dir) {
   v3 d = light_pos - hit_pos;
   float d2 = dot(d, d);
   float r2 = light.scale * light.scale;
@@ -1107,7 +1107,7 @@ __device__ float light_sphere_pdf(const DLight& light, v3 light_pos, v3 hit_pos,
 }
 
 // shader.wgsl:1501-1549
-__device__ LightSample sample_light_sphere(const DLight& light, v3 light_pos, v3 emit, v3 hit_pos, float xi0, float xi1) {
+static __device__ LightSample sample_light_sphere(const DLight& light, v3 light_pos, v3 emit, v3 hit_pos, float xi0, float xi1) {
   v3 d = light_pos - hit_pos;
   float d2 = dot(d, d);
   float r2 = light.scale * light.scale;
@@ -1141,7 +1141,7 @@ __device__ LightSample sample_light_sphere(const DLight& light, v3 light_pos, v3
 }
 
 // shader.wgsl:1575-1624 (the face pick draws one more random number)
-__device__ LightSample sample_light_box(const DLight& light, v3 emit, v3 hit_pos, float xi0, float xi1, uint32_t& rng) {
+static __device__ LightSample sample_light_box(const DLight& light, v3 emit, v3 hit_pos, float xi0, float xi1, uint32_t& rng) {
   BoxAreas b = box_areas(light, hit_pos);
   v3 p = b.cen;
   v3 n;

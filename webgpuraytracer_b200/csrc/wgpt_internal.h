@@ -25,6 +25,35 @@ struct DeviceScene {
 cudaError_t launch_render(const DeviceScene& d, const wgpt_scene_params& q, uint32_t first_frame, uint32_t reps,
                           uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh, float* accum, uint8_t* out,
                           uint32_t out_pitch, uint32_t* status, unsigned long long* counters, cudaStream_t st);
+// CUDA-event timing of the renderer's stages (0 ray generation / single kernel, 1 closest hit,
+// 2 shading, 3 shadow rays + accumulation) on the launching stream.
+struct StageTimer {
+  static constexpr int kMaxEvents = 8192;
+  cudaEvent_t ev[kMaxEvents];
+  int stage_of[kMaxEvents / 2];
+  int used = 0;
+  bool ready = false;
+  int open_stage = -1;
+  void begin(int stage, cudaStream_t st) {
+    if (!ready || used + 2 > kMaxEvents) return;
+    cudaEventRecord(ev[used], st);
+    stage_of[used / 2] = stage;
+    open_stage = stage;
+  }
+  void end(int stage, cudaStream_t st) {
+    if (!ready || open_stage != stage || used + 2 > kMaxEvents) return;
+    cudaEventRecord(ev[used + 1], st);
+    used += 2;
+    open_stage = -1;
+  }
+};
+
+size_t wavefront_scratch_bytes(uint32_t capacity);
+cudaError_t launch_render_wavefront(const DeviceScene& d, const wgpt_scene_params& q, uint32_t first_frame,
+                                    uint32_t reps, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh, float* accum,
+                                    uint8_t* out, uint32_t out_pitch, void* scratch, uint32_t capacity,
+                                    uint32_t* status, unsigned long long* counters, cudaStream_t st,
+                                    StageTimer* timer);
 cudaError_t launch_gbuffer(const DeviceScene& d, const wgpt_scene_params& q, uint32_t sx, uint32_t sy, uint32_t sw,
                            uint32_t sh, float* gbuf, uint8_t* out, uint32_t out_pitch, uint32_t* status,
                            cudaStream_t st);

@@ -48,8 +48,7 @@ BYTES_PER_UNIT = {
     11: 32,   # hit attributes of the winning primitive (normals)
 }
 PIXEL_BYTES = 16 + 16 + 4   # accumulation read + write, rgba8 store
-STAGES = ["raygen_or_megakernel", "extend (closest hit)", "shade", "resolve (shadow rays + accumulate)"]
-KERNELS = ["k_wf_raygen", "k_wf_extend", "k_wf_shade", "k_wf_resolve"]
+KERNELS = ["k_wf_raygen", "k_wf_extend", "k_wf_shade", "k_wf_shadow", "k_wf_resolve", "-", "-", "-"]
 
 
 def algorithmic_bytes(counters: np.ndarray, pixels: int) -> float:
@@ -59,9 +58,9 @@ def algorithmic_bytes(counters: np.ndarray, pixels: int) -> float:
 def stage_bytes(stage_counters: np.ndarray, pixels: int, megakernel: bool) -> list[float]:
     """Algorithmic bytes per stage; the accumulation traffic belongs to the stage that writes it."""
     out = []
-    for st in range(4):
+    for st in range(8):
         c = stage_counters[st]
-        px = pixels if (st == 3 or (st == 0 and megakernel)) else 0
+        px = pixels if (st == 4 or (st == 0 and megakernel)) else 0
         out.append(algorithmic_bytes(c, px))
     return out
 
@@ -265,8 +264,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier(world)
     clocks = sampler.stop()
-    stage_ms = np.zeros(4, np.float64)
-    stage_launches = np.zeros(4, np.uint32)
+    stage_ms = np.zeros(8, np.float64)
+    stage_launches = np.zeros(8, np.uint32)
     r._check(r.L.wgpt_read_stage_times(r.ctx, rd.ptr(stage_ms), rd.ptr(stage_launches)), "stage times")
     r._check(r.L.wgpt_set_stage_timing(r.ctx, 0), "stage timing")
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
@@ -291,9 +290,9 @@ def run_ours(args):
     for i in range(args.steps):
         launch(args.warmup + i)
     cnt = r.read_counters()
-    stage_cnt = np.zeros(64, np.uint64)
+    stage_cnt = np.zeros(128, np.uint64)
     r._check(r.L.wgpt_read_stage_counters(r.ctx, rd.ptr(stage_cnt)), "stage counters")
-    stage_cnt = stage_cnt.reshape(4, 16)
+    stage_cnt = stage_cnt.reshape(8, 16)
     r.set_counting(False)
     mega = args.mode == "megakernel"
     sbytes = stage_bytes(stage_cnt, WIDTH * HEIGHT * args.steps, mega)
@@ -305,7 +304,7 @@ def run_ours(args):
     achieved = bytes_per_launch / avg_launch_s / 1e9
     rays = int(cnt[1] + cnt[2])
     stages = {}
-    for st in range(4):
+    for st in range(8):
         if stage_launches[st]:
             t = stage_ms[st] / 1e3
             stages[("k_render" if mega else KERNELS[st])] = {

@@ -136,14 +136,14 @@ int wgpt_trace_rays(wgpt_ctx* ctx, const float* rays, uint32_t n, int32_t* o_idx
 int wgpt_set_counting(wgpt_ctx* ctx, int on);
 int wgpt_read_counters(wgpt_ctx* ctx, uint64_t* dst16);
 
-/* The same counters split by stage (4 x 16 u64: 0 ray generation or the single kernel,
-   1 closest hit, 2 shading, 3 shadow rays and accumulation). */
-int wgpt_read_stage_counters(wgpt_ctx* ctx, uint64_t* dst64);
+/* The same counters split by stage (8 x 16 u64: 0 ray generation or the single kernel,
+   1 closest hit, 2 shading, 3 shadow rays, 4 accumulation, 5-7 unused). */
+int wgpt_read_stage_counters(wgpt_ctx* ctx, uint64_t* dst128);
 
 /* CUDA-event timing of every stage launch queued while timing is on; wgpt_read_stage_times
-   returns the summed milliseconds and launch counts per stage (as above) and restarts. */
+   returns the summed milliseconds and launch counts of the 8 stages (as above) and restarts. */
 int wgpt_set_stage_timing(wgpt_ctx* ctx, int on);
-int wgpt_read_stage_times(wgpt_ctx* ctx, double* ms4, uint32_t* launches4);
+int wgpt_read_stage_times(wgpt_ctx* ctx, double* ms8, uint32_t* launches8);
 
 /* The context's cudaStream_t (as void*) for callers that time or order work around it. */
 void* wgpt_stream(wgpt_ctx* ctx);

@@ -320,8 +320,8 @@ int wgpt_create(int device, wgpt_ctx** out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counters, 64 * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMemset(ctx->d_counters, 0, 64 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counters, 128 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_counters, 0, 128 * sizeof(unsigned long long));
   if (e != cudaSuccess) {
     wgpt_destroy(ctx);
     return WGPT_E_CUDA;
@@ -611,23 +611,26 @@ int wgpt_set_render_mode(wgpt_ctx* ctx, int mode) {
 int wgpt_set_counting(wgpt_ctx* ctx, int on) {
   if (!ctx) return WGPT_E_INVALID;
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-  if (on && !ctx->counting) CK(cudaMemsetAsync(ctx->d_counters, 0, 64 * sizeof(unsigned long long), ctx->stream), "reset counters");
+  if (on && !ctx->counting) CK(cudaMemsetAsync(ctx->d_counters, 0, 128 * sizeof(unsigned long long), ctx->stream), "reset counters");
   ctx->counting = on != 0;
   return WGPT_OK;
 }
 
 int wgpt_read_counters(wgpt_ctx* ctx, uint64_t* dst) {
   if (!ctx || !dst) return WGPT_E_INVALID;
-  uint64_t all[64];
+  uint64_t all[128];
   int rc = readback(ctx, all, ctx->d_counters, sizeof all, "read counters");
   if (rc) return rc;
-  for (int k = 0; k < 16; ++k) dst[k] = all[k] + all[16 + k] + all[32 + k] + all[48 + k];
+  for (int k = 0; k < 16; ++k) {
+    dst[k] = 0;
+    for (int st = 0; st < 8; ++st) dst[k] += all[16 * st + k];
+  }
   return WGPT_OK;
 }
 
-int wgpt_read_stage_counters(wgpt_ctx* ctx, uint64_t* dst64) {
+int wgpt_read_stage_counters(wgpt_ctx* ctx, uint64_t* dst128) {
   if (!ctx) return WGPT_E_INVALID;
-  return readback(ctx, dst64, ctx->d_counters, 64 * sizeof(unsigned long long), "read stage counters");
+  return readback(ctx, dst128, ctx->d_counters, 128 * sizeof(unsigned long long), "read stage counters");
 }
 
 int wgpt_set_stage_timing(wgpt_ctx* ctx, int on) {
@@ -643,9 +646,9 @@ int wgpt_set_stage_timing(wgpt_ctx* ctx, int on) {
   return WGPT_OK;
 }
 
-int wgpt_read_stage_times(wgpt_ctx* ctx, double* ms4, uint32_t* launches4) {
-  if (!ctx || !ms4 || !launches4) return WGPT_E_INVALID;
-  for (int k = 0; k < 4; ++k) { ms4[k] = 0; launches4[k] = 0; }
+int wgpt_read_stage_times(wgpt_ctx* ctx, double* ms8, uint32_t* launches8) {
+  if (!ctx || !ms8 || !launches8) return WGPT_E_INVALID;
+  for (int k = 0; k < 8; ++k) { ms8[k] = 0; launches8[k] = 0; }
   if (!ctx->timer) return WGPT_OK;
   int rc = wgpt_synchronize(ctx);
   if (rc) return rc;
@@ -653,8 +656,8 @@ int wgpt_read_stage_times(wgpt_ctx* ctx, double* ms4, uint32_t* launches4) {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, ctx->timer->ev[i], ctx->timer->ev[i + 1]), "cudaEventElapsedTime");
     int stg = ctx->timer->stage_of[i / 2];
-    ms4[stg] += ms;
-    launches4[stg] += 1;
+    ms8[stg] += ms;
+    launches8[stg] += 1;
   }
   ctx->timer->used = 0;
   return WGPT_OK;

@@ -135,7 +135,7 @@ static __device__ v3 sky_bilinear(const DScene& s, v2 uv, Counters<COUNT>& cn) {
 
 // shader.wgsl:176-188
 template <bool COUNT>
-static __device__ v3 sample_sky(const DScene& s, v3 dir, Counters<COUNT>& cn) {
+static __device__ __noinline__ v3 sample_sky(const DScene& s, v3 dir, Counters<COUNT>& cn) {
   float phi = atan2_(dir.z, dir.x);
   float theta = asin_(clamp(dir.y, -1.0f, 1.0f));
   return sky_bilinear(s, mk2(0.5f + phi / TWO_PI, 0.5f - theta / PI), cn);
@@ -156,7 +156,7 @@ static __device__ __forceinline__ uint32_t binary_search_cdf(const DScene& s, ui
 
 // shader.wgsl:208-229
 template <bool COUNT>
-static __device__ float get_sky_pdf(const DScene& s, const DParams& p, v3 dir, Counters<COUNT>& cn) {
+static __device__ __noinline__ float get_sky_pdf(const DScene& s, const DParams& p, v3 dir, Counters<COUNT>& cn) {
   float phi = atan2_(dir.z, dir.x);
   float theta = acos_(clamp(dir.y, -1.0f, 1.0f));
   float u = (phi + PI) / (2.0f * PI);
@@ -172,7 +172,7 @@ struct LightSample { v3 dir; v3 color; float dist; float pdf; };
 
 // shader.wgsl:231-254
 template <bool COUNT>
-static __device__ LightSample sample_env_cdf(const DScene& s, const DParams& p, float ux, float uy, Counters<COUNT>& cn) {
+static __device__ __noinline__ LightSample sample_env_cdf(const DScene& s, const DParams& p, float ux, float uy, Counters<COUNT>& cn) {
   LightSample samp;
   uint32_t v_idx = binary_search_cdf(s, 0u, p.sky_height, uy, cn);
   uint32_t row_offset = p.sky_cdf_index + (v_idx * (p.sky_width + 1u));
@@ -256,7 +256,7 @@ static __device__ __forceinline__ float hit_unit_cube(const Ray& r) {
 }
 
 // shader.wgsl:323-379
-static __device__ bool hit_cylinder(const Ray& r, float r0, float r1, float* t_out, v3* n_out) {
+static __device__ __noinline__ bool hit_cylinder(const Ray& r, float r0, float r1, float* t_out, v3* n_out) {
   float h = 1.0f;
   float dr = r1 - r0;
   float k = dr / h;
@@ -303,7 +303,7 @@ static __device__ bool hit_cylinder(const Ray& r, float r0, float r1, float* t_o
 }
 
 // shader.wgsl:381-471
-static __device__ float hit_torus(const Ray& r, float Ra, float ra) {
+static __device__ __noinline__ float hit_torus(const Ray& r, float Ra, float ra) {
   float po = 1.0f;
   float Ra2 = Ra * Ra;
   float ra2 = ra * ra;
@@ -541,7 +541,7 @@ static __device__ HitRec trace_scene(const DScene& s, const Ray& ray, uint32_t& 
 }
 
 // World-space normal of the winning primitive (the hit_n the reference leaves in SurfaceHit).
-static __device__ v3 hit_normal(const DScene& s, const Ray& rw, const HitRec& hit) {
+static __device__ __noinline__ v3 hit_normal(const DScene& s, const Ray& rw, const HitRec& hit) {
   if (hit.kind == 1) return f3(ld4(s.planes + (size_t)hit.id * 2));
   if (hit.kind == 2 || hit.kind == 4) {
     m4 inv = hit.kind == 2 ? load_m4(s.objs + (size_t)hit.o_idx * 6) : load_m4(s.meshes + (size_t)hit.aux * 5);
@@ -641,7 +641,7 @@ static __device__ bool mesh_occludes(const DScene& s, const Ray& rw, const m4& i
 }
 
 // shader.wgsl:1019-1034
-static __device__ float solve_cubic_real(float a, float b, float cc) {
+static __device__ __noinline__ float solve_cubic_real(float a, float b, float cc) {
   float q = (a * a - 3.0f * b) / 9.0f;
   float r = (2.0f * a * a * a - 9.0f * a * b + 27.0f * cc) / 54.0f;
   float r2 = r * r;
@@ -657,7 +657,7 @@ static __device__ float solve_cubic_real(float a, float b, float cc) {
 }
 
 // shader.wgsl:1037-1087
-static __device__ void solve_quartic_real(float a, float b, float cc, float d, float roots[4]) {
+static __device__ __noinline__ void solve_quartic_real(float a, float b, float cc, float d, float roots[4]) {
   roots[0] = roots[1] = roots[2] = roots[3] = -1.0f;
   float a2 = a * a;
   float y = solve_cubic_real(-b, a * cc - 4.0f * d, 4.0f * b * d - a2 * d - cc * cc);
@@ -696,7 +696,7 @@ static __device__ void solve_quartic_real(float a, float b, float cc, float d, f
 
 // Analytic shadow tests: shader.wgsl:874-905 (sphere), 926-956 (cube), 964-1016 (cylinder),
 // 1096-1132 (torus).
-static __device__ bool analytic_occludes(const m4& inv, const ObjHdr& h, const Ray& rw, float target_dist) {
+static __device__ __noinline__ bool analytic_occludes(const m4& inv, const ObjHdr& h, const Ray& rw, float target_dist) {
   Ray lr = to_local(inv, rw);
   if (h.type == 1) {
     float a = dot(lr.direction, lr.direction);
@@ -886,7 +886,7 @@ static __device__ __forceinline__ float G1_GGX_div_NV(float NdotV, float alpha2)
 }
 
 // eval_surface and pdf_surface of shader.wgsl:1831-2047 evaluated together.
-static __device__ void bsdf_eval_pdf(v3 V, v3 L, const DMat& mat, const SurfCtx& ctx, const MediumStack& stack, v3* f_out, float* pdf_out) {
+static __device__ __noinline__ void bsdf_eval_pdf(v3 V, v3 L, const DMat& mat, const SurfCtx& ctx, const MediumStack& stack, v3* f_out, float* pdf_out) {
   bool entering = dot(ctx.normal, V) > 0.0f;
   v3 n_orient = entering ? ctx.normal : -ctx.normal;
   float dotNV = dot(n_orient, V);
@@ -1004,7 +1004,7 @@ static __device__ void bsdf_eval_pdf(v3 V, v3 L, const DMat& mat, const SurfCtx&
 }
 
 // shader.wgsl:1806-1829
-static __device__ v3 ImportanceSampleVNDF_GGX(float xi0, float xi1, v3 V, v3 N, float alpha_ggx) {
+static __device__ __noinline__ v3 ImportanceSampleVNDF_GGX(float xi0, float xi1, v3 V, v3 N, float alpha_ggx) {
   v3 up = absf(N.y) > 0.999f ? mk3(0.0f, 0.0f, 1.0f) : mk3(0.0f, 1.0f, 0.0f);
   v3 T = normalize(cross(up, N));
   v3 B = cross(N, T);
@@ -1025,7 +1025,7 @@ static __device__ v3 ImportanceSampleVNDF_GGX(float xi0, float xi1, v3 V, v3 N, 
 }
 
 // shader.wgsl:1751-1763
-static __device__ v3 ImportanceSampleCosine(float xi0, float xi1, v3 N) {
+static __device__ __noinline__ v3 ImportanceSampleCosine(float xi0, float xi1, v3 N) {
   float phi = TWO_PI * xi0;
   float cosTheta = sqrtf(clamp(xi1, 0.0f, 1.0f));
   float sinTheta = sqrtf(wmax(0.0f, 1.0f - xi1));
@@ -1076,7 +1076,7 @@ static __device__ __forceinline__ DLight load_light(const DScene& s, uint32_t i)
 }
 
 struct BoxAreas { v3 v1, v2, v3_, cen; float s1, s2, s3, a1, a2, a3, total; };
-static __device__ BoxAreas box_areas(const DLight& light, v3 hit_pos) {
+static __device__ __noinline__ BoxAreas box_areas(const DLight& light, v3 hit_pos) {
   BoxAreas b;
   b.v1 = xyz(light.matrix.c[0]); b.v2 = xyz(light.matrix.c[1]); b.v3_ = xyz(light.matrix.c[2]); b.cen = xyz(light.matrix.c[3]);
   v3 d = b.cen - hit_pos;
@@ -1091,7 +1091,7 @@ static __device__ BoxAreas box_areas(const DLight& light, v3 hit_pos) {
 }
 
 // shader.wgsl:1473-1499
-static __device__ float light_sphere_pdf(const DLight& light, v3 light_pos, v3 hit_pos, v3 dir) {
+static __device__ __noinline__ float light_sphere_pdf(const DLight& light, v3 light_pos, v3 hit_pos, v3 dir) {
   v3 d = light_pos - hit_pos;
   float d2 = dot(d, d);
   float r2 = light.scale * light.scale;
@@ -1107,7 +1107,7 @@ static __device__ float light_sphere_pdf(const DLight& light, v3 light_pos, v3 h
 }
 
 // shader.wgsl:1501-1549
-static __device__ LightSample sample_light_sphere(const DLight& light, v3 light_pos, v3 emit, v3 hit_pos, float xi0, float xi1) {
+static __device__ __noinline__ LightSample sample_light_sphere(const DLight& light, v3 light_pos, v3 emit, v3 hit_pos, float xi0, float xi1) {
   v3 d = light_pos - hit_pos;
   float d2 = dot(d, d);
   float r2 = light.scale * light.scale;
@@ -1141,7 +1141,7 @@ static __device__ LightSample sample_light_sphere(const DLight& light, v3 light_
 }
 
 // shader.wgsl:1575-1624 (the face pick draws one more random number)
-static __device__ LightSample sample_light_box(const DLight& light, v3 emit, v3 hit_pos, float xi0, float xi1, uint32_t& rng) {
+static __device__ __noinline__ LightSample sample_light_box(const DLight& light, v3 emit, v3 hit_pos, float xi0, float xi1, uint32_t& rng) {
   BoxAreas b = box_areas(light, hit_pos);
   v3 p = b.cen;
   v3 n;

@@ -8,9 +8,11 @@
 //     k_wf_shade      media, sky / emission terms, light and environment NEE set-up, BSDF
 //                     sampling, Russian roulette; appends surviving paths to the next queue and
 //                     records up to two next-event contributions with their shadow rays
-//     k_wf_resolve    traces the recorded shadow rays and adds the contributions (light first,
-//                     then environment, as main does), then accumulates finished paths into the
-//                     running mean and the rgba8 image
+//     k_wf_shadow     traces the recorded shadow rays (their own compacted queue, fetched
+//                     dynamically by warps) and stores one visibility byte per record
+//     k_wf_resolve    adds the next-event contributions (light first, then environment, as main
+//                     does), then accumulates finished paths into the running mean and the rgba8
+//                     image
 // Each stage keeps only its own code and registers resident, so warps stay converged on one
 // code path and the instruction cache holds the stage (the single-kernel form stalls on
 // instruction fetch).  Every floating-point operation and random draw happens in the order of
@@ -32,8 +34,11 @@ struct WfBuffers {
   uint4* hit;        // 2 per path: (t, m_idx, o_idx, kind), (id, aux, bu, bv)
   float4* nee;       // 4 per path: (tp.xyz, -), (incoming.xyz, -) for the light and env records
   float4* shadow;    // 4 per path: (origin.xyz, target_dist), (direction.xyz, ignore_idx) x 2
+  uint8_t* vis;      // 2 per path: 1 if the record's shadow ray reached its light
   uint32_t* queue[2];
-  uint32_t* counts;  // per bounce: live paths entering the bounce
+  uint32_t* shq;     // shadow-ray queue: slot * 2 + record
+  uint32_t* counts;  // [b]: live paths entering bounce b; [128 + b]: shadow rays of bounce b;
+                     // [192 + b]: shadow rays handed out to warps
 };
 
 // meta.y flags
@@ -181,7 +186,7 @@ __device__ void record_nee(const WfArgs& a, uint32_t slot, int rec, const LightS
   a.b.nee[slot * 4 + rec * 2 + 1] = make_float4(incoming.x, incoming.y, incoming.z, 0.0f);
   flags |= rec == 0 ? F_NEE_LIGHT : F_NEE_ENV;
   if (shadow) {
-    flags |= rec == 0 ? F_SHADOW_LIGHT : F_SHADOW_ENV;
+    flags |= rec == 0 ? F_SHADOW_LIGHT : F_SHADOW_ENV;   // queued after the shading body
     a.b.shadow[slot * 4 + rec * 2] = make_float4(so.x, so.y, so.z, ls.dist);
     a.b.shadow[slot * 4 + rec * 2 + 1] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, __int_as_float(ignore_idx));
   }
@@ -190,14 +195,14 @@ __device__ void record_nee(const WfArgs& a, uint32_t slot, int rec, const LightS
 template <bool COUNT>
 __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const uint32_t* __restrict__ q,
                                                   const uint32_t* count_ptr, uint32_t* __restrict__ q_next,
-                                                  uint32_t* count_next) {
+                                                  uint32_t* count_next, uint32_t* sh_count) {
   Counters<COUNT> cn; cn.init();
   const DScene& s = a.s;
   const DParams& p = a.p;
   uint32_t n = *count_ptr;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
-    bool alive = false;
+    bool alive = false, sh_light = false, sh_env = false;
     uint32_t slot = 0;
     if (i < n) {
       slot = q[i];
@@ -354,21 +359,22 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const ui
             v3 L = mk3s(0.0f);
             bool is_transmission = false;
             bool done = false, ok = true;
+            // lobe choice; the VNDF sampler has one call site for the three microfacet lobes
+            int lobe = -1;
+            v3 Nv = n_orient;
+            float av = alpha;
             if (rsel < p_cc) {
-              v3 H = ImportanceSampleVNDF_GGX(xi0, xi1, V, sn_orient, cc_alpha);
-              L = reflect(-V, H);
+              lobe = 0; Nv = sn_orient; av = cc_alpha;
             } else if (rsel < p_cc + p_spec) {
-              v3 N_spec = n_orient;
+              lobe = 1;
               if (mat.anisotropic > 0.0f) {
                 v3 up = absf(n_orient.y) > 0.99999f ? mk3(0.0f, 0.0f, 1.0f) : mk3(0.0f, 1.0f, 0.0f);
                 v3 T = normalize(cross(up, n_orient));
                 v3 B = cross(n_orient, T);
                 float angle = mat.aniso_rotation * TWO_PI;
                 T = T * cos_(angle) + B * sin_(angle);
-                N_spec = normalize(vmix(n_orient, cross(cross(V, T), T), mat.anisotropic));
+                Nv = normalize(vmix(n_orient, cross(cross(V, T), T), mat.anisotropic));
               }
-              v3 H = ImportanceSampleVNDF_GGX(xi0, xi1, V, N_spec, alpha);
-              L = reflect(-V, H);
             } else if (rsel < p_cc + p_spec + p_trans) {
               if (absf(etai - etat) < 1e-4f) {
                 ray.direction = -V;
@@ -385,16 +391,25 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const ui
                 }
                 done = true;
               } else {
-                v3 H = ImportanceSampleVNDF_GGX(xi0, xi1, V, n_orient, alpha);
+                lobe = 2;
+              }
+            } else if (rsel < total_p) {
+              lobe = 3;
+            } else {
+              ok = false;
+            }
+            if (lobe >= 0 && lobe <= 2) {
+              v3 H = ImportanceSampleVNDF_GGX(xi0, xi1, V, Nv, av);
+              if (lobe == 2) {
                 float eta_ratio = etai / etat;
                 L = refract(-V, H, eta_ratio);
                 if (length(L) < 0.1f) L = reflect(-V, H);
                 else is_transmission = true;
+              } else {
+                L = reflect(-V, H);
               }
-            } else if (rsel < total_p) {
+            } else if (lobe == 3) {
               L = ImportanceSampleCosine(xi0, xi1, n_orient);
-            } else {
-              ok = false;
             }
             if (ok && !done) {
               float dotNL = dot(n_orient, L);
@@ -438,6 +453,8 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const ui
       } while (false);
       if (bounce + 1 >= s.bounce_limit) alive = false;
       if (alive) flags |= F_ALIVE;
+      sh_light = (flags & F_SHADOW_LIGHT) != 0u;
+      sh_env = (flags & F_SHADOW_ENV) != 0u;
       a.b.ray_o[slot] = make_float4(ray.origin.x, ray.origin.y, ray.origin.z, 0.0f);
       a.b.ray_d[slot] = make_float4(ray.direction.x, ray.direction.y, ray.direction.z, 0.0f);
       a.b.tp[slot] = make_float4(throughput.x, throughput.y, throughput.z, last_surface_pdf);
@@ -445,15 +462,43 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const ui
       a.b.meta[slot] = make_uint4(rng, flags, (uint32_t)bounce, (uint32_t)stack.count);
     }
     queue_push(q_next, count_next, slot, alive);
+    queue_push(a.b.shq, sh_count, slot * 2u, sh_light);
+    queue_push(a.b.shq, sh_count, slot * 2u + 1u, sh_env);
   }
   flush_wf<COUNT>(cn, a.counters, true);
+}
+
+// ---------------------------------------------------------------------------- shadow
+// Warps take 32 queue entries at a time from a shared cursor, so warps whose rays finish early
+// keep working instead of idling behind the slowest warp of a static partition.
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_wf_shadow(WfArgs a, const uint32_t* count_ptr, uint32_t* cursor) {
+  Counters<COUNT> cn; cn.init();
+  uint32_t err = 0;
+  const uint32_t n = *count_ptr;
+  const int lane = threadIdx.x & 31;
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(cursor, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    uint32_t i = base + lane;
+    if (i < n) {
+      uint32_t e = a.b.shq[i];
+      float4 so = a.b.shadow[(e >> 1) * 4 + (e & 1u) * 2], sd = a.b.shadow[(e >> 1) * 4 + (e & 1u) * 2 + 1];
+      Ray sr; sr.origin = mk3(so.x, so.y, so.z); sr.direction = mk3(sd.x, sd.y, sd.z);
+      bool occ = scene_occluded<COUNT>(a.s, sr, __float_as_int(sd.w), so.w, err, cn);
+      a.b.vis[e] = occ ? 0u : 1u;
+    }
+  }
+  flush_wf<COUNT>(cn, a.counters, true);
+  if (err) atomicOr(a.status, err);
 }
 
 // ---------------------------------------------------------------------------- resolve
 template <bool COUNT>
 __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a, const uint32_t* __restrict__ q, const uint32_t* count_ptr) {
   Counters<COUNT> cn; cn.init();
-  uint32_t err = 0;
   uint32_t n = *count_ptr;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
@@ -472,11 +517,7 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a, const uint32_t* __
           if (!(flags & has)) continue;
           float4 t4 = a.b.nee[slot * 4 + rec * 2], c4 = a.b.nee[slot * 4 + rec * 2 + 1];
           v3 incoming = mk3(c4.x, c4.y, c4.z);
-          if (flags & needs) {
-            float4 so = a.b.shadow[slot * 4 + rec * 2], sd = a.b.shadow[slot * 4 + rec * 2 + 1];
-            Ray sr; sr.origin = mk3(so.x, so.y, so.z); sr.direction = mk3(sd.x, sd.y, sd.z);
-            if (scene_occluded<COUNT>(a.s, sr, __float_as_int(sd.w), so.w, err, cn)) incoming = mk3s(0.0f);
-          }
+          if ((flags & needs) && a.b.vis[slot * 2 + rec] == 0u) incoming = mk3s(0.0f);
           radiance = radiance + mk3(t4.x, t4.y, t4.z) * clamp_firefly(incoming, bounce);
         }
         a.b.rad[slot] = make_float4(radiance.x, radiance.y, radiance.z, rd4.w);
@@ -498,7 +539,6 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a, const uint32_t* __
     }
   }
   flush_wf<COUNT>(cn, a.counters, true);
-  if (err) atomicOr(a.status, err);
 }
 
 }  // namespace pt
@@ -537,8 +577,9 @@ static DParams to_dparams_wf(const wgpt_scene_params& q, uint32_t sec_x, uint32_
 }
 
 size_t wavefront_bytes_per_path() {
-  // ray 32 + tp 16 + rad 16 + meta 16 + media 128 + hit 32 + nee 64 + shadow 64 + 2 queues 8
-  return 32 + 16 + 16 + 16 + 128 + 32 + 64 + 64 + 8;
+  // ray 32 + tp 16 + rad 16 + meta 16 + media 128 + hit 32 + nee 64 + shadow 64 + vis 2 +
+  // 2 path queues 8 + shadow queue 8
+  return 32 + 16 + 16 + 16 + 128 + 32 + 64 + 64 + 2 + 8 + 8;
 }
 
 // Carves the path-state arrays out of one scratch allocation of wavefront_bytes_per_path() *
@@ -557,20 +598,23 @@ static WfBuffers carve(void* scratch, uint32_t capacity) {
   b.hit = (uint4*)take(n * 32);
   b.nee = (float4*)take(n * 64);
   b.shadow = (float4*)take(n * 64);
+  b.vis = (uint8_t*)take(n * 2);
   b.queue[0] = (uint32_t*)take(n * 4);
   b.queue[1] = (uint32_t*)take(n * 4);
+  b.shq = (uint32_t*)take(n * 8);
   b.counts = (uint32_t*)take(256 * 4);
   return b;
 }
 
 size_t wavefront_scratch_bytes(uint32_t capacity) {
   size_t n = capacity, s = 0;
-  size_t parts[11] = {n * 16, n * 16, n * 16, n * 16, n * 16, n * 128, n * 32, n * 64, n * 64, n * 4, n * 4};
+  size_t parts[13] = {n * 16, n * 16, n * 16, n * 16, n * 16, n * 128, n * 32, n * 64, n * 64, n * 2, n * 4, n * 4,
+                      n * 8};
   for (size_t x : parts) s += (x + 255) & ~(size_t)255;
   return s + 256 * 4;
 }
 
-static int g_grid[4] = {0, 0, 0, 0};   // persistent grid size per stage (computed once)
+static int g_grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // persistent grid size per stage (computed once)
 
 template <typename K>
 static int grid_for(K kernel, int stage) {
@@ -599,7 +643,8 @@ static cudaError_t render_wf(const WfArgs& a0, uint32_t first_frame, uint32_t re
   int g_ray = grid_for(k_wf_raygen<COUNT>, 0);
   int g_ext = grid_for(k_wf_extend<COUNT>, 1);
   int g_sh = grid_for(k_wf_shade<COUNT>, 2);
-  int g_res = grid_for(k_wf_resolve<COUNT>, 3);
+  int g_shw = grid_for(k_wf_shadow<COUNT>, 3);
+  int g_res = grid_for(k_wf_resolve<COUNT>, 4);
   int need = (int)((n + 255) / 256);
   for (uint32_t r = 0; r < reps; ++r) {
     a.sample_number = first_frame + r;
@@ -615,11 +660,15 @@ static cudaError_t render_wf(const WfArgs& a0, uint32_t first_frame, uint32_t re
       if (timer) timer->end(1, st);
       if (timer) timer->begin(2, st);
       k_wf_shade<COUNT><<<std::min(g_sh, need), 256, 0, st>>>(stage_args(2), b, qin, a.b.counts + b, qout,
-                                                               a.b.counts + b + 1);
+                                                               a.b.counts + b + 1, a.b.counts + 128 + b);
       if (timer) timer->end(2, st);
       if (timer) timer->begin(3, st);
-      k_wf_resolve<COUNT><<<std::min(g_res, need), 256, 0, st>>>(stage_args(3), qin, a.b.counts + b);
+      k_wf_shadow<COUNT><<<std::min(g_shw, 2 * need), 256, 0, st>>>(stage_args(3), a.b.counts + 128 + b,
+                                                                   a.b.counts + 192 + b);
       if (timer) timer->end(3, st);
+      if (timer) timer->begin(4, st);
+      k_wf_resolve<COUNT><<<std::min(g_res, need), 256, 0, st>>>(stage_args(4), qin, a.b.counts + b);
+      if (timer) timer->end(4, st);
     }
   }
   return cudaGetLastError();

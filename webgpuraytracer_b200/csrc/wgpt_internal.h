@@ -26,7 +26,7 @@ cudaError_t launch_render(const DeviceScene& d, const wgpt_scene_params& q, uint
                           uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh, float* accum, uint8_t* out,
                           uint32_t out_pitch, uint32_t* status, unsigned long long* counters, cudaStream_t st);
 // CUDA-event timing of the renderer's stages (0 ray generation / single kernel, 1 closest hit,
-// 2 shading, 3 shadow rays + accumulation) on the launching stream.
+// 2 shading, 3 shadow rays, 4 accumulation) on the launching stream.
 struct StageTimer {
   static constexpr int kMaxEvents = 8192;
   cudaEvent_t ev[kMaxEvents];

@@ -8,6 +8,7 @@
 #include <vector>
 #include <set>
 #include <utility>
+#include <algorithm>
 
 #include "../../include/wgpt.h"
 #include "wgpt_internal.h"
@@ -45,6 +46,10 @@ struct wgpt_ctx {
   bool counting = false;
   // wavefront path state (scratch sized for the whole image)
   int mode = WGPT_MODE_WAVEFRONT;
+  // derived child-pair node arrays (64 bytes per node) of the TLAS and the BLAS buffer
+  void* d_pairs_tlas = nullptr;
+  void* d_pairs_bvh = nullptr;
+  size_t pairs_cap[2] = {0, 0};
   wgpt::StageTimer* timer = nullptr;
   bool timing = false;
   void* wf_scratch = nullptr;
@@ -193,6 +198,67 @@ std::string validate(const HostScene& s, uint32_t flags, std::set<std::pair<uint
   return "";
 }
 
+// Child-pair record of inner node i: both children's boxes; .w of each child's max is the
+// absolute node index of an inner child or the reference's relative first item of a leaf.
+void fill_pairs(const wgpt_bvh_node* nodes, uint32_t root, uint32_t base, float* pairs, std::vector<uint8_t>& done) {
+  std::vector<uint32_t> st;
+  st.push_back(root);
+  while (!st.empty()) {
+    uint32_t i = st.back();
+    st.pop_back();
+    const wgpt_bvh_node& nd = nodes[i];
+    if (nd.num_triangles > 0u || done[i]) continue;
+    done[i] = 1;
+    uint32_t li = i + 1, ri = base + nd.next;
+    const wgpt_bvh_node* ch[2] = {&nodes[li], &nodes[ri]};
+    uint32_t abs_idx[2] = {li, ri};
+    float* out = pairs + (size_t)i * 16;
+    for (int c = 0; c < 2; ++c) {
+      const wgpt_bvh_node& x = *ch[c];
+      uint32_t w = x.num_triangles > 0u ? x.next : abs_idx[c];
+      memcpy(out + c * 8 + 0, x.aabb_min, 12);
+      memcpy(out + c * 8 + 3, &x.num_triangles, 4);
+      memcpy(out + c * 8 + 4, x.aabb_max, 12);
+      memcpy(out + c * 8 + 7, &w, 4);
+      if (x.num_triangles == 0u) st.push_back(abs_idx[c]);
+    }
+  }
+}
+
+int upload_pairs(wgpt_ctx* ctx, const HostScene& hs, uint32_t flags) {
+  const uint32_t tlas_flags = WGPT_HAS_SPHERES | WGPT_HAS_CUBES | WGPT_HAS_CYLINDERS | WGPT_HAS_TORI | WGPT_HAS_MESHES;
+  std::vector<float> pt((size_t)std::max(1u, hs.n_tlas) * 16, 0.0f), pb((size_t)std::max(1u, hs.n_bvh) * 16, 0.0f);
+  if ((flags & tlas_flags) && hs.n_tlas) {
+    std::vector<uint8_t> done(hs.n_tlas, 0);
+    fill_pairs(hs.tlas, 0, 0, pt.data(), done);
+  }
+  std::vector<uint8_t> done(std::max(1u, hs.n_bvh), 0);
+  std::set<uint32_t> roots;
+  if (flags & WGPT_HAS_MESHES)
+    for (uint32_t i = 0; i < hs.n_objs; ++i)
+      if (hs.objs[i].object_type == 0) { uint32_t no; memcpy(&no, &hs.objs[i].param0, 4); roots.insert(no); }
+  if (flags & WGPT_HAS_LIST_MESHES)
+    for (uint32_t i = 0; i < hs.n_meshes; ++i) {
+      wgpt_mesh_instance mi;
+      memcpy(&mi, hs.meshes + (size_t)i * WGPT_STRIDE_MESH_READ, sizeof mi);
+      roots.insert(mi.node_offset);
+    }
+  for (uint32_t r : roots) fill_pairs(hs.bvh, r, r, pb.data(), done);
+  void** dst[2] = {&ctx->d_pairs_tlas, &ctx->d_pairs_bvh};
+  std::vector<float>* src[2] = {&pt, &pb};
+  for (int k = 0; k < 2; ++k) {
+    size_t bytes = src[k]->size() * sizeof(float);
+    if (bytes > ctx->pairs_cap[k]) {
+      dfree(*dst[k]);
+      ctx->pairs_cap[k] = 0;
+      CK(cudaMalloc(dst[k], bytes), "cudaMalloc node pairs");
+      ctx->pairs_cap[k] = bytes;
+    }
+    CK(cudaMemcpy(*dst[k], src[k]->data(), bytes, cudaMemcpyHostToDevice), "upload node pairs");
+  }
+  return WGPT_OK;
+}
+
 int upload_buffers(wgpt_ctx* ctx, const wgpt_scene_desc* d, bool in_place_only) {
   const wgpt_buffer* src[9] = {&d->materials, &d->objects, &d->tlas, &d->meshes, &d->bvh,
                                &d->triangles, &d->planes, &d->lights, &d->sky_cdf};
@@ -338,6 +404,7 @@ int wgpt_destroy(wgpt_ctx* ctx) {
   dfree_t(ctx->accum); dfree_t(ctx->out); dfree_t(ctx->gbuf);
   dfree_t(ctx->dn_a); dfree_t(ctx->dn_b); dfree_t(ctx->dn_guide); dfree_t(ctx->dn_comp);
   dfree_t(ctx->canvas); dfree_t(ctx->d_status); dfree_t(ctx->d_counters); dfree(ctx->wf_scratch);
+  dfree(ctx->d_pairs_tlas); dfree(ctx->d_pairs_bvh);
   if (ctx->timer) {
     if (ctx->timer->ready)
       for (int i = 0; i < wgpt::StageTimer::kMaxEvents; ++i) cudaEventDestroy(ctx->timer->ev[i]);
@@ -371,6 +438,8 @@ int wgpt_upload_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   CK(cudaStreamSynchronize(ctx->stream), "drain before upload");
   rc = upload_buffers(ctx, desc, false);
   if (rc) return rc;
+  rc = upload_pairs(ctx, hs, desc->feature_flags);
+  if (rc) return rc;
   fill_device_scene(ctx, desc);
   ctx->has_scene = true;
   return WGPT_OK;
@@ -387,6 +456,8 @@ int wgpt_update_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->stream), "drain before update");
   rc = upload_buffers(ctx, desc, true);
+  if (rc) return rc;
+  rc = upload_pairs(ctx, hs, desc->feature_flags);
   if (rc) return rc;
   fill_device_scene(ctx, desc);
   return WGPT_OK;
@@ -451,7 +522,8 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
     ctx->wf_capacity = need;
   }
   CK(wgpt::launch_render_wavefront(ctx->ds, ctx->params, first_frame, reps, sx, sy, sw, sh, ctx->accum, ctx->out,
-                                   ctx->w, ctx->wf_scratch, ctx->wf_capacity, ctx->d_status, cnt, ctx->stream, tm),
+                                   ctx->w, ctx->wf_scratch, ctx->wf_capacity, ctx->d_status, cnt, ctx->stream, tm,
+                                   ctx->d_pairs_tlas, ctx->d_pairs_bvh),
      "wavefront render launch");
   return WGPT_OK;
 }

@@ -20,6 +20,7 @@
 // form and the CPU restatement bit for bit.
 #include <algorithm>
 #include "pt_device.cuh"
+#include "traverse.cuh"
 #include "wgpt_internal.h"
 
 namespace pt {
@@ -37,8 +38,8 @@ struct WfBuffers {
   uint8_t* vis;      // 2 per path: 1 if the record's shadow ray reached its light
   uint32_t* queue[2];
   uint32_t* shq;     // shadow-ray queue: slot * 2 + record
-  uint32_t* counts;  // [b]: live paths entering bounce b; [128 + b]: shadow rays of bounce b;
-                     // [192 + b]: shadow rays handed out to warps
+  uint32_t* counts;  // [b]: live paths entering bounce b; [64 + b]: rays handed out to warps;
+                     // [128 + b]: shadow rays of bounce b; [192 + b]: shadow rays handed out
 };
 
 // meta.y flags
@@ -52,6 +53,7 @@ enum : uint32_t {
 
 struct WfArgs {
   DScene s;
+  DPairs P;
   DParams p;
   WfBuffers b;
   uint32_t sec_w, sec_h;
@@ -124,20 +126,54 @@ __global__ void __launch_bounds__(256) k_wf_raygen(WfArgs a) {
 }
 
 // ---------------------------------------------------------------------------- extend
+constexpr unsigned FULL = 0xffffffffu;
+
+// Hands queue entries to the lanes of a warp that have no ray, from a shared cursor; returns the
+// entry index for this lane (>= n when there is none).  `exhausted` becomes true (warp-uniform)
+// once the queue has been handed out completely.
+__device__ __forceinline__ uint32_t refill(bool have, uint32_t* cursor, uint32_t n, bool& exhausted) {
+  uint32_t qi = 0xffffffffu;
+  unsigned need = __ballot_sync(FULL, !have);
+  if (need) {
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(need) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(cursor, (uint32_t)__popc(need));
+    base = __shfl_sync(FULL, base, leader);
+    if (!have) qi = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+    if (base + (uint32_t)__popc(need) >= n) exhausted = true;
+  }
+  return qi;
+}
+
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_wf_extend(WfArgs a, const uint32_t* __restrict__ q, const uint32_t* count_ptr) {
+__global__ void __launch_bounds__(256) k_wf_extend(WfArgs a, const uint32_t* __restrict__ q, const uint32_t* count_ptr,
+                                                   uint32_t* cursor) {
   Counters<COUNT> cn; cn.init();
   uint32_t err = 0;
-  uint32_t n = *count_ptr;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    uint32_t i = base + threadIdx.x;
-    if (i < n) {
-      uint32_t slot = q[i];
-      float4 o = a.b.ray_o[slot], d = a.b.ray_d[slot];
-      Ray r; r.origin = mk3(o.x, o.y, o.z); r.direction = mk3(d.x, d.y, d.z);
-      HitRec h = trace_scene<COUNT>(a.s, r, err, cn);
+  const uint32_t n = *count_ptr;
+  ClosestTrav t;
+  bool have = false, exhausted = false;
+  uint32_t slot = 0;
+  while (true) {
+    if (!exhausted) {
+      uint32_t qi = refill(have, cursor, n, exhausted);
+      if (!have && qi < n) {
+        slot = q[qi];
+        float4 o = a.b.ray_o[slot], d = a.b.ray_d[slot];
+        t.rw.origin = mk3(o.x, o.y, o.z);
+        t.rw.direction = mk3(d.x, d.y, d.z);
+        closest_init<COUNT>(a.s, t, cn);
+        have = true;
+      }
+    }
+    if (!__any_sync(FULL, have)) break;
+    if (have && closest_step<COUNT>(a.s, a.P, t, err, cn)) {
+      closest_finish<COUNT>(a.s, t, err, cn);
+      const HitRec& h = t.hit;
       a.b.hit[slot * 2 + 0] = make_uint4(__float_as_uint(h.t), (uint32_t)h.m_idx, (uint32_t)h.o_idx, (uint32_t)h.kind);
       a.b.hit[slot * 2 + 1] = make_uint4((uint32_t)h.id, (uint32_t)h.aux, __float_as_uint(h.bu), __float_as_uint(h.bv));
+      have = false;
     }
   }
   flush_wf<COUNT>(cn, a.counters, true);
@@ -469,26 +505,33 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const ui
 }
 
 // ---------------------------------------------------------------------------- shadow
-// Warps take 32 queue entries at a time from a shared cursor, so warps whose rays finish early
-// keep working instead of idling behind the slowest warp of a static partition.
 template <bool COUNT>
 __global__ void __launch_bounds__(256) k_wf_shadow(WfArgs a, const uint32_t* count_ptr, uint32_t* cursor) {
   Counters<COUNT> cn; cn.init();
   uint32_t err = 0;
   const uint32_t n = *count_ptr;
-  const int lane = threadIdx.x & 31;
+  ShadowTrav t;
+  bool have = false, exhausted = false;
+  uint32_t e = 0;
   while (true) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(cursor, 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    uint32_t i = base + lane;
-    if (i < n) {
-      uint32_t e = a.b.shq[i];
-      float4 so = a.b.shadow[(e >> 1) * 4 + (e & 1u) * 2], sd = a.b.shadow[(e >> 1) * 4 + (e & 1u) * 2 + 1];
-      Ray sr; sr.origin = mk3(so.x, so.y, so.z); sr.direction = mk3(sd.x, sd.y, sd.z);
-      bool occ = scene_occluded<COUNT>(a.s, sr, __float_as_int(sd.w), so.w, err, cn);
-      a.b.vis[e] = occ ? 0u : 1u;
+    if (!exhausted) {
+      uint32_t qi = refill(have, cursor, n, exhausted);
+      if (!have && qi < n) {
+        e = a.b.shq[qi];
+        float4 so = a.b.shadow[(e >> 1) * 4 + (e & 1u) * 2], sd = a.b.shadow[(e >> 1) * 4 + (e & 1u) * 2 + 1];
+        t.rw.origin = mk3(so.x, so.y, so.z);
+        t.rw.direction = mk3(sd.x, sd.y, sd.z);
+        t.target_dist = so.w;
+        t.target_idx = __float_as_int(sd.w);
+        shadow_init<COUNT>(a.s, t, cn);
+        have = true;
+      }
+    }
+    if (!__any_sync(FULL, have)) break;
+    if (have && shadow_step<COUNT>(a.s, a.P, t, err, cn)) {
+      shadow_finish<COUNT>(a.s, t, err, cn);
+      a.b.vis[e] = t.occluded ? 0u : 1u;
+      have = false;
     }
   }
   flush_wf<COUNT>(cn, a.counters, true);
@@ -656,7 +699,8 @@ static cudaError_t render_wf(const WfArgs& a0, uint32_t first_frame, uint32_t re
       uint32_t* qin = a.b.queue[b & 1];
       uint32_t* qout = a.b.queue[(b + 1) & 1];
       if (timer) timer->begin(1, st);
-      k_wf_extend<COUNT><<<std::min(g_ext, need), 256, 0, st>>>(stage_args(1), qin, a.b.counts + b);
+      k_wf_extend<COUNT><<<std::min(g_ext, need), 256, 0, st>>>(stage_args(1), qin, a.b.counts + b,
+                                                                a.b.counts + 64 + b);
       if (timer) timer->end(1, st);
       if (timer) timer->begin(2, st);
       k_wf_shade<COUNT><<<std::min(g_sh, need), 256, 0, st>>>(stage_args(2), b, qin, a.b.counts + b, qout,
@@ -678,12 +722,14 @@ cudaError_t launch_render_wavefront(const DeviceScene& d, const wgpt_scene_param
                                     uint32_t reps, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh, float* accum,
                                     uint8_t* out, uint32_t out_pitch, void* scratch, uint32_t capacity,
                                     uint32_t* status, unsigned long long* counters, cudaStream_t st,
-                                    StageTimer* timer) {
+                                    StageTimer* timer, const void* pairs_tlas, const void* pairs_bvh) {
   uint32_t n = sw * sh;
   if (n == 0) return cudaSuccess;
   if (n > capacity || !scratch) return cudaErrorInvalidValue;
   WfArgs a;
   a.s = to_dscene_wf(d);
+  a.P.tlas = (const float4*)pairs_tlas;
+  a.P.bvh = (const float4*)pairs_bvh;
   a.p = to_dparams_wf(q, sx, sy);
   a.b = carve(scratch, capacity);
   a.sec_w = sw; a.sec_h = sh;

@@ -53,7 +53,7 @@ cudaError_t launch_render_wavefront(const DeviceScene& d, const wgpt_scene_param
                                     uint32_t reps, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh, float* accum,
                                     uint8_t* out, uint32_t out_pitch, void* scratch, uint32_t capacity,
                                     uint32_t* status, unsigned long long* counters, cudaStream_t st,
-                                    StageTimer* timer);
+                                    StageTimer* timer, const void* pairs_tlas, const void* pairs_bvh);
 cudaError_t launch_gbuffer(const DeviceScene& d, const wgpt_scene_params& q, uint32_t sx, uint32_t sy, uint32_t sw,
                            uint32_t sh, float* gbuf, uint8_t* out, uint32_t out_pitch, uint32_t* status,
                            cudaStream_t st);

@@ -48,7 +48,7 @@ BYTES_PER_UNIT = {
     11: 32,   # hit attributes of the winning primitive (normals)
 }
 PIXEL_BYTES = 16 + 16 + 4   # accumulation read + write, rgba8 store
-KERNELS = ["k_wf_raygen", "k_wf_extend", "k_wf_shade", "k_wf_shadow", "k_wf_resolve", "-", "-", "-"]
+KERNELS = ["k_wf_raygen", "k_wf_extend", "k_wf_shade", "k_wf_shadow", "k_wf_resolve", "k_wf_shade_miss", "-", "-"]
 
 
 def algorithmic_bytes(counters: np.ndarray, pixels: int) -> float:

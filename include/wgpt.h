@@ -137,7 +137,7 @@ int wgpt_set_counting(wgpt_ctx* ctx, int on);
 int wgpt_read_counters(wgpt_ctx* ctx, uint64_t* dst16);
 
 /* The same counters split by stage (8 x 16 u64: 0 ray generation or the single kernel,
-   1 closest hit, 2 shading, 3 shadow rays, 4 accumulation, 5-7 unused). */
+   1 closest hit, 2 surface shading, 3 shadow rays, 4 accumulation, 5 miss shading, 6-7 unused). */
 int wgpt_read_stage_counters(wgpt_ctx* ctx, uint64_t* dst128);
 
 /* CUDA-event timing of every stage launch queued while timing is on; wgpt_read_stage_times

@@ -5,7 +5,9 @@
 //   k_wf_raygen       per pixel: RNG seed and discard, jittered camera ray, path state
 //   per bounce b:
 //     k_wf_extend     closest hit of every live path (two-level BVH, planes, list meshes)
-//     k_wf_shade      media, sky / emission terms, light and environment NEE set-up, BSDF
+//     k_wf_shade_miss walks the live queue in order: queues surface hits, shades paths that left
+//                     the scene (media and the sky term)
+//     k_wf_shade      surface hits: media, emission, light and environment NEE set-up, BSDF
 //                     sampling, Russian roulette; appends surviving paths to the next queue and
 //                     records up to two next-event contributions with their shadow rays
 //     k_wf_shadow     traces the recorded shadow rays (their own compacted queue, fetched
@@ -38,9 +40,13 @@ struct WfBuffers {
   uint8_t* vis;      // 2 per path: 1 if the record's shadow ray reached its light
   uint32_t* queue[2];
   uint32_t* shq;     // shadow-ray queue: slot * 2 + record
-  uint32_t* counts;  // [b]: live paths entering bounce b; [64 + b]: rays handed out to warps;
-                     // [128 + b]: shadow rays of bounce b; [192 + b]: shadow rays handed out
+  uint32_t* hitq;    // paths of the current bounce that hit a surface
+  uint32_t* missq;   // paths of the current bounce that left the scene
+  uint32_t* counts;  // counts[c * 256 + b] for bounce b and counter c (see enum Cnt)
 };
+
+enum Cnt : int { CNT_LIVE = 0, CNT_EXT_CURSOR = 1, CNT_HIT = 2, CNT_MISS = 3, CNT_SHADOW = 4, CNT_SH_CURSOR = 5,
+                 CNT_KINDS = 6 };
 
 // meta.y flags
 enum : uint32_t {
@@ -121,7 +127,7 @@ __global__ void __launch_bounds__(256) k_wf_raygen(WfArgs a) {
       a.b.queue[0][slot] = slot;
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) a.b.counts[0] = n;
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.b.counts[CNT_LIVE * 256] = n;
   flush_wf<COUNT>(cn, a.counters, true);
 }
 
@@ -193,6 +199,73 @@ __device__ __forceinline__ void store_medium(const WfArgs& a, uint32_t slot, uin
   a.b.med[slot * 8 + m * 2 + 1] = make_float4(md.emission.x, md.emission.y, md.emission.z, 0.0f);
 }
 
+// Beer-Lambert attenuation and emission of the medium the path travels in (shader.wgsl:2327-2342).
+__device__ __forceinline__ void apply_medium(const MediumStack& stack, const HitRec& hit, int bounce, v3& throughput,
+                                             v3& radiance) {
+  if (stack.count > 0) {
+    Medium cm = peek_medium(stack);
+    if (cm.ior > 1.0f || length(cm.sigma) > 0.0f) {
+      float dist = hit.m_idx == -1 ? 1000.0f : hit.t;
+      v3 attenuation = vexp(-cm.sigma * dist);
+      float ex = cm.sigma.x > 1e-4f ? cm.emission.x * (1.0f - attenuation.x) / cm.sigma.x : cm.emission.x * dist;
+      float ey = cm.sigma.y > 1e-4f ? cm.emission.y * (1.0f - attenuation.y) / cm.sigma.y : cm.emission.y * dist;
+      float ez = cm.sigma.z > 1e-4f ? cm.emission.z * (1.0f - attenuation.z) / cm.sigma.z : cm.emission.z * dist;
+      radiance = radiance + throughput * clamp_firefly(mk3(ex, ey, ez), bounce);
+      throughput = throughput * attenuation;
+    }
+  }
+}
+
+// Walks the bounce's live queue in order: paths that hit a surface go to the hit queue (kept in
+// queue order within each warp, so the surface stage and the next bounce see rays as coherent as
+// the camera's); paths that left the scene are shaded here: medium, then the sky (MIS-weighted
+// after the first bounce) or the background colour (shader.wgsl:2344-2358).  They end here.
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a, int bounce, const uint32_t* __restrict__ q,
+                                                       const uint32_t* count_ptr, uint32_t* hit_count) {
+  Counters<COUNT> cn; cn.init();
+  const DScene& s = a.s;
+  uint32_t n = *count_ptr;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    bool is_hit = false;
+    uint32_t slot = 0;
+    if (i < n) {
+      slot = q[i];
+      is_hit = (int32_t)a.b.hit[slot * 2].y != -1;
+    }
+    queue_push(a.b.hitq, hit_count, slot, is_hit);
+    if (i < n && !is_hit) {
+      float4 d4 = a.b.ray_d[slot], tp4 = a.b.tp[slot], rd4 = a.b.rad[slot];
+      uint4 meta = a.b.meta[slot];
+      HitRec hit;
+      hit.m_idx = -1; hit.t = __uint_as_float(a.b.hit[slot * 2].x);
+      v3 dir = mk3(d4.x, d4.y, d4.z);
+      v3 throughput = mk3(tp4.x, tp4.y, tp4.z);
+      v3 radiance = mk3(rd4.x, rd4.y, rd4.z);
+      if (meta.w > 0u) {
+        MediumStack stack;
+        load_stack(a, slot, meta.w, stack);
+        apply_medium(stack, hit, bounce, throughput, radiance);
+      }
+      if (HAS(s, WGPT_HAS_SKYBOX)) {
+        v3 sky_color = sample_sky(s, dir, cn);
+        float weight = 1.0f;
+        if (bounce > 0 && HAS(s, WGPT_MIS_SKYBOX)) {
+          float sky_pdf = get_sky_pdf(s, a.p, dir, cn);
+          weight = mis_weight(tp4.w, sky_pdf);
+        }
+        radiance = radiance + throughput * clamp_firefly(sky_color * weight, bounce);
+      } else {
+        radiance = radiance + throughput * clamp_firefly(mk3(0.02f, 0.03f, 0.05f), bounce);
+      }
+      a.b.rad[slot] = make_float4(radiance.x, radiance.y, radiance.z, rd4.w);
+      a.b.meta[slot] = make_uint4(meta.x, 0u, (uint32_t)bounce, meta.w);
+    }
+  }
+  flush_wf<COUNT>(cn, a.counters, true);
+}
+
 // Records one next-event contribution: the throughput it is weighted by, the incoming
 // radiance if the light is visible, and the shadow ray to test (when evaluate_nee reaches it).
 template <bool COUNT>
@@ -259,33 +332,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const ui
       MediumStack stack;
       load_stack(a, slot, mcount, stack);
       do {
-        // shader.wgsl:2327-2342
-        if (stack.count > 0) {
-          Medium cm = peek_medium(stack);
-          if (cm.ior > 1.0f || length(cm.sigma) > 0.0f) {
-            float dist = hit.m_idx == -1 ? 1000.0f : hit.t;
-            v3 attenuation = vexp(-cm.sigma * dist);
-            float ex = cm.sigma.x > 1e-4f ? cm.emission.x * (1.0f - attenuation.x) / cm.sigma.x : cm.emission.x * dist;
-            float ey = cm.sigma.y > 1e-4f ? cm.emission.y * (1.0f - attenuation.y) / cm.sigma.y : cm.emission.y * dist;
-            float ez = cm.sigma.z > 1e-4f ? cm.emission.z * (1.0f - attenuation.z) / cm.sigma.z : cm.emission.z * dist;
-            radiance = radiance + throughput * clamp_firefly(mk3(ex, ey, ez), bounce);
-            throughput = throughput * attenuation;
-          }
-        }
-        if (hit.m_idx == -1) {
-          if (HAS(s, WGPT_HAS_SKYBOX)) {
-            v3 sky_color = sample_sky(s, ray.direction, cn);
-            float weight = 1.0f;
-            if (bounce > 0 && HAS(s, WGPT_MIS_SKYBOX)) {
-              float sky_pdf = get_sky_pdf(s, p, ray.direction, cn);
-              weight = mis_weight(last_surface_pdf, sky_pdf);
-            }
-            radiance = radiance + throughput * clamp_firefly(sky_color * weight, bounce);
-          } else {
-            radiance = radiance + throughput * clamp_firefly(mk3(0.02f, 0.03f, 0.05f), bounce);
-          }
-          break;
-        }
+        apply_medium(stack, hit, bounce, throughput, radiance);
         cn.add(C_SHADE);
         cn.add(C_HIT_ATTR);
         DMat mat = load_mat(s, hit.m_idx);
@@ -621,8 +668,8 @@ static DParams to_dparams_wf(const wgpt_scene_params& q, uint32_t sec_x, uint32_
 
 size_t wavefront_bytes_per_path() {
   // ray 32 + tp 16 + rad 16 + meta 16 + media 128 + hit 32 + nee 64 + shadow 64 + vis 2 +
-  // 2 path queues 8 + shadow queue 8
-  return 32 + 16 + 16 + 16 + 128 + 32 + 64 + 64 + 2 + 8 + 8;
+  // 2 path queues 8 + shadow queue 8 + hit and miss queues 8
+  return 32 + 16 + 16 + 16 + 128 + 32 + 64 + 64 + 2 + 8 + 8 + 8;
 }
 
 // Carves the path-state arrays out of one scratch allocation of wavefront_bytes_per_path() *
@@ -645,16 +692,18 @@ static WfBuffers carve(void* scratch, uint32_t capacity) {
   b.queue[0] = (uint32_t*)take(n * 4);
   b.queue[1] = (uint32_t*)take(n * 4);
   b.shq = (uint32_t*)take(n * 8);
-  b.counts = (uint32_t*)take(256 * 4);
+  b.hitq = (uint32_t*)take(n * 4);
+  b.missq = (uint32_t*)take(n * 4);
+  b.counts = (uint32_t*)take(CNT_KINDS * 256 * 4);
   return b;
 }
 
 size_t wavefront_scratch_bytes(uint32_t capacity) {
   size_t n = capacity, s = 0;
-  size_t parts[13] = {n * 16, n * 16, n * 16, n * 16, n * 16, n * 128, n * 32, n * 64, n * 64, n * 2, n * 4, n * 4,
-                      n * 8};
+  size_t parts[15] = {n * 16, n * 16, n * 16, n * 16, n * 16, n * 128, n * 32, n * 64, n * 64, n * 2, n * 4, n * 4,
+                      n * 8, n * 4, n * 4};
   for (size_t x : parts) s += (x + 255) & ~(size_t)255;
-  return s + 256 * 4;
+  return s + CNT_KINDS * 256 * 4;
 }
 
 static int g_grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // persistent grid size per stage (computed once)
@@ -682,16 +731,19 @@ static cudaError_t render_wf(const WfArgs& a0, uint32_t first_frame, uint32_t re
     return x;
   };
   int bl = a.s.bounce_limit;
-  if (bl > 250) return cudaErrorInvalidValue;
+  if (bl > 255) return cudaErrorInvalidValue;
   int g_ray = grid_for(k_wf_raygen<COUNT>, 0);
   int g_ext = grid_for(k_wf_extend<COUNT>, 1);
   int g_sh = grid_for(k_wf_shade<COUNT>, 2);
   int g_shw = grid_for(k_wf_shadow<COUNT>, 3);
   int g_res = grid_for(k_wf_resolve<COUNT>, 4);
   int need = (int)((n + 255) / 256);
+  int g_miss = grid_for(k_wf_shade_miss<COUNT>, 5);
+  uint32_t* C = a.b.counts;
+  auto cnt = [&](int kind, int b) { return C + kind * 256 + b; };
   for (uint32_t r = 0; r < reps; ++r) {
     a.sample_number = first_frame + r;
-    cudaMemsetAsync(a.b.counts, 0, 256 * 4, st);
+    cudaMemsetAsync(C, 0, CNT_KINDS * 256 * 4, st);
     if (timer) timer->begin(0, st);
     k_wf_raygen<COUNT><<<std::min(g_ray, need), 256, 0, st>>>(stage_args(0));
     if (timer) timer->end(0, st);
@@ -699,19 +751,23 @@ static cudaError_t render_wf(const WfArgs& a0, uint32_t first_frame, uint32_t re
       uint32_t* qin = a.b.queue[b & 1];
       uint32_t* qout = a.b.queue[(b + 1) & 1];
       if (timer) timer->begin(1, st);
-      k_wf_extend<COUNT><<<std::min(g_ext, need), 256, 0, st>>>(stage_args(1), qin, a.b.counts + b,
-                                                                a.b.counts + 64 + b);
+      k_wf_extend<COUNT><<<std::min(g_ext, need), 256, 0, st>>>(stage_args(1), qin, cnt(CNT_LIVE, b),
+                                                                cnt(CNT_EXT_CURSOR, b));
       if (timer) timer->end(1, st);
+      if (timer) timer->begin(5, st);
+      k_wf_shade_miss<COUNT><<<std::min(g_miss, need), 256, 0, st>>>(stage_args(5), b, qin, cnt(CNT_LIVE, b),
+                                                                     cnt(CNT_HIT, b));
+      if (timer) timer->end(5, st);
       if (timer) timer->begin(2, st);
-      k_wf_shade<COUNT><<<std::min(g_sh, need), 256, 0, st>>>(stage_args(2), b, qin, a.b.counts + b, qout,
-                                                               a.b.counts + b + 1, a.b.counts + 128 + b);
+      k_wf_shade<COUNT><<<std::min(g_sh, need), 256, 0, st>>>(stage_args(2), b, a.b.hitq, cnt(CNT_HIT, b), qout,
+                                                               cnt(CNT_LIVE, b + 1), cnt(CNT_SHADOW, b));
       if (timer) timer->end(2, st);
       if (timer) timer->begin(3, st);
-      k_wf_shadow<COUNT><<<std::min(g_shw, 2 * need), 256, 0, st>>>(stage_args(3), a.b.counts + 128 + b,
-                                                                   a.b.counts + 192 + b);
+      k_wf_shadow<COUNT><<<std::min(g_shw, 2 * need), 256, 0, st>>>(stage_args(3), cnt(CNT_SHADOW, b),
+                                                                   cnt(CNT_SH_CURSOR, b));
       if (timer) timer->end(3, st);
       if (timer) timer->begin(4, st);
-      k_wf_resolve<COUNT><<<std::min(g_res, need), 256, 0, st>>>(stage_args(4), qin, a.b.counts + b);
+      k_wf_resolve<COUNT><<<std::min(g_res, need), 256, 0, st>>>(stage_args(4), qin, cnt(CNT_LIVE, b));
       if (timer) timer->end(4, st);
     }
   }

@@ -1849,9 +1849,10 @@ int oracle_bsdf(const void* material144, const float* normal3, float roughness, 
   return 0;
 }
 
-// The PCG stream of one pixel (shader.wgsl:146-154, 2280-2282): the discard is included.
+// The PCG stream of one pixel (shader.wgsl:146-154, 2280-2282) after the seeding discard.
 void oracle_rng_stream(uint32_t idx, uint32_t sample_number, uint32_t seed, uint32_t n, float* out) {
   uint32_t st = (idx * 1973u + sample_number * 9277u + seed * 26699u) | 1u;
+  rand_pcg(st);
   for (uint32_t i = 0; i < n; ++i) out[i] = rand_pcg(st);
 }
 

@@ -30,7 +30,8 @@ enum wgpt_status {
   WGPT_E_STATE = 5,       /* call out of order (no scene, no size, no G-buffer) */
   WGPT_E_UNSUPPORTED = 6, /* textures / parallax maps (not part of this build) */
   WGPT_E_REBUILD = 7,     /* wgpt_update_scene: the new data does not fit, upload again */
-  WGPT_E_DEVICE = 8       /* a kernel reported an error (traversal stack overflow) */
+  WGPT_E_DEVICE = 8,      /* a kernel reported an error (traversal stack overflow) */
+  WGPT_E_TOO_LARGE = 9    /* wgpt_denoise_noalloc: more than WGPT_NOALLOC_MAX_PIXELS pixels */
 };
 
 typedef struct wgpt_ctx wgpt_ctx;
@@ -147,6 +148,25 @@ int wgpt_read_stage_times(wgpt_ctx* ctx, double* ms8, uint32_t* launches8);
 
 /* The context's cudaStream_t (as void*) for callers that time or order work around it. */
 void* wgpt_stream(wgpt_ctx* ctx);
+
+/* Denoiser without any allocation (no counterpart in the reference).  For callers that cannot
+   call cudaMalloc: code running while a stream is being captured into a CUDA graph (where the
+   runtime refuses allocations), hosts that fix their GPU memory budget up front, and real-time
+   loops that must not stall on the allocator.  It runs the same prepass / a-trous / composite
+   kernels as wgpt_denoise, with the same results, but takes every input and output as a caller
+   device pointer (color: W*H float4, gbuf: W*H 48-byte texels, out_rgba8: W*H*4 bytes,
+   out_composited: W*H float4 or NULL) and keeps its intermediate images in one static device
+   array of WGPT_NOALLOC_MAX_PIXELS * 80 bytes (10 MiB) that each GPU loading the library holds
+   until the process exits.  uniforms_48 and steps are host memory.  Images larger than
+   WGPT_NOALLOC_MAX_PIXELS return WGPT_E_TOO_LARGE before any work is queued.  The first call on
+   a device looks up the array's device address (cudaGetSymbolAddress) with that device current:
+   make that first call before capturing a stream.  Work is queued on `stream` (a
+   cudaStream_t, NULL for the legacy default stream) on the current device.  All calls share the
+   one array: calls that overlap on the GPU (different streams, or different host threads)
+   race and corrupt each other's intermediates; queue them on one stream. */
+#define WGPT_NOALLOC_MAX_PIXELS 131072u
+int wgpt_denoise_noalloc(const float* color, const void* gbuf, const void* uniforms_48, const uint32_t* steps,
+                         uint32_t passes, uint8_t* out_rgba8, float* out_composited, void* stream);
 
 /* Host-side builders of the scene buffers (tracer.js host math, native): */
 /* ModelData.generateBVH (tracer.js:1025-1118): binned-SAH BLAS over n triangles given as

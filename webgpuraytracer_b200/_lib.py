@@ -14,7 +14,9 @@ WGPT_OK = 0
 STATUS_NAMES = {
     0: "WGPT_OK", 1: "WGPT_E_INVALID", 2: "WGPT_E_LAYOUT", 3: "WGPT_E_CUDA", 4: "WGPT_E_NOMEM",
     5: "WGPT_E_STATE", 6: "WGPT_E_UNSUPPORTED", 7: "WGPT_E_REBUILD", 8: "WGPT_E_DEVICE",
+    9: "WGPT_E_TOO_LARGE",
 }
+NOALLOC_MAX_PIXELS = 131072
 
 MODE_WAVEFRONT = 0
 MODE_MEGAKERNEL = 1
@@ -81,6 +83,7 @@ EXPORTS = {
     "wgpt_read_canvas": ([_P, _P, _U32, _U32], C.c_int),
     "wgpt_trace_rays": ([_P, _P, _U32, _P, _P, _P, _P, _P], C.c_int),
     "wgpt_set_render_mode": ([_P, C.c_int], C.c_int),
+    "wgpt_denoise_noalloc": ([_P, _P, _P, _P, _U32, _P, _P, _P], C.c_int),
     "wgpt_set_counting": ([_P, C.c_int], C.c_int),
     "wgpt_read_counters": ([_P, _P], C.c_int),
     "wgpt_read_stage_counters": ([_P, _P], C.c_int),

@@ -10,9 +10,12 @@
 // normal (3), normal length, depth mapped by d/(d+3), tonemapped albedo (3),
 // and (transmission, roughness, metallic) -- 12 floats, so the per-tap arithmetic is unchanged.
 #include <stdint.h>
+#include <string.h>
+#include <mutex>
 #include <cuda_runtime.h>
 #include "wgsl_builtins.h"
 #include "wgpt_internal.h"
+#include "../../include/wgpt.h"
 
 using namespace wb;
 
@@ -208,3 +211,53 @@ cudaError_t launch_resample(const uint8_t* src, uint32_t sw, uint32_t sh, uint8_
 }
 
 }  // namespace wgpt
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free denoiser entry point.
+//
+// The ping-pong buffers (16 B/pixel each) and the guide record (48 B/pixel) of the denoiser
+// live in one file-scope device array of WGPT_NOALLOC_MAX_PIXELS * 80 bytes (10 MiB) that every
+// GPU loading this library holds until the process exits.  Host code cannot use the array's
+// name as a device address (it is a host-side stand-in), so the first call on each device looks
+// the address up with cudaGetSymbolAddress while that device is current and keeps it.
+static __device__ __align__(256) float4 g_noalloc_scratch[(size_t)WGPT_NOALLOC_MAX_PIXELS * 5];
+
+namespace {
+constexpr int kMaxDevices = 64;
+float4* g_noalloc_addr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mu;
+}  // namespace
+
+extern "C" int wgpt_denoise_noalloc(const float* color, const void* gbuf, const void* uniforms_48,
+                                    const uint32_t* steps, uint32_t passes, uint8_t* out_rgba8,
+                                    float* out_composited, void* stream) {
+  if (!color || !gbuf || !uniforms_48 || !out_rgba8 || (passes && !steps)) return WGPT_E_INVALID;
+  wgpt_denoise_uniforms u;
+  memcpy(&u, uniforms_48, sizeof u);
+  if (u.width == 0 || u.height == 0) return WGPT_E_INVALID;
+  if ((uint64_t)u.width * u.height > WGPT_NOALLOC_MAX_PIXELS) return WGPT_E_TOO_LARGE;
+  if (passes > 64) return WGPT_E_INVALID;
+  for (uint32_t i = 0; i < passes; ++i)
+    if (steps[i] == 0 || steps[i] > (1u << 20)) return WGPT_E_INVALID;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return WGPT_E_CUDA;
+  float4* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return WGPT_E_CUDA;
+      g_noalloc_addr[dev] = (float4*)p;
+    }
+    base = g_noalloc_addr[dev];
+  }
+  // Nothing in the scratch has to start at zero: the prepass writes every pixel of the first
+  // buffer and of the guide, and every pass writes each pixel it later reads.
+  const size_t npix = (size_t)u.width * u.height;
+  float* buf_a = (float*)base;
+  float* buf_b = (float*)(base + npix);
+  float* guide = (float*)(base + 2 * npix);
+  cudaError_t e = wgpt::launch_denoise(color, (const float*)gbuf, u, steps, passes, buf_a, buf_b, guide,
+                                       out_composited, out_rgba8, nullptr, (cudaStream_t)stream);
+  return e == cudaSuccess ? WGPT_OK : WGPT_E_CUDA;
+}

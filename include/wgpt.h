@@ -90,13 +90,23 @@ int wgpt_set_params(wgpt_ctx* ctx, const void* scene_params_112);
 int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sec_x, uint32_t sec_y,
                 uint32_t sec_w, uint32_t sec_h);
 
-/* How wgpt_render runs a sample: WGPT_MODE_WAVEFRONT (default) splits each bounce into closest-
-   hit, shading and shadow/accumulate kernels over compacted path queues (path state in a
-   context-owned buffer of about 440 bytes per pixel); WGPT_MODE_MEGAKERNEL runs one thread per
-   path through all bounces, like the reference's single compute entry point.  Both produce
-   identical results. */
+/* How wgpt_render runs its samples: WGPT_MODE_WAVEFRONT (default) treats every (sample, pixel)
+   of the call as a work unit traced by a pool of path slots through closest-hit, shading,
+   shadow and resolve kernels over compacted queues; a slot whose path ends starts the next unit
+   at once (path regeneration), the iteration loop is one CUDA-graph launch, and each pixel's
+   samples are folded into the running mean in sample order at the end.  WGPT_MODE_MEGAKERNEL
+   runs one thread per pixel through all bounces and samples, like the reference's single
+   compute entry point.  Both produce identical results. */
 enum { WGPT_MODE_WAVEFRONT = 0, WGPT_MODE_MEGAKERNEL = 1 };
 int wgpt_set_render_mode(wgpt_ctx* ctx, int mode);
+
+/* Wavefront sizing (no counterpart in the reference, whose dispatch has no path pool):
+   pool_paths path slots (1,024 .. 67,108,864; default 2,097,152; about 420 bytes each) and at
+   most units_per_pass samples held (65,536 .. 2^30; default 2^27; 16 bytes each) before they are
+   folded into the images; a call with more samples runs in several passes.  Results do not
+   depend on either.  0 keeps the current value. */
+int wgpt_set_wavefront_config(wgpt_ctx* ctx, uint32_t pool_paths, uint64_t units_per_pass);
+int wgpt_get_wavefront_config(wgpt_ctx* ctx, uint32_t* pool_paths, uint64_t* units_per_pass);
 
 /* setScene(scene, true) + render(): one dispatch of gbuf_main (shader.wgsl:2510-2603) into the
    G-buffer and the debug quadrant image. */

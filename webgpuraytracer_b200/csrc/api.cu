@@ -44,7 +44,6 @@ struct wgpt_ctx {
   uint32_t* d_status = nullptr;
   unsigned long long* d_counters = nullptr;
   bool counting = false;
-  // wavefront path state (scratch sized for the whole image)
   int mode = WGPT_MODE_WAVEFRONT;
   // derived child-pair node arrays (64 bytes per node) of the TLAS and the BLAS buffer
   void* d_pairs_tlas = nullptr;
@@ -52,8 +51,7 @@ struct wgpt_ctx {
   size_t pairs_cap[2] = {0, 0};
   wgpt::StageTimer* timer = nullptr;
   bool timing = false;
-  void* wf_scratch = nullptr;
-  uint32_t wf_capacity = 0;
+  wgpt::WfEngine* wf = nullptr;   // wavefront renderer: path pool, sample buffer, loop graph
 };
 
 namespace {
@@ -403,7 +401,8 @@ int wgpt_destroy(wgpt_ctx* ctx) {
   for (int k = 0; k < 10; ++k) dfree(ctx->d_buf[k]);
   dfree_t(ctx->accum); dfree_t(ctx->out); dfree_t(ctx->gbuf);
   dfree_t(ctx->dn_a); dfree_t(ctx->dn_b); dfree_t(ctx->dn_guide); dfree_t(ctx->dn_comp);
-  dfree_t(ctx->canvas); dfree_t(ctx->d_status); dfree_t(ctx->d_counters); dfree(ctx->wf_scratch);
+  dfree_t(ctx->canvas); dfree_t(ctx->d_status); dfree_t(ctx->d_counters); wgpt::wf_engine_destroy(ctx->wf);
+  ctx->wf = nullptr;
   dfree(ctx->d_pairs_tlas); dfree(ctx->d_pairs_bvh);
   if (ctx->timer) {
     if (ctx->timer->ready)
@@ -513,18 +512,18 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
     if (tm) tm->end(0, ctx->stream);
     return WGPT_OK;
   }
-  uint32_t need = ctx->w * ctx->h;
-  if (ctx->wf_capacity < need) {
-    CK(cudaStreamSynchronize(ctx->stream), "drain before path-state allocation");
-    dfree(ctx->wf_scratch);
-    ctx->wf_capacity = 0;
-    CK(cudaMalloc(&ctx->wf_scratch, wgpt::wavefront_scratch_bytes(need)), "cudaMalloc path state");
-    ctx->wf_capacity = need;
-  }
-  CK(wgpt::launch_render_wavefront(ctx->ds, ctx->params, first_frame, reps, sx, sy, sw, sh, ctx->accum, ctx->out,
-                                   ctx->w, ctx->wf_scratch, ctx->wf_capacity, ctx->d_status, cnt, ctx->stream, tm,
-                                   ctx->d_pairs_tlas, ctx->d_pairs_bvh),
-     "wavefront render launch");
+  if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
+  wgpt::WfJobView v;
+  v.q = ctx->params;
+  v.sx = sx; v.sy = sy; v.sw = sw; v.sh = sh;
+  v.first_frame = first_frame;
+  v.spp = reps;
+  v.accum = ctx->accum;
+  v.out = ctx->out;
+  v.out_pitch = ctx->w;
+  CK(wgpt::wf_render(ctx->wf, ctx->ds, ctx->d_pairs_tlas, ctx->d_pairs_bvh, &v, 1, ctx->d_status, cnt, ctx->stream,
+                     tm),
+     "wavefront render");
   return WGPT_OK;
 }
 
@@ -588,7 +587,8 @@ int wgpt_synchronize(wgpt_ctx* ctx) {
   CK(cudaMemcpy(&st, ctx->d_status, sizeof st, cudaMemcpyDeviceToHost), "status readback");
   if (st) {
     CK(cudaMemset(ctx->d_status, 0, sizeof st), "status reset");
-    return fail(ctx, WGPT_E_DEVICE, "a kernel overflowed its 64-entry traversal stack");
+    if (st & 2u) return fail(ctx, WGPT_E_DEVICE, "the wavefront loop reached its iteration bound with paths left");
+    return fail(ctx, WGPT_E_DEVICE, "a kernel overflowed its traversal stack");
   }
   return WGPT_OK;
 }
@@ -677,6 +677,26 @@ int wgpt_set_render_mode(wgpt_ctx* ctx, int mode) {
   if (!ctx) return WGPT_E_INVALID;
   if (mode != WGPT_MODE_WAVEFRONT && mode != WGPT_MODE_MEGAKERNEL) return fail(ctx, WGPT_E_INVALID, "unknown render mode");
   ctx->mode = mode;
+  return WGPT_OK;
+}
+
+int wgpt_set_wavefront_config(wgpt_ctx* ctx, uint32_t pool_paths, uint64_t units_per_pass) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
+  uint32_t cur_pool = 0;
+  uint64_t cur_units = 0;
+  wgpt::wf_engine_get(ctx->wf, &cur_pool, &cur_units);
+  if (pool_paths == 0) pool_paths = cur_pool;
+  if (units_per_pass == 0) units_per_pass = cur_units;
+  if (wgpt::wf_engine_configure(ctx->wf, pool_paths, units_per_pass))
+    return fail(ctx, WGPT_E_INVALID, "wavefront sizing out of range (pool 1024..2^26 paths, 2^16..2^30 units)");
+  return WGPT_OK;
+}
+
+int wgpt_get_wavefront_config(wgpt_ctx* ctx, uint32_t* pool_paths, uint64_t* units_per_pass) {
+  if (!ctx || !pool_paths || !units_per_pass) return WGPT_E_INVALID;
+  if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
+  wgpt::wf_engine_get(ctx->wf, pool_paths, units_per_pass);
   return WGPT_OK;
 }
 

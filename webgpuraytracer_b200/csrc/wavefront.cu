@@ -1,26 +1,32 @@
 // Wavefront form of the progressive renderer's path tracing (shader.wgsl main, 2273-2492).
 //
-// A sample of a section is rendered by a sequence of small kernels over compacted path queues
-// instead of one thread running a whole path:
-//   k_wf_raygen       per pixel: RNG seed and discard, jittered camera ray, path state
-//   per bounce b:
-//     k_wf_extend     closest hit of every live path (two-level BVH, planes, list meshes)
-//     k_wf_shade_miss walks the live queue in order: queues surface hits, shades paths that left
-//                     the scene (media and the sky term)
-//     k_wf_shade      surface hits: media, emission, light and environment NEE set-up, BSDF
-//                     sampling, Russian roulette; appends surviving paths to the next queue and
-//                     records up to two next-event contributions with their shadow rays
-//     k_wf_shadow     traces the recorded shadow rays (their own compacted queue, fetched
-//                     dynamically by warps) and stores one visibility byte per record
-//     k_wf_resolve    adds the next-event contributions (light first, then environment, as main
-//                     does), then accumulates finished paths into the running mean and the rgba8
-//                     image
-// Each stage keeps only its own code and registers resident, so warps stay converged on one
-// code path and the instruction cache holds the stage (the single-kernel form stalls on
-// instruction fetch).  Every floating-point operation and random draw happens in the order of
-// the reference; only the place where it happens changes, so results equal the single-kernel
-// form and the CPU restatement bit for bit.
+// The samples of one render call -- every (view, sample, pixel) of a batch of camera views --
+// are work units, numbered view by view, sample-major inside a view.  A fixed pool of path slots
+// traces them; a slot whose path ends takes the next unit at once (path regeneration), so the
+// queues stay full until the last units drain instead of shrinking bounce after bounce.
+// One iteration runs each stage once over the slots that hold a path:
+//   k_wf_extend     closest hit of every queued path (two-level BVH, planes, list meshes)
+//   k_wf_shade_miss walks the queue in order: queues surface hits, shades paths that left the
+//                   scene (media and the sky term)
+//   k_wf_shade      surface hits: media, emission, light and environment NEE set-up, BSDF
+//                   sampling, Russian roulette; records up to two next-event contributions with
+//                   their shadow rays
+//   k_wf_shadow     traces the recorded shadow rays (their own compacted queue, fetched
+//                   dynamically by warps) and stores one visibility byte per record
+//   k_wf_resolve    adds the next-event contributions (light first, then environment, as main
+//                   does); a path that continues is queued for the next iteration, a finished
+//                   path stores its radiance under its unit and the slot starts the next unit
+//   k_wf_control    advances the iteration and decides whether another one runs
+// The loop is a WHILE node of a CUDA graph (the control kernel sets its condition), so a render
+// call is one graph launch.  k_wf_accumulate then folds each pixel's samples into the running
+// mean in sample order, so the accumulation buffer and the rgba8 image equal the reference's
+// frame-by-frame result bit for bit, whatever order the paths finished in.  Every
+// floating-point operation and random draw of a path happens in the order of the reference;
+// only the place where it happens changes, so results equal the single-kernel form and the CPU
+// restatement bit for bit.
 #include <algorithm>
+#include <cstring>
+#include <vector>
 #include "pt_device.cuh"
 #include "traverse.cuh"
 #include "wgpt_internal.h"
@@ -32,21 +38,21 @@ struct WfBuffers {
   float4* ray_d;     // direction.xyz
   float4* tp;        // throughput.xyz, last_surface_pdf
   float4* rad;       // radiance.xyz, last_weight_sum
-  uint4* meta;       // rng, flags, bounce of the pending records, medium count
+  uint4* meta;       // rng, flags, bounce of the current segment, medium count
+  uint32_t* unit;    // work unit of the slot's path
   float4* med;       // 8 per path: (ior, sigma.xyz), (emission.xyz, -) for media 0..3
   uint4* hit;        // 2 per path: (t, m_idx, o_idx, kind), (id, aux, bu, bv)
   float4* nee;       // 4 per path: (tp.xyz, -), (incoming.xyz, -) for the light and env records
   float4* shadow;    // 4 per path: (origin.xyz, target_dist), (direction.xyz, ignore_idx) x 2
   uint8_t* vis;      // 2 per path: 1 if the record's shadow ray reached its light
-  uint32_t* queue[2];
+  uint32_t* qcont[2];  // paths continuing into the iteration (ping-pong by iteration parity)
+  uint32_t* qnew[2];   // slots that started a new unit for the iteration
+  uint32_t* hitq;    // paths of the iteration that hit a surface
   uint32_t* shq;     // shadow-ray queue: slot * 2 + record
-  uint32_t* hitq;    // paths of the current bounce that hit a surface
-  uint32_t* missq;   // paths of the current bounce that left the scene
-  uint32_t* counts;  // counts[c * 256 + b] for bounce b and counter c (see enum Cnt)
 };
 
-enum Cnt : int { CNT_LIVE = 0, CNT_EXT_CURSOR = 1, CNT_HIT = 2, CNT_MISS = 3, CNT_SHADOW = 4, CNT_SH_CURSOR = 5,
-                 CNT_KINDS = 6 };
+// Per-iteration counters, a ring of four sets indexed by iteration & 3.
+enum Cnt : int { K_CONT = 0, K_NEW = 1, K_EXT_CURSOR = 2, K_HIT = 3, K_SHADOW = 4, K_SH_CURSOR = 5, K_NKINDS = 8 };
 
 // meta.y flags
 enum : uint32_t {
@@ -57,23 +63,70 @@ enum : uint32_t {
   F_SHADOW_ENV = 16u
 };
 
+}  // namespace pt
+
+namespace wgpt {
+
+// One camera view of a pass: its parameters, its section and the samples it gets.
+struct WfView {
+  pt::DParams p;          // the view's 112-byte parameters; sec_x/sec_y = section origin
+  uint32_t sec_w, npix;   // section width, section pixel count
+  uint32_t first_frame;   // sample_number of the pass's first sample of the view
+  uint32_t spp;           // samples of the view in the pass
+  uint32_t unit_base;     // unit = unit_base + sample * npix + pixel
+  uint32_t pix_base;      // first pixel of the view in the pass's pixel numbering
+  uint32_t out_pitch;     // pixels per row of the view's images
+  uint32_t pad;
+  float4* accum;
+  uchar4* out;
+};
+
+// Device control block of a pass.
+struct WfCtl {
+  uint32_t iter;          // current iteration
+  uint32_t unit_next;     // next unit to hand out
+  uint32_t n_units;       // units of the pass
+  uint32_t max_iter;      // bound on the iterations (host-computed; the loop stops there)
+  uint32_t n_views, n_pixels, fill_count, cond;
+  uint32_t counts[4][pt::K_NKINDS];
+  pt::DParams sp;         // scene-level parameters (sky size, luminance, CDF offset) of the pass
+};
+
+}  // namespace wgpt
+
+namespace pt {
+
+using wgpt::WfCtl;
+using wgpt::WfView;
+
+enum : uint32_t { ERR_ITER = 2u };   // the iteration bound was reached with paths left
+
 struct WfArgs {
   DScene s;
   DPairs P;
-  DParams p;
   WfBuffers b;
-  uint32_t sec_w, sec_h;
-  uint32_t sample_number;
-  float4* accum;
-  uchar4* out;
-  uint32_t out_pitch;
+  const WfView* views;
+  WfCtl* ctl;
+  float4* samples;        // radiance of every unit of the pass
   uint32_t* status;
   unsigned long long* counters;
 };
 
-__device__ __forceinline__ void px_of(const WfArgs& a, uint32_t slot, uint32_t& ix, uint32_t& iy) {
-  ix = a.p.sec_x + slot % a.sec_w;
-  iy = a.p.sec_y + slot / a.sec_w;
+// The iteration's input queue: continuing paths, then the slots that started a new unit.
+struct QIn {
+  const uint32_t* qc;
+  const uint32_t* qn;
+  uint32_t nc, n;
+  __device__ __forceinline__ uint32_t at(uint32_t i) const { return i < nc ? qc[i] : qn[i - nc]; }
+};
+__device__ __forceinline__ QIn queue_in(const WfArgs& a, uint32_t iter) {
+  QIn q;
+  uint32_t r = iter & 3u, p = iter & 1u;
+  q.qc = a.b.qcont[p];
+  q.qn = a.b.qnew[p];
+  q.nc = a.ctl->counts[r][K_CONT];
+  q.n = q.nc + a.ctl->counts[r][K_NEW];
+  return q;
 }
 
 template <bool COUNT>
@@ -100,34 +153,60 @@ __device__ __forceinline__ void queue_push(uint32_t* q, uint32_t* count, uint32_
   if (push) q[base + __popc(mask & ((1u << lane) - 1u))] = slot;
 }
 
-// ---------------------------------------------------------------------------- raygen
+// The view a unit belongs to (views are ordered by unit_base).
+__device__ __forceinline__ const WfView* find_view(const WfArgs& a, uint32_t n_views, uint32_t u) {
+  uint32_t lo = 0, hi = n_views;
+  while (hi - lo > 1u) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (a.views[mid].unit_base <= u) lo = mid; else hi = mid;
+  }
+  return a.views + lo;
+}
+
+// Starts unit `u` in path slot `slot`: RNG seeding and discard, jittered camera ray
+// (shader.wgsl:2276-2287 with sample_number = the unit's sample).
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_wf_raygen(WfArgs a) {
+__device__ __forceinline__ void spawn(const WfArgs& a, uint32_t n_views, uint32_t slot, uint32_t u,
+                                      Counters<COUNT>& cn) {
+  const WfView* v = find_view(a, n_views, u);
+  uint32_t l = u - v->unit_base;
+  uint32_t k = l / v->npix;
+  uint32_t pix = l - k * v->npix;
+  uint32_t ix = v->p.sec_x + pix % v->sec_w;
+  uint32_t iy = v->p.sec_y + pix / v->sec_w;
+  uint32_t width = v->p.width, height = v->p.height;
+  uint32_t idx = iy * width + ix;
+  uint32_t sample_number = v->first_frame + k;
+  uint32_t rng = (idx * 1973u + sample_number * 9277u + v->p.seed * 26699u) | 1u;
+  rand_pcg(rng);
+  cn.add(C_PATHS);
+  float j0 = rand_pcg(rng);
+  float j1 = rand_pcg(rng);
+  float su = ((float)ix + j0) / (float)width;
+  float sv = ((float)iy + j1) / (float)height;
+  v3 d = normalize(vmix(vmix(v->p.ray00, v->p.ray10, su), vmix(v->p.ray01, v->p.ray11, su), 1.0f - sv));
+  v3 eye = v->p.eye;
+  a.b.ray_o[slot] = make_float4(eye.x, eye.y, eye.z, 0.0f);
+  a.b.ray_d[slot] = make_float4(d.x, d.y, d.z, 0.0f);
+  a.b.tp[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+  a.b.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  a.b.meta[slot] = make_uint4(rng, 0u, 0u, 0u);
+  a.b.unit[slot] = u;
+}
+
+// ---------------------------------------------------------------------------- fill
+// Starts the pass: slot i takes unit i for the first fill_count units.
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_wf_fill(WfArgs a) {
   Counters<COUNT> cn; cn.init();
-  uint32_t n = a.sec_w * a.sec_h;
+  const uint32_t n = a.ctl->fill_count, n_views = a.ctl->n_views;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t slot = base + threadIdx.x;
     if (slot < n) {
-      uint32_t ix, iy;
-      px_of(a, slot, ix, iy);
-      uint32_t idx = iy * a.p.width + ix;
-      uint32_t rng = (idx * 1973u + a.sample_number * 9277u + a.p.seed * 26699u) | 1u;
-      rand_pcg(rng);
-      cn.add(C_PATHS);
-      float j0 = rand_pcg(rng);
-      float j1 = rand_pcg(rng);
-      float su = ((float)ix + j0) / (float)a.p.width;
-      float sv = ((float)iy + j1) / (float)a.p.height;
-      v3 d = normalize(vmix(vmix(a.p.ray00, a.p.ray10, su), vmix(a.p.ray01, a.p.ray11, su), 1.0f - sv));
-      a.b.ray_o[slot] = make_float4(a.p.eye.x, a.p.eye.y, a.p.eye.z, 0.0f);
-      a.b.ray_d[slot] = make_float4(d.x, d.y, d.z, 0.0f);
-      a.b.tp[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-      a.b.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      a.b.meta[slot] = make_uint4(rng, 0u, 0u, 0u);
-      a.b.queue[0][slot] = slot;
+      spawn<COUNT>(a, n_views, slot, slot, cn);
+      a.b.qnew[0][slot] = slot;
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) a.b.counts[CNT_LIVE * 256] = n;
   flush_wf<COUNT>(cn, a.counters, true);
 }
 
@@ -153,11 +232,13 @@ __device__ __forceinline__ uint32_t refill(bool have, uint32_t* cursor, uint32_t
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_wf_extend(WfArgs a, const uint32_t* __restrict__ q, const uint32_t* count_ptr,
-                                                   uint32_t* cursor) {
+__global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   uint32_t err = 0;
-  const uint32_t n = *count_ptr;
+  const uint32_t iter = a.ctl->iter;
+  const QIn q = queue_in(a, iter);
+  const uint32_t n = q.n;
+  uint32_t* cursor = &a.ctl->counts[iter & 3u][K_EXT_CURSOR];
   ClosestTrav t;
   bool have = false, exhausted = false;
   uint32_t slot = 0;
@@ -165,7 +246,7 @@ __global__ void __launch_bounds__(256) k_wf_extend(WfArgs a, const uint32_t* __r
     if (!exhausted) {
       uint32_t qi = refill(have, cursor, n, exhausted);
       if (!have && qi < n) {
-        slot = q[qi];
+        slot = q.at(qi);
         float4 o = a.b.ray_o[slot], d = a.b.ray_d[slot];
         t.rw.origin = mk3(o.x, o.y, o.z);
         t.rw.direction = mk3(d.x, d.y, d.z);
@@ -216,28 +297,32 @@ __device__ __forceinline__ void apply_medium(const MediumStack& stack, const Hit
   }
 }
 
-// Walks the bounce's live queue in order: paths that hit a surface go to the hit queue (kept in
-// queue order within each warp, so the surface stage and the next bounce see rays as coherent as
-// the camera's); paths that left the scene are shaded here: medium, then the sky (MIS-weighted
-// after the first bounce) or the background colour (shader.wgsl:2344-2358).  They end here.
+// Walks the iteration's queue in order: paths that hit a surface go to the hit queue (kept in
+// queue order within each warp, so the surface stage sees rays as coherent as the queue); paths
+// that left the scene are shaded here: medium, then the sky (MIS-weighted after the first
+// bounce) or the background colour (shader.wgsl:2344-2358).  They end here.
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a, int bounce, const uint32_t* __restrict__ q,
-                                                       const uint32_t* count_ptr, uint32_t* hit_count) {
+__global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   const DScene& s = a.s;
-  uint32_t n = *count_ptr;
+  const uint32_t iter = a.ctl->iter;
+  const QIn q = queue_in(a, iter);
+  const uint32_t n = q.n;
+  uint32_t* hit_count = &a.ctl->counts[iter & 3u][K_HIT];
+  const DParams& sp = a.ctl->sp;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     bool is_hit = false;
     uint32_t slot = 0;
     if (i < n) {
-      slot = q[i];
+      slot = q.at(i);
       is_hit = (int32_t)a.b.hit[slot * 2].y != -1;
     }
     queue_push(a.b.hitq, hit_count, slot, is_hit);
     if (i < n && !is_hit) {
       float4 d4 = a.b.ray_d[slot], tp4 = a.b.tp[slot], rd4 = a.b.rad[slot];
       uint4 meta = a.b.meta[slot];
+      const int bounce = (int)meta.z;
       HitRec hit;
       hit.m_idx = -1; hit.t = __uint_as_float(a.b.hit[slot * 2].x);
       v3 dir = mk3(d4.x, d4.y, d4.z);
@@ -252,7 +337,7 @@ __global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a, int bounce, con
         v3 sky_color = sample_sky(s, dir, cn);
         float weight = 1.0f;
         if (bounce > 0 && HAS(s, WGPT_MIS_SKYBOX)) {
-          float sky_pdf = get_sky_pdf(s, a.p, dir, cn);
+          float sky_pdf = get_sky_pdf(s, sp, dir, cn);
           weight = mis_weight(tp4.w, sky_pdf);
         }
         radiance = radiance + throughput * clamp_firefly(sky_color * weight, bounce);
@@ -260,7 +345,7 @@ __global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a, int bounce, con
         radiance = radiance + throughput * clamp_firefly(mk3(0.02f, 0.03f, 0.05f), bounce);
       }
       a.b.rad[slot] = make_float4(radiance.x, radiance.y, radiance.z, rd4.w);
-      a.b.meta[slot] = make_uint4(meta.x, 0u, (uint32_t)bounce, meta.w);
+      a.b.meta[slot] = make_uint4(meta.x, 0u, meta.z, meta.w);
     }
   }
   flush_wf<COUNT>(cn, a.counters, true);
@@ -302,13 +387,14 @@ __device__ void record_nee(const WfArgs& a, uint32_t slot, int rec, const LightS
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const uint32_t* __restrict__ q,
-                                                  const uint32_t* count_ptr, uint32_t* __restrict__ q_next,
-                                                  uint32_t* count_next, uint32_t* sh_count) {
+__global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   const DScene& s = a.s;
-  const DParams& p = a.p;
-  uint32_t n = *count_ptr;
+  const uint32_t iter = a.ctl->iter;
+  const uint32_t* __restrict__ q = a.b.hitq;
+  const uint32_t n = a.ctl->counts[iter & 3u][K_HIT];
+  uint32_t* sh_count = &a.ctl->counts[iter & 3u][K_SHADOW];
+  const DParams& p = a.ctl->sp;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     bool alive = false, sh_light = false, sh_env = false;
@@ -317,6 +403,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const ui
       slot = q[i];
       float4 o4 = a.b.ray_o[slot], d4 = a.b.ray_d[slot], tp4 = a.b.tp[slot], rd4 = a.b.rad[slot];
       uint4 meta = a.b.meta[slot];
+      const int bounce = (int)meta.z;
       uint4 h0 = a.b.hit[slot * 2], h1 = a.b.hit[slot * 2 + 1];
       HitRec hit;
       hit.t = __uint_as_float(h0.x); hit.m_idx = (int32_t)h0.y; hit.o_idx = (int32_t)h0.z; hit.kind = (int32_t)h0.w;
@@ -544,7 +631,6 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const ui
       a.b.rad[slot] = make_float4(radiance.x, radiance.y, radiance.z, last_weight_sum);
       a.b.meta[slot] = make_uint4(rng, flags, (uint32_t)bounce, (uint32_t)stack.count);
     }
-    queue_push(q_next, count_next, slot, alive);
     queue_push(a.b.shq, sh_count, slot * 2u, sh_light);
     queue_push(a.b.shq, sh_count, slot * 2u + 1u, sh_env);
   }
@@ -553,10 +639,12 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a, int bounce, const ui
 
 // ---------------------------------------------------------------------------- shadow
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_wf_shadow(WfArgs a, const uint32_t* count_ptr, uint32_t* cursor) {
+__global__ void __launch_bounds__(256) k_wf_shadow(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   uint32_t err = 0;
-  const uint32_t n = *count_ptr;
+  const uint32_t iter = a.ctl->iter;
+  const uint32_t n = a.ctl->counts[iter & 3u][K_SHADOW];
+  uint32_t* cursor = &a.ctl->counts[iter & 3u][K_SH_CURSOR];
   ShadowTrav t;
   bool have = false, exhausted = false;
   uint32_t e = 0;
@@ -586,14 +674,25 @@ __global__ void __launch_bounds__(256) k_wf_shadow(WfArgs a, const uint32_t* cou
 }
 
 // ---------------------------------------------------------------------------- resolve
+// Adds the recorded next-event contributions (shader.wgsl:2271 with the shadow result), queues
+// continuing paths for the next iteration, stores the radiance of finished paths under their
+// unit and starts the next units in the freed slots (handed out in queue order within a warp).
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a, const uint32_t* __restrict__ q, const uint32_t* count_ptr) {
+__global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a) {
   Counters<COUNT> cn; cn.init();
-  uint32_t n = *count_ptr;
+  const uint32_t iter = a.ctl->iter;
+  const QIn q = queue_in(a, iter);
+  const uint32_t n = q.n;
+  const uint32_t r1 = (iter + 1u) & 3u, p1 = (iter + 1u) & 1u;
+  uint32_t* cont_count = &a.ctl->counts[r1][K_CONT];
+  uint32_t* new_count = &a.ctl->counts[r1][K_NEW];
+  const uint32_t n_units = a.ctl->n_units, n_views = a.ctl->n_views;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
+    bool alive = false, ended = false;
+    uint32_t slot = 0;
     if (i < n) {
-      uint32_t slot = q[i];
+      slot = q.at(i);
       uint4 meta = a.b.meta[slot];
       uint32_t flags = meta.y;
       int bounce = (int)meta.z;
@@ -610,25 +709,91 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a, const uint32_t* __
           if ((flags & needs) && a.b.vis[slot * 2 + rec] == 0u) incoming = mk3s(0.0f);
           radiance = radiance + mk3(t4.x, t4.y, t4.z) * clamp_firefly(incoming, bounce);
         }
-        a.b.rad[slot] = make_float4(radiance.x, radiance.y, radiance.z, rd4.w);
       }
-      if (!(flags & F_ALIVE)) {
-        uint32_t ix, iy;
-        px_of(a, slot, ix, iy);
-        size_t idx = (size_t)iy * a.p.width + ix;
-        float4 acc4 = a.accum[idx];
-        float weight = 1.0f / (float)(a.sample_number + 1u);
-        v3 acc = vmix(mk3(acc4.x, acc4.y, acc4.z), radiance, weight);
-        a.accum[idx] = make_float4(acc.x, acc.y, acc.z, 1.0f);
-        v3 c = acc * mk3s(a.p.exposure);
-        c = c / (c + mk3s(0.3f));
-        c = vpow(c, 0.4545f);
-        a.out[(size_t)iy * a.out_pitch + ix] =
-            make_uchar4((unsigned char)unorm8(c.x), (unsigned char)unorm8(c.y), (unsigned char)unorm8(c.z), 255);
+      if (flags & F_ALIVE) {
+        alive = true;
+        if (flags & (F_NEE_LIGHT | F_NEE_ENV)) a.b.rad[slot] = make_float4(radiance.x, radiance.y, radiance.z, rd4.w);
+        a.b.meta[slot] = make_uint4(meta.x, 0u, meta.z + 1u, meta.w);
+      } else {
+        a.samples[a.b.unit[slot]] = make_float4(radiance.x, radiance.y, radiance.z, 0.0f);
+        ended = true;
       }
     }
+    queue_push(a.b.qcont[p1], cont_count, slot, alive);
+    unsigned em = __ballot_sync(0xffffffffu, ended);
+    bool started = false;
+    if (em) {
+      int lane = threadIdx.x & 31;
+      int leader = __ffs(em) - 1;
+      uint32_t ubase = 0;
+      if (lane == leader) ubase = atomicAdd(&a.ctl->unit_next, (uint32_t)__popc(em));
+      ubase = __shfl_sync(0xffffffffu, ubase, leader);
+      if (ended) {
+        uint32_t u = ubase + (uint32_t)__popc(em & ((1u << lane) - 1u));
+        if (u < n_units) {
+          spawn<COUNT>(a, n_views, slot, u, cn);
+          started = true;
+        }
+      }
+    }
+    queue_push(a.b.qnew[p1], new_count, slot, started);
   }
   flush_wf<COUNT>(cn, a.counters, true);
+}
+
+// ---------------------------------------------------------------------------- control
+// Ends an iteration: clears the counter set the next iteration writes into, advances the
+// iteration and continues the loop while paths are queued (and the iteration bound is not hit).
+template <bool GRAPH>
+__global__ void k_wf_control(WfArgs a, cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  WfCtl* c = a.ctl;
+  const uint32_t iter = c->iter;
+  const uint32_t r1 = (iter + 1u) & 3u, r2 = (iter + 2u) & 3u;
+  for (int k = 0; k < K_NKINDS; ++k) c->counts[r2][k] = 0u;
+  uint32_t next = c->counts[r1][K_CONT] + c->counts[r1][K_NEW];
+  uint32_t go = next > 0u ? 1u : 0u;
+  if (go && iter + 1u >= c->max_iter) {
+    go = 0u;
+    atomicOr(a.status, ERR_ITER);
+  }
+  c->iter = iter + 1u;
+  c->cond = go;
+  if (GRAPH) cudaGraphSetConditional(h, go);
+}
+
+// ---------------------------------------------------------------------------- accumulate
+// Folds each pixel's samples into the running mean in sample order (shader.wgsl:2482-2491 once
+// per sample: accum = mix(accum, L, 1/(sample_number+1)), alpha 1) and writes the rgba8 image of
+// the last sample.
+__global__ void __launch_bounds__(256) k_wf_accumulate(WfArgs a) {
+  const uint32_t n = a.ctl->n_pixels, n_views = a.ctl->n_views;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = n_views;
+    while (hi - lo > 1u) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (a.views[mid].pix_base <= g) lo = mid; else hi = mid;
+    }
+    const WfView* v = a.views + lo;
+    uint32_t pix = g - v->pix_base;
+    uint32_t ix = v->p.sec_x + pix % v->sec_w;
+    uint32_t iy = v->p.sec_y + pix / v->sec_w;
+    size_t idx = (size_t)iy * v->p.width + ix;
+    float4 acc4 = v->accum[idx];
+    v3 acc = mk3(acc4.x, acc4.y, acc4.z);
+    const float4* smp = a.samples + v->unit_base + pix;
+    for (uint32_t k = 0; k < v->spp; ++k) {
+      float4 L = smp[(size_t)k * v->npix];
+      float weight = 1.0f / (float)(v->first_frame + k + 1u);
+      acc = vmix(acc, mk3(L.x, L.y, L.z), weight);
+    }
+    v->accum[idx] = make_float4(acc.x, acc.y, acc.z, 1.0f);
+    v3 c = acc * mk3s(v->p.exposure);
+    c = c / (c + mk3s(0.3f));
+    c = vpow(c, 0.4545f);
+    v->out[(size_t)iy * v->out_pitch + ix] =
+        make_uchar4((unsigned char)unorm8(c.x), (unsigned char)unorm8(c.y), (unsigned char)unorm8(c.z), 255);
+  }
 }
 
 }  // namespace pt
@@ -637,8 +802,7 @@ namespace wgpt {
 
 using namespace pt;
 
-static DScene to_dscene_wf(const DeviceScene& d) {
-  DScene s;
+static void fill_dscene(DScene& s, const DeviceScene& d) {
   s.mats = (const float4*)d.mats; s.n_mats = d.n_mats;
   s.objs = (const float4*)d.objs; s.n_objs = d.n_objs;
   s.tlas = (const float4*)d.tlas; s.n_tlas = d.n_tlas;
@@ -650,11 +814,9 @@ static DScene to_dscene_wf(const DeviceScene& d) {
   s.sky = (const uint2*)d.sky; s.sky_w = d.sky_w; s.sky_h = d.sky_h;
   s.cdf = (const float*)d.cdf; s.n_cdf = d.n_cdf;
   s.bounce_limit = d.bounce_limit; s.flags = d.flags;
-  return s;
 }
 
-static DParams to_dparams_wf(const wgpt_scene_params& q, uint32_t sec_x, uint32_t sec_y) {
-  DParams p;
+static void fill_dparams(DParams& p, const wgpt_scene_params& q, uint32_t sec_x, uint32_t sec_y) {
   p.eye = mk3(q.eye[0], q.eye[1], q.eye[2]); p.sample_number = q.sample_number;
   p.ray00 = mk3(q.ray00[0], q.ray00[1], q.ray00[2]); p.width = q.width;
   p.ray10 = mk3(q.ray10[0], q.ray10[1], q.ray10[2]); p.height = q.height;
@@ -663,17 +825,26 @@ static DParams to_dparams_wf(const wgpt_scene_params& q, uint32_t sec_x, uint32_
   p.sky_width = q.sky_width; p.sky_height = q.sky_height;
   p.sky_total_lum = q.sky_total_lum; p.total_light_power = q.total_light_power;
   p.sec_x = sec_x; p.sec_y = sec_y; p.sky_cdf_index = q.sky_cdf_index;
-  return p;
 }
 
-size_t wavefront_bytes_per_path() {
-  // ray 32 + tp 16 + rad 16 + meta 16 + media 128 + hit 32 + nee 64 + shadow 64 + vis 2 +
-  // 2 path queues 8 + shadow queue 8 + hit and miss queues 8
-  return 32 + 16 + 16 + 16 + 128 + 32 + 64 + 64 + 2 + 8 + 8 + 8;
+// Path-slot state: ray 32 + tp 16 + rad 16 + meta 16 + unit 4 + media 128 + hit 32 + nee 64 +
+// shadow 64 + vis 2 + continuing and new queues 16 + hit queue 4 + shadow queue 8.
+static constexpr int kParts = 16;
+static void part_sizes(size_t n, size_t out[kParts]) {
+  size_t v[kParts] = {n * 16, n * 16, n * 16, n * 16, n * 16, n * 4, n * 128, n * 32,
+                      n * 64, n * 64, n * 2, n * 4, n * 4, n * 4, n * 4, n * 4};
+  for (int i = 0; i < kParts; ++i) out[i] = v[i];
+}
+// plus the shadow queue (n * 8), carved last
+size_t wavefront_bytes_per_path() { return 32 + 16 + 16 + 16 + 4 + 128 + 32 + 64 + 64 + 2 + 16 + 4 + 8; }
+
+static size_t pool_bytes(uint32_t capacity) {
+  size_t parts[kParts], s = 0;
+  part_sizes(capacity, parts);
+  for (size_t x : parts) s += (x + 255) & ~(size_t)255;
+  return s + (((size_t)capacity * 8 + 255) & ~(size_t)255);
 }
 
-// Carves the path-state arrays out of one scratch allocation of wavefront_bytes_per_path() *
-// capacity + 256 * 16 bytes (256-byte aligned base).
 static WfBuffers carve(void* scratch, uint32_t capacity) {
   char* p = (char*)scratch;
   auto take = [&](size_t bytes) { char* r = p; p += (bytes + 255) & ~(size_t)255; return (void*)r; };
@@ -684,119 +855,319 @@ static WfBuffers carve(void* scratch, uint32_t capacity) {
   b.tp = (float4*)take(n * 16);
   b.rad = (float4*)take(n * 16);
   b.meta = (uint4*)take(n * 16);
+  b.unit = (uint32_t*)take(n * 4);
   b.med = (float4*)take(n * 128);
   b.hit = (uint4*)take(n * 32);
   b.nee = (float4*)take(n * 64);
   b.shadow = (float4*)take(n * 64);
   b.vis = (uint8_t*)take(n * 2);
-  b.queue[0] = (uint32_t*)take(n * 4);
-  b.queue[1] = (uint32_t*)take(n * 4);
-  b.shq = (uint32_t*)take(n * 8);
+  b.qcont[0] = (uint32_t*)take(n * 4);
+  b.qcont[1] = (uint32_t*)take(n * 4);
+  b.qnew[0] = (uint32_t*)take(n * 4);
+  b.qnew[1] = (uint32_t*)take(n * 4);
   b.hitq = (uint32_t*)take(n * 4);
-  b.missq = (uint32_t*)take(n * 4);
-  b.counts = (uint32_t*)take(CNT_KINDS * 256 * 4);
+  b.shq = (uint32_t*)take(n * 8);
   return b;
 }
 
-size_t wavefront_scratch_bytes(uint32_t capacity) {
-  size_t n = capacity, s = 0;
-  size_t parts[15] = {n * 16, n * 16, n * 16, n * 16, n * 16, n * 128, n * 32, n * 64, n * 64, n * 2, n * 4, n * 4,
-                      n * 8, n * 4, n * 4};
-  for (size_t x : parts) s += (x + 255) & ~(size_t)255;
-  return s + CNT_KINDS * 256 * 4;
+struct WfEngine {
+  uint32_t pool_paths = 1u << 21;          // path slots of the pool (upper bound)
+  uint64_t units_per_pass = 1ull << 27;    // samples held before they are folded into the images
+  void* pool = nullptr;
+  uint32_t pool_cap = 0;
+  float4* samples = nullptr;
+  uint64_t samples_cap = 0;
+  WfView* d_views = nullptr;
+  uint32_t views_cap = 0;
+  WfCtl* d_ctl = nullptr;
+  uint32_t* h_cond = nullptr;              // pinned copy of the loop condition (host-driven loop)
+  int grids[2][8] = {{0}, {0}};              // launch grid per stage (counting / plain variants)
+  int* grid = grids[0];
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  WfArgs key;
+  bool key_count = false;
+  bool has_graph = false;
+};
+
+WfEngine* wf_engine_create() { return new WfEngine(); }
+
+static void drop_graph(WfEngine* e) {
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  e->exec = nullptr;
+  e->graph = nullptr;
+  e->has_graph = false;
 }
 
-static int g_grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // persistent grid size per stage (computed once)
+void wf_engine_destroy(WfEngine* e) {
+  if (!e) return;
+  drop_graph(e);
+  if (e->pool) cudaFree(e->pool);
+  if (e->samples) cudaFree(e->samples);
+  if (e->d_views) cudaFree(e->d_views);
+  if (e->d_ctl) cudaFree(e->d_ctl);
+  if (e->h_cond) cudaFreeHost(e->h_cond);
+  delete e;
+}
+
+int wf_engine_configure(WfEngine* e, uint32_t pool_paths, uint64_t units_per_pass) {
+  if (pool_paths < 1024u || pool_paths > (1u << 26)) return 1;
+  if (units_per_pass < (1ull << 16) || units_per_pass > (1ull << 30)) return 1;
+  e->pool_paths = pool_paths;
+  e->units_per_pass = units_per_pass;
+  return 0;
+}
+
+void wf_engine_get(const WfEngine* e, uint32_t* pool_paths, uint64_t* units_per_pass) {
+  *pool_paths = e->pool_paths;
+  *units_per_pass = e->units_per_pass;
+}
 
 template <typename K>
-static int grid_for(K kernel, int stage) {
-  if (g_grid[stage] == 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
-    g_grid[stage] = sms * (per_sm > 0 ? per_sm : 1);
-  }
-  return g_grid[stage];
+static int occupancy_grid(K kernel) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+  return sms * (per_sm > 0 ? per_sm : 1);
 }
 
 template <bool COUNT>
-static cudaError_t render_wf(const WfArgs& a0, uint32_t first_frame, uint32_t reps, uint32_t n, cudaStream_t st,
-                            StageTimer* timer) {
-  WfArgs a = a0;
-  unsigned long long* cbase = a0.counters;
-  auto stage_args = [&](int stage) {
-    WfArgs x = a;
-    x.counters = cbase ? cbase + 16 * stage : nullptr;
-    return x;
+static void compute_grids(WfEngine* e) {
+  e->grid = e->grids[COUNT ? 1 : 0];
+  if (e->grid[0]) return;
+  e->grid[0] = occupancy_grid(k_wf_fill<COUNT>);
+  e->grid[1] = occupancy_grid(k_wf_extend<COUNT>);
+  e->grid[2] = occupancy_grid(k_wf_shade<COUNT>);
+  e->grid[3] = occupancy_grid(k_wf_shadow<COUNT>);
+  e->grid[4] = occupancy_grid(k_wf_resolve<COUNT>);
+  e->grid[5] = occupancy_grid(k_wf_shade_miss<COUNT>);
+  e->grid[6] = occupancy_grid(k_wf_accumulate);
+  e->grid[7] = 1;
+}
+
+static WfArgs stage_args(const WfArgs& a, int stage) {
+  WfArgs x = a;
+  x.counters = a.counters ? a.counters + 16 * stage : nullptr;
+  return x;
+}
+
+// The whole pass as one graph: fill -> WHILE(extend, shade_miss, shade, shadow, resolve,
+// control) -> accumulate.  Arguments live in device memory (views, control block), so the graph
+// only changes when buffers move.
+template <bool COUNT>
+static cudaError_t build_graph(WfEngine* e, const WfArgs& a) {
+  drop_graph(e);
+  cudaError_t err;
+  cudaGraph_t g = nullptr;
+  if ((err = cudaGraphCreate(&g, 0)) != cudaSuccess) return err;
+  e->graph = g;
+  cudaGraphConditionalHandle h;
+  if ((err = cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault)) != cudaSuccess) return err;
+  WfArgs sa[8];
+  for (int st = 0; st < 8; ++st) sa[st] = stage_args(a, st);
+  auto add_kernel = [&](cudaGraph_t gr, const void* fn, int grid, void** args, const cudaGraphNode_t* dep,
+                        cudaGraphNode_t* out) -> cudaError_t {
+    cudaKernelNodeParams kp;
+    memset(&kp, 0, sizeof kp);
+    kp.func = const_cast<void*>(fn);
+    kp.gridDim = dim3((unsigned)grid);
+    kp.blockDim = dim3(grid == 1 ? 32u : 256u);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = args;
+    return cudaGraphAddKernelNode(out, gr, dep, dep ? 1 : 0, &kp);
   };
-  int bl = a.s.bounce_limit;
-  if (bl > 255) return cudaErrorInvalidValue;
-  int g_ray = grid_for(k_wf_raygen<COUNT>, 0);
-  int g_ext = grid_for(k_wf_extend<COUNT>, 1);
-  int g_sh = grid_for(k_wf_shade<COUNT>, 2);
-  int g_shw = grid_for(k_wf_shadow<COUNT>, 3);
-  int g_res = grid_for(k_wf_resolve<COUNT>, 4);
-  int need = (int)((n + 255) / 256);
-  int g_miss = grid_for(k_wf_shade_miss<COUNT>, 5);
-  uint32_t* C = a.b.counts;
-  auto cnt = [&](int kind, int b) { return C + kind * 256 + b; };
-  for (uint32_t r = 0; r < reps; ++r) {
-    a.sample_number = first_frame + r;
-    cudaMemsetAsync(C, 0, CNT_KINDS * 256 * 4, st);
-    if (timer) timer->begin(0, st);
-    k_wf_raygen<COUNT><<<std::min(g_ray, need), 256, 0, st>>>(stage_args(0));
-    if (timer) timer->end(0, st);
-    for (int b = 0; b < bl; ++b) {
-      uint32_t* qin = a.b.queue[b & 1];
-      uint32_t* qout = a.b.queue[(b + 1) & 1];
-      if (timer) timer->begin(1, st);
-      k_wf_extend<COUNT><<<std::min(g_ext, need), 256, 0, st>>>(stage_args(1), qin, cnt(CNT_LIVE, b),
-                                                                cnt(CNT_EXT_CURSOR, b));
-      if (timer) timer->end(1, st);
-      if (timer) timer->begin(5, st);
-      k_wf_shade_miss<COUNT><<<std::min(g_miss, need), 256, 0, st>>>(stage_args(5), b, qin, cnt(CNT_LIVE, b),
-                                                                     cnt(CNT_HIT, b));
-      if (timer) timer->end(5, st);
-      if (timer) timer->begin(2, st);
-      k_wf_shade<COUNT><<<std::min(g_sh, need), 256, 0, st>>>(stage_args(2), b, a.b.hitq, cnt(CNT_HIT, b), qout,
-                                                               cnt(CNT_LIVE, b + 1), cnt(CNT_SHADOW, b));
-      if (timer) timer->end(2, st);
-      if (timer) timer->begin(3, st);
-      k_wf_shadow<COUNT><<<std::min(g_shw, 2 * need), 256, 0, st>>>(stage_args(3), cnt(CNT_SHADOW, b),
-                                                                   cnt(CNT_SH_CURSOR, b));
-      if (timer) timer->end(3, st);
-      if (timer) timer->begin(4, st);
-      k_wf_resolve<COUNT><<<std::min(g_res, need), 256, 0, st>>>(stage_args(4), qin, cnt(CNT_LIVE, b));
-      if (timer) timer->end(4, st);
-    }
+  cudaGraphNode_t n_fill, n_loop, n_acc;
+  void* a_fill[] = {&sa[0]};
+  if ((err = add_kernel(g, (const void*)k_wf_fill<COUNT>, e->grid[0], a_fill, nullptr, &n_fill)) != cudaSuccess)
+    return err;
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};   // the rest zero, as the API requires
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  if ((err = cudaGraphAddNode(&n_loop, g, &n_fill, 1, &cp)) != cudaSuccess) return err;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaGraphNode_t prev, cur;
+  void* a1[] = {&sa[1]};
+  void* a5[] = {&sa[5]};
+  void* a2[] = {&sa[2]};
+  void* a3[] = {&sa[3]};
+  void* a4[] = {&sa[4]};
+  void* a7[] = {&sa[7], &h};
+  if ((err = add_kernel(body, (const void*)k_wf_extend<COUNT>, e->grid[1], a1, nullptr, &prev)) != cudaSuccess) return err;
+  if ((err = add_kernel(body, (const void*)k_wf_shade_miss<COUNT>, e->grid[5], a5, &prev, &cur)) != cudaSuccess) return err;
+  prev = cur;
+  if ((err = add_kernel(body, (const void*)k_wf_shade<COUNT>, e->grid[2], a2, &prev, &cur)) != cudaSuccess) return err;
+  prev = cur;
+  if ((err = add_kernel(body, (const void*)k_wf_shadow<COUNT>, e->grid[3], a3, &prev, &cur)) != cudaSuccess) return err;
+  prev = cur;
+  if ((err = add_kernel(body, (const void*)k_wf_resolve<COUNT>, e->grid[4], a4, &prev, &cur)) != cudaSuccess) return err;
+  prev = cur;
+  if ((err = add_kernel(body, (const void*)k_wf_control<true>, 1, a7, &prev, &cur)) != cudaSuccess) return err;
+  void* a6[] = {&sa[6]};
+  if ((err = add_kernel(g, (const void*)k_wf_accumulate, e->grid[6], a6, &n_loop, &n_acc)) != cudaSuccess) return err;
+  if ((err = cudaGraphInstantiate(&e->exec, g, 0)) != cudaSuccess) return err;
+  e->key = a;
+  e->key_count = COUNT;
+  e->has_graph = true;
+  return cudaSuccess;
+}
+
+// The same pass launched from the host, one event pair per stage launch (stage timing).
+template <bool COUNT>
+static cudaError_t run_pass_host(WfEngine* e, const WfArgs& a, uint32_t max_iter, cudaStream_t st,
+                                 StageTimer* timer) {
+  auto T0 = [&](int k) { if (timer) timer->begin(k, st); };
+  auto T1 = [&](int k) { if (timer) timer->end(k, st); };
+  T0(0); k_wf_fill<COUNT><<<e->grid[0], 256, 0, st>>>(stage_args(a, 0)); T1(0);
+  for (uint32_t it = 0; it <= max_iter; ++it) {
+    T0(1); k_wf_extend<COUNT><<<e->grid[1], 256, 0, st>>>(stage_args(a, 1)); T1(1);
+    T0(5); k_wf_shade_miss<COUNT><<<e->grid[5], 256, 0, st>>>(stage_args(a, 5)); T1(5);
+    T0(2); k_wf_shade<COUNT><<<e->grid[2], 256, 0, st>>>(stage_args(a, 2)); T1(2);
+    T0(3); k_wf_shadow<COUNT><<<e->grid[3], 256, 0, st>>>(stage_args(a, 3)); T1(3);
+    T0(4); k_wf_resolve<COUNT><<<e->grid[4], 256, 0, st>>>(stage_args(a, 4)); T1(4);
+    T0(7); k_wf_control<false><<<1, 32, 0, st>>>(stage_args(a, 7), cudaGraphConditionalHandle{}); T1(7);
+    cudaError_t err = cudaMemcpyAsync(e->h_cond, &a.ctl->cond, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    if (err != cudaSuccess) return err;
+    if (*e->h_cond == 0u) break;
   }
+  T0(6); k_wf_accumulate<<<e->grid[6], 256, 0, st>>>(stage_args(a, 6)); T1(6);
   return cudaGetLastError();
 }
 
-cudaError_t launch_render_wavefront(const DeviceScene& d, const wgpt_scene_params& q, uint32_t first_frame,
-                                    uint32_t reps, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh, float* accum,
-                                    uint8_t* out, uint32_t out_pitch, void* scratch, uint32_t capacity,
-                                    uint32_t* status, unsigned long long* counters, cudaStream_t st,
-                                    StageTimer* timer, const void* pairs_tlas, const void* pairs_bvh) {
-  uint32_t n = sw * sh;
-  if (n == 0) return cudaSuccess;
-  if (n > capacity || !scratch) return cudaErrorInvalidValue;
-  WfArgs a;
-  a.s = to_dscene_wf(d);
-  a.P.tlas = (const float4*)pairs_tlas;
-  a.P.bvh = (const float4*)pairs_bvh;
-  a.p = to_dparams_wf(q, sx, sy);
-  a.b = carve(scratch, capacity);
-  a.sec_w = sw; a.sec_h = sh;
-  a.sample_number = first_frame;
-  a.accum = (float4*)accum;
-  a.out = (uchar4*)out;
-  a.out_pitch = out_pitch;
-  a.status = status;
-  a.counters = counters;
-  if (counters) return render_wf<true>(a, first_frame, reps, n, st, timer);
-  return render_wf<false>(a, first_frame, reps, n, st, timer);
+template <bool COUNT>
+static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* pairs_tlas, const void* pairs_bvh,
+                                const WfJobView* jv, uint32_t nv, uint32_t* status, unsigned long long* counters,
+                                cudaStream_t st, StageTimer* timer) {
+  cudaError_t err;
+  compute_grids<COUNT>(e);
+  uint64_t total_npix = 0;
+  for (uint32_t v = 0; v < nv; ++v) total_npix += (uint64_t)jv[v].sw * jv[v].sh;
+  if (total_npix == 0) return cudaSuccess;
+  if (total_npix > (1ull << 30)) return cudaErrorInvalidValue;
+  const int bl = d.bounce_limit;
+  if (!e->d_ctl) {
+    if ((err = cudaMalloc(&e->d_ctl, sizeof(WfCtl))) != cudaSuccess) return err;
+    if ((err = cudaMallocHost(&e->h_cond, sizeof(uint32_t))) != cudaSuccess) return err;
+  }
+  if (e->views_cap < nv) {
+    cudaStreamSynchronize(st);
+    if (e->d_views) cudaFree(e->d_views);
+    e->d_views = nullptr;
+    e->views_cap = 0;
+    if ((err = cudaMalloc(&e->d_views, sizeof(WfView) * nv)) != cudaSuccess) return err;
+    e->views_cap = nv;
+  }
+  std::vector<uint32_t> done(nv, 0u);
+  std::vector<WfView> hv;
+  hv.reserve(nv);
+  while (true) {
+    uint64_t per = std::max<uint64_t>(1, e->units_per_pass / total_npix);
+    hv.clear();
+    uint64_t units = 0, pixels = 0;
+    std::vector<uint32_t> take(nv, 0u);
+    for (uint32_t v = 0; v < nv; ++v) {
+      uint32_t rem = jv[v].spp - done[v];
+      uint32_t npix = jv[v].sw * jv[v].sh;
+      if (rem == 0 || npix == 0) continue;
+      take[v] = (uint32_t)std::min<uint64_t>(rem, per);
+      WfView w;
+      memset(&w, 0, sizeof w);
+      fill_dparams(w.p, jv[v].q, jv[v].sx, jv[v].sy);
+      w.sec_w = jv[v].sw;
+      w.npix = npix;
+      w.first_frame = jv[v].first_frame + done[v];
+      w.spp = take[v];
+      w.unit_base = (uint32_t)units;
+      w.pix_base = (uint32_t)pixels;
+      w.out_pitch = jv[v].out_pitch;
+      w.accum = (float4*)jv[v].accum;
+      w.out = (uchar4*)jv[v].out;
+      hv.push_back(w);
+      units += (uint64_t)npix * take[v];
+      pixels += npix;
+    }
+    if (hv.empty()) break;
+    if (units >= (1ull << 31)) return cudaErrorInvalidValue;
+    // buffers: the pool never exceeds the pass's units; samples hold the pass
+    uint32_t want_pool = (uint32_t)std::min<uint64_t>(e->pool_paths, units);
+    if (e->pool_cap < want_pool || e->samples_cap < units) {
+      cudaStreamSynchronize(st);
+      drop_graph(e);
+      if (e->pool_cap < want_pool) {
+        if (e->pool) cudaFree(e->pool);
+        e->pool = nullptr;
+        e->pool_cap = 0;
+        if ((err = cudaMalloc(&e->pool, pool_bytes(want_pool))) != cudaSuccess) return err;
+        e->pool_cap = want_pool;
+      }
+      if (e->samples_cap < units) {
+        if (e->samples) cudaFree(e->samples);
+        e->samples = nullptr;
+        e->samples_cap = 0;
+        if ((err = cudaMalloc(&e->samples, units * sizeof(float4))) != cudaSuccess) return err;
+        e->samples_cap = units;
+      }
+    }
+    uint32_t fill = want_pool;   // active slots of the pass (the allocation may be larger)
+    WfCtl c;
+    memset(&c, 0, sizeof c);
+    c.iter = 0;
+    c.unit_next = fill;
+    c.n_units = (uint32_t)units;
+    uint64_t bound = (units * (uint64_t)std::max(bl, 0) + fill - 1) / fill + (uint64_t)std::max(bl, 0) + 4;
+    c.max_iter = (uint32_t)std::min<uint64_t>(bound, 1u << 22);
+    c.n_views = (uint32_t)hv.size();
+    c.n_pixels = (uint32_t)pixels;
+    c.fill_count = fill;
+    c.counts[0][K_NEW] = fill;
+    c.sp = hv[0].p;
+    if ((err = cudaMemcpyAsync(e->d_views, hv.data(), sizeof(WfView) * hv.size(), cudaMemcpyHostToDevice, st)) !=
+        cudaSuccess)
+      return err;
+    if ((err = cudaMemcpyAsync(e->d_ctl, &c, sizeof c, cudaMemcpyHostToDevice, st)) != cudaSuccess) return err;
+    WfArgs a;
+    memset(&a, 0, sizeof a);
+    fill_dscene(a.s, d);
+    a.P.tlas = (const float4*)pairs_tlas;
+    a.P.bvh = (const float4*)pairs_bvh;
+    a.b = carve(e->pool, e->pool_cap);
+    a.views = e->d_views;
+    a.ctl = e->d_ctl;
+    a.samples = e->samples;
+    a.status = status;
+    a.counters = counters;
+    if (bl <= 0) {
+      // no bounce runs: every sample's radiance is zero
+      if ((err = cudaMemsetAsync(e->samples, 0, units * sizeof(float4), st)) != cudaSuccess) return err;
+      if (timer) timer->begin(6, st);
+      k_wf_accumulate<<<e->grid[6], 256, 0, st>>>(stage_args(a, 6));
+      if (timer) timer->end(6, st);
+      if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    } else if (timer) {
+      if ((err = run_pass_host<COUNT>(e, a, c.max_iter, st, timer)) != cudaSuccess) return err;
+    } else {
+      if (!e->has_graph || e->key_count != COUNT || memcmp(&e->key, &a, sizeof a) != 0) {
+        if ((err = build_graph<COUNT>(e, a)) != cudaSuccess) {
+          drop_graph(e);
+          return err;
+        }
+      }
+      if ((err = cudaGraphLaunch(e->exec, st)) != cudaSuccess) return err;
+    }
+    for (uint32_t v = 0; v < nv; ++v) done[v] += take[v];
+  }
+  return cudaSuccess;
+}
+
+cudaError_t wf_render(WfEngine* e, const DeviceScene& d, const void* pairs_tlas, const void* pairs_bvh,
+                      const WfJobView* views, uint32_t n_views, uint32_t* status, unsigned long long* counters,
+                      cudaStream_t st, StageTimer* timer) {
+  if (!e || n_views == 0) return cudaErrorInvalidValue;
+  if (counters) return render_views<true>(e, d, pairs_tlas, pairs_bvh, views, n_views, status, counters, st, timer);
+  return render_views<false>(e, d, pairs_tlas, pairs_bvh, views, n_views, status, counters, st, timer);
 }
 
 }  // namespace wgpt

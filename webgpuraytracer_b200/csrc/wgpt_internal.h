@@ -25,8 +25,9 @@ struct DeviceScene {
 cudaError_t launch_render(const DeviceScene& d, const wgpt_scene_params& q, uint32_t first_frame, uint32_t reps,
                           uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh, float* accum, uint8_t* out,
                           uint32_t out_pitch, uint32_t* status, unsigned long long* counters, cudaStream_t st);
-// CUDA-event timing of the renderer's stages (0 ray generation / single kernel, 1 closest hit,
-// 2 shading, 3 shadow rays, 4 accumulation) on the launching stream.
+// CUDA-event timing of the renderer's stages on the launching stream: 0 path start (single
+// kernel in megakernel mode), 1 closest hit, 2 surface shading, 3 shadow rays, 4 resolve and
+// regeneration, 5 miss shading, 6 accumulation, 7 loop control.
 struct StageTimer {
   static constexpr int kMaxEvents = 8192;
   cudaEvent_t ev[kMaxEvents];
@@ -48,12 +49,25 @@ struct StageTimer {
   }
 };
 
-size_t wavefront_scratch_bytes(uint32_t capacity);
-cudaError_t launch_render_wavefront(const DeviceScene& d, const wgpt_scene_params& q, uint32_t first_frame,
-                                    uint32_t reps, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh, float* accum,
-                                    uint8_t* out, uint32_t out_pitch, void* scratch, uint32_t capacity,
-                                    uint32_t* status, unsigned long long* counters, cudaStream_t st,
-                                    StageTimer* timer, const void* pairs_tlas, const void* pairs_bvh);
+// Wavefront renderer with path regeneration (wavefront.cu).  A job is a list of camera views,
+// each with its section, first sample number, sample count and images.
+struct WfJobView {
+  wgpt_scene_params q;
+  uint32_t sx, sy, sw, sh;
+  uint32_t first_frame, spp;
+  float* accum;          // float4 per pixel, row pitch q.width
+  uint8_t* out;          // rgba8, row pitch out_pitch
+  uint32_t out_pitch;
+};
+struct WfEngine;
+WfEngine* wf_engine_create();
+void wf_engine_destroy(WfEngine* e);
+int wf_engine_configure(WfEngine* e, uint32_t pool_paths, uint64_t units_per_pass);
+void wf_engine_get(const WfEngine* e, uint32_t* pool_paths, uint64_t* units_per_pass);
+size_t wavefront_bytes_per_path();
+cudaError_t wf_render(WfEngine* e, const DeviceScene& d, const void* pairs_tlas, const void* pairs_bvh,
+                      const WfJobView* views, uint32_t n_views, uint32_t* status, unsigned long long* counters,
+                      cudaStream_t st, StageTimer* timer);
 cudaError_t launch_gbuffer(const DeviceScene& d, const wgpt_scene_params& q, uint32_t sx, uint32_t sy, uint32_t sw,
                            uint32_t sh, float* gbuf, uint8_t* out, uint32_t out_pitch, uint32_t* status,
                            cudaStream_t st);

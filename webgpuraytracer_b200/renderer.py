@@ -198,6 +198,21 @@ class Renderer:
                     "trace_rays")
         return o, m, p, t, nn
 
+    def set_render_mode(self, mode: int):
+        """MODE_WAVEFRONT (path pool with regeneration) or MODE_MEGAKERNEL (one thread per pixel)."""
+        self._check(self.L.wgpt_set_render_mode(self.ctx, int(mode)), "set_render_mode")
+
+    def set_wavefront_config(self, pool_paths: int = 0, units_per_pass: int = 0):
+        """Path-slot pool size and samples per pass of the wavefront renderer (0 keeps a value)."""
+        self._check(self.L.wgpt_set_wavefront_config(self.ctx, int(pool_paths), int(units_per_pass)),
+                    "set_wavefront_config")
+
+    def wavefront_config(self) -> tuple[int, int]:
+        pool, units = C.c_uint32(0), C.c_uint64(0)
+        self._check(self.L.wgpt_get_wavefront_config(self.ctx, C.byref(pool), C.byref(units)),
+                    "get_wavefront_config")
+        return int(pool.value), int(units.value)
+
     def set_counting(self, on: bool):
         self._check(self.L.wgpt_set_counting(self.ctx, 1 if on else 0), "set_counting")
 

@@ -218,6 +218,43 @@ def run_reference(args):
     return 0
 
 
+def stage_report(r, rd, launch_once, stream, flush, paths_per_step: int, mega: bool) -> dict:
+    """Per-stage launch times of one step (event pair around every stage launch; the iteration
+    loop is then driven from the host instead of the graph: same kernels, same stream) and the
+    work counters of one step (a separate counting pass), both outside the timed region."""
+    import torch
+    r._check(r.L.wgpt_set_stage_timing(r.ctx, 1), "stage timing")
+    with torch.cuda.stream(stream):
+        flush.fill_(0.5)
+    launch_once()
+    r.synchronize()
+    stage_ms = np.zeros(8, np.float64)
+    stage_launches = np.zeros(8, np.uint32)
+    r._check(r.L.wgpt_read_stage_times(r.ctx, rd.ptr(stage_ms), rd.ptr(stage_launches)), "stage times")
+    r._check(r.L.wgpt_set_stage_timing(r.ctx, 0), "stage timing")
+    r.set_counting(True)
+    launch_once()
+    cnt = r.read_counters()
+    stage_cnt = np.zeros(128, np.uint64)
+    r._check(r.L.wgpt_read_stage_counters(r.ctx, rd.ptr(stage_cnt)), "stage counters")
+    r.set_counting(False)
+    sbytes = stage_bytes(stage_cnt.reshape(8, 16), paths_per_step, mega)
+    dom = int(np.argmax(stage_ms))
+    bytes_per_launch = sbytes[dom] / max(1, int(stage_launches[dom]))
+    avg_launch_s = stage_ms[dom] / 1e3 / max(1, int(stage_launches[dom]))
+    stages = {}
+    for st in range(8):
+        if stage_launches[st]:
+            t = stage_ms[st] / 1e3
+            stages[("k_render" if mega else KERNELS[st])] = {
+                "launches": int(stage_launches[st]), "ms_total": float(stage_ms[st]),
+                "share": float(stage_ms[st] / stage_ms.sum()), "algorithmic_GBps": sbytes[st] / t / 1e9 if t else None}
+    # the graph runs the same kernels the timing pass launched from the host (fill, 6 per
+    # iteration, accumulate)
+    return {"stages": stages, "achieved": bytes_per_launch / avg_launch_s / 1e9, "bytes_per_launch": bytes_per_launch,
+            "avg_launch_s": avg_launch_s, "dom": dom, "cnt": cnt, "launches": int(stage_launches.sum())}
+
+
 def run_ours(args):
     rank, world, local = dist_setup(args.gpus)
     import torch
@@ -230,6 +267,9 @@ def run_ours(args):
     r.set_scene(scene, packed=packed)
     mega = args.mode == "megakernel"
     r._check(r.L.wgpt_set_render_mode(r.ctx, 1 if mega else 0), "render mode")
+    if args.pool:
+        r.set_wavefront_config(args.pool, 0)
+    pool_paths = r.wavefront_config()[0]
     stream = torch.cuda.ExternalStream(r.stream_handle(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
     scene.camera.update_rays2()
@@ -282,43 +322,12 @@ def run_ours(args):
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e_value = paths_per_step * e2e_steps * world / e2e_s
 
-    # per-stage launch times: one step with an event pair around every stage launch (the
-    # iteration loop is then driven from the host instead of the graph; same kernels, stream)
-    r._check(r.L.wgpt_set_stage_timing(r.ctx, 1), "stage timing")
-    with torch.cuda.stream(stream):
-        flush.fill_(0.5)
-    launch(args.warmup)
-    r.synchronize()
-    stage_ms = np.zeros(8, np.float64)
-    stage_launches = np.zeros(8, np.uint32)
-    r._check(r.L.wgpt_read_stage_times(r.ctx, rd.ptr(stage_ms), rd.ptr(stage_launches)), "stage times")
-    r._check(r.L.wgpt_set_stage_timing(r.ctx, 0), "stage timing")
-
-    # work counters of one step (a separate counting pass, outside the timed region)
-    r.set_counting(True)
-    launch(args.warmup)
-    cnt = r.read_counters()
-    stage_cnt = np.zeros(128, np.uint64)
-    r._check(r.L.wgpt_read_stage_counters(r.ctx, rd.ptr(stage_cnt)), "stage counters")
-    stage_cnt = stage_cnt.reshape(8, 16)
-    r.set_counting(False)
-    sbytes = stage_bytes(stage_cnt, paths_per_step, mega)
-    dom = int(np.argmax(stage_ms))
-    bytes_per_launch = sbytes[dom] / max(1, int(stage_launches[dom]))
-    avg_launch_s = stage_ms[dom] / 1e3 / max(1, int(stage_launches[dom]))
+    rep = stage_report(r, rd, lambda: launch(args.warmup), stream, flush, paths_per_step, mega)
+    stages, achieved, bytes_per_launch, avg_launch_s, dom, cnt, launches = (
+        rep["stages"], rep["achieved"], rep["bytes_per_launch"], rep["avg_launch_s"], rep["dom"], rep["cnt"],
+        rep["launches"])
     peaks, peak_kind = load_peaks()
-    achieved = bytes_per_launch / avg_launch_s / 1e9
     rays = int(cnt[1] + cnt[2])
-    stages = {}
-    for st in range(8):
-        if stage_launches[st]:
-            t = stage_ms[st] / 1e3
-            stages[("k_render" if mega else KERNELS[st])] = {
-                "launches": int(stage_launches[st]), "ms_total": float(stage_ms[st]),
-                "share": float(stage_ms[st] / stage_ms.sum()), "algorithmic_GBps": sbytes[st] / t / 1e9 if t else None}
-    # launches per step of the timed region: the graph runs the same kernels the timing pass
-    # launched from the host (fill, 6 per iteration, accumulate)
-    launches = int(stage_launches.sum())
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -334,7 +343,8 @@ def run_ours(args):
                                    "2048x1024 RGBE env with importance sampling",
                        "step": f"one render call of {spp} samples per pixel ({paths_per_step:,} paths)",
                        "l2": "flushed between timed steps (256 MB write); path state and sample buffers exceed L2",
-                       "parallelism": f"replicas x{world}", "render_mode": args.mode},
+                       "parallelism": f"replicas x{world}", "render_mode": args.mode,
+                       "path_pool": pool_paths},
             "rays_per_s": rays * world * args.steps / dev_s_max,
             "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": 112,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 4},
@@ -363,6 +373,107 @@ def run_ours(args):
     return 0
 
 
+def run_batch(args):
+    """--workload batch: 32 seeded views (sizes over 256^2..1920x1080, 4/16/64 spp, 8 bounces)
+    of the 5.24 M-triangle scene in one render_views call per step; paths/s over all views and
+    the p50/p99 of the per-view completion times (device clock, from the start of the call's
+    work to the view's last sample)."""
+    rank, world, local = dist_setup(args.gpus)
+    import torch
+    from webgpuraytracer_b200 import renderer as rd
+    from webgpuraytracer_b200 import scene as sc
+    from webgpuraytracer_b200 import synth
+
+    torch.cuda.set_device(local)
+    scene = synth.batch_scene(1)
+    packed = sc.pack_scene_data(scene)
+    views = synth.batch_views(1, 32)
+    r = rd.Renderer(16, 16, device=local)
+    r.set_scene(scene, packed=packed)
+    r.set_wavefront_config(args.pool or 0, 1 << 30)
+    r.set_views([(v["width"], v["height"]) for v in views])
+    stream = torch.cuda.ExternalStream(r.stream_handle(), device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    spp = [v["spp"] for v in views]
+    paths_per_step = sum(v["width"] * v["height"] * v["spp"] for v in views)
+
+    def launch(step, timing=False):
+        ff = [step * 64] * len(views)
+        params = [synth.view_params(scene, packed, v, f, 1 + rank) for v, f in zip(views, ff)]
+        return r.render_views(params, ff, spp, timing=timing)
+
+    for i in range(args.warmup):
+        launch(i)
+    r.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(i))
+            starts[i].record(stream)
+        launch(args.warmup + i)
+        with torch.cuda.stream(stream):
+            ends[i].record(stream)
+    r.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    dev_s = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)) / 1e3
+    dev_s_max = max_over_ranks(dev_s, world)
+    value = paths_per_step * args.steps * world / dev_s_max
+    # per-view completion times (one more step, which waits for them)
+    done = launch(args.warmup + args.steps, timing=True)
+    # end-to-end: params in, every view's rgba8 image out, every step
+    outs = [np.empty((v["height"], v["width"], 4), np.uint8) for v in views]
+    e2e_steps = max(1, min(args.steps, 4))
+    barrier(world)
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        launch(args.warmup + args.steps + 1 + i)
+        for k, o in enumerate(outs):
+            r._check(r.L.wgpt_read_view(r.ctx, k, None, rd.ptr(o)), "read_view")
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    rep = stage_report(r, rd, lambda: launch(args.warmup), stream, flush, paths_per_step, False)
+    peaks, peak_kind = load_peaks()
+    cnt = rep["cnt"]
+    if rank == 0:
+        line = {
+            "metric": "paths/s, 32 batched views (uneven size and spp), 8 bounces", "value": value,
+            "unit": "paths/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_s_max / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene and view generator)",
+            "config": {"workload": "batched views: 32 views of 16 instances x 327,680-tri BLAS + 64 prims, "
+                                   "2048x1024 RGBE env; sizes {256^2, 512^2, 1280x720, 1920x1080}, spp {4,16,64}",
+                       "step": f"one render_views call ({paths_per_step:,} paths)",
+                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}",
+                       "path_pool": r.wavefront_config()[0]},
+            "view_done_ms": {"p50": float(np.percentile(done, 50)), "p99": float(np.percentile(done, 99)),
+                             "max": float(np.max(done))},
+            "rays_per_s": int(cnt[1] + cnt[2]) * world * args.steps / dev_s_max,
+            "e2e": {"value": paths_per_step * e2e_steps * world / e2e_s, "unit": "paths/s",
+                    "h2d_bytes_per_step": 112 * len(views),
+                    "d2h_bytes_per_step": sum(v["width"] * v["height"] * 4 for v in views)},
+            "gpu_launches": rep["launches"] * args.steps,
+            "stages": rep["stages"],
+            "roofline": {"bound": "hbm", "achieved": rep["achieved"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": rep["achieved"] / peaks["hbm_gbs"], "traffic": None,
+                         "kernel": KERNELS[rep["dom"]], "launch_ms": rep["avg_launch_s"] * 1e3,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    r.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -373,11 +484,16 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", choices=["wavefront", "megakernel"], default="wavefront")
+    ap.add_argument("--pool", type=int, default=0, help="wavefront path slots (0: library default)")
+    ap.add_argument("--workload", choices=["flagship", "batch"], default="flagship",
+                    help="flagship: 1080p 64 spp; batch: 32 uneven views of the 5.24 M-triangle scene")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
     return run_ours(args)
 
 

@@ -134,6 +134,20 @@ int wgpt_write_gbuffer(wgpt_ctx* ctx, const void* src_48B_per_px);
 int wgpt_read_denoised(wgpt_ctx* ctx, float* filtered_rgba32f, float* composited_rgba32f);
 int wgpt_read_canvas(wgpt_ctx* ctx, uint8_t* dst_rgba8, uint32_t dst_w, uint32_t dst_h);
 
+/* Batched views (no counterpart in the reference, which renders one canvas per device): many
+   camera views of the uploaded scene, each with its own size, samples and images owned by the
+   context, traced by one path pool in one graph launch.  wgpt_set_views allocates n view images
+   (zeroed accumulation); wgpt_render_views adds spp[i] samples (sample_number first_frame[i] ..)
+   to view i with the 112-byte params params_112n[i] (width/height = the view size; every view's
+   sky fields equal, as they describe the one scene) and, when done_ms is not NULL, waits and
+   stores per view the milliseconds from the start of the call's work to its last sample
+   (-1 for a view without samples); npix * spp must stay below 2^32 per view.  Results equal
+   wgpt_render of each view on its own. */
+int wgpt_set_views(wgpt_ctx* ctx, uint32_t n, const uint32_t* widths, const uint32_t* heights);
+int wgpt_render_views(wgpt_ctx* ctx, const void* params_112n, const uint32_t* first_frames, const uint32_t* spp,
+                      float* done_ms);
+int wgpt_read_view(wgpt_ctx* ctx, uint32_t view, float* accum_rgba32f, uint8_t* out_rgba8);
+
 /* Closest hit of caller rays (trace_scene, shader.wgsl:754-774) for parity tests: rays are n x
    (origin, direction) floats; outputs object index, material index, global triangle index
    (-1 unless a mesh triangle), t, world normal (3 floats). Host pointers. */

@@ -52,6 +52,9 @@ struct wgpt_ctx {
   wgpt::StageTimer* timer = nullptr;
   bool timing = false;
   wgpt::WfEngine* wf = nullptr;   // wavefront renderer: path pool, sample buffer, loop graph
+  // batched views: size and images of each
+  struct View { uint32_t w, h; float* accum; uint8_t* out; };
+  std::vector<View> views;
 };
 
 namespace {
@@ -355,8 +358,7 @@ int check_section(wgpt_ctx* ctx, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t
   return WGPT_OK;
 }
 
-int check_env(wgpt_ctx* ctx) {
-  const wgpt_scene_params& p = ctx->params;
+int check_env(wgpt_ctx* ctx, const wgpt_scene_params& p) {
   if ((ctx->ds.flags & WGPT_HAS_SKYBOX) && (ctx->ds.flags & WGPT_MIS_SKYBOX)) {
     if (p.sky_width == 0 || p.sky_height == 0) return fail(ctx, WGPT_E_INVALID, "params sky_width/sky_height are zero");
     uint64_t last = (uint64_t)p.sky_cdf_index + (uint64_t)(p.sky_height - 1) * (p.sky_width + 1) + p.sky_width - 1;
@@ -404,6 +406,7 @@ int wgpt_destroy(wgpt_ctx* ctx) {
   dfree_t(ctx->canvas); dfree_t(ctx->d_status); dfree_t(ctx->d_counters); wgpt::wf_engine_destroy(ctx->wf);
   ctx->wf = nullptr;
   dfree(ctx->d_pairs_tlas); dfree(ctx->d_pairs_bvh);
+  for (auto& v : ctx->views) { dfree_t(v.accum); dfree_t(v.out); }
   if (ctx->timer) {
     if (ctx->timer->ready)
       for (int i = 0; i < wgpt::StageTimer::kMaxEvents; ++i) cudaEventDestroy(ctx->timer->ev[i]);
@@ -498,7 +501,7 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
   if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
   int rc = check_section(ctx, sx, sy, sw, sh);
   if (rc) return rc;
-  rc = check_env(ctx);
+  rc = check_env(ctx, ctx->params);
   if (rc) return rc;
   if (reps == 0) return WGPT_OK;
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -677,6 +680,87 @@ int wgpt_set_render_mode(wgpt_ctx* ctx, int mode) {
   if (!ctx) return WGPT_E_INVALID;
   if (mode != WGPT_MODE_WAVEFRONT && mode != WGPT_MODE_MEGAKERNEL) return fail(ctx, WGPT_E_INVALID, "unknown render mode");
   ctx->mode = mode;
+  return WGPT_OK;
+}
+
+int wgpt_set_views(wgpt_ctx* ctx, uint32_t n, const uint32_t* widths, const uint32_t* heights) {
+  if (!ctx || (n && (!widths || !heights))) return WGPT_E_INVALID;
+  if (n > 4096) return fail(ctx, WGPT_E_INVALID, "more than 4096 views");
+  for (uint32_t i = 0; i < n; ++i)
+    if (widths[i] == 0 || heights[i] == 0 || widths[i] > 16384 || heights[i] > 16384)
+      return fail(ctx, WGPT_E_INVALID, "view size must be 1..16384 per side");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "drain before view allocation");
+  for (auto& v : ctx->views) { dfree_t(v.accum); dfree_t(v.out); }
+  ctx->views.clear();
+  for (uint32_t i = 0; i < n; ++i) {
+    wgpt_ctx::View v{widths[i], heights[i], nullptr, nullptr};
+    size_t np = (size_t)v.w * v.h;
+    ctx->views.push_back(v);
+    CK(cudaMalloc(&ctx->views.back().accum, np * 16), "cudaMalloc view accumulation");
+    CK(cudaMalloc(&ctx->views.back().out, np * 4), "cudaMalloc view image");
+    CK(cudaMemsetAsync(ctx->views.back().accum, 0, np * 16, ctx->stream), "clear view accumulation");
+    CK(cudaMemsetAsync(ctx->views.back().out, 0, np * 4, ctx->stream), "clear view image");
+  }
+  return WGPT_OK;
+}
+
+int wgpt_render_views(wgpt_ctx* ctx, const void* params_112n, const uint32_t* first_frames, const uint32_t* spp,
+                      float* done_ms) {
+  if (!ctx || !params_112n || !first_frames || !spp) return WGPT_E_INVALID;
+  if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
+  const uint32_t n = (uint32_t)ctx->views.size();
+  if (n == 0) return fail(ctx, WGPT_E_STATE, "no views: call wgpt_set_views first");
+  std::vector<wgpt::WfJobView> jv(n);
+  wgpt_scene_params p0;
+  memcpy(&p0, params_112n, sizeof p0);
+  for (uint32_t i = 0; i < n; ++i) {
+    wgpt_scene_params q;
+    memcpy(&q, (const char*)params_112n + (size_t)i * sizeof q, sizeof q);
+    const auto& v = ctx->views[i];
+    char buf[160];
+    if (q.width != v.w || q.height != v.h) {
+      snprintf(buf, sizeof buf, "view %u: params %ux%u differ from the view size %ux%u", i, q.width, q.height, v.w, v.h);
+      return fail(ctx, WGPT_E_INVALID, buf);
+    }
+    if (q.sky_width != p0.sky_width || q.sky_height != p0.sky_height || q.sky_cdf_index != p0.sky_cdf_index ||
+        memcmp(&q.sky_total_lum, &p0.sky_total_lum, 4) != 0 || memcmp(&q.total_light_power, &p0.total_light_power, 4) != 0) {
+      snprintf(buf, sizeof buf, "view %u: sky fields differ from view 0 (all views render one scene)", i);
+      return fail(ctx, WGPT_E_INVALID, buf);
+    }
+    if ((uint64_t)v.w * v.h * spp[i] >= (1ull << 32)) {
+      snprintf(buf, sizeof buf, "view %u: pixels x samples must stay below 2^32", i);
+      return fail(ctx, WGPT_E_INVALID, buf);
+    }
+    int rc = check_env(ctx, q);
+    if (rc) return rc;
+    jv[i].q = q;
+    jv[i].sx = 0; jv[i].sy = 0; jv[i].sw = v.w; jv[i].sh = v.h;
+    jv[i].first_frame = first_frames[i];
+    jv[i].spp = spp[i];
+    jv[i].accum = v.accum;
+    jv[i].out = v.out;
+    jv[i].out_pitch = v.w;
+  }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
+  unsigned long long* cnt = ctx->counting ? ctx->d_counters : nullptr;
+  wgpt::StageTimer* tm = ctx->timing ? ctx->timer : nullptr;
+  CK(wgpt::wf_render(ctx->wf, ctx->ds, ctx->d_pairs_tlas, ctx->d_pairs_bvh, jv.data(), n, ctx->d_status, cnt,
+                     ctx->stream, tm, done_ms),
+     "batched render");
+  return WGPT_OK;
+}
+
+int wgpt_read_view(wgpt_ctx* ctx, uint32_t view, float* accum, uint8_t* out) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (view >= ctx->views.size()) return fail(ctx, WGPT_E_INVALID, "view index out of range");
+  int rc = wgpt_synchronize(ctx);
+  if (rc) return rc;
+  const auto& v = ctx->views[view];
+  size_t np = (size_t)v.w * v.h;
+  if (accum) CK(cudaMemcpy(accum, v.accum, np * 16, cudaMemcpyDeviceToHost), "read view accumulation");
+  if (out) CK(cudaMemcpy(out, v.out, np * 4, cudaMemcpyDeviceToHost), "read view image");
   return WGPT_OK;
 }
 

@@ -34,10 +34,8 @@
 namespace pt {
 
 struct WfBuffers {
-  float4* ray_o;     // origin.xyz
-  float4* ray_d;     // direction.xyz
-  float4* tp;        // throughput.xyz, last_surface_pdf
-  float4* rad;       // radiance.xyz, last_weight_sum
+  float4* ray;       // 2 per path (one 32-byte sector): origin.xyz, direction.xyz
+  float4* tr;        // 2 per path: (throughput.xyz, last_surface_pdf), (radiance.xyz, last_weight_sum)
   uint4* meta;       // rng, flags, bounce of the current segment, medium count
   uint32_t* unit;    // work unit of the slot's path
   float4* med;       // 8 per path: (ior, sigma.xyz), (emission.xyz, -) for media 0..3
@@ -76,7 +74,7 @@ struct WfView {
   uint32_t unit_base;     // unit = unit_base + sample * npix + pixel
   uint32_t pix_base;      // first pixel of the view in the pass's pixel numbering
   uint32_t out_pitch;     // pixels per row of the view's images
-  uint32_t pad;
+  uint32_t job;           // index of the view in the caller's list (completion tracking)
   float4* accum;
   uchar4* out;
 };
@@ -88,6 +86,9 @@ struct WfCtl {
   uint32_t n_units;       // units of the pass
   uint32_t max_iter;      // bound on the iterations (host-computed; the loop stops there)
   uint32_t n_views, n_pixels, fill_count, cond;
+  uint32_t track;         // record when each view's last sample finishes
+  uint32_t first_pass;    // the fill kernel records the start time
+  uint32_t pad[2];
   uint32_t counts[4][pt::K_NKINDS];
   pt::DParams sp;         // scene-level parameters (sky size, luminance, CDF offset) of the pass
 };
@@ -108,6 +109,9 @@ struct WfArgs {
   const WfView* views;
   WfCtl* ctl;
   float4* samples;        // radiance of every unit of the pass
+  uint32_t* remaining;    // per view of the call: samples still being traced
+  unsigned long long* done_ns;   // per view: global timer when its last sample finished
+  unsigned long long* t0_ns;     // global timer at the start of the call's first pass
   uint32_t* status;
   unsigned long long* counters;
 };
@@ -163,6 +167,12 @@ __device__ __forceinline__ const WfView* find_view(const WfArgs& a, uint32_t n_v
   return a.views + lo;
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Starts unit `u` in path slot `slot`: RNG seeding and discard, jittered camera ray
 // (shader.wgsl:2276-2287 with sample_number = the unit's sample).
 template <bool COUNT>
@@ -186,10 +196,10 @@ __device__ __forceinline__ void spawn(const WfArgs& a, uint32_t n_views, uint32_
   float sv = ((float)iy + j1) / (float)height;
   v3 d = normalize(vmix(vmix(v->p.ray00, v->p.ray10, su), vmix(v->p.ray01, v->p.ray11, su), 1.0f - sv));
   v3 eye = v->p.eye;
-  a.b.ray_o[slot] = make_float4(eye.x, eye.y, eye.z, 0.0f);
-  a.b.ray_d[slot] = make_float4(d.x, d.y, d.z, 0.0f);
-  a.b.tp[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-  a.b.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  a.b.ray[slot * 2] = make_float4(eye.x, eye.y, eye.z, 0.0f);
+  a.b.ray[slot * 2 + 1] = make_float4(d.x, d.y, d.z, 0.0f);
+  a.b.tr[slot * 2] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+  a.b.tr[slot * 2 + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   a.b.meta[slot] = make_uint4(rng, 0u, 0u, 0u);
   a.b.unit[slot] = u;
 }
@@ -200,6 +210,7 @@ template <bool COUNT>
 __global__ void __launch_bounds__(256) k_wf_fill(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   const uint32_t n = a.ctl->fill_count, n_views = a.ctl->n_views;
+  if (a.ctl->track && a.ctl->first_pass && blockIdx.x == 0 && threadIdx.x == 0) *a.t0_ns = global_ns();
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t slot = base + threadIdx.x;
     if (slot < n) {
@@ -247,7 +258,7 @@ __global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
       uint32_t qi = refill(have, cursor, n, exhausted);
       if (!have && qi < n) {
         slot = q.at(qi);
-        float4 o = a.b.ray_o[slot], d = a.b.ray_d[slot];
+        float4 o = a.b.ray[slot * 2], d = a.b.ray[slot * 2 + 1];
         t.rw.origin = mk3(o.x, o.y, o.z);
         t.rw.direction = mk3(d.x, d.y, d.z);
         closest_init<COUNT>(a.s, t, cn);
@@ -320,7 +331,7 @@ __global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a) {
     }
     queue_push(a.b.hitq, hit_count, slot, is_hit);
     if (i < n && !is_hit) {
-      float4 d4 = a.b.ray_d[slot], tp4 = a.b.tp[slot], rd4 = a.b.rad[slot];
+      float4 d4 = a.b.ray[slot * 2 + 1], tp4 = a.b.tr[slot * 2], rd4 = a.b.tr[slot * 2 + 1];
       uint4 meta = a.b.meta[slot];
       const int bounce = (int)meta.z;
       HitRec hit;
@@ -344,7 +355,7 @@ __global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a) {
       } else {
         radiance = radiance + throughput * clamp_firefly(mk3(0.02f, 0.03f, 0.05f), bounce);
       }
-      a.b.rad[slot] = make_float4(radiance.x, radiance.y, radiance.z, rd4.w);
+      a.b.tr[slot * 2 + 1] = make_float4(radiance.x, radiance.y, radiance.z, rd4.w);
       a.b.meta[slot] = make_uint4(meta.x, 0u, meta.z, meta.w);
     }
   }
@@ -401,7 +412,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
     uint32_t slot = 0;
     if (i < n) {
       slot = q[i];
-      float4 o4 = a.b.ray_o[slot], d4 = a.b.ray_d[slot], tp4 = a.b.tp[slot], rd4 = a.b.rad[slot];
+      float4 o4 = a.b.ray[slot * 2], d4 = a.b.ray[slot * 2 + 1], tp4 = a.b.tr[slot * 2], rd4 = a.b.tr[slot * 2 + 1];
       uint4 meta = a.b.meta[slot];
       const int bounce = (int)meta.z;
       uint4 h0 = a.b.hit[slot * 2], h1 = a.b.hit[slot * 2 + 1];
@@ -625,10 +636,10 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
       if (alive) flags |= F_ALIVE;
       sh_light = (flags & F_SHADOW_LIGHT) != 0u;
       sh_env = (flags & F_SHADOW_ENV) != 0u;
-      a.b.ray_o[slot] = make_float4(ray.origin.x, ray.origin.y, ray.origin.z, 0.0f);
-      a.b.ray_d[slot] = make_float4(ray.direction.x, ray.direction.y, ray.direction.z, 0.0f);
-      a.b.tp[slot] = make_float4(throughput.x, throughput.y, throughput.z, last_surface_pdf);
-      a.b.rad[slot] = make_float4(radiance.x, radiance.y, radiance.z, last_weight_sum);
+      a.b.ray[slot * 2] = make_float4(ray.origin.x, ray.origin.y, ray.origin.z, 0.0f);
+      a.b.ray[slot * 2 + 1] = make_float4(ray.direction.x, ray.direction.y, ray.direction.z, 0.0f);
+      a.b.tr[slot * 2] = make_float4(throughput.x, throughput.y, throughput.z, last_surface_pdf);
+      a.b.tr[slot * 2 + 1] = make_float4(radiance.x, radiance.y, radiance.z, last_weight_sum);
       a.b.meta[slot] = make_uint4(rng, flags, (uint32_t)bounce, (uint32_t)stack.count);
     }
     queue_push(a.b.shq, sh_count, slot * 2u, sh_light);
@@ -687,16 +698,17 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a) {
   uint32_t* cont_count = &a.ctl->counts[r1][K_CONT];
   uint32_t* new_count = &a.ctl->counts[r1][K_NEW];
   const uint32_t n_units = a.ctl->n_units, n_views = a.ctl->n_views;
+  const bool track = a.ctl->track != 0u;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     bool alive = false, ended = false;
-    uint32_t slot = 0;
+    uint32_t slot = 0, unit = 0;
     if (i < n) {
       slot = q.at(i);
       uint4 meta = a.b.meta[slot];
       uint32_t flags = meta.y;
       int bounce = (int)meta.z;
-      float4 rd4 = a.b.rad[slot];
+      float4 rd4 = a.b.tr[slot * 2 + 1];
       v3 radiance = mk3(rd4.x, rd4.y, rd4.z);
       if (flags & (F_NEE_LIGHT | F_NEE_ENV)) {
 #pragma unroll
@@ -712,15 +724,25 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a) {
       }
       if (flags & F_ALIVE) {
         alive = true;
-        if (flags & (F_NEE_LIGHT | F_NEE_ENV)) a.b.rad[slot] = make_float4(radiance.x, radiance.y, radiance.z, rd4.w);
+        if (flags & (F_NEE_LIGHT | F_NEE_ENV)) a.b.tr[slot * 2 + 1] = make_float4(radiance.x, radiance.y, radiance.z, rd4.w);
         a.b.meta[slot] = make_uint4(meta.x, 0u, meta.z + 1u, meta.w);
       } else {
-        a.samples[a.b.unit[slot]] = make_float4(radiance.x, radiance.y, radiance.z, 0.0f);
+        unit = a.b.unit[slot];
+        a.samples[unit] = make_float4(radiance.x, radiance.y, radiance.z, 0.0f);
         ended = true;
       }
     }
     queue_push(a.b.qcont[p1], cont_count, slot, alive);
     unsigned em = __ballot_sync(0xffffffffu, ended);
+    if (track && ended) {
+      // one atomic per view per warp; the lane that takes a view's count to zero stamps it
+      uint32_t job = find_view(a, n_views, unit)->job;
+      unsigned peers = __match_any_sync(em, job);
+      if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) {
+        uint32_t k = (uint32_t)__popc(peers);
+        if (atomicSub(&a.remaining[job], k) == k) a.done_ns[job] = global_ns();
+      }
+    }
     bool started = false;
     if (em) {
       int lane = threadIdx.x & 31;
@@ -827,11 +849,11 @@ static void fill_dparams(DParams& p, const wgpt_scene_params& q, uint32_t sec_x,
   p.sec_x = sec_x; p.sec_y = sec_y; p.sky_cdf_index = q.sky_cdf_index;
 }
 
-// Path-slot state: ray 32 + tp 16 + rad 16 + meta 16 + unit 4 + media 128 + hit 32 + nee 64 +
-// shadow 64 + vis 2 + continuing and new queues 16 + hit queue 4 + shadow queue 8.
+// Path-slot state: ray 32 + throughput/radiance 32 + meta 16 + unit 4 + media 128 + hit 32 +
+// nee 64 + shadow 64 + vis 2 + continuing and new queues 16 + hit queue 4 + shadow queue 8.
 static constexpr int kParts = 16;
 static void part_sizes(size_t n, size_t out[kParts]) {
-  size_t v[kParts] = {n * 16, n * 16, n * 16, n * 16, n * 16, n * 4, n * 128, n * 32,
+  size_t v[kParts] = {n * 32, n * 32, 0, 0, n * 16, n * 4, n * 128, n * 32,
                       n * 64, n * 64, n * 2, n * 4, n * 4, n * 4, n * 4, n * 4};
   for (int i = 0; i < kParts; ++i) out[i] = v[i];
 }
@@ -850,10 +872,8 @@ static WfBuffers carve(void* scratch, uint32_t capacity) {
   auto take = [&](size_t bytes) { char* r = p; p += (bytes + 255) & ~(size_t)255; return (void*)r; };
   WfBuffers b;
   size_t n = capacity;
-  b.ray_o = (float4*)take(n * 16);
-  b.ray_d = (float4*)take(n * 16);
-  b.tp = (float4*)take(n * 16);
-  b.rad = (float4*)take(n * 16);
+  b.ray = (float4*)take(n * 32);
+  b.tr = (float4*)take(n * 32);
   b.meta = (uint4*)take(n * 16);
   b.unit = (uint32_t*)take(n * 4);
   b.med = (float4*)take(n * 128);
@@ -880,6 +900,9 @@ struct WfEngine {
   WfView* d_views = nullptr;
   uint32_t views_cap = 0;
   WfCtl* d_ctl = nullptr;
+  uint32_t* d_remaining = nullptr;         // per-view completion tracking
+  unsigned long long* d_done = nullptr;    // track_cap stamps, then the start stamp
+  uint32_t track_cap = 0;
   uint32_t* h_cond = nullptr;              // pinned copy of the loop condition (host-driven loop)
   int grids[2][8] = {{0}, {0}};              // launch grid per stage (counting / plain variants)
   int* grid = grids[0];
@@ -907,6 +930,8 @@ void wf_engine_destroy(WfEngine* e) {
   if (e->samples) cudaFree(e->samples);
   if (e->d_views) cudaFree(e->d_views);
   if (e->d_ctl) cudaFree(e->d_ctl);
+  if (e->d_remaining) cudaFree(e->d_remaining);
+  if (e->d_done) cudaFree(e->d_done);
   if (e->h_cond) cudaFreeHost(e->h_cond);
   delete e;
 }
@@ -1040,9 +1065,10 @@ static cudaError_t run_pass_host(WfEngine* e, const WfArgs& a, uint32_t max_iter
 template <bool COUNT>
 static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* pairs_tlas, const void* pairs_bvh,
                                 const WfJobView* jv, uint32_t nv, uint32_t* status, unsigned long long* counters,
-                                cudaStream_t st, StageTimer* timer) {
+                                cudaStream_t st, StageTimer* timer, float* done_ms) {
   cudaError_t err;
   compute_grids<COUNT>(e);
+  const bool track = done_ms != nullptr;
   uint64_t total_npix = 0;
   for (uint32_t v = 0; v < nv; ++v) total_npix += (uint64_t)jv[v].sw * jv[v].sh;
   if (total_npix == 0) return cudaSuccess;
@@ -1060,15 +1086,55 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
     if ((err = cudaMalloc(&e->d_views, sizeof(WfView) * nv)) != cudaSuccess) return err;
     e->views_cap = nv;
   }
+  if (e->track_cap < nv) {
+    cudaStreamSynchronize(st);
+    drop_graph(e);
+    if (e->d_remaining) cudaFree(e->d_remaining);
+    if (e->d_done) cudaFree(e->d_done);
+    e->d_remaining = nullptr;
+    e->d_done = nullptr;
+    e->track_cap = 0;
+    if ((err = cudaMalloc(&e->d_remaining, sizeof(uint32_t) * nv)) != cudaSuccess) return err;
+    if ((err = cudaMalloc(&e->d_done, sizeof(unsigned long long) * (nv + 1))) != cudaSuccess) return err;
+    e->track_cap = nv;
+  }
+  if (track) {
+    std::vector<uint32_t> rem(nv);
+    for (uint32_t v = 0; v < nv; ++v) rem[v] = jv[v].sw * jv[v].sh * jv[v].spp;
+    if ((err = cudaMemcpyAsync(e->d_remaining, rem.data(), sizeof(uint32_t) * nv, cudaMemcpyHostToDevice, st)) !=
+        cudaSuccess)
+      return err;
+    if ((err = cudaMemsetAsync(e->d_done, 0, sizeof(unsigned long long) * (nv + 1), st)) != cudaSuccess) return err;
+  }
+  // views in ascending order of work: the unit numbering decides which views finish first, and
+  // shortest-first minimises the mean completion time; results do not depend on the order
+  std::vector<uint32_t> order(nv);
+  for (uint32_t v = 0; v < nv; ++v) order[v] = v;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+    return (uint64_t)jv[x].sw * jv[x].sh * jv[x].spp < (uint64_t)jv[y].sw * jv[y].sh * jv[y].spp;
+  });
   std::vector<uint32_t> done(nv, 0u);
   std::vector<WfView> hv;
   hv.reserve(nv);
+  bool first_pass = true;
   while (true) {
-    uint64_t per = std::max<uint64_t>(1, e->units_per_pass / total_npix);
+    // samples per view in this pass: the largest count whose units fit units_per_pass (at least 1)
+    auto units_at = [&](uint64_t s_) {
+      uint64_t u = 0;
+      for (uint32_t v = 0; v < nv; ++v) u += (uint64_t)jv[v].sw * jv[v].sh * std::min<uint64_t>(jv[v].spp - done[v], s_);
+      return u;
+    };
+    uint64_t lo = 1, hi = 1;
+    for (uint32_t v = 0; v < nv; ++v) hi = std::max<uint64_t>(hi, jv[v].spp - done[v]);
+    while (lo < hi) {
+      uint64_t mid = (lo + hi + 1) / 2;
+      if (units_at(mid) <= e->units_per_pass) lo = mid; else hi = mid - 1;
+    }
+    const uint64_t per = lo;
     hv.clear();
     uint64_t units = 0, pixels = 0;
     std::vector<uint32_t> take(nv, 0u);
-    for (uint32_t v = 0; v < nv; ++v) {
+    for (uint32_t v : order) {
       uint32_t rem = jv[v].spp - done[v];
       uint32_t npix = jv[v].sw * jv[v].sh;
       if (rem == 0 || npix == 0) continue;
@@ -1085,6 +1151,7 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
       w.out_pitch = jv[v].out_pitch;
       w.accum = (float4*)jv[v].accum;
       w.out = (uchar4*)jv[v].out;
+      w.job = v;
       hv.push_back(w);
       units += (uint64_t)npix * take[v];
       pixels += npix;
@@ -1124,6 +1191,8 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
     c.fill_count = fill;
     c.counts[0][K_NEW] = fill;
     c.sp = hv[0].p;
+    c.track = track ? 1u : 0u;
+    c.first_pass = first_pass ? 1u : 0u;
     if ((err = cudaMemcpyAsync(e->d_views, hv.data(), sizeof(WfView) * hv.size(), cudaMemcpyHostToDevice, st)) !=
         cudaSuccess)
       return err;
@@ -1137,6 +1206,9 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
     a.views = e->d_views;
     a.ctl = e->d_ctl;
     a.samples = e->samples;
+    a.remaining = e->d_remaining;
+    a.done_ns = e->d_done;
+    a.t0_ns = e->d_done + e->track_cap;
     a.status = status;
     a.counters = counters;
     if (bl <= 0) {
@@ -1158,16 +1230,30 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
       if ((err = cudaGraphLaunch(e->exec, st)) != cudaSuccess) return err;
     }
     for (uint32_t v = 0; v < nv; ++v) done[v] += take[v];
+    first_pass = false;
+  }
+  if (track) {
+    std::vector<unsigned long long> ns(nv + 1);
+    if ((err = cudaMemcpyAsync(ns.data(), e->d_done, sizeof(unsigned long long) * nv, cudaMemcpyDeviceToHost, st)) !=
+        cudaSuccess)
+      return err;
+    if ((err = cudaMemcpyAsync(&ns[nv], e->d_done + e->track_cap, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                               st)) != cudaSuccess)
+      return err;
+    if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return err;
+    for (uint32_t v = 0; v < nv; ++v)
+      done_ms[v] = ns[v] >= ns[nv] && ns[v] != 0ull ? (float)((double)(ns[v] - ns[nv]) * 1e-6) : -1.0f;
   }
   return cudaSuccess;
 }
 
 cudaError_t wf_render(WfEngine* e, const DeviceScene& d, const void* pairs_tlas, const void* pairs_bvh,
                       const WfJobView* views, uint32_t n_views, uint32_t* status, unsigned long long* counters,
-                      cudaStream_t st, StageTimer* timer) {
+                      cudaStream_t st, StageTimer* timer, float* done_ms) {
   if (!e || n_views == 0) return cudaErrorInvalidValue;
-  if (counters) return render_views<true>(e, d, pairs_tlas, pairs_bvh, views, n_views, status, counters, st, timer);
-  return render_views<false>(e, d, pairs_tlas, pairs_bvh, views, n_views, status, counters, st, timer);
+  if (counters)
+    return render_views<true>(e, d, pairs_tlas, pairs_bvh, views, n_views, status, counters, st, timer, done_ms);
+  return render_views<false>(e, d, pairs_tlas, pairs_bvh, views, n_views, status, counters, st, timer, done_ms);
 }
 
 }  // namespace wgpt

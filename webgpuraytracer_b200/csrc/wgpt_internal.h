@@ -67,7 +67,7 @@ void wf_engine_get(const WfEngine* e, uint32_t* pool_paths, uint64_t* units_per_
 size_t wavefront_bytes_per_path();
 cudaError_t wf_render(WfEngine* e, const DeviceScene& d, const void* pairs_tlas, const void* pairs_bvh,
                       const WfJobView* views, uint32_t n_views, uint32_t* status, unsigned long long* counters,
-                      cudaStream_t st, StageTimer* timer);
+                      cudaStream_t st, StageTimer* timer, float* done_ms = nullptr);
 cudaError_t launch_gbuffer(const DeviceScene& d, const wgpt_scene_params& q, uint32_t sx, uint32_t sy, uint32_t sw,
                            uint32_t sh, float* gbuf, uint8_t* out, uint32_t out_pitch, uint32_t* status,
                            cudaStream_t st);

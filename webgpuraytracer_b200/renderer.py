@@ -213,6 +213,33 @@ class Renderer:
                     "get_wavefront_config")
         return int(pool.value), int(units.value)
 
+    # -- batched views (many cameras of the uploaded scene in one call)
+    def set_views(self, sizes):
+        """Allocates one image pair (accumulation, rgba8) per (width, height)."""
+        w = np.array([x[0] for x in sizes], np.uint32)
+        h = np.array([x[1] for x in sizes], np.uint32)
+        self._views = [(int(a), int(b)) for a, b in zip(w, h)]
+        self._check(self.L.wgpt_set_views(self.ctx, len(w), ptr(w), ptr(h)), "set_views")
+
+    def render_views(self, params, first_frames, spp, timing: bool = True):
+        """Adds spp[i] samples to view i (params: n x 112-byte SceneParams).  Returns the
+        per-view completion times in ms from the start of the call's work (timing=True)."""
+        blob = np.ascontiguousarray(np.concatenate([np.frombuffer(np.asarray(p).tobytes(), np.uint8)
+                                                    for p in params]))
+        ff = np.ascontiguousarray(first_frames, np.uint32)
+        sp = np.ascontiguousarray(spp, np.uint32)
+        done = np.full(len(ff), -1.0, np.float32)
+        self._check(self.L.wgpt_render_views(self.ctx, ptr(blob), ptr(ff), ptr(sp), ptr(done) if timing else None),
+                    "render_views")
+        return done
+
+    def read_view(self, i: int):
+        w, h = self._views[i]
+        acc = np.empty((h, w, 4), np.float32)
+        out = np.empty((h, w, 4), np.uint8)
+        self._check(self.L.wgpt_read_view(self.ctx, i, ptr(acc), ptr(out)), "read_view")
+        return acc, out
+
     def set_counting(self, on: bool):
         self._check(self.L.wgpt_set_counting(self.ctx, 1 if on else 0), "set_counting")
 

@@ -323,3 +323,41 @@ def flagship_scene(seed: int = 1, width: int = 1920, height: int = 1080, bounces
     cam.exposure = 1.0
     cam.aspect = width / height
     return s
+
+
+BATCH_SIZES = ((256, 256), (512, 512), (1280, 720), (1920, 1080))
+BATCH_SPP = (4, 16, 64)
+
+
+def batch_scene(seed: int = 1, bounces: int = 8) -> sc.Scene:
+    """The batched-views workload's scene: the displaced icosphere at 7 subdivisions (327,680
+    triangles, the icosphere level nearest above a 262,144-triangle mesh) instanced 16 times
+    (5.24 M triangles) plus 64 analytic primitives, under the importance-sampled procedural sky."""
+    return flagship_scene(seed, 1920, 1080, bounces, instances=16, prims=64, subdivisions=7)
+
+
+def batch_views(seed: int = 1, n: int = 32) -> list[dict]:
+    """n camera views with seeded sizes (uniform over BATCH_SIZES), samples (uniform over
+    BATCH_SPP) and positions on a ring around the scene, looking at its centre region."""
+    rnd = mulberry32(seed * 7919 + 17)
+    views = []
+    for i in range(n):
+        w, h = BATCH_SIZES[min(int(rnd() * len(BATCH_SIZES)), len(BATCH_SIZES) - 1)]
+        spp = BATCH_SPP[min(int(rnd() * len(BATCH_SPP)), len(BATCH_SPP) - 1)]
+        ang = rnd() * 2.0 * math.pi
+        radius = _uniform(rnd, 16.0, 26.0)
+        eye = (radius * math.cos(ang), _uniform(rnd, 2.0, 10.0), radius * math.sin(ang))
+        target = (_uniform(rnd, -3, 3), _uniform(rnd, 0.5, 3.0), _uniform(rnd, -3, 3))
+        views.append({"width": w, "height": h, "spp": spp, "eye": eye, "target": target})
+    return views
+
+
+def view_params(scene: sc.Scene, packed, view: dict, frame: int = 0, seed: int = 1) -> np.ndarray:
+    """The 112-byte SceneParams of one view: the scene's camera moved to the view's eye and
+    target, with the view's aspect ratio."""
+    cam = scene.camera
+    cam.position = sc.gm.vec3(*view["eye"])
+    cam.target = sc.gm.vec3(*view["target"])
+    cam.aspect = view["width"] / view["height"]
+    cam.update_rays2()
+    return sc.pack_params(scene, packed, view["width"], view["height"], frame, seed)

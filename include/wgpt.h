@@ -148,6 +148,11 @@ int wgpt_render_views(wgpt_ctx* ctx, const void* params_112n, const uint32_t* fi
                       float* done_ms);
 int wgpt_read_view(wgpt_ctx* ctx, uint32_t view, float* accum_rgba32f, uint8_t* out_rgba8);
 
+/* BF16 GEMM on the tensor cores (tcgen05, FP32 accumulation in tensor memory), the core of the
+   learned denoiser's kernels (no counterpart in the reference): C[m x n] = A[m x k] * B[n x k]^T
+   with row-major host matrices of BF16 bit patterns, k a multiple of 8.  For tests and tools. */
+int wgpt_gemm_bf16(int device, const uint16_t* a, const uint16_t* b, float* c, int m, int n, int k);
+
 /* Closest hit of caller rays (trace_scene, shader.wgsl:754-774) for parity tests: rays are n x
    (origin, direction) floats; outputs object index, material index, global triangle index
    (-1 unless a mesh triangle), t, world normal (3 floats). Host pointers. */

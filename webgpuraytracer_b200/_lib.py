@@ -85,6 +85,7 @@ EXPORTS = {
     "wgpt_set_render_mode": ([_P, C.c_int], C.c_int),
     "wgpt_set_wavefront_config": ([_P, C.c_uint32, C.c_uint64], C.c_int),
     "wgpt_set_views": ([_P, C.c_uint32, _P, _P], C.c_int),
+    "wgpt_gemm_bf16": ([C.c_int, _P, _P, _P, C.c_int, C.c_int, C.c_int], C.c_int),
     "wgpt_render_views": ([_P, _P, _P, _P, _P], C.c_int),
     "wgpt_read_view": ([_P, C.c_uint32, _P, _P], C.c_int),
     "wgpt_get_wavefront_config": ([_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)], C.c_int),

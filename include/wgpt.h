@@ -153,6 +153,36 @@ int wgpt_read_view(wgpt_ctx* ctx, uint32_t view, float* accum_rgba32f, uint8_t* 
    with row-major host matrices of BF16 bit patterns, k a multiple of 8.  For tests and tools. */
 int wgpt_gemm_bf16(int device, const uint16_t* a, const uint16_t* b, float* c, int m, int n, int k);
 
+/* Learned kernel-predicting denoiser (no counterpart in the reference, whose only denoiser is
+   the a-trous filter, which stays the fallback).  A 5-level encoder-decoder (32/48/64/96/128
+   channels, ~0.73 M parameters) over 10 features of the accumulation and G-buffer (log colour,
+   albedo, normal, depth) predicts a 5x5 filter per pixel, applied to the noisy colour.  BF16
+   weights and activations, FP32 accumulation on the tensor cores, FP32 master weights trained
+   by Adam on the relative L2 loss sum((f-t)^2/(t^2+0.01))/(3 pixels).  Parameters are one flat
+   FP32 array, per layer W[cout][taps][cin] then bias[cout] (layer table in kpcn.cu).
+   Examples are (noisy rgba32f, 48-byte G-buffer, target rgba32f) images of one common size;
+   training samples `batch` random crops of crop x crop pixels per step (losses: steps floats).
+   wgpt_kpcn_loss_and_grads evaluates one whole image (for gradient checks).  wgpt_kpcn_denoise
+   filters a context's accumulation with its G-buffer into its rgba8 image (tonemapped with
+   `exposure`), ordered after the context's queued work; filtered (nullable, host) receives the
+   linear result. */
+typedef struct wgpt_kpcn wgpt_kpcn;
+int wgpt_kpcn_create(int device, uint64_t seed, wgpt_kpcn** out);
+int wgpt_kpcn_destroy(wgpt_kpcn* k);
+const char* wgpt_kpcn_last_error(wgpt_kpcn* k);
+int wgpt_kpcn_num_params(wgpt_kpcn* k, uint64_t* n);
+int wgpt_kpcn_get_params(wgpt_kpcn* k, float* dst);
+int wgpt_kpcn_set_params(wgpt_kpcn* k, const float* src);
+int wgpt_kpcn_add_example(wgpt_kpcn* k, const float* noisy_rgba32f, const void* gbuf_48B, const float* target_rgba32f,
+                          uint32_t w, uint32_t h);
+int wgpt_kpcn_num_examples(wgpt_kpcn* k, uint32_t* n);
+int wgpt_kpcn_train(wgpt_kpcn* k, uint32_t steps, uint32_t batch, uint32_t crop, float lr, uint64_t seed,
+                    float* losses);
+int wgpt_kpcn_loss_and_grads(wgpt_kpcn* k, const float* noisy_rgba32f, const void* gbuf_48B,
+                             const float* target_rgba32f, uint32_t w, uint32_t h, float* loss, float* grads,
+                             float* out_rgba32f);
+int wgpt_kpcn_denoise(wgpt_kpcn* k, wgpt_ctx* ctx, float exposure, float* filtered_rgba32f);
+
 /* Closest hit of caller rays (trace_scene, shader.wgsl:754-774) for parity tests: rays are n x
    (origin, direction) floats; outputs object index, material index, global triangle index
    (-1 unless a mesh triangle), t, world normal (3 floats). Host pointers. */

@@ -34,3 +34,98 @@ def test_tc_gemm_matches_fp32(m, n, k):
     # FP32 accumulation of k products of BF16 values (exact in FP32): rounding only
     tol = 1e-5 * np.sqrt(k) * np.abs(bf16_value(a)).max() * np.abs(bf16_value(b)).max() * 4
     assert err.max() <= max(tol, 1e-4), f"max abs error {err.max()} (tol {tol})"
+
+
+# ------------------------------------------------------------------------ the learned denoiser
+import oracle.kpcn_ref as kref
+from webgpuraytracer_b200 import kpcn
+from webgpuraytracer_b200 import renderer as rd
+from webgpuraytracer_b200 import synth
+
+
+def _random_image(h, w, seed):
+    rng = np.random.default_rng(seed)
+    noisy = (np.abs(rng.standard_normal((h, w, 4))) * 0.6).astype(np.float32)
+    gbuf = rng.standard_normal((h, w, 12)).astype(np.float32)
+    gbuf[..., 4:7] = rng.random((h, w, 3))
+    gbuf[..., 11] = rng.random((h, w)) * 8.0
+    target = (np.abs(rng.standard_normal((h, w, 4))) * 0.5).astype(np.float32)
+    return noisy, gbuf, target
+
+
+def test_kpcn_layout_and_params_roundtrip():
+    k = kpcn.Kpcn(0, seed=3)
+    assert k.n_params == kpcn.N_PARAMS == 727_584
+    p = k.get_params()
+    sl = kpcn.param_slices()
+    w0 = p[sl["E0a"][0]].reshape(32, 9, 16)
+    assert np.all(w0[:, :, 10:] == 0.0), "padded input channels start at zero"
+    wo = p[sl["OUT"][0]].reshape(32, 32)
+    assert np.all(wo[25:] == 0.0), "padded logits start at zero"
+    q = p * 0.5
+    k.set_params(q)
+    np.testing.assert_array_equal(k.get_params(), q)
+    k.close()
+
+
+@pytest.mark.parametrize("h,w", [(40, 48), (33, 70)])
+def test_kpcn_loss_and_gradients_match_fp64_reference(h, w):
+    """Forward (filtered colour, loss) and backward (every parameter gradient) of the BF16
+    tensor-core network against the float64 restatement with the same BF16-rounded inputs and
+    weights.  Odd sizes exercise the partial pooling windows and the cropped upsampling."""
+    noisy, gbuf, target = _random_image(h, w, h * 1000 + w)
+    k = kpcn.Kpcn(0, seed=5)
+    p = k.get_params()
+    # larger output weights than the initialisation, so every layer carries gradient
+    sl = kpcn.param_slices()
+    p[sl["OUT"][0]] *= 10.0
+    k.set_params(p)
+    loss_g, grad_g, out_g = k.loss_and_grads(noisy, gbuf, target)
+    loss_r, grad_r, out_r = kref.loss_and_grads(p, noisy, gbuf, target)
+    assert abs(loss_g - loss_r) <= 0.02 * abs(loss_r), (loss_g, loss_r)
+    np.testing.assert_allclose(out_g[..., :3], out_r, rtol=0.03, atol=0.02 * float(np.abs(out_r).max()))
+    for l in kpcn.LAYERS:
+        for part, s in zip(("W", "b"), sl[l.name]):
+            g, r = grad_g[s].astype(np.float64), grad_r[s]
+            nr = np.linalg.norm(r)
+            assert nr > 0, f"{l.name}.{part}: no gradient in the reference"
+            cos = float(g @ r / (np.linalg.norm(g) * nr + 1e-30))
+            rel = float(np.linalg.norm(g - r) / nr)
+            assert cos > 0.99 and rel < 0.12, f"{l.name}.{part}: cosine {cos:.4f}, relative error {rel:.4f}"
+    k.close()
+
+
+def _example(seed, size, spp, target_spp):
+    s = synth.small_scene(seed, size, size, 4)
+    return kpcn.render_example(s, size, spp, target_spp, seed=seed, target_seed=10_000 + seed)
+
+
+def test_kpcn_training_gains_over_atrous():
+    """Trained on path-traced pairs of one scene family, the network denoises a held-out scene
+    at 4 spp with lower display-space RMSE than the a-trous filter and than no filter."""
+    size, spp, tspp = 128, 4, 512
+    k = kpcn.Kpcn(0, seed=11)
+    for seed in range(2, 26):
+        k.add_example(*_example(seed, size, spp, tspp))
+    losses = k.train(600, batch=8, crop=64, lr=1e-3, seed=3)
+    assert np.all(np.isfinite(losses))
+    assert losses[-50:].mean() < 0.6 * losses[:50].mean(), (losses[:50].mean(), losses[-50:].mean())
+    noisy, gbuf, target = _example(1, size, spp, tspp)
+    s = synth.small_scene(1, size, size, 4)
+    r = rd.Renderer(size, size)
+    r.set_scene(s, isgbuf=True)
+    r.write_accum(noisy)
+    r.write_gbuffer(gbuf)
+    lin = k.denoise(r, exposure=1.0)
+    dn = rd.Denoiser(r, passes=4)
+    dn.execute()
+    _, comp, _ = dn.read()
+    ref = kpcn.tonemap(target)
+    e_noisy = kpcn.rmse(noisy, target)
+    e_kpcn = kpcn.rmse(lin, target)
+    e_atrous = float(np.sqrt(np.mean((np.clip(comp[..., :3], 0, 1) - ref) ** 2)))
+    print(f"display RMSE: noisy {e_noisy:.4f}  a-trous {e_atrous:.4f}  kpcn {e_kpcn:.4f}")
+    assert e_kpcn < e_noisy
+    assert e_kpcn < e_atrous
+    r.close()
+    k.close()

@@ -86,6 +86,17 @@ EXPORTS = {
     "wgpt_set_wavefront_config": ([_P, C.c_uint32, C.c_uint64], C.c_int),
     "wgpt_set_views": ([_P, C.c_uint32, _P, _P], C.c_int),
     "wgpt_gemm_bf16": ([C.c_int, _P, _P, _P, C.c_int, C.c_int, C.c_int], C.c_int),
+    "wgpt_kpcn_create": ([C.c_int, C.c_uint64, C.POINTER(_P)], C.c_int),
+    "wgpt_kpcn_destroy": ([_P], C.c_int),
+    "wgpt_kpcn_last_error": ([_P], C.c_char_p),
+    "wgpt_kpcn_num_params": ([_P, C.POINTER(C.c_uint64)], C.c_int),
+    "wgpt_kpcn_get_params": ([_P, _P], C.c_int),
+    "wgpt_kpcn_set_params": ([_P, _P], C.c_int),
+    "wgpt_kpcn_add_example": ([_P, _P, _P, _P, C.c_uint32, C.c_uint32], C.c_int),
+    "wgpt_kpcn_num_examples": ([_P, C.POINTER(C.c_uint32)], C.c_int),
+    "wgpt_kpcn_train": ([_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64, _P], C.c_int),
+    "wgpt_kpcn_loss_and_grads": ([_P, _P, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P], C.c_int),
+    "wgpt_kpcn_denoise": ([_P, _P, C.c_float, _P], C.c_int),
     "wgpt_render_views": ([_P, _P, _P, _P, _P], C.c_int),
     "wgpt_read_view": ([_P, C.c_uint32, _P, _P], C.c_int),
     "wgpt_get_wavefront_config": ([_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)], C.c_int),

@@ -370,6 +370,18 @@ int check_env(wgpt_ctx* ctx, const wgpt_scene_params& p) {
 
 }  // namespace
 
+bool wgpt::ctx_images(wgpt_ctx* ctx, wgpt::CtxImages* out) {
+  if (!ctx || !out || ctx->w == 0 || !ctx->accum) return false;
+  out->device = ctx->device;
+  out->w = ctx->w;
+  out->h = ctx->h;
+  out->accum = ctx->accum;
+  out->gbuf = ctx->gbuf;
+  out->out = ctx->out;
+  out->stream = ctx->stream;
+  return true;
+}
+
 extern "C" {
 
 int wgpt_abi_version(void) { return WGPT_ABI_VERSION; }

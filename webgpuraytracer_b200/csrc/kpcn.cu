@@ -18,6 +18,10 @@ struct RowMajor {
     if (row >= rows || k8 * 8 >= k) return make_uint4(0u, 0u, 0u, 0u);
     return *reinterpret_cast<const uint4*>(p + (size_t)row * ld + k8 * 8);
   }
+  template <int ROWS>
+  __device__ __forceinline__ void fill(uint8_t* tile, int row0, int k0, int tid) const {
+    tc::fill_chunks<ROWS>(*this, tile, row0, k0, tid);
+  }
 };
 
 struct StoreF32 {
@@ -37,8 +41,9 @@ cudaError_t launch_gemm(const LA& la, const LB& lb, const EP& ep, int M, int N, 
   const int smem = tc::Smem<BN>::BYTES;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)((M + tc::BM - 1) / tc::BM), (unsigned)((N + BN - 1) / BN));
-  kern<<<grid, tc::THREADS, smem, st>>>(la, lb, ep, M, N, K, err);
+  const int kt_all = (K + tc::BK - 1) / tc::BK;
+  dim3 grid((unsigned)((M + tc::BM - 1) / tc::BM), (unsigned)((N + BN - 1) / BN), 1u);
+  kern<<<grid, tc::THREADS, smem, st>>>(la, lb, ep, M, N, K, kt_all, err);
   return cudaGetLastError();
 }
 
@@ -75,3 +80,1016 @@ extern "C" int wgpt_gemm_bf16(int device, const uint16_t* a, const uint16_t* b, 
   cudaFree(da); cudaFree(db); cudaFree(dc); cudaFree(derr);
   return rc;
 }
+
+// ============================================================================================
+// Kernel-predicting convolutional denoiser (KPCN).
+//
+// A 5-level encoder-decoder over 10 input features (log colour, albedo, normal, depth) predicts
+// per pixel a 5x5 filter (softmax over 25 logits) that is applied to the noisy linear colour.
+// Activations are NHWC BF16 with channel counts padded to multiples of 16; every convolution
+// (forward, data gradient, weight gradient) is one tensor-core GEMM whose loaders gather the
+// implicit im2col operand straight from the NHWC tensors (2x nearest upsampling and the skip
+// concatenation of the decoder are folded into the gather).  Weights are FP32 masters with BF16
+// copies for the GEMMs, trained by Adam on a relative-L2 loss.
+//
+// Layer table (channels, resolution level):
+//   E0a 10(16)->32 L0   E0 32->32 L0   E1 32->48 L1   E2 48->64 L2   E3 64->96 L3
+//   E4a 96->128 L4      E4 128->128 L4
+//   D3 [up E4 128, E3 96]->96 L3   D2 [up D3 96, E2 64]->64 L2   D1 [up D2 64, E1 48]->48 L1
+//   D0 [up D1 48, E0 32]->32 L0    OUT 1x1 32->25(32) L0
+// with 2x2 average pooling between encoder levels (E0->P1, E1->P2, E2->P3, E3->P4).
+// ============================================================================================
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace kp {
+
+__device__ __forceinline__ uint16_t f2bf(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ float bf2f(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
+__device__ __forceinline__ uint4 zero4() { return make_uint4(0u, 0u, 0u, 0u); }
+
+// 8-channel vectors of a convolution's input: a coarse tensor read 2x-upsampled (nearest),
+// channels [0, cu), concatenated with a tensor at the output resolution, channels [cu, cu+cs).
+struct ConvSrc {
+  const uint16_t* u;
+  int cu, hc, wc;
+  const uint16_t* s;
+  int cs;
+  int h, w;      // output resolution of one image
+  int taps;      // 9 (3x3, padding 1) or 1
+  int sign;      // +1: neighbour at p + offset (forward, weight gradient); -1: p - offset (data gradient)
+  __device__ __forceinline__ uint4 vec(int p, int tap, int ci0) const {
+    const int hw = h * w;
+    const int b = p / hw;
+    const int r = p - b * hw;
+    int y = r / w, x = r - (r / w) * w;
+    if (taps == 9) {
+      y += sign * (tap / 3 - 1);
+      x += sign * (tap % 3 - 1);
+    }
+    if (y < 0 || y >= h || x < 0 || x >= w) return zero4();
+    if (ci0 < cu) {
+      size_t q = ((size_t)b * hc + (y >> 1)) * wc + (x >> 1);
+      return *reinterpret_cast<const uint4*>(u + q * cu + ci0);
+    }
+    size_t q = ((size_t)b * h + y) * w + x;
+    return *reinterpret_cast<const uint4*>(s + q * cs + (ci0 - cu));
+  }
+};
+
+// A operand of a convolution: row = output pixel, k = tap * cin + ci.
+struct ConvA {
+  ConvSrc src;
+  int P, cin;
+  __device__ __forceinline__ uint4 chunk(int row, int k8) const {
+    if (row >= P) return zero4();
+    const int k = k8 * 8, tap = k / cin;
+    if (tap >= src.taps) return zero4();
+    return src.vec(row, tap, k - tap * cin);
+  }
+  template <int ROWS>
+  __device__ __forceinline__ void fill(uint8_t* tile, int row0, int k0, int tid) const {
+    tc::fill_chunks<ROWS>(*this, tile, row0, k0, tid);
+  }
+};
+
+__device__ __forceinline__ void scatter8(uint8_t* tile, int r0, int k, uint4 v) {
+  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    uint16_t h = (uint16_t)((w[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu);
+    *reinterpret_cast<uint16_t*>(tile + tc::elem_off(r0 + i, k)) = h;
+  }
+}
+
+// Weight gradient, A operand: row = output channel co, k = pixel; dZ is NHWC [P][cout].
+struct WgradA {
+  const uint16_t* dz;
+  int cout, P;
+  template <int ROWS>
+  __device__ __forceinline__ void fill(uint8_t* tile, int row0, int k0, int tid) const {
+    const int G = ROWS / 8;
+    for (int i = tid; i < G * tc::BK; i += tc::THREADS) {
+      const int g = i % G, j = i / G, p = k0 + j, co0 = row0 + g * 8;
+      uint4 v = zero4();
+      if (p < P && co0 < cout) v = *reinterpret_cast<const uint4*>(dz + (size_t)p * cout + co0);
+      scatter8(tile, g * 8, j, v);
+    }
+  }
+};
+
+// Weight gradient, B operand: row n = tap * cin + ci, k = pixel; the input gathered at the tap.
+struct WgradB {
+  ConvSrc src;
+  int cin, P, n_total;
+  template <int ROWS>
+  __device__ __forceinline__ void fill(uint8_t* tile, int row0, int k0, int tid) const {
+    const int G = ROWS / 8;
+    for (int i = tid; i < G * tc::BK; i += tc::THREADS) {
+      const int g = i % G, j = i / G, p = k0 + j, n = row0 + g * 8;
+      uint4 v = zero4();
+      if (p < P && n < n_total) {
+        const int tap = n / cin;
+        v = src.vec(p, tap, n - tap * cin);
+      }
+      scatter8(tile, g * 8, j, v);
+    }
+  }
+};
+
+// bias + optional ReLU, BF16 NHWC store of 16 channels.
+struct EpiAct {
+  uint16_t* y;
+  const float* bias;
+  int cstride, relu;
+  __device__ __forceinline__ void operator()(int row, int col0, const float (&v)[16]) const {
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      float a = v[2 * i] + bias[col0 + 2 * i], b = v[2 * i + 1] + bias[col0 + 2 * i + 1];
+      if (relu) { a = fmaxf(a, 0.0f); b = fmaxf(b, 0.0f); }
+      w[i] = (uint32_t)f2bf(a) | ((uint32_t)f2bf(b) << 16);
+    }
+    uint4* dst = reinterpret_cast<uint4*>(y + (size_t)row * cstride + col0);
+    dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+  }
+};
+
+// bias, FP32 store (filter logits).
+struct EpiLogits {
+  float* y;
+  const float* bias;
+  int cstride;
+  __device__ __forceinline__ void operator()(int row, int col0, const float (&v)[16]) const {
+    float4* dst = reinterpret_cast<float4*>(y + (size_t)row * cstride + col0);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      dst[i] = make_float4(v[4 * i] + bias[col0 + 4 * i], v[4 * i + 1] + bias[col0 + 4 * i + 1],
+                           v[4 * i + 2] + bias[col0 + 4 * i + 2], v[4 * i + 3] + bias[col0 + 4 * i + 3]);
+  }
+};
+
+// BF16 store without bias (data gradients).
+struct EpiStore {
+  uint16_t* y;
+  int cstride;
+  __device__ __forceinline__ void operator()(int row, int col0, const float (&v)[16]) const {
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) w[i] = (uint32_t)f2bf(v[2 * i]) | ((uint32_t)f2bf(v[2 * i + 1]) << 16);
+    uint4* dst = reinterpret_cast<uint4*>(y + (size_t)row * cstride + col0);
+    dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+  }
+};
+
+// FP32 atomic accumulation (split-K weight gradients).
+struct EpiAtomic {
+  float* dw;
+  int ld, ncols;
+  __device__ __forceinline__ void operator()(int row, int col0, const float (&v)[16]) const {
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      if (col0 + i < ncols && v[i] != 0.0f) atomicAdd(dw + (size_t)row * ld + col0 + i, v[i]);
+  }
+};
+
+template <int BN, class LA, class LB, class EP>
+cudaError_t gemm(const LA& la, const LB& lb, const EP& ep, int M, int N, int K, int splits, uint32_t* err,
+                 cudaStream_t st) {
+  auto kern = tc::k_tc_gemm<BN, LA, LB, EP>;
+  const int smem = tc::Smem<BN>::BYTES;
+  static bool attr_set = false;   // one instantiation per template: set its smem limit once
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  const int kt_all = (K + tc::BK - 1) / tc::BK;
+  const int kt_per = (kt_all + splits - 1) / splits;
+  dim3 grid((unsigned)((M + tc::BM - 1) / tc::BM), (unsigned)((N + BN - 1) / BN), (unsigned)splits);
+  kern<<<grid, tc::THREADS, smem, st>>>(la, lb, ep, M, N, K, kt_per, err);
+  return cudaGetLastError();
+}
+
+// GEMMs whose N is an output-channel count (forward, data gradient): one N tile when N <= 128.
+template <class LA, class LB, class EP>
+cudaError_t gemm_n(const LA& la, const LB& lb, const EP& ep, int M, int N, int K, uint32_t* err, cudaStream_t st) {
+  if (N <= 32) return gemm<32>(la, lb, ep, M, N, K, 1, err, st);
+  if (N <= 64) return gemm<64>(la, lb, ep, M, N, K, 1, err, st);
+  return gemm<128>(la, lb, ep, M, N, K, 1, err, st);
+}
+
+// ---------------------------------------------------------------------------- small kernels
+struct Crop { int e, oy, ox, pad; };
+
+// Batch gather: features (log1p colour, albedo, normal, depth/(depth+3); 16 channels, BF16),
+// noisy colour and target of each crop pixel.  Dataset images are e x h_img x w_img.
+__global__ void k_gather(const float4* __restrict__ col, const float* __restrict__ gbuf, const float4* __restrict__ tgt,
+                         int h_img, int w_img, const Crop* __restrict__ crops, int B, int h, int w,
+                         uint16_t* __restrict__ x0, float4* __restrict__ col_out, float4* __restrict__ tgt_out) {
+  const int P = B * h * w;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
+    const Crop c = crops[b];
+    const size_t src = ((size_t)c.e * h_img + (c.oy + y)) * w_img + (c.ox + x);
+    float4 cl = col[src];
+    const float* g = gbuf + src * 12;
+    float f[16];
+    f[0] = log1pf(fmaxf(cl.x, 0.0f)); f[1] = log1pf(fmaxf(cl.y, 0.0f)); f[2] = log1pf(fmaxf(cl.z, 0.0f));
+    f[3] = g[4]; f[4] = g[5]; f[5] = g[6];
+    f[6] = g[0]; f[7] = g[1]; f[8] = g[2];
+    float d = fmaxf(g[11], 0.0f);
+    f[9] = d / (d + 3.0f);
+#pragma unroll
+    for (int i = 10; i < 16; ++i) f[i] = 0.0f;
+    uint32_t wv[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) wv[i] = (uint32_t)f2bf(f[2 * i]) | ((uint32_t)f2bf(f[2 * i + 1]) << 16);
+    uint4* dst = reinterpret_cast<uint4*>(x0 + (size_t)p * 16);
+    dst[0] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+    dst[1] = make_uint4(wv[4], wv[5], wv[6], wv[7]);
+    col_out[p] = cl;
+    if (tgt) tgt_out[p] = tgt[src];
+  }
+}
+
+__device__ __forceinline__ void coarse_dims(int h, int w, int& hc, int& wc) { hc = (h + 1) >> 1; wc = (w + 1) >> 1; }
+
+// 2x2 average pooling (children beyond an odd edge are left out of the mean).
+__global__ void k_avgpool(const uint16_t* __restrict__ in, uint16_t* __restrict__ out, int B, int h, int w, int C) {
+  int hc, wc;
+  coarse_dims(h, w, hc, wc);
+  const size_t n = (size_t)B * hc * wc * (C / 8);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int g = (int)(i % (C / 8));
+    const size_t q = i / (C / 8);
+    const int b = (int)(q / ((size_t)hc * wc)), r = (int)(q - (size_t)b * hc * wc), yc = r / wc, xc = r - (r / wc) * wc;
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int cnt = 0;
+    for (int dy = 0; dy < 2; ++dy)
+      for (int dx = 0; dx < 2; ++dx) {
+        int y = 2 * yc + dy, x = 2 * xc + dx;
+        if (y >= h || x >= w) continue;
+        ++cnt;
+        uint4 v = *reinterpret_cast<const uint4*>(in + (((size_t)b * h + y) * w + x) * C + g * 8);
+        const uint32_t ww[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] += bf2f((uint16_t)(ww[k >> 1] >> ((k & 1) * 16)));
+      }
+    const float inv = 1.0f / (float)cnt;
+    uint32_t o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[k] = (uint32_t)f2bf(acc[2 * k] * inv) | ((uint32_t)f2bf(acc[2 * k + 1] * inv) << 16);
+    *reinterpret_cast<uint4*>(out + q * C + g * 8) = make_uint4(o[0], o[1], o[2], o[3]);
+  }
+}
+
+// Softmax over the 25 logits, 5x5 filter (clamp-to-edge) applied to the noisy colour; with a
+// target also the relative-L2 loss sum((f-t)^2 / (t^2 + 0.01)) / (3 P) and its logit gradient.
+__global__ void k_apply(const float* __restrict__ logits, const float4* __restrict__ col, int B, int h, int w,
+                        float4* __restrict__ out, const float4* __restrict__ tgt, uint16_t* __restrict__ dlogits,
+                        float* __restrict__ loss) {
+  const int P = B * h * w;
+  const float norm = 1.0f / (3.0f * (float)P);
+  float local = 0.0f;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
+    const float* lg = logits + (size_t)p * 32;
+    float mx = lg[0];
+    for (int k = 1; k < 25; ++k) mx = fmaxf(mx, lg[k]);
+    float wk[25], sum = 0.0f;
+    for (int k = 0; k < 25; ++k) { wk[k] = __expf(lg[k] - mx); sum += wk[k]; }
+    const float inv = 1.0f / sum;
+    float3 f = make_float3(0.0f, 0.0f, 0.0f);
+    float3 cs[25];
+    for (int k = 0; k < 25; ++k) {
+      int yy = min(max(y + k / 5 - 2, 0), h - 1), xx = min(max(x + k % 5 - 2, 0), w - 1);
+      float4 c = col[((size_t)b * h + yy) * w + xx];
+      cs[k] = make_float3(c.x, c.y, c.z);
+      wk[k] *= inv;
+      f.x += wk[k] * c.x; f.y += wk[k] * c.y; f.z += wk[k] * c.z;
+    }
+    out[p] = make_float4(f.x, f.y, f.z, 1.0f);
+    if (tgt) {
+      float4 t = tgt[p];
+      float ex = f.x - t.x, ey = f.y - t.y, ez = f.z - t.z;
+      float dx = 1.0f / (t.x * t.x + 0.01f), dy = 1.0f / (t.y * t.y + 0.01f), dz = 1.0f / (t.z * t.z + 0.01f);
+      local += ex * ex * dx + ey * ey * dy + ez * ez * dz;
+      float3 gf = make_float3(2.0f * ex * dx * norm, 2.0f * ey * dy * norm, 2.0f * ez * dz * norm);
+      float g[25], gw = 0.0f;
+      for (int k = 0; k < 25; ++k) {
+        g[k] = gf.x * cs[k].x + gf.y * cs[k].y + gf.z * cs[k].z;
+        gw += wk[k] * g[k];
+      }
+      uint32_t o[16];
+      for (int k = 0; k < 16; ++k) {
+        float a = 2 * k < 25 ? wk[2 * k] * (g[2 * k] - gw) : 0.0f;
+        float c = 2 * k + 1 < 25 ? wk[2 * k + 1] * (g[2 * k + 1] - gw) : 0.0f;
+        o[k] = (uint32_t)f2bf(a) | ((uint32_t)f2bf(c) << 16);
+      }
+      uint4* dst = reinterpret_cast<uint4*>(dlogits + (size_t)p * 32);
+      for (int k = 0; k < 4; ++k) dst[k] = make_uint4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+    }
+  }
+  if (tgt) {
+    for (int off = 16; off > 0; off >>= 1) local += __shfl_down_sync(0xffffffffu, local, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, local * norm);
+  }
+}
+
+// d = (y > 0) ? d : 0 over n BF16 values (ReLU backward; in place).
+__global__ void k_relu_mask(uint16_t* __restrict__ d, const uint16_t* __restrict__ y, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    if (!(bf2f(y[i]) > 0.0f)) d[i] = 0;
+}
+
+// Data gradient of a decoder convolution's input [up(coarse) cu | skip cs] at fine resolution:
+// the coarse part sums its 2x2 children and is masked by the coarse activation's ReLU.
+__global__ void k_split_up(const uint16_t* __restrict__ dx, int cu, int cs, int B, int h, int w,
+                           const uint16_t* __restrict__ coarse_act, uint16_t* __restrict__ dcoarse) {
+  int hc, wc;
+  coarse_dims(h, w, hc, wc);
+  const int cin = cu + cs;
+  const size_t n = (size_t)B * hc * wc * cu;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % cu);
+    const size_t q = i / cu;
+    const int b = (int)(q / ((size_t)hc * wc)), r = (int)(q - (size_t)b * hc * wc), yc = r / wc, xc = r - (r / wc) * wc;
+    float s = 0.0f;
+    for (int dy = 0; dy < 2; ++dy)
+      for (int dxx = 0; dxx < 2; ++dxx) {
+        int y = 2 * yc + dy, x = 2 * xc + dxx;
+        if (y < h && x < w) s += bf2f(dx[(((size_t)b * h + y) * w + x) * cin + c]);
+      }
+    dcoarse[i] = bf2f(coarse_act[i]) > 0.0f ? f2bf(s) : (uint16_t)0;
+  }
+}
+
+// Gradient of an encoder activation E (fine): skip part from the decoder's concat gradient plus
+// the pooled path's gradient spread over the 2x2 children, masked by E's ReLU.
+__global__ void k_enc_grad(const uint16_t* __restrict__ dx_cat, int cat_stride, int cat_off,
+                           const uint16_t* __restrict__ dpool, const uint16_t* __restrict__ e, int B, int h, int w,
+                           int C, uint16_t* __restrict__ dz) {
+  int hc, wc;
+  coarse_dims(h, w, hc, wc);
+  const size_t n = (size_t)B * h * w * C;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const size_t p = i / C;
+    const int b = (int)(p / ((size_t)h * w)), r = (int)(p - (size_t)b * h * w), y = r / w, x = r - (r / w) * w;
+    float g = bf2f(dx_cat[p * cat_stride + cat_off + c]);
+    if (dpool) {
+      const int yc = y >> 1, xc = x >> 1;
+      const int cnt = (min(2 * yc + 2, h) - 2 * yc) * (min(2 * xc + 2, w) - 2 * xc);
+      g += bf2f(dpool[(((size_t)b * hc + yc) * wc + xc) * C + c]) / (float)cnt;
+    }
+    dz[i] = bf2f(e[i]) > 0.0f ? f2bf(g) : (uint16_t)0;
+  }
+}
+
+// Bias gradient: column sums of dZ [P][C] (FP32 atomics per block).
+__global__ void k_bias_grad(const uint16_t* __restrict__ dz, int P, int C, float* __restrict__ db) {
+  extern __shared__ float acc[];
+  for (int c = threadIdx.x; c < C; c += blockDim.x) acc[c] = 0.0f;
+  __syncthreads();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)P * C; i += (size_t)gridDim.x * blockDim.x)
+    atomicAdd(&acc[i % C], bf2f(dz[i]));
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += blockDim.x)
+    if (acc[c] != 0.0f) atomicAdd(&db[c], acc[c]);
+}
+
+// Adam (bias-corrected) over the flat FP32 parameters.
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       size_t n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    float gi = g[i];
+    float mi = b1 * m[i] + (1.0f - b1) * gi;
+    float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+// BF16 copies of one layer's weights W[co][tap][ci]: as stored (forward, weight-gradient
+// layout) and transposed to Wt[ci][tap][co] (data gradient).
+__global__ void k_weights_bf16(const float* __restrict__ wf, int cout, int taps, int cin, uint16_t* __restrict__ wb,
+                               uint16_t* __restrict__ wt) {
+  const int n = cout * taps * cin;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int ci = i % cin, t = (i / cin) % taps, co = i / (cin * taps);
+    uint16_t b = f2bf(wf[i]);
+    wb[i] = b;
+    wt[((size_t)ci * taps + t) * cout + co] = b;
+  }
+}
+
+// Linear colour -> rgba8 with the accumulation pass's tonemap (shader.wgsl:2487-2490).
+__global__ void k_tonemap(const float4* __restrict__ c, int n, float exposure, uchar4* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 v = c[i];
+    float r = v.x * exposure, g = v.y * exposure, b = v.z * exposure;
+    r = powf(r / (r + 0.3f), 0.4545f); g = powf(g / (g + 0.3f), 0.4545f); b = powf(b / (b + 0.3f), 0.4545f);
+    auto u8 = [](float x) { return (unsigned char)floorf(fminf(fmaxf(x, 0.0f), 1.0f) * 255.0f + 0.5f); };
+    out[i] = make_uchar4(u8(r), u8(g), u8(b), 255);
+  }
+}
+
+// ---------------------------------------------------------------------------- the network
+struct Layer {
+  const char* name;
+  int cu, cs;        // input channels: upsampled coarse part, same-resolution part (padded)
+  int cout;          // output channels (padded)
+  int taps;          // 9 or 1
+  int relu;
+  int level;         // output resolution level
+  int real_cin, real_cout;   // channels before padding (initialisation)
+  size_t w_off, b_off;       // offsets into the flat parameters
+  uint16_t* wb = nullptr;    // BF16 [cout][taps][cin]
+  uint16_t* wt = nullptr;    // BF16 [cin][taps][cout]
+  int cin() const { return cu + cs; }
+  size_t nw() const { return (size_t)cout * taps * cin(); }
+};
+
+enum { L_E0A, L_E0, L_E1, L_E2, L_E3, L_E4A, L_E4, L_D3, L_D2, L_D1, L_D0, L_OUT, NLAYERS };
+
+struct Net {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  Layer L[NLAYERS];
+  size_t n_params = 0;
+  float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;   // FP32 parameters, gradients, Adam moments
+  int adam_t = 0;
+  uint32_t* err = nullptr;
+  // activations / gradients for the current batch shape
+  int B = 0, H = 0, W = 0, cap_px = 0;
+  int hl[5], wl[5];
+  uint16_t *x0 = nullptr, *e0a = nullptr, *e0 = nullptr, *p1 = nullptr, *e1 = nullptr, *p2 = nullptr, *e2 = nullptr,
+           *p3 = nullptr, *e3 = nullptr, *p4 = nullptr, *e4a = nullptr, *e4 = nullptr, *d3 = nullptr, *d2 = nullptr,
+           *d1 = nullptr, *d0 = nullptr;
+  float* logits = nullptr;
+  float4 *col = nullptr, *tgt = nullptr, *out = nullptr;
+  uint16_t *dlog = nullptr, *dx = nullptr, *g_a = nullptr, *g_b = nullptr, *g_pool = nullptr, *g_skip = nullptr;
+  std::vector<void*> bufs;
+  float* loss = nullptr;
+  Crop* crops = nullptr;
+  int crops_cap = 0;
+  // dataset
+  float4 *ds_col = nullptr, *ds_tgt = nullptr;
+  float* ds_gbuf = nullptr;
+  int ds_n = 0, ds_cap = 0, ds_h = 0, ds_w = 0;
+};
+
+static void set_layer(Layer& l, const char* name, int cu, int cs, int cout, int taps, int relu, int level, int rcin,
+                      int rcout) {
+  l.name = name; l.cu = cu; l.cs = cs; l.cout = cout; l.taps = taps; l.relu = relu; l.level = level;
+  l.real_cin = rcin; l.real_cout = rcout;
+}
+
+static void define_layers(Net& n) {
+  set_layer(n.L[L_E0A], "E0a", 0, 16, 32, 9, 1, 0, 10, 32);
+  set_layer(n.L[L_E0], "E0", 0, 32, 32, 9, 1, 0, 32, 32);
+  set_layer(n.L[L_E1], "E1", 0, 32, 48, 9, 1, 1, 32, 48);
+  set_layer(n.L[L_E2], "E2", 0, 48, 64, 9, 1, 2, 48, 64);
+  set_layer(n.L[L_E3], "E3", 0, 64, 96, 9, 1, 3, 64, 96);
+  set_layer(n.L[L_E4A], "E4a", 0, 96, 128, 9, 1, 4, 96, 128);
+  set_layer(n.L[L_E4], "E4", 0, 128, 128, 9, 1, 4, 128, 128);
+  set_layer(n.L[L_D3], "D3", 128, 96, 96, 9, 1, 3, 224, 96);
+  set_layer(n.L[L_D2], "D2", 96, 64, 64, 9, 1, 2, 160, 64);
+  set_layer(n.L[L_D1], "D1", 64, 48, 48, 9, 1, 1, 112, 48);
+  set_layer(n.L[L_D0], "D0", 48, 32, 32, 9, 1, 0, 80, 32);
+  set_layer(n.L[L_OUT], "OUT", 0, 32, 32, 1, 0, 0, 32, 25);
+  size_t off = 0;
+  for (int i = 0; i < NLAYERS; ++i) {
+    n.L[i].w_off = off;
+    off += n.L[i].nw();
+    n.L[i].b_off = off;
+    off += n.L[i].cout;
+  }
+  n.n_params = off;
+}
+
+static int grid1(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+static cudaError_t refresh_bf16(Net& n) {
+  for (int i = 0; i < NLAYERS; ++i) {
+    Layer& l = n.L[i];
+    k_weights_bf16<<<grid1(l.nw()), 256, 0, n.st>>>(n.w + l.w_off, l.cout, l.taps, l.cin(), l.wb, l.wt);
+  }
+  return cudaGetLastError();
+}
+
+static cudaError_t ensure_batch(Net& n, int B, int H, int W) {
+  if (n.B == B && n.H == H && n.W == W) return cudaSuccess;
+  cudaStreamSynchronize(n.st);
+  for (void* p : n.bufs) cudaFree(p);
+  n.bufs.clear();
+  n.B = B; n.H = H; n.W = W;
+  n.hl[0] = H; n.wl[0] = W;
+  for (int l = 1; l < 5; ++l) { n.hl[l] = (n.hl[l - 1] + 1) / 2; n.wl[l] = (n.wl[l - 1] + 1) / 2; }
+  auto px = [&](int l) { return (size_t)B * n.hl[l] * n.wl[l]; };
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&p, std::max<size_t>(bytes, 256));
+    if (p) n.bufs.push_back(p);
+    return p;
+  };
+  n.x0 = (uint16_t*)alloc(px(0) * 16 * 2);
+  n.e0a = (uint16_t*)alloc(px(0) * 32 * 2);
+  n.e0 = (uint16_t*)alloc(px(0) * 32 * 2);
+  n.p1 = (uint16_t*)alloc(px(1) * 32 * 2);
+  n.e1 = (uint16_t*)alloc(px(1) * 48 * 2);
+  n.p2 = (uint16_t*)alloc(px(2) * 48 * 2);
+  n.e2 = (uint16_t*)alloc(px(2) * 64 * 2);
+  n.p3 = (uint16_t*)alloc(px(3) * 64 * 2);
+  n.e3 = (uint16_t*)alloc(px(3) * 96 * 2);
+  n.p4 = (uint16_t*)alloc(px(4) * 96 * 2);
+  n.e4a = (uint16_t*)alloc(px(4) * 128 * 2);
+  n.e4 = (uint16_t*)alloc(px(4) * 128 * 2);
+  n.d3 = (uint16_t*)alloc(px(3) * 96 * 2);
+  n.d2 = (uint16_t*)alloc(px(2) * 64 * 2);
+  n.d1 = (uint16_t*)alloc(px(1) * 48 * 2);
+  n.d0 = (uint16_t*)alloc(px(0) * 32 * 2);
+  n.logits = (float*)alloc(px(0) * 32 * 4);
+  n.col = (float4*)alloc(px(0) * 16);
+  n.tgt = (float4*)alloc(px(0) * 16);
+  n.out = (float4*)alloc(px(0) * 16);
+  n.dlog = (uint16_t*)alloc(px(0) * 32 * 2);
+  // the largest data gradient: a concat input (fine) of any level
+  size_t dx_max = std::max({px(0) * 80, px(1) * 112, px(2) * 160, px(3) * 224, px(4) * 128});
+  n.dx = (uint16_t*)alloc(dx_max * 2);
+  size_t g_max = std::max({px(0) * 32, px(1) * 48, px(2) * 64, px(3) * 96, px(4) * 128});
+  n.g_a = (uint16_t*)alloc(g_max * 2);
+  n.g_b = (uint16_t*)alloc(g_max * 2);
+  n.g_pool = (uint16_t*)alloc(g_max * 2);
+  n.g_skip = (uint16_t*)alloc(dx_max * 2);
+  return e;
+}
+
+// Convolution of layer l over its sources (coarse u read upsampled, s at the output level).
+static cudaError_t conv_fwd(Net& n, const Layer& l, const uint16_t* u, const uint16_t* s, void* y, bool logits) {
+  const int lv = l.level, h = n.hl[lv], w = n.wl[lv];
+  const int P = n.B * h * w;
+  ConvSrc src{u, l.cu, lv + 1 < 5 ? n.hl[lv + 1] : 1, lv + 1 < 5 ? n.wl[lv + 1] : 1, s, l.cs, h, w, l.taps, 1};
+  ConvA a{src, P, l.cin()};
+  RowMajor b{l.wb, l.cout, l.taps * l.cin(), l.taps * l.cin()};
+  if (logits) return gemm_n(a, b, EpiLogits{(float*)y, n.w + l.b_off, l.cout}, P, l.cout, l.taps * l.cin(), n.err, n.st);
+  return gemm_n(a, b, EpiAct{(uint16_t*)y, n.w + l.b_off, l.cout, l.relu}, P, l.cout, l.taps * l.cin(), n.err, n.st);
+}
+
+// Weight and bias gradients of layer l from dZ (its output gradient) and its sources; the data
+// gradient of its (concatenated) input into n.dx when want_dx.
+static cudaError_t conv_bwd(Net& n, const Layer& l, const uint16_t* dz, const uint16_t* u, const uint16_t* s,
+                            bool want_dx) {
+  const int lv = l.level, h = n.hl[lv], w = n.wl[lv];
+  const int P = n.B * h * w, cin = l.cin(), K = l.taps * cin;
+  ConvSrc src{u, l.cu, lv + 1 < 5 ? n.hl[lv + 1] : 1, lv + 1 < 5 ? n.wl[lv + 1] : 1, s, l.cs, h, w, l.taps, 1};
+  // weight gradient: M = cout, N = taps * cin, K = pixels, split over pixel ranges
+  const int kt_all = (P + tc::BK - 1) / tc::BK;
+  const int n_tiles = (K + 127) / 128;
+  int splits = std::max(1, std::min(kt_all, (148 * 2) / std::max(1, n_tiles)));
+  cudaError_t e = gemm<128>(WgradA{dz, l.cout, P}, WgradB{src, cin, P, K}, EpiAtomic{n.g + l.w_off, K, K}, l.cout, K,
+                            P, splits, n.err, n.st);
+  if (e != cudaSuccess) return e;
+  k_bias_grad<<<std::min(grid1((size_t)P * l.cout), 512), 256, l.cout * 4, n.st>>>(dz, P, l.cout, n.g + l.b_off);
+  if (!want_dx) return cudaGetLastError();
+  // data gradient: M = pixels, N = cin, K = taps * cout, source = dZ read at p - offset
+  ConvSrc dsrc{nullptr, 0, 1, 1, dz, l.cout, h, w, l.taps, -1};
+  ConvA a{dsrc, P, l.cout};
+  RowMajor b{l.wt, cin, l.taps * l.cout, l.taps * l.cout};
+  return gemm_n(a, b, EpiStore{n.dx, cin}, P, cin, l.taps * l.cout, n.err, n.st);
+}
+
+static cudaError_t forward(Net& n) {
+  cudaError_t e;
+  const int B = n.B;
+  auto pool = [&](const uint16_t* in, uint16_t* outp, int lv, int C) {
+    size_t cnt = (size_t)B * n.hl[lv + 1] * n.wl[lv + 1] * (C / 8);
+    k_avgpool<<<grid1(cnt), 256, 0, n.st>>>(in, outp, B, n.hl[lv], n.wl[lv], C);
+  };
+  if ((e = conv_fwd(n, n.L[L_E0A], nullptr, n.x0, n.e0a, false))) return e;
+  if ((e = conv_fwd(n, n.L[L_E0], nullptr, n.e0a, n.e0, false))) return e;
+  pool(n.e0, n.p1, 0, 32);
+  if ((e = conv_fwd(n, n.L[L_E1], nullptr, n.p1, n.e1, false))) return e;
+  pool(n.e1, n.p2, 1, 48);
+  if ((e = conv_fwd(n, n.L[L_E2], nullptr, n.p2, n.e2, false))) return e;
+  pool(n.e2, n.p3, 2, 64);
+  if ((e = conv_fwd(n, n.L[L_E3], nullptr, n.p3, n.e3, false))) return e;
+  pool(n.e3, n.p4, 3, 96);
+  if ((e = conv_fwd(n, n.L[L_E4A], nullptr, n.p4, n.e4a, false))) return e;
+  if ((e = conv_fwd(n, n.L[L_E4], nullptr, n.e4a, n.e4, false))) return e;
+  if ((e = conv_fwd(n, n.L[L_D3], n.e4, n.e3, n.d3, false))) return e;
+  if ((e = conv_fwd(n, n.L[L_D2], n.d3, n.e2, n.d2, false))) return e;
+  if ((e = conv_fwd(n, n.L[L_D1], n.d2, n.e1, n.d1, false))) return e;
+  if ((e = conv_fwd(n, n.L[L_D0], n.d1, n.e0, n.d0, false))) return e;
+  if ((e = conv_fwd(n, n.L[L_OUT], nullptr, n.d0, n.logits, true))) return e;
+  return cudaGetLastError();
+}
+
+// Loss and all parameter gradients (n.g, zeroed here) for the batch in n.x0 / n.col / n.tgt.
+static cudaError_t backward(Net& n) {
+  cudaError_t e;
+  const int B = n.B;
+  auto px = [&](int lv) { return (size_t)B * n.hl[lv] * n.wl[lv]; };
+  if ((e = cudaMemsetAsync(n.g, 0, n.n_params * 4, n.st))) return e;
+  if ((e = cudaMemsetAsync(n.loss, 0, 4, n.st))) return e;
+  k_apply<<<grid1(px(0)), 256, 0, n.st>>>(n.logits, n.col, B, n.H, n.W, n.out, n.tgt, n.dlog, n.loss);
+  // OUT (1x1 over D0)
+  if ((e = conv_bwd(n, n.L[L_OUT], n.dlog, nullptr, n.d0, true))) return e;
+  uint16_t* gd0 = n.g_a;
+  cudaMemcpyAsync(gd0, n.dx, px(0) * 32 * 2, cudaMemcpyDeviceToDevice, n.st);
+  k_relu_mask<<<grid1(px(0) * 32), 256, 0, n.st>>>(gd0, n.d0, px(0) * 32);
+  // decoder: dZ of D_l -> its gradients; input gradient split into the coarse part (masked by
+  // the coarse activation) and the skip part (kept in g_skip for the encoder)
+  struct Dec { int layer; const uint16_t* u; const uint16_t* s; int lv; int cu; int cs; };
+  const Dec dec[4] = {{L_D0, n.d1, n.e0, 0, 48, 32}, {L_D1, n.d2, n.e1, 1, 64, 48}, {L_D2, n.d3, n.e2, 2, 96, 64},
+                      {L_D3, n.e4, n.e3, 3, 128, 96}};
+  // skip gradients of E0..E3 are needed after the decoder pass: keep them at offsets in g_skip
+  size_t skip_off[4], off = 0;
+  for (int i = 0; i < 4; ++i) { skip_off[i] = off; off += px(i) * dec[i].cs; }
+  uint16_t* gz = gd0;
+  uint16_t* gnext = n.g_b;
+  for (int i = 0; i < 4; ++i) {
+    const Dec& d = dec[i];
+    if ((e = conv_bwd(n, n.L[d.layer], gz, d.u, d.s, true))) return e;
+    size_t nc = (size_t)B * n.hl[d.lv + 1] * n.wl[d.lv + 1] * d.cu;
+    k_split_up<<<grid1(nc), 256, 0, n.st>>>(n.dx, d.cu, d.cs, B, n.hl[d.lv], n.wl[d.lv], d.u, gnext);
+    // skip part: copy channels [cu, cu+cs) of dx into g_skip (strided copy via 2D memcpy)
+    cudaMemcpy2DAsync(n.g_skip + skip_off[d.lv], (size_t)d.cs * 2, n.dx + d.cu, (size_t)(d.cu + d.cs) * 2,
+                      (size_t)d.cs * 2, px(d.lv), cudaMemcpyDeviceToDevice, n.st);
+    std::swap(gz, gnext);
+  }
+  // gz = dZ of E4 (level 4, 128 channels)
+  if ((e = conv_bwd(n, n.L[L_E4], gz, nullptr, n.e4a, true))) return e;
+  uint16_t* ge4a = gnext;
+  cudaMemcpyAsync(ge4a, n.dx, px(4) * 128 * 2, cudaMemcpyDeviceToDevice, n.st);
+  k_relu_mask<<<grid1(px(4) * 128), 256, 0, n.st>>>(ge4a, n.e4a, px(4) * 128);
+  if ((e = conv_bwd(n, n.L[L_E4A], ge4a, nullptr, n.p4, true))) return e;
+  // encoder levels 3..0: dZ_E = mask(E) (skip + unpool(dP)), then the level's convolution
+  struct Enc { int layer; const uint16_t* in; const uint16_t* e; int lv; int C; int cin; };
+  const Enc enc[4] = {{L_E3, n.p3, n.e3, 3, 96, 64}, {L_E2, n.p2, n.e2, 2, 64, 48}, {L_E1, n.p1, n.e1, 1, 48, 32},
+                      {L_E0, n.e0a, n.e0, 0, 32, 32}};
+  for (int i = 0; i < 4; ++i) {
+    const Enc& en = enc[i];
+    // n.dx holds dP_{lv+1} (the data gradient of the next level's first convolution)
+    cudaMemcpyAsync(n.g_pool, n.dx, px(en.lv + 1) * en.C * 2, cudaMemcpyDeviceToDevice, n.st);
+    uint16_t* gz_e = n.g_a;
+    k_enc_grad<<<grid1(px(en.lv) * en.C), 256, 0, n.st>>>(n.g_skip + skip_off[en.lv], en.C, 0, n.g_pool, en.e, B,
+                                                          n.hl[en.lv], n.wl[en.lv], en.C, gz_e);
+    if ((e = conv_bwd(n, n.L[en.layer], gz_e, nullptr, en.in, true))) return e;
+  }
+  // n.dx = gradient of E0a (level 0, 32 channels)
+  uint16_t* ge0a = n.g_b;
+  cudaMemcpyAsync(ge0a, n.dx, px(0) * 32 * 2, cudaMemcpyDeviceToDevice, n.st);
+  k_relu_mask<<<grid1(px(0) * 32), 256, 0, n.st>>>(ge0a, n.e0a, px(0) * 32);
+  if ((e = conv_bwd(n, n.L[L_E0A], ge0a, nullptr, n.x0, false))) return e;
+  return cudaGetLastError();
+}
+
+}  // namespace kp
+
+// ============================================================================================
+// C ABI of the learned denoiser.
+// ============================================================================================
+#include <string>
+#include "wgpt_internal.h"
+
+struct wgpt_kpcn {
+  kp::Net net;
+  std::string err;
+  float* d_losses = nullptr;
+  int losses_cap = 0;
+  kp::Crop* d_crops = nullptr;
+  size_t crops_cap = 0;
+  float4* d_img_col = nullptr;   // single-image staging (gradient check)
+  float4* d_img_tgt = nullptr;
+  float* d_img_gbuf = nullptr;
+  size_t img_cap = 0;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+};
+
+namespace {
+
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+double uniform01(uint64_t& s) { return (double)(splitmix(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+int kfail(wgpt_kpcn* k, int code, const std::string& m) {
+  if (k) k->err = m;
+  return code;
+}
+int kcuda(wgpt_kpcn* k, cudaError_t e, const char* what) {
+  return kfail(k, e == cudaErrorMemoryAllocation ? WGPT_E_NOMEM : WGPT_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define KCK(call, what)                                   \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return kcuda(k, e_, what);     \
+  } while (0)
+
+int check_device_error(wgpt_kpcn* k) {
+  uint32_t herr = 0;
+  KCK(cudaMemcpyAsync(&herr, k->net.err, 4, cudaMemcpyDeviceToHost, k->net.st), "error readback");
+  KCK(cudaStreamSynchronize(k->net.st), "synchronize");
+  if (herr) {
+    cudaMemsetAsync(k->net.err, 0, 4, k->net.st);
+    return kfail(k, WGPT_E_DEVICE, "a tensor-core kernel timed out waiting for its MMAs");
+  }
+  return WGPT_OK;
+}
+
+// He-uniform initialisation over the real (unpadded) fan-in; padded weights stay zero.  The
+// output layer starts small, so the first filters are close to a 5x5 box.
+void init_params(kp::Net& n, uint64_t seed, std::vector<float>& w) {
+  w.assign(n.n_params, 0.0f);
+  uint64_t s = seed * 0x2545F4914F6CDD1Dull + 12345u;
+  for (int i = 0; i < kp::NLAYERS; ++i) {
+    const kp::Layer& l = n.L[i];
+    const double a = std::sqrt(6.0 / (double)(l.taps * l.real_cin)) * (i == kp::L_OUT ? 0.1 : 1.0);
+    for (int co = 0; co < l.cout; ++co)
+      for (int t = 0; t < l.taps; ++t)
+        for (int ci = 0; ci < l.cin(); ++ci) {
+          float v = (float)((2.0 * uniform01(s) - 1.0) * a);
+          bool real = co < l.real_cout && (i != kp::L_E0A || ci < l.real_cin);
+          w[l.w_off + ((size_t)co * l.taps + t) * l.cin() + ci] = real ? v : 0.0f;
+        }
+  }
+}
+
+int stage_images(wgpt_kpcn* k, size_t npix) {
+  if (k->img_cap >= npix) return WGPT_OK;
+  cudaStreamSynchronize(k->net.st);
+  cudaFree(k->d_img_col); cudaFree(k->d_img_tgt); cudaFree(k->d_img_gbuf);
+  k->d_img_col = nullptr; k->d_img_tgt = nullptr; k->d_img_gbuf = nullptr; k->img_cap = 0;
+  KCK(cudaMalloc(&k->d_img_col, npix * 16), "cudaMalloc image");
+  KCK(cudaMalloc(&k->d_img_tgt, npix * 16), "cudaMalloc image");
+  KCK(cudaMalloc(&k->d_img_gbuf, npix * 48), "cudaMalloc image");
+  k->img_cap = npix;
+  return WGPT_OK;
+}
+
+int ensure_crops(wgpt_kpcn* k, size_t n) {
+  if (k->crops_cap >= n) return WGPT_OK;
+  cudaStreamSynchronize(k->net.st);
+  cudaFree(k->d_crops);
+  k->d_crops = nullptr;
+  k->crops_cap = 0;
+  KCK(cudaMalloc(&k->d_crops, n * sizeof(kp::Crop)), "cudaMalloc crops");
+  k->crops_cap = n;
+  return WGPT_OK;
+}
+
+cudaError_t adam_step(kp::Net& n, float lr) {
+  n.adam_t += 1;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - (float)std::pow(0.9, n.adam_t), c2 = 1.0f - (float)std::pow(0.999, n.adam_t);
+  kp::k_adam<<<kp::grid1(n.n_params), 256, 0, n.st>>>(n.w, n.g, n.m, n.v, n.n_params, lr, b1, b2, 1e-8f, c1, c2);
+  return kp::refresh_bf16(n);
+}
+
+}  // namespace
+
+extern "C" {
+
+int wgpt_kpcn_create(int device, uint64_t seed, wgpt_kpcn** out) {
+  if (!out) return WGPT_E_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return WGPT_E_CUDA;
+  if (device < 0 || device >= ndev) return WGPT_E_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return WGPT_E_CUDA;
+  wgpt_kpcn* k = new wgpt_kpcn();
+  kp::Net& n = k->net;
+  n.device = device;
+  kp::define_layers(n);
+  cudaError_t e = cudaStreamCreateWithFlags(&n.st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&n.w, n.n_params * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&n.g, n.n_params * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&n.m, n.n_params * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&n.v, n.n_params * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&n.err, 4);
+  if (e == cudaSuccess) e = cudaMalloc(&n.loss, 4);
+  for (int i = 0; i < kp::NLAYERS && e == cudaSuccess; ++i) {
+    e = cudaMalloc(&n.L[i].wb, n.L[i].nw() * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&n.L[i].wt, n.L[i].nw() * 2);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&k->ev_in, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&k->ev_out, cudaEventDisableTiming);
+  std::vector<float> w;
+  if (e == cudaSuccess) {
+    init_params(n, seed, w);
+    e = cudaMemcpy(n.w, w.data(), n.n_params * 4, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaMemset(n.m, 0, n.n_params * 4);
+  if (e == cudaSuccess) e = cudaMemset(n.v, 0, n.n_params * 4);
+  if (e == cudaSuccess) e = cudaMemset(n.err, 0, 4);
+  if (e == cudaSuccess) e = kp::refresh_bf16(n);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(n.st);
+  if (e != cudaSuccess) {
+    wgpt_kpcn_destroy(k);
+    return e == cudaErrorMemoryAllocation ? WGPT_E_NOMEM : WGPT_E_CUDA;
+  }
+  *out = k;
+  return WGPT_OK;
+}
+
+int wgpt_kpcn_destroy(wgpt_kpcn* k) {
+  if (!k) return WGPT_E_INVALID;
+  kp::Net& n = k->net;
+  cudaSetDevice(n.device);
+  if (n.st) cudaStreamSynchronize(n.st);
+  for (void* p : n.bufs) cudaFree(p);
+  for (int i = 0; i < kp::NLAYERS; ++i) { cudaFree(n.L[i].wb); cudaFree(n.L[i].wt); }
+  cudaFree(n.w); cudaFree(n.g); cudaFree(n.m); cudaFree(n.v); cudaFree(n.err); cudaFree(n.loss);
+  cudaFree(n.ds_col); cudaFree(n.ds_tgt); cudaFree(n.ds_gbuf);
+  cudaFree(k->d_losses); cudaFree(k->d_crops);
+  cudaFree(k->d_img_col); cudaFree(k->d_img_tgt); cudaFree(k->d_img_gbuf);
+  if (k->ev_in) cudaEventDestroy(k->ev_in);
+  if (k->ev_out) cudaEventDestroy(k->ev_out);
+  if (n.st) cudaStreamDestroy(n.st);
+  delete k;
+  return WGPT_OK;
+}
+
+const char* wgpt_kpcn_last_error(wgpt_kpcn* k) { return k ? k->err.c_str() : "null denoiser"; }
+
+int wgpt_kpcn_num_params(wgpt_kpcn* k, uint64_t* n) {
+  if (!k || !n) return WGPT_E_INVALID;
+  *n = k->net.n_params;
+  return WGPT_OK;
+}
+
+int wgpt_kpcn_get_params(wgpt_kpcn* k, float* dst) {
+  if (!k || !dst) return WGPT_E_INVALID;
+  cudaSetDevice(k->net.device);
+  KCK(cudaMemcpyAsync(dst, k->net.w, k->net.n_params * 4, cudaMemcpyDeviceToHost, k->net.st), "read params");
+  KCK(cudaStreamSynchronize(k->net.st), "synchronize");
+  return WGPT_OK;
+}
+
+int wgpt_kpcn_set_params(wgpt_kpcn* k, const float* src) {
+  if (!k || !src) return WGPT_E_INVALID;
+  kp::Net& n = k->net;
+  cudaSetDevice(n.device);
+  KCK(cudaMemcpyAsync(n.w, src, n.n_params * 4, cudaMemcpyHostToDevice, n.st), "write params");
+  KCK(cudaMemsetAsync(n.m, 0, n.n_params * 4, n.st), "reset moments");
+  KCK(cudaMemsetAsync(n.v, 0, n.n_params * 4, n.st), "reset moments");
+  n.adam_t = 0;
+  KCK(kp::refresh_bf16(n), "bf16 weights");
+  KCK(cudaStreamSynchronize(n.st), "synchronize");
+  return WGPT_OK;
+}
+
+int wgpt_kpcn_add_example(wgpt_kpcn* k, const float* noisy, const void* gbuf, const float* target, uint32_t w,
+                          uint32_t h) {
+  if (!k || !noisy || !gbuf || !target || w < 16 || h < 16) return WGPT_E_INVALID;
+  kp::Net& n = k->net;
+  cudaSetDevice(n.device);
+  if (n.ds_n > 0 && ((int)w != n.ds_w || (int)h != n.ds_h))
+    return kfail(k, WGPT_E_INVALID, "every example must have the size of the first");
+  const size_t npix = (size_t)w * h;
+  if (n.ds_n == n.ds_cap) {
+    int cap = std::max(8, n.ds_cap * 2);
+    float4 *c = nullptr, *t = nullptr;
+    float* g = nullptr;
+    KCK(cudaMalloc(&c, npix * 16 * cap), "cudaMalloc dataset");
+    KCK(cudaMalloc(&t, npix * 16 * cap), "cudaMalloc dataset");
+    KCK(cudaMalloc(&g, npix * 48 * cap), "cudaMalloc dataset");
+    if (n.ds_n) {
+      KCK(cudaMemcpyAsync(c, n.ds_col, npix * 16 * n.ds_n, cudaMemcpyDeviceToDevice, n.st), "copy dataset");
+      KCK(cudaMemcpyAsync(t, n.ds_tgt, npix * 16 * n.ds_n, cudaMemcpyDeviceToDevice, n.st), "copy dataset");
+      KCK(cudaMemcpyAsync(g, n.ds_gbuf, npix * 48 * n.ds_n, cudaMemcpyDeviceToDevice, n.st), "copy dataset");
+    }
+    KCK(cudaStreamSynchronize(n.st), "synchronize");
+    cudaFree(n.ds_col); cudaFree(n.ds_tgt); cudaFree(n.ds_gbuf);
+    n.ds_col = c; n.ds_tgt = t; n.ds_gbuf = g;
+    n.ds_cap = cap;
+  }
+  n.ds_w = (int)w;
+  n.ds_h = (int)h;
+  KCK(cudaMemcpyAsync(n.ds_col + npix * n.ds_n, noisy, npix * 16, cudaMemcpyHostToDevice, n.st), "upload example");
+  KCK(cudaMemcpyAsync(n.ds_tgt + npix * n.ds_n, target, npix * 16, cudaMemcpyHostToDevice, n.st), "upload example");
+  KCK(cudaMemcpyAsync(n.ds_gbuf + npix * 12 * n.ds_n, gbuf, npix * 48, cudaMemcpyHostToDevice, n.st), "upload example");
+  KCK(cudaStreamSynchronize(n.st), "synchronize");
+  n.ds_n += 1;
+  return WGPT_OK;
+}
+
+int wgpt_kpcn_num_examples(wgpt_kpcn* k, uint32_t* n) {
+  if (!k || !n) return WGPT_E_INVALID;
+  *n = (uint32_t)k->net.ds_n;
+  return WGPT_OK;
+}
+
+int wgpt_kpcn_train(wgpt_kpcn* k, uint32_t steps, uint32_t batch, uint32_t crop, float lr, uint64_t seed,
+                    float* losses) {
+  if (!k || batch == 0 || batch > 64 || crop < 16 || crop > 512 || (crop % 16) != 0 || !(lr > 0.0f))
+    return WGPT_E_INVALID;
+  kp::Net& n = k->net;
+  if (n.ds_n == 0) return kfail(k, WGPT_E_STATE, "no training examples");
+  if ((int)crop > n.ds_w || (int)crop > n.ds_h) return kfail(k, WGPT_E_INVALID, "crop larger than the examples");
+  if (steps == 0) return WGPT_OK;
+  cudaSetDevice(n.device);
+  KCK(kp::ensure_batch(n, (int)batch, (int)crop, (int)crop), "batch buffers");
+  int rc = ensure_crops(k, (size_t)steps * batch);
+  if (rc) return rc;
+  if (k->losses_cap < (int)steps) {
+    cudaFree(k->d_losses);
+    k->d_losses = nullptr;
+    KCK(cudaMalloc(&k->d_losses, steps * 4), "cudaMalloc losses");
+    k->losses_cap = (int)steps;
+  }
+  std::vector<kp::Crop> crops((size_t)steps * batch);
+  uint64_t s = seed * 0x9E3779B97F4A7C15ull + 7u;
+  for (auto& c : crops) {
+    c.e = (int)(splitmix(s) % (uint64_t)n.ds_n);
+    c.oy = (int)(splitmix(s) % (uint64_t)(n.ds_h - (int)crop + 1));
+    c.ox = (int)(splitmix(s) % (uint64_t)(n.ds_w - (int)crop + 1));
+    c.pad = 0;
+  }
+  KCK(cudaMemcpyAsync(k->d_crops, crops.data(), crops.size() * sizeof(kp::Crop), cudaMemcpyHostToDevice, n.st),
+      "upload crops");
+  const size_t P = (size_t)batch * crop * crop;
+  for (uint32_t it = 0; it < steps; ++it) {
+    kp::k_gather<<<kp::grid1(P), 256, 0, n.st>>>(n.ds_col, n.ds_gbuf, n.ds_tgt, n.ds_h, n.ds_w,
+                                                 k->d_crops + (size_t)it * batch, (int)batch, (int)crop, (int)crop,
+                                                 n.x0, n.col, n.tgt);
+    KCK(kp::forward(n), "forward");
+    KCK(kp::backward(n), "backward");
+    KCK(cudaMemcpyAsync(k->d_losses + it, n.loss, 4, cudaMemcpyDeviceToDevice, n.st), "loss copy");
+    KCK(adam_step(n, lr), "adam");
+  }
+  if (losses) KCK(cudaMemcpyAsync(losses, k->d_losses, steps * 4, cudaMemcpyDeviceToHost, n.st), "losses readback");
+  return check_device_error(k);
+}
+
+int wgpt_kpcn_loss_and_grads(wgpt_kpcn* k, const float* noisy, const void* gbuf, const float* target, uint32_t w,
+                             uint32_t h, float* loss, float* grads, float* out_rgba32f) {
+  if (!k || !noisy || !gbuf || !target || w < 16 || h < 16 || w > 4096 || h > 4096) return WGPT_E_INVALID;
+  kp::Net& n = k->net;
+  cudaSetDevice(n.device);
+  const size_t npix = (size_t)w * h;
+  int rc = stage_images(k, npix);
+  if (rc) return rc;
+  rc = ensure_crops(k, 1);
+  if (rc) return rc;
+  KCK(kp::ensure_batch(n, 1, (int)h, (int)w), "batch buffers");
+  kp::Crop c0{0, 0, 0, 0};
+  KCK(cudaMemcpyAsync(k->d_crops, &c0, sizeof c0, cudaMemcpyHostToDevice, n.st), "upload crop");
+  KCK(cudaMemcpyAsync(k->d_img_col, noisy, npix * 16, cudaMemcpyHostToDevice, n.st), "upload image");
+  KCK(cudaMemcpyAsync(k->d_img_tgt, target, npix * 16, cudaMemcpyHostToDevice, n.st), "upload image");
+  KCK(cudaMemcpyAsync(k->d_img_gbuf, gbuf, npix * 48, cudaMemcpyHostToDevice, n.st), "upload image");
+  kp::k_gather<<<kp::grid1(npix), 256, 0, n.st>>>(k->d_img_col, k->d_img_gbuf, k->d_img_tgt, (int)h, (int)w,
+                                                  k->d_crops, 1, (int)h, (int)w, n.x0, n.col, n.tgt);
+  KCK(kp::forward(n), "forward");
+  KCK(kp::backward(n), "backward");
+  if (loss) KCK(cudaMemcpyAsync(loss, n.loss, 4, cudaMemcpyDeviceToHost, n.st), "loss readback");
+  if (grads) KCK(cudaMemcpyAsync(grads, n.g, n.n_params * 4, cudaMemcpyDeviceToHost, n.st), "grads readback");
+  if (out_rgba32f) KCK(cudaMemcpyAsync(out_rgba32f, n.out, npix * 16, cudaMemcpyDeviceToHost, n.st), "output readback");
+  return check_device_error(k);
+}
+
+int wgpt_kpcn_denoise(wgpt_kpcn* k, wgpt_ctx* ctx, float exposure, float* filtered_rgba32f) {
+  if (!k || !ctx) return WGPT_E_INVALID;
+  kp::Net& n = k->net;
+  wgpt::CtxImages im;
+  if (!wgpt::ctx_images(ctx, &im)) return kfail(k, WGPT_E_STATE, "context has no image (resize first)");
+  if (!im.gbuf) return kfail(k, WGPT_E_STATE, "context has no G-buffer: resize with want_gbuf and render it");
+  if (im.device != n.device) return kfail(k, WGPT_E_INVALID, "context and denoiser are on different devices");
+  cudaSetDevice(n.device);
+  const size_t npix = (size_t)im.w * im.h;
+  int rc = ensure_crops(k, 1);
+  if (rc) return rc;
+  KCK(kp::ensure_batch(n, 1, (int)im.h, (int)im.w), "batch buffers");
+  kp::Crop c0{0, 0, 0, 0};
+  KCK(cudaMemcpyAsync(k->d_crops, &c0, sizeof c0, cudaMemcpyHostToDevice, n.st), "upload crop");
+  // the denoiser's stream waits for the context's queued work and the context's stream for the
+  // denoiser's result
+  KCK(cudaEventRecord(k->ev_in, im.stream), "event");
+  KCK(cudaStreamWaitEvent(n.st, k->ev_in, 0), "event wait");
+  kp::k_gather<<<kp::grid1(npix), 256, 0, n.st>>>((const float4*)im.accum, im.gbuf, nullptr, (int)im.h, (int)im.w,
+                                                  k->d_crops, 1, (int)im.h, (int)im.w, n.x0, n.col, nullptr);
+  KCK(kp::forward(n), "forward");
+  kp::k_apply<<<kp::grid1(npix), 256, 0, n.st>>>(n.logits, n.col, 1, (int)im.h, (int)im.w, n.out, nullptr, nullptr,
+                                                 nullptr);
+  kp::k_tonemap<<<kp::grid1(npix), 256, 0, n.st>>>(n.out, (int)npix, exposure, (uchar4*)im.out);
+  KCK(cudaGetLastError(), "denoise launch");
+  KCK(cudaEventRecord(k->ev_out, n.st), "event");
+  KCK(cudaStreamWaitEvent(im.stream, k->ev_out, 0), "event wait");
+  if (filtered_rgba32f) {
+    KCK(cudaMemcpyAsync(filtered_rgba32f, n.out, npix * 16, cudaMemcpyDeviceToHost, n.st), "filtered readback");
+    return check_device_error(k);
+  }
+  return WGPT_OK;
+}
+
+}  // extern "C"

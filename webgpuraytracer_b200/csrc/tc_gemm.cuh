@@ -118,11 +118,28 @@ __host__ __device__ constexpr uint32_t tmem_cols(int bn) {
 __device__ __forceinline__ void put_chunk(uint8_t* tile, int r, int c, uint4 v) {
   *reinterpret_cast<uint4*>(tile + ((r >> 3) * (BK / 8) + c) * 128 + (r & 7) * 16) = v;
 }
+// Byte offset of element (r, k) of a tile in the core-matrix layout.
+__device__ __forceinline__ int elem_off(int r, int k) { return ((r >> 3) * (BK / 8) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2; }
 
-// Loader contract: `uint4 chunk(int row, int k8) const` returns K-elements [8*k8, 8*k8 + 8) of
-// operand row `row` as 8 BF16 values (zero outside the matrix).
+// Fills a ROWS x BK tile from a chunk loader: `uint4 chunk(int row, int k8) const` returns
+// K-elements [8*k8, 8*k8 + 8) of operand row `row` as 8 BF16 values (zero outside the matrix).
+// Consecutive threads take consecutive rows of one K-chunk: conflict-free 16-byte smem stores.
+template <int ROWS, class L>
+__device__ __forceinline__ void fill_chunks(const L& l, uint8_t* tile, int row0, int k0, int tid) {
+  const int k8 = k0 >> 3;
+  for (int i = tid; i < ROWS * (BK / 8); i += THREADS) {
+    int r = i % ROWS, c = i / ROWS;
+    put_chunk(tile, r, c, l.chunk(row0 + r, k8 + c));
+  }
+}
+
+// Loader contract: `template <int ROWS> void fill(uint8_t* tile, int row0, int k0, int tid) const`
+// writes rows [row0, row0 + ROWS) x K-elements [k0, k0 + BK) of the operand into a tile (all of
+// it, zeros outside the matrix); the 128 threads of the CTA call it together.
+// Split K: blockIdx.z takes K-tiles [z * kt_per, (z + 1) * kt_per).
 template <int BN, class LA, class LB, class EP>
-__global__ void __launch_bounds__(THREADS) k_tc_gemm(LA la, LB lb, EP ep, int M, int N, int K, uint32_t* err) {
+__global__ void __launch_bounds__(THREADS) k_tc_gemm(LA la, LB lb, EP ep, int M, int N, int K, int kt_per,
+                                                     uint32_t* err) {
   extern __shared__ __align__(1024) uint8_t smem[];
   using S = Smem<BN>;
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -141,7 +158,9 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(LA la, LB lb, EP ep, int M,
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int KT = (K + BK - 1) / BK;
+  const int KT_ALL = (K + BK - 1) / BK;
+  const int kt_begin = blockIdx.z * kt_per;
+  const int KT = max(0, min(KT_ALL - kt_begin, kt_per));   // k-tiles of this CTA
   constexpr uint32_t IDESC = idesc_bf16(BN);
   bool ok = true;
   int committed = 0;   // k-tiles whose MMAs were committed
@@ -156,15 +175,9 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(LA la, LB lb, EP ep, int M,
       __syncthreads();
       if (*flag == 0u) { ok = false; break; }
     }
-    const int k8 = kt * (BK / 8);
-    for (int i = tid; i < BM * (BK / 8); i += THREADS) {
-      int r = i % BM, c = i / BM;
-      put_chunk(ta, r, c, la.chunk(m0 + r, k8 + c));
-    }
-    for (int i = tid; i < BN * (BK / 8); i += THREADS) {
-      int r = i % BN, c = i / BN;
-      put_chunk(tb, r, c, lb.chunk(n0 + r, k8 + c));
-    }
+    const int k0 = (kt_begin + kt) * BK;
+    la.template fill<BM>(ta, m0, k0, tid);
+    lb.template fill<BN>(tb, n0, k0, tid);
     fence_async_smem();
     __syncthreads();
     if (tid == 0) {

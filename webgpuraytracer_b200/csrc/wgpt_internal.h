@@ -4,7 +4,21 @@
 #include <cuda_runtime.h>
 #include "../../include/wgpt_layout.h"
 
+struct wgpt_ctx;
+
 namespace wgpt {
+
+// The images of a context (for the learned denoiser, which reads the accumulation and the
+// G-buffer and writes the rgba8 image).
+struct CtxImages {
+  int device;
+  uint32_t w, h;
+  float* accum;
+  float* gbuf;
+  uint8_t* out;
+  cudaStream_t stream;
+};
+bool ctx_images(::wgpt_ctx* ctx, CtxImages* out);
 
 // Device copies of the scene buffers, in the reference's packed layouts.
 struct DeviceScene {

@@ -1,0 +1,170 @@
+"""Learned kernel-predicting denoiser (host side of wgpt_kpcn_*).
+
+The network runs and trains on the GPU through the C ABI; this module holds its layer table
+(mirroring kpcn.cu, for tools that read the flat parameter array), the training-example
+generator that renders (noisy, G-buffer, target) triples with the path tracer itself, and the
+image metrics used to compare it with the a-trous filter.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import renderer as rd
+from . import scene as sc
+from ._lib import WgptError, lib, ptr
+
+
+@dataclass(frozen=True)
+class LayerSpec:
+    name: str
+    cu: int        # upsampled coarse input channels (padded)
+    cs: int        # same-resolution input channels (padded)
+    cout: int      # output channels (padded)
+    taps: int      # 9 (3x3) or 1
+    relu: bool
+    level: int     # resolution level of the output (0 = full)
+
+    @property
+    def cin(self) -> int:
+        return self.cu + self.cs
+
+    @property
+    def n_weights(self) -> int:
+        return self.cout * self.taps * self.cin
+
+
+LAYERS = (
+    LayerSpec("E0a", 0, 16, 32, 9, True, 0),
+    LayerSpec("E0", 0, 32, 32, 9, True, 0),
+    LayerSpec("E1", 0, 32, 48, 9, True, 1),
+    LayerSpec("E2", 0, 48, 64, 9, True, 2),
+    LayerSpec("E3", 0, 64, 96, 9, True, 3),
+    LayerSpec("E4a", 0, 96, 128, 9, True, 4),
+    LayerSpec("E4", 0, 128, 128, 9, True, 4),
+    LayerSpec("D3", 128, 96, 96, 9, True, 3),
+    LayerSpec("D2", 96, 64, 64, 9, True, 2),
+    LayerSpec("D1", 64, 48, 48, 9, True, 1),
+    LayerSpec("D0", 48, 32, 32, 9, True, 0),
+    LayerSpec("OUT", 0, 32, 32, 1, False, 0),
+)
+
+
+def param_slices() -> dict[str, tuple[slice, slice]]:
+    """Per layer: (weights, bias) slices of the flat parameter array."""
+    out, off = {}, 0
+    for l in LAYERS:
+        w = slice(off, off + l.n_weights)
+        off += l.n_weights
+        b = slice(off, off + l.cout)
+        off += l.cout
+        out[l.name] = (w, b)
+    return out
+
+
+N_PARAMS = sum(l.n_weights + l.cout for l in LAYERS)
+
+
+class Kpcn:
+    """wgpt_kpcn_* through ctypes."""
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        self.L = lib()
+        h = C.c_void_p()
+        rc = self.L.wgpt_kpcn_create(device, seed, C.byref(h))
+        if rc != 0:
+            raise WgptError(rc, "wgpt_kpcn_create")
+        self.h = h.value
+        n = C.c_uint64()
+        self._check(self.L.wgpt_kpcn_num_params(self.h, C.byref(n)), "num_params")
+        self.n_params = int(n.value)
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = self.L.wgpt_kpcn_last_error(self.h) if getattr(self, "h", None) else b""
+            raise WgptError(rc, what, (msg or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.wgpt_kpcn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self) -> np.ndarray:
+        a = np.empty(self.n_params, np.float32)
+        self._check(self.L.wgpt_kpcn_get_params(self.h, ptr(a)), "get_params")
+        return a
+
+    def set_params(self, a: np.ndarray):
+        a = np.ascontiguousarray(a, np.float32)
+        assert a.size == self.n_params
+        self._check(self.L.wgpt_kpcn_set_params(self.h, ptr(a)), "set_params")
+
+    def add_example(self, noisy: np.ndarray, gbuf: np.ndarray, target: np.ndarray):
+        h, w = noisy.shape[:2]
+        noisy = np.ascontiguousarray(noisy, np.float32)
+        gbuf = np.ascontiguousarray(gbuf, np.float32)
+        target = np.ascontiguousarray(target, np.float32)
+        assert noisy.shape == (h, w, 4) and target.shape == (h, w, 4) and gbuf.shape == (h, w, 12)
+        self._check(self.L.wgpt_kpcn_add_example(self.h, ptr(noisy), ptr(gbuf), ptr(target), w, h), "add_example")
+
+    def train(self, steps: int, batch: int = 8, crop: int = 64, lr: float = 1e-3, seed: int = 1) -> np.ndarray:
+        losses = np.zeros(steps, np.float32)
+        self._check(self.L.wgpt_kpcn_train(self.h, steps, batch, crop, lr, seed, ptr(losses)), "train")
+        return losses
+
+    def loss_and_grads(self, noisy, gbuf, target):
+        h, w = noisy.shape[:2]
+        noisy = np.ascontiguousarray(noisy, np.float32)
+        gbuf = np.ascontiguousarray(gbuf, np.float32)
+        target = np.ascontiguousarray(target, np.float32)
+        loss = np.zeros(1, np.float32)
+        grads = np.zeros(self.n_params, np.float32)
+        out = np.zeros((h, w, 4), np.float32)
+        self._check(self.L.wgpt_kpcn_loss_and_grads(self.h, ptr(noisy), ptr(gbuf), ptr(target), w, h, ptr(loss),
+                                                    ptr(grads), ptr(out)), "loss_and_grads")
+        return float(loss[0]), grads, out
+
+    def denoise(self, r: rd.Renderer, exposure: float = 1.0, want_linear: bool = True):
+        """Filters the renderer's accumulation with its G-buffer into its rgba8 image."""
+        lin = np.zeros((r.height, r.width, 4), np.float32) if want_linear else None
+        self._check(self.L.wgpt_kpcn_denoise(self.h, r.ctx, exposure, ptr(lin) if want_linear else None), "denoise")
+        return lin
+
+
+def render_example(scene: sc.Scene, size: int, spp: int, target_spp: int, seed: int = 1, target_seed: int = 977):
+    """(noisy accumulation at `spp`, G-buffer, target accumulation at `target_spp`) of one view,
+    rendered by the path tracer; the target uses an independent sample stream."""
+    scene.camera.aspect = 1.0
+    r = rd.Renderer(size, size, seed_fn=lambda: seed)
+    r.set_scene(scene, isgbuf=True)
+    r.render_gbuffer()
+    gbuf = r.read_gbuffer()
+    r.reset()
+    r.render(tsize=size, reps=spp)
+    noisy = r.read_accum()
+    r.close()
+    t = rd.Renderer(size, size, seed_fn=lambda: target_seed)
+    t.set_scene(scene)
+    t.render(tsize=size, reps=target_spp)
+    target = t.read_accum()
+    t.close()
+    return noisy, gbuf, target
+
+
+def tonemap(c: np.ndarray, exposure: float = 1.0) -> np.ndarray:
+    """The accumulation pass's display transform (shader.wgsl:2487-2490) in float64."""
+    x = np.maximum(np.asarray(c, np.float64)[..., :3], 0.0) * exposure
+    return np.power(x / (x + 0.3), 0.4545)
+
+
+def rmse(a: np.ndarray, b: np.ndarray, exposure: float = 1.0) -> float:
+    """RMSE between two linear images in display space (tonemapped, [0, 1])."""
+    return float(np.sqrt(np.mean((tonemap(a, exposure) - tonemap(b, exposure)) ** 2)))

@@ -255,6 +255,145 @@ def stage_report(r, rd, launch_once, stream, flush, paths_per_step: int, mega: b
             "avg_launch_s": avg_launch_s, "dom": dom, "cnt": cnt, "launches": int(stage_launches.sum())}
 
 
+def time_to_rmse(args) -> dict:
+    """Time to display-space RMSE <= threshold against a converged FP64 reference, at 1920x1080
+    on a held-out scene of the small-configuration family (4 bounces): plain accumulation plus
+    the a-trous filter against accumulation plus the learned denoiser.  The network is trained
+    here, on the GPU, from pairs this tracer renders (scenes seeded 1000.., 256x256, inputs at
+    1/2/4/8 spp, targets at --kpcn-target-spp)."""
+    import torch
+    from webgpuraytracer_b200 import kpcn
+    from webgpuraytracer_b200 import renderer as rd
+    from webgpuraytracer_b200 import synth
+    W, H, thr = 1920, 1080, args.rmse_threshold
+    out = {"threshold": thr, "space": "display (shader.wgsl tonemap, exposure 1)",
+           "scene": "small-configuration family, seed 1 (held out), 1920x1080, 4 bounces",
+           "reference": f"{args.ref_spp} spp, FP64 Welford accumulation"}
+    t0 = time.perf_counter()
+    k = kpcn.Kpcn(0, seed=1)
+    n_ex = kpcn.build_training_set(k, range(1000, 1000 + args.kpcn_scenes), 256, (1, 2, 4, 8), args.kpcn_target_spp)
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    losses = k.train(args.kpcn_steps, batch=16, crop=128, lr=1e-3, seed=1)
+    t_train = time.perf_counter() - t0
+    out["training"] = {"scenes": args.kpcn_scenes, "examples": n_ex, "target_spp": args.kpcn_target_spp,
+                       "steps": args.kpcn_steps, "batch": "16 x 128^2 crops", "data_s": t_data, "train_s": t_train,
+                       "loss_first_50": float(np.mean(losses[:50])), "loss_last_50": float(np.mean(losses[-50:])),
+                       "params": k.n_params}
+    scene = synth.small_scene(1, W, H, 4)
+    scene.camera.aspect = W / H
+    ref_r = rd.Renderer(W, H, seed_fn=lambda: 4242)
+    ref_r.set_scene(scene)
+    ref_r.set_accum_f64(True)
+    done = 0
+    t0 = time.perf_counter()
+    while done < args.ref_spp:
+        n = min(4096, args.ref_spp - done)
+        ref_r.render(tsize=W, reps=n)
+        done += n
+    ref, _, _ = ref_r.read_accum_f64()
+    out["reference_s"] = time.perf_counter() - t0
+    ref_r.close()
+    ref_disp = kpcn.tonemap(ref)
+
+    def disp_rmse(d):
+        return float(np.sqrt(np.mean((np.clip(d[..., :3], 0.0, 1.0) - ref_disp) ** 2)))
+
+    ev = rd.Renderer(W, H, seed_fn=lambda: 7)
+    ev.set_scene(scene, isgbuf=True)
+    ev.render_gbuffer()
+    ev.reset()
+    atrous = rd.Denoiser(ev, passes=5)
+    sweep, done, spp = [], 0, 1
+    while spp <= args.max_spp:
+        ev.render(tsize=W, reps=spp - done)
+        done = spp
+        e_raw = kpcn.rmse(ev.read_accum(), ref)
+        atrous.execute()
+        e_at = disp_rmse(atrous.read()[1])
+        e_nn = kpcn.rmse(k.denoise(ev), ref)
+        sweep.append({"spp": spp, "accum": e_raw, "atrous": e_at, "kpcn": e_nn})
+        if min(e_raw, e_at) <= thr and e_nn <= thr:
+            break
+        spp *= 2
+    ev.close()
+    out["sweep"] = sweep
+
+    def first(key_fn):
+        for row in sweep:
+            if key_fn(row) <= thr:
+                return row["spp"]
+        return None
+
+    s_plain = first(lambda r_: min(r_["accum"], r_["atrous"]))
+    s_nn = first(lambda r_: r_["kpcn"])
+
+    def timed(spp_, filt):
+        """Device time of rendering spp_ samples from scratch and filtering once."""
+        r_ = rd.Renderer(W, H, seed_fn=lambda: 7)
+        r_.set_scene(scene, isgbuf=True)
+        r_.render_gbuffer()
+        r_.reset()
+        st = torch.cuda.ExternalStream(r_.stream_handle())
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(st)
+        r_.render(tsize=W, reps=spp_, sync=False)
+        e1.record(st)
+        if filt == "atrous":
+            rd.Denoiser(r_, passes=5).execute()
+        elif filt == "kpcn":
+            k.denoise(r_, want_linear=False)
+        e2.record(st)
+        r_.synchronize()
+        torch.cuda.synchronize()
+        r_.close()
+        return e0.elapsed_time(e1), e1.elapsed_time(e2)
+
+    def arm(s_, filt_best):
+        if s_ is None:
+            last = sweep[-1]
+            s_est = last["spp"] * (last["accum"] / thr) ** 2
+            r_ms, _ = timed(last["spp"], "none")
+            return {"spp": None, "spp_extrapolated": s_est, "ms": r_ms * s_est / last["spp"],
+                    "method": "accumulation (1/sqrt(spp) extrapolation of the last sweep point)"}
+        r_ms, f_ms = timed(s_, filt_best)
+        return {"spp": s_, "ms": r_ms + f_ms, "render_ms": r_ms, "filter_ms": f_ms, "method": filt_best}
+
+    row_p = next((r_ for r_ in sweep if r_["spp"] == s_plain), None)
+    plain_filter = "atrous" if row_p is not None and row_p["atrous"] <= row_p["accum"] else "none"
+    out["plain"] = arm(s_plain, plain_filter)
+    out["neural"] = arm(s_nn, "kpcn")
+    if out["plain"]["ms"] and out["neural"]["ms"]:
+        out["plain_over_neural"] = out["plain"]["ms"] / out["neural"]["ms"]
+    # inference throughput at 1080p on the tensor cores
+    r_ = rd.Renderer(W, H, seed_fn=lambda: 7)
+    r_.set_scene(scene, isgbuf=True)
+    r_.render_gbuffer()
+    r_.reset()
+    r_.render(tsize=W, reps=1)
+    st = torch.cuda.ExternalStream(r_.stream_handle())
+    for _ in range(3):
+        k.denoise(r_, want_linear=False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    reps = 10
+    for _ in range(reps):
+        k.denoise(r_, want_linear=False)
+    e1.record(st)
+    r_.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    flops = kpcn.gemm_flops(W, H)
+    peaks, kind = load_peaks()
+    tf = flops / (ms / 1e3) / 1e12
+    out["kpcn_inference_1080p"] = {"ms": ms, "gemm_tflops": tf, "gemm_flops": flops,
+                                   "frac_of_bf16_peak": tf / peaks["bf16_tflops"] if "bf16_tflops" in peaks else None,
+                                   "peak_source": f"{kind} MEASURED_PEAKS.json bf16_tflops"}
+    r_.close()
+    k.close()
+    return out
+
+
 def run_ours(args):
     rank, world, local = dist_setup(args.gpus)
     import torch
@@ -333,6 +472,9 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, sample = cpu_sample(scene, packed, 1, args.cpu_seconds, 8)
         cpu = {"value": v, "unit": "paths/s", "cores": cores, "kind": "port", "sample": sample}
+    ttr = None
+    if rank == 0 and world == 1 and not args.no_rmse and not mega:
+        ttr = time_to_rmse(args)
 
     if rank == 0:
         line = {
@@ -365,6 +507,8 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if ttr:
+            line["time_to_rmse"] = ttr
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:
@@ -485,6 +629,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", choices=["wavefront", "megakernel"], default="wavefront")
     ap.add_argument("--pool", type=int, default=0, help="wavefront path slots (0: library default)")
+    ap.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE measurement")
+    ap.add_argument("--rmse-threshold", type=float, default=0.01)
+    ap.add_argument("--ref-spp", type=int, default=65536, help="samples of the FP64 reference image")
+    ap.add_argument("--max-spp", type=int, default=4096, help="largest sample count of the RMSE sweep")
+    ap.add_argument("--kpcn-scenes", type=int, default=128)
+    ap.add_argument("--kpcn-target-spp", type=int, default=1024)
+    ap.add_argument("--kpcn-steps", type=int, default=2000)
     ap.add_argument("--workload", choices=["flagship", "batch"], default="flagship",
                     help="flagship: 1080p 64 spp; batch: 32 uneven views of the 5.24 M-triangle scene")
     args = ap.parse_args()

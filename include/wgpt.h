@@ -100,6 +100,14 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sec
 enum { WGPT_MODE_WAVEFRONT = 0, WGPT_MODE_MEGAKERNEL = 1 };
 int wgpt_set_render_mode(wgpt_ctx* ctx, int mode);
 
+/* FP64 accumulation (no counterpart in the reference): with it on, the wavefront mode also
+   folds every sample, in sample order, into a per-pixel FP64 Welford record of 8 doubles
+   (mean r, g, b; sum of squared deviations r, g, b; sample count; unused) alongside the FP32
+   running mean; cleared when switched on and by wgpt_resize.  Used for converged reference
+   images and per-pixel confidence intervals.  The megakernel mode rejects it. */
+int wgpt_set_accum_f64(wgpt_ctx* ctx, int on);
+int wgpt_read_accum_f64(wgpt_ctx* ctx, double* dst_8_per_px);
+
 /* Wavefront sizing (no counterpart in the reference, whose dispatch has no path pool):
    pool_paths path slots (1,024 .. 67,108,864; default 2,097,152; about 420 bytes each) and at
    most units_per_pass samples held (65,536 .. 2^30; default 2^27; 16 bytes each) before they are

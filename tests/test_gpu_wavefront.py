@@ -138,3 +138,32 @@ def test_wavefront_config_rejects_out_of_range():
     r.set_wavefront_config(4096, 0)
     assert r.wavefront_config()[0] == 4096
     r.close()
+
+
+def test_fp64_accumulation_and_3_sigma_agreement_with_oracle():
+    """The FP64 Welford record holds the same samples as the FP32 running mean; a 4096-spp GPU
+    estimate and an independent 256-spp oracle estimate agree within 3 sigma per pixel."""
+    s = synth.small_scene(1, 256, 256, 4)
+    packed = sc.pack_scene_data(s)
+    sec = (112, 96, 32, 32)
+    r = rd.Renderer(256, 256, seed_fn=lambda: 5)
+    r.set_scene(s, packed=packed)
+    r.set_accum_f64(True)
+    for f0 in range(0, 4096, 1024):
+        p = _params(s, packed, 256, 256, frame=f0, seed=5, section=sec[:2])
+        r._check(r.L.wgpt_set_params(r.ctx, rd.ptr(p)), "params")
+        r._check(r.L.wgpt_render(r.ctx, f0, 1024, *sec), "render")
+    r.synchronize()
+    mean, var, n = r.read_accum_f64()
+    acc = r.read_accum()
+    ys, xs = slice(96, 128), slice(112, 144)
+    assert np.all(n[ys, xs] == 4096) and np.all(n[:96] == 0)
+    np.testing.assert_allclose(mean[ys, xs], acc[ys, xs, :3], rtol=2e-3, atol=1e-5)
+    po = _params(s, packed, 256, 256, seed=99, section=sec[:2])
+    acc_o, _ = _oracle(packed, po, 256, 256, 0, 256, sec)
+    mo = acc_o[ys, xs, :3].astype(np.float64)
+    sigma = np.sqrt(var[ys, xs] / 4096.0 + var[ys, xs] / 256.0)
+    inside = np.abs(mean[ys, xs] - mo) <= 3.0 * sigma + 1e-9
+    frac = float(inside.mean())
+    assert frac >= 0.98, f"only {frac:.4f} of pixel channels within 3 sigma"
+    r.close()

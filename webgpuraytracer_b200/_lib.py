@@ -85,6 +85,8 @@ EXPORTS = {
     "wgpt_set_render_mode": ([_P, C.c_int], C.c_int),
     "wgpt_set_wavefront_config": ([_P, C.c_uint32, C.c_uint64], C.c_int),
     "wgpt_set_views": ([_P, C.c_uint32, _P, _P], C.c_int),
+    "wgpt_set_accum_f64": ([_P, C.c_int], C.c_int),
+    "wgpt_read_accum_f64": ([_P, _P], C.c_int),
     "wgpt_gemm_bf16": ([C.c_int, _P, _P, _P, C.c_int, C.c_int, C.c_int], C.c_int),
     "wgpt_kpcn_create": ([C.c_int, C.c_uint64, C.POINTER(_P)], C.c_int),
     "wgpt_kpcn_destroy": ([_P], C.c_int),

@@ -55,6 +55,7 @@ struct wgpt_ctx {
   // batched views: size and images of each
   struct View { uint32_t w, h; float* accum; uint8_t* out; };
   std::vector<View> views;
+  double* acc64 = nullptr;        // optional FP64 Welford accumulation (8 doubles per pixel)
 };
 
 namespace {
@@ -417,6 +418,7 @@ int wgpt_destroy(wgpt_ctx* ctx) {
   dfree_t(ctx->dn_a); dfree_t(ctx->dn_b); dfree_t(ctx->dn_guide); dfree_t(ctx->dn_comp);
   dfree_t(ctx->canvas); dfree_t(ctx->d_status); dfree_t(ctx->d_counters); wgpt::wf_engine_destroy(ctx->wf);
   ctx->wf = nullptr;
+  dfree_t(ctx->acc64);
   dfree(ctx->d_pairs_tlas); dfree(ctx->d_pairs_bvh);
   for (auto& v : ctx->views) { dfree_t(v.accum); dfree_t(v.out); }
   if (ctx->timer) {
@@ -484,7 +486,9 @@ int wgpt_resize(wgpt_ctx* ctx, uint32_t width, uint32_t height, int want_gbuf) {
   CK(cudaStreamSynchronize(ctx->stream), "drain before resize");
   size_t npix = (size_t)width * height;
   bool same = width == ctx->w && height == ctx->h;
+  const bool had_f64 = ctx->acc64 != nullptr;
   if (!same) {
+    dfree_t(ctx->acc64);
     dfree_t(ctx->accum); dfree_t(ctx->out); dfree_t(ctx->gbuf);
     dfree_t(ctx->dn_a); dfree_t(ctx->dn_b); dfree_t(ctx->dn_guide); dfree_t(ctx->dn_comp);
     ctx->dn_final = nullptr;
@@ -496,6 +500,8 @@ int wgpt_resize(wgpt_ctx* ctx, uint32_t width, uint32_t height, int want_gbuf) {
   CK(cudaMemsetAsync(ctx->accum, 0, npix * 16, ctx->stream), "clear accum");
   CK(cudaMemsetAsync(ctx->out, 0, npix * 4, ctx->stream), "clear output");
   if (want_gbuf) CK(cudaMemsetAsync(ctx->gbuf, 0, npix * 48, ctx->stream), "clear gbuffer");
+  if (had_f64 && !ctx->acc64) CK(cudaMalloc(&ctx->acc64, npix * 64), "cudaMalloc FP64 accumulation");
+  if (ctx->acc64) CK(cudaMemsetAsync(ctx->acc64, 0, npix * 64, ctx->stream), "clear FP64 accumulation");
   ctx->w = width; ctx->h = height;
   CK(cudaStreamSynchronize(ctx->stream), "resize");
   return WGPT_OK;
@@ -520,6 +526,7 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
   unsigned long long* cnt = ctx->counting ? ctx->d_counters : nullptr;
   wgpt::StageTimer* tm = ctx->timing ? ctx->timer : nullptr;
   if (ctx->mode == WGPT_MODE_MEGAKERNEL) {
+    if (ctx->acc64) return fail(ctx, WGPT_E_UNSUPPORTED, "FP64 accumulation needs the wavefront mode");
     if (tm) tm->begin(0, ctx->stream);
     CK(wgpt::launch_render(ctx->ds, ctx->params, first_frame, reps, sx, sy, sw, sh, ctx->accum, ctx->out, ctx->w,
                            ctx->d_status, cnt, ctx->stream),
@@ -536,6 +543,7 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
   v.accum = ctx->accum;
   v.out = ctx->out;
   v.out_pitch = ctx->w;
+  v.acc64 = ctx->acc64;
   CK(wgpt::wf_render(ctx->wf, ctx->ds, ctx->d_pairs_tlas, ctx->d_pairs_bvh, &v, 1, ctx->d_status, cnt, ctx->stream,
                      tm),
      "wavefront render");
@@ -774,6 +782,25 @@ int wgpt_read_view(wgpt_ctx* ctx, uint32_t view, float* accum, uint8_t* out) {
   if (accum) CK(cudaMemcpy(accum, v.accum, np * 16, cudaMemcpyDeviceToHost), "read view accumulation");
   if (out) CK(cudaMemcpy(out, v.out, np * 4, cudaMemcpyDeviceToHost), "read view image");
   return WGPT_OK;
+}
+
+int wgpt_set_accum_f64(wgpt_ctx* ctx, int on) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (ctx->w == 0) return fail(ctx, WGPT_E_STATE, "no image size: call wgpt_resize first");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "drain");
+  dfree_t(ctx->acc64);
+  if (on) {
+    size_t bytes = (size_t)ctx->w * ctx->h * 64;
+    CK(cudaMalloc(&ctx->acc64, bytes), "cudaMalloc FP64 accumulation");
+    CK(cudaMemsetAsync(ctx->acc64, 0, bytes, ctx->stream), "clear FP64 accumulation");
+  }
+  return WGPT_OK;
+}
+
+int wgpt_read_accum_f64(wgpt_ctx* ctx, double* dst) {
+  if (!ctx) return WGPT_E_INVALID;
+  return readback(ctx, dst, ctx->acc64, (size_t)ctx->w * ctx->h * 64, "read FP64 accumulation");
 }
 
 int wgpt_set_wavefront_config(wgpt_ctx* ctx, uint32_t pool_paths, uint64_t units_per_pass) {

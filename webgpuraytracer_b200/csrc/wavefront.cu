@@ -77,6 +77,8 @@ struct WfView {
   uint32_t job;           // index of the view in the caller's list (completion tracking)
   float4* accum;
   uchar4* out;
+  double* acc64;          // optional FP64 Welford records (8 doubles per pixel)
+  uint64_t pad2;
 };
 
 // Device control block of a pass.
@@ -810,6 +812,19 @@ __global__ void __launch_bounds__(256) k_wf_accumulate(WfArgs a) {
       acc = vmix(acc, mk3(L.x, L.y, L.z), weight);
     }
     v->accum[idx] = make_float4(acc.x, acc.y, acc.z, 1.0f);
+    if (v->acc64) {
+      // the same samples, in the same order, into an FP64 mean and sum of squared deviations
+      double* r = v->acc64 + idx * 8;
+      double m0 = r[0], m1 = r[1], m2 = r[2], q0 = r[3], q1 = r[4], q2 = r[5], cnt = r[6];
+      for (uint32_t k = 0; k < v->spp; ++k) {
+        float4 L = smp[(size_t)k * v->npix];
+        cnt += 1.0;
+        double d0 = (double)L.x - m0, d1 = (double)L.y - m1, d2 = (double)L.z - m2;
+        m0 += d0 / cnt; m1 += d1 / cnt; m2 += d2 / cnt;
+        q0 += d0 * ((double)L.x - m0); q1 += d1 * ((double)L.y - m1); q2 += d2 * ((double)L.z - m2);
+      }
+      r[0] = m0; r[1] = m1; r[2] = m2; r[3] = q0; r[4] = q1; r[5] = q2; r[6] = cnt;
+    }
     v3 c = acc * mk3s(v->p.exposure);
     c = c / (c + mk3s(0.3f));
     c = vpow(c, 0.4545f);
@@ -1151,6 +1166,7 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
       w.out_pitch = jv[v].out_pitch;
       w.accum = (float4*)jv[v].accum;
       w.out = (uchar4*)jv[v].out;
+      w.acc64 = jv[v].acc64;
       w.job = v;
       hv.push_back(w);
       units += (uint64_t)npix * take[v];

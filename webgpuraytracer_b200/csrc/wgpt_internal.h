@@ -72,6 +72,7 @@ struct WfJobView {
   float* accum;          // float4 per pixel, row pitch q.width
   uint8_t* out;          // rgba8, row pitch out_pitch
   uint32_t out_pitch;
+  double* acc64 = nullptr;   // optional FP64 Welford record per pixel (mean.rgb, m2.rgb, n, -), row pitch q.width
 };
 struct WfEngine;
 WfEngine* wf_engine_create();

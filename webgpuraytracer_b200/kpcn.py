@@ -168,3 +168,42 @@ def tonemap(c: np.ndarray, exposure: float = 1.0) -> np.ndarray:
 def rmse(a: np.ndarray, b: np.ndarray, exposure: float = 1.0) -> float:
     """RMSE between two linear images in display space (tonemapped, [0, 1])."""
     return float(np.sqrt(np.mean((tonemap(a, exposure) - tonemap(b, exposure)) ** 2)))
+
+
+def build_training_set(k: Kpcn, seeds, size: int = 256, spps=(1, 2, 4, 8), target_spp: int = 1024,
+                       bounces: int = 4) -> int:
+    """Adds, for every seeded scene of the small-configuration family, one example per input
+    sample count: (progressive accumulation at that count, G-buffer, target at target_spp with
+    an independent sample stream).  Returns the number of examples added."""
+    from . import synth
+    n = 0
+    for seed in seeds:
+        s = synth.small_scene(int(seed), size, size, bounces)
+        s.camera.aspect = 1.0
+        t = rd.Renderer(size, size, seed_fn=lambda: 100_000 + int(seed))
+        t.set_scene(s)
+        t.render(tsize=size, reps=target_spp)
+        target = t.read_accum()
+        t.close()
+        r = rd.Renderer(size, size, seed_fn=lambda: int(seed))
+        r.set_scene(s, isgbuf=True)
+        r.render_gbuffer()
+        gbuf = r.read_gbuffer()
+        r.reset()
+        done = 0
+        for spp in spps:
+            r.render(tsize=size, reps=spp - done)
+            done = spp
+            k.add_example(r.read_accum(), gbuf, target)
+            n += 1
+        r.close()
+    return n
+
+
+def gemm_flops(width: int, height: int) -> int:
+    """Tensor-core FLOPs of one inference at width x height (padded channel counts, as executed)."""
+    h, w = [height], [width]
+    for _ in range(4):
+        h.append((h[-1] + 1) // 2)
+        w.append((w[-1] + 1) // 2)
+    return sum(2 * h[l.level] * w[l.level] * l.cout * l.taps * l.cin for l in LAYERS)

@@ -198,6 +198,18 @@ class Renderer:
                     "trace_rays")
         return o, m, p, t, nn
 
+    def set_accum_f64(self, on: bool = True):
+        """FP64 Welford accumulation of every sample next to the FP32 running mean."""
+        self._check(self.L.wgpt_set_accum_f64(self.ctx, 1 if on else 0), "set_accum_f64")
+
+    def read_accum_f64(self):
+        """(mean (H, W, 3), per-sample variance (H, W, 3), sample count (H, W)) in float64."""
+        a = np.empty((self.height, self.width, 8), np.float64)
+        self._check(self.L.wgpt_read_accum_f64(self.ctx, ptr(a)), "read_accum_f64")
+        n = a[..., 6]
+        var = a[..., 3:6] / np.maximum(n - 1.0, 1.0)[..., None]
+        return a[..., 0:3], var, n
+
     def set_render_mode(self, mode: int):
         """MODE_WAVEFRONT (path pool with regeneration) or MODE_MEGAKERNEL (one thread per pixel)."""
         self._check(self.L.wgpt_set_render_mode(self.ctx, int(mode)), "set_render_mode")

@@ -164,7 +164,8 @@ int wgpt_gemm_bf16(int device, const uint16_t* a, const uint16_t* b, float* c, i
 /* Learned kernel-predicting denoiser (no counterpart in the reference, whose only denoiser is
    the a-trous filter, which stays the fallback).  A 5-level encoder-decoder (32/48/64/96/128
    channels, ~0.73 M parameters) over 10 features of the accumulation and G-buffer (log colour,
-   albedo, normal, depth) predicts a 5x5 filter per pixel, applied to the noisy colour.  BF16
+   albedo, normal, depth) predicts three 5x5 filters per pixel, applied to the noisy colour as
+   a cascade at dilations 1, 2 and 4 (29 x 29 footprint).  BF16
    weights and activations, FP32 accumulation on the tensor cores, FP32 master weights trained
    by Adam on the relative L2 loss sum((f-t)^2/(t^2+0.01))/(3 pixels).  Parameters are one flat
    FP32 array, per layer W[cout][taps][cin] then bias[cout] (layer table in kpcn.cu).

@@ -4,9 +4,10 @@ loss and gradients, used only by tests to check the tensor-core kernels.
 It follows kpcn.cu's definition layer by layer: features (log1p colour, albedo, normal,
 depth/(depth+3), zero-padded to 16 channels), 3x3 convolutions with zero padding, 2x2 average
 pooling whose mean leaves out children beyond an odd edge, nearest 2x upsampling cropped to the
-skip tensor's size, [upsampled, skip] concatenation, a 1x1 output convolution whose first 25
-channels are softmax-normalised into a 5x5 filter applied with clamp-to-edge to the noisy colour,
-and the relative L2 loss sum((f - t)^2 / (t^2 + 0.01)) / (3 pixels).  Parameters use the flat
+skip tensor's size, [upsampled, skip] concatenation, a 1x1 output convolution whose channels
+[25s, 25s + 25) are softmax-normalised into the 5x5 filter of stage s, the three stages applied
+in turn at dilations 1, 2, 4 with clamp-to-edge neighbours, starting from the noisy colour, and
+the relative L2 loss sum((f - t)^2 / (t^2 + 0.01)) / (3 pixels).  Parameters use the flat
 layout of wgpt_kpcn_get_params (per layer W[cout][ky*3+kx][cin], then bias).  Inputs and
 weights can be rounded to bfloat16 first, as the GPU stores them.
 """
@@ -84,15 +85,17 @@ def forward_loss(params: np.ndarray, noisy: np.ndarray, gbuf: np.ndarray, target
     d2 = conv("D2", torch.cat([up(d3, e2), e2], 1))
     d1 = conv("D1", torch.cat([up(d2, e1), e1], 1))
     d0 = conv("D0", torch.cat([up(d1, e0), e0], 1))
-    logits = conv("OUT", d0, relu=False)[0, :25]            # (25, H, W)
-    wk = torch.softmax(logits, 0)
-    col = t(noisy[..., :3]).permute(2, 0, 1)[None]
-    colp = F.pad(col, (2, 2, 2, 2), mode="replicate")[0]     # (3, H+4, W+4)
+    logits = conv("OUT", d0, relu=False)[0]                  # (80, H, W)
     h, w = noisy.shape[:2]
-    f = torch.zeros(3, h, w, dtype=torch.float64)
-    for k in range(25):
-        dy, dx = k // 5, k % 5
-        f = f + wk[k][None] * colp[:, dy:dy + h, dx:dx + w]
+    f = t(noisy[..., :3]).permute(2, 0, 1)                     # (3, H, W)
+    for stage, d in enumerate((1, 2, 4)):
+        wk = torch.softmax(logits[25 * stage:25 * stage + 25], 0)
+        fp = F.pad(f[None], (2 * d, 2 * d, 2 * d, 2 * d), mode="replicate")[0]
+        g = torch.zeros(3, h, w, dtype=torch.float64)
+        for k in range(25):
+            oy, ox = 2 * d + d * (k // 5 - 2), 2 * d + d * (k % 5 - 2)
+            g = g + wk[k][None] * fp[:, oy:oy + h, ox:ox + w]
+        f = g
     tg = t(target[..., :3]).permute(2, 0, 1)
     loss = ((f - tg) ** 2 / (tg ** 2 + 0.01)).sum() / (3.0 * h * w)
     return loss, f.permute(1, 2, 0), P

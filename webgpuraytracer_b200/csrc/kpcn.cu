@@ -85,7 +85,8 @@ extern "C" int wgpt_gemm_bf16(int device, const uint16_t* a, const uint16_t* b, 
 // Kernel-predicting convolutional denoiser (KPCN).
 //
 // A 5-level encoder-decoder over 10 input features (log colour, albedo, normal, depth) predicts
-// per pixel a 5x5 filter (softmax over 25 logits) that is applied to the noisy linear colour.
+// per pixel three 5x5 filters (softmax over 25 logits each) applied to the noisy linear colour
+// as a cascade at dilations 1, 2 and 4.
 // Activations are NHWC BF16 with channel counts padded to multiples of 16; every convolution
 // (forward, data gradient, weight gradient) is one tensor-core GEMM whose loaders gather the
 // implicit im2col operand straight from the NHWC tensors (2x nearest upsampling and the skip
@@ -96,7 +97,7 @@ extern "C" int wgpt_gemm_bf16(int device, const uint16_t* a, const uint16_t* b, 
 //   E0a 10(16)->32 L0   E0 32->32 L0   E1 32->48 L1   E2 48->64 L2   E3 64->96 L3
 //   E4a 96->128 L4      E4 128->128 L4
 //   D3 [up E4 128, E3 96]->96 L3   D2 [up D3 96, E2 64]->64 L2   D1 [up D2 64, E1 48]->48 L1
-//   D0 [up D1 48, E0 32]->32 L0    OUT 1x1 32->25(32) L0
+//   D0 [up D1 48, E0 32]->32 L0    OUT 1x1 32->75(80) L0
 // with 2x2 average pooling between encoder levels (E0->P1, E1->P2, E2->P3, E3->P4).
 // ============================================================================================
 #include <algorithm>
@@ -347,56 +348,85 @@ __global__ void k_avgpool(const uint16_t* __restrict__ in, uint16_t* __restrict_
   }
 }
 
-// Softmax over the 25 logits, 5x5 filter (clamp-to-edge) applied to the noisy colour; with a
-// target also the relative-L2 loss sum((f-t)^2 / (t^2 + 0.01)) / (3 P) and its logit gradient.
-__global__ void k_apply(const float* __restrict__ logits, const float4* __restrict__ col, int B, int h, int w,
-                        float4* __restrict__ out, const float4* __restrict__ tgt, uint16_t* __restrict__ dlogits,
-                        float* __restrict__ loss) {
+// The predicted filters: three 5x5 kernels per pixel (softmax over logits [25s, 25s + 25) of the
+// 80-channel logit tensor) applied as a cascade at dilations 1, 2 and 4 -- f1 = K1 * colour,
+// f2 = K2 (dilated 2) * f1, f3 = K3 (dilated 4) * f2 -- with clamp-to-edge neighbours, so the
+// footprint grows to 29 x 29 pixels while every kernel stays 5 x 5.
+constexpr int LOGITS = 80;
+
+__device__ __forceinline__ void softmax25(const float* lg, float (&wk)[25]) {
+  float mx = lg[0];
+  for (int k = 1; k < 25; ++k) mx = fmaxf(mx, lg[k]);
+  float sum = 0.0f;
+  for (int k = 0; k < 25; ++k) { wk[k] = __expf(lg[k] - mx); sum += wk[k]; }
+  const float inv = 1.0f / sum;
+  for (int k = 0; k < 25; ++k) wk[k] *= inv;
+}
+
+__device__ __forceinline__ size_t tap_index(int b, int y, int x, int k, int d, int h, int w) {
+  int yy = min(max(y + d * (k / 5 - 2), 0), h - 1), xx = min(max(x + d * (k % 5 - 2), 0), w - 1);
+  return ((size_t)b * h + yy) * w + xx;
+}
+
+__global__ void k_filter_fwd(const float* __restrict__ logits, int stage, int d, const float4* __restrict__ in,
+                             float4* __restrict__ out, int B, int h, int w) {
   const int P = B * h * w;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
+    float wk[25];
+    softmax25(logits + (size_t)p * LOGITS + stage * 25, wk);
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    for (int k = 0; k < 25; ++k) {
+      float4 c = in[tap_index(b, y, x, k, d, h, w)];
+      fx += wk[k] * c.x; fy += wk[k] * c.y; fz += wk[k] * c.z;
+    }
+    out[p] = make_float4(fx, fy, fz, 1.0f);
+  }
+}
+
+// Relative L2 loss sum((f-t)^2 / (t^2 + 0.01)) / (3 P) and its gradient with respect to f.
+__global__ void k_filter_loss(const float4* __restrict__ f, const float4* __restrict__ tgt, int P,
+                              float4* __restrict__ g, float* __restrict__ loss) {
   const float norm = 1.0f / (3.0f * (float)P);
   float local = 0.0f;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-    const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
-    const float* lg = logits + (size_t)p * 32;
-    float mx = lg[0];
-    for (int k = 1; k < 25; ++k) mx = fmaxf(mx, lg[k]);
-    float wk[25], sum = 0.0f;
-    for (int k = 0; k < 25; ++k) { wk[k] = __expf(lg[k] - mx); sum += wk[k]; }
-    const float inv = 1.0f / sum;
-    float3 f = make_float3(0.0f, 0.0f, 0.0f);
-    float3 cs[25];
-    for (int k = 0; k < 25; ++k) {
-      int yy = min(max(y + k / 5 - 2, 0), h - 1), xx = min(max(x + k % 5 - 2, 0), w - 1);
-      float4 c = col[((size_t)b * h + yy) * w + xx];
-      cs[k] = make_float3(c.x, c.y, c.z);
-      wk[k] *= inv;
-      f.x += wk[k] * c.x; f.y += wk[k] * c.y; f.z += wk[k] * c.z;
-    }
-    out[p] = make_float4(f.x, f.y, f.z, 1.0f);
-    if (tgt) {
-      float4 t = tgt[p];
-      float ex = f.x - t.x, ey = f.y - t.y, ez = f.z - t.z;
-      float dx = 1.0f / (t.x * t.x + 0.01f), dy = 1.0f / (t.y * t.y + 0.01f), dz = 1.0f / (t.z * t.z + 0.01f);
-      local += ex * ex * dx + ey * ey * dy + ez * ez * dz;
-      float3 gf = make_float3(2.0f * ex * dx * norm, 2.0f * ey * dy * norm, 2.0f * ez * dz * norm);
-      float g[25], gw = 0.0f;
-      for (int k = 0; k < 25; ++k) {
-        g[k] = gf.x * cs[k].x + gf.y * cs[k].y + gf.z * cs[k].z;
-        gw += wk[k] * g[k];
-      }
-      uint32_t o[16];
-      for (int k = 0; k < 16; ++k) {
-        float a = 2 * k < 25 ? wk[2 * k] * (g[2 * k] - gw) : 0.0f;
-        float c = 2 * k + 1 < 25 ? wk[2 * k + 1] * (g[2 * k + 1] - gw) : 0.0f;
-        o[k] = (uint32_t)f2bf(a) | ((uint32_t)f2bf(c) << 16);
-      }
-      uint4* dst = reinterpret_cast<uint4*>(dlogits + (size_t)p * 32);
-      for (int k = 0; k < 4; ++k) dst[k] = make_uint4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
-    }
+    float4 a = f[p], t = tgt[p];
+    float ex = a.x - t.x, ey = a.y - t.y, ez = a.z - t.z;
+    float dx = 1.0f / (t.x * t.x + 0.01f), dy = 1.0f / (t.y * t.y + 0.01f), dz = 1.0f / (t.z * t.z + 0.01f);
+    local += ex * ex * dx + ey * ey * dy + ez * ez * dz;
+    g[p] = make_float4(2.0f * ex * dx * norm, 2.0f * ey * dy * norm, 2.0f * ez * dz * norm, 0.0f);
   }
-  if (tgt) {
-    for (int off = 16; off > 0; off >>= 1) local += __shfl_down_sync(0xffffffffu, local, off);
-    if ((threadIdx.x & 31) == 0) atomicAdd(loss, local * norm);
+  for (int off = 16; off > 0; off >>= 1) local += __shfl_down_sync(0xffffffffu, local, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, local * norm);
+}
+
+// Backward of one filter stage: logit gradients of its 25 kernel weights (softmax Jacobian) and,
+// when gin is given, the gradient of its input, scattered to the tap neighbours (atomics).
+__global__ void k_filter_bwd(const float* __restrict__ logits, int stage, int d, const float4* __restrict__ in,
+                             const float4* __restrict__ gout, uint16_t* __restrict__ dlogits, float* __restrict__ gin,
+                             int B, int h, int w) {
+  const int P = B * h * w;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
+    float wk[25], G[25];
+    softmax25(logits + (size_t)p * LOGITS + stage * 25, wk);
+    const float4 g = gout[p];
+    float gw = 0.0f;
+    for (int k = 0; k < 25; ++k) {
+      const size_t q = tap_index(b, y, x, k, d, h, w);
+      float4 c = in[q];
+      G[k] = g.x * c.x + g.y * c.y + g.z * c.z;
+      gw += wk[k] * G[k];
+      if (gin) {
+        atomicAdd(gin + q * 4 + 0, wk[k] * g.x);
+        atomicAdd(gin + q * 4 + 1, wk[k] * g.y);
+        atomicAdd(gin + q * 4 + 2, wk[k] * g.z);
+      }
+    }
+    uint16_t* dl = dlogits + (size_t)p * LOGITS + stage * 25;
+    for (int k = 0; k < 25; ++k) dl[k] = f2bf(wk[k] * (G[k] - gw));
+    if (stage == 2)
+      for (int k = 75; k < LOGITS; ++k) dlogits[(size_t)p * LOGITS + k] = 0;
   }
 }
 
@@ -532,7 +562,8 @@ struct Net {
            *p3 = nullptr, *e3 = nullptr, *p4 = nullptr, *e4a = nullptr, *e4 = nullptr, *d3 = nullptr, *d2 = nullptr,
            *d1 = nullptr, *d0 = nullptr;
   float* logits = nullptr;
-  float4 *col = nullptr, *tgt = nullptr, *out = nullptr;
+  float4 *col = nullptr, *tgt = nullptr, *out = nullptr, *f1 = nullptr, *f2 = nullptr, *gf_a = nullptr,
+         *gf_b = nullptr;
   uint16_t *dlog = nullptr, *dx = nullptr, *g_a = nullptr, *g_b = nullptr, *g_pool = nullptr, *g_skip = nullptr;
   std::vector<void*> bufs;
   float* loss = nullptr;
@@ -562,7 +593,7 @@ static void define_layers(Net& n) {
   set_layer(n.L[L_D2], "D2", 96, 64, 64, 9, 1, 2, 160, 64);
   set_layer(n.L[L_D1], "D1", 64, 48, 48, 9, 1, 1, 112, 48);
   set_layer(n.L[L_D0], "D0", 48, 32, 32, 9, 1, 0, 80, 32);
-  set_layer(n.L[L_OUT], "OUT", 0, 32, 32, 1, 0, 0, 32, 25);
+  set_layer(n.L[L_OUT], "OUT", 0, 32, LOGITS, 1, 0, 0, 32, 75);
   size_t off = 0;
   for (int i = 0; i < NLAYERS; ++i) {
     n.L[i].w_off = off;
@@ -615,11 +646,15 @@ static cudaError_t ensure_batch(Net& n, int B, int H, int W) {
   n.d2 = (uint16_t*)alloc(px(2) * 64 * 2);
   n.d1 = (uint16_t*)alloc(px(1) * 48 * 2);
   n.d0 = (uint16_t*)alloc(px(0) * 32 * 2);
-  n.logits = (float*)alloc(px(0) * 32 * 4);
+  n.logits = (float*)alloc(px(0) * LOGITS * 4);
   n.col = (float4*)alloc(px(0) * 16);
   n.tgt = (float4*)alloc(px(0) * 16);
   n.out = (float4*)alloc(px(0) * 16);
-  n.dlog = (uint16_t*)alloc(px(0) * 32 * 2);
+  n.f1 = (float4*)alloc(px(0) * 16);
+  n.f2 = (float4*)alloc(px(0) * 16);
+  n.gf_a = (float4*)alloc(px(0) * 16);
+  n.gf_b = (float4*)alloc(px(0) * 16);
+  n.dlog = (uint16_t*)alloc(px(0) * LOGITS * 2);
   // the largest data gradient: a concat input (fine) of any level
   size_t dx_max = std::max({px(0) * 80, px(1) * 112, px(2) * 160, px(3) * 224, px(4) * 128});
   n.dx = (uint16_t*)alloc(dx_max * 2);
@@ -688,6 +723,10 @@ static cudaError_t forward(Net& n) {
   if ((e = conv_fwd(n, n.L[L_D1], n.d2, n.e1, n.d1, false))) return e;
   if ((e = conv_fwd(n, n.L[L_D0], n.d1, n.e0, n.d0, false))) return e;
   if ((e = conv_fwd(n, n.L[L_OUT], nullptr, n.d0, n.logits, true))) return e;
+  const int P0 = B * n.H * n.W;
+  k_filter_fwd<<<grid1(P0), 256, 0, n.st>>>(n.logits, 0, 1, n.col, n.f1, B, n.H, n.W);
+  k_filter_fwd<<<grid1(P0), 256, 0, n.st>>>(n.logits, 1, 2, n.f1, n.f2, B, n.H, n.W);
+  k_filter_fwd<<<grid1(P0), 256, 0, n.st>>>(n.logits, 2, 4, n.f2, n.out, B, n.H, n.W);
   return cudaGetLastError();
 }
 
@@ -698,7 +737,13 @@ static cudaError_t backward(Net& n) {
   auto px = [&](int lv) { return (size_t)B * n.hl[lv] * n.wl[lv]; };
   if ((e = cudaMemsetAsync(n.g, 0, n.n_params * 4, n.st))) return e;
   if ((e = cudaMemsetAsync(n.loss, 0, 4, n.st))) return e;
-  k_apply<<<grid1(px(0)), 256, 0, n.st>>>(n.logits, n.col, B, n.H, n.W, n.out, n.tgt, n.dlog, n.loss);
+  const int P0 = (int)px(0);
+  k_filter_loss<<<grid1(px(0)), 256, 0, n.st>>>(n.out, n.tgt, P0, n.gf_a, n.loss);
+  if ((e = cudaMemsetAsync(n.gf_b, 0, px(0) * 16, n.st))) return e;
+  k_filter_bwd<<<grid1(px(0)), 256, 0, n.st>>>(n.logits, 2, 4, n.f2, n.gf_a, n.dlog, (float*)n.gf_b, B, n.H, n.W);
+  if ((e = cudaMemsetAsync(n.gf_a, 0, px(0) * 16, n.st))) return e;
+  k_filter_bwd<<<grid1(px(0)), 256, 0, n.st>>>(n.logits, 1, 2, n.f1, n.gf_b, n.dlog, (float*)n.gf_a, B, n.H, n.W);
+  k_filter_bwd<<<grid1(px(0)), 256, 0, n.st>>>(n.logits, 0, 1, n.col, n.gf_a, n.dlog, nullptr, B, n.H, n.W);
   // OUT (1x1 over D0)
   if ((e = conv_bwd(n, n.L[L_OUT], n.dlog, nullptr, n.d0, true))) return e;
   uint16_t* gd0 = n.g_a;
@@ -1079,8 +1124,6 @@ int wgpt_kpcn_denoise(wgpt_kpcn* k, wgpt_ctx* ctx, float exposure, float* filter
   kp::k_gather<<<kp::grid1(npix), 256, 0, n.st>>>((const float4*)im.accum, im.gbuf, nullptr, (int)im.h, (int)im.w,
                                                   k->d_crops, 1, (int)im.h, (int)im.w, n.x0, n.col, nullptr);
   KCK(kp::forward(n), "forward");
-  kp::k_apply<<<kp::grid1(npix), 256, 0, n.st>>>(n.logits, n.col, 1, (int)im.h, (int)im.w, n.out, nullptr, nullptr,
-                                                 nullptr);
   kp::k_tonemap<<<kp::grid1(npix), 256, 0, n.st>>>(n.out, (int)npix, exposure, (uchar4*)im.out);
   KCK(cudaGetLastError(), "denoise launch");
   KCK(cudaEventRecord(k->ev_out, n.st), "event");

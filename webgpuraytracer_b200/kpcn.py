@@ -48,7 +48,7 @@ LAYERS = (
     LayerSpec("D2", 96, 64, 64, 9, True, 2),
     LayerSpec("D1", 64, 48, 48, 9, True, 1),
     LayerSpec("D0", 48, 32, 32, 9, True, 0),
-    LayerSpec("OUT", 0, 32, 32, 1, False, 0),
+    LayerSpec("OUT", 0, 32, 80, 1, False, 0),
 )
 
 

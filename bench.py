@@ -618,6 +618,51 @@ def run_batch(args):
     return 0
 
 
+def run_denoise(args):
+    """--workload denoise: the learned denoiser's inference (1920x1080, untrained weights, which
+    cost the same) and the a-trous filter (5 passes) on a 4-spp accumulation of the small-
+    configuration scene; one step = one filter of the frame.  For kernel profiles."""
+    import torch
+    from webgpuraytracer_b200 import kpcn
+    from webgpuraytracer_b200 import renderer as rd
+    from webgpuraytracer_b200 import synth
+    W, H = 1920, 1080
+    scene = synth.small_scene(1, W, H, 4)
+    scene.camera.aspect = W / H
+    r = rd.Renderer(W, H, seed_fn=lambda: 7)
+    r.set_scene(scene, isgbuf=True)
+    r.render_gbuffer()
+    r.reset()
+    r.render(tsize=W, reps=4)
+    k = kpcn.Kpcn(0, seed=1)
+    st = torch.cuda.ExternalStream(r.stream_handle())
+    atrous = rd.Denoiser(r, passes=5)
+    res = {}
+    for name, fn_ in (("kpcn", lambda: k.denoise(r, want_linear=False)), ("atrous", atrous.execute)):
+        for _ in range(args.warmup):
+            fn_()
+        r.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            fn_()
+        e1.record(st)
+        r.synchronize()
+        torch.cuda.synchronize()
+        res[name] = e0.elapsed_time(e1) / args.steps
+    flops = kpcn.gemm_flops(W, H)
+    peaks, kind = load_peaks()
+    tf = flops / (res["kpcn"] / 1e3) / 1e12
+    print(json.dumps({"metric": "denoise ms per 1920x1080 frame", "value": res["kpcn"], "unit": "ms",
+                      "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+                      "atrous_ms": res["atrous"], "kpcn_gemm_tflops": tf,
+                      "kpcn_frac_of_bf16_peak": tf / peaks.get("bf16_tflops", 1590.0),
+                      "config": {"workload": "denoise 1920x1080, small-configuration scene at 4 spp"}}), flush=True)
+    k.close()
+    r.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -636,8 +681,9 @@ def main():
     ap.add_argument("--kpcn-scenes", type=int, default=128)
     ap.add_argument("--kpcn-target-spp", type=int, default=1024)
     ap.add_argument("--kpcn-steps", type=int, default=2000)
-    ap.add_argument("--workload", choices=["flagship", "batch"], default="flagship",
-                    help="flagship: 1080p 64 spp; batch: 32 uneven views of the 5.24 M-triangle scene")
+    ap.add_argument("--workload", choices=["flagship", "batch", "denoise"], default="flagship",
+                    help="flagship: 1080p 64 spp; batch: 32 uneven views of the 5.24 M-triangle scene; "
+                         "denoise: learned and a-trous filters on one 1080p frame")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -645,6 +691,8 @@ def main():
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "denoise":
+        return run_denoise(args)
     return run_ours(args)
 
 

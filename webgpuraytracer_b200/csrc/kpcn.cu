@@ -257,6 +257,165 @@ struct EpiAtomic {
   }
 };
 
+// ---------------------------------------------------------------------------- 3x3 halo convolution
+// A 3x3 convolution (padding 1) as 9 shifted GEMMs over one shared-memory halo tile: a CTA owns a
+// 16 x 16 block of output pixels as two 128-pixel M tiles (8 wide x 16 tall each) and an NT-wide
+// slice of the output channels.  Per 16 input channels it loads the 18 x 18 halo once (two 8-
+// channel planes of 16-byte pixel vectors) and the weights of all 9 taps; tap (dy, dx) is then
+// just a descriptor offset into the halo: 8 consecutive pixels of an output row are 8 consecutive
+// 16-byte halo vectors (a core matrix), the next output row is 18 vectors further (SBO) and the
+// next 8 channels one plane further (LBO).  Each input value is read from global memory about
+// 1.3 times instead of 9 times.  Two accumulators (one per M tile) live in tensor memory.
+constexpr int HALO_W = 18, HALO_P = HALO_W * HALO_W;
+
+struct HaloSrc {
+  const uint16_t* u;   // coarse tensor read 2x upsampled, channels [0, cu)
+  int cu, hc, wc;
+  const uint16_t* s;   // tensor at the output resolution, channels [cu, cu + cs)
+  int cs;
+  int h, w;
+  __device__ __forceinline__ uint4 at(int b, int y, int x, int ci0) const {
+    if (y < 0 || y >= h || x < 0 || x >= w) return zero4();
+    if (ci0 < cu) return *reinterpret_cast<const uint4*>(u + (((size_t)b * hc + (y >> 1)) * wc + (x >> 1)) * cu + ci0);
+    return *reinterpret_cast<const uint4*>(s + (((size_t)b * h + y) * w + x) * cs + (ci0 - cu));
+  }
+};
+
+template <int NT>
+struct HaloSmem {
+  static constexpr int HALO = 2 * HALO_P * 16;   // 16 channels
+  static constexpr int WTS = 9 * NT * 32;        // per tap: NT rows x 16 channels
+  static constexpr int STAGE = HALO + WTS;
+  static constexpr int BYTES = 2 * STAGE + 64;
+};
+
+// wb: [N][9][cin] BF16 weights (output channel, tap, input channel); grid (ceil(w/16),
+// ceil(h/16), images * ceil(N/NT)); the epilogue gets (pixel index, first column, 16 values).
+template <int NT, class EP>
+__global__ void __launch_bounds__(tc::THREADS) k_conv3x3(HaloSrc src, const uint16_t* __restrict__ wb, int cin, int N,
+                                                        EP ep, uint32_t* err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  using S = HaloSmem<NT>;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int ntiles = (N + NT - 1) / NT;
+  const int b = blockIdx.z / ntiles, n0 = (blockIdx.z % ntiles) * NT;
+  const int x0 = blockIdx.x * 16, y0 = blockIdx.y * 16;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * S::STAGE);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + 2 * S::STAGE + 16);
+  volatile uint32_t* flag = reinterpret_cast<volatile uint32_t*>(smem + 2 * S::STAGE + 20);
+  const uint32_t bar0 = tc::smem_u32(&bars[0]), bar1 = tc::smem_u32(&bars[1]);
+  constexpr uint32_t NCOLS = tc::tmem_cols(2 * NT);
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(tmem_slot), NCOLS);
+  if (tid == 0) {
+    tc::mbar_init(bar0, 1);
+    tc::mbar_init(bar1, 1);
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int KT = cin / 16;
+  constexpr uint32_t IDESC = tc::idesc_bf16(NT);
+  bool ok = true;
+  int committed = 0;
+  for (int kt = 0; kt < KT; ++kt) {
+    const int st = kt & 1;
+    uint8_t* halo = smem + st * S::STAGE;
+    uint8_t* wts = halo + S::HALO;
+    if (kt >= 2) {
+      if (tid == 0) *flag = tc::mbar_wait(st ? bar1 : bar0, (uint32_t)((kt >> 1) - 1) & 1u) ? 1u : 0u;
+      __syncthreads();
+      if (*flag == 0u) { ok = false; break; }
+    }
+    const int ci = kt * 16;
+    for (int i = tid; i < 2 * HALO_P; i += tc::THREADS) {
+      const int c = i / HALO_P, q = i - c * HALO_P, hy = q / HALO_W, hx = q - hy * HALO_W;
+      *reinterpret_cast<uint4*>(halo + i * 16) = src.at(b, y0 - 1 + hy, x0 - 1 + hx, ci + c * 8);
+    }
+    for (int i = tid; i < 9 * NT * 2; i += tc::THREADS) {
+      const int c = i & 1, n = (i >> 1) % NT, t = (i >> 1) / NT, gn = n0 + n;
+      uint4 v = zero4();
+      if (gn < N) v = *reinterpret_cast<const uint4*>(wb + ((size_t)gn * 9 + t) * cin + ci + c * 8);
+      *reinterpret_cast<uint4*>(wts + t * NT * 32 + ((n >> 3) * 2 + c) * 128 + (n & 7) * 16) = v;
+    }
+    tc::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::tc_fence_after();
+      const uint32_t ha = tc::smem_u32(halo), wa = tc::smem_u32(wts);
+#pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        const int dy = t / 3, dx = t % 3;
+        const uint64_t db = tc::smem_desc(wa + t * NT * 32, 128, 256);
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+          const uint64_t da = tc::smem_desc(ha + (dy * HALO_W + 8 * m + dx) * 16, HALO_P * 16, HALO_W * 16);
+          tc::mma_bf16(tmem + (uint32_t)(m * NT), da, db, IDESC, (kt > 0 || t > 0) ? 1u : 0u);
+        }
+      }
+      tc::mma_commit(st ? bar1 : bar0);
+    }
+    committed = kt + 1;
+  }
+  if (tid == 0) {
+    const int last = committed - 1;
+    *flag = committed == 0 || tc::mbar_wait((last & 1) ? bar1 : bar0, (uint32_t)(last >> 1) & 1u) ? 1u : 0u;
+  }
+  __syncthreads();
+  ok = ok && *flag != 0u;
+  if (!ok) {
+    if (tid == 0) atomicOr(err, tc::ERR_TC_TIMEOUT);
+  } else if (KT > 0) {
+    tc::tc_fence_after();
+    const int r = warp * 32 + (tid & 31), ty = r >> 3, tx = r & 7, y = y0 + ty;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      const int x = x0 + 8 * m + tx;
+      for (int c0 = 0; c0 < NT; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(m * NT + c0), v);
+        if (y < src.h && x < src.w && n0 + c0 < N) ep((int)(((size_t)b * src.h + y) * src.w + x), n0 + c0, v);
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_free(tmem, NCOLS);
+}
+
+template <int NT, class EP>
+cudaError_t conv3x3_nt(const HaloSrc& src, const uint16_t* wb, int cin, int N, int B, const EP& ep, uint32_t* err,
+                       cudaStream_t st) {
+  auto kern = k_conv3x3<NT, EP>;
+  const int smem = HaloSmem<NT>::BYTES;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  const int ntiles = (N + NT - 1) / NT;
+  dim3 grid((unsigned)((src.w + 15) / 16), (unsigned)((src.h + 15) / 16), (unsigned)(B * ntiles));
+  kern<<<grid, tc::THREADS, smem, st>>>(src, wb, cin, N, ep, err);
+  return cudaGetLastError();
+}
+
+// Output-channel slice width per launch: the whole N when it fits one MMA pair (two
+// accumulators of N columns in 256 TMEM columns), else 128-wide slices.
+template <class EP>
+cudaError_t conv3x3(const HaloSrc& src, const uint16_t* wb, int cin, int N, int B, const EP& ep, uint32_t* err,
+                    cudaStream_t st) {
+  switch (N) {
+    case 32: return conv3x3_nt<32>(src, wb, cin, N, B, ep, err, st);
+    case 48: return conv3x3_nt<48>(src, wb, cin, N, B, ep, err, st);
+    case 64: return conv3x3_nt<64>(src, wb, cin, N, B, ep, err, st);
+    case 80: return conv3x3_nt<80>(src, wb, cin, N, B, ep, err, st);
+    case 96: return conv3x3_nt<96>(src, wb, cin, N, B, ep, err, st);
+    case 112: return conv3x3_nt<112>(src, wb, cin, N, B, ep, err, st);
+    default: return conv3x3_nt<128>(src, wb, cin, N, B, ep, err, st);
+  }
+}
+
 template <int BN, class LA, class LB, class EP>
 cudaError_t gemm(const LA& la, const LB& lb, const EP& ep, int M, int N, int K, int splits, uint32_t* err,
                  cudaStream_t st) {
@@ -505,8 +664,9 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float
   }
 }
 
-// BF16 copies of one layer's weights W[co][tap][ci]: as stored (forward, weight-gradient
-// layout) and transposed to Wt[ci][tap][co] (data gradient).
+// BF16 copies of one layer's weights W[co][tap][ci]: as stored (forward) and transposed with the
+// taps mirrored, Wt[ci][taps-1-tap][co], so the data gradient is the same 3x3 convolution of the
+// output gradient with Wt.
 __global__ void k_weights_bf16(const float* __restrict__ wf, int cout, int taps, int cin, uint16_t* __restrict__ wb,
                                uint16_t* __restrict__ wt) {
   const int n = cout * taps * cin;
@@ -514,7 +674,7 @@ __global__ void k_weights_bf16(const float* __restrict__ wf, int cout, int taps,
     const int ci = i % cin, t = (i / cin) % taps, co = i / (cin * taps);
     uint16_t b = f2bf(wf[i]);
     wb[i] = b;
-    wt[((size_t)ci * taps + t) * cout + co] = b;
+    wt[((size_t)ci * taps + (taps - 1 - t)) * cout + co] = b;
   }
 }
 
@@ -671,6 +831,10 @@ static cudaError_t conv_fwd(Net& n, const Layer& l, const uint16_t* u, const uin
   const int lv = l.level, h = n.hl[lv], w = n.wl[lv];
   const int P = n.B * h * w;
   ConvSrc src{u, l.cu, lv + 1 < 5 ? n.hl[lv + 1] : 1, lv + 1 < 5 ? n.wl[lv + 1] : 1, s, l.cs, h, w, l.taps, 1};
+  if (l.taps == 9 && !logits) {
+    HaloSrc hs{u, l.cu, src.hc, src.wc, s, l.cs, h, w};
+    return conv3x3(hs, l.wb, l.cin(), l.cout, n.B, EpiAct{(uint16_t*)y, n.w + l.b_off, l.cout, l.relu}, n.err, n.st);
+  }
   ConvA a{src, P, l.cin()};
   RowMajor b{l.wb, l.cout, l.taps * l.cin(), l.taps * l.cin()};
   if (logits) return gemm_n(a, b, EpiLogits{(float*)y, n.w + l.b_off, l.cout}, P, l.cout, l.taps * l.cin(), n.err, n.st);
@@ -693,7 +857,12 @@ static cudaError_t conv_bwd(Net& n, const Layer& l, const uint16_t* dz, const ui
   if (e != cudaSuccess) return e;
   k_bias_grad<<<std::min(grid1((size_t)P * l.cout), 512), 256, l.cout * 4, n.st>>>(dz, P, l.cout, n.g + l.b_off);
   if (!want_dx) return cudaGetLastError();
-  // data gradient: M = pixels, N = cin, K = taps * cout, source = dZ read at p - offset
+  // data gradient: the 3x3 convolution of dZ with the tap-mirrored transposed weights
+  if (l.taps == 9) {
+    HaloSrc hs{nullptr, 0, 1, 1, dz, l.cout, h, w};
+    return conv3x3(hs, l.wt, l.cout, cin, n.B, EpiStore{n.dx, cin}, n.err, n.st);
+  }
+  // (1x1: M = pixels, N = cin, K = cout)
   ConvSrc dsrc{nullptr, 0, 1, 1, dz, l.cout, h, w, l.taps, -1};
   ConvA a{dsrc, P, l.cout};
   RowMajor b{l.wt, cin, l.taps * l.cout, l.taps * l.cout};

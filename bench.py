@@ -121,32 +121,23 @@ class ClockSampler:
 
 
 def dist_setup(n_gpus: int):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    return rank, world, local
+    from webgpuraytracer_b200 import replicas
+    return replicas.setup("nccl")
 
 
 def max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from webgpuraytracer_b200 import replicas
+    return replicas.max_over_ranks(x, world)
 
 
 def barrier(world: int):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from webgpuraytracer_b200 import replicas
+    replicas.barrier(world)
+
+
+def replicas_seed(rank: int) -> int:
+    from webgpuraytracer_b200 import replicas
+    return replicas.rank_seed(1, rank)
 
 
 def build_workload(seed: int = 1):
@@ -402,7 +393,7 @@ def run_ours(args):
 
     torch.cuda.set_device(local)
     scene, packed = build_workload()
-    r = rd.Renderer(WIDTH, HEIGHT, device=local, seed_fn=lambda: 1 + rank)
+    r = rd.Renderer(WIDTH, HEIGHT, device=local, seed_fn=lambda: replicas_seed(rank))
     r.set_scene(scene, packed=packed)
     mega = args.mode == "megakernel"
     r._check(r.L.wgpt_set_render_mode(r.ctx, 1 if mega else 0), "render mode")
@@ -416,7 +407,7 @@ def run_ours(args):
 
     def launch(step):
         frame = step * spp
-        p = sc.pack_params(scene, packed, WIDTH, HEIGHT, frame, 1 + rank)
+        p = sc.pack_params(scene, packed, WIDTH, HEIGHT, frame, replicas_seed(rank))
         r._check(r.L.wgpt_set_params(r.ctx, rd.ptr(p)), "set_params")
         r._check(r.L.wgpt_render(r.ctx, frame, spp, 0, 0, WIDTH, HEIGHT), "render")
 
@@ -511,9 +502,8 @@ def run_ours(args):
             line["time_to_rmse"] = ttr
         print(json.dumps(line), flush=True)
     r.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from webgpuraytracer_b200 import replicas
+    replicas.teardown(world)
     return 0
 
 
@@ -543,7 +533,7 @@ def run_batch(args):
 
     def launch(step, timing=False):
         ff = [step * 64] * len(views)
-        params = [synth.view_params(scene, packed, v, f, 1 + rank) for v, f in zip(views, ff)]
+        params = [synth.view_params(scene, packed, v, f, replicas_seed(rank)) for v, f in zip(views, ff)]
         return r.render_views(params, ff, spp, timing=timing)
 
     for i in range(args.warmup):
@@ -612,9 +602,8 @@ def run_batch(args):
         }
         print(json.dumps(line), flush=True)
     r.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from webgpuraytracer_b200 import replicas
+    replicas.teardown(world)
     return 0
 
 

@@ -509,32 +509,57 @@ def run_ours(args):
 
 def run_batch(args):
     """--workload batch: 32 seeded views (sizes over 256^2..1920x1080, 4/16/64 spp, 8 bounces)
-    of the 5.24 M-triangle scene in one render_views call per step; paths/s over all views and
-    the p50/p99 of the per-view completion times (device clock, from the start of the call's
-    work to the view's last sample)."""
+    of the 5.24 M-triangle scene.  The views are shared out over the ranks longest-first (LPT by
+    width x height x spp; strong scaling of the fixed batch); each rank autotunes its path pool
+    on a quarter-sample probe, then traces all its views in one render_views call per step and
+    finishes every view with the learned denoiser.  Reports paths/s over all views and the
+    p50/p99 of the per-view completion times (device clock from the start of the call's work to
+    the view's last sample) and of the finished times (denoised image ready)."""
     rank, world, local = dist_setup(args.gpus)
     import torch
+    from webgpuraytracer_b200 import autotune
+    from webgpuraytracer_b200 import kpcn
     from webgpuraytracer_b200 import renderer as rd
+    from webgpuraytracer_b200 import replicas
     from webgpuraytracer_b200 import scene as sc
     from webgpuraytracer_b200 import synth
 
     torch.cuda.set_device(local)
     scene = synth.batch_scene(1)
     packed = sc.pack_scene_data(scene)
-    views = synth.batch_views(1, 32)
+    all_views = synth.batch_views(1, 32)
+    work = [v["width"] * v["height"] * v["spp"] for v in all_views]
+    mine = replicas.assign_lpt(work, world)[rank]
+    views = [all_views[i] for i in mine]
     r = rd.Renderer(16, 16, device=local)
     r.set_scene(scene, packed=packed)
-    r.set_wavefront_config(args.pool or 0, 1 << 30)
     r.set_views([(v["width"], v["height"]) for v in views])
     stream = torch.cuda.ExternalStream(r.stream_handle(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     spp = [v["spp"] for v in views]
-    paths_per_step = sum(v["width"] * v["height"] * v["spp"] for v in views)
+    paths_mine = sum(v["width"] * v["height"] * v["spp"] for v in views)
+    paths_all = sum(work)
+
+    def params_for(step):
+        ff = [step * 64] * len(views)
+        return [synth.view_params(scene, packed, v, f, 1) for v, f in zip(views, ff)], ff
 
     def launch(step, timing=False):
-        ff = [step * 64] * len(views)
-        params = [synth.view_params(scene, packed, v, f, replicas_seed(rank)) for v, f in zip(views, ff)]
+        params, ff = params_for(step)
         return r.render_views(params, ff, spp, timing=timing)
+
+    r.render_views_gbuffer(params_for(0)[0])
+    probe_spp = [max(1, x // 4) for x in spp]
+    p0, f0 = params_for(0)
+    if args.pool:
+        r.set_wavefront_config(args.pool, 1 << 30)
+        tuned = {"pool_paths": args.pool, "units_per_pass": 1 << 30, "table": "fixed by --pool"}
+    else:
+        tuned = autotune.tune_wavefront(r, lambda: r.render_views(p0, f0, probe_spp, timing=False),
+                                        units=(1 << 27, 1 << 30))
+    net = kpcn.Kpcn(local, seed=1)   # untrained weights: the same kernels and cost as trained ones
+    for i in range(len(views)):      # first use loads the network's kernels and sizes its buffers
+        net.denoise_view(r, i)
 
     for i in range(args.warmup):
         launch(i)
@@ -559,39 +584,66 @@ def run_batch(args):
     clocks = sampler.stop()
     dev_s = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)) / 1e3
     dev_s_max = max_over_ranks(dev_s, world)
-    value = paths_per_step * args.steps * world / dev_s_max
-    # per-view completion times (one more step, which waits for them)
+    value = paths_all * args.steps / dev_s_max
+    # per-view completion (device stamps) and finishing by the learned denoiser, views in the
+    # order their samples completed
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
     done = launch(args.warmup + args.steps, timing=True)
-    # end-to-end: params in, every view's rgba8 image out, every step
+    e1.record(stream)
+    torch.cuda.synchronize()
+    call_ms = e0.elapsed_time(e1)
+    finished = [0.0] * len(views)
+    t_acc = call_ms
+    for i in sorted(range(len(views)), key=lambda j: done[j]):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        net.denoise_view(r, i)
+        b.record(stream)
+        torch.cuda.synchronize()
+        t_acc += a.elapsed_time(b)
+        finished[i] = t_acc
+    done_all = replicas.gather_lists([float(x) for x in done], world)
+    fin_all = replicas.gather_lists(finished, world)
+    # end-to-end: params in, every view traced, denoised and read back as rgba8, every step
     outs = [np.empty((v["height"], v["width"], 4), np.uint8) for v in views]
     e2e_steps = max(1, min(args.steps, 4))
     barrier(world)
     t0 = time.perf_counter()
     for i in range(e2e_steps):
         launch(args.warmup + args.steps + 1 + i)
-        for k, o in enumerate(outs):
-            r._check(r.L.wgpt_read_view(r.ctx, k, None, rd.ptr(o)), "read_view")
+        for k_, o in enumerate(outs):
+            net.denoise_view(r, k_)
+            r._check(r.L.wgpt_read_view(r.ctx, k_, None, rd.ptr(o)), "read_view")
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    rep = stage_report(r, rd, lambda: launch(args.warmup), stream, flush, paths_per_step, False)
+    rep = stage_report(r, rd, lambda: launch(args.warmup), stream, flush, paths_mine, False)
     peaks, peak_kind = load_peaks()
     cnt = rep["cnt"]
+    rays_all = replicas.sum_over_ranks(float(cnt[1] + cnt[2]), world)
     if rank == 0:
         line = {
             "metric": "paths/s, 32 batched views (uneven size and spp), 8 bounces", "value": value,
             "unit": "paths/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dev_s_max / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": dev_s_max / args.steps * 1e3, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene and view generator)",
             "config": {"workload": "batched views: 32 views of 16 instances x 327,680-tri BLAS + 64 prims, "
                                    "2048x1024 RGBE env; sizes {256^2, 512^2, 1280x720, 1920x1080}, spp {4,16,64}",
-                       "step": f"one render_views call ({paths_per_step:,} paths)",
-                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}",
-                       "path_pool": r.wavefront_config()[0]},
-            "view_done_ms": {"p50": float(np.percentile(done, 50)), "p99": float(np.percentile(done, 99)),
-                             "max": float(np.max(done))},
-            "rays_per_s": int(cnt[1] + cnt[2]) * world * args.steps / dev_s_max,
-            "e2e": {"value": paths_per_step * e2e_steps * world / e2e_s, "unit": "paths/s",
-                    "h2d_bytes_per_step": 112 * len(views),
-                    "d2h_bytes_per_step": sum(v["width"] * v["height"] * 4 for v in views)},
+                       "step": f"one render_views call per rank ({paths_all:,} paths over all ranks)",
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"views LPT-assigned over {world} rank(s)",
+                       "autotuned": {"pool_paths": tuned["pool_paths"], "units_per_pass": tuned["units_per_pass"]}},
+            "autotune_table_ms": tuned["table"],
+            "view_done_ms": {"p50": float(np.percentile(done_all, 50)), "p99": float(np.percentile(done_all, 99)),
+                             "max": float(np.max(done_all))},
+            "view_finished_ms": {"p50": float(np.percentile(fin_all, 50)), "p99": float(np.percentile(fin_all, 99)),
+                                 "max": float(np.max(fin_all)),
+                                 "note": "render call end + learned-denoiser passes in completion order"},
+            "rays_per_s": rays_all * args.steps / dev_s_max,
+            "e2e": {"value": paths_all * e2e_steps / e2e_s, "unit": "paths/s",
+                    "h2d_bytes_per_step": 112 * len(all_views),
+                    "d2h_bytes_per_step": sum(v["width"] * v["height"] * 4 for v in all_views),
+                    "includes": "render, learned denoiser per view, rgba8 readback"},
             "gpu_launches": rep["launches"] * args.steps,
             "stages": rep["stages"],
             "roofline": {"bound": "hbm", "achieved": rep["achieved"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -601,8 +653,8 @@ def run_batch(args):
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
+    net.close()
     r.close()
-    from webgpuraytracer_b200 import replicas
     replicas.teardown(world)
     return 0
 

@@ -155,6 +155,9 @@ int wgpt_set_views(wgpt_ctx* ctx, uint32_t n, const uint32_t* widths, const uint
 int wgpt_render_views(wgpt_ctx* ctx, const void* params_112n, const uint32_t* first_frames, const uint32_t* spp,
                       float* done_ms);
 int wgpt_read_view(wgpt_ctx* ctx, uint32_t view, float* accum_rgba32f, uint8_t* out_rgba8);
+/* gbuf_main for every view (params as for wgpt_render_views; the G-buffers are allocated on first
+   use), so the learned denoiser can finish each view (wgpt_kpcn_denoise_view). */
+int wgpt_render_views_gbuffer(wgpt_ctx* ctx, const void* params_112n);
 
 /* BF16 GEMM on the tensor cores (tcgen05, FP32 accumulation in tensor memory), the core of the
    learned denoiser's kernels (no counterpart in the reference): C[m x n] = A[m x k] * B[n x k]^T
@@ -191,6 +194,7 @@ int wgpt_kpcn_loss_and_grads(wgpt_kpcn* k, const float* noisy_rgba32f, const voi
                              const float* target_rgba32f, uint32_t w, uint32_t h, float* loss, float* grads,
                              float* out_rgba32f);
 int wgpt_kpcn_denoise(wgpt_kpcn* k, wgpt_ctx* ctx, float exposure, float* filtered_rgba32f);
+int wgpt_kpcn_denoise_view(wgpt_kpcn* k, wgpt_ctx* ctx, uint32_t view, float exposure, float* filtered_rgba32f);
 
 /* Closest hit of caller rays (trace_scene, shader.wgsl:754-774) for parity tests: rays are n x
    (origin, direction) floats; outputs object index, material index, global triangle index

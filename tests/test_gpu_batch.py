@@ -85,3 +85,33 @@ def test_batch_rejects_inconsistent_views(flagship):
     done = b.render_views(good, [0, 0], [0, 2])
     assert done[0] == -1.0 and done[1] >= 0.0
     b.close()
+
+
+def test_views_gbuffer_and_learned_denoiser_per_view(flagship):
+    """Each batched view gets its G-buffer and is finished by the learned denoiser exactly as a
+    single-view renderer holding the same accumulation and G-buffer would be."""
+    from webgpuraytracer_b200 import kpcn
+    scene, packed = flagship
+    views = VIEWS[:2]
+    params = [synth.view_params(scene, packed, v, 0, seed=3) for v in views]
+    b = rd.Renderer(16, 16)
+    b.set_scene(scene, packed=packed)
+    b.set_views([(v["width"], v["height"]) for v in views])
+    b.render_views_gbuffer(params)
+    b.render_views(params, [0, 0], [v["spp"] for v in views], timing=False)
+    net = kpcn.Kpcn(0, seed=2)
+    for i, v in enumerate(views):
+        lin_b = net.denoise_view(b, i, want_linear=True)
+        _, out_b = b.read_view(i)
+        r = rd.Renderer(v["width"], v["height"])
+        r.set_scene(scene, isgbuf=True, packed=packed)
+        r._check(r.L.wgpt_set_params(r.ctx, rd.ptr(params[i])), "params")
+        r._check(r.L.wgpt_render_gbuffer(r.ctx, 0, 0, v["width"], v["height"]), "gbuffer")
+        r._check(r.L.wgpt_render(r.ctx, 0, v["spp"], 0, 0, v["width"], v["height"]), "render")
+        r.synchronize()
+        lin_r = net.denoise(r)
+        _same(lin_b, lin_r, f"view {i} denoised")
+        _same(out_b, r.read_output(), f"view {i} denoised rgba8")
+        r.close()
+    net.close()
+    b.close()

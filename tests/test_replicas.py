@@ -61,3 +61,17 @@ def test_single_process_defaults():
     a = np.ones((2, 2, 4))
     m, n = replicas.merge_accumulations(a, 5, 1)
     assert m is a and n == 5
+
+
+def test_lpt_assignment_balances_views():
+    from webgpuraytracer_b200 import synth
+    views = synth.batch_views(1, 32)
+    work = [v["width"] * v["height"] * v["spp"] for v in views]
+    for world in (1, 2, 4, 8):
+        parts = replicas.assign_lpt(work, world)
+        assert sorted(i for p in parts for i in p) == list(range(32))
+        loads = [sum(work[i] for i in p) for p in parts]
+        # LPT is within 4/3 of optimal; the optimum is at least max(total/world, largest job)
+        bound = max(sum(work) / world, max(work))
+        assert max(loads) <= bound * 4 / 3 + 1
+    assert replicas.assign_lpt([5, 4, 3, 3, 3], 2) == [[0, 3], [1, 2, 4]]

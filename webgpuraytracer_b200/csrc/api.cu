@@ -53,7 +53,7 @@ struct wgpt_ctx {
   bool timing = false;
   wgpt::WfEngine* wf = nullptr;   // wavefront renderer: path pool, sample buffer, loop graph
   // batched views: size and images of each
-  struct View { uint32_t w, h; float* accum; uint8_t* out; };
+  struct View { uint32_t w, h; float* accum; uint8_t* out; float* gbuf; };
   std::vector<View> views;
   double* acc64 = nullptr;        // optional FP64 Welford accumulation (8 doubles per pixel)
 };
@@ -371,15 +371,26 @@ int check_env(wgpt_ctx* ctx, const wgpt_scene_params& p) {
 
 }  // namespace
 
-bool wgpt::ctx_images(wgpt_ctx* ctx, wgpt::CtxImages* out) {
-  if (!ctx || !out || ctx->w == 0 || !ctx->accum) return false;
+bool wgpt::ctx_images(wgpt_ctx* ctx, int view, wgpt::CtxImages* out) {
+  if (!ctx || !out) return false;
   out->device = ctx->device;
-  out->w = ctx->w;
-  out->h = ctx->h;
-  out->accum = ctx->accum;
-  out->gbuf = ctx->gbuf;
-  out->out = ctx->out;
   out->stream = ctx->stream;
+  if (view < 0) {
+    if (ctx->w == 0 || !ctx->accum) return false;
+    out->w = ctx->w;
+    out->h = ctx->h;
+    out->accum = ctx->accum;
+    out->gbuf = ctx->gbuf;
+    out->out = ctx->out;
+    return true;
+  }
+  if ((size_t)view >= ctx->views.size()) return false;
+  const auto& v = ctx->views[(size_t)view];
+  out->w = v.w;
+  out->h = v.h;
+  out->accum = v.accum;
+  out->gbuf = v.gbuf;
+  out->out = v.out;
   return true;
 }
 
@@ -420,7 +431,7 @@ int wgpt_destroy(wgpt_ctx* ctx) {
   ctx->wf = nullptr;
   dfree_t(ctx->acc64);
   dfree(ctx->d_pairs_tlas); dfree(ctx->d_pairs_bvh);
-  for (auto& v : ctx->views) { dfree_t(v.accum); dfree_t(v.out); }
+  for (auto& v : ctx->views) { dfree_t(v.accum); dfree_t(v.out); dfree_t(v.gbuf); }
   if (ctx->timer) {
     if (ctx->timer->ready)
       for (int i = 0; i < wgpt::StageTimer::kMaxEvents; ++i) cudaEventDestroy(ctx->timer->ev[i]);
@@ -711,10 +722,10 @@ int wgpt_set_views(wgpt_ctx* ctx, uint32_t n, const uint32_t* widths, const uint
       return fail(ctx, WGPT_E_INVALID, "view size must be 1..16384 per side");
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "drain before view allocation");
-  for (auto& v : ctx->views) { dfree_t(v.accum); dfree_t(v.out); }
+  for (auto& v : ctx->views) { dfree_t(v.accum); dfree_t(v.out); dfree_t(v.gbuf); }
   ctx->views.clear();
   for (uint32_t i = 0; i < n; ++i) {
-    wgpt_ctx::View v{widths[i], heights[i], nullptr, nullptr};
+    wgpt_ctx::View v{widths[i], heights[i], nullptr, nullptr, nullptr};
     size_t np = (size_t)v.w * v.h;
     ctx->views.push_back(v);
     CK(cudaMalloc(&ctx->views.back().accum, np * 16), "cudaMalloc view accumulation");
@@ -769,6 +780,23 @@ int wgpt_render_views(wgpt_ctx* ctx, const void* params_112n, const uint32_t* fi
   CK(wgpt::wf_render(ctx->wf, ctx->ds, ctx->d_pairs_tlas, ctx->d_pairs_bvh, jv.data(), n, ctx->d_status, cnt,
                      ctx->stream, tm, done_ms),
      "batched render");
+  return WGPT_OK;
+}
+
+int wgpt_render_views_gbuffer(wgpt_ctx* ctx, const void* params_112n) {
+  if (!ctx || !params_112n) return WGPT_E_INVALID;
+  if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
+  if (ctx->views.empty()) return fail(ctx, WGPT_E_STATE, "no views: call wgpt_set_views first");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  for (size_t i = 0; i < ctx->views.size(); ++i) {
+    auto& v = ctx->views[i];
+    wgpt_scene_params q;
+    memcpy(&q, (const char*)params_112n + i * sizeof q, sizeof q);
+    if (q.width != v.w || q.height != v.h) return fail(ctx, WGPT_E_INVALID, "view params size differs from the view");
+    if (!v.gbuf) CK(cudaMalloc(&v.gbuf, (size_t)v.w * v.h * 48), "cudaMalloc view G-buffer");
+    CK(wgpt::launch_gbuffer(ctx->ds, q, 0, 0, v.w, v.h, v.gbuf, v.out, v.w, ctx->d_status, ctx->stream),
+       "view gbuffer launch");
+  }
   return WGPT_OK;
 }
 

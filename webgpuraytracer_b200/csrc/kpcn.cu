@@ -716,7 +716,8 @@ struct Net {
   int adam_t = 0;
   uint32_t* err = nullptr;
   // activations / gradients for the current batch shape
-  int B = 0, H = 0, W = 0, cap_px = 0;
+  int B = 0, H = 0, W = 0;
+  size_t cap[5] = {0, 0, 0, 0, 0};   // allocated pixels per level
   int hl[5], wl[5];
   uint16_t *x0 = nullptr, *e0a = nullptr, *e0 = nullptr, *p1 = nullptr, *e1 = nullptr, *p2 = nullptr, *e2 = nullptr,
            *p3 = nullptr, *e3 = nullptr, *p4 = nullptr, *e4a = nullptr, *e4 = nullptr, *d3 = nullptr, *d2 = nullptr,
@@ -774,15 +775,21 @@ static cudaError_t refresh_bf16(Net& n) {
   return cudaGetLastError();
 }
 
+// Sets the batch shape; the buffers grow to the largest shape seen (per level) and are reused
+// for smaller ones, so alternating image sizes (batched views) cost no allocation.
 static cudaError_t ensure_batch(Net& n, int B, int H, int W) {
   if (n.B == B && n.H == H && n.W == W) return cudaSuccess;
-  cudaStreamSynchronize(n.st);
-  for (void* p : n.bufs) cudaFree(p);
-  n.bufs.clear();
   n.B = B; n.H = H; n.W = W;
   n.hl[0] = H; n.wl[0] = W;
   for (int l = 1; l < 5; ++l) { n.hl[l] = (n.hl[l - 1] + 1) / 2; n.wl[l] = (n.wl[l - 1] + 1) / 2; }
-  auto px = [&](int l) { return (size_t)B * n.hl[l] * n.wl[l]; };
+  bool fits = !n.bufs.empty();
+  for (int l = 0; l < 5; ++l) fits = fits && (size_t)B * n.hl[l] * n.wl[l] <= n.cap[l];
+  if (fits) return cudaSuccess;
+  for (int l = 0; l < 5; ++l) n.cap[l] = std::max(n.cap[l], (size_t)B * n.hl[l] * n.wl[l]);
+  cudaStreamSynchronize(n.st);
+  for (void* p : n.bufs) cudaFree(p);
+  n.bufs.clear();
+  auto px = [&](int l) { return n.cap[l]; };
   cudaError_t e = cudaSuccess;
   auto alloc = [&](size_t bytes) -> void* {
     void* p = nullptr;
@@ -1272,11 +1279,11 @@ int wgpt_kpcn_loss_and_grads(wgpt_kpcn* k, const float* noisy, const void* gbuf,
   return check_device_error(k);
 }
 
-int wgpt_kpcn_denoise(wgpt_kpcn* k, wgpt_ctx* ctx, float exposure, float* filtered_rgba32f) {
+static int denoise_image(wgpt_kpcn* k, wgpt_ctx* ctx, int view, float exposure, float* filtered_rgba32f) {
   if (!k || !ctx) return WGPT_E_INVALID;
   kp::Net& n = k->net;
   wgpt::CtxImages im;
-  if (!wgpt::ctx_images(ctx, &im)) return kfail(k, WGPT_E_STATE, "context has no image (resize first)");
+  if (!wgpt::ctx_images(ctx, view, &im)) return kfail(k, WGPT_E_STATE, "no such image (resize or set views first)");
   if (!im.gbuf) return kfail(k, WGPT_E_STATE, "context has no G-buffer: resize with want_gbuf and render it");
   if (im.device != n.device) return kfail(k, WGPT_E_INVALID, "context and denoiser are on different devices");
   cudaSetDevice(n.device);
@@ -1302,6 +1309,14 @@ int wgpt_kpcn_denoise(wgpt_kpcn* k, wgpt_ctx* ctx, float exposure, float* filter
     return check_device_error(k);
   }
   return WGPT_OK;
+}
+
+int wgpt_kpcn_denoise(wgpt_kpcn* k, wgpt_ctx* ctx, float exposure, float* filtered_rgba32f) {
+  return denoise_image(k, ctx, -1, exposure, filtered_rgba32f);
+}
+
+int wgpt_kpcn_denoise_view(wgpt_kpcn* k, wgpt_ctx* ctx, uint32_t view, float exposure, float* filtered_rgba32f) {
+  return denoise_image(k, ctx, (int)view, exposure, filtered_rgba32f);
 }
 
 }  // extern "C"

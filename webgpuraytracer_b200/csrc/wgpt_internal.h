@@ -18,7 +18,7 @@ struct CtxImages {
   uint8_t* out;
   cudaStream_t stream;
 };
-bool ctx_images(::wgpt_ctx* ctx, CtxImages* out);
+bool ctx_images(::wgpt_ctx* ctx, int view, CtxImages* out);   // view -1: the main image
 
 // Device copies of the scene buffers, in the reference's packed layouts.
 struct DeviceScene {

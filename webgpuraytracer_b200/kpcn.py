@@ -139,6 +139,15 @@ class Kpcn:
         return lin
 
 
+    def denoise_view(self, r: rd.Renderer, view: int, exposure: float = 1.0, want_linear: bool = False):
+        """Filters one batched view of the renderer (accumulation + view G-buffer) into its image."""
+        w, h = r._views[view]
+        lin = np.zeros((h, w, 4), np.float32) if want_linear else None
+        self._check(self.L.wgpt_kpcn_denoise_view(self.h, r.ctx, view, exposure, ptr(lin) if want_linear else None),
+                    "denoise_view")
+        return lin
+
+
 def render_example(scene: sc.Scene, size: int, spp: int, target_spp: int, seed: int = 1, target_seed: int = 977):
     """(noisy accumulation at `spp`, G-buffer, target accumulation at `target_spp`) of one view,
     rendered by the path tracer; the target uses an independent sample stream."""

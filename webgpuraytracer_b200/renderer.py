@@ -245,6 +245,12 @@ class Renderer:
                     "render_views")
         return done
 
+    def render_views_gbuffer(self, params):
+        """gbuf_main for every view (allocates the view G-buffers on first use)."""
+        blob = np.ascontiguousarray(np.concatenate([np.frombuffer(np.asarray(p).tobytes(), np.uint8)
+                                                    for p in params]))
+        self._check(self.L.wgpt_render_views_gbuffer(self.ctx, ptr(blob)), "render_views_gbuffer")
+
     def read_view(self, i: int):
         w, h = self._views[i]
         acc = np.empty((h, w, 4), np.float32)

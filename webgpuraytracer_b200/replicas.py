@@ -95,3 +95,27 @@ def teardown(world: int):
         import torch.distributed as dist
         if dist.is_initialized():
             dist.destroy_process_group()
+
+
+def assign_lpt(work: list[float], world: int) -> list[list[int]]:
+    """Longest-processing-time-first assignment of independent jobs (e.g. camera views weighted
+    by width x height x spp) to `world` ranks: jobs in descending order of work, each to the rank
+    with the least work so far (ties to the lower rank).  Returns the job indices per rank."""
+    order = sorted(range(len(work)), key=lambda i: (-work[i], i))
+    load = [0.0] * world
+    out: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += work[i]
+    return out
+
+
+def gather_lists(values: list[float], world: int) -> list[float]:
+    """Every rank's list of values, concatenated in rank order (on every rank)."""
+    if world == 1:
+        return list(values)
+    import torch.distributed as dist
+    parts: list = [None] * world
+    dist.all_gather_object(parts, list(values))
+    return [x for part in parts for x in part]

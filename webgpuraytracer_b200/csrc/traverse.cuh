@@ -137,15 +137,18 @@ __device__ __forceinline__ void enter_mesh(const DScene& s, TravCommon& t, const
   t.push(t.root_entry(lo, hi, node_offset, true), err);
 }
 
-// One traversal step; returns true when the stack is empty (the ray is done).
+// Pops and processes inner nodes until the stack top is something else, which is popped into
+// `e` (true), or the stack runs empty (false).  No leaf is processed in between, so the pruning
+// limit is the same as when entries are taken one at a time: the order of work is unchanged.
+// Running inner nodes back to back keeps a warp's lanes on the node code together and then on
+// the leaf code together, instead of splitting every step between the two.
 template <bool COUNT>
-__device__ __forceinline__ bool closest_step(const DScene& s, const DPairs& P, ClosestTrav& t, uint32_t& err,
-                                             Counters<COUNT>& cn) {
-  if (t.sp == 0) return true;
-  uint2 e = t.stack[--t.sp];
-  uint32_t kind = e.x >> 29, cnt = e.x & 0x1fffffffu;
-  HitRec& hit = t.hit;
-  if (kind == K_BLAS_INNER || kind == K_TLAS_INNER) {
+__device__ __forceinline__ bool inner_run(const DPairs& P, TravCommon& t, float limit, uint32_t& err,
+                                          Counters<COUNT>& cn, uint2& e) {
+  while (t.sp > 0) {
+    e = t.stack[--t.sp];
+    const uint32_t kind = e.x >> 29;
+    if (kind != K_BLAS_INNER && kind != K_TLAS_INNER) return true;
     cn.add(C_NODES);
     bool blas = kind == K_BLAS_INNER;
     const float4* pp = (blas ? P.bvh : P.tlas) + (size_t)e.y * 4;
@@ -155,8 +158,21 @@ __device__ __forceinline__ bool closest_step(const DScene& s, const DPairs& P, C
     cn.add(C_CHILD_TESTS, 2);
     float lt = intersect_aabb(r.origin, inv, a, b);
     float rt = intersect_aabb(r.origin, inv, c, d);
-    t.push_children(lt, rt, hit.t, a, b, c, d, blas, err);
-  } else if (kind == K_BLAS_LEAF) {
+    t.push_children(lt, rt, limit, a, b, c, d, blas, err);
+  }
+  return false;
+}
+
+// A run of inner nodes and then one leaf (or instance end); returns true when the stack is
+// empty (the ray is done).
+template <bool COUNT>
+__device__ __forceinline__ bool closest_step(const DScene& s, const DPairs& P, ClosestTrav& t, uint32_t& err,
+                                             Counters<COUNT>& cn) {
+  HitRec& hit = t.hit;
+  uint2 e;
+  if (!inner_run<COUNT>(P, t, hit.t, err, cn, e)) return true;
+  uint32_t kind = e.x >> 29, cnt = e.x & 0x1fffffffu;
+  if (kind == K_BLAS_LEAF) {
     cn.add(C_NODES);
     uint32_t start = t.tri_offset + e.y;
     for (uint32_t i = start; i < start + cnt; i++) {
@@ -243,21 +259,11 @@ __device__ __forceinline__ void shadow_init(const DScene& s, ShadowTrav& t, Coun
 template <bool COUNT>
 __device__ __forceinline__ bool shadow_step(const DScene& s, const DPairs& P, ShadowTrav& t, uint32_t& err,
                                             Counters<COUNT>& cn) {
-  if (t.occluded || t.sp == 0) return true;
-  uint2 e = t.stack[--t.sp];
+  if (t.occluded) return true;
+  uint2 e;
+  if (!inner_run<COUNT>(P, t, t.target_dist, err, cn, e)) return true;
   uint32_t kind = e.x >> 29, cnt = e.x & 0x1fffffffu;
-  if (kind == K_BLAS_INNER || kind == K_TLAS_INNER) {
-    cn.add(C_NODES);
-    bool blas = kind == K_BLAS_INNER;
-    const float4* pp = (blas ? P.bvh : P.tlas) + (size_t)e.y * 4;
-    float4 a = ld4(pp), b = ld4(pp + 1), c = ld4(pp + 2), d = ld4(pp + 3);
-    const Ray& r = blas ? t.rl : t.rw;
-    v3 inv = blas ? t.inv_l : t.inv_w;
-    cn.add(C_CHILD_TESTS, 2);
-    float lt = intersect_aabb(r.origin, inv, a, b);
-    float rt = intersect_aabb(r.origin, inv, c, d);
-    t.push_children(lt, rt, t.target_dist, a, b, c, d, blas, err);
-  } else if (kind == K_BLAS_LEAF) {
+  if (kind == K_BLAS_LEAF) {
     cn.add(C_NODES);
     uint32_t start = t.tri_offset + e.y;
     for (uint32_t i = start; i < start + cnt; i++) {

@@ -173,18 +173,24 @@ __device__ __forceinline__ bool closest_step(const DScene& s, const DPairs& P, C
   if (!inner_run<COUNT>(P, t, hit.t, err, cn, e)) return true;
   uint32_t kind = e.x >> 29, cnt = e.x & 0x1fffffffu;
   if (kind == K_BLAS_LEAF) {
-    cn.add(C_NODES);
-    uint32_t start = t.tri_offset + e.y;
-    for (uint32_t i = start; i < start + cnt; i++) {
-      const float4* tp = s.tris + (size_t)i * 8;
-      float t_tri, u, v;
-      cn.add(C_TRI_TESTS);
-      if (intersect_triangle(t.rl, ld4(tp), ld4(tp + 1), ld4(tp + 2), &t_tri, &u, &v)) {
-        if (t_tri >= 0.0f && t_tri < hit.t) {
-          hit.t = t_tri; hit.m_idx = t.inst_mat; hit.o_idx = t.inst_oidx;
-          hit.kind = 2; hit.id = (int32_t)i; hit.aux = -1; hit.bu = u; hit.bv = v;
+    // this leaf and any leaves directly under it on the stack (taken in stack order)
+    while (true) {
+      cn.add(C_NODES);
+      uint32_t start = t.tri_offset + e.y;
+      for (uint32_t i = start; i < start + cnt; i++) {
+        const float4* tp = s.tris + (size_t)i * 8;
+        float t_tri, u, v;
+        cn.add(C_TRI_TESTS);
+        if (intersect_triangle(t.rl, ld4(tp), ld4(tp + 1), ld4(tp + 2), &t_tri, &u, &v)) {
+          if (t_tri >= 0.0f && t_tri < hit.t) {
+            hit.t = t_tri; hit.m_idx = t.inst_mat; hit.o_idx = t.inst_oidx;
+            hit.kind = 2; hit.id = (int32_t)i; hit.aux = -1; hit.bu = u; hit.bv = v;
+          }
         }
       }
+      if (t.sp == 0 || (t.stack[t.sp - 1].x >> 29) != K_BLAS_LEAF) break;
+      e = t.stack[--t.sp];
+      cnt = e.x & 0x1fffffffu;
     }
   } else if (kind == K_TLAS_LEAF || kind == K_TLAS_REST) {
     if (kind == K_TLAS_LEAF) cn.add(C_NODES);
@@ -264,15 +270,20 @@ __device__ __forceinline__ bool shadow_step(const DScene& s, const DPairs& P, Sh
   if (!inner_run<COUNT>(P, t, t.target_dist, err, cn, e)) return true;
   uint32_t kind = e.x >> 29, cnt = e.x & 0x1fffffffu;
   if (kind == K_BLAS_LEAF) {
-    cn.add(C_NODES);
-    uint32_t start = t.tri_offset + e.y;
-    for (uint32_t i = start; i < start + cnt; i++) {
-      const float4* tp = s.tris + (size_t)i * 8;
-      float t_tri, u, v;
-      cn.add(C_TRI_TESTS);
-      if (intersect_triangle(t.rl, ld4(tp), ld4(tp + 1), ld4(tp + 2), &t_tri, &u, &v)) {
-        if (t_tri >= 0.0f && t_tri < t.target_dist) { t.occluded = true; return true; }
+    while (true) {
+      cn.add(C_NODES);
+      uint32_t start = t.tri_offset + e.y;
+      for (uint32_t i = start; i < start + cnt; i++) {
+        const float4* tp = s.tris + (size_t)i * 8;
+        float t_tri, u, v;
+        cn.add(C_TRI_TESTS);
+        if (intersect_triangle(t.rl, ld4(tp), ld4(tp + 1), ld4(tp + 2), &t_tri, &u, &v)) {
+          if (t_tri >= 0.0f && t_tri < t.target_dist) { t.occluded = true; return true; }
+        }
       }
+      if (t.sp == 0 || (t.stack[t.sp - 1].x >> 29) != K_BLAS_LEAF) break;
+      e = t.stack[--t.sp];
+      cnt = e.x & 0x1fffffffu;
     }
   } else if (kind == K_TLAS_LEAF || kind == K_TLAS_REST) {
     if (kind == K_TLAS_LEAF) cn.add(C_NODES);

@@ -49,6 +49,9 @@ BYTES_PER_UNIT = {
     11: 32,   # hit attributes of the winning primitive (normals)
 }
 PIXEL_BYTES = 16 + 16 + 4   # accumulation read + write, rgba8 store
+# DRAM bytes (read + write) of one full-pool closest-hit launch of this workload, from an ncu
+# capture (bench cannot run ncu itself); the algorithmic bytes of the same launch are ~3.9 GB.
+EXTEND_DRAM_BYTES_PER_LAUNCH = 4.23e8
 KERNELS = ["k_wf_fill", "k_wf_extend", "k_wf_shade", "k_wf_shadow", "k_wf_resolve", "k_wf_shade_miss",
            "k_wf_accumulate", "k_wf_control"]
 
@@ -484,7 +487,11 @@ def run_ours(args):
             "gpu_launches": launches * args.steps,
             "stages": stages,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                         "frac": achieved / peaks["hbm_gbs"],
+                         "traffic": None if mega else EXTEND_DRAM_BYTES_PER_LAUNCH,
+                         "traffic_source": None if mega else
+                         "ncu dram__bytes_read.sum + dram__bytes_write.sum of steady-state k_wf_extend launches "
+                         "(mean of launches 21-23 of this workload's stage-timing pass)",
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
                          "kernel": "k_render" if mega else KERNELS[dom],

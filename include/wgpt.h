@@ -259,6 +259,17 @@ int wgpt_build_env_cdf(const uint16_t* rgba16f, uint32_t w, uint32_t h, double e
 int wgpt_decode_rgbe(const uint8_t* file, size_t bytes, double exposure, uint16_t* rgba16f, uint32_t* w,
                      uint32_t* h);
 
+/* Model.parseOBJ + generateTriangles (tracer.js:949-1021): an OBJ text (v, vt, vn, f with
+   1-based v/vt/vn indices, polygons fan-triangulated) to n_tris triangles of 24 floats
+   (v0 v1 v2 n0 n1 n2 uv0 uv1 uv2), the input of wgpt_build_blas.  JavaScript number semantics:
+   parseFloat/parseInt prefixes, face indices stored through an Int32Array (NaN -> 0), and NaN
+   wherever the reference reads outside its vertex arrays (missing vt/vn, bad indices).  Call
+   with tris24 = NULL to get the count, then with room for `capacity` >= n_tris triangles.
+   positions (nullable) receives the vertex_positions array (n_positions floats, 3 per vertex)
+   that Model.getBounds walks. */
+int wgpt_parse_obj(const char* text, size_t bytes, float* tris24, uint32_t capacity, uint32_t* n_tris,
+                   float* positions, uint32_t pos_capacity, uint32_t* n_positions);
+
 #ifdef __cplusplus
 }
 #endif

@@ -364,3 +364,91 @@ def bsdf_f64(mat: dict, normal, albedo, roughness, metallic, V, L):
             if p_trans > 0:
                 pdf += p_trans * (_G1(nv, a2) * D * max(0.0, vh)) * (etat * etat * abs(lh)) / max(den * den, 1e-7)
     return f, max(pdf, 1e-7)
+
+
+# ------------------------------------------------------------------ OBJ (tracer.js:949-1021)
+_FLOAT_RE = None
+
+
+def _js_parse_float(s: str) -> float:
+    import re
+    global _FLOAT_RE
+    if _FLOAT_RE is None:
+        _FLOAT_RE = re.compile(r"[+-]?(Infinity|(\d+\.?\d*|\.\d+)([eE][+-]?\d+)?)")
+    m = _FLOAT_RE.match(s.lstrip(" \t\r\n\v\f"))
+    if not m:
+        return math.nan
+    t = m.group(0)
+    if t.lstrip("+-") == "Infinity":
+        return -math.inf if t.startswith("-") else math.inf
+    return float(t)
+
+
+def _js_parse_int(s: str) -> float:
+    s = s.lstrip(" \t\r\n\v\f")
+    sign, i = 1.0, 0
+    if s[:1] in ("+", "-"):
+        sign = -1.0 if s[0] == "-" else 1.0
+        i = 1
+    base = 10
+    if s[i:i + 2].lower() == "0x":
+        base, i = 16, i + 2
+    digits = "0123456789abcdef"[:base]
+    v, n = 0, 0
+    while i < len(s) and s[i].lower() in digits:
+        v = v * base + digits.index(s[i].lower())
+        i += 1
+        n += 1
+    return sign * v if n else math.nan
+
+
+def _int32(x: float) -> float:
+    if not math.isfinite(x):
+        return 0.0
+    m = math.fmod(math.trunc(x), 4294967296.0)
+    if m < 0:
+        m += 4294967296.0
+    return m - 4294967296.0 if m >= 2147483648.0 else m
+
+
+def _at(a, index: float) -> float:
+    if not (index >= 0) or index != math.floor(index) or index >= len(a):
+        return math.nan
+    return float(np.float32(a[int(index)]))
+
+
+def parse_obj(text: str) -> np.ndarray:
+    """Model.parseOBJ + generateTriangles in plain Python with JavaScript semantics: n x 24
+    float32 triangles (v0 v1 v2 n0 n1 n2 uv0 uv1 uv2)."""
+    import re
+    P, U, N, fp, fu, fn = [], [], [], [], [], []
+    for line in text.split("\n"):
+        parts = re.split(r"[ \t\r\n\v\f]+", line.strip(" \t\r\n\v\f"))
+        part = lambda i: parts[i] if i < len(parts) else ""
+        typ = parts[0]
+        if typ == "v":
+            P += [_js_parse_float(part(1)), _js_parse_float(part(2)), _js_parse_float(part(3))]
+        elif typ == "vt":
+            U += [_js_parse_float(part(1)), _js_parse_float(part(2))]
+        elif typ == "vn":
+            N += [_js_parse_float(part(1)), _js_parse_float(part(2)), _js_parse_float(part(3))]
+        elif typ == "f":
+            face = []
+            for p in parts[1:]:
+                idx = p.split("/")
+                face.append((_js_parse_int(idx[0]) - 1,
+                             _js_parse_int(idx[1]) - 1 if len(idx) > 1 and idx[1] else -1,
+                             _js_parse_int(idx[2]) - 1 if len(idx) > 2 and idx[2] else -1))
+            for i in range(1, len(face) - 1):
+                for c in (face[0], face[i], face[i + 1]):
+                    fp.append(c[0]); fu.append(c[1]); fn.append(c[2])
+    out = np.zeros((len(fp) // 3, 24), np.float32)
+    for t in range(len(fp) // 3):
+        for c in range(3):
+            ip, iu, iN = _int32(fp[t * 3 + c]), _int32(fu[t * 3 + c]), _int32(fn[t * 3 + c])
+            for d in range(3):
+                out[t, c * 3 + d] = _at(P, ip * 3 + d)
+                out[t, 9 + c * 3 + d] = _at(N, iN * 3 + d)
+            for d in range(2):
+                out[t, 18 + c * 2 + d] = _at(U, iu * 2 + d)
+    return out

@@ -115,6 +115,8 @@ EXPORTS = {
     "wgpt_build_tlas": ([_P, _U32, _P, C.POINTER(_U32)], C.c_int),
     "wgpt_build_env_cdf": ([_P, _U32, _U32, C.c_double, _P, C.POINTER(C.c_double)], C.c_int),
     "wgpt_decode_rgbe": ([_P, C.c_size_t, C.c_double, _P, C.POINTER(_U32), C.POINTER(_U32)], C.c_int),
+    "wgpt_parse_obj": ([_P, C.c_size_t, _P, C.c_uint32, C.POINTER(C.c_uint32), _P, C.c_uint32,
+                        C.POINTER(C.c_uint32)], C.c_int),
 }
 
 _lib: C.CDLL | None = None

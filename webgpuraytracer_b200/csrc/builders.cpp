@@ -11,6 +11,9 @@
 #include <stdio.h>
 #include <string.h>
 #include <math.h>
+#include <cctype>
+#include <cmath>
+#include <cstdlib>
 #include <algorithm>
 #include <string>
 #include <vector>
@@ -392,3 +395,163 @@ int wgpt_decode_rgbe(const uint8_t* buf, size_t len, double exposure_f, uint16_t
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------- OBJ
+// Model.parseOBJ + generateTriangles (tracer.js:949-1021): positions (v), texture coordinates
+// (vt) and normals (vn) as JavaScript numbers, faces (f) as 1-based v/vt/vn index triples,
+// polygons fan-triangulated from their first vertex.  Triangles come out as the 24 floats the
+// BLAS builder takes (v0 v1 v2 n0 n1 n2 uv0 uv1 uv2), each value rounded to float32 the way the
+// reference's Float32Array does.  Where the reference indexes outside its arrays (a missing vt or
+// vn, an index out of range, a negative relative index, an unparsable number) it reads
+// `undefined`, which a Float32Array stores as NaN; the same NaN is produced here.
+namespace {
+
+bool js_space(unsigned char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\n' || c == '\v' || c == '\f'; }
+
+// parseFloat: the longest prefix that is a decimal literal or "Infinity" (after leading white
+// space and an optional sign); NaN when there is none.
+double js_parse_float(const std::string& s) {
+  size_t i = 0, n = s.size();
+  while (i < n && js_space((unsigned char)s[i])) ++i;
+  size_t start = i;
+  if (i < n && (s[i] == '+' || s[i] == '-')) ++i;
+  if (s.compare(i, 8, "Infinity") == 0) {
+    return s[start] == '-' ? -HUGE_VAL : HUGE_VAL;
+  }
+  size_t digits = 0, j = i;
+  while (j < n && isdigit((unsigned char)s[j])) { ++j; ++digits; }
+  if (j < n && s[j] == '.') {
+    ++j;
+    while (j < n && isdigit((unsigned char)s[j])) { ++j; ++digits; }
+  }
+  if (digits == 0) return NAN;
+  if (j < n && (s[j] == 'e' || s[j] == 'E')) {
+    size_t k = j + 1;
+    if (k < n && (s[k] == '+' || s[k] == '-')) ++k;
+    size_t kd = k;
+    while (k < n && isdigit((unsigned char)s[k])) ++k;
+    if (k > kd) j = k;
+  }
+  return strtod(s.substr(start, j - start).c_str(), nullptr);
+}
+
+// parseInt without a radix: optional sign, "0x" selects hexadecimal, then the longest run of
+// digits; NaN when there is none.
+double js_parse_int(const std::string& s) {
+  size_t i = 0, n = s.size();
+  while (i < n && js_space((unsigned char)s[i])) ++i;
+  double sign = 1.0;
+  if (i < n && (s[i] == '+' || s[i] == '-')) { if (s[i] == '-') sign = -1.0; ++i; }
+  int base = 10;
+  if (i + 1 < n && s[i] == '0' && (s[i + 1] == 'x' || s[i + 1] == 'X')) { base = 16; i += 2; }
+  double v = 0.0;
+  size_t digits = 0;
+  for (; i < n; ++i) {
+    int d;
+    char c = s[i];
+    if (c >= '0' && c <= '9') d = c - '0';
+    else if (base == 16 && c >= 'a' && c <= 'f') d = c - 'a' + 10;
+    else if (base == 16 && c >= 'A' && c <= 'F') d = c - 'A' + 10;
+    else break;
+    v = v * base + d;
+    ++digits;
+  }
+  return digits ? sign * v : NAN;
+}
+
+// array[index] of a JavaScript array of numbers: undefined (NaN once stored) unless the index is
+// a non-negative integer inside the array.
+float js_at(const std::vector<double>& a, double index) {
+  if (!(index >= 0.0) || index != std::floor(index) || index >= (double)a.size()) return NAN;
+  return (float)a[(size_t)index];
+}
+
+}  // namespace
+
+extern "C" int wgpt_parse_obj(const char* text, size_t bytes, float* tris24, uint32_t capacity, uint32_t* n_tris,
+                              float* positions, uint32_t pos_capacity, uint32_t* n_positions) {
+  if ((!text && bytes) || !n_tris) return WGPT_E_INVALID;
+  std::vector<double> P, U, N;
+  std::vector<double> fp, fu, fn;   // per triangle corner: position, uv, normal index (0-based)
+  size_t pos = 0;
+  std::vector<std::string> parts;
+  while (pos <= bytes) {
+    size_t end = pos;
+    while (end < bytes && text[end] != '\n') ++end;
+    // line.trim().split(/\s+/)
+    size_t a = pos, b = end;
+    while (a < b && js_space((unsigned char)text[a])) ++a;
+    while (b > a && js_space((unsigned char)text[b - 1])) --b;
+    parts.clear();
+    size_t k = a;
+    while (true) {
+      size_t t = k;
+      while (t < b && !js_space((unsigned char)text[t])) ++t;
+      parts.emplace_back(text + k, t - k);
+      if (t >= b) break;
+      k = t;
+      while (k < b && js_space((unsigned char)text[k])) ++k;
+    }
+    const std::string& type = parts[0];
+    auto part = [&](size_t i) -> std::string { return i < parts.size() ? parts[i] : std::string(); };
+    if (type == "v") {
+      P.push_back(js_parse_float(part(1))); P.push_back(js_parse_float(part(2))); P.push_back(js_parse_float(part(3)));
+    } else if (type == "vt") {
+      U.push_back(js_parse_float(part(1))); U.push_back(js_parse_float(part(2)));
+    } else if (type == "vn") {
+      N.push_back(js_parse_float(part(1))); N.push_back(js_parse_float(part(2))); N.push_back(js_parse_float(part(3)));
+    } else if (type == "f") {
+      struct Corner { double v, u, n; };
+      std::vector<Corner> face;
+      for (size_t i = 1; i < parts.size(); ++i) {
+        std::vector<std::string> idx;
+        size_t s0 = 0;
+        const std::string& p = parts[i];
+        while (true) {
+          size_t sl = p.find('/', s0);
+          idx.push_back(p.substr(s0, sl == std::string::npos ? std::string::npos : sl - s0));
+          if (sl == std::string::npos) break;
+          s0 = sl + 1;
+        }
+        Corner c;
+        c.v = js_parse_int(idx[0]) - 1.0;
+        c.u = idx.size() > 1 && !idx[1].empty() ? js_parse_int(idx[1]) - 1.0 : -1.0;
+        c.n = idx.size() > 2 && !idx[2].empty() ? js_parse_int(idx[2]) - 1.0 : -1.0;
+        face.push_back(c);
+      }
+      for (size_t i = 1; i + 1 < face.size(); ++i) {
+        const Corner* cs[3] = {&face[0], &face[i], &face[i + 1]};
+        for (const Corner* c : cs) { fp.push_back(c->v); fu.push_back(c->u); fn.push_back(c->n); }
+      }
+    }
+    if (end >= bytes) break;
+    pos = end + 1;
+  }
+  // Int32Array stores of the face indices: NaN becomes 0, values wrap to 32 bits
+  auto i32 = [](double x) -> double {
+    if (!std::isfinite(x)) return 0.0;
+    double t = std::trunc(x);
+    double m = std::fmod(t, 4294967296.0);
+    if (m < 0) m += 4294967296.0;
+    return m >= 2147483648.0 ? m - 4294967296.0 : m;
+  };
+  const size_t ntri = fp.size() / 3;
+  *n_tris = (uint32_t)ntri;
+  if (n_positions) *n_positions = (uint32_t)P.size();
+  if (positions) {
+    if (pos_capacity < P.size()) return WGPT_E_INVALID;
+    for (size_t i = 0; i < P.size(); ++i) positions[i] = (float)P[i];
+  }
+  if (!tris24) return WGPT_OK;
+  if (capacity < ntri) return WGPT_E_INVALID;
+  for (size_t t = 0; t < ntri; ++t) {
+    float* o = tris24 + t * 24;
+    for (int c = 0; c < 3; ++c) {
+      double ip = i32(fp[t * 3 + c]), in = i32(fn[t * 3 + c]), iu = i32(fu[t * 3 + c]);
+      for (int d = 0; d < 3; ++d) o[c * 3 + d] = js_at(P, ip * 3 + d);
+      for (int d = 0; d < 3; ++d) o[9 + c * 3 + d] = js_at(N, in * 3 + d);
+      for (int d = 0; d < 2; ++d) o[18 + c * 2 + d] = js_at(U, iu * 2 + d);
+    }
+  }
+  return WGPT_OK;
+}

@@ -326,8 +326,27 @@ class ModelData:
         self._node_offset = 0
         self._tri_offset = 0
 
+    @classmethod
+    def from_obj(cls, text, name: str = "New Model") -> "ModelData":
+        """Model.parseOBJ + generateTriangles (tracer.js:949-1021) of an OBJ file's text, parsed
+        natively (wgpt_parse_obj) with the reference's JavaScript number semantics."""
+        raw = text.encode() if isinstance(text, str) else bytes(text)
+        buf = np.frombuffer(raw, np.uint8) if raw else np.zeros(1, np.uint8)
+        L = lib()
+        nt, npos = C.c_uint32(0), C.c_uint32(0)
+        check(L.wgpt_parse_obj(ptr(buf), len(raw), None, 0, C.byref(nt), None, 0, C.byref(npos)), "parse_obj")
+        tris = np.zeros((nt.value, 24), np.float32)
+        pos = np.zeros(npos.value, np.float32)
+        check(L.wgpt_parse_obj(ptr(buf), len(raw), ptr(tris), nt.value, C.byref(nt), ptr(pos), npos.value,
+                               C.byref(npos)), "parse_obj")
+        m = cls(name, pos, np.zeros(0, np.float32), np.zeros(0, np.float32), np.zeros(0, np.int64))
+        m._tris24 = tris
+        return m
+
     def triangles24(self) -> np.ndarray:
         """generateTriangles (tracer.js:989-1021) as n x 24 float32 (v0 v1 v2 n0 n1 n2 uv0 uv1 uv2)."""
+        if getattr(self, "_tris24", None) is not None:
+            return self._tris24
         ip = self.index_positions.reshape(-1, 3)
         inn = self.index_normals.reshape(-1, 3)
         iuv = self.index_texcoords.reshape(-1, 3)

@@ -57,6 +57,14 @@ typedef struct wgpt_scene_desc {
   uint32_t sky_height;
   int32_t bounce_limit;     /* override constant 0 (BOUNCE_LIMIT) */
   uint32_t feature_flags;   /* override constants 1..11 as WGPT_HAS_* bits */
+  /* binding 11, texture_list (prepareTextureArray, tracer.js:1919-1953): tex_layers images of
+     tex_width x tex_height rgba8 texels, layer after layer (the reference resizes every texture
+     to 512 x 512); NULL / 0 when no material references a texture.  Sampled bilinearly with
+     repeat addressing (sampler of tracer.js:1965-1968) in FP32. */
+  const uint8_t* textures_rgba8;
+  uint32_t tex_width;
+  uint32_t tex_height;
+  uint32_t tex_layers;
 } wgpt_scene_desc;
 
 /* Renderer constructor + init() (tracer.js:1720-1770): binds CUDA device `device`. */

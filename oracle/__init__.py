@@ -44,6 +44,8 @@ def lib() -> C.CDLL:
         L.oracle_denoise.argtypes = [_P, _P, _P, _P, _U32, _P, _P, _P, C.c_int]
         L.oracle_resample.argtypes = [_P, _U32, _U32, _P, _U32, _U32, C.c_float, C.c_float]
         L.oracle_builtin.argtypes = [C.c_int, _P, _P, _U32, _P]
+        L.oracle_sample_texture.argtypes = [_P, _U32, _U32, _U32, C.c_int32, _P, _U32, _P]
+        L.oracle_sample_texture.restype = None
         for name in ("oracle_render", "oracle_gbuffer", "oracle_trace_closest", "oracle_bsdf", "oracle_denoise",
                      "oracle_resample"):
             getattr(L, name).restype = C.c_int
@@ -62,13 +64,15 @@ class OracleScene:
 
     def __init__(self, packed):
         self.packed = packed
+        tex = packed.textures if packed.textures is not None else np.zeros((1, 1, 1, 4), np.uint8)
         bufs = [packed.materials, packed.objects, packed.tlas, packed.meshes, packed.bvh, packed.triangles,
-                packed.planes, packed.lights, packed.sky_cdf, packed.sky]
+                packed.planes, packed.lights, packed.sky_cdf, packed.sky, tex]
         self._keep = [np.ascontiguousarray(b) for b in bufs]
-        self.ptrs = (C.c_void_p * 10)(*[b.ctypes.data for b in self._keep])
+        self.ptrs = (C.c_void_p * 11)(*[b.ctypes.data for b in self._keep])
         self.sizes = np.array([b.nbytes for b in self._keep], dtype=np.uint64)
-        self.meta = np.array([packed.sky_width, packed.sky_height, packed.bounce_limit, packed.flags],
-                             dtype=np.uint32)
+        layers = tex.shape[0] if packed.textures is not None else 0
+        self.meta = np.array([packed.sky_width, packed.sky_height, packed.bounce_limit, packed.flags,
+                              tex.shape[2], tex.shape[1], layers], dtype=np.uint32)
 
     def args(self):
         return (C.cast(self.ptrs, C.c_void_p), _p(self.sizes), _p(self.meta))
@@ -139,6 +143,15 @@ def builtin(op: int, x: np.ndarray, y: np.ndarray | None = None) -> np.ndarray:
     y = np.zeros_like(x) if y is None else np.ascontiguousarray(y, np.float32)
     out = np.empty_like(x)
     lib().oracle_builtin(op, _p(x), _p(y), x.size, _p(out))
+    return out
+
+
+def sample_texture(textures: np.ndarray, layer: int, uv: np.ndarray) -> np.ndarray:
+    """The material sampler on a (layers, H, W, 4) uint8 array at uv (n, 2); returns (n, 4) float32."""
+    tex = np.ascontiguousarray(textures, np.uint8)
+    uv = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    out = np.empty((uv.shape[0], 4), np.float32)
+    lib().oracle_sample_texture(_p(tex), tex.shape[2], tex.shape[1], tex.shape[0], layer, _p(uv), uv.shape[0], _p(out))
     return out
 
 

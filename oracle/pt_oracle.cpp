@@ -47,6 +47,7 @@ struct Scene {
   const wgpt_light* lights; uint32_t n_lights;
   const uint16_t* sky; uint32_t sky_w, sky_h;    // rgba16float texels
   const float* cdf; uint32_t n_cdf;
+  const uint8_t* tex; uint32_t tex_w, tex_h, tex_layers;   // texture_list, rgba8, layer-major
   int32_t bounce_limit;
   uint32_t flags;
 };
@@ -76,6 +77,7 @@ inline m4 load_m4(const float* f) {
   return r;
 }
 inline v3 L3(const float* f) { return mk3(f[0], f[1], f[2]); }
+inline v2 L2(const float* f) { return mk2(f[0], f[1]); }
 
 struct MeshInstance { m4 inv_matrix; int32_t material_idx; uint32_t node_offset, tri_offset; };
 
@@ -124,6 +126,18 @@ v3 sky_bilinear(Ctx& c, v2 uv) {
 }
 
 // shader.wgsl:176-188
+// sample_texture (shader.wgsl:170-173): layer idx of texture_list, vec4(1) for a negative index.
+v4 sample_texture(const Scene* s, int32_t idx, v2 uv) {
+  if (idx < 0) return mk4(1.0f, 1.0f, 1.0f, 1.0f);
+  const uint8_t* base = s->tex + (size_t)idx * s->tex_w * s->tex_h * 4;
+  const uint32_t w = s->tex_w;
+  auto fetch = [&](uint32_t x, uint32_t y) {
+    const uint8_t* t = base + ((size_t)y * w + x) * 4;
+    return (uint32_t)t[0] | ((uint32_t)t[1] << 8) | ((uint32_t)t[2] << 16) | ((uint32_t)t[3] << 24);
+  };
+  return sample_rgba8_repeat(fetch, s->tex_w, s->tex_h, uv);
+}
+
 v3 sample_sky(Ctx& c, v3 dir) {
   float phi = atan2_(dir.z, dir.x);
   float theta = asin_(clamp(dir.y, -1.0f, 1.0f));
@@ -655,10 +669,54 @@ SurfaceHit trace_scene(Ctx& c, const Ray& ray) {
 }
 
 // ------------------------------------------------------------------------ shadow rays
-// shader.wgsl:777-811: without an albedo texture any surface blocks fully.
-bool evaluate_shadow_attenuation(const wgpt_material& mat, v2 /*uv*/, float /*dist*/, v3* /*shadow*/) {
-  (void)mat;
-  return true;   // albedo_idx < 0 is enforced on upload
+// shader.wgsl:777-811: a surface without an albedo texture blocks fully; one with it lets
+// (1 - alpha) through and blocks once alpha exceeds 0.9999 (the distance is unused).
+// An occluder with material index -1 (read out of bounds by the WGSL, where the value is not
+// pinned) blocks like an untextured one.
+const wgpt_material* occluder_material(const Scene* s, int32_t idx) { return idx >= 0 ? &s->mats[idx] : nullptr; }
+
+bool evaluate_shadow_attenuation(const Scene* s, const wgpt_material* mat, v2 uv, float /*dist*/, v3* shadow) {
+  if (mat && mat->albedo_idx >= 0) {
+    v4 tex_color = sample_texture(s, mat->albedo_idx, uv * L2(mat->uv_scale));
+    *shadow = *shadow * (1.0f - tex_color.w);
+    if (tex_color.w > 0.9999f) return true;
+  } else {
+    return true;
+  }
+  return false;
+}
+
+// shader.wgsl:1090-1094
+v2 get_torus_uv(v3 p) {
+  float u = (atan2_(p.z, p.x) / TWO_PI) + 0.5f;
+  float v = (atan2_(p.y, length(mk2(p.x, p.z)) - 1.0f) / TWO_PI) + 0.5f;
+  return mk2(u, v);
+}
+
+// shader.wgsl:907-924
+v2 get_cube_uv(v3 local_hit) {
+  v3 d = vabs(local_hit);
+  float max_d = max_component(d);
+  if (max_d == d.x) {
+    float sg = sign(local_hit.x);
+    return mk2((-sg * local_hit.z) * 0.5f + 0.5f, local_hit.y * 0.5f + 0.5f);
+  } else if (max_d == d.y) {
+    float sg = sign(local_hit.y);
+    return mk2(local_hit.x * 0.5f + 0.5f, (sg * local_hit.z) * 0.5f + 0.5f);
+  }
+  float sg = sign(local_hit.z);
+  return mk2((sg * local_hit.x) * 0.5f + 0.5f, local_hit.y * 0.5f + 0.5f);
+}
+
+// shader.wgsl:958-962
+v2 get_frustum_uv(v3 p, float r0, float r1) {
+  if (p.y > 0.999f) return mk2(p.x / (r1 * 2.0f) + 0.5f, p.z / (r1 * 2.0f) + 0.5f);
+  if (p.y < 0.001f) return mk2(p.x / (r0 * 2.0f) + 0.5f, p.z / (r0 * 2.0f) + 0.5f);
+  return mk2(atan2_(p.z, p.x) / TWO_PI + 0.5f, p.y);
+}
+
+v2 sphere_uv(v3 p) {
+  return mk2(0.5f + atan2_(p.z, p.x) / TWO_PI, 0.5f + asin_(clamp(p.y, -1.0f, 1.0f)) / PI);
 }
 
 // shader.wgsl:813-872
@@ -677,7 +735,7 @@ bool trace_mesh_shadow(Ctx& c, const Ray& ray_world, const MeshInstance& mesh, f
   if (base_t < 0.0f || base_t >= target_dist) return false;
   float last_t = 0.0f;
   bool is_inside = false;
-  const wgpt_material& mat = s->mats[mesh.material_idx];
+  const wgpt_material* mat = occluder_material(s, mesh.material_idx);
   while (stack_ptr > 0) {
     stack_ptr--;
     c.count(C_NODES);
@@ -693,7 +751,7 @@ bool trace_mesh_shadow(Ctx& c, const Ray& ray_world, const MeshInstance& mesh, f
         if (intersect_triangle(ray_local, tri, &t_tri, &uv_tri, &bary)) {
           if (t_tri >= 0.0f && t_tri < target_dist) {
             float volume_dist = sel(0.0f, t_tri - last_t, is_inside);
-            if (evaluate_shadow_attenuation(mat, uv_tri, volume_dist, shadow)) return true;
+            if (evaluate_shadow_attenuation(s, mat, uv_tri, volume_dist, shadow)) return true;
             last_t = t_tri;
             is_inside = !is_inside;
           }
@@ -734,9 +792,11 @@ bool trace_sphere_shadow(Ctx& c, const Ray& ray_world, const wgpt_object& so, fl
   float h1 = wmax(0.001f, t1);
   float h2 = wmin(target_dist, t2);
   if (h1 < h2) {
-    const wgpt_material& mat = c.s->mats[so.material_idx];
-    if (evaluate_shadow_attenuation(mat, mk2(0.0f, 0.0f), 0.0f, shadow)) return true;
-    return evaluate_shadow_attenuation(mat, mk2(0.0f, 0.0f), h2 - h1, shadow);
+    const wgpt_material* mat = occluder_material(c.s, so.material_idx);
+    v3 p1 = local_ray.origin + local_ray.direction * h1;
+    if (evaluate_shadow_attenuation(c.s, mat, sphere_uv(p1), 0.0f, shadow)) return true;
+    v3 p2 = local_ray.origin + local_ray.direction * h2;
+    return evaluate_shadow_attenuation(c.s, mat, sphere_uv(p2), h2 - h1, shadow);
   }
   return false;
 }
@@ -757,9 +817,11 @@ bool trace_cube_shadow(Ctx& c, const Ray& ray_world, const wgpt_object& co, floa
   float h1 = wmax(0.001f, t1);
   float h2 = wmin(target_dist, t2);
   if (h1 < h2) {
-    const wgpt_material& mat = c.s->mats[co.material_idx];
-    if (evaluate_shadow_attenuation(mat, mk2(0.0f, 0.0f), 0.0f, shadow)) return true;
-    return evaluate_shadow_attenuation(mat, mk2(0.0f, 0.0f), h2 - h1, shadow);
+    const wgpt_material* mat = occluder_material(c.s, co.material_idx);
+    v3 p1 = local_ray.origin + local_ray.direction * h1;
+    if (evaluate_shadow_attenuation(c.s, mat, get_cube_uv(p1), 0.0f, shadow)) return true;
+    v3 p2 = local_ray.origin + local_ray.direction * h2;
+    return evaluate_shadow_attenuation(c.s, mat, get_cube_uv(p2), h2 - h1, shadow);
   }
   return false;
 }
@@ -799,9 +861,11 @@ bool trace_cylinder_shadow(Ctx& c, const Ray& ray_world, const wgpt_object& f, f
     float final_h1 = wmax(0.001f, h1);
     float final_h2 = wmin(target_dist, h2);
     if (final_h1 < final_h2) {
-      const wgpt_material& mat = c.s->mats[f.material_idx];
-      if (evaluate_shadow_attenuation(mat, mk2(0.0f, 0.0f), 0.0f, shadow)) return true;
-      return evaluate_shadow_attenuation(mat, mk2(0.0f, 0.0f), final_h2 - final_h1, shadow);
+      const wgpt_material* mat = occluder_material(c.s, f.material_idx);
+      v2 uv1 = get_frustum_uv(r.origin + r.direction * final_h1, 1.0f, top_radius);
+      if (evaluate_shadow_attenuation(c.s, mat, uv1, 0.0f, shadow)) return true;
+      v2 uv2 = get_frustum_uv(r.origin + r.direction * final_h2, 1.0f, top_radius);
+      return evaluate_shadow_attenuation(c.s, mat, uv2, final_h2 - final_h1, shadow);
     }
   }
   return false;
@@ -877,15 +941,17 @@ bool trace_torus_shadow(Ctx& c, const Ray& ray_world, const wgpt_object& tor, fl
   float E = K * K - 4.0f * R * R * (l_r.origin.x * l_r.origin.x + l_r.origin.z * l_r.origin.z);
   float roots[4];
   solve_quartic_real(B, C, D, E, roots);
-  const wgpt_material& mat = c.s->mats[tor.material_idx];
+  const wgpt_material* mat = occluder_material(c.s, tor.material_idx);
   for (int i = 0; i < 4; i += 2) {
     float t_near = roots[i]; float t_far = roots[i + 1];
     if (t_near < 0.0f || t_near > target_dist * ray_scale) continue;
     float h1 = wmax(0.001f, t_near) / ray_scale;
     float h2 = wmin(target_dist * ray_scale, t_far) / ray_scale;
     if (h1 < h2) {
-      if (evaluate_shadow_attenuation(mat, mk2(0.0f, 0.0f), 0.0f, shadow)) return true;
-      if (evaluate_shadow_attenuation(mat, mk2(0.0f, 0.0f), h2 - h1, shadow)) return true;
+      v2 uv1 = get_torus_uv(l_r.origin + l_r.direction * (h1 * ray_scale));
+      if (evaluate_shadow_attenuation(c.s, mat, uv1, 0.0f, shadow)) return true;
+      v2 uv2 = get_torus_uv(l_r.origin + l_r.direction * (h2 * ray_scale));
+      if (evaluate_shadow_attenuation(c.s, mat, uv2, h2 - h1, shadow)) return true;
     }
   }
   return false;
@@ -950,8 +1016,14 @@ bool trace_plane_shadow(Ctx& c, const Ray& ray, const wgpt_plane& p, float targe
   if (absf(denom) > 1e-6f) {
     float t = (p.d - dot(pn, ray.origin)) / denom;
     if (t > 0.001f && t < target_dist) {
-      const wgpt_material& mat = c.s->mats[p.material_idx];
-      return evaluate_shadow_attenuation(mat, mk2(0.0f, 0.0f), 0.0f, shadow);
+      v3 hit_pos = ray.origin + ray.direction * t;
+      const wgpt_material* mat = occluder_material(c.s, p.material_idx);
+      v3 tangent = mk3(1.0f, 0.0f, 0.0f);
+      if (absf(pn.x) > 0.9999f) tangent = mk3(0.0f, 0.0f, 1.0f);
+      tangent = normalize(cross(pn, tangent));
+      v3 bitangent = normalize(cross(pn, tangent));
+      v2 uv = mk2(dot(hit_pos, tangent), dot(hit_pos, bitangent));
+      return evaluate_shadow_attenuation(c.s, mat, uv, length(ray.origin - hit_pos), shadow);
     }
   }
   return false;
@@ -981,16 +1053,34 @@ v3 trace_scene_shadow(Ctx& c, const Ray& ray, int32_t target_idx, float target_d
 // ------------------------------------------------------------------------ shading
 struct SurfaceContext { v3 normal, surface_normal, albedo; float roughness, metallic; v3 emittance; float alpha; };
 
-// shader.wgsl:1393-1440 with every texture index negative
-SurfaceContext get_surface_context(const SurfaceHit& hit, const wgpt_material& mat) {
+// shader.wgsl:1393-1440
+SurfaceContext get_surface_context(const Scene* s, const SurfaceHit& hit, const wgpt_material& mat, const m3& tbn,
+                                   v2 uv) {
   SurfaceContext ctx;
   ctx.normal = hit.hit_n;
   ctx.surface_normal = hit.hit_n;
+  if (mat.normal_idx >= 0) {
+    v4 t = sample_texture(s, mat.normal_idx, uv);
+    v3 n_map = mk3(t.x, t.y, t.z) * 2.0f - mk3s(1.0f);
+    n_map = normalize(n_map * mk3(mat.height_params[0], mat.height_params[0], 1.0f));
+    ctx.normal = normalize(mul3(tbn, n_map));
+  }
   ctx.albedo = L3(mat.color);
   ctx.alpha = 1.0f;
+  if (mat.albedo_idx >= 0) {
+    v4 tex_color = sample_texture(s, mat.albedo_idx, uv);
+    ctx.alpha = tex_color.w;
+    ctx.albedo = ctx.albedo * vpow(mk3(tex_color.x, tex_color.y, tex_color.z), 2.2f);
+  }
   ctx.metallic = mat.metallic;
   ctx.roughness = mat.roughness;
+  if (mat.roughness_idx >= 0) ctx.roughness *= sample_texture(s, mat.roughness_idx, uv).y;
+  if (mat.metallic_idx >= 0) ctx.metallic *= sample_texture(s, mat.metallic_idx, uv).z;
   ctx.emittance = L3(mat.emittance);
+  if (mat.emissive_idx >= 0) {
+    v4 e = sample_texture(s, mat.emissive_idx, uv);
+    ctx.emittance = ctx.emittance * vpow(mk3(e.x, e.y, e.z), 2.2f);
+  }
   return ctx;
 }
 
@@ -1559,7 +1649,10 @@ void main_pixel(Ctx& c, uint32_t ix, uint32_t iy, float* accum, uint8_t* out) {
     }
     c.count(C_SHADE);
     const wgpt_material& mat = s->mats[hit.m_idx];
-    SurfaceContext ctx = get_surface_context(hit, mat);
+    // shader.wgsl:2361-2375 (the POM branch needs HAS_HEIGHTMAPS, which is rejected on upload)
+    v2 final_uv = hit.hit_uv * L2(mat.uv_scale);
+    m3 tbn; tbn.c[0] = hit.tangent; tbn.c[1] = hit.bitangent; tbn.c[2] = hit.hit_n;
+    SurfaceContext ctx = get_surface_context(s, hit, mat, tbn, final_uv);
     if (length(ctx.emittance) > 0.0f) {
       float weight = 1.0f;
       if (HAS(s, WGPT_HAS_LIGHTS) && bounce > 0 && hit.o_idx >= 0 && obj.light_idx >= 0) {
@@ -1661,7 +1754,9 @@ void gbuf_pixel(Ctx& c, uint32_t ix, uint32_t iy, float* gbuf, uint8_t* out) {
       break;
     }
     mat = s->mats[hit.m_idx];
-    ctx = get_surface_context(hit, mat);
+    m3 tbn; tbn.c[0] = hit.tangent; tbn.c[1] = hit.bitangent; tbn.c[2] = hit.hit_n;
+    v2 final_uv = hit.hit_uv * L2(mat.uv_scale);
+    ctx = get_surface_context(s, hit, mat, tbn, final_uv);
     ctx.normal = vsel(-ctx.normal, ctx.normal, dot(ctx.normal, -ray.direction) > 0.0f);
     dist += hit.t;
     if (ctx.alpha < 1.0f) {
@@ -1717,6 +1812,8 @@ void fill_scene(Scene* s, const void* const* bufs, const uint64_t* sizes, const 
   s->sky_w = meta[0]; s->sky_h = meta[1];
   s->bounce_limit = (int32_t)meta[2];
   s->flags = meta[3];
+  s->tex = (const uint8_t*)bufs[10];
+  s->tex_w = meta[4]; s->tex_h = meta[5]; s->tex_layers = meta[6];
 }
 
 // denoiser.wgsl:41-50
@@ -2028,6 +2125,19 @@ int oracle_resample(const uint8_t* src, uint32_t src_w, uint32_t src_h, uint8_t*
 
 // Elementary-function probe for the accuracy tests: op 0 sin, 1 cos, 2 exp, 3 log, 4 exp2, 5 log2,
 // 6 atan2(x, y2), 7 asin, 8 acos, 9 pow(x, y2).
+// textureSampleLevel of layer `layer` of an rgba8 array (w x h x layers) at n texture
+// coordinates uv (2 floats each); out: 4 floats each.
+void oracle_sample_texture(const uint8_t* tex, uint32_t w, uint32_t h, uint32_t layers, int32_t layer,
+                           const float* uv, uint32_t n, float* out) {
+  Scene s;
+  memset(&s, 0, sizeof s);
+  s.tex = tex; s.tex_w = w; s.tex_h = h; s.tex_layers = layers;
+  for (uint32_t i = 0; i < n; ++i) {
+    v4 c = sample_texture(&s, layer, mk2(uv[2 * i], uv[2 * i + 1]));
+    out[4 * i] = c.x; out[4 * i + 1] = c.y; out[4 * i + 2] = c.z; out[4 * i + 3] = c.w;
+  }
+}
+
 void oracle_builtin(int op, const float* x, const float* y2, uint32_t n, float* out) {
   for (uint32_t i = 0; i < n; ++i) {
     float v = x[i];

@@ -69,13 +69,18 @@ def test_validate_accepts_generated_scenes_and_rejects_bad_indices():
     bad.objects = ob.view(np.uint8).reshape(-1).copy()
     d = _desc(bad)
     assert L.wgpt_validate_scene(C.byref(d), msg, 256) == 2
-    # textures are not part of this build
+    # a texture index beyond the texture array (here: no array at all) is a layout error
     bad = sc.PackedScene(**{**p.__dict__})
     mt = p.materials.copy().view(np.int32).reshape(-1, 36)
     mt[0, 24] = 0                    # albedo_idx
     bad.materials = mt.view(np.uint8).reshape(-1).copy()
     d = _desc(bad)
-    assert L.wgpt_validate_scene(C.byref(d), msg, 256) == 6
+    assert L.wgpt_validate_scene(C.byref(d), msg, 256) == 2
+    assert b"texture index" in msg.value
+    # ... and accepted once the array has that layer
+    bad.textures = np.zeros((1, 8, 8, 4), np.uint8)
+    d = _desc(bad)
+    assert L.wgpt_validate_scene(C.byref(d), msg, 256) == 0, msg.value
     # parallax maps are not part of this build
     bad = sc.PackedScene(**{**p.__dict__})
     bad.flags = p.flags | _lib.HAS_HEIGHTMAPS

@@ -45,6 +45,8 @@ class SceneDesc(C.Structure):
         ("triangles", Buffer), ("planes", Buffer), ("lights", Buffer), ("sky_cdf", Buffer),
         ("sky_rgba16f", C.c_void_p), ("sky_width", C.c_uint32), ("sky_height", C.c_uint32),
         ("bounce_limit", C.c_int32), ("feature_flags", C.c_uint32),
+        ("textures_rgba8", C.c_void_p), ("tex_width", C.c_uint32), ("tex_height", C.c_uint32),
+        ("tex_layers", C.c_uint32),
     ]
 
 

@@ -18,10 +18,10 @@ struct wgpt_ctx {
   cudaStream_t stream = nullptr;
   std::string err;
   // scene buffers: 0 materials, 1 objects, 2 tlas, 3 meshes, 4 bvh, 5 triangles, 6 planes,
-  // 7 lights, 8 sky_cdf, 9 sky texels
-  void* d_buf[10] = {nullptr};
-  size_t cap[10] = {0};
-  size_t bytes[10] = {0};
+  // 7 lights, 8 sky_cdf, 9 sky texels, 10 texture array
+  void* d_buf[11] = {nullptr};
+  size_t cap[11] = {0};
+  size_t bytes[11] = {0};
   wgpt::DeviceScene ds{};
   bool has_scene = false;
   // images
@@ -86,10 +86,10 @@ void dfree_t(T*& p) {
   p = nullptr;
 }
 
-const uint32_t kStride[10] = {WGPT_STRIDE_MATERIAL, WGPT_STRIDE_OBJECT, WGPT_STRIDE_NODE, WGPT_STRIDE_MESH_READ,
-                              WGPT_STRIDE_NODE, WGPT_STRIDE_TRIANGLE, WGPT_STRIDE_PLANE, WGPT_STRIDE_LIGHT, 4, 8};
-const char* kName[10] = {"materials", "objects", "tlas", "meshes", "bvh", "triangles", "planes", "lights",
-                         "sky_cdf", "sky"};
+const uint32_t kStride[11] = {WGPT_STRIDE_MATERIAL, WGPT_STRIDE_OBJECT, WGPT_STRIDE_NODE, WGPT_STRIDE_MESH_READ,
+                              WGPT_STRIDE_NODE, WGPT_STRIDE_TRIANGLE, WGPT_STRIDE_PLANE, WGPT_STRIDE_LIGHT, 4, 8, 4};
+const char* kName[11] = {"materials", "objects", "tlas", "meshes", "bvh", "triangles", "planes", "lights",
+                         "sky_cdf", "sky", "textures"};
 
 struct HostScene {
   const wgpt_material* mats; uint32_t n_mats;
@@ -100,6 +100,7 @@ struct HostScene {
   const wgpt_triangle* tris; uint32_t n_tris;
   const wgpt_plane* planes; uint32_t n_planes;
   const wgpt_light* lights; uint32_t n_lights;
+  uint32_t tex_layers;
 };
 
 constexpr uint32_t kMaxDepth = 62;   // traversal stacks hold 64 entries (shader.wgsl:17)
@@ -145,11 +146,13 @@ std::string validate(const HostScene& s, uint32_t flags, std::set<std::pair<uint
   if (s.n_mats == 0) return "materials: at least one material record is required";
   for (uint32_t i = 0; i < s.n_mats; ++i) {
     const wgpt_material& m = s.mats[i];
-    if (m.emissive_idx >= 0 || m.albedo_idx >= 0 || m.normal_idx >= 0 || m.height_idx >= 0 ||
-        m.roughness_idx >= 0 || m.metallic_idx >= 0) {
-      snprintf(buf, sizeof buf, "materials[%u]: texture indices are not supported by this build", i);
-      return std::string("U") + buf;
-    }
+    const int32_t idx[6] = {m.emissive_idx, m.albedo_idx, m.normal_idx, m.height_idx, m.roughness_idx, m.metallic_idx};
+    for (int32_t t : idx)
+      if (t >= 0 && (uint32_t)t >= s.tex_layers) {
+        snprintf(buf, sizeof buf, "materials[%u]: texture index %d beyond the %u layers of the texture array", i, t,
+                 s.tex_layers);
+        return buf;
+      }
   }
   auto mat_ok = [&](int32_t m) { return m >= -1 && m < (int32_t)s.n_mats; };
   auto blas_ok = [&](uint32_t node_offset, uint32_t tri_offset, const char* what) -> std::string {
@@ -265,9 +268,10 @@ int upload_buffers(wgpt_ctx* ctx, const wgpt_scene_desc* d, bool in_place_only) 
   const wgpt_buffer* src[9] = {&d->materials, &d->objects, &d->tlas, &d->meshes, &d->bvh,
                                &d->triangles, &d->planes, &d->lights, &d->sky_cdf};
   size_t sky_bytes = (size_t)d->sky_width * d->sky_height * 8;
-  for (int k = 0; k < 10; ++k) {
-    const void* p = k < 9 ? src[k]->ptr : (const void*)d->sky_rgba16f;
-    size_t n = k < 9 ? src[k]->bytes : sky_bytes;
+  const size_t tex_bytes = d->textures_rgba8 ? (size_t)d->tex_width * d->tex_height * d->tex_layers * 4 : 0;
+  for (int k = 0; k < 11; ++k) {
+    const void* p = k < 9 ? src[k]->ptr : k == 9 ? (const void*)d->sky_rgba16f : (const void*)d->textures_rgba8;
+    size_t n = k < 9 ? src[k]->bytes : k == 9 ? sky_bytes : tex_bytes;
     if (n == 0 || p == nullptr) {
       // empty arrays are bound as one zeroed element (tracer.js:1789, makeBuf minimum sizes)
       n = kStride[k];
@@ -309,6 +313,10 @@ int check_desc(wgpt_ctx* ctx, const wgpt_scene_desc* d, HostScene& hs) {
   if (d->feature_flags & ~0x7ffu) return fail(ctx, WGPT_E_INVALID, "unknown feature flag bits");
   if ((d->feature_flags & WGPT_HAS_SKYBOX) && (!d->sky_rgba16f || d->sky_width == 0 || d->sky_height == 0))
     return fail(ctx, WGPT_E_INVALID, "sky texture missing while HAS_SKYBOX is set");
+  if (d->textures_rgba8 && (d->tex_width == 0 || d->tex_height == 0 || d->tex_layers == 0 ||
+                            (uint64_t)d->tex_width * d->tex_height * d->tex_layers > (1ull << 30)))
+    return fail(ctx, WGPT_E_INVALID, "texture array size must be nonzero and at most 2^30 texels");
+  hs.tex_layers = d->textures_rgba8 ? d->tex_layers : 0u;
   auto cnt = [&](int k) { return (uint32_t)(b[k]->bytes / kStride[k]); };
   hs.mats = (const wgpt_material*)b[0]->ptr; hs.n_mats = cnt(0);
   hs.objs = (const wgpt_object*)b[1]->ptr; hs.n_objs = cnt(1);
@@ -342,8 +350,20 @@ void fill_device_scene(wgpt_ctx* ctx, const wgpt_scene_desc* d) {
   s.sky = ctx->d_buf[9];
   s.sky_w = d->sky_rgba16f ? d->sky_width : 1u;
   s.sky_h = d->sky_rgba16f ? d->sky_height : 1u;
+  s.tex = ctx->d_buf[10];
+  s.tex_w = d->textures_rgba8 ? d->tex_width : 1u;
+  s.tex_h = d->textures_rgba8 ? d->tex_height : 1u;
+  s.tex_layers = d->textures_rgba8 ? d->tex_layers : 0u;
   s.bounce_limit = d->bounce_limit;
   s.flags = d->feature_flags;
+  const wgpt_material* m = (const wgpt_material*)d->materials.ptr;
+  for (uint32_t i = 0; i < (uint32_t)(d->materials.bytes / WGPT_STRIDE_MATERIAL); ++i) {
+    if (m[i].emissive_idx >= 0 || m[i].albedo_idx >= 0 || m[i].normal_idx >= 0 || m[i].roughness_idx >= 0 ||
+        m[i].metallic_idx >= 0)
+      s.flags |= wgpt::SCENE_TEXTURED;
+    if (m[i].albedo_idx >= 0) s.flags |= wgpt::SCENE_ALPHA_SHADOWS;
+    if (m[i].normal_idx >= 0) s.flags |= wgpt::SCENE_NORMAL_MAPS;
+  }
 }
 
 int check_section(wgpt_ctx* ctx, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh) {
@@ -424,7 +444,7 @@ int wgpt_destroy(wgpt_ctx* ctx) {
   if (!ctx) return WGPT_E_INVALID;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  for (int k = 0; k < 10; ++k) dfree(ctx->d_buf[k]);
+  for (int k = 0; k < 11; ++k) dfree(ctx->d_buf[k]);
   dfree_t(ctx->accum); dfree_t(ctx->out); dfree_t(ctx->gbuf);
   dfree_t(ctx->dn_a); dfree_t(ctx->dn_b); dfree_t(ctx->dn_guide); dfree_t(ctx->dn_comp);
   dfree_t(ctx->canvas); dfree_t(ctx->d_status); dfree_t(ctx->d_counters); wgpt::wf_engine_destroy(ctx->wf);
@@ -476,7 +496,7 @@ int wgpt_update_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   if (!ctx) return WGPT_E_INVALID;
   if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-  if (desc && (desc->feature_flags != ctx->ds.flags || desc->bounce_limit != ctx->ds.bounce_limit))
+  if (desc && (desc->feature_flags != (ctx->ds.flags & 0x7ffu) || desc->bounce_limit != ctx->ds.bounce_limit))
     return fail(ctx, WGPT_E_REBUILD, "pipeline constants changed: full upload required");
   HostScene hs;
   int rc = check_desc(ctx, desc, hs);

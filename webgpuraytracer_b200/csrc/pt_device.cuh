@@ -15,6 +15,7 @@
 #include <cuda_fp16.h>
 #include "wgsl_builtins.h"
 #include "../../include/wgpt_layout.h"
+#include "wgpt_internal.h"
 
 namespace pt {
 
@@ -45,8 +46,9 @@ struct DScene {
   const float4* lights; uint32_t n_lights; // 5 x float4
   const uint2* sky; uint32_t sky_w, sky_h; // rgba16f texel = 8 bytes
   const float* cdf; uint32_t n_cdf;
+  const uint32_t* tex; uint32_t tex_w, tex_h;   // rgba8 texture array, one 32-bit texel per entry
   int32_t bounce_limit;
-  uint32_t flags;
+  uint32_t flags;   // WGPT_HAS_* plus the wgpt::SCENE_* bits derived from the materials
 };
 
 struct DParams {
@@ -73,6 +75,10 @@ struct Counters {
 };
 
 static __device__ __forceinline__ bool HAS(const DScene& s, uint32_t f) { return (s.flags & f) != 0u; }
+// A texture feature bit (wgpt::SCENE_*) in code instantiated with texture support (TEX); the
+// untextured instantiations compile the texture paths out.
+template <bool TEX>
+static __device__ __forceinline__ bool HAS_TEX(const DScene& s, uint32_t f) { return TEX && HAS(s, f); }
 static __device__ __forceinline__ float4 ld4(const float4* p) { return __ldg(p); }
 static __device__ __forceinline__ v3 f3(float4 a) { return mk3(a.x, a.y, a.z); }
 static __device__ __forceinline__ int32_t bi(float f) { return __float_as_int(f); }
@@ -106,6 +112,27 @@ static __device__ __forceinline__ DMat load_mat(const DScene& s, int32_t i) {
 }
 static __device__ __forceinline__ v3 load_mat_emittance(const DScene& s, int32_t i) {
   return f3(ld4(s.mats + (size_t)i * 9 + 5));
+}
+
+// Texture fields of a material record (words 23-35 of the 144-byte record).
+struct DMatTex { int32_t emissive, albedo, normal, roughness, metallic; v2 uv_scale; float height0; };
+static __device__ __forceinline__ DMatTex load_mat_tex(const DScene& s, int32_t i) {
+  const float4* p = s.mats + (size_t)i * 9;
+  float4 f = ld4(p + 5), g = ld4(p + 6), h = ld4(p + 7), k = ld4(p + 8);
+  DMatTex t;
+  t.emissive = bi(f.w); t.albedo = bi(g.x); t.normal = bi(g.y); t.roughness = bi(g.w); t.metallic = bi(h.x);
+  t.uv_scale = mk2(h.z, h.w); t.height0 = k.x;
+  return t;
+}
+
+// sample_texture (shader.wgsl:170-173): layer idx of the material texture array sampled with the
+// linear, repeating sampler; vec4(1) for a negative index.
+static __device__ __forceinline__ v4 sample_texture(const DScene& s, int32_t idx, v2 uv) {
+  if (idx < 0) return mk4(1.0f, 1.0f, 1.0f, 1.0f);
+  const uint32_t w = s.tex_w;
+  const uint32_t* base = s.tex + (size_t)idx * w * s.tex_h;
+  auto fetch = [&](uint32_t x, uint32_t y) { return __ldg(base + (size_t)y * w + x); };
+  return sample_rgba8_repeat(fetch, w, s.tex_h, uv);
 }
 
 // ------------------------------------------------------------------------ sky and env CDF
@@ -194,10 +221,14 @@ struct Ray { v3 origin, direction; };
 
 // Closest hit record.  kind: 0 none, 1 plane (id = plane), 2 TLAS mesh triangle (id = triangle),
 // 3 analytic TLAS object, 4 list-mesh triangle (id = triangle, aux = list index).
+// tsrc/tsrc_t: the last plane (-2 - plane), sphere or cube (object index) accepted as the closest
+// candidate and its distance, -1 when none was: the source of the tangent frame the reference
+// leaves in SurfaceHit (triangles, cylinders and tori do not write one).
 struct HitRec {
   float t; int32_t m_idx; int32_t o_idx;
   int32_t kind; int32_t id; int32_t aux;
   float bu, bv;   // barycentrics (u, v) of a triangle hit
+  int32_t tsrc; float tsrc_t;
 };
 
 // shader.wgsl:256-265.  IEEE fminf/fmaxf: the sign of a zero result can differ from WGSL's
@@ -255,8 +286,11 @@ static __device__ __forceinline__ float hit_unit_cube(const Ray& r) {
   return -1.0f;
 }
 
-// shader.wgsl:323-379
-static __device__ __noinline__ bool hit_cylinder(const Ray& r, float r0, float r1, float* t_out, v3* n_out) {
+// shader.wgsl:323-379; UV also returns the texture coordinate of the hit (side: angle and
+// height, caps: planar in units of the larger diameter).
+template <bool UV>
+static __device__ __noinline__ bool hit_cylinder(const Ray& r, float r0, float r1, float* t_out, v3* n_out,
+                                                 v2* uv_out) {
   float h = 1.0f;
   float dr = r1 - r0;
   float k = dr / h;
@@ -280,6 +314,7 @@ static __device__ __noinline__ bool hit_cylinder(const Ray& r, float r0, float r
         v3 p = r.origin + t * r.direction;
         float slant = -k * (r0 + k * y);
         *n_out = normalize(mk3(p.x, slant, p.z));
+        if (UV) *uv_out = mk2(atan2_(p.z, p.x) / TWO_PI + 0.5f, y);
         hit = true;
       }
     }
@@ -294,6 +329,10 @@ static __device__ __noinline__ bool hit_cylinder(const Ray& r, float r0, float r
       if (p.x * p.x + p.z * p.z <= rad * rad) {
         t_min = t;
         *n_out = mk3(0.0f, (float)i * 2.0f - 1.0f, 0.0f);
+        if (UV) {
+          float den = wmax(r0, r1) * 2.0f;
+          *uv_out = mk2(p.x / den + 0.5f, p.z / den + 0.5f);
+        }
         hit = true;
       }
     }
@@ -450,7 +489,7 @@ static __device__ __forceinline__ bool analytic_t(const m4& inv, const ObjHdr& h
   if (h.type == 2) { float t = hit_unit_cube(rl); *t_out = t; return t > 0.001f; }
   if (h.type == 3) {
     float t; v3 n;
-    if (hit_cylinder(rl, 1.0f, h.param0, &t, &n)) { *t_out = t; return true; }
+    if (hit_cylinder<false>(rl, 1.0f, h.param0, &t, &n, nullptr)) { *t_out = t; return true; }
     return false;
   }
   float ray_scale = length(rl.direction);
@@ -466,6 +505,7 @@ static __device__ HitRec trace_scene(const DScene& s, const Ray& ray, uint32_t& 
   cn.add(C_RAYS_EXT);
   HitRec hit;
   hit.t = 1e10f; hit.m_idx = -1; hit.o_idx = -1; hit.kind = 0; hit.id = -1; hit.aux = -1; hit.bu = 0.0f; hit.bv = 0.0f;
+  hit.tsrc = -1; hit.tsrc_t = 0.0f;
   if (HAS(s, WGPT_HAS_PLANES)) {
     for (uint32_t i = 0; i < s.n_planes; i++) {
       float4 a = ld4(s.planes + (size_t)i * 2);
@@ -477,7 +517,10 @@ static __device__ HitRec trace_scene(const DScene& s, const Ray& ray, uint32_t& 
         float tt = (a.w - dot(pn, ray.origin)) / denom;
         if (tt > 0.001f) t = tt;
       }
-      if (t > 0.001f && t < hit.t) { hit.t = t; hit.m_idx = bi(b.x); hit.kind = 1; hit.id = (int32_t)i; }
+      if (t > 0.001f && t < hit.t) {
+        hit.t = t; hit.m_idx = bi(b.x); hit.kind = 1; hit.id = (int32_t)i;
+        hit.tsrc = -2 - (int32_t)i; hit.tsrc_t = t;
+      }
     }
   }
   if (HAS(s, WGPT_HAS_SPHERES | WGPT_HAS_CUBES | WGPT_HAS_CYLINDERS | WGPT_HAS_TORI | WGPT_HAS_MESHES)) {
@@ -507,7 +550,10 @@ static __device__ HitRec trace_scene(const DScene& s, const Ray& ray, uint32_t& 
               trace_mesh<COUNT>(s, ray, inv, bu(h.param0), bu(h.param1), h.material_idx, (int32_t)i, 2, -1, hit, err, cn);
             } else {
               float t = 0.0f;
-              if (analytic_t(inv, h, ray, &t) && t < hit.t) { hit.t = t; hit.m_idx = h.material_idx; hit.o_idx = (int32_t)i; hit.kind = 3; hit.id = (int32_t)i; }
+              if (analytic_t(inv, h, ray, &t) && t < hit.t) {
+                hit.t = t; hit.m_idx = h.material_idx; hit.o_idx = (int32_t)i; hit.kind = 3; hit.id = (int32_t)i;
+                if (h.type <= 2) { hit.tsrc = (int32_t)i; hit.tsrc_t = t; }
+              }
             }
           }
         } else {
@@ -573,7 +619,7 @@ static __device__ __noinline__ v3 hit_normal(const DScene& s, const Ray& rw, con
   }
   if (h.type == 3) {
     float t; v3 n = mk3s(0.0f);
-    hit_cylinder(rl, 1.0f, h.param0, &t, &n);
+    hit_cylinder<false>(rl, 1.0f, h.param0, &t, &n, nullptr);
     return normalize(mul3(n_mat, n));
   }
   // torus: the reference multiplies by mat3(inv) without the transpose (shader.wgsl:681)
@@ -586,13 +632,163 @@ static __device__ __noinline__ v3 hit_normal(const DScene& s, const Ray& rw, con
   return normalize(mul3(upper3(inv), local_n));
 }
 
+// ------------------------------------------------------------------------ texture coordinates
+// Tangent and bitangent of a plane with normal pn (shader.wgsl:630-633 with thresh 0.9 for the
+// closest hit; 1197-1200 with 0.9999 for shadow rays).
+static __device__ __forceinline__ void plane_frame(v3 pn, float thresh, v3* T, v3* B) {
+  v3 tangent = absf(pn.x) > thresh ? mk3(0.0f, 0.0f, 1.0f) : mk3(1.0f, 0.0f, 0.0f);
+  *T = normalize(cross(pn, tangent));
+  *B = normalize(cross(pn, *T));
+}
+
+// Face frame and texture coordinate of a point on the unit cube (shader.wgsl:590-608, 907-924).
+static __device__ __forceinline__ void cube_face(v3 lh, v3* lt, v3* lb, v2* uv) {
+  v3 d = vabs(lh);
+  float max_d = max_component(d);
+  if (max_d == d.x) {
+    float sg = sign(lh.x);
+    *lt = mk3(0.0f, 0.0f, -sg); *lb = mk3(0.0f, 1.0f, 0.0f);
+    *uv = mk2((-sg * lh.z) * 0.5f + 0.5f, lh.y * 0.5f + 0.5f);
+  } else if (max_d == d.y) {
+    float sg = sign(lh.y);
+    *lt = mk3(1.0f, 0.0f, 0.0f); *lb = mk3(0.0f, 0.0f, sg);
+    *uv = mk2(lh.x * 0.5f + 0.5f, (sg * lh.z) * 0.5f + 0.5f);
+  } else {
+    float sg = sign(lh.z);
+    *lt = mk3(sg, 0.0f, 0.0f); *lb = mk3(0.0f, 1.0f, 0.0f);
+    *uv = mk2((sg * lh.x) * 0.5f + 0.5f, lh.y * 0.5f + 0.5f);
+  }
+}
+
+// Texture coordinate of a point on the unit sphere (shader.wgsl:556-558, 893-899).
+static __device__ __forceinline__ v2 sphere_uv(v3 p) {
+  return mk2(0.5f + atan2_(p.z, p.x) / TWO_PI, 0.5f + asin_(clamp(p.y, -1.0f, 1.0f)) / PI);
+}
+
+// Texture coordinate of a point on the torus (shader.wgsl:684-686, 1090-1094).
+static __device__ __forceinline__ v2 torus_uv(v3 p) {
+  float u = (atan2_(p.z, p.x) / TWO_PI) + 0.5f;
+  float v = (atan2_(p.y, length2(mk2(p.x, p.z)) - 1.0f) / TWO_PI) + 0.5f;
+  return mk2(u, v);
+}
+
+// The closest hit's texture coordinate (SurfaceHit.hit_uv, before the material's uv scale) and
+// the tangent frame the reference leaves beside it: the frame of the candidate hit.tsrc names,
+// recomputed at its distance, or zero vectors.
+struct UvFrame { v2 uv; v3 T, B; };
+static __device__ __noinline__ UvFrame hit_uv_frame(const DScene& s, const Ray& rw, const HitRec& hit) {
+  UvFrame f;
+  f.uv = mk2(0.0f, 0.0f);
+  if (hit.kind == 1) {
+    v3 pn = f3(ld4(s.planes + (size_t)hit.id * 2));
+    v3 T, B;
+    plane_frame(pn, 0.9f, &T, &B);
+    v3 hp = rw.origin + rw.direction * hit.t;
+    f.uv = mk2(dot(hp, T), dot(hp, B));
+  } else if (hit.kind == 2 || hit.kind == 4) {
+    const float4* tp = s.tris + (size_t)hit.id * 8;
+    float4 a = ld4(tp + 6), b = ld4(tp + 7);
+    float u = hit.bu, v = hit.bv;
+    v3 bary = mk3(1.0f - u - v, u, v);
+    f.uv = (mk2(a.x, a.y) * bary.x + mk2(a.z, a.w) * bary.y) + mk2(b.x, b.y) * bary.z;
+  } else if (hit.kind == 3) {
+    ObjHdr h = load_obj_hdr(s, (uint32_t)hit.o_idx);
+    m4 inv = load_m4(s.objs + (size_t)hit.o_idx * 6);
+    Ray rl = to_local(inv, rw);
+    if (h.type == 1) {
+      f.uv = sphere_uv(rl.origin + rl.direction * hit.t);
+    } else if (h.type == 2) {
+      v3 lt, lb;
+      cube_face(rl.origin + rl.direction * hit.t, &lt, &lb, &f.uv);
+    } else if (h.type == 3) {
+      float t; v3 n;
+      hit_cylinder<true>(rl, 1.0f, h.param0, &t, &n, &f.uv);
+    } else {
+      float ray_scale = length(rl.direction);
+      rl.direction = rl.direction / ray_scale;
+      float tl = hit_torus(rl, 1.0f, h.param0 * 1.0f);
+      f.uv = torus_uv(rl.origin + rl.direction * tl);
+    }
+  }
+  f.T = mk3s(0.0f);
+  f.B = mk3s(0.0f);
+  if (hit.tsrc <= -2) {
+    plane_frame(f3(ld4(s.planes + (size_t)(-2 - hit.tsrc) * 2)), 0.9f, &f.T, &f.B);
+  } else if (hit.tsrc >= 0) {
+    ObjHdr h = load_obj_hdr(s, (uint32_t)hit.tsrc);
+    m4 inv = load_m4(s.objs + (size_t)hit.tsrc * 6);
+    Ray rl = to_local(inv, rw);
+    v3 lp = rl.origin + rl.direction * hit.tsrc_t;
+    v3 lt, lb;
+    if (h.type == 1) {
+      lt = absf(lp.y) > 0.9999f ? mk3(1.0f, 0.0f, 0.0f) : mk3(-lp.z, 0.0f, lp.x);
+      lt = normalize(lt);
+      lb = cross(lp, lt);
+    } else {
+      v2 uv;
+      cube_face(lp, &lt, &lb, &uv);
+    }
+    m3 n_mat = transpose3(upper3(inv));
+    f.T = normalize(mul3(n_mat, lt));
+    f.B = normalize(mul3(n_mat, lb));
+  }
+  return f;
+}
+
 // ------------------------------------------------------------------------ shadow rays
-// Any surface without an albedo texture blocks completely (shader.wgsl:777-811), so every
-// shadow test reduces to "is anything hit in (0.001, target_dist)" with the reference's interval
-// rules per primitive.
-template <bool COUNT>
-static __device__ bool mesh_occludes(const DScene& s, const Ray& rw, const m4& inv_m, uint32_t node_offset,
-                              uint32_t tri_offset, float target_dist, uint32_t& err, Counters<COUNT>& cn) {
+// Shadow rays carry a transmittance: a surface without an albedo texture blocks completely; one
+// with it lets (1 - alpha) through at every crossing and blocks once alpha exceeds 0.9999
+// (evaluate_shadow_attenuation, shader.wgsl:777-811).  The crossings are taken in the
+// reference's order (planes, TLAS traversal, list meshes; entry before exit), so the product
+// is rounded the same way.  Without albedo textures in the scene every crossing blocks and no
+// material or texture coordinate is read.
+struct OccMat { int32_t albedo; v2 uv_scale; };
+template <bool TEX>
+static __device__ __forceinline__ OccMat occ_mat(const DScene& s, int32_t m) {
+  OccMat o;
+  o.albedo = -1;
+  o.uv_scale = mk2(0.0f, 0.0f);
+  if (HAS_TEX<TEX>(s, wgpt::SCENE_ALPHA_SHADOWS) && m >= 0) {
+    float4 g = ld4(s.mats + (size_t)m * 9 + 6), h = ld4(s.mats + (size_t)m * 9 + 7);
+    o.albedo = bi(g.x);
+    o.uv_scale = mk2(h.z, h.w);
+  }
+  return o;
+}
+// One crossing of a textured occluder at texture coordinate uv (before the uv scale); true when
+// it blocks.
+static __device__ __forceinline__ bool attenuate(const DScene& s, const OccMat& m, v2 uv, float& trans) {
+  v4 c = sample_texture(s, m.albedo, uv * m.uv_scale);
+  trans = trans * (1.0f - c.w);
+  return c.w > 0.9999f;
+}
+// Crossing of triangle tp at barycentrics (u, v) (trace_mesh_shadow, shader.wgsl:846-852).
+static __device__ __forceinline__ bool tri_blocks(const DScene& s, const OccMat& m, const float4* tp, float u,
+                                                  float v, float& trans) {
+  if (m.albedo < 0) return true;
+  float4 a = ld4(tp + 6), b = ld4(tp + 7);
+  v3 bary = mk3(1.0f - u - v, u, v);
+  v2 uv = (mk2(a.x, a.y) * bary.x + mk2(a.z, a.w) * bary.y) + mk2(b.x, b.y) * bary.z;
+  return attenuate(s, m, uv, trans);
+}
+// Crossing of plane i (normal pn) at distance t (trace_plane_shadow, shader.wgsl:1190-1201).
+template <bool TEX>
+static __device__ __forceinline__ bool plane_blocks(const DScene& s, uint32_t i, v3 pn, const Ray& ray, float t,
+                                                    float& trans) {
+  if (!HAS_TEX<TEX>(s, wgpt::SCENE_ALPHA_SHADOWS)) return true;
+  OccMat m = occ_mat<TEX>(s, bi(ld4(s.planes + (size_t)i * 2 + 1).x));
+  if (m.albedo < 0) return true;
+  v3 hit_pos = ray.origin + ray.direction * t;
+  v3 T, B;
+  plane_frame(pn, 0.9999f, &T, &B);
+  return attenuate(s, m, mk2(dot(hit_pos, T), dot(hit_pos, B)), trans);
+}
+
+// BLAS shadow traversal (trace_mesh_shadow, shader.wgsl:813-872); true when blocked.
+template <bool COUNT, bool TEX>
+static __device__ bool mesh_shadow(const DScene& s, const Ray& rw, const m4& inv_m, uint32_t node_offset,
+                                   uint32_t tri_offset, int32_t material, float target_dist, float& trans,
+                                   uint32_t& err, Counters<COUNT>& cn) {
   Ray rl = to_local(inv_m, rw);
   v3 inv_dir = 1.0f / rl.direction;
   uint32_t stack[STACK_SIZE];
@@ -604,6 +800,7 @@ static __device__ bool mesh_occludes(const DScene& s, const Ray& rw, const m4& i
     float base_t = intersect_aabb(rl.origin, inv_dir, ld4(rn), ld4(rn + 1));
     if (base_t < 0.0f || base_t >= target_dist) return false;
   }
+  const OccMat om = occ_mat<TEX>(s, material);
   while (sp > 0) {
     cn.add(C_NODES);
     uint32_t node_idx = stack[--sp];
@@ -617,7 +814,7 @@ static __device__ bool mesh_occludes(const DScene& s, const Ray& rw, const m4& i
         float t_tri, u, v;
         cn.add(C_TRI_TESTS);
         if (intersect_triangle(rl, ld4(tp), ld4(tp + 1), ld4(tp + 2), &t_tri, &u, &v)) {
-          if (t_tri >= 0.0f && t_tri < target_dist) return true;
+          if (t_tri >= 0.0f && t_tri < target_dist && tri_blocks(s, om, tp, u, v, trans)) return true;
         }
       }
     } else {
@@ -694,28 +891,54 @@ static __device__ __noinline__ void solve_quartic_real(float a, float b, float c
   }
 }
 
+// Texture coordinate of a point on the cylinder or frustum (shader.wgsl:958-962).
+static __device__ __forceinline__ v2 frustum_uv(v3 p, float r0, float r1) {
+  if (p.y > 0.999f) return mk2(p.x / (r1 * 2.0f) + 0.5f, p.z / (r1 * 2.0f) + 0.5f);
+  if (p.y < 0.001f) return mk2(p.x / (r0 * 2.0f) + 0.5f, p.z / (r0 * 2.0f) + 0.5f);
+  return mk2(atan2_(p.z, p.x) / TWO_PI + 0.5f, p.y);
+}
+
 // Analytic shadow tests: shader.wgsl:874-905 (sphere), 926-956 (cube), 964-1016 (cylinder),
-// 1096-1132 (torus).
-static __device__ __noinline__ bool analytic_occludes(const m4& inv, const ObjHdr& h, const Ray& rw, float target_dist) {
+// 1096-1132 (torus).  An overlap of the object's interval with (0.001, target_dist) crosses it
+// at the interval's entry and exit; true when blocked.
+template <bool TEX>
+static __device__ __noinline__ bool analytic_shadow(const DScene& s, const m4& inv, const ObjHdr& h, const Ray& rw,
+                                                    float target_dist, float& trans) {
   Ray lr = to_local(inv, rw);
-  if (h.type == 1) {
-    float a = dot(lr.direction, lr.direction);
-    float half_b = dot(lr.origin, lr.direction);
-    float cc = dot(lr.origin, lr.origin) - 1.0f;
-    float disc = half_b * half_b - a * cc;
-    if (disc < 0.0f) return false;
-    float sqrtd = sqrtf(disc);
-    float t1 = (-half_b - sqrtd) / a;
-    float t2 = (-half_b + sqrtd) / a;
-    return wmax(0.001f, t1) < wmin(target_dist, t2);
-  }
-  if (h.type == 2) {
-    v3 inv_dir = 1.0f / lr.direction;
-    v3 tn = (-1.0f - lr.origin) * inv_dir;
-    v3 tf = (1.0f - lr.origin) * inv_dir;
-    float t1 = max_component(vmin(tn, tf));
-    float t2 = min_component(vmax(tn, tf));
-    return wmax(0.001f, t1) < wmin(target_dist, t2);
+  if (h.type == 1 || h.type == 2) {
+    float t1, t2;
+    if (h.type == 1) {
+      float a = dot(lr.direction, lr.direction);
+      float half_b = dot(lr.origin, lr.direction);
+      float cc = dot(lr.origin, lr.origin) - 1.0f;
+      float disc = half_b * half_b - a * cc;
+      if (disc < 0.0f) return false;
+      float sqrtd = sqrtf(disc);
+      t1 = (-half_b - sqrtd) / a;
+      t2 = (-half_b + sqrtd) / a;
+    } else {
+      v3 inv_dir = 1.0f / lr.direction;
+      v3 tn = (-1.0f - lr.origin) * inv_dir;
+      v3 tf = (1.0f - lr.origin) * inv_dir;
+      t1 = max_component(vmin(tn, tf));
+      t2 = min_component(vmax(tn, tf));
+    }
+    float h1 = wmax(0.001f, t1), h2 = wmin(target_dist, t2);
+    if (!(h1 < h2)) return false;
+    OccMat om = occ_mat<TEX>(s, h.material_idx);
+    if (om.albedo < 0) return true;
+    v3 p1 = lr.origin + lr.direction * h1, p2 = lr.origin + lr.direction * h2;
+    v2 uv1, uv2;
+    if (h.type == 1) {
+      uv1 = sphere_uv(p1);
+      uv2 = sphere_uv(p2);
+    } else {
+      v3 lt, lb;
+      cube_face(p1, &lt, &lb, &uv1);
+      cube_face(p2, &lt, &lb, &uv2);
+    }
+    if (attenuate(s, om, uv1, trans)) return true;
+    return attenuate(s, om, uv2, trans);
   }
   if (h.type == 3) {
     const Ray& r = lr;
@@ -746,8 +969,14 @@ static __device__ __noinline__ bool analytic_occludes(const m4& inv, const ObjHd
       v3 p = r.origin + t * r.direction;
       if (p.x * p.x + p.z * p.z <= rad * rad) { h1 = wmin(h1, t); h2 = wmax(h2, t); hit_count++; }
     }
-    if (hit_count >= 2u) return wmax(0.001f, h1) < wmin(target_dist, h2);
-    return false;
+    if (hit_count < 2u) return false;
+    float final_h1 = wmax(0.001f, h1);
+    float final_h2 = wmin(target_dist, h2);
+    if (!(final_h1 < final_h2)) return false;
+    OccMat om = occ_mat<TEX>(s, h.material_idx);
+    if (om.albedo < 0) return true;
+    if (attenuate(s, om, frustum_uv(r.origin + r.direction * final_h1, 1.0f, top_radius), trans)) return true;
+    return attenuate(s, om, frustum_uv(r.origin + r.direction * final_h2, 1.0f, top_radius), trans);
   }
   // torus
   float ray_scale = length(lr.direction);
@@ -767,15 +996,23 @@ static __device__ __noinline__ bool analytic_occludes(const m4& inv, const ObjHd
     if (t_near < 0.0f || t_near > target_dist * ray_scale) continue;
     float h1 = wmax(0.001f, t_near) / ray_scale;
     float h2 = wmin(target_dist * ray_scale, t_far) / ray_scale;
-    if (h1 < h2) return true;
+    if (h1 < h2) {
+      OccMat om = occ_mat<TEX>(s, h.material_idx);
+      if (om.albedo < 0) return true;
+      if (attenuate(s, om, torus_uv(lr.origin + lr.direction * (h1 * ray_scale)), trans)) return true;
+      if (attenuate(s, om, torus_uv(lr.origin + lr.direction * (h2 * ray_scale)), trans)) return true;
+    }
   }
   return false;
 }
 
-// shader.wgsl:1206-1229: true if the shadow ray is blocked.
-template <bool COUNT>
-static __device__ bool scene_occluded(const DScene& s, const Ray& ray, int32_t target_idx, float target_dist, uint32_t& err, Counters<COUNT>& cn) {
+// shader.wgsl:1206-1229: the shadow ray's transmittance (one component of trace_scene_shadow's
+// equal-component result), 0 when blocked.
+template <bool COUNT, bool TEX>
+static __device__ float scene_shadow(const DScene& s, const Ray& ray, int32_t target_idx, float target_dist,
+                                     uint32_t& err, Counters<COUNT>& cn) {
   cn.add(C_RAYS_SHADOW);
+  float trans = 1.0f;
   if (HAS(s, WGPT_HAS_PLANES)) {
     for (uint32_t i = 0; i < s.n_planes; i++) {
       float4 a = ld4(s.planes + (size_t)i * 2);
@@ -783,7 +1020,7 @@ static __device__ bool scene_occluded(const DScene& s, const Ray& ray, int32_t t
       float denom = dot(pn, ray.direction);
       if (absf(denom) > 1e-6f) {
         float t = (a.w - dot(pn, ray.origin)) / denom;
-        if (t > 0.001f && t < target_dist) return true;
+        if (t > 0.001f && t < target_dist && plane_blocks<TEX>(s, i, pn, ray, t, trans)) return 0.0f;
       }
     }
   }
@@ -809,9 +1046,11 @@ static __device__ bool scene_occluded(const DScene& s, const Ray& ray, int32_t t
           if (!on) continue;
           m4 inv = load_m4(s.objs + (size_t)i * 6);
           if (h.type == 0) {
-            if (mesh_occludes<COUNT>(s, ray, inv, bu(h.param0), bu(h.param1), target_dist, err, cn)) return true;
-          } else if (analytic_occludes(inv, h, ray, target_dist)) {
-            return true;
+            if (mesh_shadow<COUNT, TEX>(s, ray, inv, bu(h.param0), bu(h.param1), h.material_idx, target_dist, trans,
+                                        err, cn))
+              return 0.0f;
+          } else if (analytic_shadow<TEX>(s, inv, h, ray, target_dist, trans)) {
+            return 0.0f;
           }
         }
       } else {
@@ -837,10 +1076,10 @@ static __device__ bool scene_occluded(const DScene& s, const Ray& ray, int32_t t
       const float4* mp = s.meshes + (size_t)i * 5;
       m4 inv = load_m4(mp);
       float4 e = ld4(mp + 4);
-      if (mesh_occludes<COUNT>(s, ray, inv, bu(e.z), bu(e.w), target_dist, err, cn)) return true;
+      if (mesh_shadow<COUNT, TEX>(s, ray, inv, bu(e.z), bu(e.w), bi(e.x), target_dist, trans, err, cn)) return 0.0f;
     }
   }
-  return false;
+  return trans;
 }
 
 // ------------------------------------------------------------------------ BSDF
@@ -853,7 +1092,62 @@ static __device__ __forceinline__ float peek_outer_ior(const MediumStack& st) { 
 static __device__ __forceinline__ void push_medium(MediumStack& st, const Medium& m) { if (st.count < 4) { st.media[st.count] = m; st.count += 1; } }
 static __device__ __forceinline__ void pop_medium(MediumStack& st) { if (st.count > 0) st.count -= 1; }
 
-struct SurfCtx { v3 normal; v3 albedo; float roughness, metallic; v3 emittance; };
+// SurfaceContext of shader.wgsl:1393-1440: shading normal, geometric normal, albedo, alpha ...
+struct SurfCtx { v3 normal; v3 surface_normal; v3 albedo; float roughness, metallic; v3 emittance; float alpha; };
+
+// The context of an untextured material.
+static __device__ __forceinline__ SurfCtx plain_context(const DMat& mat, v3 hit_n) {
+  SurfCtx c;
+  c.normal = hit_n; c.surface_normal = hit_n;
+  c.albedo = mat.color; c.roughness = mat.roughness; c.metallic = mat.metallic; c.emittance = mat.emittance;
+  c.alpha = 1.0f;
+  return c;
+}
+
+// get_surface_context (shader.wgsl:1393-1440, without the parallax branch): normal map in the
+// frame (T, B, hit_n), albedo (sRGB-decoded, alpha from its fourth channel), roughness (second
+// channel), metallic (third channel) and emissive maps at uv * uv_scale.
+static __device__ __noinline__ SurfCtx surface_context(const DScene& s, int32_t m_idx, const DMat& mat, v3 hit_n,
+                                                      const UvFrame& f) {
+  DMatTex mt = load_mat_tex(s, m_idx);
+  v2 uv = f.uv * mt.uv_scale;
+  SurfCtx c;
+  c.normal = hit_n;
+  c.surface_normal = hit_n;
+  if (mt.normal >= 0) {
+    v4 t = sample_texture(s, mt.normal, uv);
+    v3 n_map = mk3(t.x, t.y, t.z) * 2.0f - mk3s(1.0f);
+    n_map = normalize(n_map * mk3(mt.height0, mt.height0, 1.0f));
+    m3 tbn;
+    tbn.c[0] = f.T; tbn.c[1] = f.B; tbn.c[2] = hit_n;
+    c.normal = normalize(mul3(tbn, n_map));
+  }
+  c.albedo = mat.color;
+  c.alpha = 1.0f;
+  if (mt.albedo >= 0) {
+    v4 t = sample_texture(s, mt.albedo, uv);
+    c.alpha = t.w;
+    c.albedo = c.albedo * vpow(mk3(t.x, t.y, t.z), 2.2f);
+  }
+  c.metallic = mat.metallic;
+  c.roughness = mat.roughness;
+  if (mt.roughness >= 0) c.roughness *= sample_texture(s, mt.roughness, uv).y;
+  if (mt.metallic >= 0) c.metallic *= sample_texture(s, mt.metallic, uv).z;
+  c.emittance = mat.emittance;
+  if (mt.emissive >= 0) {
+    v4 e = sample_texture(s, mt.emissive, uv);
+    c.emittance = c.emittance * vpow(mk3(e.x, e.y, e.z), 2.2f);
+  }
+  return c;
+}
+
+// The surface context of the closest hit hn = hit_normal(...) of material hit.m_idx.
+template <bool TEX>
+static __device__ __forceinline__ SurfCtx hit_context(const DScene& s, const Ray& rw, const HitRec& hit,
+                                                      const DMat& mat, v3 hn) {
+  if (!HAS_TEX<TEX>(s, wgpt::SCENE_TEXTURED)) return plain_context(mat, hn);
+  return surface_context(s, hit.m_idx, mat, hn, hit_uv_frame(s, rw, hit));
+}
 
 // shader.wgsl:1700-1704
 static __device__ __forceinline__ float D_GGX(float NdotH, float alpha2) {
@@ -885,7 +1179,9 @@ static __device__ __forceinline__ float G1_GGX_div_NV(float NdotV, float alpha2)
   return 2.0f / (NdotV + sqrtf(wmax(0.0f, alpha2 + (1.0f - alpha2) * NdotV * NdotV)) + 1e-7f);
 }
 
-// eval_surface and pdf_surface of shader.wgsl:1831-2047 evaluated together.
+// eval_surface and pdf_surface of shader.wgsl:1831-2047 evaluated together.  Untextured
+// instantiations (TEX false) have alpha 1, where the final "* ctx.alpha" is exact.
+template <bool TEX>
 static __device__ __noinline__ void bsdf_eval_pdf(v3 V, v3 L, const DMat& mat, const SurfCtx& ctx, const MediumStack& stack, v3* f_out, float* pdf_out) {
   bool entering = dot(ctx.normal, V) > 0.0f;
   v3 n_orient = entering ? ctx.normal : -ctx.normal;
@@ -998,9 +1294,9 @@ static __device__ __noinline__ void bsdf_eval_pdf(v3 V, v3 L, const DMat& mat, c
       }
     }
   }
-  // ctx.alpha == 1 without textures: the reference's final "* ctx.alpha" is exact.
-  *f_out = f * 1.0f;
-  *pdf_out = wmax(pdf, 1e-7f) * 1.0f;
+  const float alpha_c = TEX ? ctx.alpha : 1.0f;
+  *f_out = f * alpha_c;
+  *pdf_out = wmax(pdf, 1e-7f) * alpha_c;
 }
 
 // shader.wgsl:1806-1829

@@ -20,32 +20,32 @@ struct PathState {
 };
 
 // shader.wgsl:2226-2271 (heightmaps off)
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 __device__ v3 evaluate_nee(const DScene& s, const LightSample& ls, v3 hit_pos, v3 n_orient, v3 V, const DMat& mat,
                            const SurfCtx& ctx, const MediumStack& stack, int32_t ignore_obj_idx, PathState<COUNT>& ps) {
   if (ls.pdf <= 0.0f) return mk3s(0.0f);
   float dotNL = dot(n_orient, ls.dir);
   if (dotNL <= 0.0f && mat.transmission <= 0.0f) return mk3s(0.0f);
   v3 bsdf_val; float bsdf_pdf;
-  bsdf_eval_pdf(V, ls.dir, mat, ctx, stack, &bsdf_val, &bsdf_pdf);
+  bsdf_eval_pdf<TEX>(V, ls.dir, mat, ctx, stack, &bsdf_val, &bsdf_pdf);
   float weight = mis_weight(ls.pdf, bsdf_pdf);
   v3 c_weight = (bsdf_val * weight) / wmax(ls.pdf, 1e-6f);
   if (max_component(ls.color * c_weight) < 1e-5f) return mk3s(0.0f);
   v3 ray_offset = dotNL < 0.0f ? -n_orient * 0.001f : n_orient * 0.001f;
   Ray sr; sr.origin = hit_pos + ray_offset; sr.direction = ls.dir;
-  if (scene_occluded<COUNT>(s, sr, ignore_obj_idx, ls.dist, ps.err, ps.cn)) return mk3s(0.0f);
-  // shadow == (1,1,1): sample_color * shadow_hit is exact
-  return (ls.color * mk3s(1.0f)) * c_weight;
+  float shadow = scene_shadow<COUNT, TEX>(s, sr, ignore_obj_idx, ls.dist, ps.err, ps.cn);
+  if (shadow < 0.001f) return mk3s(0.0f);
+  return (ls.color * shadow) * c_weight;
 }
 
-// shader.wgsl:2052-2175 (alpha == 1)
-template <bool COUNT>
+// shader.wgsl:2052-2175
+template <bool COUNT, bool TEX>
 __device__ bool sample_surface(Ray& ray, v3& throughput, v3 hit_pos, const DMat& mat, const SurfCtx& ctx,
                                MediumStack& stack, float& last_surface_pdf, PathState<COUNT>& ps) {
   v3 V = -ray.direction;
   bool entering = dot(ctx.normal, V) > 0.0f;
   v3 n_orient = entering ? ctx.normal : -ctx.normal;
-  v3 sn_orient = n_orient;   // surface_normal == normal without normal maps
+  v3 sn_orient = entering ? ctx.surface_normal : -ctx.surface_normal;
   float dotSNV = wmax(dot(sn_orient, V), 1e-6f);
   float roughness_val = clamp(ctx.roughness, 0.01f, 1.0f);
   float alpha = roughness_val * roughness_val;
@@ -67,7 +67,7 @@ __device__ bool sample_surface(Ray& ray, v3& throughput, v3 hit_pos, const DMat&
   float p_diff = (1.0f - p_cc) * (1.0f - f_avg) * (1.0f - mat.transmission) * (1.0f - ctx.metallic);
   float total_p = p_cc + p_spec + p_trans + p_diff;
 
-  if (rand_pcg(ps.rng) > 1.0f) {   // alpha test: never taken for alpha == 1, but the draw is made
+  if (rand_pcg(ps.rng) > ctx.alpha) {   // alpha cut-out: the path passes through
     ray.origin = hit_pos - n_orient * 0.005f;
     return true;
   }
@@ -127,7 +127,7 @@ __device__ bool sample_surface(Ray& ray, v3& throughput, v3 hit_pos, const DMat&
   }
   ray.direction = L;
   v3 bsdf_val; float pdf_val;
-  bsdf_eval_pdf(V, L, mat, ctx, stack, &bsdf_val, &pdf_val);
+  bsdf_eval_pdf<TEX>(V, L, mat, ctx, stack, &bsdf_val, &pdf_val);
   if (pdf_val > 0.0f) throughput = throughput * (bsdf_val / pdf_val);
   else return false;
   last_surface_pdf = pdf_val;
@@ -145,7 +145,7 @@ __device__ bool sample_surface(Ray& ray, v3& throughput, v3 hit_pos, const DMat&
 }
 
 // One camera path of main (shader.wgsl:2280-2480); returns the path's radiance.
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 __device__ v3 trace_path(const DScene& s, const DParams& p, uint32_t ix, uint32_t iy, uint32_t sample_number, PathState<COUNT>& ps) {
   uint32_t idx = iy * p.width + ix;
   ps.rng = (idx * 1973u + sample_number * 9277u + p.seed * 26699u) | 1u;
@@ -196,9 +196,8 @@ __device__ v3 trace_path(const DScene& s, const DParams& p, uint32_t ix, uint32_
     ps.cn.add(C_SHADE);
     ps.cn.add(C_HIT_ATTR);
     DMat mat = load_mat(s, hit.m_idx);
-    SurfCtx ctx;
-    ctx.normal = hit_normal(s, ray, hit);
-    ctx.albedo = mat.color; ctx.roughness = mat.roughness; ctx.metallic = mat.metallic; ctx.emittance = mat.emittance;
+    v3 hn = hit_normal(s, ray, hit);
+    SurfCtx ctx = hit_context<TEX>(s, ray, hit, mat, hn);
 
     // shader.wgsl:2378-2395 implicit light hit
     float em_len = length(ctx.emittance);
@@ -213,7 +212,7 @@ __device__ v3 trace_path(const DScene& s, const DParams& p, uint32_t ix, uint32_
             raw_light_pdf = light_sphere_pdf(light, oh.world_position, ray.origin, ray.direction);
           } else if (HAS(s, WGPT_HAS_CUBES) && oh.type == 2) {
             BoxAreas b = box_areas(light, ray.origin);
-            float cos_l = wmax(dot(-ray.direction, ctx.normal), 1e-6f);
+            float cos_l = wmax(dot(-ray.direction, hn), 1e-6f);
             raw_light_pdf = (hit.t * hit.t) / (b.total * cos_l);
           }
           v3 to_light = oh.world_position - ray.origin;
@@ -259,7 +258,7 @@ __device__ v3 trace_path(const DScene& s, const DParams& p, uint32_t ix, uint32_
         }
         if (ls.pdf > 0.0f) {
           ls.pdf *= selected_weight / weight_sum;
-          v3 incoming = evaluate_nee<COUNT>(s, ls, hit_pos, n_orient, V, mat, ctx, stack, light.obj_idx, ps);
+          v3 incoming = evaluate_nee<COUNT, TEX>(s, ls, hit_pos, n_orient, V, mat, ctx, stack, light.obj_idx, ps);
           radiance = radiance + throughput * clamp_firefly(incoming, bounce);
         }
       }
@@ -271,10 +270,10 @@ __device__ v3 trace_path(const DScene& s, const DParams& p, uint32_t ix, uint32_
       float u0 = rand_pcg(ps.rng);
       float u1 = rand_pcg(ps.rng);
       LightSample env = sample_env_cdf(s, p, u0, u1, ps.cn);
-      v3 incoming = evaluate_nee<COUNT>(s, env, hit_pos, n_orient, V, mat, ctx, stack, -1, ps);
+      v3 incoming = evaluate_nee<COUNT, TEX>(s, env, hit_pos, n_orient, V, mat, ctx, stack, -1, ps);
       radiance = radiance + throughput * clamp_firefly(incoming, bounce);
     }
-    if (!sample_surface<COUNT>(ray, throughput, hit_pos, mat, ctx, stack, last_surface_pdf, ps)) break;
+    if (!sample_surface<COUNT, TEX>(ray, throughput, hit_pos, mat, ctx, stack, last_surface_pdf, ps)) break;
     if (bounce < 2) continue;
     float survival_prob = clamp(max_component(throughput), 0.05f, 0.95f);
     if (rand_pcg(ps.rng) > survival_prob) break;
@@ -295,7 +294,7 @@ __device__ __forceinline__ void flush_counters(PathState<COUNT>& ps, unsigned lo
   }
 }
 
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 __global__ void __launch_bounds__(128)
 k_render(DScene s, DParams p, uint32_t first_frame, uint32_t reps, uint32_t sec_w, uint32_t sec_h,
          float4* __restrict__ accum, uchar4* __restrict__ out, uint32_t out_pitch, uint32_t* status,
@@ -314,7 +313,7 @@ k_render(DScene s, DParams p, uint32_t first_frame, uint32_t reps, uint32_t sec_
     v3 acc = mk3(a.x, a.y, a.z);
     for (uint32_t r = 0; r < reps; ++r) {
       uint32_t sn = first_frame + r;
-      v3 radiance = trace_path<COUNT>(s, p, ix, iy, sn, ps);
+      v3 radiance = trace_path<COUNT, TEX>(s, p, ix, iy, sn, ps);
       float weight = 1.0f / (float)(sn + 1u);
       acc = vmix(acc, radiance, weight);
     }
@@ -330,6 +329,7 @@ k_render(DScene s, DParams p, uint32_t first_frame, uint32_t reps, uint32_t sec_
 }
 
 // shader.wgsl:2510-2603
+template <bool TEX>
 __global__ void __launch_bounds__(128)
 k_gbuffer(DScene s, DParams p, uint32_t sec_w, uint32_t sec_h, float* __restrict__ gbuf, uchar4* __restrict__ out,
           uint32_t out_pitch, uint32_t* status) {
@@ -357,12 +357,16 @@ k_gbuffer(DScene s, DParams p, uint32_t sec_w, uint32_t sec_h, float* __restrict
       break;
     }
     DMat mat = load_mat(s, hit.m_idx);
-    v3 n = hit_normal(s, ray, hit);
-    c_albedo = mat.color; c_rough = mat.roughness; c_metal = mat.metallic; c_emit = mat.emittance;
+    SurfCtx ctx = hit_context<TEX>(s, ray, hit, mat, hit_normal(s, ray, hit));
+    c_albedo = ctx.albedo; c_rough = ctx.roughness; c_metal = ctx.metallic; c_emit = ctx.emittance;
     m_trans = mat.transmission;
-    c_normal = dot(n, -ray.direction) > 0.0f ? n : -n;
+    c_normal = dot(ctx.normal, -ray.direction) > 0.0f ? ctx.normal : -ctx.normal;
     dist += hit.t;
-    // alpha == 1 without textures: the cut-out branch is never taken
+    if (ctx.alpha < 1.0f) {   // cut-out: tint by the albedo's coverage and continue behind the surface
+      tint = tint * vmix(mk3s(1.0f), c_albedo, ctx.alpha);
+      ray.origin = (ray.origin + ray.direction * hit.t) - c_normal * 0.001f;
+      continue;
+    }
     if (mat.metallic >= 0.99f && mat.roughness <= 0.01f) {
       tint = tint * c_albedo;
       ray.origin = (ray.origin + ray.direction * hit.t) + c_normal * 0.001f;
@@ -426,6 +430,7 @@ static DScene to_dscene(const wgpt::DeviceScene& d) {
   s.lights = (const float4*)d.lights; s.n_lights = d.n_lights;
   s.sky = (const uint2*)d.sky; s.sky_w = d.sky_w; s.sky_h = d.sky_h;
   s.cdf = (const float*)d.cdf; s.n_cdf = d.n_cdf;
+  s.tex = (const uint32_t*)d.tex; s.tex_w = d.tex_w; s.tex_h = d.tex_h;
   s.bounce_limit = d.bounce_limit; s.flags = d.flags;
   return s;
 }
@@ -451,10 +456,15 @@ cudaError_t launch_render(const DeviceScene& d, const wgpt_scene_params& q, uint
   DScene s = to_dscene(d);
   DParams p = to_dparams(q, sx, sy);
   dim3 grid((sw + 7) / 8, (sh + 15) / 16);
-  if (counters)
-    k_render<true><<<grid, 128, 0, st>>>(s, p, first_frame, reps, sw, sh, (float4*)accum, (uchar4*)out, out_pitch, status, counters);
-  else
-    k_render<false><<<grid, 128, 0, st>>>(s, p, first_frame, reps, sw, sh, (float4*)accum, (uchar4*)out, out_pitch, status, nullptr);
+  auto launch = [&](auto kernel, unsigned long long* c) {
+    kernel<<<grid, 128, 0, st>>>(s, p, first_frame, reps, sw, sh, (float4*)accum, (uchar4*)out, out_pitch, status, c);
+  };
+  const bool tex = (s.flags & wgpt::SCENE_TEXTURED) != 0u;
+  if (counters) {
+    if (tex) launch(k_render<true, true>, counters); else launch(k_render<true, false>, counters);
+  } else {
+    if (tex) launch(k_render<false, true>, nullptr); else launch(k_render<false, false>, nullptr);
+  }
   return cudaGetLastError();
 }
 
@@ -464,7 +474,10 @@ cudaError_t launch_gbuffer(const DeviceScene& d, const wgpt_scene_params& q, uin
   DScene s = to_dscene(d);
   DParams p = to_dparams(q, sx, sy);
   dim3 grid((sw + 7) / 8, (sh + 15) / 16);
-  k_gbuffer<<<grid, 128, 0, st>>>(s, p, sw, sh, gbuf, (uchar4*)out, out_pitch, status);
+  if (s.flags & wgpt::SCENE_TEXTURED)
+    k_gbuffer<true><<<grid, 128, 0, st>>>(s, p, sw, sh, gbuf, (uchar4*)out, out_pitch, status);
+  else
+    k_gbuffer<false><<<grid, 128, 0, st>>>(s, p, sw, sh, gbuf, (uchar4*)out, out_pitch, status);
   return cudaGetLastError();
 }
 

@@ -95,6 +95,7 @@ __device__ __forceinline__ void closest_init(const DScene& s, ClosestTrav& t, Co
   cn.add(C_RAYS_EXT);
   HitRec& hit = t.hit;
   hit.t = 1e10f; hit.m_idx = -1; hit.o_idx = -1; hit.kind = 0; hit.id = -1; hit.aux = -1; hit.bu = 0.0f; hit.bv = 0.0f;
+  hit.tsrc = -1; hit.tsrc_t = 0.0f;
   t.sp = 0;
   if (HAS(s, WGPT_HAS_PLANES)) {
     for (uint32_t i = 0; i < s.n_planes; i++) {
@@ -107,7 +108,10 @@ __device__ __forceinline__ void closest_init(const DScene& s, ClosestTrav& t, Co
         float x = (a.w - dot(pn, t.rw.origin)) / denom;
         if (x > 0.001f) tt = x;
       }
-      if (tt > 0.001f && tt < hit.t) { hit.t = tt; hit.m_idx = __float_as_int(b.x); hit.kind = 1; hit.id = (int32_t)i; }
+      if (tt > 0.001f && tt < hit.t) {
+        hit.t = tt; hit.m_idx = __float_as_int(b.x); hit.kind = 1; hit.id = (int32_t)i;
+        hit.tsrc = -2 - (int32_t)i; hit.tsrc_t = tt;
+      }
     }
   }
   t.inv_w = 1.0f / t.rw.direction;
@@ -209,6 +213,7 @@ __device__ __forceinline__ bool closest_step(const DScene& s, const DPairs& P, C
       float ta = 0.0f;
       if (analytic_t(inv, h, t.rw, &ta) && ta < hit.t) {
         hit.t = ta; hit.m_idx = h.material_idx; hit.o_idx = (int32_t)i; hit.kind = 3; hit.id = (int32_t)i;
+        if (h.type <= 2) { hit.tsrc = (int32_t)i; hit.tsrc_t = ta; }
       }
     }
   }
@@ -235,15 +240,17 @@ struct ShadowTrav : TravCommon {
   float target_dist;
   int32_t target_idx;
   bool occluded;
+  float trans;   // transmittance through the textured occluders crossed so far
 };
 
 // Planes first, then the TLAS from its root without a root test (shader.wgsl:1206-1218,
 // 1134-1140).
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 __device__ __forceinline__ void shadow_init(const DScene& s, ShadowTrav& t, Counters<COUNT>& cn) {
   cn.add(C_RAYS_SHADOW);
   t.sp = 0;
   t.occluded = false;
+  t.trans = 1.0f;
   if (HAS(s, WGPT_HAS_PLANES)) {
     for (uint32_t i = 0; i < s.n_planes; i++) {
       float4 a = ld4(s.planes + (size_t)i * 2);
@@ -251,7 +258,10 @@ __device__ __forceinline__ void shadow_init(const DScene& s, ShadowTrav& t, Coun
       float denom = dot(pn, t.rw.direction);
       if (absf(denom) > 1e-6f) {
         float x = (a.w - dot(pn, t.rw.origin)) / denom;
-        if (x > 0.001f && x < t.target_dist) { t.occluded = true; return; }
+        if (x > 0.001f && x < t.target_dist && plane_blocks<TEX>(s, i, pn, t.rw, x, t.trans)) {
+          t.occluded = true;
+          return;
+        }
       }
     }
   }
@@ -262,7 +272,7 @@ __device__ __forceinline__ void shadow_init(const DScene& s, ShadowTrav& t, Coun
   }
 }
 
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 __device__ __forceinline__ bool shadow_step(const DScene& s, const DPairs& P, ShadowTrav& t, uint32_t& err,
                                             Counters<COUNT>& cn) {
   if (t.occluded) return true;
@@ -278,7 +288,10 @@ __device__ __forceinline__ bool shadow_step(const DScene& s, const DPairs& P, Sh
         float t_tri, u, v;
         cn.add(C_TRI_TESTS);
         if (intersect_triangle(t.rl, ld4(tp), ld4(tp + 1), ld4(tp + 2), &t_tri, &u, &v)) {
-          if (t_tri >= 0.0f && t_tri < t.target_dist) { t.occluded = true; return true; }
+          if (t_tri >= 0.0f && t_tri < t.target_dist && tri_blocks(s, occ_mat<TEX>(s, t.inst_mat), tp, u, v, t.trans)) {
+            t.occluded = true;
+            return true;
+          }
         }
       }
       if (t.sp == 0 || (t.stack[t.sp - 1].x >> 29) != K_BLAS_LEAF) break;
@@ -300,13 +313,13 @@ __device__ __forceinline__ bool shadow_step(const DScene& s, const DPairs& P, Sh
                           (int32_t)i, t.target_dist, err, cn);
         break;
       }
-      if (analytic_occludes(inv, h, t.rw, t.target_dist)) { t.occluded = true; return true; }
+      if (analytic_shadow<TEX>(s, inv, h, t.rw, t.target_dist, t.trans)) { t.occluded = true; return true; }
     }
   }
   return t.sp == 0;
 }
 
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 __device__ __forceinline__ void shadow_finish(const DScene& s, ShadowTrav& t, uint32_t& err, Counters<COUNT>& cn) {
   if (t.occluded) return;
   if (HAS(s, WGPT_HAS_LIST_MESHES)) {
@@ -314,7 +327,8 @@ __device__ __forceinline__ void shadow_finish(const DScene& s, ShadowTrav& t, ui
       const float4* mp = s.meshes + (size_t)i * 5;
       m4 inv = load_m4(mp);
       float4 e = ld4(mp + 4);
-      if (mesh_occludes<COUNT>(s, t.rw, inv, __float_as_uint(e.z), __float_as_uint(e.w), t.target_dist, err, cn)) {
+      if (mesh_shadow<COUNT, TEX>(s, t.rw, inv, __float_as_uint(e.z), __float_as_uint(e.w), __float_as_int(e.x),
+                             t.target_dist, t.trans, err, cn)) {
         t.occluded = true;
         return;
       }

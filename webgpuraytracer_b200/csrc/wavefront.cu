@@ -40,9 +40,12 @@ struct WfBuffers {
   uint32_t* unit;    // work unit of the slot's path
   float4* med;       // 8 per path: (ior, sigma.xyz), (emission.xyz, -) for media 0..3
   uint4* hit;        // 2 per path: (t, m_idx, o_idx, kind), (id, aux, bu, bv)
-  float4* nee;       // 4 per path: (tp.xyz, -), (incoming.xyz, -) for the light and env records
+  uint2* tsrc;       // 1 per path: tangent-frame source of the hit (tsrc, tsrc_t), with normal maps
+  float4* nee;       // 4 per path: (tp.xyz, -), (incoming.xyz, -) for the light and env records;
+                     // with alpha-textured shadows `incoming` holds the BSDF weight alone
+  float4* necol;     // 2 per path: the records' light colour (alpha-textured shadows only)
   float4* shadow;    // 4 per path: (origin.xyz, target_dist), (direction.xyz, ignore_idx) x 2
-  uint8_t* vis;      // 2 per path: 1 if the record's shadow ray reached its light
+  float* vis;        // 2 per path: transmittance of the record's shadow ray (0 when blocked)
   uint32_t* qcont[2];  // paths continuing into the iteration (ping-pong by iteration parity)
   uint32_t* qnew[2];   // slots that started a new unit for the iteration
   uint32_t* hitq;    // paths of the iteration that hit a surface
@@ -273,6 +276,7 @@ __global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
       const HitRec& h = t.hit;
       a.b.hit[slot * 2 + 0] = make_uint4(__float_as_uint(h.t), (uint32_t)h.m_idx, (uint32_t)h.o_idx, (uint32_t)h.kind);
       a.b.hit[slot * 2 + 1] = make_uint4((uint32_t)h.id, (uint32_t)h.aux, __float_as_uint(h.bu), __float_as_uint(h.bv));
+      if (HAS(a.s, wgpt::SCENE_NORMAL_MAPS)) a.b.tsrc[slot] = make_uint2((uint32_t)h.tsrc, __float_as_uint(h.tsrc_t));
       have = false;
     }
   }
@@ -366,7 +370,7 @@ __global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a) {
 
 // Records one next-event contribution: the throughput it is weighted by, the incoming
 // radiance if the light is visible, and the shadow ray to test (when evaluate_nee reaches it).
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 __device__ void record_nee(const WfArgs& a, uint32_t slot, int rec, const LightSample& ls, v3 hit_pos, v3 n_orient,
                            v3 V, const DMat& mat, const SurfCtx& ctx, const MediumStack& stack, int32_t ignore_idx,
                            v3 throughput, uint32_t& flags) {
@@ -378,13 +382,19 @@ __device__ void record_nee(const WfArgs& a, uint32_t slot, int rec, const LightS
     float dotNL = dot(n_orient, ls.dir);
     if (!(dotNL <= 0.0f && mat.transmission <= 0.0f)) {
       v3 bsdf_val; float bsdf_pdf;
-      bsdf_eval_pdf(V, ls.dir, mat, ctx, stack, &bsdf_val, &bsdf_pdf);
+      bsdf_eval_pdf<TEX>(V, ls.dir, mat, ctx, stack, &bsdf_val, &bsdf_pdf);
       float weight = mis_weight(ls.pdf, bsdf_pdf);
       v3 c_weight = (bsdf_val * weight) / wmax(ls.pdf, 1e-6f);
       if (!(max_component(ls.color * c_weight) < 1e-5f)) {
         v3 ray_offset = dotNL < 0.0f ? -n_orient * 0.001f : n_orient * 0.001f;
         so = hit_pos + ray_offset;
-        incoming = (ls.color * mk3s(1.0f)) * c_weight;
+        if (HAS_TEX<TEX>(a.s, wgpt::SCENE_ALPHA_SHADOWS)) {
+          // (colour * transmittance) * weight once the shadow ray is traced
+          incoming = c_weight;
+          a.b.necol[slot * 2 + rec] = make_float4(ls.color.x, ls.color.y, ls.color.z, 0.0f);
+        } else {
+          incoming = ls.color * c_weight;   // transmittance 1 or 0
+        }
         shadow = true;
       }
     }
@@ -399,7 +409,7 @@ __device__ void record_nee(const WfArgs& a, uint32_t slot, int rec, const LightS
   }
 }
 
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   const DScene& s = a.s;
@@ -421,6 +431,11 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
       HitRec hit;
       hit.t = __uint_as_float(h0.x); hit.m_idx = (int32_t)h0.y; hit.o_idx = (int32_t)h0.z; hit.kind = (int32_t)h0.w;
       hit.id = (int32_t)h1.x; hit.aux = (int32_t)h1.y; hit.bu = __uint_as_float(h1.z); hit.bv = __uint_as_float(h1.w);
+      hit.tsrc = -1; hit.tsrc_t = 0.0f;
+      if (HAS_TEX<TEX>(s, wgpt::SCENE_NORMAL_MAPS)) {
+        uint2 ts = a.b.tsrc[slot];
+        hit.tsrc = (int32_t)ts.x; hit.tsrc_t = __uint_as_float(ts.y);
+      }
       Ray ray; ray.origin = mk3(o4.x, o4.y, o4.z); ray.direction = mk3(d4.x, d4.y, d4.z);
       v3 throughput = mk3(tp4.x, tp4.y, tp4.z);
       float last_surface_pdf = tp4.w;
@@ -436,9 +451,8 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
         cn.add(C_SHADE);
         cn.add(C_HIT_ATTR);
         DMat mat = load_mat(s, hit.m_idx);
-        SurfCtx ctx;
-        ctx.normal = hit_normal(s, ray, hit);
-        ctx.albedo = mat.color; ctx.roughness = mat.roughness; ctx.metallic = mat.metallic; ctx.emittance = mat.emittance;
+        v3 hn = hit_normal(s, ray, hit);
+        SurfCtx ctx = hit_context<TEX>(s, ray, hit, mat, hn);
         float em_len = length(ctx.emittance);
         if (em_len > 0.0f) {
           float weight = 1.0f;
@@ -451,7 +465,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
                 raw_light_pdf = light_sphere_pdf(light, oh.world_position, ray.origin, ray.direction);
               } else if (HAS(s, WGPT_HAS_CUBES) && oh.type == 2) {
                 BoxAreas bx = box_areas(light, ray.origin);
-                float cos_l = wmax(dot(-ray.direction, ctx.normal), 1e-6f);
+                float cos_l = wmax(dot(-ray.direction, hn), 1e-6f);
                 raw_light_pdf = (hit.t * hit.t) / (bx.total * cos_l);
               }
               v3 to_light = oh.world_position - ray.origin;
@@ -495,7 +509,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
             }
             if (ls.pdf > 0.0f) {
               ls.pdf *= selected_weight / weight_sum;
-              record_nee<COUNT>(a, slot, 0, ls, hit_pos, n_orient, V, mat, ctx, stack, light.obj_idx, throughput, flags);
+              record_nee<COUNT, TEX>(a, slot, 0, ls, hit_pos, n_orient, V, mat, ctx, stack, light.obj_idx, throughput, flags);
             }
           }
           last_weight_sum = weight_sum;
@@ -505,13 +519,13 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
           float u0 = rand_pcg(rng);
           float u1 = rand_pcg(rng);
           LightSample env = sample_env_cdf(s, p, u0, u1, cn);
-          record_nee<COUNT>(a, slot, 1, env, hit_pos, n_orient, V, mat, ctx, stack, -1, throughput, flags);
+          record_nee<COUNT, TEX>(a, slot, 1, env, hit_pos, n_orient, V, mat, ctx, stack, -1, throughput, flags);
         }
-        // shader.wgsl:2052-2175 (alpha == 1) -- the same arithmetic as the single-kernel form
+        // shader.wgsl:2052-2175 -- the same arithmetic as the single-kernel form
         int32_t count_before = stack.count;
         {
           bool entering = dot(ctx.normal, V) > 0.0f;
-          v3 sn_orient = n_orient;
+          v3 sn_orient = entering ? ctx.surface_normal : -ctx.surface_normal;
           float dotSNV = wmax(dot(sn_orient, V), 1e-6f);
           float roughness_val = clamp(ctx.roughness, 0.01f, 1.0f);
           float alpha = roughness_val * roughness_val;
@@ -532,7 +546,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
           float p_trans = (1.0f - p_cc) * (1.0f - f_avg) * mat.transmission * (1.0f - ctx.metallic);
           float p_diff = (1.0f - p_cc) * (1.0f - f_avg) * (1.0f - mat.transmission) * (1.0f - ctx.metallic);
           float total_p = p_cc + p_spec + p_trans + p_diff;
-          if (rand_pcg(rng) > 1.0f) {   // alpha test draw (alpha == 1)
+          if (rand_pcg(rng) > ctx.alpha) {   // alpha cut-out: the path passes through
             ray.origin = hit_pos - n_orient * 0.005f;
             alive = true;
           } else {
@@ -606,7 +620,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
               if (ok) {
                 ray.direction = L;
                 v3 bsdf_val; float pdf_val;
-                bsdf_eval_pdf(V, L, mat, ctx, stack, &bsdf_val, &pdf_val);
+                bsdf_eval_pdf<TEX>(V, L, mat, ctx, stack, &bsdf_val, &pdf_val);
                 if (pdf_val > 0.0f) throughput = throughput * (bsdf_val / pdf_val);
                 else ok = false;
                 if (ok) {
@@ -651,7 +665,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
 }
 
 // ---------------------------------------------------------------------------- shadow
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 __global__ void __launch_bounds__(256) k_wf_shadow(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   uint32_t err = 0;
@@ -671,14 +685,14 @@ __global__ void __launch_bounds__(256) k_wf_shadow(WfArgs a) {
         t.rw.direction = mk3(sd.x, sd.y, sd.z);
         t.target_dist = so.w;
         t.target_idx = __float_as_int(sd.w);
-        shadow_init<COUNT>(a.s, t, cn);
+        shadow_init<COUNT, TEX>(a.s, t, cn);
         have = true;
       }
     }
     if (!__any_sync(FULL, have)) break;
-    if (have && shadow_step<COUNT>(a.s, a.P, t, err, cn)) {
-      shadow_finish<COUNT>(a.s, t, err, cn);
-      a.b.vis[e] = t.occluded ? 0u : 1u;
+    if (have && shadow_step<COUNT, TEX>(a.s, a.P, t, err, cn)) {
+      shadow_finish<COUNT, TEX>(a.s, t, err, cn);
+      a.b.vis[e] = t.occluded ? 0.0f : t.trans;
       have = false;
     }
   }
@@ -720,7 +734,15 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a) {
           if (!(flags & has)) continue;
           float4 t4 = a.b.nee[slot * 4 + rec * 2], c4 = a.b.nee[slot * 4 + rec * 2 + 1];
           v3 incoming = mk3(c4.x, c4.y, c4.z);
-          if ((flags & needs) && a.b.vis[slot * 2 + rec] == 0u) incoming = mk3s(0.0f);
+          if (flags & needs) {
+            float sh = a.b.vis[slot * 2 + rec];
+            if (sh < 0.001f) {
+              incoming = mk3s(0.0f);
+            } else if (HAS(a.s, wgpt::SCENE_ALPHA_SHADOWS)) {
+              float4 col = a.b.necol[slot * 2 + rec];
+              incoming = (mk3(col.x, col.y, col.z) * sh) * incoming;
+            }
+          }
           radiance = radiance + mk3(t4.x, t4.y, t4.z) * clamp_firefly(incoming, bounce);
         }
       }
@@ -850,6 +872,7 @@ static void fill_dscene(DScene& s, const DeviceScene& d) {
   s.lights = (const float4*)d.lights; s.n_lights = d.n_lights;
   s.sky = (const uint2*)d.sky; s.sky_w = d.sky_w; s.sky_h = d.sky_h;
   s.cdf = (const float*)d.cdf; s.n_cdf = d.n_cdf;
+  s.tex = (const uint32_t*)d.tex; s.tex_w = d.tex_w; s.tex_h = d.tex_h;
   s.bounce_limit = d.bounce_limit; s.flags = d.flags;
 }
 
@@ -864,22 +887,21 @@ static void fill_dparams(DParams& p, const wgpt_scene_params& q, uint32_t sec_x,
   p.sec_x = sec_x; p.sec_y = sec_y; p.sky_cdf_index = q.sky_cdf_index;
 }
 
-// Path-slot state: ray 32 + throughput/radiance 32 + meta 16 + unit 4 + media 128 + hit 32 +
-// nee 64 + shadow 64 + vis 2 + continuing and new queues 16 + hit queue 4 + shadow queue 8.
-static constexpr int kParts = 16;
-static void part_sizes(size_t n, size_t out[kParts]) {
-  size_t v[kParts] = {n * 32, n * 32, 0, 0, n * 16, n * 4, n * 128, n * 32,
-                      n * 64, n * 64, n * 2, n * 4, n * 4, n * 4, n * 4, n * 4};
-  for (int i = 0; i < kParts; ++i) out[i] = v[i];
+// Path-slot state, in carving order: ray 32 + throughput/radiance 32 + meta 16 + unit 4 +
+// media 128 + hit 32 + tangent source 8 + nee 64 + light colour 32 + shadow 64 + vis 8 +
+// continuing and new queues 16 + hit queue 4 + shadow queue 8.
+static constexpr int kParts = 17;
+static const uint32_t kPartBytes[kParts] = {32, 32, 16, 4, 128, 32, 8, 64, 32, 64, 8, 4, 4, 4, 4, 4, 8};
+size_t wavefront_bytes_per_path() {
+  size_t s = 0;
+  for (uint32_t x : kPartBytes) s += x;
+  return s;
 }
-// plus the shadow queue (n * 8), carved last
-size_t wavefront_bytes_per_path() { return 32 + 16 + 16 + 16 + 4 + 128 + 32 + 64 + 64 + 2 + 16 + 4 + 8; }
 
 static size_t pool_bytes(uint32_t capacity) {
-  size_t parts[kParts], s = 0;
-  part_sizes(capacity, parts);
-  for (size_t x : parts) s += (x + 255) & ~(size_t)255;
-  return s + (((size_t)capacity * 8 + 255) & ~(size_t)255);
+  size_t s = 0;
+  for (uint32_t x : kPartBytes) s += ((size_t)capacity * x + 255) & ~(size_t)255;
+  return s;
 }
 
 static WfBuffers carve(void* scratch, uint32_t capacity) {
@@ -893,9 +915,11 @@ static WfBuffers carve(void* scratch, uint32_t capacity) {
   b.unit = (uint32_t*)take(n * 4);
   b.med = (float4*)take(n * 128);
   b.hit = (uint4*)take(n * 32);
+  b.tsrc = (uint2*)take(n * 8);
   b.nee = (float4*)take(n * 64);
+  b.necol = (float4*)take(n * 32);
   b.shadow = (float4*)take(n * 64);
-  b.vis = (uint8_t*)take(n * 2);
+  b.vis = (float*)take(n * 8);
   b.qcont[0] = (uint32_t*)take(n * 4);
   b.qcont[1] = (uint32_t*)take(n * 4);
   b.qnew[0] = (uint32_t*)take(n * 4);
@@ -919,7 +943,7 @@ struct WfEngine {
   unsigned long long* d_done = nullptr;    // track_cap stamps, then the start stamp
   uint32_t track_cap = 0;
   uint32_t* h_cond = nullptr;              // pinned copy of the loop condition (host-driven loop)
-  int grids[2][8] = {{0}, {0}};              // launch grid per stage (counting / plain variants)
+  int grids[4][8] = {{0}};                 // launch grid per stage, per (counting, textured) variant
   int* grid = grids[0];
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -973,14 +997,14 @@ static int occupancy_grid(K kernel) {
   return sms * (per_sm > 0 ? per_sm : 1);
 }
 
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 static void compute_grids(WfEngine* e) {
-  e->grid = e->grids[COUNT ? 1 : 0];
+  e->grid = e->grids[(COUNT ? 2 : 0) + (TEX ? 1 : 0)];
   if (e->grid[0]) return;
   e->grid[0] = occupancy_grid(k_wf_fill<COUNT>);
   e->grid[1] = occupancy_grid(k_wf_extend<COUNT>);
-  e->grid[2] = occupancy_grid(k_wf_shade<COUNT>);
-  e->grid[3] = occupancy_grid(k_wf_shadow<COUNT>);
+  e->grid[2] = occupancy_grid(k_wf_shade<COUNT, TEX>);
+  e->grid[3] = occupancy_grid(k_wf_shadow<COUNT, TEX>);
   e->grid[4] = occupancy_grid(k_wf_resolve<COUNT>);
   e->grid[5] = occupancy_grid(k_wf_shade_miss<COUNT>);
   e->grid[6] = occupancy_grid(k_wf_accumulate);
@@ -996,7 +1020,7 @@ static WfArgs stage_args(const WfArgs& a, int stage) {
 // The whole pass as one graph: fill -> WHILE(extend, shade_miss, shade, shadow, resolve,
 // control) -> accumulate.  Arguments live in device memory (views, control block), so the graph
 // only changes when buffers move.
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 static cudaError_t build_graph(WfEngine* e, const WfArgs& a) {
   drop_graph(e);
   cudaError_t err;
@@ -1038,9 +1062,9 @@ static cudaError_t build_graph(WfEngine* e, const WfArgs& a) {
   if ((err = add_kernel(body, (const void*)k_wf_extend<COUNT>, e->grid[1], a1, nullptr, &prev)) != cudaSuccess) return err;
   if ((err = add_kernel(body, (const void*)k_wf_shade_miss<COUNT>, e->grid[5], a5, &prev, &cur)) != cudaSuccess) return err;
   prev = cur;
-  if ((err = add_kernel(body, (const void*)k_wf_shade<COUNT>, e->grid[2], a2, &prev, &cur)) != cudaSuccess) return err;
+  if ((err = add_kernel(body, (const void*)k_wf_shade<COUNT, TEX>, e->grid[2], a2, &prev, &cur)) != cudaSuccess) return err;
   prev = cur;
-  if ((err = add_kernel(body, (const void*)k_wf_shadow<COUNT>, e->grid[3], a3, &prev, &cur)) != cudaSuccess) return err;
+  if ((err = add_kernel(body, (const void*)k_wf_shadow<COUNT, TEX>, e->grid[3], a3, &prev, &cur)) != cudaSuccess) return err;
   prev = cur;
   if ((err = add_kernel(body, (const void*)k_wf_resolve<COUNT>, e->grid[4], a4, &prev, &cur)) != cudaSuccess) return err;
   prev = cur;
@@ -1055,7 +1079,7 @@ static cudaError_t build_graph(WfEngine* e, const WfArgs& a) {
 }
 
 // The same pass launched from the host, one event pair per stage launch (stage timing).
-template <bool COUNT>
+template <bool COUNT, bool TEX>
 static cudaError_t run_pass_host(WfEngine* e, const WfArgs& a, uint32_t max_iter, cudaStream_t st,
                                  StageTimer* timer) {
   auto T0 = [&](int k) { if (timer) timer->begin(k, st); };
@@ -1064,8 +1088,8 @@ static cudaError_t run_pass_host(WfEngine* e, const WfArgs& a, uint32_t max_iter
   for (uint32_t it = 0; it <= max_iter; ++it) {
     T0(1); k_wf_extend<COUNT><<<e->grid[1], 256, 0, st>>>(stage_args(a, 1)); T1(1);
     T0(5); k_wf_shade_miss<COUNT><<<e->grid[5], 256, 0, st>>>(stage_args(a, 5)); T1(5);
-    T0(2); k_wf_shade<COUNT><<<e->grid[2], 256, 0, st>>>(stage_args(a, 2)); T1(2);
-    T0(3); k_wf_shadow<COUNT><<<e->grid[3], 256, 0, st>>>(stage_args(a, 3)); T1(3);
+    T0(2); k_wf_shade<COUNT, TEX><<<e->grid[2], 256, 0, st>>>(stage_args(a, 2)); T1(2);
+    T0(3); k_wf_shadow<COUNT, TEX><<<e->grid[3], 256, 0, st>>>(stage_args(a, 3)); T1(3);
     T0(4); k_wf_resolve<COUNT><<<e->grid[4], 256, 0, st>>>(stage_args(a, 4)); T1(4);
     T0(7); k_wf_control<false><<<1, 32, 0, st>>>(stage_args(a, 7), cudaGraphConditionalHandle{}); T1(7);
     cudaError_t err = cudaMemcpyAsync(e->h_cond, &a.ctl->cond, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
@@ -1082,7 +1106,8 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
                                 const WfJobView* jv, uint32_t nv, uint32_t* status, unsigned long long* counters,
                                 cudaStream_t st, StageTimer* timer, float* done_ms) {
   cudaError_t err;
-  compute_grids<COUNT>(e);
+  const bool tex = (d.flags & SCENE_TEXTURED) != 0u;
+  if (tex) compute_grids<COUNT, true>(e); else compute_grids<COUNT, false>(e);
   const bool track = done_ms != nullptr;
   uint64_t total_npix = 0;
   for (uint32_t v = 0; v < nv; ++v) total_npix += (uint64_t)jv[v].sw * jv[v].sh;
@@ -1235,10 +1260,13 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
       if (timer) timer->end(6, st);
       if ((err = cudaGetLastError()) != cudaSuccess) return err;
     } else if (timer) {
-      if ((err = run_pass_host<COUNT>(e, a, c.max_iter, st, timer)) != cudaSuccess) return err;
+      err = tex ? run_pass_host<COUNT, true>(e, a, c.max_iter, st, timer)
+                : run_pass_host<COUNT, false>(e, a, c.max_iter, st, timer);
+      if (err != cudaSuccess) return err;
     } else {
       if (!e->has_graph || e->key_count != COUNT || memcmp(&e->key, &a, sizeof a) != 0) {
-        if ((err = build_graph<COUNT>(e, a)) != cudaSuccess) {
+        err = tex ? build_graph<COUNT, true>(e, a) : build_graph<COUNT, false>(e, a);
+        if (err != cudaSuccess) {
           drop_graph(e);
           return err;
         }

@@ -20,6 +20,11 @@ struct CtxImages {
 };
 bool ctx_images(::wgpt_ctx* ctx, int view, CtxImages* out);   // view -1: the main image
 
+// Scene flag bits derived from the materials on upload (above the WGPT_HAS_* bits): some
+// material samples a texture; some has an albedo texture (shadow rays then attenuate through
+// it); some has a normal map (closest hits then carry their tangent-frame source).
+enum : uint32_t { SCENE_TEXTURED = 1u << 24, SCENE_ALPHA_SHADOWS = 1u << 25, SCENE_NORMAL_MAPS = 1u << 26 };
+
 // Device copies of the scene buffers, in the reference's packed layouts.
 struct DeviceScene {
   const void* mats; uint32_t n_mats;
@@ -32,6 +37,7 @@ struct DeviceScene {
   const void* lights; uint32_t n_lights;
   const void* sky; uint32_t sky_w, sky_h;
   const void* cdf; uint32_t n_cdf;
+  const void* tex; uint32_t tex_w, tex_h, tex_layers;   // rgba8 texture array
   int32_t bounce_limit;
   uint32_t flags;
 };

@@ -370,6 +370,7 @@ WB_HD v3 cross(v3 a, v3 b) {
   return mk3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 WB_HD float length(v3 a) { return sqrtf(dot(a, a)); }
+WB_HD float length(v2 a) { return sqrtf(a.x * a.x + a.y * a.y); }
 WB_HD float length2(v2 a) { return sqrtf(dot2(a, a)); }
 // WGSL normalize(e) = e / length(e); one reciprocal keeps the two IEEE ops correctly rounded.
 WB_HD v3 normalize(v3 a) { float inv = 1.0f / sqrtf(dot(a, a)); return a * inv; }
@@ -445,6 +446,34 @@ WB_HD float rand_pcg(uint32_t& state) {
   uint32_t word = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
   word = (word >> 22u) ^ word;
   return (float)word * 2.3283064365386963e-10f;
+}
+
+// textureSampleLevel(texture_2d_array<f32>, sampler, uv, layer, 0.0) for an rgba8unorm array with
+// the reference's sampler (linear min/mag filter, repeat addressing; tracer.js:1965-1968), pinned
+// to FP32 arithmetic like the sky: texel (c / 255), centres at uv * size - 0.5, the two integer
+// neighbours wrapped modulo the size, weights the fractional part, mixed along x then y.  A
+// non-finite coordinate samples as coordinate 0 (hardware behaviour is undefined there).
+// `fetch(x, y)` returns the packed rgba8 texel of the layer.
+WB_HD v4 unorm8x4(uint32_t t) {
+  return mk4((float)(t & 255u) / 255.0f, (float)((t >> 8) & 255u) / 255.0f, (float)((t >> 16) & 255u) / 255.0f,
+             (float)(t >> 24) / 255.0f);
+}
+template <class Fetch>
+WB_HD v4 sample_rgba8_repeat(const Fetch& fetch, uint32_t w, uint32_t h, v2 uv) {
+  float fx = uv.x * (float)w - 0.5f;
+  float fy = uv.y * (float)h - 0.5f;
+  if (!(fx == fx) || fx > 3.0e38f || fx < -3.0e38f) fx = 0.0f;
+  if (!(fy == fy) || fy > 3.0e38f || fy < -3.0e38f) fy = 0.0f;
+  float x0f = floorf(fx), y0f = floorf(fy);
+  float tx = fx - x0f, ty = fy - y0f;
+  float mx = fmodf(x0f, (float)w), my = fmodf(y0f, (float)h);
+  if (mx < 0.0f) mx += (float)w;
+  if (my < 0.0f) my += (float)h;
+  uint32_t xa = (uint32_t)mx, ya = (uint32_t)my;
+  uint32_t xb = xa + 1u == w ? 0u : xa + 1u, yb = ya + 1u == h ? 0u : ya + 1u;
+  v4 t00 = unorm8x4(fetch(xa, ya)), t10 = unorm8x4(fetch(xb, ya));
+  v4 t01 = unorm8x4(fetch(xa, yb)), t11 = unorm8x4(fetch(xb, yb));
+  return vmix4(vmix4(t00, t10, tx), vmix4(t01, t11, tx), ty);
 }
 
 }  // namespace wb

@@ -43,6 +43,9 @@ def scene_desc(p: sc.PackedScene) -> SceneDesc:
     d.sky_height = p.sky_height
     d.bounce_limit = p.bounce_limit
     d.feature_flags = p.flags
+    if p.textures is not None:
+        d.textures_rgba8 = ptr(p.textures)
+        d.tex_layers, d.tex_height, d.tex_width = p.textures.shape[:3]
     return d
 
 

@@ -80,6 +80,21 @@ class HDRTexture:
 
 
 # ----------------------------------------------------------------------------- materials
+class Texture:
+    """tracer.js:5-20: one image of the texture array.  `image` is (H, W, 4) uint8 rgba, already at
+    the array's common size (prepareTextureArray, tracer.js:1919-1953, resizes every texture to
+    512 x 512 in the browser); texIndex is its layer once a scene is packed."""
+
+    def __init__(self, image, name: str = "New Texture"):
+        self.name = name
+        self.image = np.ascontiguousarray(image, dtype=np.uint8)
+        assert self.image.ndim == 3 and self.image.shape[2] == 4, "texture images are (H, W, 4) rgba8"
+        self.texIndex = -1
+
+
+TEXTURE_SLOTS = ("emissiveTex", "albedoTex", "normalTex", "heightTex", "roughnessTex", "metallicTex")
+
+
 class Material:
     """tracer.js:208-256"""
 
@@ -108,20 +123,23 @@ class Material:
         self.heightMultiplier = o["heightMultiplier"] if o.get("heightMultiplier") is not None else 0.05
         self.heightSamp = _js_or(o.get("heightSamp"), 32)
         self.heightOffset = _js_or(o.get("heightOffset"), 0.0)
+        for slot in TEXTURE_SLOTS:
+            setattr(self, slot, o.get(slot) or None)
         self._index = -1
 
     def schema(self):
-        """Material.getSchema (tracer.js:258-297); every texture index is -1 (no texture array)."""
+        """Material.getSchema (tracer.js:258-297)."""
         m = self
+        idx = lambda t: t.texIndex if t is not None else -1
         return [
             ("vec3f", [v ** 2.2 for v in m.color]), ("f32", m.metallic),
             ("f32", m.roughness), ("f32", m.ior), ("f32", m.specularTint), ("f32", m.anisotropic),
             ("f32", m.anisotropicRotation), ("f32", m.sheen), ("f32", m.sheenTint), ("f32", m.clearcoat),
             ("f32", m.clearcoatGloss), ("f32", m.clearcoatIor), ("f32", m.transmission), ("f32", m.concentration),
             ("vec3f", [v ** 2.2 for v in m.subsurfaceTint]), ("f32", m.subsurface),
-            ("vec3f", [v * m.emissionIntensity for v in m.emittance]), ("i32", -1),
-            ("i32", -1), ("i32", -1), ("i32", -1),
-            ("i32", -1), ("i32", -1), ("pad", None),
+            ("vec3f", [v * m.emissionIntensity for v in m.emittance]), ("i32", idx(m.emissiveTex)),
+            ("i32", idx(m.albedoTex)), ("i32", idx(m.normalTex)), ("i32", idx(m.heightTex)),
+            ("i32", idx(m.roughnessTex)), ("i32", idx(m.metallicTex)), ("pad", None),
             ("vec2f", m.uvScale),
             ("vec4f", [m.normalMultiplier, m.heightMultiplier, m.heightSamp, m.heightOffset]),
         ]
@@ -494,11 +512,23 @@ class Scene:
                 mats.append(m)
         return mats
 
+    def get_textures(self):
+        """tracer.js:1643-1653: distinct textures in material order, slot order within one."""
+        texs = []
+        for m in self.get_materials():
+            for slot in TEXTURE_SLOTS:
+                t = getattr(m, slot, None)
+                if t is not None and all(t is not x for x in texs):
+                    texs.append(t)
+        return texs
+
     @staticmethod
     def light_power(obj):
         if obj.type not in ("Sphere", "Cube"):
             return 0.0, None
         m = obj.material
+        if getattr(m, "emissiveTex", None) is not None:
+            return 0.0, None
         lum = (0.2126 * m.emittance[0] + 0.7152 * m.emittance[1] + 0.0722 * m.emittance[2]) * m.emissionIntensity
         if lum <= 0:
             return 0.0, None
@@ -575,6 +605,7 @@ class PackedScene:
     total_light_power: float
     bounce_limit: int
     flags: int
+    textures: np.ndarray | None = None     # (layers, H, W, 4) uint8 texture array, or None
     extra: dict = field(default_factory=dict)
 
 
@@ -596,9 +627,22 @@ def build_tlas(objects) -> np.ndarray:
 def pack_scene_data(scene: Scene) -> PackedScene:
     """Renderer.packSceneData(true) (tracer.js:1819-1917) plus the sky texture and CDF of
     setScene (tracer.js:1976-2004)."""
+    # prepareTextureArray runs first in setScene (tracer.js:1964): layers follow getTextures order
+    textures = scene.get_textures()
+    for i, t in enumerate(textures):
+        t.texIndex = i
+    tex_array = None
+    if textures:
+        shape = textures[0].image.shape
+        if any(t.image.shape != shape for t in textures):
+            raise ValueError("every texture must have the array's common size (the reference resizes to 512 x 512)")
+        tex_array = np.ascontiguousarray(np.stack([t.image for t in textures]), dtype=np.uint8)
     mats = scene.get_materials()
+    has_height_maps = False
     for i, m in enumerate(mats):
         m._index = i
+        if getattr(m, "heightTex", None) is not None:
+            has_height_maps = True
     mat_buf, _ = pack_data_from_schema(mats, lambda m: m.schema(), _MAT_EMPTY)
     models = [o for o in scene.objects if o.type == "Model"]
     prims = [o for o in scene.objects if o.type in ("Sphere", "Cube", "Cylinder", "Torus")]
@@ -641,6 +685,7 @@ def pack_scene_data(scene: Scene) -> PackedScene:
     flags |= HAS_LIST_MESHES if listed else 0
     flags |= HAS_PLANES if planes else 0
     flags |= HAS_LIGHTS if lights else 0
+    flags |= HAS_HEIGHTMAPS if has_height_maps else 0
     flags |= HAS_SKYBOX if scene.background is not None else 0
     flags |= MIS_SKYBOX if (scene.background is not None and not bg.plainColor and bg.enableNEE) else 0
     return PackedScene(
@@ -648,7 +693,7 @@ def pack_scene_data(scene: Scene) -> PackedScene:
         meshes=mesh_buf, bvh=bvh, triangles=tris, planes=plane_buf, lights=light_buf, sky_cdf=cdf,
         sky=np.ascontiguousarray(bg.data, dtype=np.uint16), sky_width=bg.width, sky_height=bg.height,
         sky_cdf_index=cdf_index, sky_total_lum=total, total_light_power=total_light_power,
-        bounce_limit=scene.bounces, flags=flags,
+        bounce_limit=scene.bounces, flags=flags, textures=tex_array,
     )
 
 

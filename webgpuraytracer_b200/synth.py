@@ -325,6 +325,97 @@ def flagship_scene(seed: int = 1, width: int = 1920, height: int = 1080, bounces
     return s
 
 
+# ----------------------------------------------------------------------------- textured scenes
+def texture_set(size: int = 64, seed: int = 1) -> dict[str, sc.Texture]:
+    """Seeded rgba8 images at one common size: an albedo whose alpha mixes fully transparent,
+    partly covered and opaque cells; a tangent-space normal map of sinusoidal bumps; roughness
+    (green), metallic (blue) and emissive images of value noise."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:size, 0:size].astype(np.float64) / size
+    albedo = np.empty((size, size, 4), np.uint8)
+    albedo[..., :3] = rng.integers(40, 256, (size, size, 3))
+    cells = ((x * 8).astype(int) + (y * 8).astype(int) * 3) % 4
+    albedo[..., 3] = np.array([0, 77, 200, 255], np.uint8)[cells]
+    hx = 0.35 * np.cos(2 * math.pi * 3 * x) * np.sin(2 * math.pi * 2 * y)
+    hy = 0.35 * np.sin(2 * math.pi * 3 * x) * np.cos(2 * math.pi * 2 * y)
+    n = np.stack([-hx, -hy, np.ones_like(hx)], -1)
+    n /= np.linalg.norm(n, axis=-1, keepdims=True)
+    normal = np.empty((size, size, 4), np.uint8)
+    normal[..., :3] = np.clip(np.round((n * 0.5 + 0.5) * 255), 0, 255).astype(np.uint8)
+    normal[..., 3] = 255
+
+    def noise_image(channel):
+        img = np.full((size, size, 4), 255, np.uint8)
+        img[..., :3] = 0
+        img[..., channel] = rng.integers(0, 256, (size, size))
+        return img
+
+    emissive = np.full((size, size, 4), 255, np.uint8)
+    emissive[..., :3] = (rng.random((size, size, 1)) * np.array([255, 200, 120])).astype(np.uint8)
+    return {"albedo": sc.Texture(albedo, "albedo"), "normal": sc.Texture(normal, "normal"),
+            "roughness": sc.Texture(noise_image(1), "roughness"), "metallic": sc.Texture(noise_image(2), "metallic"),
+            "emissive": sc.Texture(emissive, "emissive")}
+
+
+def textured_scene(seed: int = 1, width: int = 128, height: int = 128, bounces: int = 6, tex_size: int = 64,
+                   sky: bool = True) -> sc.Scene:
+    """Every primitive kind with textured materials: alpha cut-outs (albedo alpha) on a sphere,
+    a cube, a mesh instance, a listed mesh and a plane, so shadow rays cross partly covered
+    surfaces; normal maps on a cube, a torus and meshes (triangles and tori keep the tangent frame
+    of an earlier closest candidate); roughness and metallic maps on a cylinder; an emissive map;
+    a sphere and a box light sampled explicitly, and an importance-sampled sky."""
+    rnd = mulberry32(seed)
+    t = texture_set(tex_size, seed)
+    s = sc.Scene(width, height)
+    s.bounces = bounces
+    cut = sc.Material("cutout", [0.9, 0.8, 0.7], 0.8, albedoTex=t["albedo"], uvScale=[2.0, 1.0])
+    bumpy = sc.Material("bumpy", [0.6, 0.7, 0.9], 0.3, metallic=0.3, normalTex=t["normal"], normalMultiplier=1.5)
+    rough = sc.Material("rough", [0.8, 0.5, 0.3], 0.9, metallic=1.0, roughnessTex=t["roughness"],
+                        metallicTex=t["metallic"], clearcoat=0.5)
+    glow = sc.Material("glow", [1, 1, 1], 1.0, emittance=[1.0, 0.8, 0.6], emissionIntensity=2.0, emissiveTex=t["emissive"])
+    all_in = sc.Material("all", [0.7, 0.7, 0.7], 0.5, albedoTex=t["albedo"], normalTex=t["normal"],
+                         roughnessTex=t["roughness"], uvScale=[3.0, 3.0])
+    ground = sc.Material("ground", [0.8, 0.8, 0.8], 0.7, albedoTex=t["albedo"], normalTex=t["normal"],
+                         uvScale=[0.25, 0.25])
+    s.add(sc.Sphere("cut_sphere", cut, _uniform(rnd, -2.5, -1.5), 0.5, 0.0, 1.0))
+    s.add(sc.Cube("cut_cube", all_in, 0.5, -1.0, -1.5, 1.7, 0.2, -0.3))
+    s.add(sc.Cube("bump_cube", bumpy, -0.6, -1.9, 1.0, 0.4, -0.9, 2.0))
+    tor = s.add(sc.Torus("bump_torus", bumpy, 1.0, 0.35))
+    tor.set_position(2.2, 0.6, 1.0)
+    tor.rotate(0.7, 1, 0, 0)
+    cyl = sc.Cylinder("rough_cyl", rough, 0.6)
+    cyl.position = sc.gm.vec3(-0.5, -2.0, -2.5)
+    cyl.scale = sc.gm.vec3(0.8, 2.0, 0.8)
+    s.add(cyl)
+    s.add(sc.Sphere("glow_sphere", glow, 0.0, 2.3, -1.0, 0.4))
+    mesh = displaced_icosphere(2, 0.15, seed=seed)
+    m1 = s.add(sc.Model("cut_mesh", all_in, mesh))
+    m1.position = sc.gm.vec3(-1.2, -1.2, 2.2)
+    m1.scale = sc.gm.vec3(0.8, 0.8, 0.8)
+    m2 = s.add(sc.Model("bump_list_mesh", bumpy, mesh, in_scene_bvh=False))
+    m2.position = sc.gm.vec3(1.6, -1.4, 2.6)
+    m2.scale = sc.gm.vec3(0.6, 0.6, 0.6)
+    s.add(sc.Plane("ground", ground, 0, 1, 0, -2.0))
+    lamp = sc.Material("lamp", [1, 0.9, 0.8], 1.0, emittance=[1, 0.9, 0.7], emissionIntensity=8.0)
+    a = s.add(sc.Sphere("lamp0", lamp, 0.8, 4.0, 1.5, 0.5))
+    a.enableNEE = True
+    b = s.add(sc.Cube("lamp1", lamp, -3.0, 3.0, -2.0, -2.2, 3.5, -1.4))
+    b.enableNEE = True
+    if sky:
+        s.background = sc.HDRTexture.from_rgbe(encode_rgbe(procedural_sky(256, 128, sun_radiance=2e3,
+                                                                          sun_diameter_deg=3.0)), exposure=1.0)
+    else:
+        s.background = sc.HDRTexture([1.0, 1.0, 1.0])
+    cam = s.camera
+    cam.position = sc.gm.vec3(0.0, 2.0, 9.0)
+    cam.target = sc.gm.vec3(0.0, -0.5, 0.0)
+    cam.fov = 50.0
+    cam.aperture = 0.0
+    cam.exposure = 1.0
+    cam.aspect = width / height
+    return s
+
+
 BATCH_SIZES = ((256, 256), (512, 512), (1280, 720), (1920, 1080))
 BATCH_SPP = (4, 16, 64)
 

@@ -28,7 +28,7 @@ enum wgpt_status {
   WGPT_E_CUDA = 3,        /* a CUDA runtime call failed */
   WGPT_E_NOMEM = 4,       /* device allocation failed */
   WGPT_E_STATE = 5,       /* call out of order (no scene, no size, no G-buffer) */
-  WGPT_E_UNSUPPORTED = 6, /* textures / parallax maps (not part of this build) */
+  WGPT_E_UNSUPPORTED = 6, /* a combination this build does not run (e.g. FP64 accumulation in the single-kernel mode) */
   WGPT_E_REBUILD = 7,     /* wgpt_update_scene: the new data does not fit, upload again */
   WGPT_E_DEVICE = 8,      /* a kernel reported an error (traversal stack overflow) */
   WGPT_E_TOO_LARGE = 9    /* wgpt_denoise_noalloc: more than WGPT_NOALLOC_MAX_PIXELS pixels */

@@ -13,8 +13,8 @@
 // Parity is unpinned by the reference itself (it ships no tests, golden images or known-answer
 // vectors and its WGSL cannot run without a graphics stack).
 //
-// Textures (binding 11/12) and parallax mapping are not restated: every texture index must be
-// negative (sample_texture(idx<0) = vec4(1), shader.wgsl:170-173) and HAS_HEIGHTMAPS must be off.
+// Textures (bindings 11/12) are sampled by wgsl_builtins.h's pinned FP32 bilinear, repeating
+// sampler (the WebGPU sampler's precision is implementation-defined).
 #include <stdint.h>
 #include <string.h>
 #include <math.h>
@@ -1084,6 +1084,72 @@ SurfaceContext get_surface_context(const Scene* s, const SurfaceHit& hit, const 
   return ctx;
 }
 
+// shader.wgsl:1230-1278.  A result that leaves through the early return keeps WGSL's zero
+// initialisation (uv (0, 0), height 0), which main then uses as the texture coordinate.
+struct PomResult { v2 uv; float height; bool hit; };
+float height_depth(const Scene* s, int32_t height_idx, v2 uv, bool is_height_map) {
+  float v = sample_texture(s, height_idx, uv).x;
+  return is_height_map ? 1.0f - v : v;
+}
+PomResult calculate_pom(const Scene* s, v2 initial_uv, v3 view_ts, float start_depth, const wgpt_material& mat,
+                        int32_t height_idx) {
+  PomResult res;
+  res.uv = mk2(0.0f, 0.0f); res.height = 0.0f; res.hit = false;
+  float hm = mat.height_params[1];
+  bool is_height_map = hm < 0.0f;
+  float scale = absf(hm);
+  float num_layers = mat.height_params[2];
+  float layer_depth = 1.0f / num_layers;
+  float cur_layer = clamp(start_depth, 0.0f, 1.0f);
+  v2 P = mk2(-(view_ts.x / view_ts.z), -(view_ts.y / view_ts.z)) * scale;
+  v2 delta = mk2(P.x / num_layers, P.y / num_layers);
+  v2 cur_uv = initial_uv - P * mat.height_params[3];
+  float cur_depth = height_depth(s, height_idx, cur_uv, is_height_map);
+  for (int i = 0; i < 64; i++) {
+    if ((float)i >= num_layers || cur_layer >= cur_depth) break;
+    if (cur_layer > 1.0f || cur_layer < 0.0f) return res;
+    cur_uv = cur_uv + delta;
+    cur_depth = height_depth(s, height_idx, cur_uv, is_height_map);
+    cur_layer += layer_depth;
+  }
+  v2 prev_uv = cur_uv - delta;
+  float prev_depth = height_depth(s, height_idx, prev_uv, is_height_map);
+  float after = cur_depth - cur_layer;
+  float before = prev_depth - cur_layer + layer_depth;
+  float weight = after / (after - before);
+  res.uv = mk2(mix(cur_uv.x, prev_uv.x, weight), mix(cur_uv.y, prev_uv.y, weight));
+  res.height = mix(cur_layer, cur_layer - layer_depth, weight);
+  res.hit = true;
+  return res;
+}
+
+// shader.wgsl:1280-1328
+PomResult calculate_shadow_pom(const Scene* s, v2 current_uv, float current_height, v3 light_ts,
+                               const wgpt_material& mat, int32_t height_idx) {
+  PomResult res;
+  res.hit = false; res.uv = current_uv; res.height = current_height;
+  if (light_ts.z <= 0.0f) { res.hit = true; return res; }
+  float hm = mat.height_params[1];
+  bool is_height_map = hm < 0.0f;
+  float scale = absf(hm);
+  float num_layers = mat.height_params[2];
+  float layer_depth = 1.0f / num_layers;
+  v2 p = (mk2(light_ts.x / light_ts.z, light_ts.y / light_ts.z) * scale) * layer_depth;
+  v2 shadow_uv = current_uv;
+  float shadow_depth = current_height;
+  for (int i = 0; i < 32; i++) {
+    if ((float)i / 2.0f >= num_layers || shadow_depth <= 0.0f) break;
+    shadow_uv = shadow_uv + p;
+    shadow_depth -= layer_depth;
+    float map_depth = height_depth(s, height_idx, shadow_uv, is_height_map);
+    if (map_depth < shadow_depth) {
+      res.hit = true; res.uv = shadow_uv; res.height = map_depth;
+      return res;
+    }
+  }
+  return res;
+}
+
 // shader.wgsl:1459-1464
 m3 build_tangent_space(v3 N) {
   v3 a = vsel(mk3(0.0f, 1.0f, 0.0f), mk3(0.0f, 0.0f, 1.0f), absf(N.y) > 0.99999f);
@@ -1573,9 +1639,10 @@ v3 clamp_firefly(v3 rad, int bounce) {
   return rad;
 }
 
-// shader.wgsl:2226-2271 (without heightmaps)
+// shader.wgsl:2226-2271
 v3 evaluate_nee(Ctx& c, const LightSample& ls, v3 hit_pos, v3 n_orient, v3 V, const wgpt_material& mat,
-                const SurfaceContext& ctx, const MediumStack* stack, int32_t ignore_obj_idx) {
+                const SurfaceContext& ctx, const m3& tbn, float currentheight, v2 final_uv,
+                const MediumStack* stack, int32_t ignore_obj_idx) {
   if (ls.pdf <= 0.0f) return mk3s(0.0f);
   float dotNL = dot(n_orient, ls.dir);
   if (dotNL <= 0.0f && mat.transmission <= 0.0f) return mk3s(0.0f);
@@ -1588,9 +1655,15 @@ v3 evaluate_nee(Ctx& c, const LightSample& ls, v3 hit_pos, v3 n_orient, v3 V, co
   v3 ray_offset = dotNL < 0.0f ? -n_orient * 0.001f : n_orient * 0.001f;
   Ray shadow_ray; shadow_ray.origin = hit_pos + ray_offset; shadow_ray.direction = ls.dir;
   bool in_shadow = false;
-  v3 shadow_hit = trace_scene_shadow(c, shadow_ray, ignore_obj_idx, ls.dist);
-  sample_color = sample_color * shadow_hit;
-  if (max_component(shadow_hit) < 0.001f) in_shadow = true;
+  if (HAS(c.s, WGPT_HAS_HEIGHTMAPS) && mat.height_idx >= 0) {
+    v3 light_ts = normalize(mul3t(tbn, ls.dir));
+    if (calculate_shadow_pom(c.s, final_uv, currentheight, light_ts, mat, mat.height_idx).hit) in_shadow = true;
+  }
+  if (!in_shadow) {
+    v3 shadow_hit = trace_scene_shadow(c, shadow_ray, ignore_obj_idx, ls.dist);
+    sample_color = sample_color * shadow_hit;
+    if (max_component(shadow_hit) < 0.001f) in_shadow = true;
+  }
   if (!in_shadow) return sample_color * c_weight;
   return mk3s(0.0f);
 }
@@ -1649,9 +1722,18 @@ void main_pixel(Ctx& c, uint32_t ix, uint32_t iy, float* accum, uint8_t* out) {
     }
     c.count(C_SHADE);
     const wgpt_material& mat = s->mats[hit.m_idx];
-    // shader.wgsl:2361-2375 (the POM branch needs HAS_HEIGHTMAPS, which is rejected on upload)
+    // shader.wgsl:2361-2375
     v2 final_uv = hit.hit_uv * L2(mat.uv_scale);
     m3 tbn; tbn.c[0] = hit.tangent; tbn.c[1] = hit.bitangent; tbn.c[2] = hit.hit_n;
+    float currentheight = 0.0f;
+    if (HAS(s, WGPT_HAS_HEIGHTMAPS) && mat.height_idx >= 0) {
+      v3 view_ts = normalize(mul3t(tbn, -ray.direction));
+      if (view_ts.z > 0.0f) {
+        PomResult pom = calculate_pom(s, final_uv, view_ts, 0.0f, mat, mat.height_idx);
+        final_uv = pom.uv;
+        currentheight = pom.height;
+      }
+    }
     SurfaceContext ctx = get_surface_context(s, hit, mat, tbn, final_uv);
     if (length(ctx.emittance) > 0.0f) {
       float weight = 1.0f;
@@ -1695,7 +1777,8 @@ void main_pixel(Ctx& c, uint32_t ix, uint32_t iy, float* accum, uint8_t* out) {
         if (light_sample.pdf > 0.0f) {
           float selection_pdf = selected_weight / weight_sum;
           light_sample.pdf *= selection_pdf;
-          v3 incoming = evaluate_nee(c, light_sample, hit_pos, n_orient, V, mat, ctx, &stack, light.obj_idx);
+          v3 incoming = evaluate_nee(c, light_sample, hit_pos, n_orient, V, mat, ctx, tbn, currentheight, final_uv,
+                                     &stack, light.obj_idx);
           radiance = radiance + throughput * clamp_firefly(incoming, bounce);
         }
       }
@@ -1706,10 +1789,23 @@ void main_pixel(Ctx& c, uint32_t ix, uint32_t iy, float* accum, uint8_t* out) {
       float u0 = rand_pcg(c.rng);
       float u1 = rand_pcg(c.rng);
       LightSample env_sample = sample_env_cdf(c, mk2(u0, u1));
-      v3 incoming = evaluate_nee(c, env_sample, hit_pos, n_orient, V, mat, ctx, &stack, -1);
+      v3 incoming = evaluate_nee(c, env_sample, hit_pos, n_orient, V, mat, ctx, tbn, currentheight, final_uv, &stack,
+                                 -1);
       radiance = radiance + throughput * clamp_firefly(incoming, bounce);
     }
     if (!sample_surface(c, &ray, &throughput, hit_pos, mat, ctx, &stack, &last_surface_pdf)) break;
+    // shader.wgsl:2458-2472: self-shadowing of the height field along the sampled direction
+    if (HAS(s, WGPT_HAS_HEIGHTMAPS) && mat.height_idx >= 0) {
+      v3 light_ts = normalize(mul3t(tbn, ray.direction));
+      PomResult sh = calculate_shadow_pom(s, final_uv, currentheight, light_ts, mat, mat.height_idx);
+      if (sh.hit) {
+        final_uv = sh.uv;
+        SurfaceContext ctx_pom = get_surface_context(s, hit, mat, tbn, final_uv);
+        radiance = radiance + throughput * clamp_firefly(ctx_pom.emittance, bounce);
+        if (length(ctx_pom.emittance) > 1.0f) break;
+        if (!sample_surface(c, &ray, &throughput, hit_pos, mat, ctx_pom, &stack, &last_surface_pdf)) break;
+      }
+    }
     if (bounce < 2) continue;
     float pmax = max_component(throughput);
     float survival_prob = clamp(pmax, 0.05f, 0.95f);

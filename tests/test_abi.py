@@ -81,11 +81,17 @@ def test_validate_accepts_generated_scenes_and_rejects_bad_indices():
     bad.textures = np.zeros((1, 8, 8, 4), np.uint8)
     d = _desc(bad)
     assert L.wgpt_validate_scene(C.byref(d), msg, 256) == 0, msg.value
-    # parallax maps are not part of this build
+    # parallax maps are accepted; a height-map index beyond the array is a layout error too
     bad = sc.PackedScene(**{**p.__dict__})
     bad.flags = p.flags | _lib.HAS_HEIGHTMAPS
     d = _desc(bad)
-    assert L.wgpt_validate_scene(C.byref(d), msg, 256) == 6
+    assert L.wgpt_validate_scene(C.byref(d), msg, 256) == 0, msg.value
+    mt = p.materials.copy().view(np.int32).reshape(-1, 36)
+    mt[0, 26] = 0                    # height_idx
+    bad.materials = mt.view(np.uint8).reshape(-1).copy()
+    d = _desc(bad)
+    assert L.wgpt_validate_scene(C.byref(d), msg, 256) == 2
+    assert b"texture index" in msg.value
     # a size that is not a whole number of records
     bad = sc.PackedScene(**{**p.__dict__})
     bad.objects = p.objects[:-4].copy()

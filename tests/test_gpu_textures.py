@@ -4,7 +4,10 @@ The scene covers every primitive kind with albedo (alpha cut-out), normal, rough
 and emissive maps; shadow rays of the sphere and box lights and of the sky cross alpha-textured
 occluders (transmittance products), and mesh and torus hits with normal maps use the tangent
 frame of the last plane, sphere or cube accepted before them on the ray, as the reference does.
-Both forms of main (wavefront and single kernel) and gbuf_main are compared.
+With height fields, main's parallax occlusion mapping (coordinate shift, the height field's
+shadow test in next-event estimation and the second BSDF sample after a self-shadowed
+direction) is exercised too.  Both forms of main (wavefront and single kernel) and gbuf_main
+are compared.
 """
 from __future__ import annotations
 
@@ -19,10 +22,13 @@ from webgpuraytracer_b200 import synth
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module", params=[True, False], ids=["sky", "plain"])
+@pytest.fixture(scope="module", params=[(True, False), (False, False), (True, True)], ids=["sky", "plain", "pom"])
 def textured(request):
-    s = synth.textured_scene(1, 128, 128, 6, sky=request.param)
-    return s, sc.pack_scene_data(s)
+    sky, pom = request.param
+    s = synth.textured_scene(1, 128, 128, 6, sky=sky, pom=pom)
+    p = sc.pack_scene_data(s)
+    assert bool(p.flags & sc.HAS_HEIGHTMAPS) == pom
+    return s, p
 
 
 def _params(scene, packed, w, h):

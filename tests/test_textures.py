@@ -118,3 +118,24 @@ def test_textured_scene_oracle_effects():
                          oracle.default_threads()) == 0
     assert np.isfinite(acc).all() and np.isfinite(acc2).all()
     assert (np.abs(acc - acc2)[..., :3].max(-1) > 1e-3).mean() > 0.3
+
+
+def test_parallax_scene_oracle():
+    """Height fields shift the texture coordinates and shadow: the parallax scene renders finite
+    values that differ from the same scene with HAS_HEIGHTMAPS cleared."""
+    s = synth.textured_scene(1, 48, 48, 4, tex_size=16, pom=True)
+    p = sc.pack_scene_data(s)
+    assert p.flags & sc.HAS_HEIGHTMAPS
+    s.camera.update_rays2()
+    params = sc.pack_params(s, p, 48, 48, 0, 1, (0, 0))
+    out = np.zeros((48, 48, 4), np.uint8)
+    accs = []
+    for flags in (p.flags, p.flags & ~sc.HAS_HEIGHTMAPS):
+        q = sc.PackedScene(**{**p.__dict__})
+        q.flags = flags
+        acc = np.zeros((48, 48, 4), np.float32)
+        assert oracle.render(oracle.OracleScene(q), params, 0, 2, (0, 0, 48, 48), acc, out,
+                             oracle.default_threads()) == 0
+        accs.append(acc)
+    assert np.isfinite(accs[0]).all()
+    assert (np.abs(accs[0] - accs[1])[..., :3].max(-1) > 1e-3).mean() > 0.05

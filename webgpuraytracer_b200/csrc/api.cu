@@ -309,7 +309,6 @@ int check_desc(wgpt_ctx* ctx, const wgpt_scene_desc* d, HostScene& hs) {
       return fail(ctx, WGPT_E_LAYOUT, std::string(kName[k]) + ": size is not a multiple of its record size");
   }
   if (d->bounce_limit < 0) return fail(ctx, WGPT_E_INVALID, "bounce_limit must be >= 0");
-  if (d->feature_flags & WGPT_HAS_HEIGHTMAPS) return fail(ctx, WGPT_E_UNSUPPORTED, "HAS_HEIGHTMAPS (parallax maps) is not supported by this build");
   if (d->feature_flags & ~0x7ffu) return fail(ctx, WGPT_E_INVALID, "unknown feature flag bits");
   if ((d->feature_flags & WGPT_HAS_SKYBOX) && (!d->sky_rgba16f || d->sky_width == 0 || d->sky_height == 0))
     return fail(ctx, WGPT_E_INVALID, "sky texture missing while HAS_SKYBOX is set");
@@ -357,12 +356,14 @@ void fill_device_scene(wgpt_ctx* ctx, const wgpt_scene_desc* d) {
   s.bounce_limit = d->bounce_limit;
   s.flags = d->feature_flags;
   const wgpt_material* m = (const wgpt_material*)d->materials.ptr;
+  const bool pom = (d->feature_flags & WGPT_HAS_HEIGHTMAPS) != 0u;
   for (uint32_t i = 0; i < (uint32_t)(d->materials.bytes / WGPT_STRIDE_MATERIAL); ++i) {
+    const bool height = pom && m[i].height_idx >= 0;
     if (m[i].emissive_idx >= 0 || m[i].albedo_idx >= 0 || m[i].normal_idx >= 0 || m[i].roughness_idx >= 0 ||
-        m[i].metallic_idx >= 0)
+        m[i].metallic_idx >= 0 || height)
       s.flags |= wgpt::SCENE_TEXTURED;
     if (m[i].albedo_idx >= 0) s.flags |= wgpt::SCENE_ALPHA_SHADOWS;
-    if (m[i].normal_idx >= 0) s.flags |= wgpt::SCENE_NORMAL_MAPS;
+    if (m[i].normal_idx >= 0 || height) s.flags |= wgpt::SCENE_TANGENTS;
   }
 }
 

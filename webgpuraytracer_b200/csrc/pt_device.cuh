@@ -114,14 +114,16 @@ static __device__ __forceinline__ v3 load_mat_emittance(const DScene& s, int32_t
   return f3(ld4(s.mats + (size_t)i * 9 + 5));
 }
 
-// Texture fields of a material record (words 23-35 of the 144-byte record).
-struct DMatTex { int32_t emissive, albedo, normal, roughness, metallic; v2 uv_scale; float height0; };
+// Texture fields of a material record (words 23-35 of the 144-byte record); hp = height_params
+// (normal multiplier, height multiplier, layer count, offset).
+struct DMatTex { int32_t emissive, albedo, normal, height, roughness, metallic; v2 uv_scale; v4 hp; };
 static __device__ __forceinline__ DMatTex load_mat_tex(const DScene& s, int32_t i) {
   const float4* p = s.mats + (size_t)i * 9;
   float4 f = ld4(p + 5), g = ld4(p + 6), h = ld4(p + 7), k = ld4(p + 8);
   DMatTex t;
-  t.emissive = bi(f.w); t.albedo = bi(g.x); t.normal = bi(g.y); t.roughness = bi(g.w); t.metallic = bi(h.x);
-  t.uv_scale = mk2(h.z, h.w); t.height0 = k.x;
+  t.emissive = bi(f.w); t.albedo = bi(g.x); t.normal = bi(g.y); t.height = bi(g.z); t.roughness = bi(g.w);
+  t.metallic = bi(h.x);
+  t.uv_scale = mk2(h.z, h.w); t.hp = mk4(k.x, k.y, k.z, k.w);
   return t;
 }
 
@@ -1104,23 +1106,90 @@ static __device__ __forceinline__ SurfCtx plain_context(const DMat& mat, v3 hit_
   return c;
 }
 
-// get_surface_context (shader.wgsl:1393-1440, without the parallax branch): normal map in the
-// frame (T, B, hit_n), albedo (sRGB-decoded, alpha from its fourth channel), roughness (second
-// channel), metallic (third channel) and emissive maps at uv * uv_scale.
-static __device__ __noinline__ SurfCtx surface_context(const DScene& s, int32_t m_idx, const DMat& mat, v3 hit_n,
-                                                      const UvFrame& f) {
-  DMatTex mt = load_mat_tex(s, m_idx);
-  v2 uv = f.uv * mt.uv_scale;
+// Texture state of a shading point: the material's texture fields, the frame (tangent,
+// bitangent, hit normal), the texture coordinate after the uv scale and parallax shift, and the
+// depth parallax mapping found (currentheight of main).
+struct TexPoint { DMatTex mt; m3 tbn; v2 uv; float height; };
+
+// calculate_pom (shader.wgsl:1237-1278).  A result that leaves through the early return keeps
+// WGSL's zero initialisation (uv (0, 0), height 0), which main then uses as the coordinate.
+struct PomResult { v2 uv; float height; bool hit; };
+static __device__ __forceinline__ float height_depth(const DScene& s, int32_t idx, v2 uv, bool is_height_map) {
+  float v = sample_texture(s, idx, uv).x;
+  return is_height_map ? 1.0f - v : v;
+}
+static __device__ __noinline__ PomResult calculate_pom(const DScene& s, v2 initial_uv, v3 view_ts, float start_depth,
+                                                       const DMatTex& mt) {
+  PomResult res;
+  res.uv = mk2(0.0f, 0.0f); res.height = 0.0f; res.hit = false;
+  const bool is_height_map = mt.hp.y < 0.0f;
+  const float scale = absf(mt.hp.y);
+  const float num_layers = mt.hp.z;
+  const float layer_depth = 1.0f / num_layers;
+  float cur_layer = clamp(start_depth, 0.0f, 1.0f);
+  v2 P = mk2(-(view_ts.x / view_ts.z), -(view_ts.y / view_ts.z)) * scale;
+  v2 delta = mk2(P.x / num_layers, P.y / num_layers);
+  v2 cur_uv = initial_uv - P * mt.hp.w;
+  float cur_depth = height_depth(s, mt.height, cur_uv, is_height_map);
+  for (int i = 0; i < 64; i++) {
+    if ((float)i >= num_layers || cur_layer >= cur_depth) break;
+    if (cur_layer > 1.0f || cur_layer < 0.0f) return res;
+    cur_uv = cur_uv + delta;
+    cur_depth = height_depth(s, mt.height, cur_uv, is_height_map);
+    cur_layer += layer_depth;
+  }
+  v2 prev_uv = cur_uv - delta;
+  float prev_depth = height_depth(s, mt.height, prev_uv, is_height_map);
+  float after = cur_depth - cur_layer;
+  float before = prev_depth - cur_layer + layer_depth;
+  float weight = after / (after - before);
+  res.uv = mk2(mix(cur_uv.x, prev_uv.x, weight), mix(cur_uv.y, prev_uv.y, weight));
+  res.height = mix(cur_layer, cur_layer - layer_depth, weight);
+  res.hit = true;
+  return res;
+}
+
+// calculate_shadow_pom (shader.wgsl:1280-1328): marches from the parallax point toward the
+// surface along light_ts; hit when the height field is above the ray (or the light is behind).
+static __device__ __noinline__ PomResult calculate_shadow_pom(const DScene& s, v2 current_uv, float current_height,
+                                                              v3 light_ts, const DMatTex& mt) {
+  PomResult res;
+  res.hit = false; res.uv = current_uv; res.height = current_height;
+  if (light_ts.z <= 0.0f) { res.hit = true; return res; }
+  const bool is_height_map = mt.hp.y < 0.0f;
+  const float scale = absf(mt.hp.y);
+  const float num_layers = mt.hp.z;
+  const float layer_depth = 1.0f / num_layers;
+  v2 p = (mk2(light_ts.x / light_ts.z, light_ts.y / light_ts.z) * scale) * layer_depth;
+  v2 shadow_uv = current_uv;
+  float shadow_depth = current_height;
+  for (int i = 0; i < 32; i++) {
+    if ((float)i / 2.0f >= num_layers || shadow_depth <= 0.0f) break;
+    shadow_uv = shadow_uv + p;
+    shadow_depth -= layer_depth;
+    float map_depth = height_depth(s, mt.height, shadow_uv, is_height_map);
+    if (map_depth < shadow_depth) {
+      res.hit = true; res.uv = shadow_uv; res.height = map_depth;
+      return res;
+    }
+  }
+  return res;
+}
+
+// get_surface_context (shader.wgsl:1393-1440): normal map in the frame tp.tbn, albedo
+// (sRGB-decoded, alpha from its fourth channel), roughness (second channel), metallic (third
+// channel) and emissive maps at the coordinate uv.
+static __device__ __noinline__ SurfCtx surface_context(const DScene& s, const DMat& mat, v3 hit_n, const TexPoint& tp,
+                                                      v2 uv) {
+  const DMatTex& mt = tp.mt;
   SurfCtx c;
   c.normal = hit_n;
   c.surface_normal = hit_n;
   if (mt.normal >= 0) {
     v4 t = sample_texture(s, mt.normal, uv);
     v3 n_map = mk3(t.x, t.y, t.z) * 2.0f - mk3s(1.0f);
-    n_map = normalize(n_map * mk3(mt.height0, mt.height0, 1.0f));
-    m3 tbn;
-    tbn.c[0] = f.T; tbn.c[1] = f.B; tbn.c[2] = hit_n;
-    c.normal = normalize(mul3(tbn, n_map));
+    n_map = normalize(n_map * mk3(mt.hp.x, mt.hp.x, 1.0f));
+    c.normal = normalize(mul3(tp.tbn, n_map));
   }
   c.albedo = mat.color;
   c.alpha = 1.0f;
@@ -1141,12 +1210,38 @@ static __device__ __noinline__ SurfCtx surface_context(const DScene& s, int32_t 
   return c;
 }
 
-// The surface context of the closest hit hn = hit_normal(...) of material hit.m_idx.
+// The surface context of the closest hit hn = hit_normal(...) of material hit.m_idx
+// (shader.wgsl:2361-2375): texture coordinate, tangent frame and (with `parallax`, which main
+// applies and gbuf_main does not) the parallax shift into *tp.
 template <bool TEX>
 static __device__ __forceinline__ SurfCtx hit_context(const DScene& s, const Ray& rw, const HitRec& hit,
-                                                      const DMat& mat, v3 hn) {
+                                                      const DMat& mat, v3 hn, TexPoint* tp, bool parallax) {
   if (!HAS_TEX<TEX>(s, wgpt::SCENE_TEXTURED)) return plain_context(mat, hn);
-  return surface_context(s, hit.m_idx, mat, hn, hit_uv_frame(s, rw, hit));
+  UvFrame f = hit_uv_frame(s, rw, hit);
+  tp->mt = load_mat_tex(s, hit.m_idx);
+  tp->tbn.c[0] = f.T; tp->tbn.c[1] = f.B; tp->tbn.c[2] = hn;
+  tp->uv = f.uv * tp->mt.uv_scale;
+  tp->height = 0.0f;
+  if (parallax && HAS(s, WGPT_HAS_HEIGHTMAPS) && tp->mt.height >= 0) {
+    v3 view_ts = normalize(mul3t(tp->tbn, -rw.direction));
+    if (view_ts.z > 0.0f) {
+      PomResult pom = calculate_pom(s, tp->uv, view_ts, 0.0f, tp->mt);
+      tp->uv = pom.uv;
+      tp->height = pom.height;
+    }
+  }
+  return surface_context(s, mat, hn, *tp, tp->uv);
+}
+
+// True when the point's height field shadows direction dir (evaluate_nee's parallax test and
+// main's after sample_surface, shader.wgsl:2254-2257, 2459-2461); *uv receives the result's
+// coordinate.
+template <bool TEX>
+static __device__ __forceinline__ bool pom_shadowed(const DScene& s, const TexPoint& tp, v3 dir, v2* uv) {
+  if (!(HAS_TEX<TEX>(s, WGPT_HAS_HEIGHTMAPS) && tp.mt.height >= 0)) return false;
+  PomResult r = calculate_shadow_pom(s, tp.uv, tp.height, normalize(mul3t(tp.tbn, dir)), tp.mt);
+  *uv = r.uv;
+  return r.hit;
 }
 
 // shader.wgsl:1700-1704

@@ -19,10 +19,11 @@ struct PathState {
   Counters<COUNT> cn;
 };
 
-// shader.wgsl:2226-2271 (heightmaps off)
+// shader.wgsl:2226-2271
 template <bool COUNT, bool TEX>
 __device__ v3 evaluate_nee(const DScene& s, const LightSample& ls, v3 hit_pos, v3 n_orient, v3 V, const DMat& mat,
-                           const SurfCtx& ctx, const MediumStack& stack, int32_t ignore_obj_idx, PathState<COUNT>& ps) {
+                           const SurfCtx& ctx, const TexPoint& tp, const MediumStack& stack, int32_t ignore_obj_idx,
+                           PathState<COUNT>& ps) {
   if (ls.pdf <= 0.0f) return mk3s(0.0f);
   float dotNL = dot(n_orient, ls.dir);
   if (dotNL <= 0.0f && mat.transmission <= 0.0f) return mk3s(0.0f);
@@ -33,6 +34,8 @@ __device__ v3 evaluate_nee(const DScene& s, const LightSample& ls, v3 hit_pos, v
   if (max_component(ls.color * c_weight) < 1e-5f) return mk3s(0.0f);
   v3 ray_offset = dotNL < 0.0f ? -n_orient * 0.001f : n_orient * 0.001f;
   Ray sr; sr.origin = hit_pos + ray_offset; sr.direction = ls.dir;
+  v2 pom_uv;
+  if (pom_shadowed<TEX>(s, tp, ls.dir, &pom_uv)) return mk3s(0.0f);
   float shadow = scene_shadow<COUNT, TEX>(s, sr, ignore_obj_idx, ls.dist, ps.err, ps.cn);
   if (shadow < 0.001f) return mk3s(0.0f);
   return (ls.color * shadow) * c_weight;
@@ -197,7 +200,8 @@ __device__ v3 trace_path(const DScene& s, const DParams& p, uint32_t ix, uint32_
     ps.cn.add(C_HIT_ATTR);
     DMat mat = load_mat(s, hit.m_idx);
     v3 hn = hit_normal(s, ray, hit);
-    SurfCtx ctx = hit_context<TEX>(s, ray, hit, mat, hn);
+    TexPoint tp;
+    SurfCtx ctx = hit_context<TEX>(s, ray, hit, mat, hn, &tp, true);
 
     // shader.wgsl:2378-2395 implicit light hit
     float em_len = length(ctx.emittance);
@@ -258,7 +262,7 @@ __device__ v3 trace_path(const DScene& s, const DParams& p, uint32_t ix, uint32_
         }
         if (ls.pdf > 0.0f) {
           ls.pdf *= selected_weight / weight_sum;
-          v3 incoming = evaluate_nee<COUNT, TEX>(s, ls, hit_pos, n_orient, V, mat, ctx, stack, light.obj_idx, ps);
+          v3 incoming = evaluate_nee<COUNT, TEX>(s, ls, hit_pos, n_orient, V, mat, ctx, tp, stack, light.obj_idx, ps);
           radiance = radiance + throughput * clamp_firefly(incoming, bounce);
         }
       }
@@ -270,10 +274,19 @@ __device__ v3 trace_path(const DScene& s, const DParams& p, uint32_t ix, uint32_
       float u0 = rand_pcg(ps.rng);
       float u1 = rand_pcg(ps.rng);
       LightSample env = sample_env_cdf(s, p, u0, u1, ps.cn);
-      v3 incoming = evaluate_nee<COUNT, TEX>(s, env, hit_pos, n_orient, V, mat, ctx, stack, -1, ps);
+      v3 incoming = evaluate_nee<COUNT, TEX>(s, env, hit_pos, n_orient, V, mat, ctx, tp, stack, -1, ps);
       radiance = radiance + throughput * clamp_firefly(incoming, bounce);
     }
     if (!sample_surface<COUNT, TEX>(ray, throughput, hit_pos, mat, ctx, stack, last_surface_pdf, ps)) break;
+    // shader.wgsl:2458-2472: the height field shadows the sampled direction: shade the occluding
+    // texel and sample again from it
+    v2 pom_uv;
+    if (pom_shadowed<TEX>(s, tp, ray.direction, &pom_uv)) {
+      SurfCtx cp = surface_context(s, mat, hn, tp, pom_uv);
+      radiance = radiance + throughput * clamp_firefly(cp.emittance, bounce);
+      if (length(cp.emittance) > 1.0f) break;
+      if (!sample_surface<COUNT, TEX>(ray, throughput, hit_pos, mat, cp, stack, last_surface_pdf, ps)) break;
+    }
     if (bounce < 2) continue;
     float survival_prob = clamp(max_component(throughput), 0.05f, 0.95f);
     if (rand_pcg(ps.rng) > survival_prob) break;
@@ -357,7 +370,8 @@ k_gbuffer(DScene s, DParams p, uint32_t sec_w, uint32_t sec_h, float* __restrict
       break;
     }
     DMat mat = load_mat(s, hit.m_idx);
-    SurfCtx ctx = hit_context<TEX>(s, ray, hit, mat, hit_normal(s, ray, hit));
+    TexPoint tp;
+    SurfCtx ctx = hit_context<TEX>(s, ray, hit, mat, hit_normal(s, ray, hit), &tp, false);
     c_albedo = ctx.albedo; c_rough = ctx.roughness; c_metal = ctx.metallic; c_emit = ctx.emittance;
     m_trans = mat.transmission;
     c_normal = dot(ctx.normal, -ray.direction) > 0.0f ? ctx.normal : -ctx.normal;

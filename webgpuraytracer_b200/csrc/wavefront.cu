@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(256) k_wf_extend(WfArgs a) {
       const HitRec& h = t.hit;
       a.b.hit[slot * 2 + 0] = make_uint4(__float_as_uint(h.t), (uint32_t)h.m_idx, (uint32_t)h.o_idx, (uint32_t)h.kind);
       a.b.hit[slot * 2 + 1] = make_uint4((uint32_t)h.id, (uint32_t)h.aux, __float_as_uint(h.bu), __float_as_uint(h.bv));
-      if (HAS(a.s, wgpt::SCENE_NORMAL_MAPS)) a.b.tsrc[slot] = make_uint2((uint32_t)h.tsrc, __float_as_uint(h.tsrc_t));
+      if (HAS(a.s, wgpt::SCENE_TANGENTS)) a.b.tsrc[slot] = make_uint2((uint32_t)h.tsrc, __float_as_uint(h.tsrc_t));
       have = false;
     }
   }
@@ -372,8 +372,8 @@ __global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a) {
 // radiance if the light is visible, and the shadow ray to test (when evaluate_nee reaches it).
 template <bool COUNT, bool TEX>
 __device__ void record_nee(const WfArgs& a, uint32_t slot, int rec, const LightSample& ls, v3 hit_pos, v3 n_orient,
-                           v3 V, const DMat& mat, const SurfCtx& ctx, const MediumStack& stack, int32_t ignore_idx,
-                           v3 throughput, uint32_t& flags) {
+                           v3 V, const DMat& mat, const SurfCtx& ctx, const TexPoint& tp, const MediumStack& stack,
+                           int32_t ignore_idx, v3 throughput, uint32_t& flags) {
   v3 incoming = mk3s(0.0f);
   bool shadow = false;
   v3 so = mk3s(0.0f);
@@ -385,7 +385,8 @@ __device__ void record_nee(const WfArgs& a, uint32_t slot, int rec, const LightS
       bsdf_eval_pdf<TEX>(V, ls.dir, mat, ctx, stack, &bsdf_val, &bsdf_pdf);
       float weight = mis_weight(ls.pdf, bsdf_pdf);
       v3 c_weight = (bsdf_val * weight) / wmax(ls.pdf, 1e-6f);
-      if (!(max_component(ls.color * c_weight) < 1e-5f)) {
+      v2 pom_uv;
+      if (!(max_component(ls.color * c_weight) < 1e-5f) && !pom_shadowed<TEX>(a.s, tp, ls.dir, &pom_uv)) {
         v3 ray_offset = dotNL < 0.0f ? -n_orient * 0.001f : n_orient * 0.001f;
         so = hit_pos + ray_offset;
         if (HAS_TEX<TEX>(a.s, wgpt::SCENE_ALPHA_SHADOWS)) {
@@ -407,6 +408,136 @@ __device__ void record_nee(const WfArgs& a, uint32_t slot, int rec, const LightS
     a.b.shadow[slot * 4 + rec * 2] = make_float4(so.x, so.y, so.z, ls.dist);
     a.b.shadow[slot * 4 + rec * 2 + 1] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, __int_as_float(ignore_idx));
   }
+}
+
+// sample_surface (shader.wgsl:2052-2175) with the single-kernel form's arithmetic; the VNDF
+// sampler has one call site for the three microfacet lobes.  False when the path ends.
+template <bool TEX>
+__device__ __forceinline__ bool wf_sample_surface(Ray& ray, v3& throughput, v3 hit_pos, const DMat& mat,
+                                                  const SurfCtx& ctx, MediumStack& stack, float& last_surface_pdf,
+                                                  uint32_t& rng) {
+  const v3 V = -ray.direction;
+  const v3 n_orient = dot(ctx.normal, V) > 0.0f ? ctx.normal : -ctx.normal;
+  bool alive = false;
+  {
+    bool entering = dot(ctx.normal, V) > 0.0f;
+    v3 sn_orient = entering ? ctx.surface_normal : -ctx.surface_normal;
+    float dotSNV = wmax(dot(sn_orient, V), 1e-6f);
+    float roughness_val = clamp(ctx.roughness, 0.01f, 1.0f);
+    float alpha = roughness_val * roughness_val;
+    float cc_roughness = clamp(1.0f - mat.clearcoat_gloss, 0.01f, 1.0f);
+    float cc_alpha = cc_roughness * cc_roughness;
+    float etai = peek_ior(stack);
+    float etat = entering ? mat.ior : peek_outer_ior(stack);
+    float cc_F_est = fresnel_dielectric(dotSNV, 1.0f, mat.clearcoat_ior);
+    float w_cc = entering ? mat.clearcoat * cc_F_est : 0.0f;
+    float F_est_raw = fresnel_dielectric(dotSNV, etai, etat);
+    float F0_d = pow2c((etai - etat) / (etai + etat));
+    float F_est = mix(F_est_raw, F0_d, roughness_val);
+    v3 F_metal = ctx.albedo + (mk3s(1.0f) - ctx.albedo) * pow_(wmax(0.0f, 1.0f - dotSNV), 5.0f);
+    v3 F_actual = vmix3(mk3s(F_est), F_metal, mk3s(ctx.metallic));
+    float f_avg = clamp((F_actual.x + F_actual.y + F_actual.z) / 3.0f, 0.0f, 1.0f);
+    float p_cc = w_cc;
+    float p_spec = (1.0f - p_cc) * f_avg;
+    float p_trans = (1.0f - p_cc) * (1.0f - f_avg) * mat.transmission * (1.0f - ctx.metallic);
+    float p_diff = (1.0f - p_cc) * (1.0f - f_avg) * (1.0f - mat.transmission) * (1.0f - ctx.metallic);
+    float total_p = p_cc + p_spec + p_trans + p_diff;
+    if (rand_pcg(rng) > ctx.alpha) {   // alpha cut-out: the path passes through
+      ray.origin = hit_pos - n_orient * 0.005f;
+      alive = true;
+    } else {
+      float rsel = rand_pcg(rng);
+      float xi0 = rand_pcg(rng);
+      float xi1 = rand_pcg(rng);
+      v3 L = mk3s(0.0f);
+      bool is_transmission = false;
+      bool done = false, ok = true;
+      // lobe choice; the VNDF sampler has one call site for the three microfacet lobes
+      int lobe = -1;
+      v3 Nv = n_orient;
+      float av = alpha;
+      if (rsel < p_cc) {
+        lobe = 0; Nv = sn_orient; av = cc_alpha;
+      } else if (rsel < p_cc + p_spec) {
+        lobe = 1;
+        if (mat.anisotropic > 0.0f) {
+          v3 up = absf(n_orient.y) > 0.99999f ? mk3(0.0f, 0.0f, 1.0f) : mk3(0.0f, 1.0f, 0.0f);
+          v3 T = normalize(cross(up, n_orient));
+          v3 B = cross(n_orient, T);
+          float angle = mat.aniso_rotation * TWO_PI;
+          T = T * cos_(angle) + B * sin_(angle);
+          Nv = normalize(vmix(n_orient, cross(cross(V, T), T), mat.anisotropic));
+        }
+      } else if (rsel < p_cc + p_spec + p_trans) {
+        if (absf(etai - etat) < 1e-4f) {
+          ray.direction = -V;
+          ray.origin = hit_pos - n_orient * 0.001f;
+          throughput = throughput * mk3s(mat.transmission * (1.0f - ctx.metallic));
+          last_surface_pdf = p_trans;
+          if (entering) {
+            Medium m; m.ior = mat.ior;
+            m.sigma = (-vlog(vmax(ctx.albedo, mk3s(0.0001f)))) * mat.concentration;
+            m.emission = mat.emittance;
+            push_medium(stack, m);
+          } else {
+            pop_medium(stack);
+          }
+          done = true;
+        } else {
+          lobe = 2;
+        }
+      } else if (rsel < total_p) {
+        lobe = 3;
+      } else {
+        ok = false;
+      }
+      if (lobe >= 0 && lobe <= 2) {
+        v3 H = ImportanceSampleVNDF_GGX(xi0, xi1, V, Nv, av);
+        if (lobe == 2) {
+          float eta_ratio = etai / etat;
+          L = refract(-V, H, eta_ratio);
+          if (length(L) < 0.1f) L = reflect(-V, H);
+          else is_transmission = true;
+        } else {
+          L = reflect(-V, H);
+        }
+      } else if (lobe == 3) {
+        L = ImportanceSampleCosine(xi0, xi1, n_orient);
+      }
+      if (ok && !done) {
+        float dotNL = dot(n_orient, L);
+        if (is_transmission) {
+          if (dotNL >= 0.0f) ok = false;
+          else ray.origin = hit_pos - n_orient * 0.001f;
+        } else {
+          if (dotNL <= 0.0f) ok = false;
+          else ray.origin = hit_pos + n_orient * 0.001f;
+        }
+        if (ok) {
+          ray.direction = L;
+          v3 bsdf_val; float pdf_val;
+          bsdf_eval_pdf<TEX>(V, L, mat, ctx, stack, &bsdf_val, &pdf_val);
+          if (pdf_val > 0.0f) throughput = throughput * (bsdf_val / pdf_val);
+          else ok = false;
+          if (ok) {
+            last_surface_pdf = pdf_val;
+            if (is_transmission) {
+              if (entering) {
+                Medium m; m.ior = mat.ior;
+                m.sigma = (-vlog(vmax(ctx.albedo, mk3s(0.0001f)))) * mat.concentration;
+                m.emission = mat.emittance;
+                push_medium(stack, m);
+              } else {
+                pop_medium(stack);
+              }
+            }
+          }
+        }
+      }
+      alive = ok;
+    }
+  }
+  return alive;
 }
 
 template <bool COUNT, bool TEX>
@@ -432,7 +563,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
       hit.t = __uint_as_float(h0.x); hit.m_idx = (int32_t)h0.y; hit.o_idx = (int32_t)h0.z; hit.kind = (int32_t)h0.w;
       hit.id = (int32_t)h1.x; hit.aux = (int32_t)h1.y; hit.bu = __uint_as_float(h1.z); hit.bv = __uint_as_float(h1.w);
       hit.tsrc = -1; hit.tsrc_t = 0.0f;
-      if (HAS_TEX<TEX>(s, wgpt::SCENE_NORMAL_MAPS)) {
+      if (HAS_TEX<TEX>(s, wgpt::SCENE_TANGENTS)) {
         uint2 ts = a.b.tsrc[slot];
         hit.tsrc = (int32_t)ts.x; hit.tsrc_t = __uint_as_float(ts.y);
       }
@@ -452,7 +583,8 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
         cn.add(C_HIT_ATTR);
         DMat mat = load_mat(s, hit.m_idx);
         v3 hn = hit_normal(s, ray, hit);
-        SurfCtx ctx = hit_context<TEX>(s, ray, hit, mat, hn);
+        TexPoint tp;
+        SurfCtx ctx = hit_context<TEX>(s, ray, hit, mat, hn, &tp, true);
         float em_len = length(ctx.emittance);
         if (em_len > 0.0f) {
           float weight = 1.0f;
@@ -509,7 +641,8 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
             }
             if (ls.pdf > 0.0f) {
               ls.pdf *= selected_weight / weight_sum;
-              record_nee<COUNT, TEX>(a, slot, 0, ls, hit_pos, n_orient, V, mat, ctx, stack, light.obj_idx, throughput, flags);
+              record_nee<COUNT, TEX>(a, slot, 0, ls, hit_pos, n_orient, V, mat, ctx, tp, stack, light.obj_idx, throughput,
+                                     flags);
             }
           }
           last_weight_sum = weight_sum;
@@ -519,130 +652,28 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
           float u0 = rand_pcg(rng);
           float u1 = rand_pcg(rng);
           LightSample env = sample_env_cdf(s, p, u0, u1, cn);
-          record_nee<COUNT, TEX>(a, slot, 1, env, hit_pos, n_orient, V, mat, ctx, stack, -1, throughput, flags);
+          record_nee<COUNT, TEX>(a, slot, 1, env, hit_pos, n_orient, V, mat, ctx, tp, stack, -1, throughput, flags);
         }
         // shader.wgsl:2052-2175 -- the same arithmetic as the single-kernel form
         int32_t count_before = stack.count;
-        {
-          bool entering = dot(ctx.normal, V) > 0.0f;
-          v3 sn_orient = entering ? ctx.surface_normal : -ctx.surface_normal;
-          float dotSNV = wmax(dot(sn_orient, V), 1e-6f);
-          float roughness_val = clamp(ctx.roughness, 0.01f, 1.0f);
-          float alpha = roughness_val * roughness_val;
-          float cc_roughness = clamp(1.0f - mat.clearcoat_gloss, 0.01f, 1.0f);
-          float cc_alpha = cc_roughness * cc_roughness;
-          float etai = peek_ior(stack);
-          float etat = entering ? mat.ior : peek_outer_ior(stack);
-          float cc_F_est = fresnel_dielectric(dotSNV, 1.0f, mat.clearcoat_ior);
-          float w_cc = entering ? mat.clearcoat * cc_F_est : 0.0f;
-          float F_est_raw = fresnel_dielectric(dotSNV, etai, etat);
-          float F0_d = pow2c((etai - etat) / (etai + etat));
-          float F_est = mix(F_est_raw, F0_d, roughness_val);
-          v3 F_metal = ctx.albedo + (mk3s(1.0f) - ctx.albedo) * pow_(wmax(0.0f, 1.0f - dotSNV), 5.0f);
-          v3 F_actual = vmix3(mk3s(F_est), F_metal, mk3s(ctx.metallic));
-          float f_avg = clamp((F_actual.x + F_actual.y + F_actual.z) / 3.0f, 0.0f, 1.0f);
-          float p_cc = w_cc;
-          float p_spec = (1.0f - p_cc) * f_avg;
-          float p_trans = (1.0f - p_cc) * (1.0f - f_avg) * mat.transmission * (1.0f - ctx.metallic);
-          float p_diff = (1.0f - p_cc) * (1.0f - f_avg) * (1.0f - mat.transmission) * (1.0f - ctx.metallic);
-          float total_p = p_cc + p_spec + p_trans + p_diff;
-          if (rand_pcg(rng) > ctx.alpha) {   // alpha cut-out: the path passes through
-            ray.origin = hit_pos - n_orient * 0.005f;
-            alive = true;
-          } else {
-            float rsel = rand_pcg(rng);
-            float xi0 = rand_pcg(rng);
-            float xi1 = rand_pcg(rng);
-            v3 L = mk3s(0.0f);
-            bool is_transmission = false;
-            bool done = false, ok = true;
-            // lobe choice; the VNDF sampler has one call site for the three microfacet lobes
-            int lobe = -1;
-            v3 Nv = n_orient;
-            float av = alpha;
-            if (rsel < p_cc) {
-              lobe = 0; Nv = sn_orient; av = cc_alpha;
-            } else if (rsel < p_cc + p_spec) {
-              lobe = 1;
-              if (mat.anisotropic > 0.0f) {
-                v3 up = absf(n_orient.y) > 0.99999f ? mk3(0.0f, 0.0f, 1.0f) : mk3(0.0f, 1.0f, 0.0f);
-                v3 T = normalize(cross(up, n_orient));
-                v3 B = cross(n_orient, T);
-                float angle = mat.aniso_rotation * TWO_PI;
-                T = T * cos_(angle) + B * sin_(angle);
-                Nv = normalize(vmix(n_orient, cross(cross(V, T), T), mat.anisotropic));
-              }
-            } else if (rsel < p_cc + p_spec + p_trans) {
-              if (absf(etai - etat) < 1e-4f) {
-                ray.direction = -V;
-                ray.origin = hit_pos - n_orient * 0.001f;
-                throughput = throughput * mk3s(mat.transmission * (1.0f - ctx.metallic));
-                last_surface_pdf = p_trans;
-                if (entering) {
-                  Medium m; m.ior = mat.ior;
-                  m.sigma = (-vlog(vmax(ctx.albedo, mk3s(0.0001f)))) * mat.concentration;
-                  m.emission = mat.emittance;
-                  push_medium(stack, m);
-                } else {
-                  pop_medium(stack);
-                }
-                done = true;
-              } else {
-                lobe = 2;
-              }
-            } else if (rsel < total_p) {
-              lobe = 3;
-            } else {
-              ok = false;
-            }
-            if (lobe >= 0 && lobe <= 2) {
-              v3 H = ImportanceSampleVNDF_GGX(xi0, xi1, V, Nv, av);
-              if (lobe == 2) {
-                float eta_ratio = etai / etat;
-                L = refract(-V, H, eta_ratio);
-                if (length(L) < 0.1f) L = reflect(-V, H);
-                else is_transmission = true;
-              } else {
-                L = reflect(-V, H);
-              }
-            } else if (lobe == 3) {
-              L = ImportanceSampleCosine(xi0, xi1, n_orient);
-            }
-            if (ok && !done) {
-              float dotNL = dot(n_orient, L);
-              if (is_transmission) {
-                if (dotNL >= 0.0f) ok = false;
-                else ray.origin = hit_pos - n_orient * 0.001f;
-              } else {
-                if (dotNL <= 0.0f) ok = false;
-                else ray.origin = hit_pos + n_orient * 0.001f;
-              }
-              if (ok) {
-                ray.direction = L;
-                v3 bsdf_val; float pdf_val;
-                bsdf_eval_pdf<TEX>(V, L, mat, ctx, stack, &bsdf_val, &pdf_val);
-                if (pdf_val > 0.0f) throughput = throughput * (bsdf_val / pdf_val);
-                else ok = false;
-                if (ok) {
-                  last_surface_pdf = pdf_val;
-                  if (is_transmission) {
-                    if (entering) {
-                      Medium m; m.ior = mat.ior;
-                      m.sigma = (-vlog(vmax(ctx.albedo, mk3s(0.0001f)))) * mat.concentration;
-                      m.emission = mat.emittance;
-                      push_medium(stack, m);
-                    } else {
-                      pop_medium(stack);
-                    }
-                  }
-                }
-              }
-            }
-            alive = ok;
-          }
-        }
+        alive = wf_sample_surface<TEX>(ray, throughput, hit_pos, mat, ctx, stack, last_surface_pdf, rng);
         if (!alive) break;
-        if (stack.count > count_before) store_medium(a, slot, (uint32_t)(stack.count - 1), stack.media[stack.count - 1]);
+        const int32_t low = count_before < stack.count ? count_before : stack.count;
+        // shader.wgsl:2458-2472: the height field shadows the sampled direction: shade the
+        // occluding texel and sample again from it
+        v2 pom_uv;
+        if (pom_shadowed<TEX>(s, tp, ray.direction, &pom_uv)) {
+          SurfCtx cp = surface_context(s, mat, hn, tp, pom_uv);
+          radiance = radiance + throughput * clamp_firefly(cp.emittance, bounce);
+          if (length(cp.emittance) > 1.0f) { alive = false; break; }
+          alive = wf_sample_surface<TEX>(ray, throughput, hit_pos, mat, cp, stack, last_surface_pdf, rng);
+          if (!alive) break;
+        }
+        if (TEX) {
+          for (int32_t m = low; m < stack.count; ++m) store_medium(a, slot, (uint32_t)m, stack.media[m]);
+        } else if (stack.count > count_before) {
+          store_medium(a, slot, (uint32_t)(stack.count - 1), stack.media[stack.count - 1]);
+        }
         if (bounce < 2) break;
         float survival_prob = clamp(max_component(throughput), 0.05f, 0.95f);
         if (rand_pcg(rng) > survival_prob) { alive = false; break; }

@@ -22,8 +22,9 @@ bool ctx_images(::wgpt_ctx* ctx, int view, CtxImages* out);   // view -1: the ma
 
 // Scene flag bits derived from the materials on upload (above the WGPT_HAS_* bits): some
 // material samples a texture; some has an albedo texture (shadow rays then attenuate through
-// it); some has a normal map (closest hits then carry their tangent-frame source).
-enum : uint32_t { SCENE_TEXTURED = 1u << 24, SCENE_ALPHA_SHADOWS = 1u << 25, SCENE_NORMAL_MAPS = 1u << 26 };
+// it); some reads the tangent frame, through a normal map or a height field (closest hits then
+// carry their tangent-frame source).
+enum : uint32_t { SCENE_TEXTURED = 1u << 24, SCENE_ALPHA_SHADOWS = 1u << 25, SCENE_TANGENTS = 1u << 26 };
 
 // Device copies of the scene buffers, in the reference's packed layouts.
 struct DeviceScene {

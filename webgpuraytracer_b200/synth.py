@@ -328,8 +328,9 @@ def flagship_scene(seed: int = 1, width: int = 1920, height: int = 1080, bounces
 # ----------------------------------------------------------------------------- textured scenes
 def texture_set(size: int = 64, seed: int = 1) -> dict[str, sc.Texture]:
     """Seeded rgba8 images at one common size: an albedo whose alpha mixes fully transparent,
-    partly covered and opaque cells; a tangent-space normal map of sinusoidal bumps; roughness
-    (green), metallic (blue) and emissive images of value noise."""
+    partly covered and opaque cells; a tangent-space normal map of sinusoidal bumps; a height
+    field (red) of rounded tiles; roughness (green), metallic (blue) and emissive images of
+    value noise."""
     rng = np.random.default_rng(seed)
     y, x = np.mgrid[0:size, 0:size].astype(np.float64) / size
     albedo = np.empty((size, size, 4), np.uint8)
@@ -344,6 +345,11 @@ def texture_set(size: int = 64, seed: int = 1) -> dict[str, sc.Texture]:
     normal[..., :3] = np.clip(np.round((n * 0.5 + 0.5) * 255), 0, 255).astype(np.uint8)
     normal[..., 3] = 255
 
+    tile = np.sin(math.pi * ((x * 4) % 1.0)) * np.sin(math.pi * ((y * 4) % 1.0))
+    height = np.full((size, size, 4), 255, np.uint8)
+    height[..., :3] = 0
+    height[..., 0] = np.clip(np.round(np.sqrt(np.maximum(tile, 0.0)) * 255), 0, 255).astype(np.uint8)
+
     def noise_image(channel):
         img = np.full((size, size, 4), 255, np.uint8)
         img[..., :3] = 0
@@ -353,17 +359,20 @@ def texture_set(size: int = 64, seed: int = 1) -> dict[str, sc.Texture]:
     emissive = np.full((size, size, 4), 255, np.uint8)
     emissive[..., :3] = (rng.random((size, size, 1)) * np.array([255, 200, 120])).astype(np.uint8)
     return {"albedo": sc.Texture(albedo, "albedo"), "normal": sc.Texture(normal, "normal"),
+            "height": sc.Texture(height, "height"),
             "roughness": sc.Texture(noise_image(1), "roughness"), "metallic": sc.Texture(noise_image(2), "metallic"),
             "emissive": sc.Texture(emissive, "emissive")}
 
 
 def textured_scene(seed: int = 1, width: int = 128, height: int = 128, bounces: int = 6, tex_size: int = 64,
-                   sky: bool = True) -> sc.Scene:
+                   sky: bool = True, pom: bool = False) -> sc.Scene:
     """Every primitive kind with textured materials: alpha cut-outs (albedo alpha) on a sphere,
     a cube, a mesh instance, a listed mesh and a plane, so shadow rays cross partly covered
     surfaces; normal maps on a cube, a torus and meshes (triangles and tori keep the tangent frame
     of an earlier closest candidate); roughness and metallic maps on a cylinder; an emissive map;
-    a sphere and a box light sampled explicitly, and an importance-sampled sky."""
+    a sphere and a box light sampled explicitly, and an importance-sampled sky.  With `pom`, the
+    ground, the bumpy material and a cube also carry height fields (parallax occlusion mapping:
+    a depth map and an inverted height map with different layer counts and offsets)."""
     rnd = mulberry32(seed)
     t = texture_set(tex_size, seed)
     s = sc.Scene(width, height)
@@ -377,8 +386,17 @@ def textured_scene(seed: int = 1, width: int = 128, height: int = 128, bounces: 
                          roughnessTex=t["roughness"], uvScale=[3.0, 3.0])
     ground = sc.Material("ground", [0.8, 0.8, 0.8], 0.7, albedoTex=t["albedo"], normalTex=t["normal"],
                          uvScale=[0.25, 0.25])
+    if pom:
+        ground.heightTex = t["height"]
+        ground.heightMultiplier, ground.heightSamp, ground.heightOffset = 0.08, 24, 0.5
+        bumpy.heightTex = t["height"]
+        bumpy.heightMultiplier, bumpy.heightSamp = -0.05, 12
     s.add(sc.Sphere("cut_sphere", cut, _uniform(rnd, -2.5, -1.5), 0.5, 0.0, 1.0))
     s.add(sc.Cube("cut_cube", all_in, 0.5, -1.0, -1.5, 1.7, 0.2, -0.3))
+    if pom:
+        s.add(sc.Cube("relief_cube", sc.Material("relief", [0.5, 0.8, 0.5], 0.4, heightTex=t["height"],
+                                                 heightMultiplier=0.1, heightSamp=40, uvScale=[2.0, 2.0]),
+                      2.4, -2.0, -1.8, 3.4, -1.0, -0.8))
     s.add(sc.Cube("bump_cube", bumpy, -0.6, -1.9, 1.0, 0.4, -0.9, 2.0))
     tor = s.add(sc.Torus("bump_torus", bumpy, 1.0, 0.35))
     tor.set_position(2.2, 0.6, 1.0)

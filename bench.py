@@ -514,6 +514,32 @@ def run_ours(args):
     return 0
 
 
+def scene_update_ms(r, rd, sc, scene, reps: int = 20) -> dict:
+    """Host milliseconds per ABI call after one animation step of the scene (every primitive and
+    instance moved, then re-packed by the caller): wgpt_update_objects (the updateObjects fast
+    path: five small buffers and the TLAS node pairs), wgpt_update_scene (every buffer rewritten
+    and validated) and wgpt_upload_scene (setScene).  Leaves the moved scene uploaded."""
+    import ctypes as C
+    for o in scene.objects:
+        if o.type in ("Sphere", "Cube", "Cylinder", "Torus", "Model"):
+            p = o.position
+            o.set_position(float(p[0]) + 0.01, float(p[1]), float(p[2]))
+    packed = sc.pack_scene_data(scene)      # keeps the buffers the descriptor points at alive
+    desc = rd.scene_desc(packed)
+    out = {}
+    for name in ("wgpt_update_objects", "wgpt_update_scene", "wgpt_upload_scene"):
+        fn = getattr(r.L, name)
+        r._check(fn(r.ctx, C.byref(desc)), name)
+        r.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r._check(fn(r.ctx, C.byref(desc)), name)
+        r.synchronize()
+        out[name] = (time.perf_counter() - t0) / reps * 1e3
+    out["note"] = "host wall time per call, the scene's packing excluded"
+    return out
+
+
 def run_batch(args):
     """--workload batch: 32 seeded views (sizes over 256^2..1920x1080, 4/16/64 spp, 8 bounces)
     of the 5.24 M-triangle scene.  The views are shared out over the ranks longest-first (LPT by
@@ -625,6 +651,7 @@ def run_batch(args):
             r._check(r.L.wgpt_read_view(r.ctx, k_, None, rd.ptr(o)), "read_view")
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     rep = stage_report(r, rd, lambda: launch(args.warmup), stream, flush, paths_mine, False)
+    upd = scene_update_ms(r, rd, sc, scene)
     peaks, peak_kind = load_peaks()
     cnt = rep["cnt"]
     rays_all = replicas.sum_over_ranks(float(cnt[1] + cnt[2]), world)
@@ -647,6 +674,7 @@ def run_batch(args):
                                  "max": float(np.max(fin_all)),
                                  "note": "render call end + learned-denoiser passes in completion order"},
             "rays_per_s": rays_all * args.steps / dev_s_max,
+            "scene_update_ms": upd,
             "e2e": {"value": paths_all * e2e_steps / e2e_s, "unit": "paths/s",
                     "h2d_bytes_per_step": 112 * len(all_views),
                     "d2h_bytes_per_step": sum(v["width"] * v["height"] * 4 for v in all_views),

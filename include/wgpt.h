@@ -29,7 +29,7 @@ enum wgpt_status {
   WGPT_E_NOMEM = 4,       /* device allocation failed */
   WGPT_E_STATE = 5,       /* call out of order (no scene, no size, no G-buffer) */
   WGPT_E_UNSUPPORTED = 6, /* a combination this build does not run (e.g. FP64 accumulation in the single-kernel mode) */
-  WGPT_E_REBUILD = 7,     /* wgpt_update_scene: the new data does not fit, upload again */
+  WGPT_E_REBUILD = 7,     /* wgpt_update_scene / wgpt_update_objects: upload the scene again */
   WGPT_E_DEVICE = 8,      /* a kernel reported an error (traversal stack overflow) */
   WGPT_E_TOO_LARGE = 9    /* wgpt_denoise_noalloc: more than WGPT_NOALLOC_MAX_PIXELS pixels */
 };
@@ -81,9 +81,19 @@ int wgpt_upload_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc);
    would return; msg (nullable) receives the reason. */
 int wgpt_validate_scene(const wgpt_scene_desc* desc, char* msg, size_t msg_len);
 
-/* updateObjects fast path (tracer.js:2132-2164): rewrites objects, tlas, planes, meshes and
-   materials in place when they fit and the flags are unchanged, else WGPT_E_REBUILD. */
+/* Rewrites every buffer of the scene in place (validated like wgpt_upload_scene) when each
+   fits its resident buffer and the pipeline constants are unchanged, else WGPT_E_REBUILD.  No
+   reference counterpart: a full setScene without reallocation. */
 int wgpt_update_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc);
+
+/* updateObjects fast path (tracer.js:2132-2164): reads only desc->objects, tlas, planes, meshes
+   and materials (tracer.js:2151-2155), writes each at offset 0 of its resident buffer (the
+   buffer keeps the length wgpt_upload_scene gave it, as a WebGPU writeBuffer does), rebuilds
+   the TLAS node pairs, and leaves lights, BLAS, triangles, sky, CDF and textures as they are.
+   WGPT_E_REBUILD when the flags differ, a buffer does not fit, or a mesh instance names a BLAS
+   that was not uploaded (the caller then uploads the scene again, as setScene does);
+   WGPT_E_LAYOUT for an out-of-range index in the new records. */
+int wgpt_update_objects(wgpt_ctx* ctx, const wgpt_scene_desc* desc);
 
 /* resize (tracer.js:2166-2205): accumulation (16 B/px), rgba8 output and, with want_gbuf, the
    48 B/px G-buffer; all zero-filled. */
@@ -198,6 +208,14 @@ int wgpt_kpcn_add_example(wgpt_kpcn* k, const float* noisy_rgba32f, const void* 
 int wgpt_kpcn_num_examples(wgpt_kpcn* k, uint32_t* n);
 int wgpt_kpcn_train(wgpt_kpcn* k, uint32_t steps, uint32_t batch, uint32_t crop, float lr, uint64_t seed,
                     float* losses);
+/* Data-parallel training in two halves around the caller's gradient all-reduce (no reference
+   counterpart).  wgpt_kpcn_grads: forward and backward of `batch` crops drawn with `seed` from
+   this denoiser's examples; writes the FP32 gradient (num_params floats) into dev_grads, DEVICE
+   memory on the denoiser's device, and the batch loss to *loss (nullable); returns once both
+   are written.  wgpt_kpcn_apply: one Adam step with the gradient dev_grads * scale (e.g. the
+   sum over ranks with scale 1/ranks). */
+int wgpt_kpcn_grads(wgpt_kpcn* k, uint32_t batch, uint32_t crop, uint64_t seed, float* loss, float* dev_grads);
+int wgpt_kpcn_apply(wgpt_kpcn* k, const float* dev_grads, float scale, float lr);
 int wgpt_kpcn_loss_and_grads(wgpt_kpcn* k, const float* noisy_rgba32f, const void* gbuf_48B,
                              const float* target_rgba32f, uint32_t w, uint32_t h, float* loss, float* grads,
                              float* out_rgba32f);

@@ -134,3 +134,64 @@ def test_kpcn_training_gains_over_atrous():
     assert e_kpcn < e_atrous
     r.close()
     k.close()
+
+
+# ------------------------------------------------------------------------ data-parallel training
+def test_kpcn_grads_match_whole_image_gradient():
+    """wgpt_kpcn_grads over one crop covering the only example equals the whole-image gradient
+    (up to the order of the floating-point atomics that sum the weight gradients)."""
+    import torch
+    noisy, gbuf, target = _random_image(64, 64, 11)
+    k = kpcn.Kpcn(0, seed=5)
+    k.add_example(noisy, gbuf, target)
+    loss_ref, g_ref, _ = k.loss_and_grads(noisy, gbuf, target)
+    g = torch.empty(k.n_params, dtype=torch.float32, device="cuda:0")
+    loss = k.grads(1, 64, 123, g)
+    assert abs(loss - loss_ref) <= 1e-5 * abs(loss_ref)
+    gd = g.cpu().numpy().astype(np.float64)
+    # split-K weight gradients are summed with float atomics over BF16 activations: the
+    # run-to-run spread is ~1e-3 of the norm
+    assert np.linalg.norm(gd - g_ref) <= 5e-3 * np.linalg.norm(g_ref)
+    with pytest.raises(_lib.WgptError):
+        k.grads(1, 64, 1, torch.empty(k.n_params, dtype=torch.float32))     # host memory is refused
+    k.close()
+
+
+def _learnable_image(h, w, seed):
+    """A random noisy image, G-buffer, and as target a fixed function of the noisy image."""
+    noisy, gbuf, _ = _random_image(h, w, seed)
+    return noisy, gbuf, (noisy * 0.5).astype(np.float32)
+
+
+def test_kpcn_emulated_two_rank_steps_keep_weights_identical():
+    """Two denoisers with different examples, one gradient sum per step (what all_reduce
+    gives every rank), the mean applied on both: the weights stay bit-identical, the loss falls."""
+    import torch
+    ks = [kpcn.Kpcn(0, seed=2) for _ in range(2)]
+    for r, k in enumerate(ks):
+        for e in range(3):
+            k.add_example(*_learnable_image(64, 64, 100 * r + e))
+    gs = [torch.empty(ks[0].n_params, dtype=torch.float32, device="cuda:0") for _ in ks]
+    first = last = None
+    for step in range(12):
+        # each rank keeps its batch (seed r), so the summed loss is of the same data every step
+        losses = [k.grads(2, 32, r, g) for r, (k, g) in enumerate(zip(ks, gs))]
+        total = gs[0] + gs[1]
+        torch.cuda.synchronize()
+        for k in ks:
+            k.apply(total, 0.5, 2e-3)
+        first = first if first is not None else sum(losses)
+        last = sum(losses)
+    assert np.array_equal(ks[0].get_params(), ks[1].get_params())
+    assert last < first
+    for k in ks:
+        k.close()
+
+
+def test_kpcn_train_data_parallel_single_rank():
+    k = kpcn.Kpcn(0, seed=4)
+    for e in range(2):
+        k.add_example(*_learnable_image(64, 64, 300 + e))
+    losses = kpcn.train_data_parallel(k, 30, batch=4, crop=64, lr=2e-3, seed=1)
+    assert np.isfinite(losses).all() and losses[-5:].mean() < losses[:5].mean()
+    k.close()

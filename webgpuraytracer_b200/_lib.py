@@ -69,6 +69,7 @@ EXPORTS = {
     "wgpt_validate_scene": ([C.POINTER(SceneDesc), C.c_char_p, C.c_size_t], C.c_int),
     "wgpt_upload_scene": ([_P, C.POINTER(SceneDesc)], C.c_int),
     "wgpt_update_scene": ([_P, C.POINTER(SceneDesc)], C.c_int),
+    "wgpt_update_objects": ([_P, C.POINTER(SceneDesc)], C.c_int),
     "wgpt_resize": ([_P, _U32, _U32, C.c_int], C.c_int),
     "wgpt_set_params": ([_P, _P], C.c_int),
     "wgpt_render": ([_P, _U32, _U32, _U32, _U32, _U32, _U32], C.c_int),
@@ -100,6 +101,8 @@ EXPORTS = {
     "wgpt_kpcn_num_examples": ([_P, C.POINTER(C.c_uint32)], C.c_int),
     "wgpt_kpcn_train": ([_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64, _P], C.c_int),
     "wgpt_kpcn_loss_and_grads": ([_P, _P, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P], C.c_int),
+    "wgpt_kpcn_grads": ([_P, C.c_uint32, C.c_uint32, C.c_uint64, _P, _P], C.c_int),
+    "wgpt_kpcn_apply": ([_P, _P, C.c_float, C.c_float], C.c_int),
     "wgpt_kpcn_denoise": ([_P, _P, C.c_float, _P], C.c_int),
     "wgpt_render_views": ([_P, _P, _P, _P, _P], C.c_int),
     "wgpt_read_view": ([_P, C.c_uint32, _P, _P], C.c_int),

@@ -56,6 +56,11 @@ struct wgpt_ctx {
   struct View { uint32_t w, h; float* accum; uint8_t* out; float* gbuf; };
   std::vector<View> views;
   double* acc64 = nullptr;        // optional FP64 Welford accumulation (8 doubles per pixel)
+  // kept from the last full upload for the objects fast path: the (node, triangle) offset
+  // pairs whose BLAS passed validation, and a host copy of the material buffer
+  std::set<std::pair<uint32_t, uint32_t>> blas_checked;
+  std::vector<wgpt_material> host_mats;
+  std::vector<int32_t> light_objs;   // obj_idx of each resident light record
 };
 
 namespace {
@@ -298,7 +303,8 @@ int upload_buffers(wgpt_ctx* ctx, const wgpt_scene_desc* d, bool in_place_only) 
   return WGPT_OK;
 }
 
-int check_desc(wgpt_ctx* ctx, const wgpt_scene_desc* d, HostScene& hs) {
+int check_desc(wgpt_ctx* ctx, const wgpt_scene_desc* d, HostScene& hs,
+               std::set<std::pair<uint32_t, uint32_t>>* checked_out = nullptr) {
   if (!d) return fail(ctx, WGPT_E_INVALID, "scene descriptor is null");
   const wgpt_buffer* b[9] = {&d->materials, &d->objects, &d->tlas, &d->meshes, &d->bvh,
                              &d->triangles, &d->planes, &d->lights, &d->sky_cdf};
@@ -331,7 +337,23 @@ int check_desc(wgpt_ctx* ctx, const wgpt_scene_desc* d, HostScene& hs) {
     if (e[0] == 'U') return fail(ctx, WGPT_E_UNSUPPORTED, e.substr(1));
     return fail(ctx, WGPT_E_LAYOUT, e);
   }
+  if (checked_out) checked_out->swap(checked);
   return WGPT_OK;
+}
+
+// The wgpt::SCENE_* bits implied by a material buffer under the given feature flags.
+uint32_t derived_flags(const wgpt_material* m, size_t n, uint32_t feature_flags) {
+  uint32_t f = 0;
+  const bool pom = (feature_flags & WGPT_HAS_HEIGHTMAPS) != 0u;
+  for (size_t i = 0; i < n; ++i) {
+    const bool height = pom && m[i].height_idx >= 0;
+    if (m[i].emissive_idx >= 0 || m[i].albedo_idx >= 0 || m[i].normal_idx >= 0 || m[i].roughness_idx >= 0 ||
+        m[i].metallic_idx >= 0 || height)
+      f |= wgpt::SCENE_TEXTURED;
+    if (m[i].albedo_idx >= 0) f |= wgpt::SCENE_ALPHA_SHADOWS;
+    if (m[i].normal_idx >= 0 || height) f |= wgpt::SCENE_TANGENTS;
+  }
+  return f;
 }
 
 void fill_device_scene(wgpt_ctx* ctx, const wgpt_scene_desc* d) {
@@ -354,17 +376,13 @@ void fill_device_scene(wgpt_ctx* ctx, const wgpt_scene_desc* d) {
   s.tex_h = d->textures_rgba8 ? d->tex_height : 1u;
   s.tex_layers = d->textures_rgba8 ? d->tex_layers : 0u;
   s.bounce_limit = d->bounce_limit;
-  s.flags = d->feature_flags;
   const wgpt_material* m = (const wgpt_material*)d->materials.ptr;
-  const bool pom = (d->feature_flags & WGPT_HAS_HEIGHTMAPS) != 0u;
-  for (uint32_t i = 0; i < (uint32_t)(d->materials.bytes / WGPT_STRIDE_MATERIAL); ++i) {
-    const bool height = pom && m[i].height_idx >= 0;
-    if (m[i].emissive_idx >= 0 || m[i].albedo_idx >= 0 || m[i].normal_idx >= 0 || m[i].roughness_idx >= 0 ||
-        m[i].metallic_idx >= 0 || height)
-      s.flags |= wgpt::SCENE_TEXTURED;
-    if (m[i].albedo_idx >= 0) s.flags |= wgpt::SCENE_ALPHA_SHADOWS;
-    if (m[i].normal_idx >= 0 || height) s.flags |= wgpt::SCENE_TANGENTS;
-  }
+  const size_t nm = d->materials.bytes / WGPT_STRIDE_MATERIAL;
+  ctx->host_mats.assign(m, m + nm);
+  s.flags = d->feature_flags | derived_flags(m, nm, d->feature_flags);
+  const wgpt_light* lt = (const wgpt_light*)d->lights.ptr;
+  ctx->light_objs.clear();
+  for (size_t i = 0; i < d->lights.bytes / WGPT_STRIDE_LIGHT; ++i) ctx->light_objs.push_back(lt[i].obj_idx);
 }
 
 int check_section(wgpt_ctx* ctx, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh) {
@@ -481,7 +499,8 @@ int wgpt_upload_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   if (!ctx) return WGPT_E_INVALID;
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
   HostScene hs;
-  int rc = check_desc(ctx, desc, hs);
+  std::set<std::pair<uint32_t, uint32_t>> checked;
+  int rc = check_desc(ctx, desc, hs, &checked);
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->stream), "drain before upload");
   rc = upload_buffers(ctx, desc, false);
@@ -489,6 +508,7 @@ int wgpt_upload_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   rc = upload_pairs(ctx, hs, desc->feature_flags);
   if (rc) return rc;
   fill_device_scene(ctx, desc);
+  ctx->blas_checked.swap(checked);
   ctx->has_scene = true;
   return WGPT_OK;
 }
@@ -500,7 +520,8 @@ int wgpt_update_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   if (desc && (desc->feature_flags != (ctx->ds.flags & 0x7ffu) || desc->bounce_limit != ctx->ds.bounce_limit))
     return fail(ctx, WGPT_E_REBUILD, "pipeline constants changed: full upload required");
   HostScene hs;
-  int rc = check_desc(ctx, desc, hs);
+  std::set<std::pair<uint32_t, uint32_t>> checked;
+  int rc = check_desc(ctx, desc, hs, &checked);
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->stream), "drain before update");
   rc = upload_buffers(ctx, desc, true);
@@ -508,6 +529,121 @@ int wgpt_update_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   rc = upload_pairs(ctx, hs, desc->feature_flags);
   if (rc) return rc;
   fill_device_scene(ctx, desc);
+  ctx->blas_checked.swap(checked);
+  return WGPT_OK;
+}
+
+// updateObjects fast path (tracer.js:2132-2164).  Only the five buffers the reference rewrites
+// are read from the descriptor; each is written at offset 0 of the resident buffer, whose length
+// (and so every arrayLength-bounded loop) stays what the upload set, like queue.writeBuffer into
+// the existing GPU buffer.  The new records are validated against the resident scene: indices
+// within the resident buffers, the TLAS self-contained, mesh instances only of BLAS offsets
+// validated on upload.  Lights, BLAS, triangles, the sky and textures are not touched.
+int wgpt_update_objects(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (!desc) return fail(ctx, WGPT_E_INVALID, "scene descriptor is null");
+  if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  const uint32_t flags = desc->feature_flags;
+  if (flags != (ctx->ds.flags & 0x7ffu)) return fail(ctx, WGPT_E_REBUILD, "pipeline constants changed: full upload required");
+  const int ks[5] = {1, 2, 6, 3, 0};   // objects, tlas, planes, meshes, materials (tracer.js:2151-2155)
+  const wgpt_buffer* b[5] = {&desc->objects, &desc->tlas, &desc->planes, &desc->meshes, &desc->materials};
+  for (int j = 0; j < 5; ++j) {
+    const int k = ks[j];
+    if (b[j]->bytes && !b[j]->ptr) return fail(ctx, WGPT_E_INVALID, std::string(kName[k]) + ": null pointer with nonzero size");
+    if (k != 3 && b[j]->bytes % kStride[k] != 0)
+      return fail(ctx, WGPT_E_LAYOUT, std::string(kName[k]) + ": size is not a multiple of its record size");
+    if (b[j]->bytes > ctx->bytes[k])
+      return fail(ctx, WGPT_E_REBUILD, std::string(kName[k]) + ": does not fit the uploaded buffer");
+  }
+  const uint32_t n_mats = (uint32_t)(ctx->bytes[0] / WGPT_STRIDE_MATERIAL);
+  const uint32_t n_objs = (uint32_t)(ctx->bytes[1] / WGPT_STRIDE_OBJECT);
+  const uint32_t n_lights = (uint32_t)(ctx->bytes[7] / WGPT_STRIDE_LIGHT);
+  const wgpt_material* mats = (const wgpt_material*)desc->materials.ptr;
+  const wgpt_object* objs = (const wgpt_object*)desc->objects.ptr;
+  const wgpt_bvh_node* tlas = (const wgpt_bvh_node*)desc->tlas.ptr;
+  const wgpt_plane* planes = (const wgpt_plane*)desc->planes.ptr;
+  const uint32_t nm = (uint32_t)(desc->materials.bytes / WGPT_STRIDE_MATERIAL);
+  const uint32_t no = (uint32_t)(desc->objects.bytes / WGPT_STRIDE_OBJECT);
+  const uint32_t nt = (uint32_t)(desc->tlas.bytes / WGPT_STRIDE_NODE);
+  const uint32_t np = (uint32_t)(desc->planes.bytes / WGPT_STRIDE_PLANE);
+  const uint32_t nl = (uint32_t)(desc->meshes.bytes / WGPT_STRIDE_MESH_READ);
+  char buf[256];
+  for (uint32_t i = 0; i < nm; ++i) {
+    const int32_t idx[6] = {mats[i].emissive_idx, mats[i].albedo_idx, mats[i].normal_idx, mats[i].height_idx,
+                            mats[i].roughness_idx, mats[i].metallic_idx};
+    for (int32_t t : idx)
+      if (t >= 0 && (uint32_t)t >= ctx->ds.tex_layers) {
+        snprintf(buf, sizeof buf, "materials[%u]: texture index %d beyond the %u layers of the texture array", i, t,
+                 ctx->ds.tex_layers);
+        return fail(ctx, WGPT_E_LAYOUT, buf);
+      }
+  }
+  auto mat_ok = [&](int32_t m) { return m >= -1 && m < (int32_t)n_mats; };
+  const uint32_t tlas_flags = WGPT_HAS_SPHERES | WGPT_HAS_CUBES | WGPT_HAS_CYLINDERS | WGPT_HAS_TORI | WGPT_HAS_MESHES;
+  if ((flags & tlas_flags) && nt > 0) {
+    std::string e = check_tree(tlas, nt, 0, 0, 0, n_objs, "tlas");
+    if (!e.empty()) return fail(ctx, WGPT_E_LAYOUT, e);
+  }
+  for (uint32_t i = 0; i < no; ++i) {
+    const wgpt_object& o = objs[i];
+    if (!mat_ok(o.material_idx)) { snprintf(buf, sizeof buf, "objects[%u]: material %d out of range", i, o.material_idx); return fail(ctx, WGPT_E_LAYOUT, buf); }
+    if ((flags & WGPT_HAS_LIGHTS) && o.light_idx >= (int32_t)n_lights) {
+      snprintf(buf, sizeof buf, "objects[%u]: light %d out of range", i, o.light_idx);
+      return fail(ctx, WGPT_E_LAYOUT, buf);
+    }
+    if (o.object_type == 0 && (flags & WGPT_HAS_MESHES)) {
+      uint32_t nof, tof;
+      memcpy(&nof, &o.param0, 4); memcpy(&tof, &o.param1, 4);
+      if (!ctx->blas_checked.count({nof, tof})) {
+        snprintf(buf, sizeof buf, "objects[%u]: mesh instance of a BLAS that is not resident", i);
+        return fail(ctx, WGPT_E_REBUILD, buf);
+      }
+      if (o.material_idx < 0) { snprintf(buf, sizeof buf, "objects[%u]: mesh without material", i); return fail(ctx, WGPT_E_LAYOUT, buf); }
+    }
+  }
+  if (flags & WGPT_HAS_LIST_MESHES) {
+    for (uint32_t i = 0; i < nl; ++i) {
+      wgpt_mesh_instance mi;
+      memcpy(&mi, (const uint8_t*)desc->meshes.ptr + (size_t)i * WGPT_STRIDE_MESH_READ, sizeof mi);
+      if (!mat_ok(mi.material_idx)) {
+        snprintf(buf, sizeof buf, "meshes[%u] (80-byte read stride): material %d out of range", i, mi.material_idx);
+        return fail(ctx, WGPT_E_LAYOUT, buf);
+      }
+      if (!ctx->blas_checked.count({mi.node_offset, mi.tri_offset})) {
+        snprintf(buf, sizeof buf, "meshes[%u] (80-byte read stride): BLAS not resident", i);
+        return fail(ctx, WGPT_E_REBUILD, buf);
+      }
+    }
+  }
+  for (uint32_t i = 0; i < np; ++i)
+    if (!mat_ok(planes[i].material_idx)) { snprintf(buf, sizeof buf, "planes[%u]: material out of range", i); return fail(ctx, WGPT_E_LAYOUT, buf); }
+  // the resident light records keep their object indices: those objects need a material
+  for (size_t i = 0; i < ctx->light_objs.size(); ++i) {
+    const int32_t oi = ctx->light_objs[i];
+    if (oi >= 0 && (uint32_t)oi < no && objs[oi].material_idx < 0) {
+      snprintf(buf, sizeof buf, "lights[%zu]: object %d without material", i, oi);
+      return fail(ctx, WGPT_E_LAYOUT, buf);
+    }
+  }
+  // the writes (renders already queued read the old data first)
+  CK(cudaStreamSynchronize(ctx->stream), "drain before update");
+  for (int j = 0; j < 5; ++j)
+    if (b[j]->bytes) CK(cudaMemcpyAsync(ctx->d_buf[ks[j]], b[j]->ptr, b[j]->bytes, cudaMemcpyHostToDevice, ctx->stream), "update buffer");
+  if (nt > 0 && (flags & tlas_flags)) {
+    std::vector<float> pt((size_t)nt * 16, 0.0f);
+    std::vector<uint8_t> done(nt, 0);
+    fill_pairs(tlas, 0, 0, pt.data(), done);
+    CK(cudaMemcpyAsync(ctx->d_pairs_tlas, pt.data(), pt.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
+       "update node pairs");
+    CK(cudaStreamSynchronize(ctx->stream), "update");
+  } else {
+    CK(cudaStreamSynchronize(ctx->stream), "update");
+  }
+  if (nm) {
+    std::copy(mats, mats + nm, ctx->host_mats.begin());
+    ctx->ds.flags = flags | derived_flags(ctx->host_mats.data(), ctx->host_mats.size(), flags);
+  }
   return WGPT_OK;
 }
 

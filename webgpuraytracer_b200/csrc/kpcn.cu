@@ -651,11 +651,11 @@ __global__ void k_bias_grad(const uint16_t* __restrict__ dz, int P, int C, float
     if (acc[c] != 0.0f) atomicAdd(&db[c], acc[c]);
 }
 
-// Adam (bias-corrected) over the flat FP32 parameters.
+// Adam (bias-corrected) over the flat FP32 parameters, with the gradient g * scale.
 __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
-                       size_t n, float lr, float b1, float b2, float eps, float c1, float c2) {
+                       size_t n, float lr, float b1, float b2, float eps, float c1, float c2, float scale) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    float gi = g[i];
+    float gi = g[i] * scale;
     float mi = b1 * m[i] + (1.0f - b1) * gi;
     float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
     m[i] = mi;
@@ -1069,12 +1069,33 @@ int ensure_crops(wgpt_kpcn* k, size_t n) {
   return WGPT_OK;
 }
 
-cudaError_t adam_step(kp::Net& n, float lr) {
+cudaError_t adam_step(kp::Net& n, float lr, const float* g = nullptr, float scale = 1.0f) {
   n.adam_t += 1;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.0f - (float)std::pow(0.9, n.adam_t), c2 = 1.0f - (float)std::pow(0.999, n.adam_t);
-  kp::k_adam<<<kp::grid1(n.n_params), 256, 0, n.st>>>(n.w, n.g, n.m, n.v, n.n_params, lr, b1, b2, 1e-8f, c1, c2);
+  kp::k_adam<<<kp::grid1(n.n_params), 256, 0, n.st>>>(n.w, g ? g : n.g, n.m, n.v, n.n_params, lr, b1, b2, 1e-8f, c1,
+                                                      c2, scale);
   return kp::refresh_bf16(n);
+}
+
+// Draws `count` crops of crop x crop pixels from the examples with the splitmix stream of `seed`
+// and uploads them to k->d_crops.
+int draw_crops(wgpt_kpcn* k, size_t count, uint32_t crop, uint64_t seed) {
+  kp::Net& n = k->net;
+  int rc = ensure_crops(k, count);
+  if (rc) return rc;
+  std::vector<kp::Crop> crops(count);
+  uint64_t s = seed * 0x9E3779B97F4A7C15ull + 7u;
+  for (auto& c : crops) {
+    c.e = (int)(splitmix(s) % (uint64_t)n.ds_n);
+    c.oy = (int)(splitmix(s) % (uint64_t)(n.ds_h - (int)crop + 1));
+    c.ox = (int)(splitmix(s) % (uint64_t)(n.ds_w - (int)crop + 1));
+    c.pad = 0;
+  }
+  KCK(cudaMemcpyAsync(k->d_crops, crops.data(), crops.size() * sizeof(kp::Crop), cudaMemcpyHostToDevice, n.st),
+      "upload crops");
+  KCK(cudaStreamSynchronize(n.st), "crops");
+  return WGPT_OK;
 }
 
 }  // namespace
@@ -1221,24 +1242,14 @@ int wgpt_kpcn_train(wgpt_kpcn* k, uint32_t steps, uint32_t batch, uint32_t crop,
   if (steps == 0) return WGPT_OK;
   cudaSetDevice(n.device);
   KCK(kp::ensure_batch(n, (int)batch, (int)crop, (int)crop), "batch buffers");
-  int rc = ensure_crops(k, (size_t)steps * batch);
-  if (rc) return rc;
   if (k->losses_cap < (int)steps) {
     cudaFree(k->d_losses);
     k->d_losses = nullptr;
     KCK(cudaMalloc(&k->d_losses, steps * 4), "cudaMalloc losses");
     k->losses_cap = (int)steps;
   }
-  std::vector<kp::Crop> crops((size_t)steps * batch);
-  uint64_t s = seed * 0x9E3779B97F4A7C15ull + 7u;
-  for (auto& c : crops) {
-    c.e = (int)(splitmix(s) % (uint64_t)n.ds_n);
-    c.oy = (int)(splitmix(s) % (uint64_t)(n.ds_h - (int)crop + 1));
-    c.ox = (int)(splitmix(s) % (uint64_t)(n.ds_w - (int)crop + 1));
-    c.pad = 0;
-  }
-  KCK(cudaMemcpyAsync(k->d_crops, crops.data(), crops.size() * sizeof(kp::Crop), cudaMemcpyHostToDevice, n.st),
-      "upload crops");
+  int rc = draw_crops(k, (size_t)steps * batch, crop, seed);
+  if (rc) return rc;
   const size_t P = (size_t)batch * crop * crop;
   for (uint32_t it = 0; it < steps; ++it) {
     kp::k_gather<<<kp::grid1(P), 256, 0, n.st>>>(n.ds_col, n.ds_gbuf, n.ds_tgt, n.ds_h, n.ds_w,
@@ -1250,6 +1261,48 @@ int wgpt_kpcn_train(wgpt_kpcn* k, uint32_t steps, uint32_t batch, uint32_t crop,
     KCK(adam_step(n, lr), "adam");
   }
   if (losses) KCK(cudaMemcpyAsync(losses, k->d_losses, steps * 4, cudaMemcpyDeviceToHost, n.st), "losses readback");
+  return check_device_error(k);
+}
+
+int wgpt_kpcn_grads(wgpt_kpcn* k, uint32_t batch, uint32_t crop, uint64_t seed, float* loss, float* dev_grads) {
+  if (!k || !dev_grads || batch == 0 || batch > 64 || crop < 16 || crop > 512 || (crop % 16) != 0)
+    return WGPT_E_INVALID;
+  kp::Net& n = k->net;
+  if (n.ds_n == 0) return kfail(k, WGPT_E_STATE, "no training examples");
+  if ((int)crop > n.ds_w || (int)crop > n.ds_h) return kfail(k, WGPT_E_INVALID, "crop larger than the examples");
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, dev_grads) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+      at.device != n.device) {
+    cudaGetLastError();
+    return kfail(k, WGPT_E_INVALID, "dev_grads must be device memory on the denoiser's device");
+  }
+  cudaSetDevice(n.device);
+  KCK(kp::ensure_batch(n, (int)batch, (int)crop, (int)crop), "batch buffers");
+  int rc = draw_crops(k, batch, crop, seed);
+  if (rc) return rc;
+  const size_t P = (size_t)batch * crop * crop;
+  kp::k_gather<<<kp::grid1(P), 256, 0, n.st>>>(n.ds_col, n.ds_gbuf, n.ds_tgt, n.ds_h, n.ds_w, k->d_crops, (int)batch,
+                                               (int)crop, (int)crop, n.x0, n.col, n.tgt);
+  KCK(kp::forward(n), "forward");
+  KCK(kp::backward(n), "backward");
+  KCK(cudaMemcpyAsync(dev_grads, n.g, n.n_params * 4, cudaMemcpyDeviceToDevice, n.st), "gradient copy");
+  if (loss) KCK(cudaMemcpyAsync(loss, n.loss, 4, cudaMemcpyDeviceToHost, n.st), "loss readback");
+  KCK(cudaStreamSynchronize(n.st), "synchronize");
+  return check_device_error(k);
+}
+
+int wgpt_kpcn_apply(wgpt_kpcn* k, const float* dev_grads, float scale, float lr) {
+  if (!k || !dev_grads || !(lr > 0.0f) || !(scale == scale)) return WGPT_E_INVALID;
+  kp::Net& n = k->net;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, dev_grads) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+      at.device != n.device) {
+    cudaGetLastError();
+    return kfail(k, WGPT_E_INVALID, "dev_grads must be device memory on the denoiser's device");
+  }
+  cudaSetDevice(n.device);
+  KCK(adam_step(n, lr, dev_grads, scale), "adam");
+  KCK(cudaStreamSynchronize(n.st), "synchronize");
   return check_device_error(k);
 }
 

@@ -120,6 +120,19 @@ class Kpcn:
         self._check(self.L.wgpt_kpcn_train(self.h, steps, batch, crop, lr, seed, ptr(losses)), "train")
         return losses
 
+    def grads(self, batch: int, crop: int, seed: int, dev_grads) -> float:
+        """Forward and backward of `batch` crops drawn with `seed`; the FP32 gradient goes into
+        dev_grads (a CUDA tensor of num_params floats on this denoiser's device).  Returns the
+        batch loss."""
+        loss = np.zeros(1, np.float32)
+        self._check(self.L.wgpt_kpcn_grads(self.h, batch, crop, seed, ptr(loss), C.c_void_p(dev_grads.data_ptr())),
+                    "grads")
+        return float(loss[0])
+
+    def apply(self, dev_grads, scale: float, lr: float):
+        """One Adam step with the gradient dev_grads * scale."""
+        self._check(self.L.wgpt_kpcn_apply(self.h, C.c_void_p(dev_grads.data_ptr()), scale, lr), "apply")
+
     def loss_and_grads(self, noisy, gbuf, target):
         h, w = noisy.shape[:2]
         noisy = np.ascontiguousarray(noisy, np.float32)
@@ -216,3 +229,36 @@ def gemm_flops(width: int, height: int) -> int:
         h.append((h[-1] + 1) // 2)
         w.append((w[-1] + 1) // 2)
     return sum(2 * h[l.level] * w[l.level] * l.cout * l.taps * l.cin for l in LAYERS)
+
+
+def train_data_parallel(k, steps: int, batch: int = 8, crop: int = 64, lr: float = 1e-3, seed: int = 1,
+                        device=None) -> np.ndarray:
+    """Data-parallel training over the ranks of the default torch.distributed group (one
+    process per GPU, NCCL): every rank draws its own crops from its own examples, the
+    gradients are summed by all_reduce and every rank applies the same Adam step with the
+    mean, so the weights stay identical.  Rank 0's weights are broadcast first.  `k` provides
+    n_params, get_params/set_params, grads(batch, crop, seed, buf) and apply(buf, scale, lr)
+    (a Kpcn).  Returns the losses averaged over ranks, one per step."""
+    import torch
+    import torch.distributed as dist
+    on = dist.is_available() and dist.is_initialized()
+    world = dist.get_world_size() if on else 1
+    rank = dist.get_rank() if on else 0
+    device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    if world > 1:
+        w = torch.from_numpy(k.get_params()).to(device)
+        dist.broadcast(w, 0)
+        k.set_params(w.cpu().numpy())
+    g = torch.empty(k.n_params, dtype=torch.float32, device=device)
+    losses = np.zeros(steps, np.float32)
+    lv = torch.zeros(1, dtype=torch.float32, device=device)
+    for step in range(steps):
+        lv[0] = k.grads(batch, crop, (seed * 1_000_003 + step) * world + rank, g)
+        if world > 1:
+            dist.all_reduce(g)
+            dist.all_reduce(lv)
+            if device.type == "cuda":
+                torch.cuda.current_stream(device).synchronize()
+        k.apply(g, 1.0 / world, lr)
+        losses[step] = float(lv[0]) / world
+    return losses

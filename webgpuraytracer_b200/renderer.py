@@ -88,16 +88,21 @@ class Renderer:
         self._check(self.L.wgpt_upload_scene(self.ctx, C.byref(self._desc)), "upload_scene")
         self.resize()
 
-    def update_objects(self):
-        """Fast path when everything fits and the flags are unchanged, else a full set_scene."""
-        packed = sc.pack_scene_data(self.scene)
+    def update_objects(self, packed: sc.PackedScene | None = None) -> bool:
+        """Renderer.updateObjects (tracer.js:2132-2164): repacks the scene and rewrites objects,
+        TLAS, planes, list meshes and materials in place when the flags match and everything
+        fits (lights, BLAS, sky and textures stay as uploaded, as in the reference); otherwise a
+        full set_scene.  Returns True when the fast path was taken."""
+        packed = packed if packed is not None else sc.pack_scene_data(self.scene)
         desc = scene_desc(packed)
-        rc = self.L.wgpt_update_scene(self.ctx, C.byref(desc))
-        if rc == 7:   # WGPT_E_REBUILD
+        rc = self.L.wgpt_update_objects(self.ctx, C.byref(desc))
+        if rc == 7:   # WGPT_E_REBUILD: SLOW PATH, full scene rebuild
             self.set_scene(self.scene, self.isgbuf, packed)
-            return
-        self._check(rc, "update_scene")
+            return False
+        self._check(rc, "update_objects")
+        # the uniforms take the new total light power (tracer.js:1841, 2234) while the light buffer stays
         self.packed, self._desc = packed, desc
+        return True
 
     def resize(self, width: int | None = None, height: int | None = None):
         if width is not None:

@@ -183,3 +183,32 @@ def test_update_rejects_bad_records_and_keeps_the_scene():
     with pytest.raises(WgptError):
         r._check(r.L.wgpt_update_objects(r.ctx, None), "null descriptor")
     r.close()
+
+
+def test_textured_scene_update_keeps_texture_layers():
+    """Materials that start or stop sampling a resident texture layer, and moved textured
+    objects: the layers keep the indices of the upload (updateObjects does not prepare the
+    texture array again), and a texture that was never prepared packs as -1."""
+    s = synth.textured_scene(2, W, H, 5)
+    r = rd.Renderer(W, H)
+    r.set_scene(s)
+    old = r.packed
+    mats = {m.name: m for m in s.get_materials()}
+    mats["rough"].albedoTex = mats["cutout"].albedoTex        # a resident layer
+    mats["glow"].normalTex = sc.Texture(np.full((64, 64, 4), 128, np.uint8), "never prepared")
+    mats["bumpy"].normalTex = None
+    objs = {o.name: o for o in s.objects}
+    objs["cut_sphere"].set_position(-1.0, 0.8, 0.5)
+    assert r.update_objects() is True
+    new = r.packed
+    m = _as_bytes(new.materials).view(np.int32).reshape(-1, 36)
+    idx = {name: i for i, name in enumerate(x.name for x in s.get_materials())}
+    assert m[idx["rough"], 24] == mats["cutout"].albedoTex.texIndex >= 0
+    assert m[idx["glow"], 25] == -1
+    emu = _emulated(old, new)
+    params = _params(s, new, 0)
+    acc_o, out_o = _oracle(emu, params, 0, 3)
+    acc_g, out_g = _gpu(r, params, 0, 3)
+    _same(acc_g, acc_o, "accumulation")
+    _same(out_g, out_o, "rgba8")
+    r.close()

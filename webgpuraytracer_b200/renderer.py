@@ -93,11 +93,11 @@ class Renderer:
         TLAS, planes, list meshes and materials in place when the flags match and everything
         fits (lights, BLAS, sky and textures stay as uploaded, as in the reference); otherwise a
         full set_scene.  Returns True when the fast path was taken."""
-        packed = packed if packed is not None else sc.pack_scene_data(self.scene)
+        packed = packed if packed is not None else sc.pack_scene_data(self.scene, prepare_textures=False)
         desc = scene_desc(packed)
         rc = self.L.wgpt_update_objects(self.ctx, C.byref(desc))
-        if rc == 7:   # WGPT_E_REBUILD: SLOW PATH, full scene rebuild
-            self.set_scene(self.scene, self.isgbuf, packed)
+        if rc == 7:   # WGPT_E_REBUILD: SLOW PATH, full scene rebuild (setScene prepares the textures)
+            self.set_scene(self.scene, self.isgbuf)
             return False
         self._check(rc, "update_objects")
         # the uniforms take the new total light power (tracer.js:1841, 2234) while the light buffer stays

@@ -624,11 +624,13 @@ def build_tlas(objects) -> np.ndarray:
     return nodes[: count.value].reshape(-1).copy()
 
 
-def pack_scene_data(scene: Scene) -> PackedScene:
+def pack_scene_data(scene: Scene, prepare_textures: bool = True) -> PackedScene:
     """Renderer.packSceneData(true) (tracer.js:1819-1917) plus the sky texture and CDF of
-    setScene (tracer.js:1976-2004)."""
+    setScene (tracer.js:1976-2004).  With prepare_textures false (the updateObjects path,
+    tracer.js:2136) the texture layers keep the texIndex values of the last full preparation,
+    a texture that never had one packs as -1, and no texture array is built."""
     # prepareTextureArray runs first in setScene (tracer.js:1964): layers follow getTextures order
-    textures = scene.get_textures()
+    textures = scene.get_textures() if prepare_textures else []
     for i, t in enumerate(textures):
         t.texIndex = i
     tex_array = None

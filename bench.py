@@ -50,8 +50,9 @@ BYTES_PER_UNIT = {
 }
 PIXEL_BYTES = 16 + 16 + 4   # accumulation read + write, rgba8 store
 # DRAM bytes (read + write) of one full-pool closest-hit launch of this workload, from an ncu
-# capture (bench cannot run ncu itself); the algorithmic bytes of the same launch are ~3.9 GB.
-EXTEND_DRAM_BYTES_PER_LAUNCH = 4.23e8
+# capture (bench cannot run ncu itself; profiles/k_wf_extend_flagship_1080p.md); the algorithmic
+# bytes of the same launch are ~3.9 GB.
+EXTEND_DRAM_BYTES_PER_LAUNCH = 5.96e8
 KERNELS = ["k_wf_fill", "k_wf_extend", "k_wf_shade", "k_wf_shadow", "k_wf_resolve", "k_wf_shade_miss",
            "k_wf_accumulate", "k_wf_control"]
 

@@ -247,13 +247,15 @@ __device__ __forceinline__ uint32_t refill(bool have, uint32_t* cursor, uint32_t
   return qi;
 }
 
-// Traversal kernels are latency bound: five resident 256-thread blocks per SM (at most 51
-// registers, a few spilled) measured 5-6 % faster than four (64 registers, none spilled), and six
-// (40 registers) slower again.
-constexpr int kTravBlocksPerSM = 5;
+// Traversal kernels are latency bound; their block shape trades registers for resident warps.
+// Measured on one box (flagship / batch, M paths/s): 256 x 4 per SM at 64 registers 569 / 691;
+// 256 x 5 at 48 (spilling) 597 / 732; 192 x 6 at 56 (closest hit without spills) 627 / 748;
+// 128 x 9 at 56 625 / 748; 128 x 10 at 48 596 / 734.
+constexpr int kTravThreads = 192;
+constexpr int kTravBlocksPerSM = 6;
 
 template <bool COUNT>
-__global__ void __launch_bounds__(256, kTravBlocksPerSM) k_wf_extend(WfArgs a) {
+__global__ void __launch_bounds__(kTravThreads, kTravBlocksPerSM) k_wf_extend(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   uint32_t err = 0;
   const uint32_t iter = a.ctl->iter;
@@ -702,7 +704,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
 
 // ---------------------------------------------------------------------------- shadow
 template <bool COUNT, bool TEX>
-__global__ void __launch_bounds__(256, TEX ? 3 : kTravBlocksPerSM) k_wf_shadow(WfArgs a) {
+__global__ void __launch_bounds__(kTravThreads, TEX ? 3 * 256 / kTravThreads : kTravBlocksPerSM) k_wf_shadow(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   uint32_t err = 0;
   const uint32_t iter = a.ctl->iter;
@@ -1025,11 +1027,11 @@ void wf_engine_get(const WfEngine* e, uint32_t* pool_paths, uint64_t* units_per_
 }
 
 template <typename K>
-static int occupancy_grid(K kernel) {
+static int occupancy_grid(K kernel, int threads = 256) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
   return sms * (per_sm > 0 ? per_sm : 1);
 }
 
@@ -1038,9 +1040,9 @@ static void compute_grids(WfEngine* e) {
   e->grid = e->grids[(COUNT ? 2 : 0) + (TEX ? 1 : 0)];
   if (e->grid[0]) return;
   e->grid[0] = occupancy_grid(k_wf_fill<COUNT>);
-  e->grid[1] = occupancy_grid(k_wf_extend<COUNT>);
+  e->grid[1] = occupancy_grid(k_wf_extend<COUNT>, kTravThreads);
   e->grid[2] = occupancy_grid(k_wf_shade<COUNT, TEX>);
-  e->grid[3] = occupancy_grid(k_wf_shadow<COUNT, TEX>);
+  e->grid[3] = occupancy_grid(k_wf_shadow<COUNT, TEX>, kTravThreads);
   e->grid[4] = occupancy_grid(k_wf_resolve<COUNT>);
   e->grid[5] = occupancy_grid(k_wf_shade_miss<COUNT>);
   e->grid[6] = occupancy_grid(k_wf_accumulate);
@@ -1073,7 +1075,8 @@ static cudaError_t build_graph(WfEngine* e, const WfArgs& a) {
     memset(&kp, 0, sizeof kp);
     kp.func = const_cast<void*>(fn);
     kp.gridDim = dim3((unsigned)grid);
-    kp.blockDim = dim3(grid == 1 ? 32u : 256u);
+    kp.blockDim = dim3(grid == 1 ? 32u : (fn == (const void*)k_wf_extend<COUNT> || fn == (const void*)k_wf_shadow<COUNT, TEX>)
+                                           ? (unsigned)kTravThreads : 256u);
     kp.sharedMemBytes = 0;
     kp.kernelParams = args;
     return cudaGraphAddKernelNode(out, gr, dep, dep ? 1 : 0, &kp);
@@ -1122,10 +1125,10 @@ static cudaError_t run_pass_host(WfEngine* e, const WfArgs& a, uint32_t max_iter
   auto T1 = [&](int k) { if (timer) timer->end(k, st); };
   T0(0); k_wf_fill<COUNT><<<e->grid[0], 256, 0, st>>>(stage_args(a, 0)); T1(0);
   for (uint32_t it = 0; it <= max_iter; ++it) {
-    T0(1); k_wf_extend<COUNT><<<e->grid[1], 256, 0, st>>>(stage_args(a, 1)); T1(1);
+    T0(1); k_wf_extend<COUNT><<<e->grid[1], kTravThreads, 0, st>>>(stage_args(a, 1)); T1(1);
     T0(5); k_wf_shade_miss<COUNT><<<e->grid[5], 256, 0, st>>>(stage_args(a, 5)); T1(5);
     T0(2); k_wf_shade<COUNT, TEX><<<e->grid[2], 256, 0, st>>>(stage_args(a, 2)); T1(2);
-    T0(3); k_wf_shadow<COUNT, TEX><<<e->grid[3], 256, 0, st>>>(stage_args(a, 3)); T1(3);
+    T0(3); k_wf_shadow<COUNT, TEX><<<e->grid[3], kTravThreads, 0, st>>>(stage_args(a, 3)); T1(3);
     T0(4); k_wf_resolve<COUNT><<<e->grid[4], 256, 0, st>>>(stage_args(a, 4)); T1(4);
     T0(7); k_wf_control<false><<<1, 32, 0, st>>>(stage_args(a, 7), cudaGraphConditionalHandle{}); T1(7);
     cudaError_t err = cudaMemcpyAsync(e->h_cond, &a.ctl->cond, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);

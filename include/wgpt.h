@@ -31,7 +31,8 @@ enum wgpt_status {
   WGPT_E_UNSUPPORTED = 6, /* a combination this build does not run (e.g. FP64 accumulation in the single-kernel mode) */
   WGPT_E_REBUILD = 7,     /* wgpt_update_scene / wgpt_update_objects: upload the scene again */
   WGPT_E_DEVICE = 8,      /* a kernel reported an error (traversal stack overflow) */
-  WGPT_E_TOO_LARGE = 9    /* wgpt_denoise_noalloc: more than WGPT_NOALLOC_MAX_PIXELS pixels */
+  WGPT_E_TOO_LARGE = 9,   /* wgpt_denoise_noalloc: more than WGPT_NOALLOC_MAX_PIXELS pixels */
+  WGPT_E_TIMEOUT = 10     /* wgpt_synchronize_timeout: the work did not finish in time */
 };
 
 typedef struct wgpt_ctx wgpt_ctx;
@@ -125,6 +126,7 @@ int wgpt_set_render_mode(wgpt_ctx* ctx, int mode);
    images and per-pixel confidence intervals.  The megakernel mode rejects it. */
 int wgpt_set_accum_f64(wgpt_ctx* ctx, int on);
 int wgpt_read_accum_f64(wgpt_ctx* ctx, double* dst_8_per_px);
+int wgpt_write_accum_f64(wgpt_ctx* ctx, const double* src_8_per_px);   /* checkpoint resume */
 
 /* Wavefront sizing (no counterpart in the reference, whose dispatch has no path pool):
    pool_paths path slots (1,024 .. 67,108,864; default 2,097,152; about 420 bytes each) and at
@@ -150,6 +152,16 @@ int wgpt_resample(wgpt_ctx* ctx, uint32_t dst_w, uint32_t dst_h, float ratio_x, 
 
 /* Waits for queued work; returns WGPT_E_DEVICE if a kernel flagged an error. */
 int wgpt_synchronize(wgpt_ctx* ctx);
+
+/* Host watchdog (no reference counterpart): polls the queued work instead of blocking and
+   returns WGPT_E_TIMEOUT after timeout_ms (the work keeps running; call again to keep waiting). */
+int wgpt_synchronize_timeout(wgpt_ctx* ctx, uint32_t timeout_ms);
+
+/* Self-test of the device-side bounded waits (no reference counterpart): a kernel waits on an
+   mbarrier phase nothing completes, through the same wait the tensor-core kernels use, and must
+   give up after `limit` polls (1..2^24); *status receives the device status word (4 = the wait
+   timed out), *ms (nullable) the kernel's duration.  The context stays usable. */
+int wgpt_selftest_wait(int device, uint32_t limit, uint32_t* status, float* ms);
 
 /* Readback / write-back of the context images (SaveRender, gui.js:1622; checkpoint/resume). */
 int wgpt_read_accum(wgpt_ctx* ctx, float* dst_rgba32f);

@@ -14,7 +14,7 @@ WGPT_OK = 0
 STATUS_NAMES = {
     0: "WGPT_OK", 1: "WGPT_E_INVALID", 2: "WGPT_E_LAYOUT", 3: "WGPT_E_CUDA", 4: "WGPT_E_NOMEM",
     5: "WGPT_E_STATE", 6: "WGPT_E_UNSUPPORTED", 7: "WGPT_E_REBUILD", 8: "WGPT_E_DEVICE",
-    9: "WGPT_E_TOO_LARGE",
+    9: "WGPT_E_TOO_LARGE", 10: "WGPT_E_TIMEOUT",
 }
 NOALLOC_MAX_PIXELS = 131072
 
@@ -77,6 +77,8 @@ EXPORTS = {
     "wgpt_denoise": ([_P, _P, _P, _U32], C.c_int),
     "wgpt_resample": ([_P, _U32, _U32, _F, _F], C.c_int),
     "wgpt_synchronize": ([_P], C.c_int),
+    "wgpt_synchronize_timeout": ([_P, C.c_uint32], C.c_int),
+    "wgpt_selftest_wait": ([C.c_int, C.c_uint32, _P, _P], C.c_int),
     "wgpt_read_accum": ([_P, _P], C.c_int),
     "wgpt_write_accum": ([_P, _P], C.c_int),
     "wgpt_read_output": ([_P, _P], C.c_int),
@@ -90,6 +92,7 @@ EXPORTS = {
     "wgpt_set_views": ([_P, C.c_uint32, _P, _P], C.c_int),
     "wgpt_set_accum_f64": ([_P, C.c_int], C.c_int),
     "wgpt_read_accum_f64": ([_P, _P], C.c_int),
+    "wgpt_write_accum_f64": ([_P, _P], C.c_int),
     "wgpt_gemm_bf16": ([C.c_int, _P, _P, _P, C.c_int, C.c_int, C.c_int], C.c_int),
     "wgpt_kpcn_create": ([C.c_int, C.c_uint64, C.POINTER(_P)], C.c_int),
     "wgpt_kpcn_destroy": ([_P], C.c_int),

@@ -9,6 +9,8 @@
 #include <set>
 #include <utility>
 #include <algorithm>
+#include <chrono>
+#include <thread>
 
 #include "../../include/wgpt.h"
 #include "wgpt_internal.h"
@@ -770,10 +772,7 @@ int wgpt_resample(wgpt_ctx* ctx, uint32_t dst_w, uint32_t dst_h, float rx, float
   return WGPT_OK;
 }
 
-int wgpt_synchronize(wgpt_ctx* ctx) {
-  if (!ctx) return WGPT_E_INVALID;
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-  CK(cudaStreamSynchronize(ctx->stream), "stream synchronize");
+static int read_status(wgpt_ctx* ctx) {
   uint32_t st = 0;
   CK(cudaMemcpy(&st, ctx->d_status, sizeof st, cudaMemcpyDeviceToHost), "status readback");
   if (st) {
@@ -782,6 +781,36 @@ int wgpt_synchronize(wgpt_ctx* ctx) {
     return fail(ctx, WGPT_E_DEVICE, "a kernel overflowed its traversal stack");
   }
   return WGPT_OK;
+}
+
+int wgpt_synchronize(wgpt_ctx* ctx) {
+  if (!ctx) return WGPT_E_INVALID;
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "stream synchronize");
+  return read_status(ctx);
+}
+
+// Host watchdog: polls the context's stream instead of blocking on it, and gives up after
+// timeout_ms with WGPT_E_TIMEOUT (the queued work keeps running; a later call can wait again).
+int wgpt_synchronize_timeout(wgpt_ctx* ctx, uint32_t timeout_ms) {
+  if (!ctx) return WGPT_E_INVALID;
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  const auto t0 = std::chrono::steady_clock::now();
+  while (true) {
+    cudaError_t q = cudaStreamQuery(ctx->stream);
+    if (q == cudaSuccess) break;
+    if (q != cudaErrorNotReady) {
+      ctx->err = std::string("stream query: ") + cudaGetErrorString(q);
+      return WGPT_E_CUDA;
+    }
+    const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+    if ((uint64_t)ms >= timeout_ms) {
+      ctx->err = "the context's work did not finish within " + std::to_string(timeout_ms) + " ms";
+      return WGPT_E_TIMEOUT;
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(100));
+  }
+  return read_status(ctx);
 }
 
 static int readback(wgpt_ctx* ctx, void* dst, const void* src, size_t n, const char* what) {
@@ -986,6 +1015,15 @@ int wgpt_set_accum_f64(wgpt_ctx* ctx, int on) {
 int wgpt_read_accum_f64(wgpt_ctx* ctx, double* dst) {
   if (!ctx) return WGPT_E_INVALID;
   return readback(ctx, dst, ctx->acc64, (size_t)ctx->w * ctx->h * 64, "read FP64 accumulation");
+}
+
+int wgpt_write_accum_f64(wgpt_ctx* ctx, const double* src) {
+  if (!ctx || !src) return WGPT_E_INVALID;
+  if (!ctx->acc64) return fail(ctx, WGPT_E_STATE, "FP64 accumulation is off");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "drain");
+  CK(cudaMemcpy(ctx->acc64, src, (size_t)ctx->w * ctx->h * 64, cudaMemcpyHostToDevice), "write FP64 accumulation");
+  return WGPT_OK;
 }
 
 int wgpt_set_wavefront_config(wgpt_ctx* ctx, uint32_t pool_paths, uint64_t units_per_pass) {

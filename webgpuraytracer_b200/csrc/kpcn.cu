@@ -1100,7 +1100,43 @@ int draw_crops(wgpt_kpcn* k, size_t count, uint32_t crop, uint64_t seed) {
 
 }  // namespace
 
+// Self-test of the tensor-core kernels' bounded waits: one thread waits on an mbarrier phase
+// that nothing completes; the wait must give up after `limit` polls and report the timeout bit.
+__global__ void k_selftest_wait(uint32_t limit, uint32_t* status) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    const uint32_t b = tc::smem_u32(&bar);
+    tc::mbar_init(b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (!tc::mbar_wait_n(b, 0u, limit)) atomicOr(status, tc::ERR_TC_TIMEOUT);
+  }
+}
+
 extern "C" {
+
+int wgpt_selftest_wait(int device, uint32_t limit, uint32_t* status, float* ms) {
+  if (!status || limit == 0 || limit > (1u << 24)) return WGPT_E_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return WGPT_E_CUDA;
+  uint32_t* d = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = WGPT_OK;
+  if (cudaMalloc(&d, 4) != cudaSuccess) return WGPT_E_NOMEM;
+  if (cudaMemset(d, 0, 4) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    rc = WGPT_E_CUDA;
+  } else {
+    cudaEventRecord(e0);
+    k_selftest_wait<<<1, 32>>>(limit, d);
+    cudaEventRecord(e1);
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaMemcpy(status, d, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = WGPT_E_CUDA;
+    else if (ms)
+      cudaEventElapsedTime(ms, e0, e1);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(d);
+  return rc;
+}
 
 int wgpt_kpcn_create(int device, uint64_t seed, wgpt_kpcn** out) {
   if (!out) return WGPT_E_INVALID;

@@ -170,6 +170,41 @@ class Renderer:
     def synchronize(self):
         self._check(self.L.wgpt_synchronize(self.ctx), "synchronize")
 
+    def wait(self, timeout_ms: int) -> bool:
+        """Host watchdog: True once the queued work finished, False if it is still running after
+        timeout_ms (it keeps running); kernel-reported errors raise as in synchronize()."""
+        rc = self.L.wgpt_synchronize_timeout(self.ctx, int(timeout_ms))
+        if rc == 10:   # WGPT_E_TIMEOUT
+            return False
+        self._check(rc, "synchronize_timeout")
+        return True
+
+    # -- checkpoint / resume (long converged renders)
+    def save_state(self, path):
+        """Writes the accumulation (FP32 running mean, and the FP64 Welford records when they are
+        on), the frame count and the image size to an .npz file."""
+        state = {"accum": self.read_accum(), "frame": np.int64(self.frame),
+                 "size": np.array([self.width, self.height], np.int64)}
+        if getattr(self, "_acc64_on", False):
+            a = np.empty((self.height, self.width, 8), np.float64)
+            self._check(self.L.wgpt_read_accum_f64(self.ctx, ptr(a)), "read_accum_f64")
+            state["accum64"] = a
+        np.savez(path, **state)
+
+    def load_state(self, path):
+        """Restores a save_state() file into this renderer (same image size; the FP64 records
+        are restored when the file has them, switching FP64 accumulation on)."""
+        with np.load(path) as f:
+            w, h = (int(v) for v in f["size"])
+            if (w, h) != (self.width, self.height):
+                raise ValueError(f"checkpoint is {w}x{h}, renderer is {self.width}x{self.height}")
+            self.write_accum(np.ascontiguousarray(f["accum"], np.float32))
+            if "accum64" in f.files:
+                self.set_accum_f64(True)
+                a = np.ascontiguousarray(f["accum64"], np.float64)
+                self._check(self.L.wgpt_write_accum_f64(self.ctx, ptr(a)), "write_accum_f64")
+            self.frame = int(f["frame"])
+
     # -- readback
     def read_accum(self) -> np.ndarray:
         a = np.empty((self.height, self.width, 4), dtype=np.float32)
@@ -209,6 +244,7 @@ class Renderer:
     def set_accum_f64(self, on: bool = True):
         """FP64 Welford accumulation of every sample next to the FP32 running mean."""
         self._check(self.L.wgpt_set_accum_f64(self.ctx, 1 if on else 0), "set_accum_f64")
+        self._acc64_on = bool(on)
 
     def read_accum_f64(self):
         """(mean (H, W, 3), per-sample variance (H, W, 3), sample count (H, W)) in float64."""

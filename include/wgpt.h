@@ -66,6 +66,9 @@ typedef struct wgpt_scene_desc {
   uint32_t tex_width;
   uint32_t tex_height;
   uint32_t tex_layers;
+  /* optional (no reference counterpart): alias table of the sky, sky_width * sky_height entries
+     of {float prob; uint32_t alias;} from wgpt_build_env_alias, for wgpt_set_env_sampling */
+  const void* sky_alias;
 } wgpt_scene_desc;
 
 /* Renderer constructor + init() (tracer.js:1720-1770): binds CUDA device `device`. */
@@ -118,6 +121,15 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sec
    compute entry point.  Both produce identical results. */
 enum { WGPT_MODE_WAVEFRONT = 0, WGPT_MODE_MEGAKERNEL = 1 };
 int wgpt_set_render_mode(wgpt_ctx* ctx, int mode);
+
+/* Environment light sampling for next-event estimation: WGPT_ENV_CDF (default) inverts the
+   reference's CDF by binary search (shader.wgsl:192-254) and reproduces its sample stream;
+   WGPT_ENV_ALIAS draws the texel from the uploaded alias table in O(1) with the same per-texel
+   probabilities (FP64 weights; same random numbers consumed, same pdf), so images agree
+   statistically, not bit for bit.  WGPT_E_STATE when no alias table was uploaded.  The mode
+   stays set across uploads; a scene uploaded without sky_alias samples by CDF. */
+enum { WGPT_ENV_CDF = 0, WGPT_ENV_ALIAS = 1 };
+int wgpt_set_env_sampling(wgpt_ctx* ctx, int mode);
 
 /* FP64 accumulation (no counterpart in the reference): with it on, the wavefront mode also
    folds every sample, in sample order, into a per-pixel FP64 Welford record of 8 doubles
@@ -291,6 +303,10 @@ int wgpt_build_tlas(const float* aabbs6, uint32_t n, wgpt_bvh_node* nodes_out, u
    floats and the total weight (sky_total_lum).  exposure is a JavaScript number (double). */
 int wgpt_build_env_cdf(const uint16_t* rgba16f, uint32_t w, uint32_t h, double exposure, float* cdf_out,
                        double* total_weight);
+/* Alias table over the texel weights buildHDRCDF uses (FP64): prob[i] (float) and alias[i] per
+   texel, width * height entries each (no reference counterpart). */
+int wgpt_build_env_alias(const uint16_t* rgba16f, uint32_t width, uint32_t height, double exposure, float* prob,
+                         uint32_t* alias);
 /* parseHdr (lib/parse-hdr.js:125-211) + HDRTexture.updateData (tracer.js:76-87): decodes a
    Radiance RLE RGBE file into w x h rgba16f texels (exposure applied, clamp 65519). Call with
    rgba16f == NULL to query w and h. */

@@ -4,6 +4,7 @@ from __future__ import annotations
 
 import ctypes as C
 import re
+import subprocess
 from pathlib import Path
 
 import numpy as np
@@ -41,6 +42,20 @@ def test_struct_sizes_match_layout_header():
                               ("wgpt_triangle", 128), ("wgpt_light", 80), ("wgpt_gbuffer_texel", 48),
                               ("wgpt_denoise_uniforms", 48)):
         assert f"sizeof({struct_name}) == {size}" in text
+
+
+def test_scene_descriptor_matches_the_header(tmp_path):
+    """The ctypes wgpt_scene_desc has the C header's field offsets and size (gcc prints them)."""
+    fields = [f[0] for f in _lib.SceneDesc._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "wgpt.h"\nint main(void) {\n'
+                   + "".join(f'  printf("%zu\\n", offsetof(wgpt_scene_desc, {f}));\n' for f in fields)
+                   + '  printf("%zu\\n", sizeof(wgpt_scene_desc));\n  return 0;\n}\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = [getattr(_lib.SceneDesc, f).offset for f in fields] + [C.sizeof(_lib.SceneDesc)]
+    assert got == want
 
 
 def _desc(p):

@@ -275,3 +275,52 @@ def test_parse_obj_reference_assets_match_restatement():
         _same_nan(m.triangles24(), host_oracle.parse_obj(text))
         m.generate_bvh()
         assert m.nodes.shape[0] >= 1
+
+
+def _alias_realized(prob_bits, alias):
+    """Probability with which the alias table returns each texel (first number picks a bin
+    uniformly, the second keeps it with prob or takes its alias)."""
+    prob = prob_bits.view(np.float32).astype(np.float64)
+    n = prob.size
+    p = prob.copy()
+    np.add.at(p, alias, 1.0 - prob)
+    return p / n
+
+
+@pytest.mark.parametrize("w,h,exposure", [(1, 1, 1.0), (16, 8, 1.0), (64, 32, 2.5), (7, 13, 0.3)])
+def test_env_alias_reproduces_texel_weights(w, h, exposure):
+    rng = np.random.default_rng(7 * w + h)
+    img = np.ones((h, w, 4))
+    img[..., :3] = np.minimum(rng.exponential(1.0, (h, w, 3)) * np.where(rng.random((h, w, 1)) < 0.02, 5e4, 1.0), 6e4)
+    img[0, : w // 2, :3] = 0.0                      # some texels of zero weight
+    data16 = np.ascontiguousarray(img.astype(np.float16).view(np.uint16).reshape(-1))
+    sky = sc.HDRTexture(exposure=exposure, rgba16f=data16, width=w, height=h)
+    table = sky.build_env_alias()
+    assert table.shape == (w * h, 2) and table.dtype == np.uint32
+    prob = table[:, 0].view(np.float32)
+    assert np.all((prob >= 0) & (prob <= 1)) and np.all(table[:, 1] < w * h)
+    # the texel weights buildHDRCDF accumulates (FP64), normalised
+    d = data16.view(np.float16).astype(np.float64).reshape(h, w, 4)
+    rgb = np.minimum(d[..., :3] * exposure, 65536 - 16 - 1)
+    sin_t = np.sin(np.pi * (np.arange(h) + 0.5) / h)[:, None]
+    lum = (0.2126 * rgb[..., 0] + 0.7152 * rgb[..., 1] + 0.0722 * rgb[..., 2]) * sin_t
+    want = (lum / lum.sum()).reshape(-1)
+    got = _alias_realized(table[:, 0].copy(), table[:, 1])
+    # float32 probabilities: each bin is off by at most 2^-24 of 1/n, a texel collects few bins
+    np.testing.assert_allclose(got, want, rtol=0, atol=64 * 2.0 ** -24 / (w * h) + 1e-15)
+    assert np.all(got[want == 0] == 0)
+    # the same distribution the CDF encodes, to FP32 rounding of the CDF
+    cdf, _ = native_cdf(data16, w, h, exposure)
+    marg = np.diff(cdf[: h + 1].astype(np.float64))
+    cond = np.diff(cdf[h + 1:].astype(np.float64).reshape(h, w + 1), axis=1)
+    np.testing.assert_allclose((marg[:, None] * cond).reshape(-1), want, rtol=0, atol=1e-6)
+
+
+def test_env_alias_black_sky_is_uniform():
+    w, h = 8, 4
+    sky = sc.HDRTexture(exposure=1.0, rgba16f=np.zeros(w * h * 4, np.uint16), width=w, height=h)
+    table = sky.build_env_alias()
+    np.testing.assert_array_equal(table[:, 0].view(np.float32), np.ones(w * h, np.float32))
+    np.testing.assert_array_equal(table[:, 1], np.arange(w * h))
+    with pytest.raises(Exception):
+        check(lib().wgpt_build_env_alias(None, w, h, 1.0, None, None), "null")

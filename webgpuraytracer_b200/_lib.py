@@ -20,6 +20,8 @@ NOALLOC_MAX_PIXELS = 131072
 
 MODE_WAVEFRONT = 0
 MODE_MEGAKERNEL = 1
+ENV_CDF = 0
+ENV_ALIAS = 1
 
 # feature flags (pipeline override constants 1..11, shader.wgsl:1-12)
 HAS_SPHERES = 1 << 0
@@ -46,7 +48,7 @@ class SceneDesc(C.Structure):
         ("sky_rgba16f", C.c_void_p), ("sky_width", C.c_uint32), ("sky_height", C.c_uint32),
         ("bounce_limit", C.c_int32), ("feature_flags", C.c_uint32),
         ("textures_rgba8", C.c_void_p), ("tex_width", C.c_uint32), ("tex_height", C.c_uint32),
-        ("tex_layers", C.c_uint32),
+        ("tex_layers", C.c_uint32), ("sky_alias", C.c_void_p),
     ]
 
 
@@ -88,6 +90,7 @@ EXPORTS = {
     "wgpt_read_canvas": ([_P, _P, _U32, _U32], C.c_int),
     "wgpt_trace_rays": ([_P, _P, _U32, _P, _P, _P, _P, _P], C.c_int),
     "wgpt_set_render_mode": ([_P, C.c_int], C.c_int),
+    "wgpt_set_env_sampling": ([_P, C.c_int], C.c_int),
     "wgpt_set_wavefront_config": ([_P, C.c_uint32, C.c_uint64], C.c_int),
     "wgpt_set_views": ([_P, C.c_uint32, _P, _P], C.c_int),
     "wgpt_set_accum_f64": ([_P, C.c_int], C.c_int),
@@ -122,6 +125,7 @@ EXPORTS = {
     "wgpt_build_blas": ([_P, _U32, _P, C.POINTER(_U32), _P], C.c_int),
     "wgpt_build_tlas": ([_P, _U32, _P, C.POINTER(_U32)], C.c_int),
     "wgpt_build_env_cdf": ([_P, _U32, _U32, C.c_double, _P, C.POINTER(C.c_double)], C.c_int),
+    "wgpt_build_env_alias": ([_P, _U32, _U32, C.c_double, _P, _P], C.c_int),
     "wgpt_decode_rgbe": ([_P, C.c_size_t, C.c_double, _P, C.POINTER(_U32), C.POINTER(_U32)], C.c_int),
     "wgpt_parse_obj": ([_P, C.c_size_t, _P, C.c_uint32, C.POINTER(C.c_uint32), _P, C.c_uint32,
                         C.POINTER(C.c_uint32)], C.c_int),

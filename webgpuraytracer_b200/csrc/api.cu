@@ -20,10 +20,12 @@ struct wgpt_ctx {
   cudaStream_t stream = nullptr;
   std::string err;
   // scene buffers: 0 materials, 1 objects, 2 tlas, 3 meshes, 4 bvh, 5 triangles, 6 planes,
-  // 7 lights, 8 sky_cdf, 9 sky texels, 10 texture array
-  void* d_buf[11] = {nullptr};
-  size_t cap[11] = {0};
-  size_t bytes[11] = {0};
+  // 7 lights, 8 sky_cdf, 9 sky texels, 10 texture array, 11 sky alias table
+  void* d_buf[12] = {nullptr};
+  size_t cap[12] = {0};
+  size_t bytes[12] = {0};
+  bool has_alias = false;
+  int env_mode = WGPT_ENV_CDF;
   wgpt::DeviceScene ds{};
   bool has_scene = false;
   // images
@@ -93,10 +95,10 @@ void dfree_t(T*& p) {
   p = nullptr;
 }
 
-const uint32_t kStride[11] = {WGPT_STRIDE_MATERIAL, WGPT_STRIDE_OBJECT, WGPT_STRIDE_NODE, WGPT_STRIDE_MESH_READ,
-                              WGPT_STRIDE_NODE, WGPT_STRIDE_TRIANGLE, WGPT_STRIDE_PLANE, WGPT_STRIDE_LIGHT, 4, 8, 4};
-const char* kName[11] = {"materials", "objects", "tlas", "meshes", "bvh", "triangles", "planes", "lights",
-                         "sky_cdf", "sky", "textures"};
+const uint32_t kStride[12] = {WGPT_STRIDE_MATERIAL, WGPT_STRIDE_OBJECT, WGPT_STRIDE_NODE, WGPT_STRIDE_MESH_READ,
+                              WGPT_STRIDE_NODE, WGPT_STRIDE_TRIANGLE, WGPT_STRIDE_PLANE, WGPT_STRIDE_LIGHT, 4, 8, 4, 8};
+const char* kName[12] = {"materials", "objects", "tlas", "meshes", "bvh", "triangles", "planes", "lights",
+                         "sky_cdf", "sky", "textures", "sky_alias"};
 
 struct HostScene {
   const wgpt_material* mats; uint32_t n_mats;
@@ -276,9 +278,11 @@ int upload_buffers(wgpt_ctx* ctx, const wgpt_scene_desc* d, bool in_place_only) 
                                &d->triangles, &d->planes, &d->lights, &d->sky_cdf};
   size_t sky_bytes = (size_t)d->sky_width * d->sky_height * 8;
   const size_t tex_bytes = d->textures_rgba8 ? (size_t)d->tex_width * d->tex_height * d->tex_layers * 4 : 0;
-  for (int k = 0; k < 11; ++k) {
-    const void* p = k < 9 ? src[k]->ptr : k == 9 ? (const void*)d->sky_rgba16f : (const void*)d->textures_rgba8;
-    size_t n = k < 9 ? src[k]->bytes : k == 9 ? sky_bytes : tex_bytes;
+  const size_t alias_bytes = d->sky_alias ? (size_t)d->sky_width * d->sky_height * 8 : 0;
+  for (int k = 0; k < 12; ++k) {
+    const void* p = k < 9 ? src[k]->ptr : k == 9 ? (const void*)d->sky_rgba16f
+                  : k == 10 ? (const void*)d->textures_rgba8 : d->sky_alias;
+    size_t n = k < 9 ? src[k]->bytes : k == 9 ? sky_bytes : k == 10 ? tex_bytes : alias_bytes;
     if (n == 0 || p == nullptr) {
       // empty arrays are bound as one zeroed element (tracer.js:1789, makeBuf minimum sizes)
       n = kStride[k];
@@ -324,6 +328,18 @@ int check_desc(wgpt_ctx* ctx, const wgpt_scene_desc* d, HostScene& hs,
                             (uint64_t)d->tex_width * d->tex_height * d->tex_layers > (1ull << 30)))
     return fail(ctx, WGPT_E_INVALID, "texture array size must be nonzero and at most 2^30 texels");
   hs.tex_layers = d->textures_rgba8 ? d->tex_layers : 0u;
+  if (d->sky_alias) {
+    if (!d->sky_rgba16f || d->sky_width == 0 || d->sky_height == 0)
+      return fail(ctx, WGPT_E_INVALID, "sky_alias given without a sky texture");
+    const size_t na = (size_t)d->sky_width * d->sky_height;
+    const uint32_t* a = (const uint32_t*)d->sky_alias;
+    for (size_t i = 0; i < na; ++i) {
+      float pr;
+      memcpy(&pr, &a[2 * i], 4);
+      if (!(pr >= 0.0f && pr <= 1.0f) || a[2 * i + 1] >= na)
+        return fail(ctx, WGPT_E_LAYOUT, "sky_alias: entry " + std::to_string(i) + " has a probability outside [0, 1] or an alias out of range");
+    }
+  }
   auto cnt = [&](int k) { return (uint32_t)(b[k]->bytes / kStride[k]); };
   hs.mats = (const wgpt_material*)b[0]->ptr; hs.n_mats = cnt(0);
   hs.objs = (const wgpt_object*)b[1]->ptr; hs.n_objs = cnt(1);
@@ -377,11 +393,14 @@ void fill_device_scene(wgpt_ctx* ctx, const wgpt_scene_desc* d) {
   s.tex_w = d->textures_rgba8 ? d->tex_width : 1u;
   s.tex_h = d->textures_rgba8 ? d->tex_height : 1u;
   s.tex_layers = d->textures_rgba8 ? d->tex_layers : 0u;
+  s.alias = ctx->d_buf[11];
+  ctx->has_alias = d->sky_alias != nullptr;
   s.bounce_limit = d->bounce_limit;
   const wgpt_material* m = (const wgpt_material*)d->materials.ptr;
   const size_t nm = d->materials.bytes / WGPT_STRIDE_MATERIAL;
   ctx->host_mats.assign(m, m + nm);
   s.flags = d->feature_flags | derived_flags(m, nm, d->feature_flags);
+  if (ctx->has_alias && ctx->env_mode == WGPT_ENV_ALIAS) s.flags |= wgpt::SCENE_ENV_ALIAS;
   const wgpt_light* lt = (const wgpt_light*)d->lights.ptr;
   ctx->light_objs.clear();
   for (size_t i = 0; i < d->lights.bytes / WGPT_STRIDE_LIGHT; ++i) ctx->light_objs.push_back(lt[i].obj_idx);
@@ -465,7 +484,7 @@ int wgpt_destroy(wgpt_ctx* ctx) {
   if (!ctx) return WGPT_E_INVALID;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  for (int k = 0; k < 11; ++k) dfree(ctx->d_buf[k]);
+  for (int k = 0; k < 12; ++k) dfree(ctx->d_buf[k]);
   dfree_t(ctx->accum); dfree_t(ctx->out); dfree_t(ctx->gbuf);
   dfree_t(ctx->dn_a); dfree_t(ctx->dn_b); dfree_t(ctx->dn_guide); dfree_t(ctx->dn_comp);
   dfree_t(ctx->canvas); dfree_t(ctx->d_status); dfree_t(ctx->d_counters); wgpt::wf_engine_destroy(ctx->wf);
@@ -645,6 +664,7 @@ int wgpt_update_objects(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   if (nm) {
     std::copy(mats, mats + nm, ctx->host_mats.begin());
     ctx->ds.flags = flags | derived_flags(ctx->host_mats.data(), ctx->host_mats.size(), flags);
+    if (ctx->has_alias && ctx->env_mode == WGPT_ENV_ALIAS) ctx->ds.flags |= wgpt::SCENE_ENV_ALIAS;
   }
   return WGPT_OK;
 }
@@ -995,6 +1015,18 @@ int wgpt_read_view(wgpt_ctx* ctx, uint32_t view, float* accum, uint8_t* out) {
   size_t np = (size_t)v.w * v.h;
   if (accum) CK(cudaMemcpy(accum, v.accum, np * 16, cudaMemcpyDeviceToHost), "read view accumulation");
   if (out) CK(cudaMemcpy(out, v.out, np * 4, cudaMemcpyDeviceToHost), "read view image");
+  return WGPT_OK;
+}
+
+int wgpt_set_env_sampling(wgpt_ctx* ctx, int mode) {
+  if (!ctx || (mode != WGPT_ENV_CDF && mode != WGPT_ENV_ALIAS)) return WGPT_E_INVALID;
+  if (mode == WGPT_ENV_ALIAS && !(ctx->has_scene && ctx->has_alias))
+    return fail(ctx, WGPT_E_STATE, "no sky alias table uploaded (wgpt_scene_desc.sky_alias)");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "drain");
+  ctx->env_mode = mode;
+  if (mode == WGPT_ENV_ALIAS) ctx->ds.flags |= wgpt::SCENE_ENV_ALIAS;
+  else ctx->ds.flags &= ~(uint32_t)wgpt::SCENE_ENV_ALIAS;
   return WGPT_OK;
 }
 

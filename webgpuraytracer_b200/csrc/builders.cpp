@@ -3,6 +3,7 @@
 //   wgpt_build_blas    ModelData.generateBVH, binned SAH (tracer.js:1025-1118)
 //   wgpt_build_tlas    SceneBVHBuilder, median split on the widest axis (tracer.js:1509-1619)
 //   wgpt_build_env_cdf HDRTexture.buildHDRCDF (tracer.js:135-204)
+//   wgpt_build_env_alias an alias table over the same weights (opt-in sampling mode)
 //   wgpt_decode_rgbe   parseHdr (lib/parse-hdr.js:20-211) + HDRTexture.updateData (tracer.js:76-87)
 // JavaScript numbers are IEEE doubles and Float32Array / Float16Array stores round to nearest
 // even; the builders compute in double and round at the same stores, so their outputs are the
@@ -292,6 +293,56 @@ int wgpt_build_env_cdf(const uint16_t* data, uint32_t width, uint32_t height, do
     for (uint32_t y = 1; y <= height; ++y) margCDF[y] = (float)((double)y / height);
   }
   if (total_weight) *total_weight = total;
+  return WGPT_OK;
+}
+
+// Alias table (Walker / Vose) over the texels of the environment, from the same FP64 weights as
+// buildHDRCDF (luminance of the clamped, exposed texel times the row's sin(theta)): texel i is
+// drawn with probability w_i / sum(w) by picking a bin uniformly and keeping it with probability
+// prob[i], else taking alias[i].  A zero total draws texels uniformly.
+int wgpt_build_env_alias(const uint16_t* data, uint32_t width, uint32_t height, double exposure_f, float* prob,
+                         uint32_t* alias) {
+  if (!data || !prob || !alias || width == 0 || height == 0) return WGPT_E_INVALID;
+  const double exposure = exposure_f;
+  const double threshold = 65536 - 16 - 1;   // tracer.js:30
+  const size_t n = (size_t)width * height;
+  std::vector<double> w(n);
+  double total = 0;
+  for (uint32_t y = 0; y < height; ++y) {
+    const double sin_theta = sin(M_PI * (y + 0.5) / height);
+    for (uint32_t x = 0; x < width; ++x) {
+      const uint16_t* t = data + ((size_t)y * width + x) * 4;
+      double r = std::min(half_to_double(t[0]) * exposure, threshold);
+      double g = std::min(half_to_double(t[1]) * exposure, threshold);
+      double b = std::min(half_to_double(t[2]) * exposure, threshold);
+      double lum = (0.2126 * r + 0.7152 * g + 0.0722 * b) * sin_theta;
+      w[(size_t)y * width + x] = lum;
+      total += lum;
+    }
+  }
+  if (!(total > 0) || !std::isfinite(total)) {
+    for (size_t i = 0; i < n; ++i) { prob[i] = 1.0f; alias[i] = (uint32_t)i; }
+    return WGPT_OK;
+  }
+  std::vector<double> scaled(n);
+  std::vector<uint32_t> small, large;
+  small.reserve(n);
+  large.reserve(n);
+  for (size_t i = 0; i < n; ++i) {
+    scaled[i] = std::max(w[i], 0.0) * (double)n / total;
+    (scaled[i] < 1.0 ? small : large).push_back((uint32_t)i);
+  }
+  while (!small.empty() && !large.empty()) {
+    const uint32_t sm = small.back(), lg = large.back();
+    small.pop_back();
+    large.pop_back();
+    prob[sm] = (float)scaled[sm];
+    alias[sm] = lg;
+    scaled[lg] = (scaled[lg] + scaled[sm]) - 1.0;
+    (scaled[lg] < 1.0 ? small : large).push_back(lg);
+  }
+  for (uint32_t i : large) { prob[i] = 1.0f; alias[i] = i; }
+  for (uint32_t i : small) { prob[i] = 1.0f; alias[i] = i; }   // rounding leftovers
   return WGPT_OK;
 }
 

@@ -47,6 +47,7 @@ struct DScene {
   const uint2* sky; uint32_t sky_w, sky_h; // rgba16f texel = 8 bytes
   const float* cdf; uint32_t n_cdf;
   const uint32_t* tex; uint32_t tex_w, tex_h;   // rgba8 texture array, one 32-bit texel per entry
+  const uint2* alias;                           // sky alias table: (prob bits, alias) per texel
   int32_t bounce_limit;
   uint32_t flags;   // WGPT_HAS_* plus the wgpt::SCENE_* bits derived from the materials
 };
@@ -203,9 +204,21 @@ struct LightSample { v3 dir; v3 color; float dist; float pdf; };
 template <bool COUNT>
 static __device__ __noinline__ LightSample sample_env_cdf(const DScene& s, const DParams& p, float ux, float uy, Counters<COUNT>& cn) {
   LightSample samp;
-  uint32_t v_idx = binary_search_cdf(s, 0u, p.sky_height, uy, cn);
-  uint32_t row_offset = p.sky_cdf_index + (v_idx * (p.sky_width + 1u));
-  uint32_t u_idx = binary_search_cdf(s, row_offset, p.sky_width, ux, cn);
+  uint32_t v_idx, u_idx;
+  if (HAS(s, wgpt::SCENE_ENV_ALIAS)) {
+    // alias table over the same texel weights: the first number picks a bin, the second keeps
+    // it or takes its alias (validated on upload: probabilities in [0, 1], aliases in range)
+    const uint32_t n = s.sky_w * s.sky_h;
+    const uint32_t i = min((uint32_t)(ux * (float)n), n - 1u);
+    const uint2 e = __ldg(s.alias + i);
+    const uint32_t t = uy < __uint_as_float(e.x) ? i : e.y;
+    v_idx = t / s.sky_w;
+    u_idx = t - v_idx * s.sky_w;
+  } else {
+    v_idx = binary_search_cdf(s, 0u, p.sky_height, uy, cn);
+    uint32_t row_offset = p.sky_cdf_index + (v_idx * (p.sky_width + 1u));
+    u_idx = binary_search_cdf(s, row_offset, p.sky_width, ux, cn);
+  }
   float u_coord = ((float)u_idx + 0.5f) / (float)p.sky_width;
   float v_coord = ((float)v_idx + 0.5f) / (float)p.sky_height;
   float theta = PI * v_coord;

@@ -911,6 +911,7 @@ static void fill_dscene(DScene& s, const DeviceScene& d) {
   s.sky = (const uint2*)d.sky; s.sky_w = d.sky_w; s.sky_h = d.sky_h;
   s.cdf = (const float*)d.cdf; s.n_cdf = d.n_cdf;
   s.tex = (const uint32_t*)d.tex; s.tex_w = d.tex_w; s.tex_h = d.tex_h;
+  s.alias = (const uint2*)d.alias;
   s.bounce_limit = d.bounce_limit; s.flags = d.flags;
 }
 

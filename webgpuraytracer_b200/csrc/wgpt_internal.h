@@ -24,7 +24,8 @@ bool ctx_images(::wgpt_ctx* ctx, int view, CtxImages* out);   // view -1: the ma
 // material samples a texture; some has an albedo texture (shadow rays then attenuate through
 // it); some reads the tangent frame, through a normal map or a height field (closest hits then
 // carry their tangent-frame source).
-enum : uint32_t { SCENE_TEXTURED = 1u << 24, SCENE_ALPHA_SHADOWS = 1u << 25, SCENE_TANGENTS = 1u << 26 };
+enum : uint32_t { SCENE_TEXTURED = 1u << 24, SCENE_ALPHA_SHADOWS = 1u << 25, SCENE_TANGENTS = 1u << 26,
+                  SCENE_ENV_ALIAS = 1u << 27 };   // environment NEE from the alias table
 
 // Device copies of the scene buffers, in the reference's packed layouts.
 struct DeviceScene {
@@ -39,6 +40,7 @@ struct DeviceScene {
   const void* sky; uint32_t sky_w, sky_h;
   const void* cdf; uint32_t n_cdf;
   const void* tex; uint32_t tex_w, tex_h, tex_layers;   // rgba8 texture array
+  const void* alias;                                    // sky alias table (8 bytes per texel)
   int32_t bounce_limit;
   uint32_t flags;
 };

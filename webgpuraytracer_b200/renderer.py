@@ -18,7 +18,7 @@ import math
 import numpy as np
 
 from . import scene as sc
-from ._lib import SceneDesc, Buffer, check, lib, ptr
+from ._lib import ENV_ALIAS, ENV_CDF, SceneDesc, Buffer, check, lib, ptr
 
 
 def _buf(a: np.ndarray | None) -> Buffer:
@@ -46,6 +46,8 @@ def scene_desc(p: sc.PackedScene) -> SceneDesc:
     if p.textures is not None:
         d.textures_rgba8 = ptr(p.textures)
         d.tex_layers, d.tex_height, d.tex_width = p.textures.shape[:3]
+    if p.sky_alias is not None:
+        d.sky_alias = ptr(p.sky_alias)
     return d
 
 
@@ -94,6 +96,8 @@ class Renderer:
         fits (lights, BLAS, sky and textures stay as uploaded, as in the reference); otherwise a
         full set_scene.  Returns True when the fast path was taken."""
         packed = packed if packed is not None else sc.pack_scene_data(self.scene, prepare_textures=False)
+        if packed.sky_alias is None and self.packed is not None:
+            packed.sky_alias = self.packed.sky_alias     # the sky is not rewritten either
         desc = scene_desc(packed)
         rc = self.L.wgpt_update_objects(self.ctx, C.byref(desc))
         if rc == 7:   # WGPT_E_REBUILD: SLOW PATH, full scene rebuild (setScene prepares the textures)
@@ -257,6 +261,15 @@ class Renderer:
     def set_render_mode(self, mode: int):
         """MODE_WAVEFRONT (path pool with regeneration) or MODE_MEGAKERNEL (one thread per pixel)."""
         self._check(self.L.wgpt_set_render_mode(self.ctx, int(mode)), "set_render_mode")
+
+    def set_env_sampling(self, mode: int):
+        """ENV_CDF (the reference's CDF search, bit-exact) or ENV_ALIAS (O(1) alias table, same
+        texel probabilities: statistically equal images).  ENV_ALIAS builds the sky's alias table
+        and uploads the scene again when the current upload has none (the frame count restarts)."""
+        if mode == ENV_ALIAS and self.packed is not None and self.packed.sky_alias is None:
+            self.packed.sky_alias = self.scene.background.build_env_alias()
+            self.set_scene(self.scene, self.isgbuf, packed=self.packed)
+        self._check(self.L.wgpt_set_env_sampling(self.ctx, int(mode)), "set_env_sampling")
 
     def set_wavefront_config(self, pool_paths: int = 0, units_per_pass: int = 0):
         """Path-slot pool size and samples per pass of the wavefront renderer (0 keeps a value)."""

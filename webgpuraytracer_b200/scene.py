@@ -78,6 +78,16 @@ class HDRTexture:
                                        C.byref(total)), "build_env_cdf")
         return cdf, self.height + 1, total.value
 
+    def build_env_alias(self) -> np.ndarray:
+        """Alias table over buildHDRCDF's texel weights (FP64): (width * height, 2) uint32 rows of
+        (float32 probability bits, alias texel), the layout of wgpt_scene_desc.sky_alias."""
+        n = self.width * self.height
+        prob = np.zeros(n, dtype=np.float32)
+        alias = np.zeros(n, dtype=np.uint32)
+        check(lib().wgpt_build_env_alias(ptr(self.data), self.width, self.height, self.exposure, ptr(prob),
+                                         ptr(alias)), "build_env_alias")
+        return np.ascontiguousarray(np.stack([prob.view(np.uint32), alias], axis=1))
+
 
 # ----------------------------------------------------------------------------- materials
 class Texture:
@@ -606,6 +616,7 @@ class PackedScene:
     bounce_limit: int
     flags: int
     textures: np.ndarray | None = None     # (layers, H, W, 4) uint8 texture array, or None
+    sky_alias: np.ndarray | None = None    # (W*H, 2) uint32 alias table of the sky, or None
     extra: dict = field(default_factory=dict)
 
 

@@ -150,16 +150,34 @@ __device__ __forceinline__ void flush_wf(Counters<COUNT>& cn, unsigned long long
   }
 }
 
-// Warp-aggregated append of `slot` to a queue.
-__device__ __forceinline__ void queue_push(uint32_t* q, uint32_t* count, uint32_t slot, bool push) {
-  unsigned mask = __ballot_sync(0xffffffffu, push);
-  if (!mask) return;
-  int lane = threadIdx.x & 31;
-  int leader = __ffs(mask) - 1;
-  uint32_t base = 0;
-  if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (push) q[base + __popc(mask & ((1u << lane) - 1u))] = slot;
+// Block-wide allocation of `k` entries per thread from one atomicAdd on `count`; returns the
+// thread's first entry.  Every thread of the block calls it at the same point (the kernels'
+// loops run the same number of times in all threads of a block).  One atomic per block instead
+// of one per warp: all the block's pushes to a queue share a single counter, and same-address
+// atomics are serialised in L2.  `sh` is a __shared__ array of blockDim.x / 32 + 1 words.
+__device__ __forceinline__ uint32_t block_alloc(uint32_t* count, uint32_t k, uint32_t* sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint32_t x = k;   // inclusive scan over the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[warp] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t tot = 0;
+    for (int w = 0; w < nw; ++w) {
+      uint32_t c = sh[w];
+      sh[w] = tot;
+      tot += c;
+    }
+    sh[nw] = tot ? atomicAdd(count, tot) : 0u;
+  }
+  __syncthreads();
+  const uint32_t r = sh[nw] + sh[warp] + x - k;
+  __syncthreads();   // sh is reused by the next call
+  return r;
 }
 
 // The view a unit belongs to (views are ordered by unit_base).
@@ -363,6 +381,7 @@ __global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a) {
   const uint32_t n = q.n;
   uint32_t* hit_count = &a.ctl->counts[iter & 3u][K_HIT];
   const DParams& sp = a.ctl->sp;
+  __shared__ uint32_t sh[9];
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     bool is_hit = false;
@@ -371,7 +390,8 @@ __global__ void __launch_bounds__(256) k_wf_shade_miss(WfArgs a) {
       slot = q.at(i);
       is_hit = (int32_t)a.b.hit[slot * 2].y != -1;
     }
-    queue_push(a.b.hitq, hit_count, slot, is_hit);
+    const uint32_t at = block_alloc(hit_count, is_hit ? 1u : 0u, sh);
+    if (is_hit) a.b.hitq[at] = slot;
     if (i < n && !is_hit) {
       float4 d4 = a.b.ray[slot * 2 + 1], tp4 = a.b.tr[slot * 2], rd4 = a.b.tr[slot * 2 + 1];
       uint4 meta = a.b.meta[slot];
@@ -585,6 +605,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
   const uint32_t n = a.ctl->counts[iter & 3u][K_HIT];
   uint32_t* sh_count = &a.ctl->counts[iter & 3u][K_SHADOW];
   const DParams& p = a.ctl->sp;
+  __shared__ uint32_t shq[9];
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     bool alive = false, sh_light = false, sh_env = false;
@@ -725,8 +746,9 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
       a.b.tr[slot * 2 + 1] = make_float4(radiance.x, radiance.y, radiance.z, last_weight_sum);
       a.b.meta[slot] = make_uint4(rng, flags, (uint32_t)bounce, (uint32_t)stack.count);
     }
-    queue_push(a.b.shq, sh_count, slot * 2u, sh_light);
-    queue_push(a.b.shq, sh_count, slot * 2u + 1u, sh_env);
+    const uint32_t at = block_alloc(sh_count, (sh_light ? 1u : 0u) + (sh_env ? 1u : 0u), shq);
+    if (sh_light) a.b.shq[at] = slot * 2u;
+    if (sh_env) a.b.shq[at + (sh_light ? 1u : 0u)] = slot * 2u + 1u;
   }
   flush_wf<COUNT>(cn, a.counters, true);
 }
@@ -782,6 +804,7 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a) {
   uint32_t* new_count = &a.ctl->counts[r1][K_NEW];
   const uint32_t n_units = a.ctl->n_units, n_views = a.ctl->n_views;
   const bool track = a.ctl->track != 0u;
+  __shared__ uint32_t sh[9];
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     bool alive = false, ended = false;
@@ -823,7 +846,8 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a) {
         ended = true;
       }
     }
-    queue_push(a.b.qcont[p1], cont_count, slot, alive);
+    const uint32_t at = block_alloc(cont_count, alive ? 1u : 0u, sh);
+    if (alive) a.b.qcont[p1][at] = slot;
     unsigned em = __ballot_sync(0xffffffffu, ended);
     if (track && ended) {
       // one atomic per view per warp; the lane that takes a view's count to zero stamps it
@@ -835,21 +859,13 @@ __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a) {
       }
     }
     bool started = false;
-    if (em) {
-      int lane = threadIdx.x & 31;
-      int leader = __ffs(em) - 1;
-      uint32_t ubase = 0;
-      if (lane == leader) ubase = atomicAdd(&a.ctl->unit_next, (uint32_t)__popc(em));
-      ubase = __shfl_sync(0xffffffffu, ubase, leader);
-      if (ended) {
-        uint32_t u = ubase + (uint32_t)__popc(em & ((1u << lane) - 1u));
-        if (u < n_units) {
-          spawn<COUNT>(a, n_views, slot, u, cn);
-          started = true;
-        }
-      }
+    const uint32_t u = block_alloc(&a.ctl->unit_next, ended ? 1u : 0u, sh);
+    if (ended && u < n_units) {
+      spawn<COUNT>(a, n_views, slot, u, cn);
+      started = true;
     }
-    queue_push(a.b.qnew[p1], new_count, slot, started);
+    const uint32_t at_new = block_alloc(new_count, started ? 1u : 0u, sh);
+    if (started) a.b.qnew[p1][at_new] = slot;
   }
   flush_wf<COUNT>(cn, a.counters, true);
 }

@@ -49,10 +49,11 @@ BYTES_PER_UNIT = {
     11: 32,   # hit attributes of the winning primitive (normals)
 }
 PIXEL_BYTES = 16 + 16 + 4   # accumulation read + write, rgba8 store
-# DRAM bytes (read + write) of one full-pool closest-hit launch of this workload, from an ncu
-# capture (bench cannot run ncu itself; profiles/k_wf_extend_flagship_1080p.md); the algorithmic
-# bytes of the same launch are ~3.9 GB.
-EXTEND_DRAM_BYTES_PER_LAUNCH = 5.96e8
+# DRAM bytes (read + write) per closest-hit ray of this workload: 596 MB per steady-state launch of
+# a 2,097,152-slot pool (every slot holds a live path while units remain, so 2,097,152 rays per
+# launch), from an ncu capture (bench cannot run ncu itself; profiles/k_wf_extend_flagship_1080p.md).
+# A launch's traffic is this times its rays; the capture's algorithmic bytes were ~3.9 GB.
+EXTEND_DRAM_BYTES_PER_RAY = 5.96e8 / 2_097_152
 KERNELS = ["k_wf_fill", "k_wf_extend", "k_wf_shade", "k_wf_shadow", "k_wf_resolve", "k_wf_shade_miss",
            "k_wf_accumulate", "k_wf_control"]
 
@@ -327,10 +328,15 @@ def time_to_rmse(args) -> dict:
     s_nn = first(lambda r_: r_["kpcn"])
 
     def timed(spp_, filt):
-        """Device time of rendering spp_ samples from scratch and filtering once."""
+        """Device time of rendering spp_ samples from frame 0 and filtering once, on a renderer
+        that has already run one call of the same size (its path pool and sample buffer are
+        allocated and its loop graph built, as in an interactive session); frame 0 overwrites
+        the accumulation, so the timed images equal a fresh renderer's."""
         r_ = rd.Renderer(W, H, seed_fn=lambda: 7)
         r_.set_scene(scene, isgbuf=True)
         r_.render_gbuffer()
+        r_.reset()
+        r_.render(tsize=W, reps=spp_)
         r_.reset()
         st = torch.cuda.ExternalStream(r_.stream_handle())
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -466,6 +472,7 @@ def run_ours(args):
         rep["launches"])
     peaks, peak_kind = load_peaks()
     rays = int(cnt[1] + cnt[2])
+    ext_rays_per_launch = int(cnt[1]) / max(1, stages.get("k_wf_extend", {}).get("launches", 1))
 
     # the opt-in alias-table environment sampling on the same steps (statistically equal images,
     # not bit-exact, so never the headline value)
@@ -516,10 +523,11 @@ def run_ours(args):
             "stages": stages,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"],
-                         "traffic": None if mega else EXTEND_DRAM_BYTES_PER_LAUNCH,
+                         "traffic": None if mega else EXTEND_DRAM_BYTES_PER_RAY * ext_rays_per_launch,
                          "traffic_source": None if mega else
                          "ncu dram__bytes_read.sum + dram__bytes_write.sum of steady-state k_wf_extend launches "
-                         "(mean of launches 21-23 of this workload's stage-timing pass)",
+                         "of a 2,097,152-slot pool (mean of launches 21-23 of this workload's stage-timing pass: "
+                         "284 B per ray), times this run's closest-hit rays per launch",
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
                          "kernel": "k_render" if mega else KERNELS[dom],

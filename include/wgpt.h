@@ -141,7 +141,8 @@ int wgpt_read_accum_f64(wgpt_ctx* ctx, double* dst_8_per_px);
 int wgpt_write_accum_f64(wgpt_ctx* ctx, const double* src_8_per_px);   /* checkpoint resume */
 
 /* Wavefront sizing (no counterpart in the reference, whose dispatch has no path pool):
-   pool_paths path slots (1,024 .. 67,108,864; default 2,097,152; about 420 bytes each) and at
+   pool_paths path slots (1,024 .. 67,108,864; default 67,108,864; 448 bytes each; a pass uses
+   no more than its samples, and a new pool takes at most a quarter of the free device memory) and at
    most units_per_pass samples held (65,536 .. 2^30; default 2^27; 16 bytes each) before they are
    folded into the images; a call with more samples runs in several passes.  Results do not
    depend on either.  0 keeps the current value. */

@@ -11,7 +11,7 @@ from __future__ import annotations
 
 from typing import Callable, Iterable
 
-POOL_CANDIDATES = (1 << 20, 1 << 21, 1 << 22, 1 << 23)
+POOL_CANDIDATES = (1 << 23, 1 << 24, 1 << 25, 1 << 26)
 UNITS_CANDIDATES = (1 << 27, 1 << 29)
 
 

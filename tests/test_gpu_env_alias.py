@@ -2,7 +2,7 @@
 
 The reference draws environment light samples by binary search over its CDF
 (shader.wgsl:192-254); ENV_ALIAS draws the same texel distribution from an alias table in O(1).
-It consumes the same random numbers and returns the same pdf, so it is judged statistically:
+It consumes the same random numbers and returns the same pdf, so it is checked statistically:
 with the FP64 per-pixel accumulators, the two modes' means agree within their standard errors
 and their per-sample variances match.  Uploading an alias table without switching to it leaves
 the default path bit for bit unchanged.

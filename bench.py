@@ -49,11 +49,11 @@ BYTES_PER_UNIT = {
     11: 32,   # hit attributes of the winning primitive (normals)
 }
 PIXEL_BYTES = 16 + 16 + 4   # accumulation read + write, rgba8 store
-# DRAM bytes (read + write) per closest-hit ray of this workload: 596 MB per steady-state launch of
+# DRAM bytes (read + write) per closest-hit ray of this workload: 502 MB per steady-state launch of
 # a 2,097,152-slot pool (every slot holds a live path while units remain, so 2,097,152 rays per
 # launch), from an ncu capture (bench cannot run ncu itself; profiles/k_wf_extend_flagship_1080p.md).
-# A launch's traffic is this times its rays; the capture's algorithmic bytes were ~3.9 GB.
-EXTEND_DRAM_BYTES_PER_RAY = 5.96e8 / 2_097_152
+# A launch's traffic is this times its rays.
+EXTEND_DRAM_BYTES_PER_RAY = 5.02e8 / 2_097_152
 KERNELS = ["k_wf_fill", "k_wf_extend", "k_wf_shade", "k_wf_shadow", "k_wf_resolve", "k_wf_shade_miss",
            "k_wf_accumulate", "k_wf_control"]
 
@@ -527,7 +527,7 @@ def run_ours(args):
                          "traffic_source": None if mega else
                          "ncu dram__bytes_read.sum + dram__bytes_write.sum of steady-state k_wf_extend launches "
                          "of a 2,097,152-slot pool (mean of launches 21-23 of this workload's stage-timing pass: "
-                         "284 B per ray), times this run's closest-hit rays per launch",
+                         "239 B per ray), times this run's closest-hit rays per launch",
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
                          "kernel": "k_render" if mega else KERNELS[dom],

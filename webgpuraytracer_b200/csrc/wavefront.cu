@@ -604,8 +604,15 @@ __device__ __forceinline__ bool wf_sample_surface(Ray& ray, v3& throughput, v3 h
   return alive;
 }
 
+// Surface shading blocks: one 512-thread block per SM at 128 registers; textured scenes need
+// ~200 registers and keep 256-thread blocks.  Measured on the flagship (M paths/s, one box):
+// 128 threads 868.6, 256 threads 916.0, 512 threads 957.4 (shading 40.8 / 33.2 / 27.1 ms per
+// step): the larger the block, the fewer block-wide queue allocations and blocks to schedule.
+template <bool TEX>
+constexpr int shade_threads() { return TEX ? 256 : 512; }
+
 template <bool COUNT, bool TEX>
-__global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
+__global__ void __launch_bounds__(TEX ? 256 : 512) k_wf_shade(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   const DScene& s = a.s;
   const uint32_t iter = a.ctl->iter;
@@ -613,7 +620,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfArgs a) {
   const uint32_t n = a.ctl->counts[iter & 3u][K_HIT];
   uint32_t* sh_count = &a.ctl->counts[iter & 3u][K_SHADOW];
   const DParams& p = a.ctl->sp;
-  __shared__ uint32_t shq[9];
+  __shared__ uint32_t shq[512 / 32 + 1];
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     bool alive = false, sh_light = false, sh_env = false;
@@ -1101,7 +1108,7 @@ static void compute_grids(WfEngine* e) {
   if (e->grid[0]) return;
   e->grid[0] = occupancy_grid(k_wf_fill<COUNT>);
   e->grid[1] = occupancy_grid(k_wf_extend<COUNT>, kTravThreads);
-  e->grid[2] = occupancy_grid(k_wf_shade<COUNT, TEX>);
+  e->grid[2] = occupancy_grid(k_wf_shade<COUNT, TEX>, shade_threads<TEX>());
   e->grid[3] = occupancy_grid(k_wf_shadow<COUNT, TEX>, kTravThreads);
   e->grid[4] = occupancy_grid(k_wf_resolve<COUNT>);
   e->grid[5] = occupancy_grid(k_wf_shade_miss<COUNT>);
@@ -1136,7 +1143,9 @@ static cudaError_t build_graph(WfEngine* e, const WfArgs& a) {
     kp.func = const_cast<void*>(fn);
     kp.gridDim = dim3((unsigned)grid);
     kp.blockDim = dim3(grid == 1 ? 32u : (fn == (const void*)k_wf_extend<COUNT> || fn == (const void*)k_wf_shadow<COUNT, TEX>)
-                                           ? (unsigned)kTravThreads : 256u);
+                                           ? (unsigned)kTravThreads
+                                           : fn == (const void*)k_wf_shade<COUNT, TEX> ? (unsigned)shade_threads<TEX>()
+                                                                                        : 256u);
     kp.sharedMemBytes = 0;
     kp.kernelParams = args;
     return cudaGraphAddKernelNode(out, gr, dep, dep ? 1 : 0, &kp);
@@ -1187,7 +1196,7 @@ static cudaError_t run_pass_host(WfEngine* e, const WfArgs& a, uint32_t max_iter
   for (uint32_t it = 0; it <= max_iter; ++it) {
     T0(1); k_wf_extend<COUNT><<<e->grid[1], kTravThreads, 0, st>>>(stage_args(a, 1)); T1(1);
     T0(5); k_wf_shade_miss<COUNT><<<e->grid[5], 256, 0, st>>>(stage_args(a, 5)); T1(5);
-    T0(2); k_wf_shade<COUNT, TEX><<<e->grid[2], 256, 0, st>>>(stage_args(a, 2)); T1(2);
+    T0(2); k_wf_shade<COUNT, TEX><<<e->grid[2], shade_threads<TEX>(), 0, st>>>(stage_args(a, 2)); T1(2);
     T0(3); k_wf_shadow<COUNT, TEX><<<e->grid[3], kTravThreads, 0, st>>>(stage_args(a, 3)); T1(3);
     T0(4); k_wf_resolve<COUNT><<<e->grid[4], 256, 0, st>>>(stage_args(a, 4)); T1(4);
     T0(7); k_wf_control<false><<<1, 32, 0, st>>>(stage_args(a, 7), cudaGraphConditionalHandle{}); T1(7);

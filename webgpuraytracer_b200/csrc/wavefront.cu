@@ -377,7 +377,7 @@ __device__ __forceinline__ void apply_medium(const MediumStack& stack, const Hit
 }
 
 // Walks the iteration's queue in order: paths that hit a surface go to the hit queue (kept in
-// queue order within each warp, so the surface stage sees rays as coherent as the queue); paths
+// queue order within each block, so the surface stage sees rays as coherent as the queue); paths
 // that left the scene are shaded here: medium, then the sky (MIS-weighted after the first
 // bounce) or the background colour (shader.wgsl:2344-2358).  They end here.
 template <bool COUNT>
@@ -807,7 +807,7 @@ __global__ void __launch_bounds__(kTravThreads, TEX ? 3 * 256 / kTravThreads : k
 // ---------------------------------------------------------------------------- resolve
 // Adds the recorded next-event contributions (shader.wgsl:2271 with the shadow result), queues
 // continuing paths for the next iteration, stores the radiance of finished paths under their
-// unit and starts the next units in the freed slots (handed out in queue order within a warp).
+// unit and starts the next units in the freed slots (handed out in queue order within a block).
 template <bool COUNT>
 __global__ void __launch_bounds__(256) k_wf_resolve(WfArgs a) {
   Counters<COUNT> cn; cn.init();

@@ -32,14 +32,17 @@ def time_call(renderer, fn: Callable[[], object], repeats: int = 1) -> float:
 
 
 def tune_wavefront(renderer, fn: Callable[[], object], pools: Iterable[int] = POOL_CANDIDATES,
-                   units: Iterable[int] = UNITS_CANDIDATES, repeats: int = 1) -> dict:
+                   units: Iterable[int] = UNITS_CANDIDATES, repeats: int = 1, timer=None) -> dict:
     """Times fn() for every (pool, units_per_pass) pair, applies the fastest and returns
-    {"pool_paths", "units_per_pass", "ms", "table": [(pool, units, ms), ...]}."""
+    {"pool_paths", "units_per_pass", "ms", "table": [(pool, units, ms), ...]}.  `timer(renderer,
+    fn, repeats)` defaults to time_call (CUDA events on the renderer's stream); ties keep the
+    first candidate in table order."""
+    timer = timer or time_call
     table = []
     for u in units:
         for p in pools:
             renderer.set_wavefront_config(p, u)
-            table.append((p, u, time_call(renderer, fn, repeats)))
+            table.append((p, u, timer(renderer, fn, repeats)))
     best = min(table, key=lambda row: row[2])
     renderer.set_wavefront_config(best[0], best[1])
     return {"pool_paths": best[0], "units_per_pass": best[1], "ms": best[2], "table": table}

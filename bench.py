@@ -18,6 +18,7 @@ reference's WGSL cannot run here: it needs a WebGPU device and no graphics stack
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -472,6 +473,8 @@ def run_ours(args):
         rep["launches"])
     peaks, peak_kind = load_peaks()
     rays = int(cnt[1] + cnt[2])
+    l2 = C.c_double(0.0)
+    r._check(r.L.wgpt_probe_l2_read(local, 64 << 20, 200, C.byref(l2)), "L2 probe")
     ext_rays_per_launch = int(cnt[1]) / max(1, stages.get("k_wf_extend", {}).get("launches", 1))
 
     # the opt-in alias-table environment sampling on the same steps (statistically equal images,
@@ -534,7 +537,10 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": bytes_per_launch,
                          "launch_ms": avg_launch_s * 1e3,
                          "note": "scene (~80 MB) is L2-resident; traversal is latency/divergence bound; stage "
-                                 "times from a host-driven pass of the same kernels on the same stream"},
+                                 "times from a host-driven pass of the same kernels on the same stream",
+                         "l2": {"peak": l2.value, "unit": "GB/s", "frac": achieved / l2.value,
+                                "peak_source": "measured in this run: wgpt_probe_l2_read, a 64 MiB buffer read "
+                                               "200 times with L2-only loads"}},
             "counters_per_step": {"paths": int(cnt[0]), "ext_rays": int(cnt[1]), "shadow_rays": int(cnt[2]),
                                   "nodes": int(cnt[3]), "tri_tests": int(cnt[5])},
             "clocks": clocks,

@@ -176,6 +176,11 @@ int wgpt_synchronize_timeout(wgpt_ctx* ctx, uint32_t timeout_ms);
    timed out), *ms (nullable) the kernel's duration.  The context stays usable. */
 int wgpt_selftest_wait(int device, uint32_t limit, uint32_t* status, float* ms);
 
+/* L2 read bandwidth of `device` (measurement support, no reference counterpart): streams an
+   L2-resident buffer of `bytes` (1 MiB .. 96 MiB, a multiple of 16) `reps` times (1..1000) with
+   L2-only loads and writes the rate in GB/s.  Allocates and frees its buffer. */
+int wgpt_probe_l2_read(int device, uint64_t bytes, uint32_t reps, double* gbps);
+
 /* Readback / write-back of the context images (SaveRender, gui.js:1622; checkpoint/resume). */
 int wgpt_read_accum(wgpt_ctx* ctx, float* dst_rgba32f);
 int wgpt_write_accum(wgpt_ctx* ctx, const float* src_rgba32f);

@@ -128,3 +128,13 @@ def test_validate_rejects_cyclic_blas():
     bad.bvh = nodes.view(np.uint8).reshape(-1).copy()
     d = _desc(bad)
     assert L.wgpt_validate_scene(C.byref(d), msg, 256) == 2
+
+
+def test_l2_probe_rejects_bad_arguments_before_touching_a_device():
+    L = _lib.lib()
+    out = C.c_double(0.0)
+    assert L.wgpt_probe_l2_read(0, 0, 1, C.byref(out)) == 1              # below 1 MiB
+    assert L.wgpt_probe_l2_read(0, 128 << 20, 1, C.byref(out)) == 1      # above 96 MiB
+    assert L.wgpt_probe_l2_read(0, (1 << 20) + 8, 1, C.byref(out)) == 1  # not a multiple of 16
+    assert L.wgpt_probe_l2_read(0, 1 << 20, 0, C.byref(out)) == 1        # no repetitions
+    assert L.wgpt_probe_l2_read(0, 1 << 20, 1, None) == 1

@@ -107,3 +107,10 @@ def test_checkpoint_resume_is_bitexact(tmp_path):
         other.load_state(path)
     for r in (whole, resumed, other):
         r.close()
+
+
+def test_l2_probe_measures_more_than_hbm_can_stream():
+    L = _lib.lib()
+    out = C.c_double(0.0)
+    assert L.wgpt_probe_l2_read(0, 32 << 20, 50, C.byref(out)) == 0
+    assert 1000.0 < out.value < 200000.0                 # GB/s: an L2-resident read, finite

@@ -16,7 +16,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libwgpt.so"
-CU_SOURCES = ["tracer.cu", "wavefront.cu", "denoise.cu", "api.cu", "kpcn.cu"]
+CU_SOURCES = ["tracer.cu", "wavefront.cu", "denoise.cu", "api.cu", "kpcn.cu", "probe.cu"]
 CXX_SOURCES = ["builders.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [

@@ -170,17 +170,6 @@ int wgpt_synchronize(wgpt_ctx* ctx);
    returns WGPT_E_TIMEOUT after timeout_ms (the work keeps running; call again to keep waiting). */
 int wgpt_synchronize_timeout(wgpt_ctx* ctx, uint32_t timeout_ms);
 
-/* Self-test of the device-side bounded waits (no reference counterpart): a kernel waits on an
-   mbarrier phase nothing completes, through the same wait the tensor-core kernels use, and must
-   give up after `limit` polls (1..2^24); *status receives the device status word (4 = the wait
-   timed out), *ms (nullable) the kernel's duration.  The context stays usable. */
-int wgpt_selftest_wait(int device, uint32_t limit, uint32_t* status, float* ms);
-
-/* L2 read bandwidth of `device` (measurement support, no reference counterpart): streams an
-   L2-resident buffer of `bytes` (1 MiB .. 96 MiB, a multiple of 16) `reps` times (1..1000) with
-   L2-only loads and writes the rate in GB/s.  Allocates and frees its buffer. */
-int wgpt_probe_l2_read(int device, uint64_t bytes, uint32_t reps, double* gbps);
-
 /* Readback / write-back of the context images (SaveRender, gui.js:1622; checkpoint/resume). */
 int wgpt_read_accum(wgpt_ctx* ctx, float* dst_rgba32f);
 int wgpt_write_accum(wgpt_ctx* ctx, const float* src_rgba32f);
@@ -288,7 +277,11 @@ void* wgpt_stream(wgpt_ctx* ctx);
    until the process exits.  uniforms_48 and steps are host memory.  Images larger than
    WGPT_NOALLOC_MAX_PIXELS return WGPT_E_TOO_LARGE before any work is queued.  The first call on
    a device looks up the array's device address (cudaGetSymbolAddress) with that device current:
-   make that first call before capturing a stream.  Work is queued on `stream` (a
+   make that first call before capturing a stream.  The address is kept per device ordinal for
+   the life of the process: after cudaDeviceReset the module is loaded again and the array may
+   move, so a process that resets a device must not call this function on it again.  color, gbuf
+   and out_composited must be 16-byte aligned and out_rgba8 4-byte aligned (WGPT_E_INVALID
+   otherwise).  Work is queued on `stream` (a
    cudaStream_t, NULL for the legacy default stream) on the current device.  All calls share the
    one array: calls that overlap on the GPU (different streams, or different host threads)
    race and corrupt each other's intermediates; queue them on one stream. */
@@ -329,6 +322,21 @@ int wgpt_decode_rgbe(const uint8_t* file, size_t bytes, double exposure, uint16_
    that Model.getBounds walks. */
 int wgpt_parse_obj(const char* text, size_t bytes, float* tris24, uint32_t capacity, uint32_t* n_tris,
                    float* positions, uint32_t pos_capacity, uint32_t* n_positions);
+
+/* ---------------------------------------------------------------------------------------
+   Test and measurement support.  Not part of the renderer surface that tracer.js binds: the
+   robustness tests and the benchmark call these. */
+
+/* Self-test of the device-side bounded waits (no reference counterpart): a kernel waits on an
+   mbarrier phase nothing completes, through the same wait the tensor-core kernels use, and must
+   give up after `limit` polls (1..2^24); *status receives the device status word (4 = the wait
+   timed out), *ms (nullable) the kernel's duration.  The context stays usable. */
+int wgpt_selftest_wait(int device, uint32_t limit, uint32_t* status, float* ms);
+
+/* L2 read bandwidth of `device` (measurement support, no reference counterpart): streams an
+   L2-resident buffer of `bytes` (1 MiB .. 96 MiB, a multiple of 16) `reps` times (1..1000) with
+   L2-only loads and writes the rate in GB/s.  Allocates and frees its buffer. */
+int wgpt_probe_l2_read(int device, uint64_t bytes, uint32_t reps, double* gbps);
 
 #ifdef __cplusplus
 }

@@ -78,3 +78,21 @@ def test_noalloc_denoise_rejects_images_above_its_limit():
                                     small.data_ptr(), None, None)
     assert rc == 9        # WGPT_E_TOO_LARGE, nothing queued
     assert torch.count_nonzero(small).item() == 0
+
+
+def test_noalloc_denoise_rejects_misaligned_pointers():
+    import torch
+
+    dev = torch.device("cuda", 0)
+    buf = torch.zeros(4096, dtype=torch.float32, device=dev)
+    base = buf.data_ptr()
+    u = rd.denoise_uniforms(16, 16, passes=1)
+    steps = rd.step_schedule(1, "intended")
+    L = lib()
+    # colour, G-buffer and the float output are read and written as float4, the rgba8 output as uchar4
+    for color, gbuf, out8, comp in ((base + 4, base, base, None), (base, base + 8, base, None),
+                                    (base, base, base, base + 4), (base, base, base + 2, None)):
+        rc = L.wgpt_denoise_noalloc(color, gbuf, ptr(u), ptr(steps), 1, out8, comp, None)
+        assert rc == 1      # WGPT_E_INVALID, nothing queued
+    torch.cuda.synchronize(dev)
+    assert torch.count_nonzero(buf).item() == 0

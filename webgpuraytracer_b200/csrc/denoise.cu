@@ -232,6 +232,9 @@ extern "C" int wgpt_denoise_noalloc(const float* color, const void* gbuf, const 
                                     const uint32_t* steps, uint32_t passes, uint8_t* out_rgba8,
                                     float* out_composited, void* stream) {
   if (!color || !gbuf || !uniforms_48 || !out_rgba8 || (passes && !steps)) return WGPT_E_INVALID;
+  // the kernels read color and gbuf and write out_composited as float4, out_rgba8 as uchar4
+  if (((uintptr_t)color | (uintptr_t)gbuf | (uintptr_t)out_composited) & 15u) return WGPT_E_INVALID;
+  if ((uintptr_t)out_rgba8 & 3u) return WGPT_E_INVALID;
   wgpt_denoise_uniforms u;
   memcpy(&u, uniforms_48, sizeof u);
   if (u.width == 0 || u.height == 0) return WGPT_E_INVALID;

@@ -333,6 +333,19 @@ int wgpt_parse_obj(const char* text, size_t bytes, float* tris24, uint32_t capac
    timed out), *ms (nullable) the kernel's duration.  The context stays usable. */
 int wgpt_selftest_wait(int device, uint32_t limit, uint32_t* status, float* ms);
 
+/* Environment light samples of caller random pairs (known-answer tests of the CDF search; no
+   reference counterpart): for each (u.x, u.y) of u2 (n pairs), the sky texel that sample_env_cdf
+   (shader.wgsl:231-254) picks with the two binary_search_cdf calls (192-206) as (x, y) in
+   texel_xy, and the sample's pdf.  Needs an uploaded scene with an importance-sampled sky and
+   wgpt_set_params (its sky fields).  Host pointers; n <= 2^24. */
+int wgpt_sample_env(wgpt_ctx* ctx, const float* u2, uint32_t n, uint32_t* texel_xy, float* pdf);
+
+/* The random stream main draws for pixel `idx` at sample `sample_number` with `seed`
+   (rand_pcg and its seeding, shader.wgsl:146-154, 2280-2282): draws 1..n after the discarded
+   first one, computed on `device` (known-answer tests of the device's PCG; no reference
+   counterpart).  n <= 2^20; host output. */
+int wgpt_rng_stream(int device, uint32_t idx, uint32_t sample_number, uint32_t seed, uint32_t n, float* out);
+
 /* L2 read bandwidth of `device` (measurement support, no reference counterpart): streams an
    L2-resident buffer of `bytes` (1 MiB .. 96 MiB, a multiple of 16) `reps` times (1..1000) with
    L2-only loads and writes the rate in GB/s.  Allocates and frees its buffer. */

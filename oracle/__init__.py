@@ -46,6 +46,12 @@ def lib() -> C.CDLL:
         L.oracle_builtin.argtypes = [C.c_int, _P, _P, _U32, _P]
         L.oracle_sample_texture.argtypes = [_P, _U32, _U32, _U32, C.c_int32, _P, _U32, _P]
         L.oracle_sample_texture.restype = None
+        L.oracle_render_f64.argtypes = [_P, _P, _P, _P, _U32, _U32, _U32, _U32, _U32, _U32, _P, C.c_int]
+        L.oracle_render_f64.restype = C.c_int
+        L.oracle_sample_env.argtypes = [_P, _P, _P, _P, _P, _U32, _P, _P]
+        L.oracle_sample_env.restype = C.c_int
+        L.oracle_sample_surface.argtypes = [_P, _P, C.c_float, C.c_float, _P, _P, _U32, _P, _P]
+        L.oracle_sample_surface.restype = C.c_int
         for name in ("oracle_render", "oracle_gbuffer", "oracle_trace_closest", "oracle_bsdf", "oracle_denoise",
                      "oracle_resample"):
             getattr(L, name).restype = C.c_int
@@ -85,6 +91,14 @@ def render(oscene: OracleScene, params: np.ndarray, first_frame: int, reps: int,
                                nthreads, _p(counters))
 
 
+def render_f64(oscene: OracleScene, params: np.ndarray, first_frame: int, reps: int, section,
+               acc8: np.ndarray, nthreads: int = 0) -> int:
+    """oracle_render with FP64 Welford accumulation into acc8 (H, W, 8) float64 (zeroed first)."""
+    sx, sy, sw, sh = section
+    assert acc8.dtype == np.float64 and acc8.flags.c_contiguous
+    return lib().oracle_render_f64(*oscene.args(), _p(params), first_frame, reps, sx, sy, sw, sh, _p(acc8), nthreads)
+
+
 def gbuffer(oscene: OracleScene, params: np.ndarray, section, gbuf: np.ndarray, out: np.ndarray,
             nthreads: int = 0) -> int:
     sx, sy, sw, sh = section
@@ -101,6 +115,28 @@ def trace_closest(oscene: OracleScene, rays: np.ndarray, nthreads: int = 0):
     nn = np.empty((n, 3), np.float32)
     lib().oracle_trace_closest(*oscene.args(), _p(rays), n, _p(o), _p(m), _p(pr), _p(t), _p(nn), nthreads)
     return o, m, pr, t, nn
+
+
+def sample_env(oscene: OracleScene, params: np.ndarray, u2: np.ndarray):
+    """sample_env_cdf of each random pair: (texel (n, 2) as x, y; pdf (n,))."""
+    u2 = np.ascontiguousarray(u2, np.float32).reshape(-1, 2)
+    n = u2.shape[0]
+    texel = np.empty((n, 2), np.uint32)
+    pdf = np.empty(n, np.float32)
+    lib().oracle_sample_env(*oscene.args(), _p(params), _p(u2), n, _p(texel), _p(pdf))
+    return texel, pdf
+
+
+def sample_surface(material144: np.ndarray, normal, roughness, metallic, albedo, V, rng_state: int):
+    """One sample_surface call in air: (continues, new direction (3,), throughput (3,))."""
+    d = np.empty(3, np.float32)
+    tp = np.empty(3, np.float32)
+    nrm = np.asarray(normal, np.float32)
+    alb = np.asarray(albedo, np.float32)
+    v = np.asarray(V, np.float32)
+    cont = lib().oracle_sample_surface(_p(material144), _p(nrm), roughness, metallic, _p(alb), _p(v),
+                                       rng_state & 0xFFFFFFFF, _p(d), _p(tp))
+    return bool(cont), d, tp
 
 
 def rng_stream(idx: int, sample_number: int, seed: int, n: int) -> np.ndarray:

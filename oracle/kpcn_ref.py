@@ -9,7 +9,11 @@ skip tensor's size, [upsampled, skip] concatenation, a 1x1 output convolution wh
 in turn at dilations 1, 2, 4 with clamp-to-edge neighbours, starting from the noisy colour, and
 the relative L2 loss sum((f - t)^2 / (t^2 + 0.01)) / (3 pixels).  Parameters use the flat
 layout of wgpt_kpcn_get_params (per layer W[cout][ky*3+kx][cin], then bias).  Inputs and
-weights can be rounded to bfloat16 first, as the GPU stores them.
+weights can be rounded to bfloat16 first, as the GPU stores them.  With `bf16_activations` the
+restatement also rounds where the GPU kernels store bfloat16 tensors: every post-ReLU layer
+output and every pooled tensor on the way forward, and the gradient flowing back into each of
+them; the output logits are kept in FP32 and their gradient is rounded to bfloat16 (the
+filter's backward pass stores it so).  Everything between those points stays float64.
 """
 from __future__ import annotations
 
@@ -24,6 +28,35 @@ def bf16_round(a: np.ndarray) -> np.ndarray:
     u = np.ascontiguousarray(a, np.float32).view(np.uint32)
     r = ((u >> 16) & 1) + 0x7FFF
     return (((u + r) >> 16) << 16).astype(np.uint32).view(np.float32)
+
+
+def _bf16_t(x: torch.Tensor) -> torch.Tensor:
+    """Round a float64 tensor to bfloat16 values (through float32, nearest even)."""
+    return torch.from_numpy(bf16_round(x.detach().numpy().astype(np.float32)).astype(np.float64))
+
+
+class _RoundBF16(torch.autograd.Function):
+    """Forward and backward values rounded to bfloat16, as stored by the GPU kernels."""
+
+    @staticmethod
+    def forward(ctx, x):
+        return _bf16_t(x)
+
+    @staticmethod
+    def backward(ctx, g):
+        return _bf16_t(g)
+
+
+class _RoundLogits(torch.autograd.Function):
+    """FP32 logits forward; bfloat16 logit gradients backward."""
+
+    @staticmethod
+    def forward(ctx, x):
+        return torch.from_numpy(x.detach().numpy().astype(np.float32).astype(np.float64))
+
+    @staticmethod
+    def backward(ctx, g):
+        return _bf16_t(g)
 
 
 def features(noisy: np.ndarray, gbuf: np.ndarray) -> np.ndarray:
@@ -55,8 +88,9 @@ def unpack(params: np.ndarray, round_bf16: bool):
 
 
 def forward_loss(params: np.ndarray, noisy: np.ndarray, gbuf: np.ndarray, target: np.ndarray,
-                 round_bf16: bool = True):
+                 round_bf16: bool = True, bf16_activations: bool = False):
     """Returns (loss tensor, filtered (H, W, 3) tensor, per-layer parameter tensors)."""
+    q = _RoundBF16.apply if bf16_activations else (lambda a: a)
     x = features(noisy, gbuf)
     if round_bf16:
         x = bf16_round(x)
@@ -68,10 +102,10 @@ def forward_loss(params: np.ndarray, noisy: np.ndarray, gbuf: np.ndarray, target
         w, b = P[name]
         pad = 1 if w.shape[-1] == 3 else 0
         y = F.conv2d(inp, w, b, padding=pad)
-        return F.relu(y) if relu else y
+        return q(F.relu(y)) if relu else y
 
     def pool(a):
-        return F.avg_pool2d(a, 2, 2, ceil_mode=True, count_include_pad=False)
+        return q(F.avg_pool2d(a, 2, 2, ceil_mode=True, count_include_pad=False))
 
     def up(a, like):
         return F.interpolate(a, scale_factor=2, mode="nearest")[..., :like.shape[-2], :like.shape[-1]]
@@ -85,7 +119,10 @@ def forward_loss(params: np.ndarray, noisy: np.ndarray, gbuf: np.ndarray, target
     d2 = conv("D2", torch.cat([up(d3, e2), e2], 1))
     d1 = conv("D1", torch.cat([up(d2, e1), e1], 1))
     d0 = conv("D0", torch.cat([up(d1, e0), e0], 1))
-    logits = conv("OUT", d0, relu=False)[0]                  # (80, H, W)
+    logits = conv("OUT", d0, relu=False)
+    if bf16_activations:
+        logits = _RoundLogits.apply(logits)
+    logits = logits[0]                                         # (80, H, W)
     h, w = noisy.shape[:2]
     f = t(noisy[..., :3]).permute(2, 0, 1)                     # (3, H, W)
     for stage, d in enumerate((1, 2, 4)):
@@ -101,9 +138,10 @@ def forward_loss(params: np.ndarray, noisy: np.ndarray, gbuf: np.ndarray, target
     return loss, f.permute(1, 2, 0), P
 
 
-def loss_and_grads(params: np.ndarray, noisy, gbuf, target, round_bf16: bool = True):
+def loss_and_grads(params: np.ndarray, noisy, gbuf, target, round_bf16: bool = True,
+                   bf16_activations: bool = False):
     """(loss, flat gradient in the wgpt_kpcn layout, filtered (H, W, 3)) in float64."""
-    loss, f, P = forward_loss(params, noisy, gbuf, target, round_bf16)
+    loss, f, P = forward_loss(params, noisy, gbuf, target, round_bf16, bf16_activations)
     loss.backward()
     g = np.zeros(params.size, np.float64)
     sl = param_slices()

@@ -64,6 +64,7 @@ struct Ctx {
   uint32_t rng;
   uint64_t* cnt;   // per-thread counters or null
   int err;
+  double* acc64 = nullptr;   // per-pixel FP64 Welford records (8 doubles) or null
   inline void count(int k, uint64_t v = 1) { if (cnt) cnt[k] += v; }
 };
 
@@ -1812,6 +1813,17 @@ void main_pixel(Ctx& c, uint32_t ix, uint32_t iy, float* accum, uint8_t* out) {
     if (rand_pcg(c.rng) > survival_prob) break;
     throughput = throughput / survival_prob;
   }
+  if (c.acc64) {   // FP64 Welford record of every sample: mean rgb, M2 rgb, count
+    double* w = c.acc64 + (size_t)idx * 8;
+    const double n = w[6] + 1.0;
+    const double x[3] = {radiance.x, radiance.y, radiance.z};
+    for (int k = 0; k < 3; ++k) {
+      const double d = x[k] - w[k];
+      w[k] += d / n;
+      w[3 + k] += d * (x[k] - w[k]);
+    }
+    w[6] = n;
+  }
   float weight = 1.0f / (float)(p->sample_number + 1u);
   float* a = accum + (size_t)idx * 4;
   v3 old_c = mk3(a[0], a[1], a[2]);
@@ -1968,6 +1980,44 @@ int oracle_render(const void* const* bufs, const uint64_t* sizes, const uint32_t
   return err ? 2 : 0;
 }
 
+// oracle_render with every sample also folded into a per-pixel FP64 Welford record (acc8: 8
+// doubles per pixel of the params' image: mean r g b, sum of squared deviations r g b, count,
+// unused; zero it before the first call).  The paths run in FP32 as in the reference; only the
+// accumulation over samples is FP64.  The FP32 running mean goes into a scratch image.
+int oracle_render_f64(const void* const* bufs, const uint64_t* sizes, const uint32_t* meta,
+                      const void* params112, uint32_t first_frame, uint32_t reps,
+                      uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh, double* acc8, int nthreads) {
+  Scene s; fill_scene(&s, bufs, sizes, meta);
+  wgpt_scene_params p0; memcpy(&p0, params112, sizeof(p0));
+  if (sx + sw > p0.width || sy + sh > p0.height) return 1;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+  std::vector<float> accum((size_t)p0.width * p0.height * 4, 0.0f);
+  std::vector<uint8_t> out((size_t)p0.width * p0.height * 4, 0);
+  int err = 0;
+  const long long npix = (long long)sw * sh;
+#pragma omp parallel reduction(| : err)
+  {
+    // pixels are split over the threads and each thread runs all samples of its pixels, so
+    // every Welford record is updated by one thread in sample order
+#pragma omp for schedule(dynamic, 4)
+    for (long long k = 0; k < npix; ++k) {
+      uint32_t ix = sx + (uint32_t)(k % sw), iy = sy + (uint32_t)(k / sw);
+      for (uint32_t r = 0; r < reps; ++r) {
+        wgpt_scene_params p = p0;
+        p.sample_number = first_frame + r;
+        Ctx c; c.s = &s; c.p = &p; c.rng = 0; c.cnt = nullptr; c.err = 0; c.acc64 = acc8;
+        main_pixel(c, ix, iy, accum.data(), out.data());
+        err |= c.err;
+      }
+    }
+  }
+  return err ? 2 : 0;
+}
+
 // One dispatch of gbuf_main.  gbuf receives 12 floats (48 bytes) per pixel.
 int oracle_gbuffer(const void* const* bufs, const uint64_t* sizes, const uint32_t* meta,
                    const void* params112, uint32_t sx, uint32_t sy, uint32_t sw, uint32_t sh,
@@ -2040,6 +2090,51 @@ int oracle_bsdf(const void* material144, const float* normal3, float roughness, 
     pdf_out[i] = pdf_surface(V, L, mat, ctx, &st);
   }
   return 0;
+}
+
+// Environment samples (sample_env_cdf, shader.wgsl:231-254) of n random pairs: the texel the two
+// CDF searches pick, as (x, y), and the sample's pdf.  params: the 112-byte SceneParams.
+int oracle_sample_env(const void* const* bufs, const uint64_t* sizes, const uint32_t* meta, const void* params112,
+                      const float* u2, uint32_t n, uint32_t* texel_xy, float* pdf) {
+  Scene s; fill_scene(&s, bufs, sizes, meta);
+  wgpt_scene_params p; memcpy(&p, params112, sizeof(p));
+  for (uint32_t i = 0; i < n; ++i) {
+    Ctx c; c.s = &s; c.p = &p; c.rng = 0; c.cnt = nullptr; c.err = 0;
+    const v2 u = mk2(u2[2 * i], u2[2 * i + 1]);
+    const uint32_t v_idx = binary_search_cdf(c, 0u, p.sky_height, u.y);
+    const uint32_t u_idx = binary_search_cdf(c, p.sky_cdf_index + v_idx * (p.sky_width + 1u), p.sky_width, u.x);
+    texel_xy[2 * i] = u_idx;
+    texel_xy[2 * i + 1] = v_idx;
+    pdf[i] = sample_env_cdf(c, u).pdf;
+  }
+  return 0;
+}
+
+// One call of sample_surface (shader.wgsl:2052-2175) for a ray arriving along -V at a surface
+// with the given normal, material and context, in air with an empty medium stack, the random
+// stream starting at `rng_state`.  Writes the new ray direction, the throughput it carries
+// (starting from 1) and the return value (1 = the path continues).
+int oracle_sample_surface(const void* material144, const float* normal3, float roughness, float metallic,
+                          const float* albedo3, const float* V3, uint32_t rng_state, float* dir_out,
+                          float* throughput_out) {
+  wgpt_material mat; memcpy(&mat, material144, sizeof(mat));
+  SurfaceContext ctx;
+  ctx.normal = mk3(normal3[0], normal3[1], normal3[2]);
+  ctx.surface_normal = ctx.normal;
+  ctx.albedo = mk3(albedo3[0], albedo3[1], albedo3[2]);
+  ctx.roughness = roughness; ctx.metallic = metallic;
+  ctx.emittance = L3(mat.emittance); ctx.alpha = 1.0f;
+  MediumStack st; st.count = 0;
+  Scene s; memset(&s, 0, sizeof(s));
+  wgpt_scene_params p; memset(&p, 0, sizeof(p));
+  Ctx c; c.s = &s; c.p = &p; c.rng = rng_state; c.cnt = nullptr; c.err = 0;
+  Ray ray; ray.origin = mk3s(0.0f); ray.direction = -mk3(V3[0], V3[1], V3[2]);
+  v3 tp = mk3s(1.0f);
+  float last_pdf = 0.0f;
+  const bool cont = sample_surface(c, &ray, &tp, mk3s(0.0f), mat, ctx, &st, &last_pdf);
+  dir_out[0] = ray.direction.x; dir_out[1] = ray.direction.y; dir_out[2] = ray.direction.z;
+  throughput_out[0] = tp.x; throughput_out[1] = tp.y; throughput_out[2] = tp.z;
+  return cont ? 1 : 0;
 }
 
 // The PCG stream of one pixel (shader.wgsl:146-154, 2280-2282) after the seeding discard.

@@ -100,6 +100,37 @@ def test_kpcn_loss_and_gradients_match_fp64_reference(h, w):
     k.close()
 
 
+@pytest.mark.parametrize("h,w", [(40, 48), (33, 70)])
+def test_kpcn_gradients_match_bf16_rounding_reference(h, w):
+    """The same check against the restatement that rounds to bfloat16 where the kernels store
+    bfloat16 (post-ReLU activations, pooled tensors, the gradients flowing into them, logit
+    gradients): what remains is the kernels' FP32 accumulation order and the rounding points the
+    restatement places slightly differently (sums of two gradient contributions, upsampled
+    gradients), so the bound is a few percent instead of twenty."""
+    noisy, gbuf, target = _random_image(h, w, h * 1000 + w)
+    k = kpcn.Kpcn(0, seed=5)
+    p = k.get_params()
+    sl = kpcn.param_slices()
+    p[sl["OUT"][0]] *= 10.0
+    k.set_params(p)
+    loss_g, grad_g, out_g = k.loss_and_grads(noisy, gbuf, target)
+    loss_r, grad_r, out_r = kref.loss_and_grads(p, noisy, gbuf, target, bf16_activations=True)
+    assert abs(loss_g - loss_r) <= 2e-3 * abs(loss_r), (loss_g, loss_r)
+    np.testing.assert_allclose(out_g[..., :3], out_r, rtol=5e-3, atol=2e-3 * float(np.abs(out_r).max()))
+    report, worst = [], 0.0
+    for l in kpcn.LAYERS:
+        for part, s_ in zip(("W", "b"), sl[l.name]):
+            g, r = grad_g[s_].astype(np.float64), grad_r[s_]
+            nr = np.linalg.norm(r)
+            cos = float(g @ r / (np.linalg.norm(g) * nr + 1e-30))
+            rel = float(np.linalg.norm(g - r) / nr)
+            worst = max(worst, rel)
+            report.append(f"{l.name}.{part} cos {cos:.5f} rel {rel:.4f}")
+            assert cos > 0.999 and rel < 0.05, f"{l.name}.{part}: cosine {cos:.5f}, relative error {rel:.4f}"
+    print(f"worst {worst:.4f}: " + "; ".join(report))
+    k.close()
+
+
 def _example(seed, size, spp, target_spp):
     s = synth.small_scene(seed, size, size, 4)
     return kpcn.render_example(s, size, spp, target_spp, seed=seed, target_seed=10_000 + seed)

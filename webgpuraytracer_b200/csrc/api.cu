@@ -913,6 +913,43 @@ int wgpt_trace_rays(wgpt_ctx* ctx, const float* rays, uint32_t n, int32_t* o_idx
   return wgpt_synchronize(ctx);
 }
 
+int wgpt_sample_env(wgpt_ctx* ctx, const float* u2, uint32_t n, uint32_t* texel_xy, float* pdf) {
+  if (!ctx || !u2 || !texel_xy || !pdf) return WGPT_E_INVALID;
+  if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
+  if (!ctx->has_params) return fail(ctx, WGPT_E_STATE, "no scene params: call wgpt_set_params first");
+  if (!(ctx->ds.flags & WGPT_HAS_SKYBOX) || !(ctx->ds.flags & WGPT_MIS_SKYBOX))
+    return fail(ctx, WGPT_E_STATE, "the uploaded scene has no importance-sampled sky");
+  int rc = check_env(ctx, ctx->params);
+  if (rc) return rc;
+  if (n == 0) return WGPT_OK;
+  if (n > (1u << 24)) return fail(ctx, WGPT_E_INVALID, "at most 2^24 samples per call");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  void* d = nullptr;
+  CK(cudaMalloc(&d, (size_t)n * 16), "cudaMalloc env samples");
+  float* d_u = (float*)d;
+  uint32_t* d_t = (uint32_t*)(d_u + (size_t)n * 2);
+  float* d_p = (float*)(d_t + (size_t)n * 2);
+  cudaError_t e = cudaMemcpyAsync(d_u, u2, (size_t)n * 8, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = wgpt::launch_sample_env(ctx->ds, ctx->params, d_u, n, d_t, d_p, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(texel_xy, d_t, (size_t)n * 8, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(pdf, d_p, (size_t)n * 4, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "sample env");
+  return WGPT_OK;
+}
+
+int wgpt_rng_stream(int device, uint32_t idx, uint32_t sample_number, uint32_t seed, uint32_t n, float* out) {
+  if (!out || n == 0 || n > (1u << 20)) return WGPT_E_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return WGPT_E_CUDA;
+  float* d = nullptr;
+  if (cudaMalloc(&d, (size_t)n * 4) != cudaSuccess) return WGPT_E_NOMEM;
+  cudaError_t e = wgpt::launch_rng_stream(idx, sample_number, seed, n, d, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(out, d, (size_t)n * 4, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e == cudaSuccess ? WGPT_OK : WGPT_E_CUDA;
+}
+
 int wgpt_set_render_mode(wgpt_ctx* ctx, int mode) {
   if (!ctx) return WGPT_E_INVALID;
   if (mode != WGPT_MODE_WAVEFRONT && mode != WGPT_MODE_MEGAKERNEL) return fail(ctx, WGPT_E_INVALID, "unknown render mode");

@@ -428,6 +428,31 @@ __global__ void k_trace_rays(DScene s, const float* __restrict__ rays, uint32_t 
   if (ps.err) atomicOr(status, ps.err);
 }
 
+// Environment light samples of caller random pairs through sample_env_cdf (shader.wgsl:231-254):
+// the chosen texel (x, y) and the sample's pdf, for known-answer tests of the CDF search.
+__global__ void k_sample_env(DScene s, DParams p, const float* __restrict__ u2, uint32_t n, uint32_t* texel,
+                             float* pdf) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Counters<false> cn;
+  const float ux = u2[2 * i], uy = u2[2 * i + 1];
+  // the two searches sample_env_cdf makes, for the texel indices it turns into a direction
+  const uint32_t v_idx = binary_search_cdf(s, 0u, p.sky_height, uy, cn);
+  const uint32_t u_idx = binary_search_cdf(s, p.sky_cdf_index + v_idx * (p.sky_width + 1u), p.sky_width, ux, cn);
+  texel[2 * i] = u_idx;
+  texel[2 * i + 1] = v_idx;
+  pdf[i] = sample_env_cdf(s, p, ux, uy, cn).pdf;
+}
+
+// The per-pixel random stream of main (shader.wgsl:146-154, seeding 2280-2282): draws 1..n after
+// the discarded first one.
+__global__ void k_rng_stream(uint32_t idx, uint32_t sample_number, uint32_t seed, uint32_t n, float* out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  uint32_t st = (idx * 1973u + sample_number * 9277u + seed * 26699u) | 1u;
+  rand_pcg(st);
+  for (uint32_t i = 0; i < n; ++i) out[i] = rand_pcg(st);
+}
+
 }  // namespace pt
 
 using namespace pt;
@@ -500,6 +525,20 @@ cudaError_t launch_trace_rays(const DeviceScene& d, const float* rays, uint32_t 
                               int32_t* prim, float* t, float* normal, uint32_t* status, cudaStream_t st) {
   DScene s = to_dscene(d);
   k_trace_rays<<<(n + 127) / 128, 128, 0, st>>>(s, rays, n, o_idx, m_idx, prim, t, normal, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sample_env(const DeviceScene& d, const wgpt_scene_params& q, const float* u2, uint32_t n,
+                              uint32_t* texel, float* pdf, cudaStream_t st) {
+  DScene s = to_dscene(d);
+  DParams p = to_dparams(q, 0, 0);
+  k_sample_env<<<(n + 127) / 128, 128, 0, st>>>(s, p, u2, n, texel, pdf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rng_stream(uint32_t idx, uint32_t sample_number, uint32_t seed, uint32_t n, float* out,
+                              cudaStream_t st) {
+  k_rng_stream<<<1, 32, 0, st>>>(idx, sample_number, seed, n, out);
   return cudaGetLastError();
 }
 

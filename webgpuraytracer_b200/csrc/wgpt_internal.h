@@ -97,6 +97,10 @@ cudaError_t launch_gbuffer(const DeviceScene& d, const wgpt_scene_params& q, uin
                            cudaStream_t st);
 cudaError_t launch_trace_rays(const DeviceScene& d, const float* rays, uint32_t n, int32_t* o_idx, int32_t* m_idx,
                               int32_t* prim, float* t, float* normal, uint32_t* status, cudaStream_t st);
+cudaError_t launch_sample_env(const DeviceScene& d, const wgpt_scene_params& q, const float* u2, uint32_t n,
+                              uint32_t* texel, float* pdf, cudaStream_t st);
+cudaError_t launch_rng_stream(uint32_t idx, uint32_t sample_number, uint32_t seed, uint32_t n, float* out,
+                              cudaStream_t st);
 cudaError_t launch_denoise(const float* color, const float* gbuf, const wgpt_denoise_uniforms& u,
                            const uint32_t* steps, uint32_t passes, float* buf_a, float* buf_b, float* guide,
                            float* composited, uint8_t* out, const float** final_buf, cudaStream_t st);

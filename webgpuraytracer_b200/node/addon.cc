@@ -1155,6 +1155,36 @@ EXPORT(SelftestWait) {
   )
 }
 
+// sampleEnv(ctx, u2 Float32Array n x 2) -> {texel Uint32Array n x 2, pdf Float32Array}
+EXPORT(SampleEnv) {
+  BODY(
+    CtxBox* b = ctx_box(env, a.at(0));
+    View u = typed_of(env, a.at(1), napi_float32_array, 0, "u2");
+    uint32_t n = (uint32_t)(u.length / 2);
+    void *t, *p;
+    napi_value tv = new_typed(env, napi_uint32_array, (size_t)n * 2, &t);
+    napi_value pv = new_typed(env, napi_float32_array, n, &p);
+    check(wgpt_sample_env(b->ctx, static_cast<const float*>(u.data), n, static_cast<uint32_t*>(t), static_cast<float*>(p)),
+          b->ctx, "sampleEnv");
+    napi_value o;
+    napi_create_object(env, &o);
+    set(env, o, "texel", tv);
+    set(env, o, "pdf", pv);
+    return o;
+  )
+}
+
+// rngStream(device, idx, sampleNumber, seed, n) -> Float32Array of main's random draws
+EXPORT(RngStream) {
+  BODY(
+    uint32_t n = a.u32(4);
+    void* d;
+    napi_value dv = new_typed(env, napi_float32_array, n, &d);
+    check(wgpt_rng_stream(a.i32(0), a.u32(1), a.u32(2), a.u32(3), n, static_cast<float*>(d)), nullptr, "rngStream");
+    return dv;
+  )
+}
+
 // probeL2Read(device, bytes, reps) -> GB/s
 EXPORT(ProbeL2Read) {
   BODY(
@@ -1191,7 +1221,7 @@ napi_value Init(napi_env env, napi_value exports) {
       FN("kpcnDenoiseView", KpcnDenoiseView), FN("gemmBf16", GemmBf16), FN("buildBlas", BuildBlas),
       FN("buildTlas", BuildTlas), FN("buildEnvCdf", BuildEnvCdf), FN("buildEnvAlias", BuildEnvAlias),
       FN("decodeRgbe", DecodeRgbe), FN("parseObj", ParseObj), FN("selftestWait", SelftestWait),
-      FN("probeL2Read", ProbeL2Read),
+      FN("probeL2Read", ProbeL2Read), FN("sampleEnv", SampleEnv), FN("rngStream", RngStream),
   };
 #undef FN
   napi_define_properties(env, exports, sizeof props / sizeof props[0], props);

@@ -400,6 +400,86 @@ def time_to_rmse(args) -> dict:
     return out
 
 
+# FP32 operations per counted unit for the small configuration's ALU roofline (the constants
+# are the operation counts of the restated routines, rounded): slab test of one child box 12,
+# Moller-Trumbore 27, one analytic primitive (ray transform + quadric) 40, one shading event
+# (lobe probabilities, sampling, eval and pdf of the Disney BSDF, NEE set-up) 300, one CDF probe 2.
+FLOPS_PER_UNIT = {4: 12, 5: 27, 6: 40, 7: 300, 9: 2}
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 148 SMs x 128 FP32 lanes x FMA x 1965 MHz
+
+
+def small_config(steps: int = 20, warmup: int = 3) -> dict:
+    """The small configuration (256x256, 16 spp, 4 bounces, 8 analytic primitives, constant sky)
+    on the GPU: paths/s over whole 16-spp calls and the FP32 SIMT rate of the counted work
+    against the FP32 peak.  Inputs stay resident; each step is one render call."""
+    import torch
+    from webgpuraytracer_b200 import renderer as rd
+    from webgpuraytracer_b200 import scene as sc
+    from webgpuraytracer_b200 import synth
+    w = h = 256
+    spp = 16
+    s = synth.small_scene(1, w, h, 4)
+    packed = sc.pack_scene_data(s)
+    r = rd.Renderer(w, h, seed_fn=lambda: 1)
+    r.set_scene(s, packed=packed)
+    s.camera.update_rays2()
+    st = torch.cuda.ExternalStream(r.stream_handle())
+
+    def launch(i):
+        p_ = sc.pack_params(s, packed, w, h, i * spp, 1)
+        r._check(r.L.wgpt_set_params(r.ctx, rd.ptr(p_)), "params")
+        r._check(r.L.wgpt_render(r.ctx, i * spp, spp, 0, 0, w, h), "render")
+
+    for i in range(warmup):
+        launch(i)
+    r.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for i in range(steps):
+        launch(warmup + i)
+    e1.record(st)
+    r.synchronize()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    r.set_counting(True)
+    launch(warmup)
+    cnt = r.read_counters()
+    r.set_counting(False)
+    r.close()
+    flops = float(sum(int(cnt[k]) * f for k, f in FLOPS_PER_UNIT.items()))
+    tf = flops * steps / sec / 1e12
+    return {"workload": "small 256x256, 16 spp, 4 bounces, 8 primitives, constant sky (one render call per step)",
+            "paths_per_s": w * h * spp * steps / sec, "ms_per_step": sec / steps * 1e3,
+            "rays_per_s": float(cnt[1] + cnt[2]) * steps / sec,
+            "fp32_roofline": {"bound": "fp32 simt", "achieved": tf, "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
+                              "frac": tf / FP32_PEAK_TFLOPS, "flops_per_step": flops,
+                              "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 (FMA) x 1965 MHz; the kernels "
+                                             "are built without multiply-add contraction, so 0.5 is their ceiling"}}
+
+
+def cpu_atrous_baseline(passes: int = 5) -> dict:
+    """The a-trous configuration (1920x1080, 5 passes, the Denoiser defaults) through the CPU
+    restatement of denoiser.wgsl on every host core: ms per frame."""
+    import oracle
+    from webgpuraytracer_b200 import renderer as rd
+    rng = np.random.default_rng(1)
+    w, h = WIDTH, HEIGHT
+    color = (np.abs(rng.standard_normal((h, w, 4))) * 0.5).astype(np.float32)
+    gbuf = rng.standard_normal((h, w, 12)).astype(np.float32)
+    gbuf[..., 11] = np.abs(gbuf[..., 11]) * 5.0
+    u = rd.denoise_uniforms(w, h, passes=passes)
+    steps = rd.step_schedule(passes, "intended")
+    threads = os.cpu_count() or 1
+    oracle.denoise(color, gbuf, u, steps, threads)
+    t0 = time.perf_counter()
+    reps = 2
+    for _ in range(reps):
+        oracle.denoise(color, gbuf, u, steps, threads)
+    ms = (time.perf_counter() - t0) / reps * 1e3
+    return {"ms_per_frame": ms, "cores": threads, "kind": "port",
+            "sample": f"{reps} frames of 1920x1080, {passes} passes (steps 1..16), seeded synthetic buffers"}
+
+
 def run_ours(args):
     rank, world, local = dist_setup(args.gpus)
     import torch
@@ -500,13 +580,25 @@ def run_ours(args):
                  "note": "opt-in O(1) alias-table sky sampling on the same steps; images agree statistically "
                          "with the CDF search, not bit for bit"}
 
-    cpu = None
+    r.close()          # the remaining measurements use their own contexts
+    del flush
+    torch.cuda.empty_cache()
+    cpu = cpu_atrous = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, sample = cpu_sample(scene, packed, 1, args.cpu_seconds, 8)
         cpu = {"value": v, "unit": "paths/s", "cores": cores, "kind": "port", "sample": sample}
+        cpu_atrous = cpu_atrous_baseline()
     ttr = None
     if rank == 0 and world == 1 and not args.no_rmse and not mega:
         ttr = time_to_rmse(args)
+    small = batch = None
+    if rank == 0 and world == 1 and not args.no_extras and not mega:
+        small = small_config()
+        b = batch_measure(args, 0, 1, local, steps=2, warmup=3)
+        batch = {k_: b[k_] for k_ in ("value", "unit", "ms_per_step", "view_done_ms", "view_finished_ms", "e2e",
+                                      "rays_per_s", "autotune_table_ms")}
+        batch["config"] = b["config"]
+        batch["metric"] = b["metric"]
 
     if rank == 0:
         line = {
@@ -548,10 +640,15 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if cpu_atrous:
+            line["cpu_atrous_baseline"] = cpu_atrous
         if ttr:
             line["time_to_rmse"] = ttr
+        if small:
+            line["small_config"] = small
+        if batch:
+            line["batch"] = batch
         print(json.dumps(line), flush=True)
-    r.close()
     from webgpuraytracer_b200 import replicas
     replicas.teardown(world)
     return 0
@@ -592,6 +689,16 @@ def run_batch(args):
     p50/p99 of the per-view completion times (device clock from the start of the call's work to
     the view's last sample) and of the finished times (denoised image ready)."""
     rank, world, local = dist_setup(args.gpus)
+    line = batch_measure(args, rank, world, local, args.steps, args.warmup)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    from webgpuraytracer_b200 import replicas
+    replicas.teardown(world)
+    return 0
+
+
+def batch_measure(args, rank: int, world: int, local: int, steps: int, warmup: int) -> dict | None:
+    """The batched-views measurement of run_batch; returns rank 0's line (None elsewhere)."""
     import torch
     from webgpuraytracer_b200 import autotune
     from webgpuraytracer_b200 import kpcn
@@ -637,21 +744,21 @@ def run_batch(args):
     for i in range(len(views)):      # first use loads the network's kernels and sizes its buffers
         net.denoise_view(r, i)
 
-    for i in range(args.warmup):
+    for i in range(warmup):
         launch(i)
     r.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     sampler = ClockSampler(local)
     barrier(world)
     torch.cuda.synchronize()
     sampler.start()
     time.sleep(0.3)
-    for i in range(args.steps):
+    for i in range(steps):
         with torch.cuda.stream(stream):
             flush.fill_(float(i))
             starts[i].record(stream)
-        launch(args.warmup + i)
+        launch(warmup + i)
         with torch.cuda.stream(stream):
             ends[i].record(stream)
     r.synchronize()
@@ -660,13 +767,13 @@ def run_batch(args):
     clocks = sampler.stop()
     dev_s = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)) / 1e3
     dev_s_max = max_over_ranks(dev_s, world)
-    value = paths_all * args.steps / dev_s_max
+    value = paths_all * steps / dev_s_max
     # per-view completion (device stamps) and finishing by the learned denoiser, views in the
     # order their samples completed
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    done = launch(args.warmup + args.steps, timing=True)
+    done = launch(warmup + steps, timing=True)
     e1.record(stream)
     torch.cuda.synchronize()
     call_ms = e0.elapsed_time(e1)
@@ -684,16 +791,16 @@ def run_batch(args):
     fin_all = replicas.gather_lists(finished, world)
     # end-to-end: params in, every view traced, denoised and read back as rgba8, every step
     outs = [np.empty((v["height"], v["width"], 4), np.uint8) for v in views]
-    e2e_steps = max(1, min(args.steps, 4))
+    e2e_steps = max(1, min(steps, 4))
     barrier(world)
     t0 = time.perf_counter()
     for i in range(e2e_steps):
-        launch(args.warmup + args.steps + 1 + i)
+        launch(warmup + steps + 1 + i)
         for k_, o in enumerate(outs):
             net.denoise_view(r, k_)
             r._check(r.L.wgpt_read_view(r.ctx, k_, None, rd.ptr(o)), "read_view")
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    rep = stage_report(r, rd, lambda: launch(args.warmup), stream, flush, paths_mine, False)
+    rep = stage_report(r, rd, lambda: launch(warmup), stream, flush, paths_mine, False)
     upd = scene_update_ms(r, rd, sc, scene)
     peaks, peak_kind = load_peaks()
     cnt = rep["cnt"]
@@ -701,8 +808,8 @@ def run_batch(args):
     if rank == 0:
         line = {
             "metric": "paths/s, 32 batched views (uneven size and spp), 8 bounces", "value": value,
-            "unit": "paths/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dev_s_max / args.steps * 1e3, "higher_is_better": True, "scaling": "strong",
+            "unit": "paths/s", "n_gpus": world, "steps": steps, "warmup": warmup,
+            "ms_per_step": dev_s_max / steps * 1e3, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene and view generator)",
             "config": {"workload": "batched views: 32 views of 16 instances x 327,680-tri BLAS + 64 prims, "
                                    "2048x1024 RGBE env; sizes {256^2, 512^2, 1280x720, 1920x1080}, spp {4,16,64}",
@@ -716,13 +823,13 @@ def run_batch(args):
             "view_finished_ms": {"p50": float(np.percentile(fin_all, 50)), "p99": float(np.percentile(fin_all, 99)),
                                  "max": float(np.max(fin_all)),
                                  "note": "render call end + learned-denoiser passes in completion order"},
-            "rays_per_s": rays_all * args.steps / dev_s_max,
+            "rays_per_s": rays_all * steps / dev_s_max,
             "scene_update_ms": upd,
             "e2e": {"value": paths_all * e2e_steps / e2e_s, "unit": "paths/s",
                     "h2d_bytes_per_step": 112 * len(all_views),
                     "d2h_bytes_per_step": sum(v["width"] * v["height"] * 4 for v in all_views),
                     "includes": "render, learned denoiser per view, rgba8 readback"},
-            "gpu_launches": rep["launches"] * args.steps,
+            "gpu_launches": rep["launches"] * steps,
             "stages": rep["stages"],
             "roofline": {"bound": "hbm", "achieved": rep["achieved"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": rep["achieved"] / peaks["hbm_gbs"], "traffic": None,
@@ -730,11 +837,9 @@ def run_batch(args):
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
             "clocks": clocks,
         }
-        print(json.dumps(line), flush=True)
     net.close()
     r.close()
-    replicas.teardown(world)
-    return 0
+    return line if rank == 0 else None
 
 
 def run_denoise(args):
@@ -794,6 +899,8 @@ def main():
     ap.add_argument("--mode", choices=["wavefront", "megakernel"], default="wavefront")
     ap.add_argument("--pool", type=int, default=0, help="wavefront path slots (0: library default)")
     ap.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE measurement")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the small-configuration and batched-views measurements of the default line")
     ap.add_argument("--rmse-threshold", type=float, default=0.01)
     ap.add_argument("--ref-spp", type=int, default=65536, help="samples of the FP64 reference image")
     ap.add_argument("--max-spp", type=int, default=4096, help="largest sample count of the RMSE sweep")

@@ -159,6 +159,15 @@ int wgpt_render_gbuffer(wgpt_ctx* ctx, uint32_t sec_x, uint32_t sec_y, uint32_t 
    the context size; step_width and passes are taken from `steps`/`passes`). */
 int wgpt_denoise(wgpt_ctx* ctx, const void* uniforms_48, const uint32_t* steps, uint32_t passes);
 
+/* Arithmetic of the a-trous passes (no reference counterpart): WGPT_DENOISE_EXACT (default)
+   evaluates every tap's four exponential edge stops and the normal stop with the pinned FP32
+   built-ins in the reference's order, bit for bit like the CPU restatement; WGPT_DENOISE_FAST
+   uses one hardware exponential of the summed stop arguments, the hardware power and fused
+   multiply-adds, within 1e-5 relative of the exact result per pixel (the tolerance the
+   reference's filter is judged by) but not bit-exact.  Applies to wgpt_denoise on this context. */
+enum { WGPT_DENOISE_EXACT = 0, WGPT_DENOISE_FAST = 1 };
+int wgpt_set_denoise_mode(wgpt_ctx* ctx, int mode);
+
 /* renderPreview blit (tracer.js:2365-2389, scale.wgsl): bilinear resample of the output image
    (its top-left ratio_x/ratio_y part) into a dst_w x dst_h canvas image owned by the context. */
 int wgpt_resample(wgpt_ctx* ctx, uint32_t dst_w, uint32_t dst_h, float ratio_x, float ratio_y);

@@ -234,6 +234,36 @@ def test_denoise_1080p_config(small):
     r.close()
 
 
+@pytest.mark.parametrize("mode", ["intended", "as_run"])
+def test_denoise_fast_mode_within_1e5(small, mode):
+    """WGPT_DENOISE_FAST (hardware exponential and power, fused multiply-adds): not bit-exact,
+    but every filtered value within 1e-5 relative of the restatement at 1920x1080, 5 passes
+    (values below 1e-3, where a relative bar measures nothing, within 1e-8 absolute)."""
+    scene, packed = small
+    w, h = 1920, 1080
+    scene.camera.aspect = w / h
+    r = _renderer(scene, packed, w, h, gbuf=True)
+    r.render_gbuffer()
+    r.render(tsize=1024, reps=4)
+    color, gbuf = r.read_accum(), r.read_gbuffer()
+    u = rd.denoise_uniforms(w, h, passes=5)
+    steps = rd.step_schedule(5, mode)
+    f_o, c_o, o_o = oracle.denoise(color, gbuf, u, steps, oracle.default_threads())
+    r._check(r.L.wgpt_set_denoise_mode(r.ctx, 1), "denoise mode")
+    r._check(r.L.wgpt_denoise(r.ctx, rd.ptr(u), rd.ptr(steps), 5), "denoise")
+    r.synchronize()
+    f_g = np.empty_like(f_o)
+    c_g = np.empty_like(c_o)
+    r._check(r.L.wgpt_read_denoised(r.ctx, rd.ptr(f_g), rd.ptr(c_g)), "read_denoised")
+    big = np.abs(f_o) >= 1e-3
+    rel = np.abs(f_g - f_o)[big] / np.abs(f_o)[big]
+    print(f"fast a-trous: max rel {rel.max():.2e}, p99.9 {np.quantile(rel, 0.999):.2e}, "
+          f"rgba8 differing {(r.read_output() != o_o).mean():.2e}")
+    assert float(rel.max()) <= 1e-5
+    assert float(np.abs(f_g - f_o)[~big].max(initial=0.0)) <= 1e-8
+    r.close()
+
+
 def test_resample_bitexact(small):
     scene, packed = small
     scene.camera.aspect = 1.0

@@ -38,6 +38,7 @@ struct wgpt_ctx {
   float* dn_b = nullptr;
   float* dn_guide = nullptr;
   float* dn_comp = nullptr;
+  int dn_mode = WGPT_DENOISE_EXACT;
   const float* dn_final = nullptr;
   // preview canvas
   uint8_t* canvas = nullptr;
@@ -772,8 +773,15 @@ int wgpt_denoise(wgpt_ctx* ctx, const void* uniforms, const uint32_t* steps, uin
     CK(cudaMalloc(&ctx->dn_comp, npix * 16), "cudaMalloc denoise composite");
   }
   CK(wgpt::launch_denoise(ctx->accum, ctx->gbuf, u, steps, passes, ctx->dn_a, ctx->dn_b, ctx->dn_guide, ctx->dn_comp,
-                          ctx->out, &ctx->dn_final, ctx->stream),
+                          ctx->out, &ctx->dn_final, ctx->stream, ctx->dn_mode == WGPT_DENOISE_FAST),
      "denoise launch");
+  return WGPT_OK;
+}
+
+int wgpt_set_denoise_mode(wgpt_ctx* ctx, int mode) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (mode != WGPT_DENOISE_EXACT && mode != WGPT_DENOISE_FAST) return fail(ctx, WGPT_E_INVALID, "unknown denoise mode");
+  ctx->dn_mode = mode;
   return WGPT_OK;
 }
 

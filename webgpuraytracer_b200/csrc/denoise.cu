@@ -4,7 +4,8 @@
 //                a-trous pass reads instead of re-deriving it from the G-buffer 25 times;
 //   k_atrous     one 5x5 B3-spline a-trous pass with colour/normal/depth/albedo/material edge
 //                stops (denoiser.wgsl:117-189);
-//   k_composite  remodulation and the rgba8 store (denoiser.wgsl:194-213);
+//   k_composite  remodulation and the rgba8 store (denoiser.wgsl:194-213), fused into the last
+//                a-trous pass (a launch of its own only when there are no passes);
 //   k_resample   bilinear resample of an rgba8 image (scale.wgsl:6-35).
 // The guide record holds, per pixel, values the reference computes identically for every tap:
 // normal (3), normal length, depth mapped by d/(d+3), tonemapped albedo (3),
@@ -88,15 +89,49 @@ k_prepass(const float4* __restrict__ color, const float* __restrict__ gbuf, wgpt
   guide[idx * 3 + 0] = gp.a; guide[idx * 3 + 1] = gp.b; guide[idx * 3 + 2] = gp.c;
 }
 
+// One a-trous pass over a lattice tile.  The 25 taps of a pixel lie on the lattice of spacing
+// `step` through it, so a CTA takes the 16 x 16 pixels (rx + step*(16*tx + i), ry + step*(16*ty + j))
+// of one residue class (rx, ry) and stages the 20 x 20 lattice points they read (each clamped to
+// the image like the reference's taps) in shared memory once: colour and the three guide
+// vectors, 64 bytes a point, 25.6 KB a CTA.  Every tap then reads shared memory.  The per-tap
+// arithmetic and its order are denoiser.wgsl:117-189's, so results are bit-identical to a
+// direct gather.  FAST (opt-in, not bit-exact) evaluates the four exponential edge stops as one
+// hardware exponential of their summed arguments and the normal stop with the hardware power,
+// with fused multiply-adds; its results stay within 1e-5 relative of the exact ones.
+// With COMPOSITE the last pass also remodulates and stores the rgba8 image
+// (composite_main, denoiser.wgsl:194-213), which then needs no pass of its own.
+constexpr int kTile = 16, kApron = 2, kPts = kTile + 2 * kApron;   // 20 x 20 lattice points
+
+struct AtrousSmem {
+  float4 col[kPts * kPts];
+  float4 ga[kPts * kPts], gb[kPts * kPts], gc[kPts * kPts];
+};
+
+template <bool FAST, bool COMPOSITE>
 __global__ void __launch_bounds__(256)
 k_atrous(const float4* __restrict__ in, const float4* __restrict__ guide, wgpt_denoise_uniforms u, int step,
-         float4* __restrict__ out) {
-  int x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 16 + (threadIdx.x >> 4);
-  int W = (int)u.width, H = (int)u.height;
+         float4* __restrict__ out, float4* __restrict__ composited, uchar4* __restrict__ rgba) {
+  __shared__ AtrousSmem sm;
+  const int W = (int)u.width, H = (int)u.height;
+  const int rx = (int)(blockIdx.x % (unsigned)step), tx = (int)(blockIdx.x / (unsigned)step);
+  const int ry = (int)(blockIdx.y % (unsigned)step), ty = (int)(blockIdx.y / (unsigned)step);
+  const int lx0 = tx * kTile - kApron, ly0 = ty * kTile - kApron;   // first staged lattice index
+  for (int p = threadIdx.x; p < kPts * kPts; p += blockDim.x) {
+    const int px = p % kPts, py = p / kPts;
+    const int sx = min(max(rx + step * (lx0 + px), 0), W - 1);
+    const int sy = min(max(ry + step * (ly0 + py), 0), H - 1);
+    const size_t si = (size_t)sy * W + sx;
+    sm.col[p] = __ldg(in + si);
+    sm.ga[p] = __ldg(guide + si * 3);
+    sm.gb[p] = __ldg(guide + si * 3 + 1);
+    sm.gc[p] = __ldg(guide + si * 3 + 2);
+  }
+  __syncthreads();
+  const int i = (int)(threadIdx.x & 15), j = (int)(threadIdx.x >> 4);
+  const int x = rx + step * (tx * kTile + i), y = ry + step * (ty * kTile + j);
   if (x >= W || y >= H) return;
-  size_t ci = (size_t)y * W + x;
-  float4 cc = __ldg(in + ci);
-  float4 ga = __ldg(guide + ci * 3), gb = __ldg(guide + ci * 3 + 1), gc = __ldg(guide + ci * 3 + 2);
+  const int cp = (j + kApron) * kPts + (i + kApron);
+  const float4 cc = sm.col[cp], ga = sm.ga[cp], gb = sm.gb[cp], gc = sm.gc[cp];
   v3 c_n = mk3(ga.x, ga.y, ga.z);
   bool c_nflag = ga.w > 0.1f;
   float preserve = (1.0f - gc.y) * wmax(gc.z, gc.x);
@@ -104,34 +139,50 @@ k_atrous(const float4* __restrict__ in, const float4* __restrict__ guide, wgpt_d
   const float sc = u.sigma_color * u.sigma_color + 1e-5f;
   const float sd = u.sigma_depth * u.sigma_depth + 1e-5f;
   const float sa = u.sigma_albedo * u.sigma_albedo + 1e-5f;
-  const float sm = u.sigma_material * u.sigma_material + 1e-5f;
+  const float sm_ = u.sigma_material * u.sigma_material + 1e-5f;
+  const float inv_sc = __frcp_rn(sc), inv_sd = __frcp_rn(sd), inv_sa = __frcp_rn(sa), inv_sm = __frcp_rn(sm_);
   const float kern[5] = {0.0625f, 0.25f, 0.375f, 0.25f, 0.0625f};
   float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   float sum_w = 0.0f;
 #pragma unroll
   for (int dy = -2; dy <= 2; dy++) {
-    int sy = min(max(y + dy * step, 0), H - 1);
 #pragma unroll
     for (int dx = -2; dx <= 2; dx++) {
-      int sx = min(max(x + dx * step, 0), W - 1);
-      size_t si = (size_t)sy * W + sx;
-      float4 s = __ldg(in + si);
-      float4 sa4 = __ldg(guide + si * 3), sb4 = __ldg(guide + si * 3 + 1), sc4 = __ldg(guide + si * 3 + 2);
+      const int q = cp + dy * kPts + dx;
+      const float4 s = sm.col[q], sa4 = sm.ga[q], sb4 = sm.gb[q], sc4 = sm.gc[q];
       float h = kern[dx + 2] * kern[dy + 2];
-      v3 c_diff = mk3(cc.x, cc.y, cc.z) - mk3(s.x, s.y, s.z);
-      float w_color = exp_(-dot(c_diff, c_diff) / sc);
-      float w_normal = 1.0f;
-      if (c_nflag || sa4.w > 0.1f) {
-        float n_dot = wmax(0.0f, dot(c_n, mk3(sa4.x, sa4.y, sa4.z)));
-        w_normal = pow_(n_dot, u.sigma_normal);
+      float weight;
+      if (FAST) {
+        const float cx = cc.x - s.x, cy = cc.y - s.y, cz = cc.z - s.z;
+        const float dd = gb.x - sb4.x;
+        const float ax = gb.y - sb4.y, ay = gb.z - sb4.z, az = gb.w - sb4.w;
+        const float mx = gc.x - sc4.x, my = gc.y - sc4.y, mz = gc.z - sc4.z;
+        float e = __fmul_rn(__fmaf_rn(cx, cx, __fmaf_rn(cy, cy, cz * cz)), inv_sc);
+        e = __fmaf_rn(__fmul_rn(dd, dd), inv_sd, e);
+        e = __fmaf_rn(__fmaf_rn(ax, ax, __fmaf_rn(ay, ay, az * az)), inv_sa, e);
+        e = __fmaf_rn(__fmaf_rn(mx, mx, __fmaf_rn(my, my, mz * mz)), inv_sm, e);
+        float w_normal = 1.0f;
+        if (c_nflag || sa4.w > 0.1f) {
+          float n_dot = fmaxf(0.0f, __fmaf_rn(c_n.x, sa4.x, __fmaf_rn(c_n.y, sa4.y, c_n.z * sa4.z)));
+          w_normal = n_dot > 0.0f ? __powf(n_dot, u.sigma_normal) : (u.sigma_normal > 0.0f ? 0.0f : 1.0f);
+        }
+        weight = h * __expf(-e) * w_normal;
+      } else {
+        v3 c_diff = mk3(cc.x, cc.y, cc.z) - mk3(s.x, s.y, s.z);
+        float w_color = exp_(-dot(c_diff, c_diff) / sc);
+        float w_normal = 1.0f;
+        if (c_nflag || sa4.w > 0.1f) {
+          float n_dot = wmax(0.0f, dot(c_n, mk3(sa4.x, sa4.y, sa4.z)));
+          w_normal = pow_(n_dot, u.sigma_normal);
+        }
+        float d_diff = gb.x - sb4.x;
+        float w_depth = exp_(-(d_diff * d_diff) / sd);
+        v3 a_diff = mk3(gb.y, gb.z, gb.w) - mk3(sb4.y, sb4.z, sb4.w);
+        float w_albedo = exp_(-dot(a_diff, a_diff) / sa);
+        v3 m_diff = mk3(gc.x, gc.y, gc.z) - mk3(sc4.x, sc4.y, sc4.z);
+        float w_material = exp_(-dot(m_diff, m_diff) / sm_);
+        weight = h * w_color * w_normal * w_depth * w_albedo * w_material;
       }
-      float d_diff = gb.x - sb4.x;
-      float w_depth = exp_(-(d_diff * d_diff) / sd);
-      v3 a_diff = mk3(gb.y, gb.z, gb.w) - mk3(sb4.y, sb4.z, sb4.w);
-      float w_albedo = exp_(-dot(a_diff, a_diff) / sa);
-      v3 m_diff = mk3(gc.x, gc.y, gc.z) - mk3(sc4.x, sc4.y, sc4.z);
-      float w_material = exp_(-dot(m_diff, m_diff) / sm);
-      float weight = h * w_color * w_normal * w_depth * w_albedo * w_material;
       if (dx != 0 || dy != 0) weight *= attenuation;
       sum.x = sum.x + s.x * weight; sum.y = sum.y + s.y * weight;
       sum.z = sum.z + s.z * weight; sum.w = sum.w + s.w * weight;
@@ -139,7 +190,20 @@ k_atrous(const float4* __restrict__ in, const float4* __restrict__ guide, wgpt_d
     }
   }
   float d = sum_w + 1e-5f;
-  out[ci] = make_float4(sum.x / d, sum.y / d, sum.z / d, sum.w / d);
+  float4 c = make_float4(sum.x / d, sum.y / d, sum.z / d, sum.w / d);
+  const size_t ci = (size_t)y * W + x;
+  out[ci] = c;
+  if (COMPOSITE) {
+    // composite_main on this pass's result (the guide of the centre pixel is already staged)
+    bool is_sky = ga.w < 0.1f;
+    if ((u.flags & 2u) && !is_sky) {
+      v3 ma = vmax(mk3(gb.y, gb.z, gb.w), mk3s(0.001f));
+      c = make_float4(c.x * ma.x, c.y * ma.y, c.z * ma.z, c.w);
+    }
+    if (composited) composited[ci] = c;
+    rgba[ci] = make_uchar4((unsigned char)unorm8(c.x), (unsigned char)unorm8(c.y), (unsigned char)unorm8(c.z),
+                           (unsigned char)unorm8(c.w));
+  }
 }
 
 __global__ void __launch_bounds__(256)
@@ -190,16 +254,26 @@ static inline dim3 grid16(uint32_t w, uint32_t h) { return dim3((w + 15) / 16, (
 
 cudaError_t launch_denoise(const float* color, const float* gbuf, const wgpt_denoise_uniforms& u,
                            const uint32_t* steps, uint32_t passes, float* buf_a, float* buf_b, float* guide,
-                           float* composited, uint8_t* out, const float** final_buf, cudaStream_t st) {
+                           float* composited, uint8_t* out, const float** final_buf, cudaStream_t st,
+                           bool fast) {
   dim3 g = grid16(u.width, u.height);
   k_prepass<<<g, 256, 0, st>>>((const float4*)color, gbuf, u, (float4*)buf_a, (float4*)guide);
   float* in = buf_a;
   float* ob = buf_b;
   for (uint32_t i = 0; i < passes; ++i) {
-    k_atrous<<<g, 256, 0, st>>>((const float4*)in, (const float4*)guide, u, (int)steps[i], (float4*)ob);
+    const uint32_t step = steps[i];
+    // lattice tiles: per residue class, ceil(ceil(W / step) / 16) x ceil(ceil(H / step) / 16)
+    const uint32_t lw = (u.width + step - 1) / step, lh = (u.height + step - 1) / step;
+    dim3 ga(((lw + kTile - 1) / kTile) * step, ((lh + kTile - 1) / kTile) * step);
+    const bool last = i + 1 == passes;
+    auto kern = fast ? (last ? k_atrous<true, true> : k_atrous<true, false>)
+                     : (last ? k_atrous<false, true> : k_atrous<false, false>);
+    kern<<<ga, 256, 0, st>>>((const float4*)in, (const float4*)guide, u, (int)step, (float4*)ob,
+                             (float4*)composited, (uchar4*)out);
     float* t = in; in = ob; ob = t;
   }
-  k_composite<<<g, 256, 0, st>>>((const float4*)in, (const float4*)guide, u, (float4*)composited, (uchar4*)out);
+  if (passes == 0)
+    k_composite<<<g, 256, 0, st>>>((const float4*)in, (const float4*)guide, u, (float4*)composited, (uchar4*)out);
   if (final_buf) *final_buf = in;
   return cudaGetLastError();
 }

@@ -678,14 +678,142 @@ __global__ void k_weights_bf16(const float* __restrict__ wf, int cout, int taps,
   }
 }
 
-// Linear colour -> rgba8 with the accumulation pass's tonemap (shader.wgsl:2487-2490).
-__global__ void k_tonemap(const float4* __restrict__ c, int n, float exposure, uchar4* __restrict__ out) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float4 v = c[i];
-    float r = v.x * exposure, g = v.y * exposure, b = v.z * exposure;
-    r = powf(r / (r + 0.3f), 0.4545f); g = powf(g / (g + 0.3f), 0.4545f); b = powf(b / (b + 0.3f), 0.4545f);
-    auto u8 = [](float x) { return (unsigned char)floorf(fminf(fmaxf(x, 0.0f), 1.0f) * 255.0f + 0.5f); };
-    out[i] = make_uchar4(u8(r), u8(g), u8(b), 255);
+// ---------------------------------------------------------------------------- inference tail
+// Inference only.  The 1x1 output layer (32 -> 80 logits) runs on the tensor cores with the
+// three stages' softmax and the first filter stage in its epilogue, so the 80 FP32 logits of a
+// pixel never reach global memory: the epilogue writes the first stage's filtered colour and the
+// normalised 5x5 kernels of stages 2 and 3 (50 floats a pixel).  Two filter kernels apply those,
+// the last one also tonemapping into the rgba8 image.  Every value is computed with the training
+// forward's arithmetic (the same bias add, softmax and tap order), so the images are identical to
+// forward() followed by the tonemap.
+constexpr int WK23 = 50;
+
+template <int N>
+__device__ __forceinline__ void softmax_reg(const float (&lg)[80], int off, float (&wk)[N]) {
+  float mx = lg[off];
+#pragma unroll
+  for (int k = 1; k < N; ++k) mx = fmaxf(mx, lg[off + k]);
+  float sum = 0.0f;
+#pragma unroll
+  for (int k = 0; k < N; ++k) { wk[k] = __expf(lg[off + k] - mx); sum += wk[k]; }
+  const float inv = 1.0f / sum;
+#pragma unroll
+  for (int k = 0; k < N; ++k) wk[k] *= inv;
+}
+
+struct OutSmem {
+  static constexpr int A_BYTES = tc::BM * tc::BK * 2;    // 128 pixels x 64 K (32 used)
+  static constexpr int B_BYTES = LOGITS * tc::BK * 2;    // 80 logits x 64 K (32 used)
+  static constexpr int BYTES = A_BYTES + B_BYTES + 64;
+};
+
+// One CTA per 128 pixels.  d0: [P][32] BF16, wb: [80][32] BF16, bias: 80 floats.
+__global__ void __launch_bounds__(tc::THREADS)
+k_out_softmax(const uint16_t* __restrict__ d0, const uint16_t* __restrict__ wb, const float* __restrict__ bias,
+              const float4* __restrict__ col, float4* __restrict__ f1, float* __restrict__ wk23, int B, int h,
+              int w, uint32_t* err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int P = B * h * w;
+  const int p0 = blockIdx.x * tc::BM;
+  uint8_t* ta = smem;
+  uint8_t* tb = smem + OutSmem::A_BYTES;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + OutSmem::A_BYTES + OutSmem::B_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + OutSmem::A_BYTES + OutSmem::B_BYTES + 16);
+  volatile uint32_t* flag = reinterpret_cast<volatile uint32_t*>(smem + OutSmem::A_BYTES + OutSmem::B_BYTES + 20);
+  constexpr uint32_t NCOLS = tc::tmem_cols(LOGITS);
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(tmem_slot), NCOLS);
+  if (tid == 0) tc::mbar_init(tc::smem_u32(bar), 1);
+  // operand tiles: K chunks 0..3 (32 channels) of every row
+  for (int i = tid; i < tc::BM * 4; i += tc::THREADS) {
+    const int r = i % tc::BM, c = i / tc::BM, p = p0 + r;
+    tc::put_chunk(ta, r, c, p < P ? *reinterpret_cast<const uint4*>(d0 + (size_t)p * 32 + c * 8) : zero4());
+  }
+  for (int i = tid; i < LOGITS * 4; i += tc::THREADS) {
+    const int r = i % LOGITS, c = i / LOGITS;
+    tc::put_chunk(tb, r, c, *reinterpret_cast<const uint4*>(wb + (size_t)r * 32 + c * 8));
+  }
+  tc::fence_async_smem();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  if (tid == 0) {
+    constexpr uint32_t IDESC = tc::idesc_bf16(LOGITS);
+    const uint32_t a_addr = tc::smem_u32(ta), b_addr = tc::smem_u32(tb);
+#pragma unroll
+    for (int kk = 0; kk < 2; ++kk) {
+      const uint64_t da = tc::smem_desc(a_addr + kk * 256, 128, (tc::BK / 8) * 128);
+      const uint64_t db = tc::smem_desc(b_addr + kk * 256, 128, (tc::BK / 8) * 128);
+      tc::mma_bf16(tmem, da, db, IDESC, kk > 0 ? 1u : 0u);
+    }
+    tc::mma_commit(tc::smem_u32(bar));
+    *flag = tc::mbar_wait(tc::smem_u32(bar), 0u) ? 1u : 0u;
+  }
+  __syncthreads();
+  if (*flag == 0u) {
+    if (tid == 0) atomicOr(err, tc::ERR_TC_TIMEOUT);
+  } else {
+    tc::tc_fence_after();
+    float lg[80];
+#pragma unroll
+    for (int c0 = 0; c0 < 80; c0 += 16) {
+      float v[16];
+      tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) lg[c0 + i] = v[i] + bias[c0 + i];
+    }
+    const int p = p0 + warp * 32 + (tid & 31);
+    if (p < P) {
+      const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
+      float wk[25];
+      softmax_reg<25>(lg, 0, wk);
+      float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 25; ++k) {
+        float4 c = col[tap_index(b, y, x, k, 1, h, w)];
+        fx += wk[k] * c.x; fy += wk[k] * c.y; fz += wk[k] * c.z;
+      }
+      f1[p] = make_float4(fx, fy, fz, 1.0f);
+      float* dst = wk23 + (size_t)p * WK23;
+      softmax_reg<25>(lg, 25, wk);
+#pragma unroll
+      for (int k = 0; k < 25; ++k) dst[k] = wk[k];
+      softmax_reg<25>(lg, 50, wk);
+#pragma unroll
+      for (int k = 0; k < 25; ++k) dst[25 + k] = wk[k];
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_free(tmem, NCOLS);
+}
+
+// A filter stage with stored normalised kernels (25 floats at wk23 + p * 50 + off); with rgba the
+// result is also tonemapped into the rgba8 image with the accumulation pass's display transform
+// (shader.wgsl:2487-2490).
+__global__ void k_filter_stored(const float* __restrict__ wk23, int off, int d, const float4* __restrict__ in,
+                                float4* __restrict__ out, uchar4* __restrict__ rgba, float exposure, int B, int h,
+                                int w) {
+  const int P = B * h * w;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
+    const float* wk = wk23 + (size_t)p * WK23 + off;
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 25; ++k) {
+      const float wt = wk[k];
+      float4 c = in[tap_index(b, y, x, k, d, h, w)];
+      fx += wt * c.x; fy += wt * c.y; fz += wt * c.z;
+    }
+    const float4 v = make_float4(fx, fy, fz, 1.0f);
+    out[p] = v;
+    if (rgba) {
+      float rr = v.x * exposure, gg = v.y * exposure, bb = v.z * exposure;
+      rr = powf(rr / (rr + 0.3f), 0.4545f); gg = powf(gg / (gg + 0.3f), 0.4545f); bb = powf(bb / (bb + 0.3f), 0.4545f);
+      auto u8 = [](float t) { return (unsigned char)floorf(fminf(fmaxf(t, 0.0f), 1.0f) * 255.0f + 0.5f); };
+      rgba[p] = make_uchar4(u8(rr), u8(gg), u8(bb), 255);
+    }
   }
 }
 
@@ -876,7 +1004,9 @@ static cudaError_t conv_bwd(Net& n, const Layer& l, const uint16_t* dz, const ui
   return gemm_n(a, b, EpiStore{n.dx, cin}, P, cin, l.taps * l.cout, n.err, n.st);
 }
 
-static cudaError_t forward(Net& n) {
+// The network on the batch in n.x0 / n.col; with infer_rgba (inference) the fused output tail
+// also writes the tonemapped image there.
+static cudaError_t forward(Net& n, uchar4* infer_rgba = nullptr, float exposure = 1.0f) {
   cudaError_t e;
   const int B = n.B;
   auto pool = [&](const uint16_t* in, uint16_t* outp, int lv, int C) {
@@ -898,6 +1028,17 @@ static cudaError_t forward(Net& n) {
   if ((e = conv_fwd(n, n.L[L_D2], n.d3, n.e2, n.d2, false))) return e;
   if ((e = conv_fwd(n, n.L[L_D1], n.d2, n.e1, n.d1, false))) return e;
   if ((e = conv_fwd(n, n.L[L_D0], n.d1, n.e0, n.d0, false))) return e;
+  if (infer_rgba) {
+    // inference: output layer, softmax and stage 1 fused; stages 2 and 3 read the stored kernels
+    // (in the logits buffer, which inference does not otherwise use)
+    const int P0 = B * n.H * n.W;
+    const Layer& lo = n.L[L_OUT];
+    k_out_softmax<<<(P0 + tc::BM - 1) / tc::BM, tc::THREADS, OutSmem::BYTES, n.st>>>(
+        n.d0, lo.wb, n.w + lo.b_off, n.col, n.f1, n.logits, B, n.H, n.W, n.err);
+    k_filter_stored<<<grid1(P0), 256, 0, n.st>>>(n.logits, 0, 2, n.f1, n.f2, nullptr, exposure, B, n.H, n.W);
+    k_filter_stored<<<grid1(P0), 256, 0, n.st>>>(n.logits, 25, 4, n.f2, n.out, infer_rgba, exposure, B, n.H, n.W);
+    return cudaGetLastError();
+  }
   if ((e = conv_fwd(n, n.L[L_OUT], nullptr, n.d0, n.logits, true))) return e;
   const int P0 = B * n.H * n.W;
   k_filter_fwd<<<grid1(P0), 256, 0, n.st>>>(n.logits, 0, 1, n.col, n.f1, B, n.H, n.W);
@@ -1388,8 +1529,7 @@ static int denoise_image(wgpt_kpcn* k, wgpt_ctx* ctx, int view, float exposure, 
   KCK(cudaStreamWaitEvent(n.st, k->ev_in, 0), "event wait");
   kp::k_gather<<<kp::grid1(npix), 256, 0, n.st>>>((const float4*)im.accum, im.gbuf, nullptr, (int)im.h, (int)im.w,
                                                   k->d_crops, 1, (int)im.h, (int)im.w, n.x0, n.col, nullptr);
-  KCK(kp::forward(n), "forward");
-  kp::k_tonemap<<<kp::grid1(npix), 256, 0, n.st>>>(n.out, (int)npix, exposure, (uchar4*)im.out);
+  KCK(kp::forward(n, (uchar4*)im.out, exposure), "forward");
   KCK(cudaGetLastError(), "denoise launch");
   KCK(cudaEventRecord(k->ev_out, n.st), "event");
   KCK(cudaStreamWaitEvent(im.stream, k->ev_out, 0), "event wait");

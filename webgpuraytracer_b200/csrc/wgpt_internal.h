@@ -103,7 +103,8 @@ cudaError_t launch_rng_stream(uint32_t idx, uint32_t sample_number, uint32_t see
                               cudaStream_t st);
 cudaError_t launch_denoise(const float* color, const float* gbuf, const wgpt_denoise_uniforms& u,
                            const uint32_t* steps, uint32_t passes, float* buf_a, float* buf_b, float* guide,
-                           float* composited, uint8_t* out, const float** final_buf, cudaStream_t st);
+                           float* composited, uint8_t* out, const float** final_buf, cudaStream_t st,
+                           bool fast = false);
 cudaError_t launch_resample(const uint8_t* src, uint32_t sw, uint32_t sh, uint8_t* dst, uint32_t dw, uint32_t dh,
                             float rx, float ry, cudaStream_t st);
 

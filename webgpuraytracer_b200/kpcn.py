@@ -222,6 +222,72 @@ def build_training_set(k: Kpcn, seeds, size: int = 256, spps=(1, 2, 4, 8), targe
     return n
 
 
+def flagship_family_scene(seed: int, width: int = 1920, height: int = 1080, bounces: int = 8):
+    """A scene of the flagship family (seeded instances of the displaced icosphere, analytic
+    primitives and Disney materials under the importance-sampled sun sky) seen from a seeded
+    camera on a ring around it."""
+    import math
+    from . import synth
+    s = synth.flagship_scene(seed, width, height, bounces)
+    rnd = synth.mulberry32(seed * 92821 + 7)
+    ang = rnd() * 2.0 * math.pi
+    radius = 14.0 + 12.0 * rnd()
+    s.camera.position = sc.gm.vec3(radius * math.cos(ang), 2.0 + 8.0 * rnd(), radius * math.sin(ang))
+    s.camera.target = sc.gm.vec3(-3.0 + 6.0 * rnd(), 0.5 + 2.5 * rnd(), -3.0 + 6.0 * rnd())
+    return s
+
+
+def crop_origins(seed: int, n: int, width: int, height: int, size: int):
+    rnd = np.random.default_rng(seed)
+    return [(int(rnd.integers(0, width - size + 1)), int(rnd.integers(0, height - size + 1))) for _ in range(n)]
+
+
+def build_flagship_training_set(k: Kpcn, seeds, crops: int = 2, size: int = 256, spps=(1, 2, 4, 8),
+                                target_spp: int = 1024, bounces: int = 8, width: int = 1920, height: int = 1080,
+                                device: int = 0, pool_paths: int = 1 << 24) -> int:
+    """Training examples from the flagship family at the flagship's scale: for each seeded
+    scene, `crops` size x size windows of its width x height view are path traced (sections of
+    the full image, so objects keep their on-screen size) at every input sample count in
+    `spps` (progressively, seed = the scene seed) and at target_spp with an independent stream.
+    One renderer pair is reused for every scene.  Returns the number of examples added."""
+    tgt_r = rd.Renderer(width, height, device=device, seed_fn=lambda: 0)
+    in_r = rd.Renderer(width, height, device=device, seed_fn=lambda: 0)
+    tgt_r.set_wavefront_config(pool_paths, 0)
+    in_r.set_wavefront_config(pool_paths, 0)
+    n = 0
+    try:
+        for seed in seeds:
+            seed = int(seed)
+            s = flagship_family_scene(seed, width, height, bounces)
+            packed = sc.pack_scene_data(s)
+            wins = crop_origins(seed, crops, width, height, size)
+            tgt_r.seed_fn = lambda: 100_000 + seed
+            tgt_r.set_scene(s, packed=packed)
+            for (cx, cy) in wins:
+                tgt_r.render_section(0, target_spp, cx, cy, size, size)
+            tgt_r.synchronize()
+            target = tgt_r.read_accum()
+            in_r.seed_fn = lambda: seed
+            in_r.set_scene(s, isgbuf=True, packed=packed)
+            in_r.render_gbuffer()
+            gbuf = in_r.read_gbuffer()
+            done = 0
+            for spp in spps:
+                for (cx, cy) in wins:
+                    in_r.render_section(done, spp - done, cx, cy, size, size)
+                in_r.synchronize()
+                done = spp
+                acc = in_r.read_accum()
+                for (cx, cy) in wins:
+                    win = (slice(cy, cy + size), slice(cx, cx + size))
+                    k.add_example(acc[win], gbuf[win], target[win])
+                    n += 1
+    finally:
+        tgt_r.close()
+        in_r.close()
+    return n
+
+
 def gemm_flops(width: int, height: int) -> int:
     """Tensor-core FLOPs of one inference at width x height (padded channel counts, as executed)."""
     h, w = [height], [width]

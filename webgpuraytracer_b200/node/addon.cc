@@ -536,6 +536,11 @@ EXPORT(Denoise) {
   )
 }
 
+// setDenoiseMode(ctx, DENOISE_EXACT | DENOISE_FAST): arithmetic of the a-trous passes
+EXPORT(SetDenoiseMode) {
+  BODY(CtxBox* b = ctx_box(env, a.at(0)); check(wgpt_set_denoise_mode(b->ctx, a.i32(1)), b->ctx, "setDenoiseMode"); return undef(env);)
+}
+
 // renderPreview blit (tracer.js:2365-2389): resample(ctx, dstW, dstH, ratioX, ratioY)
 EXPORT(Resample) {
   BODY(
@@ -1205,7 +1210,7 @@ napi_value Init(napi_env env, napi_value exports) {
       FN("renderAsync", RenderAsync), FN("renderGBuffer", RenderGBuffer), FN("setRenderMode", SetRenderMode),
       FN("setEnvSampling", SetEnvSampling), FN("setAccumF64", SetAccumF64), FN("readAccumF64", ReadAccumF64),
       FN("writeAccumF64", WriteAccumF64), FN("setWavefrontConfig", SetWavefrontConfig),
-      FN("getWavefrontConfig", GetWavefrontConfig), FN("denoise", Denoise), FN("resample", Resample),
+      FN("getWavefrontConfig", GetWavefrontConfig), FN("denoise", Denoise), FN("setDenoiseMode", SetDenoiseMode), FN("resample", Resample),
       FN("synchronize", Synchronize), FN("synchronizeTimeout", SynchronizeTimeout),
       FN("synchronizeAsync", SynchronizeAsync), FN("readAccum", ReadAccum), FN("writeAccum", WriteAccum),
       FN("readOutput", ReadOutput), FN("readGBuffer", ReadGBuffer), FN("writeGBuffer", WriteGBuffer),
@@ -1230,6 +1235,8 @@ napi_value Init(napi_env env, napi_value exports) {
   set(env, exports, "MODE_MEGAKERNEL", make_u32(env, WGPT_MODE_MEGAKERNEL));
   set(env, exports, "ENV_CDF", make_u32(env, WGPT_ENV_CDF));
   set(env, exports, "ENV_ALIAS", make_u32(env, WGPT_ENV_ALIAS));
+  set(env, exports, "DENOISE_EXACT", make_u32(env, WGPT_DENOISE_EXACT));
+  set(env, exports, "DENOISE_FAST", make_u32(env, WGPT_DENOISE_FAST));
   set(env, exports, "NOALLOC_MAX_PIXELS", make_u32(env, WGPT_NOALLOC_MAX_PIXELS));
   return exports;
 }

@@ -247,6 +247,14 @@ int wgpt_kpcn_apply(wgpt_kpcn* k, const float* dev_grads, float scale, float lr)
 int wgpt_kpcn_loss_and_grads(wgpt_kpcn* k, const float* noisy_rgba32f, const void* gbuf_48B,
                              const float* target_rgba32f, uint32_t w, uint32_t h, float* loss, float* grads,
                              float* out_rgba32f);
+/* How the network's 3x3 convolutions run (same results up to FP32 summation order inside the
+   tensor cores): WGPT_KPCN_CONV_PIPELINED (default) is a persistent warp-specialised kernel --
+   TMA halo loads and bulk weight copies through a ring of shared-memory stages, one MMA warp,
+   double-buffered tensor-memory accumulators drained by four epilogue warps;
+   WGPT_KPCN_CONV_PER_TILE runs one CTA per 16 x 16 tile with all threads loading, then one
+   thread issuing the MMAs. */
+enum { WGPT_KPCN_CONV_PIPELINED = 0, WGPT_KPCN_CONV_PER_TILE = 1 };
+int wgpt_kpcn_set_conv_mode(wgpt_kpcn* k, int mode);
 int wgpt_kpcn_denoise(wgpt_kpcn* k, wgpt_ctx* ctx, float exposure, float* filtered_rgba32f);
 int wgpt_kpcn_denoise_view(wgpt_kpcn* k, wgpt_ctx* ctx, uint32_t view, float exposure, float* filtered_rgba32f);
 

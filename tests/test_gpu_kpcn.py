@@ -226,3 +226,49 @@ def test_kpcn_train_data_parallel_single_rank():
     losses = kpcn.train_data_parallel(k, 30, batch=4, crop=64, lr=2e-3, seed=1)
     assert np.isfinite(losses).all() and losses[-5:].mean() < losses[:5].mean()
     k.close()
+
+
+@pytest.mark.parametrize("h,w", [(40, 48), (33, 70), (96, 160)])
+def test_kpcn_pipelined_convolutions_equal_per_tile(h, w):
+    """The warp-specialised TMA convolution (default) against the one-CTA-per-tile kernel: the
+    same MMAs accumulate in the same order into tensor memory, so loss, filtered output and every
+    gradient are identical bit for bit (forward, data gradients and weight gradients)."""
+    noisy, gbuf, target = _random_image(h, w, h * 7 + w)
+    k = kpcn.Kpcn(0, seed=9)
+    p = k.get_params()
+    sl = kpcn.param_slices()
+    p[sl["OUT"][0]] *= 10.0
+    k.set_params(p)
+    L = _lib.lib()
+    res = []
+    for mode in (0, 1):
+        assert L.wgpt_kpcn_set_conv_mode(k.h, mode) == 0
+        res.append(k.loss_and_grads(noisy, gbuf, target))
+    (l0, g0, o0), (l1, g1, o1) = res
+    assert l0 == l1
+    np.testing.assert_array_equal(o0, o1)
+    np.testing.assert_array_equal(g0, g1)
+    k.close()
+
+
+def test_kpcn_pipelined_denoise_equals_per_tile():
+    """1080p inference through both convolution kernels gives the same image bit for bit."""
+    size_w, size_h = 1920, 1080
+    s = synth.small_scene(1, size_w, size_h, 4)
+    s.camera.aspect = size_w / size_h
+    r = rd.Renderer(size_w, size_h)
+    r.set_scene(s, isgbuf=True)
+    r.render_gbuffer()
+    r.reset()
+    r.render(tsize=size_w, reps=2)
+    k = kpcn.Kpcn(0, seed=4)
+    L = _lib.lib()
+    outs = []
+    for mode in (0, 1):
+        assert L.wgpt_kpcn_set_conv_mode(k.h, mode) == 0
+        lin = k.denoise(r)
+        outs.append((lin, r.read_output()))
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+    k.close()
+    r.close()

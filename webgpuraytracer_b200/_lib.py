@@ -94,6 +94,7 @@ EXPORTS = {
     "wgpt_probe_l2_read": ([C.c_int, C.c_uint64, _U32, C.POINTER(C.c_double)], C.c_int),
     "wgpt_sample_env": ([_P, _P, _U32, _P, _P], C.c_int),
     "wgpt_set_denoise_mode": ([_P, C.c_int], C.c_int),
+    "wgpt_kpcn_set_conv_mode": ([_P, C.c_int], C.c_int),
     "wgpt_rng_stream": ([C.c_int, _U32, _U32, _U32, _U32, _P], C.c_int),
     "wgpt_set_wavefront_config": ([_P, C.c_uint32, C.c_uint64], C.c_int),
     "wgpt_set_views": ([_P, C.c_uint32, _P, _P], C.c_int),

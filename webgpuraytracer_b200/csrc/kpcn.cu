@@ -7,6 +7,7 @@
 
 #include "../../include/wgpt.h"
 #include "tc_gemm.cuh"
+#include "conv_ws.cuh"
 
 namespace kp {
 
@@ -413,6 +414,91 @@ cudaError_t conv3x3(const HaloSrc& src, const uint16_t* wb, int cin, int N, int 
     case 96: return conv3x3_nt<96>(src, wb, cin, N, B, ep, err, st);
     case 112: return conv3x3_nt<112>(src, wb, cin, N, B, ep, err, st);
     default: return conv3x3_nt<128>(src, wb, cin, N, B, ep, err, st);
+  }
+}
+
+// Output-channel tile of the warp-specialised kernel for a convolution with N output channels
+// (the whole N up to 128, else 128-wide tiles), shared by the weight packing and the launches.
+__host__ __device__ inline int ws_nt(int N) {
+  return N <= 32 ? 32 : N <= 48 ? 48 : N <= 64 ? 64 : N <= 80 ? 80 : N <= 96 ? 96 : N <= 112 ? 112 : 128;
+}
+inline size_t ws_packed_elems(int N, int K) {
+  const int nt = ws_nt(N);
+  return (size_t)((N + nt - 1) / nt) * (K / 16) * 9 * nt * 16;
+}
+
+static int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  }
+  return n;
+}
+
+template <int NT, class EP>
+cudaError_t conv3x3_ws_nt(const HaloSrc& src, const uint16_t* wpk, int cin, int N, int B, const EP& ep, uint32_t* err,
+                          cudaStream_t st) {
+  // images smaller than the 18 x 18 halo box go to the per-tile kernel (the callers' fallback)
+  if (src.h < ws::HW || src.w < ws::HW) return cudaErrorNotSupported;
+  CUtensorMap map;
+  cudaError_t e = ws::make_halo_map(&map, src.s, src.cs, src.w, src.h, B);
+  if (e != cudaSuccess) return cudaErrorNotSupported;
+  auto kern = ws::k_conv3x3_ws<NT, EP>;
+  // at most two CTAs per SM when each takes 256 tensor-memory columns: ask for enough shared
+  // memory that a third cannot be resident (it would wait in tcgen05.alloc)
+  constexpr int smem = (ws::acc_cols(NT) == 256 && ws::smem_bytes(NT) < 78 * 1024) ? 78 * 1024 : ws::smem_bytes(NT);
+  static bool attr_set = false;
+  if (!attr_set) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  ws::ConvGeom g;
+  g.u = src.u; g.cu = src.cu; g.hc = src.hc; g.wc = src.wc; g.cs = src.cs;
+  g.h = src.h; g.w = src.w; g.B = B; g.cin = cin; g.N = N;
+  g.tiles_x = (src.w + 15) / 16; g.tiles_y = (src.h + 15) / 16; g.ntn = (N + NT - 1) / NT;
+  g.n_tiles = g.tiles_x * g.tiles_y * B * g.ntn;
+  const int per_sm = (ws::acc_cols(NT) <= 256 && 2 * smem <= 227 * 1024) ? 2 : 1;
+  const int grid = std::min(g.n_tiles, sm_count() * per_sm);
+  kern<<<grid, ws::THREADS, smem, st>>>(map, g, wpk, ep, err);
+  return cudaGetLastError();
+}
+
+template <class EP>
+cudaError_t conv3x3_ws(const HaloSrc& src, const uint16_t* wpk, int cin, int N, int B, const EP& ep, uint32_t* err,
+                       cudaStream_t st) {
+  switch (ws_nt(N)) {
+    case 32: return conv3x3_ws_nt<32>(src, wpk, cin, N, B, ep, err, st);
+    case 48: return conv3x3_ws_nt<48>(src, wpk, cin, N, B, ep, err, st);
+    case 64: return conv3x3_ws_nt<64>(src, wpk, cin, N, B, ep, err, st);
+    case 80: return conv3x3_ws_nt<80>(src, wpk, cin, N, B, ep, err, st);
+    case 96: return conv3x3_ws_nt<96>(src, wpk, cin, N, B, ep, err, st);
+    case 112: return conv3x3_ws_nt<112>(src, wpk, cin, N, B, ep, err, st);
+    default: return conv3x3_ws_nt<128>(src, wpk, cin, N, B, ep, err, st);
+  }
+}
+
+// Weights [N][9][K] (BF16) -> the warp-specialised kernel's blocks: per N tile and 16-channel
+// chunk, 9 taps x NT rows x 16 channels in the shared-memory core-matrix layout (zeros for rows
+// beyond N).
+__global__ void k_pack_conv_w(const uint16_t* __restrict__ w, int N, int K, int NT, uint16_t* __restrict__ out) {
+  const int KT = K / 16, ntn = (N + NT - 1) / NT;
+  const size_t total = (size_t)ntn * KT * 9 * NT * 16;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    // i enumerates (nt, kt, t, n, c) with c fastest
+    const int c = (int)(i % 16);
+    size_t q = i / 16;
+    const int n = (int)(q % NT); q /= NT;
+    const int t = (int)(q % 9); q /= 9;
+    const int kt = (int)(q % KT);
+    const int nt = (int)(q / KT);
+    const int gn = nt * NT + n;
+    const uint16_t v = gn < N ? w[((size_t)gn * 9 + t) * K + kt * 16 + c] : (uint16_t)0;
+    const size_t blk = ((size_t)nt * KT + kt) * 9 * NT * 16;   // elements
+    const size_t off = (size_t)t * NT * 16 + (((n >> 3) * 2 + (c >> 3)) * 64) + (n & 7) * 8 + (c & 7);
+    out[blk + off] = v;
   }
 }
 
@@ -829,6 +915,8 @@ struct Layer {
   size_t w_off, b_off;       // offsets into the flat parameters
   uint16_t* wb = nullptr;    // BF16 [cout][taps][cin]
   uint16_t* wt = nullptr;    // BF16 [cin][taps][cout]
+  uint16_t* wpk = nullptr;   // wb in the warp-specialised convolution's blocks (3x3 layers)
+  uint16_t* wtpk = nullptr;  // wt likewise (data gradient)
   int cin() const { return cu + cs; }
   size_t nw() const { return (size_t)cout * taps * cin(); }
 };
@@ -837,6 +925,7 @@ enum { L_E0A, L_E0, L_E1, L_E2, L_E3, L_E4A, L_E4, L_D3, L_D2, L_D1, L_D0, L_OUT
 
 struct Net {
   int device = 0;
+  int conv_mode = 0;   // 3x3 convolutions: 0 warp-specialised TMA pipeline, 1 one CTA per tile
   cudaStream_t st = nullptr;
   Layer L[NLAYERS];
   size_t n_params = 0;
@@ -899,6 +988,10 @@ static cudaError_t refresh_bf16(Net& n) {
   for (int i = 0; i < NLAYERS; ++i) {
     Layer& l = n.L[i];
     k_weights_bf16<<<grid1(l.nw()), 256, 0, n.st>>>(n.w + l.w_off, l.cout, l.taps, l.cin(), l.wb, l.wt);
+    if (l.taps == 9) {
+      k_pack_conv_w<<<grid1(ws_packed_elems(l.cout, l.cin())), 256, 0, n.st>>>(l.wb, l.cout, l.cin(), ws_nt(l.cout), l.wpk);
+      k_pack_conv_w<<<grid1(ws_packed_elems(l.cin(), l.cout)), 256, 0, n.st>>>(l.wt, l.cin(), l.cout, ws_nt(l.cin()), l.wtpk);
+    }
   }
   return cudaGetLastError();
 }
@@ -968,7 +1061,12 @@ static cudaError_t conv_fwd(Net& n, const Layer& l, const uint16_t* u, const uin
   ConvSrc src{u, l.cu, lv + 1 < 5 ? n.hl[lv + 1] : 1, lv + 1 < 5 ? n.wl[lv + 1] : 1, s, l.cs, h, w, l.taps, 1};
   if (l.taps == 9 && !logits) {
     HaloSrc hs{u, l.cu, src.hc, src.wc, s, l.cs, h, w};
-    return conv3x3(hs, l.wb, l.cin(), l.cout, n.B, EpiAct{(uint16_t*)y, n.w + l.b_off, l.cout, l.relu}, n.err, n.st);
+    const EpiAct ep{(uint16_t*)y, n.w + l.b_off, l.cout, l.relu};
+    if (n.conv_mode == 0) {
+      cudaError_t e = conv3x3_ws(hs, l.wpk, l.cin(), l.cout, n.B, ep, n.err, n.st);
+      if (e != cudaErrorNotSupported) return e;
+    }
+    return conv3x3(hs, l.wb, l.cin(), l.cout, n.B, ep, n.err, n.st);
   }
   ConvA a{src, P, l.cin()};
   RowMajor b{l.wb, l.cout, l.taps * l.cin(), l.taps * l.cin()};
@@ -995,6 +1093,10 @@ static cudaError_t conv_bwd(Net& n, const Layer& l, const uint16_t* dz, const ui
   // data gradient: the 3x3 convolution of dZ with the tap-mirrored transposed weights
   if (l.taps == 9) {
     HaloSrc hs{nullptr, 0, 1, 1, dz, l.cout, h, w};
+    if (n.conv_mode == 0) {
+      cudaError_t e = conv3x3_ws(hs, l.wtpk, l.cout, cin, n.B, EpiStore{n.dx, cin}, n.err, n.st);
+      if (e != cudaErrorNotSupported) return e;
+    }
     return conv3x3(hs, l.wt, l.cout, cin, n.B, EpiStore{n.dx, cin}, n.err, n.st);
   }
   // (1x1: M = pixels, N = cin, K = cout)
@@ -1300,6 +1402,10 @@ int wgpt_kpcn_create(int device, uint64_t seed, wgpt_kpcn** out) {
   for (int i = 0; i < kp::NLAYERS && e == cudaSuccess; ++i) {
     e = cudaMalloc(&n.L[i].wb, n.L[i].nw() * 2);
     if (e == cudaSuccess) e = cudaMalloc(&n.L[i].wt, n.L[i].nw() * 2);
+    if (e == cudaSuccess && n.L[i].taps == 9) {
+      e = cudaMalloc(&n.L[i].wpk, kp::ws_packed_elems(n.L[i].cout, n.L[i].cin()) * 2);
+      if (e == cudaSuccess) e = cudaMalloc(&n.L[i].wtpk, kp::ws_packed_elems(n.L[i].cin(), n.L[i].cout) * 2);
+    }
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&k->ev_in, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&k->ev_out, cudaEventDisableTiming);
@@ -1327,7 +1433,9 @@ int wgpt_kpcn_destroy(wgpt_kpcn* k) {
   cudaSetDevice(n.device);
   if (n.st) cudaStreamSynchronize(n.st);
   for (void* p : n.bufs) cudaFree(p);
-  for (int i = 0; i < kp::NLAYERS; ++i) { cudaFree(n.L[i].wb); cudaFree(n.L[i].wt); }
+  for (int i = 0; i < kp::NLAYERS; ++i) {
+    cudaFree(n.L[i].wb); cudaFree(n.L[i].wt); cudaFree(n.L[i].wpk); cudaFree(n.L[i].wtpk);
+  }
   cudaFree(n.w); cudaFree(n.g); cudaFree(n.m); cudaFree(n.v); cudaFree(n.err); cudaFree(n.loss);
   cudaFree(n.ds_col); cudaFree(n.ds_tgt); cudaFree(n.ds_gbuf);
   cudaFree(k->d_losses); cudaFree(k->d_crops);
@@ -1340,6 +1448,13 @@ int wgpt_kpcn_destroy(wgpt_kpcn* k) {
 }
 
 const char* wgpt_kpcn_last_error(wgpt_kpcn* k) { return k ? k->err.c_str() : "null denoiser"; }
+
+int wgpt_kpcn_set_conv_mode(wgpt_kpcn* k, int mode) {
+  if (!k) return WGPT_E_INVALID;
+  if (mode != WGPT_KPCN_CONV_PIPELINED && mode != WGPT_KPCN_CONV_PER_TILE) return kfail(k, WGPT_E_INVALID, "unknown conv mode");
+  k->net.conv_mode = mode;
+  return WGPT_OK;
+}
 
 int wgpt_kpcn_num_params(wgpt_kpcn* k, uint64_t* n) {
   if (!k || !n) return WGPT_E_INVALID;

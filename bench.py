@@ -255,35 +255,48 @@ def stage_report(r, rd, launch_once, stream, flush, paths_per_step: int, mega: b
             "avg_launch_s": avg_launch_s, "dom": dom, "cnt": cnt, "launches": int(stage_launches.sum())}
 
 
+# The plain method's filter candidates: the reference Denoiser's defaults (tracer.js:2424-2435)
+# with its own 4 passes as it runs (every pass at step 8) and as its loop intends (1, 2, 4, 8), and
+# the a-trous configuration's 5 passes (1..16).  The plain arm takes the best of them and of no
+# filter at every sample count.
+ATROUS_ARMS = {"atrous_4_as_run": (4, "as_run"), "atrous_4": (4, "intended"), "atrous_5": (5, "intended")}
+
+
 def time_to_rmse(args) -> dict:
-    """Time to display-space RMSE <= threshold against a converged FP64 reference, at 1920x1080
-    on a held-out scene of the small-configuration family (4 bounces): plain accumulation plus
-    the a-trous filter against accumulation plus the learned denoiser.  The network is trained
-    here, on the GPU, from pairs this tracer renders (scenes seeded 1000.., 256x256, inputs at
-    1/2/4/8 spp, targets at --kpcn-target-spp)."""
+    """Time to display-space RMSE <= threshold against an FP64-accumulated reference of
+    --ref-spp samples, on the flagship workload itself (1920x1080, 8 bounces, seed 1, the bench's
+    scene and camera): plain accumulation plus the a-trous filter against accumulation plus the
+    learned denoiser.  The network is trained here, on the GPU, from pairs this tracer renders:
+    flagship-family scenes (seeds 1000.., their own cameras) as 256x256 windows of their 1080p
+    views, inputs at 1/2/4/8 spp, targets at --kpcn-target-spp with an independent stream; the
+    flagship scene and the held-out evaluation scenes (seeds 5000..) are not trained on."""
     import torch
     from webgpuraytracer_b200 import kpcn
     from webgpuraytracer_b200 import renderer as rd
-    from webgpuraytracer_b200 import synth
-    W, H, thr = 1920, 1080, args.rmse_threshold
-    out = {"threshold": thr, "space": "display (shader.wgsl tonemap, exposure 1)",
-           "scene": "small-configuration family, seed 1 (held out), 1920x1080, 4 bounces",
+    from webgpuraytracer_b200 import scene as sc
+    W, H, thr = WIDTH, HEIGHT, args.rmse_threshold
+    out = {"threshold": thr, "space": "display (shader.wgsl tonemap, exposure 1); linear RMSE reported beside it",
+           "scene": f"flagship workload, seed 1, {W}x{H}, {BOUNCES} bounces (held out of training)",
            "reference": f"{args.ref_spp} spp, FP64 Welford accumulation"}
     t0 = time.perf_counter()
     k = kpcn.Kpcn(0, seed=1)
-    n_ex = kpcn.build_training_set(k, range(1000, 1000 + args.kpcn_scenes), 256, (1, 2, 4, 8), args.kpcn_target_spp)
+    n_ex = kpcn.build_flagship_training_set(k, range(1000, 1000 + args.kpcn_scenes), crops=args.kpcn_crops,
+                                            target_spp=args.kpcn_target_spp, bounces=BOUNCES)
     t_data = time.perf_counter() - t0
     t0 = time.perf_counter()
     losses = k.train(args.kpcn_steps, batch=16, crop=128, lr=1e-3, seed=1)
     t_train = time.perf_counter() - t0
-    out["training"] = {"scenes": args.kpcn_scenes, "examples": n_ex, "target_spp": args.kpcn_target_spp,
+    out["training"] = {"family": "flagship (seeded instances, primitives, Disney materials, sun sky, seeded cameras)",
+                       "scenes": args.kpcn_scenes, "windows_per_scene": args.kpcn_crops, "window": "256x256 of 1920x1080",
+                       "examples": n_ex, "input_spp": [1, 2, 4, 8], "target_spp": args.kpcn_target_spp,
                        "steps": args.kpcn_steps, "batch": "16 x 128^2 crops", "data_s": t_data, "train_s": t_train,
                        "loss_first_50": float(np.mean(losses[:50])), "loss_last_50": float(np.mean(losses[-50:])),
                        "params": k.n_params}
-    scene = synth.small_scene(1, W, H, 4)
-    scene.camera.aspect = W / H
+    out["held_out"] = held_out_eval(k, args)
+
+    scene, packed = build_workload()
     ref_r = rd.Renderer(W, H, seed_fn=lambda: 4242)
-    ref_r.set_scene(scene)
+    ref_r.set_scene(scene, packed=packed)
     ref_r.set_accum_f64(True)
     done = 0
     t0 = time.perf_counter()
@@ -291,29 +304,43 @@ def time_to_rmse(args) -> dict:
         n = min(4096, args.ref_spp - done)
         ref_r.render(tsize=W, reps=n)
         done += n
-    ref, _, _ = ref_r.read_accum_f64()
+    ref, var, _ = ref_r.read_accum_f64()
     out["reference_s"] = time.perf_counter() - t0
     ref_r.close()
     ref_disp = kpcn.tonemap(ref)
+    # the reference's own noise in display space (delta method: derivative of the tonemap times
+    # the standard error of each pixel mean)
+    x = np.maximum(ref, 0.0)
+    deriv = 0.4545 * (x / (x + 0.3)) ** (0.4545 - 1.0) * 0.3 / (x + 0.3) ** 2
+    out["reference_display_noise_rmse"] = float(np.sqrt(np.mean(deriv ** 2 * var / args.ref_spp)))
 
     def disp_rmse(d):
         return float(np.sqrt(np.mean((np.clip(d[..., :3], 0.0, 1.0) - ref_disp) ** 2)))
 
+    def lin_rmse(lin):
+        return float(np.sqrt(np.mean((np.asarray(lin, np.float64)[..., :3] - ref) ** 2)))
+
     ev = rd.Renderer(W, H, seed_fn=lambda: 7)
-    ev.set_scene(scene, isgbuf=True)
+    ev.set_scene(scene, isgbuf=True, packed=packed)
     ev.render_gbuffer()
     ev.reset()
-    atrous = rd.Denoiser(ev, passes=5)
+    dens = {name: rd.Denoiser(ev, passes=pp, mode=mode) for name, (pp, mode) in ATROUS_ARMS.items()}
     sweep, done, spp = [], 0, 1
     while spp <= args.max_spp:
         ev.render(tsize=W, reps=spp - done)
         done = spp
-        e_raw = kpcn.rmse(ev.read_accum(), ref)
-        atrous.execute()
-        e_at = disp_rmse(atrous.read()[1])
-        e_nn = kpcn.rmse(k.denoise(ev), ref)
-        sweep.append({"spp": spp, "accum": e_raw, "atrous": e_at, "kpcn": e_nn})
-        if min(e_raw, e_at) <= thr and e_nn <= thr:
+        acc = ev.read_accum()
+        row = {"spp": spp, "accum": kpcn.rmse(acc, ref), "accum_linear": lin_rmse(acc)}
+        for name, dn in dens.items():
+            dn.execute()
+            row[name] = disp_rmse(dn.read()[1])
+        if spp <= args.max_nn_spp:
+            lin = k.denoise(ev)
+            row["kpcn"] = kpcn.rmse(lin, ref)
+            row["kpcn_linear"] = lin_rmse(lin)
+        sweep.append(row)
+        plain_best = min(row[c] for c in ("accum", *ATROUS_ARMS))
+        if plain_best <= thr:
             break
         spp *= 2
     ev.close()
@@ -321,12 +348,13 @@ def time_to_rmse(args) -> dict:
 
     def first(key_fn):
         for row in sweep:
-            if key_fn(row) <= thr:
-                return row["spp"]
+            v = key_fn(row)
+            if v is not None and v <= thr:
+                return row
         return None
 
-    s_plain = first(lambda r_: min(r_["accum"], r_["atrous"]))
-    s_nn = first(lambda r_: r_["kpcn"])
+    row_p = first(lambda r_: min(r_[c] for c in ("accum", *ATROUS_ARMS)))
+    row_n = first(lambda r_: r_.get("kpcn"))
 
     def timed(spp_, filt):
         """Device time of rendering spp_ samples from frame 0 and filtering once, on a renderer
@@ -334,18 +362,24 @@ def time_to_rmse(args) -> dict:
         allocated and its loop graph built, as in an interactive session); frame 0 overwrites
         the accumulation, so the timed images equal a fresh renderer's."""
         r_ = rd.Renderer(W, H, seed_fn=lambda: 7)
-        r_.set_scene(scene, isgbuf=True)
+        r_.set_scene(scene, isgbuf=True, packed=packed)
         r_.render_gbuffer()
         r_.reset()
         r_.render(tsize=W, reps=spp_)
         r_.reset()
         st = torch.cuda.ExternalStream(r_.stream_handle())
+        dn = rd.Denoiser(r_, passes=ATROUS_ARMS[filt][0], mode=ATROUS_ARMS[filt][1]) if filt in ATROUS_ARMS else None
+        if dn:
+            dn.execute()                      # allocates the filter's buffers outside the timing
+        if filt == "kpcn":
+            k.denoise(r_, want_linear=False)
+        r_.synchronize()
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         e0.record(st)
         r_.render(tsize=W, reps=spp_, sync=False)
         e1.record(st)
-        if filt == "atrous":
-            rd.Denoiser(r_, passes=5).execute()
+        if dn:
+            dn.execute()
         elif filt == "kpcn":
             k.denoise(r_, want_linear=False)
         e2.record(st)
@@ -354,25 +388,26 @@ def time_to_rmse(args) -> dict:
         r_.close()
         return e0.elapsed_time(e1), e1.elapsed_time(e2)
 
-    def arm(s_, filt_best):
-        if s_ is None:
-            last = sweep[-1]
-            s_est = last["spp"] * (last["accum"] / thr) ** 2
-            r_ms, _ = timed(last["spp"], "none")
-            return {"spp": None, "spp_extrapolated": s_est, "ms": r_ms * s_est / last["spp"],
-                    "method": "accumulation (1/sqrt(spp) extrapolation of the last sweep point)"}
-        r_ms, f_ms = timed(s_, filt_best)
-        return {"spp": s_, "ms": r_ms + f_ms, "render_ms": r_ms, "filter_ms": f_ms, "method": filt_best}
+    def arm(row, candidates, label):
+        if row is None:
+            last = [r_ for r_ in sweep if any(c in r_ for c in candidates)][-1]
+            best = min((c for c in candidates if c in last), key=lambda c: last[c])
+            s_est = last["spp"] * (last[best] / thr) ** 2
+            r_ms, f_ms = timed(last["spp"], best)
+            return {"spp": None, "spp_extrapolated": s_est, "ms": r_ms * s_est / last["spp"] + f_ms,
+                    "method": f"{best} (1/sqrt(spp) extrapolation of the last sweep point)", "arm": label}
+        best = min((c for c in candidates if c in row and row[c] <= thr), key=lambda c: row[c])
+        r_ms, f_ms = timed(row["spp"], best)
+        return {"spp": row["spp"], "ms": r_ms + f_ms, "render_ms": r_ms, "filter_ms": f_ms, "method": best,
+                "rmse": row[best], "arm": label}
 
-    row_p = next((r_ for r_ in sweep if r_["spp"] == s_plain), None)
-    plain_filter = "atrous" if row_p is not None and row_p["atrous"] <= row_p["accum"] else "none"
-    out["plain"] = arm(s_plain, plain_filter)
-    out["neural"] = arm(s_nn, "kpcn")
+    out["plain"] = arm(row_p, ("accum", *ATROUS_ARMS), "accumulation + a-trous (best filter per sample count)")
+    out["neural"] = arm(row_n, ("kpcn",), "accumulation + learned denoiser")
     if out["plain"]["ms"] and out["neural"]["ms"]:
         out["plain_over_neural"] = out["plain"]["ms"] / out["neural"]["ms"]
     # inference throughput at 1080p on the tensor cores
     r_ = rd.Renderer(W, H, seed_fn=lambda: 7)
-    r_.set_scene(scene, isgbuf=True)
+    r_.set_scene(scene, isgbuf=True, packed=packed)
     r_.render_gbuffer()
     r_.reset()
     r_.render(tsize=W, reps=1)
@@ -400,12 +435,69 @@ def time_to_rmse(args) -> dict:
     return out
 
 
+def held_out_eval(k, args, n_scenes: int = 16, size: int = 256, spps=(4, 16), target_spp: int = 4096) -> dict:
+    """Display RMSE of the noisy input, the a-trous filter (the a-trous configuration's 5
+    passes) and the network on one 256x256 window of each of n_scenes flagship-family scenes
+    that training never saw (seeds 5000..), at each input sample count, against a target_spp
+    render with an independent stream.  The window is rendered as a section of the scene's
+    1920x1080 view; both filters run over the image and are scored on the window."""
+    from webgpuraytracer_b200 import kpcn
+    from webgpuraytracer_b200 import renderer as rd
+    from webgpuraytracer_b200 import scene as sc
+    res = {s_: {"noisy": [], "atrous_5": [], "kpcn": []} for s_ in spps}
+    tgt_r = rd.Renderer(WIDTH, HEIGHT, seed_fn=lambda: 0)
+    in_r = rd.Renderer(WIDTH, HEIGHT, seed_fn=lambda: 0)
+    for r_ in (tgt_r, in_r):
+        r_.set_wavefront_config(1 << 24, 0)
+    try:
+        for seed in range(5000, 5000 + n_scenes):
+            s = kpcn.flagship_family_scene(seed, WIDTH, HEIGHT, BOUNCES)
+            packed = sc.pack_scene_data(s)
+            (cx, cy), = kpcn.crop_origins(seed, 1, WIDTH, HEIGHT, size)
+            win = (slice(cy, cy + size), slice(cx, cx + size))
+            tgt_r.seed_fn = lambda: 200_000 + seed
+            tgt_r.set_scene(s, packed=packed)
+            tgt_r.render_section(0, target_spp, cx, cy, size, size)
+            tgt_r.synchronize()
+            target = tgt_r.read_accum()[win]
+            in_r.seed_fn = lambda: seed
+            in_r.set_scene(s, isgbuf=True, packed=packed)
+            in_r.render_gbuffer()
+            done = 0
+            for spp in spps:
+                in_r.render_section(done, spp - done, cx, cy, size, size)
+                in_r.synchronize()
+                done = spp
+                acc = in_r.read_accum()
+                res[spp]["noisy"].append(kpcn.rmse(acc[win], target))
+                dn = rd.Denoiser(in_r, passes=5)
+                dn.execute()
+                comp = dn.read()[1][win]
+                res[spp]["atrous_5"].append(float(np.sqrt(np.mean(
+                    (np.clip(comp[..., :3], 0.0, 1.0) - kpcn.tonemap(target)) ** 2))))
+                lin = k.denoise(in_r)
+                res[spp]["kpcn"].append(kpcn.rmse(lin[win], target))
+    finally:
+        tgt_r.close()
+        in_r.close()
+    return {"scenes": n_scenes, "seeds": f"5000..{5000 + n_scenes - 1}", "window": f"{size}x{size} of 1920x1080",
+            "target_spp": target_spp,
+            "mean_display_rmse": {str(s_): {m: float(np.mean(v)) for m, v in d.items()} for s_, d in res.items()},
+            "kpcn_better_than_atrous": {str(s_): int(sum(a_ < b_ for a_, b_ in zip(d["kpcn"], d["atrous_5"])))
+                                        for s_, d in res.items()}}
+
+
 # FP32 operations per counted unit for the small configuration's ALU roofline (the constants
 # are the operation counts of the restated routines, rounded): slab test of one child box 12,
 # Moller-Trumbore 27, one analytic primitive (ray transform + quadric) 40, one shading event
 # (lobe probabilities, sampling, eval and pdf of the Disney BSDF, NEE set-up) 300, one CDF probe 2.
 FLOPS_PER_UNIT = {4: 12, 5: 27, 6: 40, 7: 300, 9: 2}
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 148 SMs x 128 FP32 lanes x FMA x 1965 MHz
+
+
+def autotune_shapes() -> dict:
+    from webgpuraytracer_b200 import autotune
+    return autotune.TRAV_SHAPES
 
 
 def small_config(steps: int = 20, warmup: int = 3) -> dict:
@@ -506,6 +598,12 @@ def run_ours(args):
         r._check(r.L.wgpt_set_params(r.ctx, rd.ptr(p)), "set_params")
         r._check(r.L.wgpt_render(r.ctx, frame, spp, 0, 0, WIDTH, HEIGHT), "render")
 
+    # kernel variants and thresholds by the autotuner (coordinate descent, one render call of the
+    # workload per candidate after a warm-up call), unless fixed on the command line
+    tuned_k = None
+    if not mega and not args.no_tune:
+        from webgpuraytracer_b200 import autotune
+        tuned_k = autotune.tune_kernels(r, lambda: launch(0))
     # warm-up (builds the loop graph on the first call)
     for i in range(args.warmup):
         launch(i)
@@ -596,7 +694,7 @@ def run_ours(args):
         small = small_config()
         b = batch_measure(args, 0, 1, local, steps=2, warmup=3)
         batch = {k_: b[k_] for k_ in ("value", "unit", "ms_per_step", "view_done_ms", "view_finished_ms", "e2e",
-                                      "rays_per_s", "autotune_table_ms")}
+                                      "rays_per_s", "autotune_table_ms", "autotune_kernels_table_ms")}
         batch["config"] = b["config"]
         batch["metric"] = b["metric"]
 
@@ -610,7 +708,12 @@ def run_ours(args):
                        "step": f"one render call of {spp} samples per pixel ({paths_per_step:,} paths)",
                        "l2": "flushed between timed steps (256 MB write); path state and sample buffers exceed L2",
                        "parallelism": f"replicas x{world}", "render_mode": args.mode,
-                       "path_pool": pool_paths},
+                       "path_pool": pool_paths,
+                       "autotuned": None if tuned_k is None else {
+                           "knobs": tuned_k["tuning"],
+                           "trav_shape_names": {str(k_): v_ for k_, v_ in autotune_shapes().items()},
+                           "table_ms": tuned_k["table"],
+                           "method": "coordinate descent, one 64-spp call per candidate (CUDA events)"}},
             "rays_per_s": rays * world * args.steps / dev_s_max,
             "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": 112,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 4},
@@ -740,6 +843,7 @@ def batch_measure(args, rank: int, world: int, local: int, steps: int, warmup: i
     else:
         tuned = autotune.tune_wavefront(r, lambda: r.render_views(p0, f0, probe_spp, timing=False),
                                         units=(1 << 27, 1 << 30))
+    tuned_k = autotune.tune_kernels(r, lambda: r.render_views(p0, f0, probe_spp, timing=False))
     net = kpcn.Kpcn(local, seed=1)   # untrained weights: the same kernels and cost as trained ones
     for i in range(len(views)):      # first use loads the network's kernels and sizes its buffers
         net.denoise_view(r, i)
@@ -816,7 +920,9 @@ def batch_measure(args, rank: int, world: int, local: int, steps: int, warmup: i
                        "step": f"one render_views call per rank ({paths_all:,} paths over all ranks)",
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"views LPT-assigned over {world} rank(s)",
-                       "autotuned": {"pool_paths": tuned["pool_paths"], "units_per_pass": tuned["units_per_pass"]}},
+                       "autotuned": {"pool_paths": tuned["pool_paths"], "units_per_pass": tuned["units_per_pass"],
+                                     **tuned_k["tuning"]}},
+            "autotune_kernels_table_ms": tuned_k["table"],
             "autotune_table_ms": tuned["table"],
             "view_done_ms": {"p50": float(np.percentile(done_all, 50)), "p99": float(np.percentile(done_all, 99)),
                              "max": float(np.max(done_all))},
@@ -899,14 +1005,17 @@ def main():
     ap.add_argument("--mode", choices=["wavefront", "megakernel"], default="wavefront")
     ap.add_argument("--pool", type=int, default=0, help="wavefront path slots (0: library default)")
     ap.add_argument("--no-rmse", action="store_true", help="skip the time-to-RMSE measurement")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default kernel variants (no autotuning)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the small-configuration and batched-views measurements of the default line")
     ap.add_argument("--rmse-threshold", type=float, default=0.01)
     ap.add_argument("--ref-spp", type=int, default=65536, help="samples of the FP64 reference image")
     ap.add_argument("--max-spp", type=int, default=4096, help="largest sample count of the RMSE sweep")
-    ap.add_argument("--kpcn-scenes", type=int, default=128)
+    ap.add_argument("--kpcn-scenes", type=int, default=64, help="flagship-family training scenes")
+    ap.add_argument("--kpcn-crops", type=int, default=2, help="256x256 training windows per scene")
     ap.add_argument("--kpcn-target-spp", type=int, default=1024)
-    ap.add_argument("--kpcn-steps", type=int, default=2000)
+    ap.add_argument("--kpcn-steps", type=int, default=3000)
+    ap.add_argument("--max-nn-spp", type=int, default=256, help="largest sample count the network is evaluated at")
     ap.add_argument("--workload", choices=["flagship", "batch", "denoise"], default="flagship",
                     help="flagship: 1080p 64 spp; batch: 32 uneven views of the 5.24 M-triangle scene; "
                          "denoise: learned and a-trous filters on one 1080p frame")

@@ -149,6 +149,21 @@ int wgpt_write_accum_f64(wgpt_ctx* ctx, const double* src_8_per_px);   /* checkp
 int wgpt_set_wavefront_config(wgpt_ctx* ctx, uint32_t pool_paths, uint64_t units_per_pass);
 int wgpt_get_wavefront_config(wgpt_ctx* ctx, uint32_t* pool_paths, uint64_t* units_per_pass);
 
+/* Kernel variants and thresholds of the wavefront renderer, for the autotuner (no counterpart
+   in the reference).  trav_shape: block shape of the closest-hit and shadow traversal kernels,
+   0 = 192 threads x 6 blocks per SM (default), 1 = 128 x 9, 2 = 256 x 4 (textured scenes keep 0
+   for shadow rays); shade_block: surface-shading block of untextured scenes, 512 (default) or 256;
+   refill_closest / refill_shadow: idle lanes (1..32) a traversal warp accumulates before it takes
+   new rays from the queue (defaults 24 and 8).  Results do not depend on any of them. */
+typedef struct wgpt_wavefront_tuning {
+  uint32_t trav_shape;
+  uint32_t shade_block;
+  uint32_t refill_closest;
+  uint32_t refill_shadow;
+} wgpt_wavefront_tuning;
+int wgpt_set_wavefront_tuning(wgpt_ctx* ctx, const wgpt_wavefront_tuning* tuning);
+int wgpt_get_wavefront_tuning(wgpt_ctx* ctx, wgpt_wavefront_tuning* tuning);
+
 /* setScene(scene, true) + render(): one dispatch of gbuf_main (shader.wgsl:2510-2603) into the
    G-buffer and the debug quadrant image. */
 int wgpt_render_gbuffer(wgpt_ctx* ctx, uint32_t sec_x, uint32_t sec_y, uint32_t sec_w, uint32_t sec_h);

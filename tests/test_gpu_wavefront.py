@@ -181,3 +181,38 @@ def test_fp64_accumulation_and_3_sigma_agreement_with_oracle():
     z2 = float(np.mean((diff[live] / sigma[live]) ** 2))
     assert frac >= 0.9935, f"only {frac:.4f} of pixel channels within 3 sigma"
     assert 0.8 <= z2 <= 1.25, f"mean squared z-score {z2:.3f}"
+
+
+@pytest.mark.parametrize("tuning", [
+    {"trav_shape": 1, "shade_block": 512, "refill_closest": 24, "refill_shadow": 8},
+    {"trav_shape": 2, "shade_block": 256, "refill_closest": 8, "refill_shadow": 16},
+    {"trav_shape": 0, "shade_block": 256, "refill_closest": 32, "refill_shadow": 1},
+])
+def test_kernel_variants_leave_images_unchanged(tuning):
+    """Every tuned kernel variant (traversal block shape, shading block, refill thresholds)
+    renders the flagship-family crop bit for bit like the default variants."""
+    s = synth.flagship_scene(1, 160, 120, 8)
+    packed = sc.pack_scene_data(s)
+    out = []
+    for t in (None, tuning):
+        r = rd.Renderer(160, 120, seed_fn=lambda: 3)
+        r.set_scene(s, packed=packed)
+        if t is not None:
+            r.set_wavefront_tuning(**t)
+            assert r.wavefront_tuning() == t
+        r.render(tsize=160, reps=4)
+        out.append((r.read_accum(), r.read_output()))
+        r.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+
+
+def test_wavefront_tuning_rejects_out_of_range():
+    r = rd.Renderer(8, 8)
+    for bad in ({"trav_shape": 3}, {"shade_block": 384}, {"refill_closest": 0}, {"refill_shadow": 33}):
+        t = {"trav_shape": 0, "shade_block": 512, "refill_closest": 24, "refill_shadow": 8}
+        t.update(bad)
+        with pytest.raises(WgptError) as ei:
+            r.set_wavefront_tuning(**t)
+        assert ei.value.code == 1
+    r.close()

@@ -52,6 +52,11 @@ class SceneDesc(C.Structure):
     ]
 
 
+class WavefrontTuning(C.Structure):
+    _fields_ = [("trav_shape", C.c_uint32), ("shade_block", C.c_uint32), ("refill_closest", C.c_uint32),
+                ("refill_shadow", C.c_uint32)]
+
+
 class WgptError(RuntimeError):
     def __init__(self, code: int, what: str, msg: str = ""):
         self.code = code
@@ -95,6 +100,8 @@ EXPORTS = {
     "wgpt_sample_env": ([_P, _P, _U32, _P, _P], C.c_int),
     "wgpt_set_denoise_mode": ([_P, C.c_int], C.c_int),
     "wgpt_kpcn_set_conv_mode": ([_P, C.c_int], C.c_int),
+    "wgpt_set_wavefront_tuning": ([_P, _P], C.c_int),
+    "wgpt_get_wavefront_tuning": ([_P, _P], C.c_int),
     "wgpt_rng_stream": ([C.c_int, _U32, _U32, _U32, _U32, _P], C.c_int),
     "wgpt_set_wavefront_config": ([_P, C.c_uint32, C.c_uint64], C.c_int),
     "wgpt_set_views": ([_P, C.c_uint32, _P, _P], C.c_int),

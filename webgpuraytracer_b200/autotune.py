@@ -1,11 +1,16 @@
-"""Autotuner for the wavefront renderer's sizing.
+"""Autotuner for the wavefront renderer.
 
-The wavefront mode's throughput depends on the path-slot pool (how many paths are in flight:
-latency hiding against working-set size) and on how many samples a pass holds before they are
-folded into the images (pass count against sample-buffer memory).  Neither changes a result, so
-the tuner simply times a representative call for each candidate on the renderer's own stream
-(CUDA events, after one warm-up call) and keeps the fastest.  The chosen configuration and the
-full timing table are returned for the caller to record.
+The wavefront mode's throughput depends on knobs that never change a result:
+  * the path-slot pool (how many paths are in flight: latency hiding against working-set size)
+    and how many samples a pass holds before they are folded into the images (tune_wavefront);
+  * the compiled kernel variants and thresholds (tune_kernels): the traversal kernels' block
+    shape (192 x 6, 128 x 9 or 256 x 4 threads x blocks per SM), the surface-shading block
+    (512 or 256 threads), and how many idle lanes a closest-hit or shadow traversal warp gathers
+    before it takes new rays from the queue.
+The tuner times a representative call for each candidate on the renderer's own stream (CUDA
+events, after one warm-up call) and keeps the fastest; tune_kernels does it one knob at a time
+(coordinate descent: each knob swept with the others at their current best).  The chosen
+configuration and the full timing tables are returned for the caller to record.
 """
 from __future__ import annotations
 
@@ -46,3 +51,36 @@ def tune_wavefront(renderer, fn: Callable[[], object], pools: Iterable[int] = PO
     best = min(table, key=lambda row: row[2])
     renderer.set_wavefront_config(best[0], best[1])
     return {"pool_paths": best[0], "units_per_pass": best[1], "ms": best[2], "table": table}
+
+
+TRAV_SHAPES = {0: "192x6", 1: "128x9", 2: "256x4"}
+KERNEL_KNOBS = (
+    ("trav_shape", (0, 1, 2)),
+    ("refill_closest", (8, 16, 24, 28)),
+    ("refill_shadow", (4, 8, 16)),
+    ("shade_block", (512, 256)),
+)
+
+
+def tune_kernels(renderer, fn: Callable[[], object], knobs=KERNEL_KNOBS, repeats: int = 1, timer=None) -> dict:
+    """Coordinate descent over the wavefront kernel variants: starting from the renderer's
+    current tuning, each knob in turn is swept over its candidates (the others held at their
+    best so far) and set to its fastest value.  Returns {"tuning": {...}, "ms": best time,
+    "table": {knob: [(value, ms), ...]}}; ties keep the earlier candidate."""
+    timer = timer or time_call
+    cur = dict(renderer.wavefront_tuning())
+    tables = {}
+    best_ms = None
+    for name, cands in knobs:
+        rows = []
+        for v in cands:
+            trial = dict(cur)
+            trial[name] = v
+            renderer.set_wavefront_tuning(**trial)
+            rows.append((v, timer(renderer, fn, repeats)))
+        v_best, ms = min(rows, key=lambda row: row[1])
+        cur[name] = v_best
+        best_ms = ms
+        tables[name] = rows
+    renderer.set_wavefront_tuning(**cur)
+    return {"tuning": cur, "ms": best_ms, "table": tables}

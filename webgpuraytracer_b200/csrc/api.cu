@@ -1116,6 +1116,26 @@ int wgpt_set_wavefront_config(wgpt_ctx* ctx, uint32_t pool_paths, uint64_t units
   return WGPT_OK;
 }
 
+int wgpt_set_wavefront_tuning(wgpt_ctx* ctx, const wgpt_wavefront_tuning* t) {
+  if (!ctx || !t) return WGPT_E_INVALID;
+  if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream), "drain before retuning");
+  if (wgpt::wf_engine_tune(ctx->wf, (int)t->trav_shape, (int)t->shade_block, t->refill_closest, t->refill_shadow))
+    return fail(ctx, WGPT_E_INVALID, "wavefront tuning out of range (shape 0..2, shading block 256 or 512, refill 1..32)");
+  return WGPT_OK;
+}
+
+int wgpt_get_wavefront_tuning(wgpt_ctx* ctx, wgpt_wavefront_tuning* t) {
+  if (!ctx || !t) return WGPT_E_INVALID;
+  if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
+  int shape = 0, shade = 0;
+  wgpt::wf_engine_tuning(ctx->wf, &shape, &shade, &t->refill_closest, &t->refill_shadow);
+  t->trav_shape = (uint32_t)shape;
+  t->shade_block = (uint32_t)shade;
+  return WGPT_OK;
+}
+
 int wgpt_get_wavefront_config(wgpt_ctx* ctx, uint32_t* pool_paths, uint64_t* units_per_pass) {
   if (!ctx || !pool_paths || !units_per_pass) return WGPT_E_INVALID;
   if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();

@@ -119,6 +119,8 @@ struct WfArgs {
   unsigned long long* t0_ns;     // global timer at the start of the call's first pass
   uint32_t* status;
   unsigned long long* counters;
+  uint32_t refill_closest;       // lanes a warp lets go idle before it refills (closest hit)
+  uint32_t refill_shadow;        // the same for the shadow kernel
 };
 
 // The iteration's input queue: continuing paths, then the slots that started a new unit.
@@ -284,13 +286,14 @@ constexpr unsigned FULL = 0xffffffffu;
 // (M paths/s, one box, one threshold for both traversal kernels): 1: 658.0, 4: 665.8, 8: 674.2,
 // 16: 680.6, 20: 682.3, 24: 682.4, 28: 678.5, 32: 663.5; the shadow kernel alone is fastest at 8
 // or below (47.7 ms per step at 8, 49.0 at 24, 52.2 at 32).
-constexpr int kRefillMinClosest = 24;
-constexpr int kRefillMinShadow = 8;
-template <int MIN>
-__device__ __forceinline__ uint32_t refill(bool have, uint32_t* cursor, uint32_t n, bool& exhausted) {
+// The thresholds are arguments (WfArgs::refill_closest / refill_shadow; defaults 24 and 8, set by
+// the wavefront tuning) so the autotuner can choose them per scene.
+constexpr uint32_t kRefillMinClosest = 24;
+constexpr uint32_t kRefillMinShadow = 8;
+__device__ __forceinline__ uint32_t refill(uint32_t min_idle, bool have, uint32_t* cursor, uint32_t n, bool& exhausted) {
   uint32_t qi = 0xffffffffu;
   unsigned need = __ballot_sync(FULL, !have);
-  if (need && (__popc(need) >= MIN || need == FULL)) {
+  if (need && ((uint32_t)__popc(need) >= min_idle || need == FULL)) {
     int lane = threadIdx.x & 31;
     int leader = __ffs(need) - 1;
     uint32_t base = 0;
@@ -305,12 +308,14 @@ __device__ __forceinline__ uint32_t refill(bool have, uint32_t* cursor, uint32_t
 // Traversal kernels are latency bound; their block shape trades registers for resident warps.
 // Measured on one box (flagship / batch, M paths/s): 256 x 4 per SM at 64 registers 569 / 691;
 // 256 x 5 at 48 (spilling) 597 / 732; 192 x 6 at 56 (closest hit without spills) 627 / 748;
-// 128 x 9 at 56 625 / 748; 128 x 10 at 48 596 / 734.
-constexpr int kTravThreads = 192;
-constexpr int kTravBlocksPerSM = 6;
+// 128 x 9 at 56 625 / 748; 128 x 10 at 48 596 / 734.  Three shapes are compiled and the
+// wavefront tuning picks one: 0 = 192 x 6 (default), 1 = 128 x 9, 2 = 256 x 4.
+constexpr int kTravShapes = 3;
+__host__ __device__ constexpr int trav_threads(int shape) { return shape == 1 ? 128 : shape == 2 ? 256 : 192; }
+__host__ __device__ constexpr int trav_blocks(int shape) { return shape == 1 ? 9 : shape == 2 ? 4 : 6; }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(kTravThreads, kTravBlocksPerSM) k_wf_extend(WfArgs a) {
+template <bool COUNT, int SHAPE>
+__global__ void __launch_bounds__(trav_threads(SHAPE), trav_blocks(SHAPE)) k_wf_extend(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   uint32_t err = 0;
   const uint32_t iter = a.ctl->iter;
@@ -322,7 +327,7 @@ __global__ void __launch_bounds__(kTravThreads, kTravBlocksPerSM) k_wf_extend(Wf
   uint32_t slot = 0;
   while (true) {
     if (!exhausted) {
-      uint32_t qi = refill<kRefillMinClosest>(have, cursor, n, exhausted);
+      uint32_t qi = refill(a.refill_closest, have, cursor, n, exhausted);
       if (!have && qi < n) {
         slot = q.at(qi);
         float4 o = a.b.ray[slot * 2], d = a.b.ray[slot * 2 + 1];
@@ -608,11 +613,12 @@ __device__ __forceinline__ bool wf_sample_surface(Ray& ray, v3& throughput, v3 h
 // ~200 registers and keep 256-thread blocks.  Measured on the flagship (M paths/s, one box):
 // 128 threads 868.6, 256 threads 916.0, 512 threads 957.4 (shading 40.8 / 33.2 / 27.1 ms per
 // step): the larger the block, the fewer block-wide queue allocations and blocks to schedule.
+// The wavefront tuning can also choose 256-thread blocks for untextured scenes.
 template <bool TEX>
 constexpr int shade_threads() { return TEX ? 256 : 512; }
 
-template <bool COUNT, bool TEX>
-__global__ void __launch_bounds__(TEX ? 256 : 512) k_wf_shade(WfArgs a) {
+template <bool COUNT, bool TEX, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_wf_shade(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   const DScene& s = a.s;
   const uint32_t iter = a.ctl->iter;
@@ -769,8 +775,9 @@ __global__ void __launch_bounds__(TEX ? 256 : 512) k_wf_shade(WfArgs a) {
 }
 
 // ---------------------------------------------------------------------------- shadow
-template <bool COUNT, bool TEX>
-__global__ void __launch_bounds__(kTravThreads, TEX ? 3 * 256 / kTravThreads : kTravBlocksPerSM) k_wf_shadow(WfArgs a) {
+template <bool COUNT, bool TEX, int SHAPE>
+__global__ void __launch_bounds__(trav_threads(SHAPE), TEX ? 3 * 256 / trav_threads(SHAPE) : trav_blocks(SHAPE))
+k_wf_shadow(WfArgs a) {
   Counters<COUNT> cn; cn.init();
   uint32_t err = 0;
   const uint32_t iter = a.ctl->iter;
@@ -781,7 +788,7 @@ __global__ void __launch_bounds__(kTravThreads, TEX ? 3 * 256 / kTravThreads : k
   uint32_t e = 0;
   while (true) {
     if (!exhausted) {
-      uint32_t qi = refill<kRefillMinShadow>(have, cursor, n, exhausted);
+      uint32_t qi = refill(a.refill_shadow, have, cursor, n, exhausted);
       if (!have && qi < n) {
         e = a.b.shq[qi];
         float4 so = a.b.shadow[(e >> 1) * 4 + (e & 1u) * 2], sd = a.b.shadow[(e >> 1) * 4 + (e & 1u) * 2 + 1];
@@ -1050,6 +1057,11 @@ struct WfEngine {
   uint32_t* h_cond = nullptr;              // pinned copy of the loop condition (host-driven loop)
   int grids[4][8] = {{0}};                 // launch grid per stage, per (counting, textured) variant
   int* grid = grids[0];
+  // kernel variants and thresholds chosen by the wavefront tuning (wgpt_set_wavefront_tuning)
+  int trav_shape = 0;                      // traversal block shape (trav_threads / trav_blocks)
+  int shade_block = 512;                   // surface-shading block of untextured scenes: 512 or 256
+  uint32_t refill_closest = kRefillMinClosest;
+  uint32_t refill_shadow = kRefillMinShadow;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   WfArgs key;
@@ -1080,6 +1092,29 @@ void wf_engine_destroy(WfEngine* e) {
   delete e;
 }
 
+int wf_engine_tune(WfEngine* e, int trav_shape, int shade_block, uint32_t refill_closest, uint32_t refill_shadow) {
+  if (trav_shape < 0 || trav_shape >= kTravShapes) return 1;
+  if (shade_block != 256 && shade_block != 512) return 1;
+  if (refill_closest < 1 || refill_closest > 32 || refill_shadow < 1 || refill_shadow > 32) return 1;
+  if (trav_shape != e->trav_shape || shade_block != e->shade_block) {
+    memset(e->grids, 0, sizeof e->grids);   // new variants: new occupancy grids and a new graph
+    drop_graph(e);
+  }
+  e->trav_shape = trav_shape;
+  e->shade_block = shade_block;
+  e->refill_closest = refill_closest;
+  e->refill_shadow = refill_shadow;
+  return 0;
+}
+
+void wf_engine_tuning(const WfEngine* e, int* trav_shape, int* shade_block, uint32_t* refill_closest,
+                      uint32_t* refill_shadow) {
+  *trav_shape = e->trav_shape;
+  *shade_block = e->shade_block;
+  *refill_closest = e->refill_closest;
+  *refill_shadow = e->refill_shadow;
+}
+
 int wf_engine_configure(WfEngine* e, uint32_t pool_paths, uint64_t units_per_pass) {
   if (pool_paths < 1024u || pool_paths > (1u << 26)) return 1;
   if (units_per_pass < (1ull << 16) || units_per_pass > (1ull << 30)) return 1;
@@ -1102,14 +1137,43 @@ static int occupancy_grid(K kernel, int threads = 256) {
   return sms * (per_sm > 0 ? per_sm : 1);
 }
 
+// The tuned variants of the three kernels that have them.  Textured scenes keep the default
+// traversal shape for shadow rays and 256-thread shading blocks (their register counts).
+using KFn = void (*)(WfArgs);
+struct KernSet {
+  KFn extend, shade, shadow;
+  int t_extend, t_shade, t_shadow;
+};
+
+template <bool COUNT, bool TEX>
+static KernSet kernel_set(const WfEngine* e) {
+  KernSet k;
+  const int sh = e->trav_shape;
+  k.extend = sh == 1 ? k_wf_extend<COUNT, 1> : sh == 2 ? k_wf_extend<COUNT, 2> : k_wf_extend<COUNT, 0>;
+  k.t_extend = trav_threads(sh);
+  if (TEX) {
+    k.shadow = k_wf_shadow<COUNT, true, 0>;
+    k.t_shadow = trav_threads(0);
+    k.shade = k_wf_shade<COUNT, true, shade_threads<true>()>;
+    k.t_shade = shade_threads<true>();
+  } else {
+    k.shadow = sh == 1 ? k_wf_shadow<COUNT, false, 1> : sh == 2 ? k_wf_shadow<COUNT, false, 2> : k_wf_shadow<COUNT, false, 0>;
+    k.t_shadow = trav_threads(sh);
+    k.shade = e->shade_block == 256 ? k_wf_shade<COUNT, false, 256> : k_wf_shade<COUNT, false, 512>;
+    k.t_shade = e->shade_block == 256 ? 256 : 512;
+  }
+  return k;
+}
+
 template <bool COUNT, bool TEX>
 static void compute_grids(WfEngine* e) {
   e->grid = e->grids[(COUNT ? 2 : 0) + (TEX ? 1 : 0)];
   if (e->grid[0]) return;
+  const KernSet k = kernel_set<COUNT, TEX>(e);
   e->grid[0] = occupancy_grid(k_wf_fill<COUNT>);
-  e->grid[1] = occupancy_grid(k_wf_extend<COUNT>, kTravThreads);
-  e->grid[2] = occupancy_grid(k_wf_shade<COUNT, TEX>, shade_threads<TEX>());
-  e->grid[3] = occupancy_grid(k_wf_shadow<COUNT, TEX>, kTravThreads);
+  e->grid[1] = occupancy_grid(k.extend, k.t_extend);
+  e->grid[2] = occupancy_grid(k.shade, k.t_shade);
+  e->grid[3] = occupancy_grid(k.shadow, k.t_shadow);
   e->grid[4] = occupancy_grid(k_wf_resolve<COUNT>);
   e->grid[5] = occupancy_grid(k_wf_shade_miss<COUNT>);
   e->grid[6] = occupancy_grid(k_wf_accumulate);
@@ -1136,16 +1200,14 @@ static cudaError_t build_graph(WfEngine* e, const WfArgs& a) {
   if ((err = cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault)) != cudaSuccess) return err;
   WfArgs sa[8];
   for (int st = 0; st < 8; ++st) sa[st] = stage_args(a, st);
+  const KernSet ks = kernel_set<COUNT, TEX>(e);
   auto add_kernel = [&](cudaGraph_t gr, const void* fn, int grid, void** args, const cudaGraphNode_t* dep,
-                        cudaGraphNode_t* out) -> cudaError_t {
+                        cudaGraphNode_t* out, int threads = 256) -> cudaError_t {
     cudaKernelNodeParams kp;
     memset(&kp, 0, sizeof kp);
     kp.func = const_cast<void*>(fn);
     kp.gridDim = dim3((unsigned)grid);
-    kp.blockDim = dim3(grid == 1 ? 32u : (fn == (const void*)k_wf_extend<COUNT> || fn == (const void*)k_wf_shadow<COUNT, TEX>)
-                                           ? (unsigned)kTravThreads
-                                           : fn == (const void*)k_wf_shade<COUNT, TEX> ? (unsigned)shade_threads<TEX>()
-                                                                                        : 256u);
+    kp.blockDim = dim3(grid == 1 ? 32u : (unsigned)threads);
     kp.sharedMemBytes = 0;
     kp.kernelParams = args;
     return cudaGraphAddKernelNode(out, gr, dep, dep ? 1 : 0, &kp);
@@ -1167,12 +1229,14 @@ static cudaError_t build_graph(WfEngine* e, const WfArgs& a) {
   void* a3[] = {&sa[3]};
   void* a4[] = {&sa[4]};
   void* a7[] = {&sa[7], &h};
-  if ((err = add_kernel(body, (const void*)k_wf_extend<COUNT>, e->grid[1], a1, nullptr, &prev)) != cudaSuccess) return err;
+  if ((err = add_kernel(body, (const void*)ks.extend, e->grid[1], a1, nullptr, &prev, ks.t_extend)) != cudaSuccess)
+    return err;
   if ((err = add_kernel(body, (const void*)k_wf_shade_miss<COUNT>, e->grid[5], a5, &prev, &cur)) != cudaSuccess) return err;
   prev = cur;
-  if ((err = add_kernel(body, (const void*)k_wf_shade<COUNT, TEX>, e->grid[2], a2, &prev, &cur)) != cudaSuccess) return err;
+  if ((err = add_kernel(body, (const void*)ks.shade, e->grid[2], a2, &prev, &cur, ks.t_shade)) != cudaSuccess) return err;
   prev = cur;
-  if ((err = add_kernel(body, (const void*)k_wf_shadow<COUNT, TEX>, e->grid[3], a3, &prev, &cur)) != cudaSuccess) return err;
+  if ((err = add_kernel(body, (const void*)ks.shadow, e->grid[3], a3, &prev, &cur, ks.t_shadow)) != cudaSuccess)
+    return err;
   prev = cur;
   if ((err = add_kernel(body, (const void*)k_wf_resolve<COUNT>, e->grid[4], a4, &prev, &cur)) != cudaSuccess) return err;
   prev = cur;
@@ -1192,12 +1256,13 @@ static cudaError_t run_pass_host(WfEngine* e, const WfArgs& a, uint32_t max_iter
                                  StageTimer* timer) {
   auto T0 = [&](int k) { if (timer) timer->begin(k, st); };
   auto T1 = [&](int k) { if (timer) timer->end(k, st); };
+  const KernSet ks = kernel_set<COUNT, TEX>(e);
   T0(0); k_wf_fill<COUNT><<<e->grid[0], 256, 0, st>>>(stage_args(a, 0)); T1(0);
   for (uint32_t it = 0; it <= max_iter; ++it) {
-    T0(1); k_wf_extend<COUNT><<<e->grid[1], kTravThreads, 0, st>>>(stage_args(a, 1)); T1(1);
+    T0(1); ks.extend<<<e->grid[1], ks.t_extend, 0, st>>>(stage_args(a, 1)); T1(1);
     T0(5); k_wf_shade_miss<COUNT><<<e->grid[5], 256, 0, st>>>(stage_args(a, 5)); T1(5);
-    T0(2); k_wf_shade<COUNT, TEX><<<e->grid[2], shade_threads<TEX>(), 0, st>>>(stage_args(a, 2)); T1(2);
-    T0(3); k_wf_shadow<COUNT, TEX><<<e->grid[3], kTravThreads, 0, st>>>(stage_args(a, 3)); T1(3);
+    T0(2); ks.shade<<<e->grid[2], ks.t_shade, 0, st>>>(stage_args(a, 2)); T1(2);
+    T0(3); ks.shadow<<<e->grid[3], ks.t_shadow, 0, st>>>(stage_args(a, 3)); T1(3);
     T0(4); k_wf_resolve<COUNT><<<e->grid[4], 256, 0, st>>>(stage_args(a, 4)); T1(4);
     T0(7); k_wf_control<false><<<1, 32, 0, st>>>(stage_args(a, 7), cudaGraphConditionalHandle{}); T1(7);
     cudaError_t err = cudaMemcpyAsync(e->h_cond, &a.ctl->cond, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
@@ -1367,6 +1432,8 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
     a.t0_ns = e->d_done + e->track_cap;
     a.status = status;
     a.counters = counters;
+    a.refill_closest = e->refill_closest;
+    a.refill_shadow = e->refill_shadow;
     if (bl <= 0) {
       // no bounce runs: every sample's radiance is zero
       if ((err = cudaMemsetAsync(e->samples, 0, units * sizeof(float4), st)) != cudaSuccess) return err;

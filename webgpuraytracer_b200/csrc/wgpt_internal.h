@@ -88,6 +88,9 @@ WfEngine* wf_engine_create();
 void wf_engine_destroy(WfEngine* e);
 int wf_engine_configure(WfEngine* e, uint32_t pool_paths, uint64_t units_per_pass);
 void wf_engine_get(const WfEngine* e, uint32_t* pool_paths, uint64_t* units_per_pass);
+int wf_engine_tune(WfEngine* e, int trav_shape, int shade_block, uint32_t refill_closest, uint32_t refill_shadow);
+void wf_engine_tuning(const WfEngine* e, int* trav_shape, int* shade_block, uint32_t* refill_closest,
+                      uint32_t* refill_shadow);
 size_t wavefront_bytes_per_path();
 cudaError_t wf_render(WfEngine* e, const DeviceScene& d, const void* pairs_tlas, const void* pairs_bvh,
                       const WfJobView* views, uint32_t n_views, uint32_t* status, unsigned long long* counters,

@@ -976,6 +976,11 @@ EXPORT(KpcnLossAndGrads) {
   )
 }
 
+// kpcnSetConvMode(k, KPCN_CONV_PIPELINED | KPCN_CONV_PER_TILE)
+EXPORT(KpcnSetConvMode) {
+  BODY(wgpt_kpcn* k = kpcn_box(env, a.at(0))->k; check_k(wgpt_kpcn_set_conv_mode(k, a.i32(1)), k, "kpcnSetConvMode"); return undef(env);)
+}
+
 // kpcnDenoise(k, ctx, exposure, filtered Float32Array | null): the context's accumulation and
 // G-buffer into its rgba8 image (readOutput afterwards)
 EXPORT(KpcnDenoise) {
@@ -1222,7 +1227,7 @@ napi_value Init(napi_env env, napi_value exports) {
       FN("kpcnCreate", KpcnCreate), FN("kpcnDestroy", KpcnDestroy), FN("kpcnNumParams", KpcnNumParams),
       FN("kpcnGetParams", KpcnGetParams), FN("kpcnSetParams", KpcnSetParams), FN("kpcnAddExample", KpcnAddExample),
       FN("kpcnNumExamples", KpcnNumExamples), FN("kpcnTrain", KpcnTrain), FN("kpcnGrads", KpcnGrads),
-      FN("kpcnApply", KpcnApply), FN("kpcnLossAndGrads", KpcnLossAndGrads), FN("kpcnDenoise", KpcnDenoise),
+      FN("kpcnApply", KpcnApply), FN("kpcnLossAndGrads", KpcnLossAndGrads), FN("kpcnDenoise", KpcnDenoise), FN("kpcnSetConvMode", KpcnSetConvMode),
       FN("kpcnDenoiseView", KpcnDenoiseView), FN("gemmBf16", GemmBf16), FN("buildBlas", BuildBlas),
       FN("buildTlas", BuildTlas), FN("buildEnvCdf", BuildEnvCdf), FN("buildEnvAlias", BuildEnvAlias),
       FN("decodeRgbe", DecodeRgbe), FN("parseObj", ParseObj), FN("selftestWait", SelftestWait),
@@ -1237,6 +1242,8 @@ napi_value Init(napi_env env, napi_value exports) {
   set(env, exports, "ENV_ALIAS", make_u32(env, WGPT_ENV_ALIAS));
   set(env, exports, "DENOISE_EXACT", make_u32(env, WGPT_DENOISE_EXACT));
   set(env, exports, "DENOISE_FAST", make_u32(env, WGPT_DENOISE_FAST));
+  set(env, exports, "KPCN_CONV_PIPELINED", make_u32(env, WGPT_KPCN_CONV_PIPELINED));
+  set(env, exports, "KPCN_CONV_PER_TILE", make_u32(env, WGPT_KPCN_CONV_PER_TILE));
   set(env, exports, "NOALLOC_MAX_PIXELS", make_u32(env, WGPT_NOALLOC_MAX_PIXELS));
   return exports;
 }

@@ -18,7 +18,7 @@ import math
 import numpy as np
 
 from . import scene as sc
-from ._lib import ENV_ALIAS, ENV_CDF, SceneDesc, Buffer, check, lib, ptr
+from ._lib import ENV_ALIAS, ENV_CDF, SceneDesc, Buffer, WavefrontTuning, check, lib, ptr
 
 
 def _buf(a: np.ndarray | None) -> Buffer:
@@ -275,6 +275,20 @@ class Renderer:
         """Path-slot pool size and samples per pass of the wavefront renderer (0 keeps a value)."""
         self._check(self.L.wgpt_set_wavefront_config(self.ctx, int(pool_paths), int(units_per_pass)),
                     "set_wavefront_config")
+
+    def set_wavefront_tuning(self, trav_shape: int = 0, shade_block: int = 512, refill_closest: int = 24,
+                             refill_shadow: int = 8):
+        """Kernel variants and thresholds of the wavefront renderer (results do not depend on
+        them): traversal block shape 0 (192 x 6), 1 (128 x 9) or 2 (256 x 4); surface-shading
+        block 512 or 256; idle lanes a traversal warp gathers before refilling (1..32)."""
+        t = WavefrontTuning(trav_shape, shade_block, refill_closest, refill_shadow)
+        self._check(self.L.wgpt_set_wavefront_tuning(self.ctx, C.byref(t)), "set_wavefront_tuning")
+
+    def wavefront_tuning(self) -> dict:
+        t = WavefrontTuning()
+        self._check(self.L.wgpt_get_wavefront_tuning(self.ctx, C.byref(t)), "get_wavefront_tuning")
+        return {"trav_shape": int(t.trav_shape), "shade_block": int(t.shade_block),
+                "refill_closest": int(t.refill_closest), "refill_shadow": int(t.refill_shadow)}
 
     def wavefront_config(self) -> tuple[int, int]:
         pool, units = C.c_uint32(0), C.c_uint64(0)

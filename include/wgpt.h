@@ -154,12 +154,16 @@ int wgpt_get_wavefront_config(wgpt_ctx* ctx, uint32_t* pool_paths, uint64_t* uni
    0 = 192 threads x 6 blocks per SM (default), 1 = 128 x 9, 2 = 256 x 4 (textured scenes keep 0
    for shadow rays); shade_block: surface-shading block of untextured scenes, 512 (default) or 256;
    refill_closest / refill_shadow: idle lanes (1..32) a traversal warp accumulates before it takes
-   new rays from the queue (defaults 24 and 8).  Results do not depend on any of them. */
+   new rays from the queue (defaults 24 and 8); shadow_wide: 1 (default) walks shadow rays of
+   scenes without alpha-textured occluders over a 4-wide view of the same BVHs (quad records
+   derived on upload: each visit tests the boxes two levels down), 0 over the reference's
+   2-wide trees.  Results do not depend on any of them. */
 typedef struct wgpt_wavefront_tuning {
   uint32_t trav_shape;
   uint32_t shade_block;
   uint32_t refill_closest;
   uint32_t refill_shadow;
+  uint32_t shadow_wide;
 } wgpt_wavefront_tuning;
 int wgpt_set_wavefront_tuning(wgpt_ctx* ctx, const wgpt_wavefront_tuning* tuning);
 int wgpt_get_wavefront_tuning(wgpt_ctx* ctx, wgpt_wavefront_tuning* tuning);

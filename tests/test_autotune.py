@@ -55,7 +55,7 @@ class FakeTunable:
     """Stand-in renderer with the kernel-variant tuning interface."""
 
     def __init__(self):
-        self.t = {"trav_shape": 0, "shade_block": 512, "refill_closest": 24, "refill_shadow": 8}
+        self.t = {"trav_shape": 0, "shade_block": 512, "refill_closest": 24, "refill_shadow": 8, "shadow_wide": 1}
         self.history = []
 
     def wavefront_tuning(self):
@@ -74,16 +74,18 @@ def test_kernel_tuning_is_coordinate_descent():
         c += {8: 1.0, 16: 0.5, 24: 0.7, 28: 0.9}[t["refill_closest"]] * (2.0 if t["trav_shape"] == 1 else 1.0)
         c += {4: 0.3, 8: 0.2, 16: 0.4}[t["refill_shadow"]]
         c += {512: 0.0, 256: 0.1}[t["shade_block"]]
+        c += {1: 0.0, 0: 0.5}[t["shadow_wide"]]
         return c
 
     r = FakeTunable()
     out = autotune.tune_kernels(r, lambda: None, timer=lambda rr, fn, rep: cost(rr.t))
-    assert out["tuning"] == {"trav_shape": 1, "shade_block": 512, "refill_closest": 16, "refill_shadow": 8}
+    assert out["tuning"] == {"trav_shape": 1, "shade_block": 512, "refill_closest": 16, "refill_shadow": 8,
+                             "shadow_wide": 1}
     assert r.t == out["tuning"]
     assert [v for v, _ in out["table"]["trav_shape"]] == [0, 1, 2]
     # the refill sweep ran with the chosen shape (1), so its costs are doubled
     assert dict(out["table"]["refill_closest"])[16] == cost({**out["tuning"], "refill_shadow": 8, "refill_closest": 16})
-    assert len(r.history) == 3 + 4 + 3 + 2 + 1
+    assert len(r.history) == 2 + 3 + 4 + 3 + 2 + 1
     assert out["ms"] == min(ms for _, ms in out["table"]["shade_block"])
 
 
@@ -91,4 +93,5 @@ def test_kernel_knob_candidates_are_valid():
     knobs = dict(autotune.KERNEL_KNOBS)
     assert set(knobs["trav_shape"]) <= {0, 1, 2}
     assert set(knobs["shade_block"]) <= {256, 512}
+    assert set(knobs["shadow_wide"]) <= {0, 1}
     assert all(1 <= v <= 32 for v in knobs["refill_closest"] + knobs["refill_shadow"])

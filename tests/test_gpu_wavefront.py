@@ -184,13 +184,15 @@ def test_fp64_accumulation_and_3_sigma_agreement_with_oracle():
 
 
 @pytest.mark.parametrize("tuning", [
-    {"trav_shape": 1, "shade_block": 512, "refill_closest": 24, "refill_shadow": 8},
-    {"trav_shape": 2, "shade_block": 256, "refill_closest": 8, "refill_shadow": 16},
-    {"trav_shape": 0, "shade_block": 256, "refill_closest": 32, "refill_shadow": 1},
+    {"trav_shape": 1, "shade_block": 512, "refill_closest": 24, "refill_shadow": 8, "shadow_wide": 1},
+    {"trav_shape": 2, "shade_block": 256, "refill_closest": 8, "refill_shadow": 16, "shadow_wide": 0},
+    {"trav_shape": 0, "shade_block": 256, "refill_closest": 32, "refill_shadow": 1, "shadow_wide": 1},
+    {"trav_shape": 0, "shade_block": 512, "refill_closest": 24, "refill_shadow": 8, "shadow_wide": 0},
 ])
 def test_kernel_variants_leave_images_unchanged(tuning):
-    """Every tuned kernel variant (traversal block shape, shading block, refill thresholds)
-    renders the flagship-family crop bit for bit like the default variants."""
+    """Every tuned kernel variant (traversal block shape, shading block, refill thresholds, the
+    4-wide or 2-wide shadow walk) renders the flagship-family crop bit for bit like the default
+    variants."""
     s = synth.flagship_scene(1, 160, 120, 8)
     packed = sc.pack_scene_data(s)
     out = []
@@ -209,8 +211,9 @@ def test_kernel_variants_leave_images_unchanged(tuning):
 
 def test_wavefront_tuning_rejects_out_of_range():
     r = rd.Renderer(8, 8)
-    for bad in ({"trav_shape": 3}, {"shade_block": 384}, {"refill_closest": 0}, {"refill_shadow": 33}):
-        t = {"trav_shape": 0, "shade_block": 512, "refill_closest": 24, "refill_shadow": 8}
+    for bad in ({"trav_shape": 3}, {"shade_block": 384}, {"refill_closest": 0}, {"refill_shadow": 33},
+                {"shadow_wide": 2}):
+        t = {"trav_shape": 0, "shade_block": 512, "refill_closest": 24, "refill_shadow": 8, "shadow_wide": 1}
         t.update(bad)
         with pytest.raises(WgptError) as ei:
             r.set_wavefront_tuning(**t)

@@ -54,7 +54,7 @@ class SceneDesc(C.Structure):
 
 class WavefrontTuning(C.Structure):
     _fields_ = [("trav_shape", C.c_uint32), ("shade_block", C.c_uint32), ("refill_closest", C.c_uint32),
-                ("refill_shadow", C.c_uint32)]
+                ("refill_shadow", C.c_uint32), ("shadow_wide", C.c_uint32)]
 
 
 class WgptError(RuntimeError):

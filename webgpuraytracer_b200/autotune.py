@@ -5,8 +5,9 @@ The wavefront mode's throughput depends on knobs that never change a result:
     and how many samples a pass holds before they are folded into the images (tune_wavefront);
   * the compiled kernel variants and thresholds (tune_kernels): the traversal kernels' block
     shape (192 x 6, 128 x 9 or 256 x 4 threads x blocks per SM), the surface-shading block
-    (512 or 256 threads), and how many idle lanes a closest-hit or shadow traversal warp gathers
-    before it takes new rays from the queue.
+    (512 or 256 threads), how many idle lanes a closest-hit or shadow traversal warp gathers
+    before it takes new rays from the queue, and whether shadow rays walk a 4-wide view of the
+    BVHs.
 The tuner times a representative call for each candidate on the renderer's own stream (CUDA
 events, after one warm-up call) and keeps the fastest; tune_kernels does it one knob at a time
 (coordinate descent: each knob swept with the others at their current best).  The chosen
@@ -55,6 +56,7 @@ def tune_wavefront(renderer, fn: Callable[[], object], pools: Iterable[int] = PO
 
 TRAV_SHAPES = {0: "192x6", 1: "128x9", 2: "256x4"}
 KERNEL_KNOBS = (
+    ("shadow_wide", (1, 0)),
     ("trav_shape", (0, 1, 2)),
     ("refill_closest", (8, 16, 24, 28)),
     ("refill_shadow", (4, 8, 16)),

@@ -53,6 +53,7 @@ struct wgpt_ctx {
   // derived child-pair node arrays (64 bytes per node) of the TLAS and the BLAS buffer
   void* d_pairs_tlas = nullptr;
   void* d_pairs_bvh = nullptr;
+  uint32_t tlas_depth = 0, blas_depth = 0;   // deepest levels of the uploaded trees
   size_t pairs_cap[2] = {0, 0};
   wgpt::StageTimer* timer = nullptr;
   bool timing = false;
@@ -240,12 +241,85 @@ void fill_pairs(const wgpt_bvh_node* nodes, uint32_t root, uint32_t base, float*
   }
 }
 
+// Quad records for the any-hit (shadow) traversal over a 4-wide view of the same tree: for an
+// inner node i, up to four entries -- each child that is a leaf, and both children of each child
+// that is inner -- as (box min, count) (box max, item) float pairs, count 0xFFFFFFFF marking an
+// empty entry, the items as in the pair records.  32 floats per node, indexed like the pairs by
+// the reference node index; only nodes reached as quad roots are filled.  Boxes are copied bit
+// for bit.
+void fill_quads(const wgpt_bvh_node* nodes, uint32_t root, uint32_t base, float* quads, std::vector<uint8_t>& done) {
+  std::vector<uint32_t> st;
+  st.push_back(root);
+  while (!st.empty()) {
+    const uint32_t i = st.back();
+    st.pop_back();
+    const wgpt_bvh_node& nd = nodes[i];
+    if (nd.num_triangles > 0u || done[i]) continue;
+    done[i] = 1;
+    float* out = quads + (size_t)i * 32;
+    int k = 0;
+    auto put = [&](uint32_t idx) {
+      const wgpt_bvh_node& x = nodes[idx];
+      const uint32_t w = x.num_triangles > 0u ? x.next : idx;
+      memcpy(out + k * 8 + 0, x.aabb_min, 12);
+      memcpy(out + k * 8 + 3, &x.num_triangles, 4);
+      memcpy(out + k * 8 + 4, x.aabb_max, 12);
+      memcpy(out + k * 8 + 7, &w, 4);
+      if (x.num_triangles == 0u) st.push_back(idx);
+      ++k;
+    };
+    const uint32_t ch[2] = {i + 1, base + nd.next};
+    for (uint32_t c : ch) {
+      if (nodes[c].num_triangles > 0u) {
+        put(c);
+      } else {
+        put(c + 1);
+        put(base + nodes[c].next);
+      }
+    }
+    const uint32_t empty = 0xffffffffu;
+    for (; k < 4; ++k) memcpy(out + k * 8 + 3, &empty, 4);
+  }
+}
+
+// Levels below the root of the deepest leaf (trees validated on upload).
+uint32_t tree_depth(const wgpt_bvh_node* nodes, uint32_t root, uint32_t base) {
+  uint32_t best = 0;
+  std::vector<std::pair<uint32_t, uint32_t>> st;
+  st.push_back({root, 0u});
+  while (!st.empty()) {
+    auto [i, d] = st.back();
+    st.pop_back();
+    best = std::max(best, d);
+    const wgpt_bvh_node& nd = nodes[i];
+    if (nd.num_triangles == 0u) {
+      st.push_back({i + 1, d + 1});
+      st.push_back({base + nd.next, d + 1});
+    }
+  }
+  return best;
+}
+
+// The 4-wide shadow walk keeps at most 3 pending entries per visited level pair of each tree, plus
+// the instance's sentinel, a leaf remainder and the entry being expanded: it fits the 132-entry
+// traversal stack for TLAS + BLAS depths up to about 80 (the two-wide walk's bound is 62 each).
+bool wide_walk_fits(uint32_t tlas_depth, uint32_t blas_depth) {
+  return 3u * ((tlas_depth + 1u) / 2u + (blas_depth + 1u) / 2u) + 4u <= 132u;
+}
+
+// The pair records (16 floats per node) followed by the quad records (32 floats per node).
 int upload_pairs(wgpt_ctx* ctx, const HostScene& hs, uint32_t flags) {
   const uint32_t tlas_flags = WGPT_HAS_SPHERES | WGPT_HAS_CUBES | WGPT_HAS_CYLINDERS | WGPT_HAS_TORI | WGPT_HAS_MESHES;
-  std::vector<float> pt((size_t)std::max(1u, hs.n_tlas) * 16, 0.0f), pb((size_t)std::max(1u, hs.n_bvh) * 16, 0.0f);
+  const size_t nt = std::max(1u, hs.n_tlas), nb = std::max(1u, hs.n_bvh);
+  std::vector<float> pt(nt * 48, 0.0f), pb(nb * 48, 0.0f);
   if ((flags & tlas_flags) && hs.n_tlas) {
     std::vector<uint8_t> done(hs.n_tlas, 0);
     fill_pairs(hs.tlas, 0, 0, pt.data(), done);
+    std::fill(done.begin(), done.end(), 0);
+    fill_quads(hs.tlas, 0, 0, pt.data() + nt * 16, done);
+    ctx->tlas_depth = tree_depth(hs.tlas, 0, 0);
+  } else {
+    ctx->tlas_depth = 0;
   }
   std::vector<uint8_t> done(std::max(1u, hs.n_bvh), 0);
   std::set<uint32_t> roots;
@@ -259,6 +333,10 @@ int upload_pairs(wgpt_ctx* ctx, const HostScene& hs, uint32_t flags) {
       roots.insert(mi.node_offset);
     }
   for (uint32_t r : roots) fill_pairs(hs.bvh, r, r, pb.data(), done);
+  std::fill(done.begin(), done.end(), 0);
+  for (uint32_t r : roots) fill_quads(hs.bvh, r, r, pb.data() + nb * 16, done);
+  ctx->blas_depth = 0;
+  for (uint32_t r : roots) ctx->blas_depth = std::max(ctx->blas_depth, tree_depth(hs.bvh, r, r));
   void** dst[2] = {&ctx->d_pairs_tlas, &ctx->d_pairs_bvh};
   std::vector<float>* src[2] = {&pt, &pb};
   for (int k = 0; k < 2; ++k) {
@@ -402,6 +480,7 @@ void fill_device_scene(wgpt_ctx* ctx, const wgpt_scene_desc* d) {
   ctx->host_mats.assign(m, m + nm);
   s.flags = d->feature_flags | derived_flags(m, nm, d->feature_flags);
   if (ctx->has_alias && ctx->env_mode == WGPT_ENV_ALIAS) s.flags |= wgpt::SCENE_ENV_ALIAS;
+  if (wide_walk_fits(ctx->tlas_depth, ctx->blas_depth)) s.flags |= wgpt::SCENE_WIDE_OK;
   const wgpt_light* lt = (const wgpt_light*)d->lights.ptr;
   ctx->light_objs.clear();
   for (size_t i = 0; i < d->lights.bytes / WGPT_STRIDE_LIGHT; ++i) ctx->light_objs.push_back(lt[i].obj_idx);
@@ -653,11 +732,20 @@ int wgpt_update_objects(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   for (int j = 0; j < 5; ++j)
     if (b[j]->bytes) CK(cudaMemcpyAsync(ctx->d_buf[ks[j]], b[j]->ptr, b[j]->bytes, cudaMemcpyHostToDevice, ctx->stream), "update buffer");
   if (nt > 0 && (flags & tlas_flags)) {
-    std::vector<float> pt((size_t)nt * 16, 0.0f);
+    std::vector<float> pt((size_t)nt * 16, 0.0f), qt((size_t)nt * 32, 0.0f);
     std::vector<uint8_t> done(nt, 0);
     fill_pairs(tlas, 0, 0, pt.data(), done);
+    std::fill(done.begin(), done.end(), 0);
+    fill_quads(tlas, 0, 0, qt.data(), done);
     CK(cudaMemcpyAsync(ctx->d_pairs_tlas, pt.data(), pt.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
        "update node pairs");
+    // the quad records follow the pair records of the uploaded node count (the buffer keeps it)
+    float* quads = (float*)ctx->d_pairs_tlas + (size_t)std::max(1u, ctx->ds.n_tlas) * 16;
+    CK(cudaMemcpyAsync(quads, qt.data(), qt.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
+       "update node quads");
+    ctx->tlas_depth = tree_depth(tlas, 0, 0);
+    if (wide_walk_fits(ctx->tlas_depth, ctx->blas_depth)) ctx->ds.flags |= wgpt::SCENE_WIDE_OK;
+    else ctx->ds.flags &= ~wgpt::SCENE_WIDE_OK;
     CK(cudaStreamSynchronize(ctx->stream), "update");
   } else {
     CK(cudaStreamSynchronize(ctx->stream), "update");
@@ -666,6 +754,7 @@ int wgpt_update_objects(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
     std::copy(mats, mats + nm, ctx->host_mats.begin());
     ctx->ds.flags = flags | derived_flags(ctx->host_mats.data(), ctx->host_mats.size(), flags);
     if (ctx->has_alias && ctx->env_mode == WGPT_ENV_ALIAS) ctx->ds.flags |= wgpt::SCENE_ENV_ALIAS;
+    if (wide_walk_fits(ctx->tlas_depth, ctx->blas_depth)) ctx->ds.flags |= wgpt::SCENE_WIDE_OK;
   }
   return WGPT_OK;
 }
@@ -1121,18 +1210,21 @@ int wgpt_set_wavefront_tuning(wgpt_ctx* ctx, const wgpt_wavefront_tuning* t) {
   if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "drain before retuning");
-  if (wgpt::wf_engine_tune(ctx->wf, (int)t->trav_shape, (int)t->shade_block, t->refill_closest, t->refill_shadow))
-    return fail(ctx, WGPT_E_INVALID, "wavefront tuning out of range (shape 0..2, shading block 256 or 512, refill 1..32)");
+  if (wgpt::wf_engine_tune(ctx->wf, (int)t->trav_shape, (int)t->shade_block, t->refill_closest, t->refill_shadow,
+                           (int)t->shadow_wide))
+    return fail(ctx, WGPT_E_INVALID,
+                "wavefront tuning out of range (shape 0..2, shading block 256 or 512, refill 1..32, shadow_wide 0 or 1)");
   return WGPT_OK;
 }
 
 int wgpt_get_wavefront_tuning(wgpt_ctx* ctx, wgpt_wavefront_tuning* t) {
   if (!ctx || !t) return WGPT_E_INVALID;
   if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
-  int shape = 0, shade = 0;
-  wgpt::wf_engine_tuning(ctx->wf, &shape, &shade, &t->refill_closest, &t->refill_shadow);
+  int shape = 0, shade = 0, wide = 0;
+  wgpt::wf_engine_tuning(ctx->wf, &shape, &shade, &t->refill_closest, &t->refill_shadow, &wide);
   t->trav_shape = (uint32_t)shape;
   t->shade_block = (uint32_t)shade;
+  t->shadow_wide = (uint32_t)wide;
   return WGPT_OK;
 }
 

@@ -22,6 +22,8 @@ namespace pt {
 struct DPairs {
   const float4* tlas;   // 4 x float4 per TLAS node
   const float4* bvh;    // 4 x float4 per BLAS node
+  const float4* tlas4;  // quad records: 8 x float4 per TLAS node (4-wide any-hit traversal)
+  const float4* bvh4;   // quad records: 8 x float4 per BLAS node
 };
 
 // Stack entries: .x = kind << 29 | item count, .y = node index or first item.
@@ -167,6 +169,54 @@ __device__ __forceinline__ bool inner_run(const DPairs& P, TravCommon& t, float 
   return false;
 }
 
+// The any-hit form of inner_run over the quad records: one visit tests the up to four boxes
+// two levels down (the children that are leaves, and the children's children) and pushes the
+// hits farthest first, so the nearest is taken next.  A box inside its parent's box is hit by a
+// ray only if the parent is (the slab bounds are monotonic in the box), so exactly the leaves the
+// two-wide walk reaches are reached; any-hit occlusion of opaque occluders does not depend on
+// the order they are found in.  Used only where no occluder is alpha-textured (the transmittance
+// product of those depends on the order) and no work is counted (the counters follow the
+// reference's two-wide walk).
+__device__ __forceinline__ bool inner_run_wide(const DPairs& P, TravCommon& t, float limit, uint32_t& err, uint2& e) {
+  while (t.sp > 0) {
+    e = t.stack[--t.sp];
+    const uint32_t kind = e.x >> 29;
+    if (kind != K_BLAS_INNER && kind != K_TLAS_INNER) return true;
+    const bool blas = kind == K_BLAS_INNER;
+    const float4* qp = (blas ? P.bvh4 : P.tlas4) + (size_t)e.y * 8;
+    const Ray& r = blas ? t.rl : t.rw;
+    const v3 inv = blas ? t.inv_l : t.inv_w;
+    const uint32_t kin = blas ? K_BLAS_INNER : K_TLAS_INNER, klf = blas ? K_BLAS_LEAF : K_TLAS_LEAF;
+    float tt[4];
+    uint2 en[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const float4 lo = ld4(qp + 2 * c), hi = ld4(qp + 2 * c + 1);
+      const uint32_t n = __float_as_uint(lo.w), item = __float_as_uint(hi.w);
+      tt[c] = -1.0f;
+      en[c] = n > 0u ? ent(klf, n, item) : ent(kin, 0u, item);
+      if (n != 0xffffffffu) {
+        const float x = intersect_aabb(r.origin, inv, lo, hi);
+        if (x >= 0.0f && x < limit) tt[c] = x;
+      }
+    }
+    // push the hits in decreasing distance (a fixed four-element selection)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      int best = -1;
+      float bt = -1.0f;
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (tt[c] >= 0.0f && tt[c] >= bt) { bt = tt[c]; best = c; }
+      if (best < 0) break;
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (c == best) { t.push(en[c], err); tt[c] = -1.0f; }
+    }
+  }
+  return false;
+}
+
 // A run of inner nodes and then one leaf (or instance end); returns true when the stack is
 // empty (the ray is done).
 template <bool COUNT>
@@ -272,12 +322,16 @@ __device__ __forceinline__ void shadow_init(const DScene& s, ShadowTrav& t, Coun
   }
 }
 
-template <bool COUNT, bool TEX>
+template <bool COUNT, bool TEX, bool WIDE = false>
 __device__ __forceinline__ bool shadow_step(const DScene& s, const DPairs& P, ShadowTrav& t, uint32_t& err,
                                             Counters<COUNT>& cn) {
   if (t.occluded) return true;
   uint2 e;
-  if (!inner_run<COUNT>(P, t, t.target_dist, err, cn, e)) return true;
+  if (WIDE) {
+    if (!inner_run_wide(P, t, t.target_dist, err, e)) return true;
+  } else {
+    if (!inner_run<COUNT>(P, t, t.target_dist, err, cn, e)) return true;
+  }
   uint32_t kind = e.x >> 29, cnt = e.x & 0x1fffffffu;
   if (kind == K_BLAS_LEAF) {
     while (true) {

@@ -775,7 +775,8 @@ __global__ void __launch_bounds__(THREADS) k_wf_shade(WfArgs a) {
 }
 
 // ---------------------------------------------------------------------------- shadow
-template <bool COUNT, bool TEX, int SHAPE>
+// WIDE: the 4-wide any-hit walk over the quad records (untextured scenes, no counting).
+template <bool COUNT, bool TEX, int SHAPE, bool WIDE = false>
 __global__ void __launch_bounds__(trav_threads(SHAPE), TEX ? 3 * 256 / trav_threads(SHAPE) : trav_blocks(SHAPE))
 k_wf_shadow(WfArgs a) {
   Counters<COUNT> cn; cn.init();
@@ -801,7 +802,7 @@ k_wf_shadow(WfArgs a) {
       }
     }
     if (!__any_sync(FULL, have)) break;
-    if (have && shadow_step<COUNT, TEX>(a.s, a.P, t, err, cn)) {
+    if (have && shadow_step<COUNT, TEX, WIDE>(a.s, a.P, t, err, cn)) {
       shadow_finish<COUNT, TEX>(a.s, t, err, cn);
       a.b.vis[e] = t.occluded ? 0.0f : t.trans;
       have = false;
@@ -1055,13 +1056,15 @@ struct WfEngine {
   unsigned long long* d_done = nullptr;    // track_cap stamps, then the start stamp
   uint32_t track_cap = 0;
   uint32_t* h_cond = nullptr;              // pinned copy of the loop condition (host-driven loop)
-  int grids[4][8] = {{0}};                 // launch grid per stage, per (counting, textured) variant
+  int grids[8][8] = {{0}};                 // launch grid per stage, per (counting, textured, wide) variant
   int* grid = grids[0];
   // kernel variants and thresholds chosen by the wavefront tuning (wgpt_set_wavefront_tuning)
   int trav_shape = 0;                      // traversal block shape (trav_threads / trav_blocks)
   int shade_block = 512;                   // surface-shading block of untextured scenes: 512 or 256
   uint32_t refill_closest = kRefillMinClosest;
   uint32_t refill_shadow = kRefillMinShadow;
+  int shadow_wide = 1;                     // 4-wide any-hit walk for untextured scenes
+  bool wide_now = false;                   // this call uses it (tuning, scene, not counting)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   WfArgs key;
@@ -1092,11 +1095,13 @@ void wf_engine_destroy(WfEngine* e) {
   delete e;
 }
 
-int wf_engine_tune(WfEngine* e, int trav_shape, int shade_block, uint32_t refill_closest, uint32_t refill_shadow) {
+int wf_engine_tune(WfEngine* e, int trav_shape, int shade_block, uint32_t refill_closest, uint32_t refill_shadow,
+                   int shadow_wide) {
   if (trav_shape < 0 || trav_shape >= kTravShapes) return 1;
   if (shade_block != 256 && shade_block != 512) return 1;
   if (refill_closest < 1 || refill_closest > 32 || refill_shadow < 1 || refill_shadow > 32) return 1;
-  if (trav_shape != e->trav_shape || shade_block != e->shade_block) {
+  if (shadow_wide != 0 && shadow_wide != 1) return 1;
+  if (trav_shape != e->trav_shape || shade_block != e->shade_block || shadow_wide != e->shadow_wide) {
     memset(e->grids, 0, sizeof e->grids);   // new variants: new occupancy grids and a new graph
     drop_graph(e);
   }
@@ -1104,15 +1109,17 @@ int wf_engine_tune(WfEngine* e, int trav_shape, int shade_block, uint32_t refill
   e->shade_block = shade_block;
   e->refill_closest = refill_closest;
   e->refill_shadow = refill_shadow;
+  e->shadow_wide = shadow_wide;
   return 0;
 }
 
 void wf_engine_tuning(const WfEngine* e, int* trav_shape, int* shade_block, uint32_t* refill_closest,
-                      uint32_t* refill_shadow) {
+                      uint32_t* refill_shadow, int* shadow_wide) {
   *trav_shape = e->trav_shape;
   *shade_block = e->shade_block;
   *refill_closest = e->refill_closest;
   *refill_shadow = e->refill_shadow;
+  *shadow_wide = e->shadow_wide;
 }
 
 int wf_engine_configure(WfEngine* e, uint32_t pool_paths, uint64_t units_per_pass) {
@@ -1157,7 +1164,11 @@ static KernSet kernel_set(const WfEngine* e) {
     k.shade = k_wf_shade<COUNT, true, shade_threads<true>()>;
     k.t_shade = shade_threads<true>();
   } else {
-    k.shadow = sh == 1 ? k_wf_shadow<COUNT, false, 1> : sh == 2 ? k_wf_shadow<COUNT, false, 2> : k_wf_shadow<COUNT, false, 0>;
+    if (!COUNT && e->wide_now)
+      k.shadow = sh == 1 ? k_wf_shadow<false, false, 1, true> : sh == 2 ? k_wf_shadow<false, false, 2, true>
+                                                                      : k_wf_shadow<false, false, 0, true>;
+    else
+      k.shadow = sh == 1 ? k_wf_shadow<COUNT, false, 1> : sh == 2 ? k_wf_shadow<COUNT, false, 2> : k_wf_shadow<COUNT, false, 0>;
     k.t_shadow = trav_threads(sh);
     k.shade = e->shade_block == 256 ? k_wf_shade<COUNT, false, 256> : k_wf_shade<COUNT, false, 512>;
     k.t_shade = e->shade_block == 256 ? 256 : 512;
@@ -1167,7 +1178,7 @@ static KernSet kernel_set(const WfEngine* e) {
 
 template <bool COUNT, bool TEX>
 static void compute_grids(WfEngine* e) {
-  e->grid = e->grids[(COUNT ? 2 : 0) + (TEX ? 1 : 0)];
+  e->grid = e->grids[(COUNT ? 2 : 0) + (TEX ? 1 : 0) + (e->wide_now ? 4 : 0)];
   if (e->grid[0]) return;
   const KernSet k = kernel_set<COUNT, TEX>(e);
   e->grid[0] = occupancy_grid(k_wf_fill<COUNT>);
@@ -1280,6 +1291,9 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
                                 cudaStream_t st, StageTimer* timer, float* done_ms) {
   cudaError_t err;
   const bool tex = (d.flags & SCENE_TEXTURED) != 0u;
+  // shadow rays over the quad records: untextured scenes whose trees are shallow enough for the
+  // 4-wide walk's stack (SCENE_WIDE_OK, set on upload), when not counting work
+  e->wide_now = !COUNT && !tex && e->shadow_wide && (d.flags & SCENE_WIDE_OK) != 0u;
   if (tex) compute_grids<COUNT, true>(e); else compute_grids<COUNT, false>(e);
   const bool track = done_ms != nullptr;
   uint64_t total_npix = 0;
@@ -1423,6 +1437,8 @@ static cudaError_t render_views(WfEngine* e, const DeviceScene& d, const void* p
     fill_dscene(a.s, d);
     a.P.tlas = (const float4*)pairs_tlas;
     a.P.bvh = (const float4*)pairs_bvh;
+    a.P.tlas4 = a.P.tlas + (size_t)(d.n_tlas > 0u ? d.n_tlas : 1u) * 4;   // quads follow the pairs
+    a.P.bvh4 = a.P.bvh + (size_t)(d.n_bvh > 0u ? d.n_bvh : 1u) * 4;
     a.b = carve(e->pool, e->pool_cap);
     a.views = e->d_views;
     a.ctl = e->d_ctl;

@@ -25,7 +25,8 @@ bool ctx_images(::wgpt_ctx* ctx, int view, CtxImages* out);   // view -1: the ma
 // it); some reads the tangent frame, through a normal map or a height field (closest hits then
 // carry their tangent-frame source).
 enum : uint32_t { SCENE_TEXTURED = 1u << 24, SCENE_ALPHA_SHADOWS = 1u << 25, SCENE_TANGENTS = 1u << 26,
-                  SCENE_ENV_ALIAS = 1u << 27 };   // environment NEE from the alias table
+                  SCENE_ENV_ALIAS = 1u << 27,    // environment NEE from the alias table
+                  SCENE_WIDE_OK = 1u << 28 };    // TLAS + BLAS depths fit the 4-wide walk's stack
 
 // Device copies of the scene buffers, in the reference's packed layouts.
 struct DeviceScene {
@@ -88,9 +89,10 @@ WfEngine* wf_engine_create();
 void wf_engine_destroy(WfEngine* e);
 int wf_engine_configure(WfEngine* e, uint32_t pool_paths, uint64_t units_per_pass);
 void wf_engine_get(const WfEngine* e, uint32_t* pool_paths, uint64_t* units_per_pass);
-int wf_engine_tune(WfEngine* e, int trav_shape, int shade_block, uint32_t refill_closest, uint32_t refill_shadow);
+int wf_engine_tune(WfEngine* e, int trav_shape, int shade_block, uint32_t refill_closest, uint32_t refill_shadow,
+                   int shadow_wide);
 void wf_engine_tuning(const WfEngine* e, int* trav_shape, int* shade_block, uint32_t* refill_closest,
-                      uint32_t* refill_shadow);
+                      uint32_t* refill_shadow, int* shadow_wide);
 size_t wavefront_bytes_per_path();
 cudaError_t wf_render(WfEngine* e, const DeviceScene& d, const void* pairs_tlas, const void* pairs_bvh,
                       const WfJobView* views, uint32_t n_views, uint32_t* status, unsigned long long* counters,

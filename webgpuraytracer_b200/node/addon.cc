@@ -509,6 +509,44 @@ EXPORT(SetWavefrontConfig) {
   )
 }
 
+// setWavefrontTuning(ctx, {travShape, shadeBlock, refillClosest, refillShadow, shadowWide})
+EXPORT(SetWavefrontTuning) {
+  BODY(
+    CtxBox* b = ctx_box(env, a.at(0));
+    wgpt_wavefront_tuning t{};
+    wgpt_get_wavefront_tuning(b->ctx, &t);
+    napi_value o = a.at(1);
+    auto field = [&](const char* key, uint32_t* dst) {
+      napi_value v = get(env, o, key);
+      if (present(env, v) && napi_get_value_uint32(env, v, dst) != napi_ok) throw ArgError{std::string(key) + ": expected a number"};
+    };
+    field("travShape", &t.trav_shape);
+    field("shadeBlock", &t.shade_block);
+    field("refillClosest", &t.refill_closest);
+    field("refillShadow", &t.refill_shadow);
+    field("shadowWide", &t.shadow_wide);
+    check(wgpt_set_wavefront_tuning(b->ctx, &t), b->ctx, "setWavefrontTuning");
+    return undef(env);
+  )
+}
+
+// getWavefrontTuning(ctx) -> {travShape, shadeBlock, refillClosest, refillShadow, shadowWide}
+EXPORT(GetWavefrontTuning) {
+  BODY(
+    CtxBox* b = ctx_box(env, a.at(0));
+    wgpt_wavefront_tuning t{};
+    check(wgpt_get_wavefront_tuning(b->ctx, &t), b->ctx, "getWavefrontTuning");
+    napi_value o;
+    napi_create_object(env, &o);
+    set(env, o, "travShape", make_u32(env, t.trav_shape));
+    set(env, o, "shadeBlock", make_u32(env, t.shade_block));
+    set(env, o, "refillClosest", make_u32(env, t.refill_closest));
+    set(env, o, "refillShadow", make_u32(env, t.refill_shadow));
+    set(env, o, "shadowWide", make_u32(env, t.shadow_wide));
+    return o;
+  )
+}
+
 // getWavefrontConfig(ctx) -> {poolPaths, unitsPerPass}
 EXPORT(GetWavefrontConfig) {
   BODY(
@@ -1215,7 +1253,8 @@ napi_value Init(napi_env env, napi_value exports) {
       FN("renderAsync", RenderAsync), FN("renderGBuffer", RenderGBuffer), FN("setRenderMode", SetRenderMode),
       FN("setEnvSampling", SetEnvSampling), FN("setAccumF64", SetAccumF64), FN("readAccumF64", ReadAccumF64),
       FN("writeAccumF64", WriteAccumF64), FN("setWavefrontConfig", SetWavefrontConfig),
-      FN("getWavefrontConfig", GetWavefrontConfig), FN("denoise", Denoise), FN("setDenoiseMode", SetDenoiseMode), FN("resample", Resample),
+      FN("getWavefrontConfig", GetWavefrontConfig), FN("setWavefrontTuning", SetWavefrontTuning),
+      FN("getWavefrontTuning", GetWavefrontTuning), FN("denoise", Denoise), FN("setDenoiseMode", SetDenoiseMode), FN("resample", Resample),
       FN("synchronize", Synchronize), FN("synchronizeTimeout", SynchronizeTimeout),
       FN("synchronizeAsync", SynchronizeAsync), FN("readAccum", ReadAccum), FN("writeAccum", WriteAccum),
       FN("readOutput", ReadOutput), FN("readGBuffer", ReadGBuffer), FN("writeGBuffer", WriteGBuffer),

@@ -277,18 +277,20 @@ class Renderer:
                     "set_wavefront_config")
 
     def set_wavefront_tuning(self, trav_shape: int = 0, shade_block: int = 512, refill_closest: int = 24,
-                             refill_shadow: int = 8):
+                             refill_shadow: int = 8, shadow_wide: int = 1):
         """Kernel variants and thresholds of the wavefront renderer (results do not depend on
         them): traversal block shape 0 (192 x 6), 1 (128 x 9) or 2 (256 x 4); surface-shading
-        block 512 or 256; idle lanes a traversal warp gathers before refilling (1..32)."""
-        t = WavefrontTuning(trav_shape, shade_block, refill_closest, refill_shadow)
+        block 512 or 256; idle lanes a traversal warp gathers before refilling (1..32); shadow
+        rays over the 4-wide view of the BVHs (1) or the 2-wide trees (0)."""
+        t = WavefrontTuning(trav_shape, shade_block, refill_closest, refill_shadow, shadow_wide)
         self._check(self.L.wgpt_set_wavefront_tuning(self.ctx, C.byref(t)), "set_wavefront_tuning")
 
     def wavefront_tuning(self) -> dict:
         t = WavefrontTuning()
         self._check(self.L.wgpt_get_wavefront_tuning(self.ctx, C.byref(t)), "get_wavefront_tuning")
         return {"trav_shape": int(t.trav_shape), "shade_block": int(t.shade_block),
-                "refill_closest": int(t.refill_closest), "refill_shadow": int(t.refill_shadow)}
+                "refill_closest": int(t.refill_closest), "refill_shadow": int(t.refill_shadow),
+                "shadow_wide": int(t.shadow_wide)}
 
     def wavefront_config(self) -> tuple[int, int]:
         pool, units = C.c_uint32(0), C.c_uint64(0)

@@ -192,32 +192,54 @@ def rmse(a: np.ndarray, b: np.ndarray, exposure: float = 1.0) -> float:
     return float(np.sqrt(np.mean((tonemap(a, exposure) - tonemap(b, exposure)) ** 2)))
 
 
+def _target_image(t: rd.Renderer, f64: bool) -> np.ndarray:
+    """The target renderer's image: its FP64 Welford mean (as rgba32f, alpha 1) or its FP32
+    running mean."""
+    if not f64:
+        return t.read_accum()
+    mean, _, _ = t.read_accum_f64()
+    out = np.ones(mean.shape[:2] + (4,), np.float32)
+    out[..., :3] = mean
+    return out
+
+
 def build_training_set(k: Kpcn, seeds, size: int = 256, spps=(1, 2, 4, 8), target_spp: int = 1024,
-                       bounces: int = 4) -> int:
+                       bounces: int = 4, device: int = 0, pool_paths: int = 1 << 24, target_f64: bool = False) -> int:
     """Adds, for every seeded scene of the small-configuration family, one example per input
     sample count: (progressive accumulation at that count, G-buffer, target at target_spp with
-    an independent sample stream).  Returns the number of examples added."""
+    an independent sample stream, accumulated in FP64 with target_f64).  One renderer pair is
+    reused for every scene.  Returns the number of examples added."""
     from . import synth
     n = 0
-    for seed in seeds:
-        s = synth.small_scene(int(seed), size, size, bounces)
-        s.camera.aspect = 1.0
-        t = rd.Renderer(size, size, seed_fn=lambda: 100_000 + int(seed))
-        t.set_scene(s)
-        t.render(tsize=size, reps=target_spp)
-        target = t.read_accum()
+    t = rd.Renderer(size, size, device=device, seed_fn=lambda: 0)
+    r = rd.Renderer(size, size, device=device, seed_fn=lambda: 0)
+    t.set_wavefront_config(pool_paths, 0)
+    r.set_wavefront_config(pool_paths, 0)
+    try:
+        for seed in seeds:
+            seed = int(seed)
+            s = synth.small_scene(seed, size, size, bounces)
+            s.camera.aspect = 1.0
+            packed = sc.pack_scene_data(s)
+            t.seed_fn = lambda: 100_000 + seed
+            t.set_scene(s, packed=packed)
+            if target_f64:
+                t.set_accum_f64(True)
+            t.render(tsize=size, reps=target_spp)
+            target = _target_image(t, target_f64)
+            r.seed_fn = lambda: seed
+            r.set_scene(s, isgbuf=True, packed=packed)
+            r.render_gbuffer()
+            gbuf = r.read_gbuffer()
+            r.reset()
+            done = 0
+            for spp in spps:
+                r.render(tsize=size, reps=spp - done)
+                done = spp
+                k.add_example(r.read_accum(), gbuf, target)
+                n += 1
+    finally:
         t.close()
-        r = rd.Renderer(size, size, seed_fn=lambda: int(seed))
-        r.set_scene(s, isgbuf=True)
-        r.render_gbuffer()
-        gbuf = r.read_gbuffer()
-        r.reset()
-        done = 0
-        for spp in spps:
-            r.render(tsize=size, reps=spp - done)
-            done = spp
-            k.add_example(r.read_accum(), gbuf, target)
-            n += 1
         r.close()
     return n
 
@@ -244,12 +266,13 @@ def crop_origins(seed: int, n: int, width: int, height: int, size: int):
 
 def build_flagship_training_set(k: Kpcn, seeds, crops: int = 2, size: int = 256, spps=(1, 2, 4, 8),
                                 target_spp: int = 1024, bounces: int = 8, width: int = 1920, height: int = 1080,
-                                device: int = 0, pool_paths: int = 1 << 24) -> int:
+                                device: int = 0, pool_paths: int = 1 << 24, target_f64: bool = False) -> int:
     """Training examples from the flagship family at the flagship's scale: for each seeded
     scene, `crops` size x size windows of its width x height view are path traced (sections of
     the full image, so objects keep their on-screen size) at every input sample count in
-    `spps` (progressively, seed = the scene seed) and at target_spp with an independent stream.
-    One renderer pair is reused for every scene.  Returns the number of examples added."""
+    `spps` (progressively, seed = the scene seed) and at target_spp with an independent stream
+    (accumulated in FP64 with target_f64).  One renderer pair is reused for every scene.  Returns
+    the number of examples added."""
     tgt_r = rd.Renderer(width, height, device=device, seed_fn=lambda: 0)
     in_r = rd.Renderer(width, height, device=device, seed_fn=lambda: 0)
     tgt_r.set_wavefront_config(pool_paths, 0)
@@ -263,10 +286,12 @@ def build_flagship_training_set(k: Kpcn, seeds, crops: int = 2, size: int = 256,
             wins = crop_origins(seed, crops, width, height, size)
             tgt_r.seed_fn = lambda: 100_000 + seed
             tgt_r.set_scene(s, packed=packed)
+            if target_f64:
+                tgt_r.set_accum_f64(True)
             for (cx, cy) in wins:
                 tgt_r.render_section(0, target_spp, cx, cy, size, size)
             tgt_r.synchronize()
-            target = tgt_r.read_accum()
+            target = _target_image(tgt_r, target_f64)
             in_r.seed_fn = lambda: seed
             in_r.set_scene(s, isgbuf=True, packed=packed)
             in_r.render_gbuffer()

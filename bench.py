@@ -52,7 +52,7 @@ BYTES_PER_UNIT = {
 PIXEL_BYTES = 16 + 16 + 4   # accumulation read + write, rgba8 store
 # DRAM bytes (read + write) per closest-hit ray of this workload: 502 MB per steady-state launch of
 # a 2,097,152-slot pool (every slot holds a live path while units remain, so 2,097,152 rays per
-# launch), from an ncu capture (bench cannot run ncu itself; profiles/k_wf_extend_flagship_1080p.md).
+# launch), from an ncu capture of this workload (bench.py cannot run ncu itself).
 # A launch's traffic is this times its rays.
 EXTEND_DRAM_BYTES_PER_RAY = 5.02e8 / 2_097_152
 KERNELS = ["k_wf_fill", "k_wf_extend", "k_wf_shade", "k_wf_shadow", "k_wf_resolve", "k_wf_shade_miss",

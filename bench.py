@@ -722,6 +722,10 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"],
                          "traffic": None if mega else EXTEND_DRAM_BYTES_PER_RAY * ext_rays_per_launch,
+                         "dram_frac": None if mega or "k_wf_extend" not in stages else
+                         EXTEND_DRAM_BYTES_PER_RAY * ext_rays_per_launch
+                         / (stages["k_wf_extend"]["ms_total"] / 1e3 / stages["k_wf_extend"]["launches"])
+                         / 1e9 / peaks["hbm_gbs"],
                          "traffic_source": None if mega else
                          "ncu dram__bytes_read.sum + dram__bytes_write.sum of steady-state k_wf_extend launches "
                          "of a 2,097,152-slot pool (mean of launches 21-23 of this workload's stage-timing pass: "

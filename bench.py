@@ -435,12 +435,15 @@ def time_to_rmse(args) -> dict:
     return out
 
 
-def held_out_eval(k, args, n_scenes: int = 16, size: int = 256, spps=(4, 16), target_spp: int = 4096) -> dict:
+def held_out_eval(k, args, n_scenes: int = 16, size: int = 256, spps=(4, 8, 16), target_spp: int = 4096,
+                  margin: int = 32) -> dict:
     """Display RMSE of the noisy input, the a-trous filter (the a-trous configuration's 5
     passes) and the network on one 256x256 window of each of n_scenes flagship-family scenes
     that training never saw (seeds 5000..), at each input sample count, against a target_spp
-    render with an independent stream.  The window is rendered as a section of the scene's
-    1920x1080 view; both filters run over the image and are scored on the window."""
+    render with an independent stream.  The input is rendered as a section of the scene's
+    1920x1080 view reaching `margin` pixels beyond the window (so both filters see real
+    neighbours at the window's edges); both filters run over the image and are scored on the
+    window."""
     from webgpuraytracer_b200 import kpcn
     from webgpuraytracer_b200 import renderer as rd
     from webgpuraytracer_b200 import scene as sc
@@ -455,6 +458,8 @@ def held_out_eval(k, args, n_scenes: int = 16, size: int = 256, spps=(4, 16), ta
             packed = sc.pack_scene_data(s)
             (cx, cy), = kpcn.crop_origins(seed, 1, WIDTH, HEIGHT, size)
             win = (slice(cy, cy + size), slice(cx, cx + size))
+            x0, y0 = max(cx - margin, 0), max(cy - margin, 0)
+            x1, y1 = min(cx + size + margin, WIDTH), min(cy + size + margin, HEIGHT)
             tgt_r.seed_fn = lambda: 200_000 + seed
             tgt_r.set_scene(s, packed=packed)
             tgt_r.render_section(0, target_spp, cx, cy, size, size)
@@ -465,7 +470,7 @@ def held_out_eval(k, args, n_scenes: int = 16, size: int = 256, spps=(4, 16), ta
             in_r.render_gbuffer()
             done = 0
             for spp in spps:
-                in_r.render_section(done, spp - done, cx, cy, size, size)
+                in_r.render_section(done, spp - done, x0, y0, x1 - x0, y1 - y0)
                 in_r.synchronize()
                 done = spp
                 acc = in_r.read_accum()
@@ -481,7 +486,7 @@ def held_out_eval(k, args, n_scenes: int = 16, size: int = 256, spps=(4, 16), ta
         tgt_r.close()
         in_r.close()
     return {"scenes": n_scenes, "seeds": f"5000..{5000 + n_scenes - 1}", "window": f"{size}x{size} of 1920x1080",
-            "target_spp": target_spp,
+            "margin": margin, "target_spp": target_spp,
             "mean_display_rmse": {str(s_): {m: float(np.mean(v)) for m, v in d.items()} for s_, d in res.items()},
             "kpcn_better_than_atrous": {str(s_): int(sum(a_ < b_ for a_, b_ in zip(d["kpcn"], d["atrous_5"])))
                                         for s_, d in res.items()}}

@@ -59,7 +59,7 @@ def test_kpcn_layout_and_params_roundtrip():
     p = k.get_params()
     sl = kpcn.param_slices()
     w0 = p[sl["E0a"][0]].reshape(32, 9, 16)
-    assert np.all(w0[:, :, 10:] == 0.0), "padded input channels start at zero"
+    assert np.all(w0[:, :, 11:] == 0.0), "padded input channels start at zero"
     wo = p[sl["OUT"][0]].reshape(80, 32)
     assert np.all(wo[75:] == 0.0), "padded logits start at zero"
     q = p * 0.5
@@ -150,7 +150,7 @@ def test_kpcn_training_gains_over_atrous():
     s = synth.small_scene(1, size, size, 4)
     r = rd.Renderer(size, size)
     r.set_scene(s, isgbuf=True)
-    r.write_accum(noisy)
+    r.write_accum(noisy, samples=spp)
     r.write_gbuffer(gbuf)
     lin = k.denoise(r, exposure=1.0)
     dn = rd.Denoiser(r, passes=4)
@@ -231,8 +231,10 @@ def test_kpcn_train_data_parallel_single_rank():
 @pytest.mark.parametrize("h,w", [(40, 48), (33, 70), (96, 160)])
 def test_kpcn_pipelined_convolutions_equal_per_tile(h, w):
     """The warp-specialised TMA convolution (default) against the one-CTA-per-tile kernel: the
-    same MMAs accumulate in the same order into tensor memory, so loss, filtered output and every
-    gradient are identical bit for bit (forward, data gradients and weight gradients)."""
+    same MMAs accumulate in the same order into tensor memory, so the filtered output is identical
+    bit for bit.  The loss and the weight gradients are sums over pixels taken with FP32 atomics
+    (split over CTAs), whose order differs from run to run in either mode: they agree to FP32
+    rounding of those sums."""
     noisy, gbuf, target = _random_image(h, w, h * 7 + w)
     k = kpcn.Kpcn(0, seed=9)
     p = k.get_params()
@@ -245,9 +247,9 @@ def test_kpcn_pipelined_convolutions_equal_per_tile(h, w):
         assert L.wgpt_kpcn_set_conv_mode(k.h, mode) == 0
         res.append(k.loss_and_grads(noisy, gbuf, target))
     (l0, g0, o0), (l1, g1, o1) = res
-    assert l0 == l1
     np.testing.assert_array_equal(o0, o1)
-    np.testing.assert_array_equal(g0, g1)
+    assert abs(l0 - l1) <= 1e-6 * abs(l0)
+    np.testing.assert_allclose(g1, g0, rtol=1e-3, atol=1e-5 * float(np.abs(g0).max()))
     k.close()
 
 

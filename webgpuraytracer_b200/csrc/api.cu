@@ -33,6 +33,7 @@ struct wgpt_ctx {
   float* accum = nullptr;
   uint8_t* out = nullptr;
   float* gbuf = nullptr;
+  uint32_t samples = 0;   // samples per pixel in accum: first_frame + reps of the last render
   // denoiser
   float* dn_a = nullptr;
   float* dn_b = nullptr;
@@ -59,7 +60,7 @@ struct wgpt_ctx {
   bool timing = false;
   wgpt::WfEngine* wf = nullptr;   // wavefront renderer: path pool, sample buffer, loop graph
   // batched views: size and images of each
-  struct View { uint32_t w, h; float* accum; uint8_t* out; float* gbuf; };
+  struct View { uint32_t w, h; float* accum; uint8_t* out; float* gbuf; uint32_t samples; };
   std::vector<View> views;
   double* acc64 = nullptr;        // optional FP64 Welford accumulation (8 doubles per pixel)
   // kept from the last full upload for the objects fast path: the (node, triangle) offset
@@ -522,6 +523,7 @@ bool wgpt::ctx_images(wgpt_ctx* ctx, int view, wgpt::CtxImages* out) {
     out->accum = ctx->accum;
     out->gbuf = ctx->gbuf;
     out->out = ctx->out;
+    out->samples = ctx->samples;
     return true;
   }
   if ((size_t)view >= ctx->views.size()) return false;
@@ -531,6 +533,7 @@ bool wgpt::ctx_images(wgpt_ctx* ctx, int view, wgpt::CtxImages* out) {
   out->accum = v.accum;
   out->gbuf = v.gbuf;
   out->out = v.out;
+  out->samples = v.samples;
   return true;
 }
 
@@ -598,7 +601,7 @@ int wgpt_validate_scene(const wgpt_scene_desc* desc, char* msg, size_t msg_len) 
 
 int wgpt_upload_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   if (!ctx) return WGPT_E_INVALID;
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   HostScene hs;
   std::set<std::pair<uint32_t, uint32_t>> checked;
   int rc = check_desc(ctx, desc, hs, &checked);
@@ -617,7 +620,7 @@ int wgpt_upload_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
 int wgpt_update_scene(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   if (!ctx) return WGPT_E_INVALID;
   if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   if (desc && (desc->feature_flags != (ctx->ds.flags & 0x7ffu) || desc->bounce_limit != ctx->ds.bounce_limit))
     return fail(ctx, WGPT_E_REBUILD, "pipeline constants changed: full upload required");
   HostScene hs;
@@ -644,7 +647,7 @@ int wgpt_update_objects(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
   if (!ctx) return WGPT_E_INVALID;
   if (!desc) return fail(ctx, WGPT_E_INVALID, "scene descriptor is null");
   if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   const uint32_t flags = desc->feature_flags;
   if (flags != (ctx->ds.flags & 0x7ffu)) return fail(ctx, WGPT_E_REBUILD, "pipeline constants changed: full upload required");
   const int ks[5] = {1, 2, 6, 3, 0};   // objects, tlas, planes, meshes, materials (tracer.js:2151-2155)
@@ -762,7 +765,7 @@ int wgpt_update_objects(wgpt_ctx* ctx, const wgpt_scene_desc* desc) {
 int wgpt_resize(wgpt_ctx* ctx, uint32_t width, uint32_t height, int want_gbuf) {
   if (!ctx) return WGPT_E_INVALID;
   if (width == 0 || height == 0 || (uint64_t)width * height > (1ull << 28)) return fail(ctx, WGPT_E_INVALID, "bad image size");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "drain before resize");
   size_t npix = (size_t)width * height;
   bool same = width == ctx->w && height == ctx->h;
@@ -783,6 +786,7 @@ int wgpt_resize(wgpt_ctx* ctx, uint32_t width, uint32_t height, int want_gbuf) {
   if (had_f64 && !ctx->acc64) CK(cudaMalloc(&ctx->acc64, npix * 64), "cudaMalloc FP64 accumulation");
   if (ctx->acc64) CK(cudaMemsetAsync(ctx->acc64, 0, npix * 64, ctx->stream), "clear FP64 accumulation");
   ctx->w = width; ctx->h = height;
+  ctx->samples = 0;
   CK(cudaStreamSynchronize(ctx->stream), "resize");
   return WGPT_OK;
 }
@@ -802,7 +806,7 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
   rc = check_env(ctx, ctx->params);
   if (rc) return rc;
   if (reps == 0) return WGPT_OK;
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   unsigned long long* cnt = ctx->counting ? ctx->d_counters : nullptr;
   wgpt::StageTimer* tm = ctx->timing ? ctx->timer : nullptr;
   if (ctx->mode == WGPT_MODE_MEGAKERNEL) {
@@ -812,6 +816,7 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
                            ctx->d_status, cnt, ctx->stream),
        "render launch");
     if (tm) tm->end(0, ctx->stream);
+    ctx->samples = first_frame + reps;
     return WGPT_OK;
   }
   if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
@@ -827,6 +832,18 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
   CK(wgpt::wf_render(ctx->wf, ctx->ds, ctx->d_pairs_tlas, ctx->d_pairs_bvh, &v, 1, ctx->d_status, cnt, ctx->stream,
                      tm),
      "wavefront render");
+  ctx->samples = first_frame + reps;
+  return WGPT_OK;
+}
+
+int wgpt_set_accum_samples(wgpt_ctx* ctx, int32_t view, uint32_t samples) {
+  if (!ctx) return WGPT_E_INVALID;
+  if (view < 0) {
+    ctx->samples = samples;
+    return WGPT_OK;
+  }
+  if ((size_t)view >= ctx->views.size()) return fail(ctx, WGPT_E_INVALID, "no such view");
+  ctx->views[(size_t)view].samples = samples;
   return WGPT_OK;
 }
 
@@ -836,7 +853,7 @@ int wgpt_render_gbuffer(wgpt_ctx* ctx, uint32_t sx, uint32_t sy, uint32_t sw, ui
   int rc = check_section(ctx, sx, sy, sw, sh);
   if (rc) return rc;
   if (!ctx->gbuf) return fail(ctx, WGPT_E_STATE, "no G-buffer: resize with want_gbuf");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   CK(wgpt::launch_gbuffer(ctx->ds, ctx->params, sx, sy, sw, sh, ctx->gbuf, ctx->out, ctx->w, ctx->d_status,
                           ctx->stream),
      "gbuffer launch");
@@ -853,7 +870,7 @@ int wgpt_denoise(wgpt_ctx* ctx, const void* uniforms, const uint32_t* steps, uin
   if (passes > 64) return fail(ctx, WGPT_E_INVALID, "more than 64 passes");
   for (uint32_t i = 0; i < passes; ++i)
     if (steps[i] == 0 || steps[i] > (1u << 20)) return fail(ctx, WGPT_E_INVALID, "step width out of range");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   size_t npix = (size_t)ctx->w * ctx->h;
   if (!ctx->dn_a) {
     CK(cudaMalloc(&ctx->dn_a, npix * 16), "cudaMalloc denoise A");
@@ -878,7 +895,7 @@ int wgpt_resample(wgpt_ctx* ctx, uint32_t dst_w, uint32_t dst_h, float rx, float
   if (!ctx) return WGPT_E_INVALID;
   if (ctx->w == 0) return fail(ctx, WGPT_E_STATE, "no image size");
   if (dst_w == 0 || dst_h == 0 || (uint64_t)dst_w * dst_h > (1ull << 28)) return fail(ctx, WGPT_E_INVALID, "bad canvas size");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   if (dst_w != ctx->cw || dst_h != ctx->ch) {
     CK(cudaStreamSynchronize(ctx->stream), "drain before canvas resize");
     dfree_t(ctx->canvas);
@@ -902,7 +919,7 @@ static int read_status(wgpt_ctx* ctx) {
 
 int wgpt_synchronize(wgpt_ctx* ctx) {
   if (!ctx) return WGPT_E_INVALID;
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "stream synchronize");
   return read_status(ctx);
 }
@@ -911,7 +928,7 @@ int wgpt_synchronize(wgpt_ctx* ctx) {
 // timeout_ms with WGPT_E_TIMEOUT (the queued work keeps running; a later call can wait again).
 int wgpt_synchronize_timeout(wgpt_ctx* ctx, uint32_t timeout_ms) {
   if (!ctx) return WGPT_E_INVALID;
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   const auto t0 = std::chrono::steady_clock::now();
   while (true) {
     cudaError_t q = cudaStreamQuery(ctx->stream);
@@ -968,7 +985,7 @@ int wgpt_read_canvas(wgpt_ctx* ctx, uint8_t* dst, uint32_t dst_w, uint32_t dst_h
 int wgpt_write_accum(wgpt_ctx* ctx, const float* src) {
   if (!ctx || !src) return WGPT_E_INVALID;
   if (!ctx->accum) return fail(ctx, WGPT_E_STATE, "no image size");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "drain");
   CK(cudaMemcpy(ctx->accum, src, (size_t)ctx->w * ctx->h * 16, cudaMemcpyHostToDevice), "write accum");
   return WGPT_OK;
@@ -976,7 +993,7 @@ int wgpt_write_accum(wgpt_ctx* ctx, const float* src) {
 int wgpt_write_gbuffer(wgpt_ctx* ctx, const void* src) {
   if (!ctx || !src) return WGPT_E_INVALID;
   if (!ctx->gbuf) return fail(ctx, WGPT_E_STATE, "no G-buffer");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "drain");
   CK(cudaMemcpy(ctx->gbuf, src, (size_t)ctx->w * ctx->h * 48, cudaMemcpyHostToDevice), "write gbuffer");
   return WGPT_OK;
@@ -987,7 +1004,7 @@ int wgpt_trace_rays(wgpt_ctx* ctx, const float* rays, uint32_t n, int32_t* o_idx
   if (!ctx || !rays || !o_idx || !m_idx || !prim || !t || !normal) return WGPT_E_INVALID;
   if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
   if (n == 0) return WGPT_OK;
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   void* d = nullptr;
   size_t per = 6 * 4 + 4 + 4 + 4 + 4 + 12;
   CK(cudaMalloc(&d, (size_t)n * per), "cudaMalloc rays");
@@ -1020,7 +1037,7 @@ int wgpt_sample_env(wgpt_ctx* ctx, const float* u2, uint32_t n, uint32_t* texel_
   if (rc) return rc;
   if (n == 0) return WGPT_OK;
   if (n > (1u << 24)) return fail(ctx, WGPT_E_INVALID, "at most 2^24 samples per call");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   void* d = nullptr;
   CK(cudaMalloc(&d, (size_t)n * 16), "cudaMalloc env samples");
   float* d_u = (float*)d;
@@ -1038,7 +1055,7 @@ int wgpt_sample_env(wgpt_ctx* ctx, const float* u2, uint32_t n, uint32_t* texel_
 
 int wgpt_rng_stream(int device, uint32_t idx, uint32_t sample_number, uint32_t seed, uint32_t n, float* out) {
   if (!out || n == 0 || n > (1u << 20)) return WGPT_E_INVALID;
-  if (cudaSetDevice(device) != cudaSuccess) return WGPT_E_CUDA;
+  if (wgpt::select_device(device) != cudaSuccess) return WGPT_E_CUDA;
   float* d = nullptr;
   if (cudaMalloc(&d, (size_t)n * 4) != cudaSuccess) return WGPT_E_NOMEM;
   cudaError_t e = wgpt::launch_rng_stream(idx, sample_number, seed, n, d, 0);
@@ -1060,12 +1077,12 @@ int wgpt_set_views(wgpt_ctx* ctx, uint32_t n, const uint32_t* widths, const uint
   for (uint32_t i = 0; i < n; ++i)
     if (widths[i] == 0 || heights[i] == 0 || widths[i] > 16384 || heights[i] > 16384)
       return fail(ctx, WGPT_E_INVALID, "view size must be 1..16384 per side");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "drain before view allocation");
   for (auto& v : ctx->views) { dfree_t(v.accum); dfree_t(v.out); dfree_t(v.gbuf); }
   ctx->views.clear();
   for (uint32_t i = 0; i < n; ++i) {
-    wgpt_ctx::View v{widths[i], heights[i], nullptr, nullptr, nullptr};
+    wgpt_ctx::View v{widths[i], heights[i], nullptr, nullptr, nullptr, 0u};
     size_t np = (size_t)v.w * v.h;
     ctx->views.push_back(v);
     CK(cudaMalloc(&ctx->views.back().accum, np * 16), "cudaMalloc view accumulation");
@@ -1113,13 +1130,14 @@ int wgpt_render_views(wgpt_ctx* ctx, const void* params_112n, const uint32_t* fi
     jv[i].out = v.out;
     jv[i].out_pitch = v.w;
   }
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
   unsigned long long* cnt = ctx->counting ? ctx->d_counters : nullptr;
   wgpt::StageTimer* tm = ctx->timing ? ctx->timer : nullptr;
   CK(wgpt::wf_render(ctx->wf, ctx->ds, ctx->d_pairs_tlas, ctx->d_pairs_bvh, jv.data(), n, ctx->d_status, cnt,
                      ctx->stream, tm, done_ms),
      "batched render");
+  for (uint32_t i = 0; i < n; ++i) ctx->views[i].samples = first_frames[i] + spp[i];
   return WGPT_OK;
 }
 
@@ -1127,7 +1145,7 @@ int wgpt_render_views_gbuffer(wgpt_ctx* ctx, const void* params_112n) {
   if (!ctx || !params_112n) return WGPT_E_INVALID;
   if (!ctx->has_scene) return fail(ctx, WGPT_E_STATE, "no scene uploaded");
   if (ctx->views.empty()) return fail(ctx, WGPT_E_STATE, "no views: call wgpt_set_views first");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   for (size_t i = 0; i < ctx->views.size(); ++i) {
     auto& v = ctx->views[i];
     wgpt_scene_params q;
@@ -1156,7 +1174,7 @@ int wgpt_set_env_sampling(wgpt_ctx* ctx, int mode) {
   if (!ctx || (mode != WGPT_ENV_CDF && mode != WGPT_ENV_ALIAS)) return WGPT_E_INVALID;
   if (mode == WGPT_ENV_ALIAS && !(ctx->has_scene && ctx->has_alias))
     return fail(ctx, WGPT_E_STATE, "no sky alias table uploaded (wgpt_scene_desc.sky_alias)");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "drain");
   ctx->env_mode = mode;
   if (mode == WGPT_ENV_ALIAS) ctx->ds.flags |= wgpt::SCENE_ENV_ALIAS;
@@ -1167,7 +1185,7 @@ int wgpt_set_env_sampling(wgpt_ctx* ctx, int mode) {
 int wgpt_set_accum_f64(wgpt_ctx* ctx, int on) {
   if (!ctx) return WGPT_E_INVALID;
   if (ctx->w == 0) return fail(ctx, WGPT_E_STATE, "no image size: call wgpt_resize first");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "drain");
   dfree_t(ctx->acc64);
   if (on) {
@@ -1186,7 +1204,7 @@ int wgpt_read_accum_f64(wgpt_ctx* ctx, double* dst) {
 int wgpt_write_accum_f64(wgpt_ctx* ctx, const double* src) {
   if (!ctx || !src) return WGPT_E_INVALID;
   if (!ctx->acc64) return fail(ctx, WGPT_E_STATE, "FP64 accumulation is off");
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "drain");
   CK(cudaMemcpy(ctx->acc64, src, (size_t)ctx->w * ctx->h * 64, cudaMemcpyHostToDevice), "write FP64 accumulation");
   return WGPT_OK;
@@ -1208,7 +1226,7 @@ int wgpt_set_wavefront_config(wgpt_ctx* ctx, uint32_t pool_paths, uint64_t units
 int wgpt_set_wavefront_tuning(wgpt_ctx* ctx, const wgpt_wavefront_tuning* t) {
   if (!ctx || !t) return WGPT_E_INVALID;
   if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "drain before retuning");
   if (wgpt::wf_engine_tune(ctx->wf, (int)t->trav_shape, (int)t->shade_block, t->refill_closest, t->refill_shadow,
                            (int)t->shadow_wide))
@@ -1237,7 +1255,7 @@ int wgpt_get_wavefront_config(wgpt_ctx* ctx, uint32_t* pool_paths, uint64_t* uni
 
 int wgpt_set_counting(wgpt_ctx* ctx, int on) {
   if (!ctx) return WGPT_E_INVALID;
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   if (on && !ctx->counting) CK(cudaMemsetAsync(ctx->d_counters, 0, 128 * sizeof(unsigned long long), ctx->stream), "reset counters");
   ctx->counting = on != 0;
   return WGPT_OK;
@@ -1262,7 +1280,7 @@ int wgpt_read_stage_counters(wgpt_ctx* ctx, uint64_t* dst128) {
 
 int wgpt_set_stage_timing(wgpt_ctx* ctx, int on) {
   if (!ctx) return WGPT_E_INVALID;
-  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   if (on && !ctx->timer) {
     ctx->timer = new wgpt::StageTimer();
     for (int i = 0; i < wgpt::StageTimer::kMaxEvents; ++i) CK(cudaEventCreate(&ctx->timer->ev[i]), "cudaEventCreate");

@@ -157,16 +157,41 @@ k_conv3x3_ws(const __grid_constant__ CUtensorMap tmap, ConvGeom g, const uint16_
             mbar_arrive(full_bar(stage));
           }
         } else {
-          // upsampled coarse channels: 16-byte loads into the halo planes
+          // upsampled coarse channels: the tile's 18 x 18 halo is the 2x upsampling of 10 x 10
+          // coarse pixels (fine y = 2 cy + dy, cy from y0 / 2 - 1).  Each coarse value is loaded
+          // once, all of a thread's loads in flight together, and written to its (up to) four
+          // halo positions, zero where the fine position is outside the image.
           const int ci = kt * 16;
-          for (int i = tid; i < 2 * HW * HW; i += LOADER_THREADS) {
-            const int pl = i / (HW * HW), q = i - pl * (HW * HW), hy = q / HW, hx = q - hy * HW;
-            const int y = y0 - 1 + hy, x = x0 - 1 + hx;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (y >= 0 && y < g.h && x >= 0 && x < g.w)
-              v = __ldg(reinterpret_cast<const uint4*>(
-                  g.u + (((size_t)b * g.hc + (y >> 1)) * g.wc + (x >> 1)) * g.cu + ci + pl * 8));
-            *reinterpret_cast<uint4*>(st + pl * PLANE_STRIDE + q * 16) = v;
+          constexpr int CW = HW / 2 + 1, NV = 2 * CW * CW;
+          constexpr int PER = (NV + LOADER_THREADS - 1) / LOADER_THREADS;
+          const int cy0 = (y0 >> 1) - 1, cx0 = (x0 >> 1) - 1;
+          uint4 v[PER];
+#pragma unroll
+          for (int j = 0; j < PER; ++j) {
+            const int i = tid + j * LOADER_THREADS;
+            const int pl = i / (CW * CW), q = i - pl * (CW * CW), cy = cy0 + q / CW, cx = cx0 + q % CW;
+            v[j] = make_uint4(0u, 0u, 0u, 0u);
+            if (i < NV && cy >= 0 && cy < g.hc && cx >= 0 && cx < g.wc)
+              v[j] = __ldg(reinterpret_cast<const uint4*>(g.u + (((size_t)b * g.hc + cy) * g.wc + cx) * g.cu + ci + pl * 8));
+          }
+#pragma unroll
+          for (int j = 0; j < PER; ++j) {
+            const int i = tid + j * LOADER_THREADS;
+            if (i >= NV) break;
+            const int pl = i / (CW * CW), q = i - pl * (CW * CW), qy = q / CW, qx = q % CW;
+#pragma unroll
+            for (int dy = 0; dy < 2; ++dy) {
+              const int hy = 2 * qy - 1 + dy, y = y0 - 1 + hy;
+              if (hy < 0 || hy >= HW) continue;
+#pragma unroll
+              for (int dx = 0; dx < 2; ++dx) {
+                const int hx = 2 * qx - 1 + dx, x = x0 - 1 + hx;
+                if (hx < 0 || hx >= HW) continue;
+                const bool in = y >= 0 && y < g.h && x >= 0 && x < g.w;
+                *reinterpret_cast<uint4*>(st + pl * PLANE_STRIDE + (hy * HW + hx) * 16) =
+                    in ? v[j] : make_uint4(0u, 0u, 0u, 0u);
+              }
+            }
           }
           tc::fence_async_smem();
           if (tid == 0) {

@@ -318,6 +318,7 @@ extern "C" int wgpt_denoise_noalloc(const float* color, const void* gbuf, const 
     if (steps[i] == 0 || steps[i] > (1u << 20)) return WGPT_E_INVALID;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return WGPT_E_CUDA;
+  (void)cudaGetLastError();   // a stale non-sticky error from other code is not this call's
   float4* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);

@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include "../../include/wgpt.h"
+#include "wgpt_internal.h"
 #include "tc_gemm.cuh"
 #include "conv_ws.cuh"
 
@@ -52,7 +53,7 @@ cudaError_t launch_gemm(const LA& la, const LB& lb, const EP& ep, int M, int N, 
 
 extern "C" int wgpt_gemm_bf16(int device, const uint16_t* a, const uint16_t* b, float* c, int m, int n, int k) {
   if (!a || !b || !c || m <= 0 || n <= 0 || k <= 0 || (k % 8) != 0) return WGPT_E_INVALID;
-  if (cudaSetDevice(device) != cudaSuccess) return WGPT_E_CUDA;
+  if (wgpt::select_device(device) != cudaSuccess) return WGPT_E_CUDA;
   uint16_t *da = nullptr, *db = nullptr;
   float* dc = nullptr;
   uint32_t* derr = nullptr;
@@ -533,8 +534,11 @@ struct Crop { int e, oy, ox, pad; };
 
 // Batch gather: features (log1p colour, albedo, normal, depth/(depth+3); 16 channels, BF16),
 // noisy colour and target of each crop pixel.  Dataset images are e x h_img x w_img.
+// Input features of a pixel: log1p colour, albedo, normal, depth / (depth + 3) and the noise
+// level 1 / sqrt(samples per pixel), with the sample count given (samples > 0) or read from the
+// colour's fourth channel (training examples); counts below 1 read as 1.
 __global__ void k_gather(const float4* __restrict__ col, const float* __restrict__ gbuf, const float4* __restrict__ tgt,
-                         int h_img, int w_img, const Crop* __restrict__ crops, int B, int h, int w,
+                         int h_img, int w_img, const Crop* __restrict__ crops, int B, int h, int w, float samples,
                          uint16_t* __restrict__ x0, float4* __restrict__ col_out, float4* __restrict__ tgt_out) {
   const int P = B * h * w;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
@@ -549,8 +553,9 @@ __global__ void k_gather(const float4* __restrict__ col, const float* __restrict
     f[6] = g[0]; f[7] = g[1]; f[8] = g[2];
     float d = fmaxf(g[11], 0.0f);
     f[9] = d / (d + 3.0f);
+    f[10] = 1.0f / sqrtf(fmaxf(samples > 0.0f ? samples : cl.w, 1.0f));
 #pragma unroll
-    for (int i = 10; i < 16; ++i) f[i] = 0.0f;
+    for (int i = 11; i < 16; ++i) f[i] = 0.0f;
     uint32_t wv[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) wv[i] = (uint32_t)f2bf(f[2 * i]) | ((uint32_t)f2bf(f[2 * i + 1]) << 16);
@@ -771,8 +776,10 @@ __global__ void k_weights_bf16(const float* __restrict__ wf, int cout, int taps,
 // normalised 5x5 kernels of stages 2 and 3 (50 floats a pixel).  Two filter kernels apply those,
 // the last one also tonemapping into the rgba8 image.  Every value is computed with the training
 // forward's arithmetic (the same bias add, softmax and tap order), so the images are identical to
-// forward() followed by the tonemap.
+// forward() followed by the tonemap.  The 50 kernel weights are stored as planes (weight k of
+// pixel p at wk23[k * P + p]), so each store and each load of a warp covers 128 contiguous bytes.
 constexpr int WK23 = 50;
+static_assert(WK23 <= LOGITS, "the stored kernels live in the logits buffer (LOGITS floats a pixel)");
 
 template <int N>
 __device__ __forceinline__ void softmax_reg(const float (&lg)[80], int off, float (&wk)[N]) {
@@ -861,13 +868,13 @@ k_out_softmax(const uint16_t* __restrict__ d0, const uint16_t* __restrict__ wb, 
         fx += wk[k] * c.x; fy += wk[k] * c.y; fz += wk[k] * c.z;
       }
       f1[p] = make_float4(fx, fy, fz, 1.0f);
-      float* dst = wk23 + (size_t)p * WK23;
+      float* dst = wk23 + p;
       softmax_reg<25>(lg, 25, wk);
 #pragma unroll
-      for (int k = 0; k < 25; ++k) dst[k] = wk[k];
+      for (int k = 0; k < 25; ++k) __stcs(dst + (size_t)k * P, wk[k]);
       softmax_reg<25>(lg, 50, wk);
 #pragma unroll
-      for (int k = 0; k < 25; ++k) dst[25 + k] = wk[k];
+      for (int k = 0; k < 25; ++k) __stcs(dst + (size_t)(25 + k) * P, wk[k]);
     }
   }
   tc::tc_fence_before();
@@ -875,7 +882,7 @@ k_out_softmax(const uint16_t* __restrict__ d0, const uint16_t* __restrict__ wb, 
   if (warp == 0) tc::tmem_free(tmem, NCOLS);
 }
 
-// A filter stage with stored normalised kernels (25 floats at wk23 + p * 50 + off); with rgba the
+// A filter stage with stored normalised kernels (planes off..off+24 of wk23); with rgba the
 // result is also tonemapped into the rgba8 image with the accumulation pass's display transform
 // (shader.wgsl:2487-2490).
 __global__ void k_filter_stored(const float* __restrict__ wk23, int off, int d, const float4* __restrict__ in,
@@ -884,11 +891,11 @@ __global__ void k_filter_stored(const float* __restrict__ wk23, int off, int d, 
   const int P = B * h * w;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
     const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
-    const float* wk = wk23 + (size_t)p * WK23 + off;
+    const float* wk = wk23 + (size_t)off * P + p;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
 #pragma unroll
     for (int k = 0; k < 25; ++k) {
-      const float wt = wk[k];
+      const float wt = __ldcs(wk + (size_t)k * P);
       float4 c = in[tap_index(b, y, x, k, d, h, w)];
       fx += wt * c.x; fy += wt * c.y; fz += wt * c.z;
     }
@@ -960,7 +967,7 @@ static void set_layer(Layer& l, const char* name, int cu, int cs, int cout, int 
 }
 
 static void define_layers(Net& n) {
-  set_layer(n.L[L_E0A], "E0a", 0, 16, 32, 9, 1, 0, 10, 32);
+  set_layer(n.L[L_E0A], "E0a", 0, 16, 32, 9, 1, 0, 11, 32);
   set_layer(n.L[L_E0], "E0", 0, 32, 32, 9, 1, 0, 32, 32);
   set_layer(n.L[L_E1], "E1", 0, 32, 48, 9, 1, 1, 32, 48);
   set_layer(n.L[L_E2], "E2", 0, 48, 64, 9, 1, 2, 48, 64);
@@ -1359,7 +1366,7 @@ extern "C" {
 
 int wgpt_selftest_wait(int device, uint32_t limit, uint32_t* status, float* ms) {
   if (!status || limit == 0 || limit > (1u << 24)) return WGPT_E_INVALID;
-  if (cudaSetDevice(device) != cudaSuccess) return WGPT_E_CUDA;
+  if (wgpt::select_device(device) != cudaSuccess) return WGPT_E_CUDA;
   uint32_t* d = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int rc = WGPT_OK;
@@ -1387,7 +1394,7 @@ int wgpt_kpcn_create(int device, uint64_t seed, wgpt_kpcn** out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return WGPT_E_CUDA;
   if (device < 0 || device >= ndev) return WGPT_E_INVALID;
-  if (cudaSetDevice(device) != cudaSuccess) return WGPT_E_CUDA;
+  if (wgpt::select_device(device) != cudaSuccess) return WGPT_E_CUDA;
   wgpt_kpcn* k = new wgpt_kpcn();
   kp::Net& n = k->net;
   n.device = device;
@@ -1430,7 +1437,7 @@ int wgpt_kpcn_create(int device, uint64_t seed, wgpt_kpcn** out) {
 int wgpt_kpcn_destroy(wgpt_kpcn* k) {
   if (!k) return WGPT_E_INVALID;
   kp::Net& n = k->net;
-  cudaSetDevice(n.device);
+  wgpt::select_device(n.device);
   if (n.st) cudaStreamSynchronize(n.st);
   for (void* p : n.bufs) cudaFree(p);
   for (int i = 0; i < kp::NLAYERS; ++i) {
@@ -1464,7 +1471,7 @@ int wgpt_kpcn_num_params(wgpt_kpcn* k, uint64_t* n) {
 
 int wgpt_kpcn_get_params(wgpt_kpcn* k, float* dst) {
   if (!k || !dst) return WGPT_E_INVALID;
-  cudaSetDevice(k->net.device);
+  wgpt::select_device(k->net.device);
   KCK(cudaMemcpyAsync(dst, k->net.w, k->net.n_params * 4, cudaMemcpyDeviceToHost, k->net.st), "read params");
   KCK(cudaStreamSynchronize(k->net.st), "synchronize");
   return WGPT_OK;
@@ -1473,7 +1480,7 @@ int wgpt_kpcn_get_params(wgpt_kpcn* k, float* dst) {
 int wgpt_kpcn_set_params(wgpt_kpcn* k, const float* src) {
   if (!k || !src) return WGPT_E_INVALID;
   kp::Net& n = k->net;
-  cudaSetDevice(n.device);
+  wgpt::select_device(n.device);
   KCK(cudaMemcpyAsync(n.w, src, n.n_params * 4, cudaMemcpyHostToDevice, n.st), "write params");
   KCK(cudaMemsetAsync(n.m, 0, n.n_params * 4, n.st), "reset moments");
   KCK(cudaMemsetAsync(n.v, 0, n.n_params * 4, n.st), "reset moments");
@@ -1487,7 +1494,7 @@ int wgpt_kpcn_add_example(wgpt_kpcn* k, const float* noisy, const void* gbuf, co
                           uint32_t h) {
   if (!k || !noisy || !gbuf || !target || w < 16 || h < 16) return WGPT_E_INVALID;
   kp::Net& n = k->net;
-  cudaSetDevice(n.device);
+  wgpt::select_device(n.device);
   if (n.ds_n > 0 && ((int)w != n.ds_w || (int)h != n.ds_h))
     return kfail(k, WGPT_E_INVALID, "every example must have the size of the first");
   const size_t npix = (size_t)w * h;
@@ -1532,7 +1539,7 @@ int wgpt_kpcn_train(wgpt_kpcn* k, uint32_t steps, uint32_t batch, uint32_t crop,
   if (n.ds_n == 0) return kfail(k, WGPT_E_STATE, "no training examples");
   if ((int)crop > n.ds_w || (int)crop > n.ds_h) return kfail(k, WGPT_E_INVALID, "crop larger than the examples");
   if (steps == 0) return WGPT_OK;
-  cudaSetDevice(n.device);
+  wgpt::select_device(n.device);
   KCK(kp::ensure_batch(n, (int)batch, (int)crop, (int)crop), "batch buffers");
   if (k->losses_cap < (int)steps) {
     cudaFree(k->d_losses);
@@ -1546,7 +1553,7 @@ int wgpt_kpcn_train(wgpt_kpcn* k, uint32_t steps, uint32_t batch, uint32_t crop,
   for (uint32_t it = 0; it < steps; ++it) {
     kp::k_gather<<<kp::grid1(P), 256, 0, n.st>>>(n.ds_col, n.ds_gbuf, n.ds_tgt, n.ds_h, n.ds_w,
                                                  k->d_crops + (size_t)it * batch, (int)batch, (int)crop, (int)crop,
-                                                 n.x0, n.col, n.tgt);
+                                                 0.0f, n.x0, n.col, n.tgt);
     KCK(kp::forward(n), "forward");
     KCK(kp::backward(n), "backward");
     KCK(cudaMemcpyAsync(k->d_losses + it, n.loss, 4, cudaMemcpyDeviceToDevice, n.st), "loss copy");
@@ -1568,13 +1575,13 @@ int wgpt_kpcn_grads(wgpt_kpcn* k, uint32_t batch, uint32_t crop, uint64_t seed, 
     cudaGetLastError();
     return kfail(k, WGPT_E_INVALID, "dev_grads must be device memory on the denoiser's device");
   }
-  cudaSetDevice(n.device);
+  wgpt::select_device(n.device);
   KCK(kp::ensure_batch(n, (int)batch, (int)crop, (int)crop), "batch buffers");
   int rc = draw_crops(k, batch, crop, seed);
   if (rc) return rc;
   const size_t P = (size_t)batch * crop * crop;
   kp::k_gather<<<kp::grid1(P), 256, 0, n.st>>>(n.ds_col, n.ds_gbuf, n.ds_tgt, n.ds_h, n.ds_w, k->d_crops, (int)batch,
-                                               (int)crop, (int)crop, n.x0, n.col, n.tgt);
+                                               (int)crop, (int)crop, 0.0f, n.x0, n.col, n.tgt);
   KCK(kp::forward(n), "forward");
   KCK(kp::backward(n), "backward");
   KCK(cudaMemcpyAsync(dev_grads, n.g, n.n_params * 4, cudaMemcpyDeviceToDevice, n.st), "gradient copy");
@@ -1592,7 +1599,7 @@ int wgpt_kpcn_apply(wgpt_kpcn* k, const float* dev_grads, float scale, float lr)
     cudaGetLastError();
     return kfail(k, WGPT_E_INVALID, "dev_grads must be device memory on the denoiser's device");
   }
-  cudaSetDevice(n.device);
+  wgpt::select_device(n.device);
   KCK(adam_step(n, lr, dev_grads, scale), "adam");
   KCK(cudaStreamSynchronize(n.st), "synchronize");
   return check_device_error(k);
@@ -1602,7 +1609,7 @@ int wgpt_kpcn_loss_and_grads(wgpt_kpcn* k, const float* noisy, const void* gbuf,
                              uint32_t h, float* loss, float* grads, float* out_rgba32f) {
   if (!k || !noisy || !gbuf || !target || w < 16 || h < 16 || w > 4096 || h > 4096) return WGPT_E_INVALID;
   kp::Net& n = k->net;
-  cudaSetDevice(n.device);
+  wgpt::select_device(n.device);
   const size_t npix = (size_t)w * h;
   int rc = stage_images(k, npix);
   if (rc) return rc;
@@ -1615,7 +1622,7 @@ int wgpt_kpcn_loss_and_grads(wgpt_kpcn* k, const float* noisy, const void* gbuf,
   KCK(cudaMemcpyAsync(k->d_img_tgt, target, npix * 16, cudaMemcpyHostToDevice, n.st), "upload image");
   KCK(cudaMemcpyAsync(k->d_img_gbuf, gbuf, npix * 48, cudaMemcpyHostToDevice, n.st), "upload image");
   kp::k_gather<<<kp::grid1(npix), 256, 0, n.st>>>(k->d_img_col, k->d_img_gbuf, k->d_img_tgt, (int)h, (int)w,
-                                                  k->d_crops, 1, (int)h, (int)w, n.x0, n.col, n.tgt);
+                                                  k->d_crops, 1, (int)h, (int)w, 0.0f, n.x0, n.col, n.tgt);
   KCK(kp::forward(n), "forward");
   KCK(kp::backward(n), "backward");
   if (loss) KCK(cudaMemcpyAsync(loss, n.loss, 4, cudaMemcpyDeviceToHost, n.st), "loss readback");
@@ -1631,7 +1638,7 @@ static int denoise_image(wgpt_kpcn* k, wgpt_ctx* ctx, int view, float exposure, 
   if (!wgpt::ctx_images(ctx, view, &im)) return kfail(k, WGPT_E_STATE, "no such image (resize or set views first)");
   if (!im.gbuf) return kfail(k, WGPT_E_STATE, "context has no G-buffer: resize with want_gbuf and render it");
   if (im.device != n.device) return kfail(k, WGPT_E_INVALID, "context and denoiser are on different devices");
-  cudaSetDevice(n.device);
+  wgpt::select_device(n.device);
   const size_t npix = (size_t)im.w * im.h;
   int rc = ensure_crops(k, 1);
   if (rc) return rc;
@@ -1643,7 +1650,8 @@ static int denoise_image(wgpt_kpcn* k, wgpt_ctx* ctx, int view, float exposure, 
   KCK(cudaEventRecord(k->ev_in, im.stream), "event");
   KCK(cudaStreamWaitEvent(n.st, k->ev_in, 0), "event wait");
   kp::k_gather<<<kp::grid1(npix), 256, 0, n.st>>>((const float4*)im.accum, im.gbuf, nullptr, (int)im.h, (int)im.w,
-                                                  k->d_crops, 1, (int)im.h, (int)im.w, n.x0, n.col, nullptr);
+                                                  k->d_crops, 1, (int)im.h, (int)im.w, (float)std::max(im.samples, 1u),
+                                                  n.x0, n.col, nullptr);
   KCK(kp::forward(n, (uchar4*)im.out, exposure), "forward");
   KCK(cudaGetLastError(), "denoise launch");
   KCK(cudaEventRecord(k->ev_out, n.st), "event");

@@ -8,6 +8,15 @@ struct wgpt_ctx;
 
 namespace wgpt {
 
+// Selects the device and drops a non-sticky error left in this thread's runtime state by code
+// outside this library, so that the cudaGetLastError() after each of the library's launches
+// reports that launch alone (a sticky error is returned again by the next runtime call).
+inline cudaError_t select_device(int device) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) (void)cudaGetLastError();
+  return e;
+}
+
 // The images of a context (for the learned denoiser, which reads the accumulation and the
 // G-buffer and writes the rgba8 image).
 struct CtxImages {
@@ -17,6 +26,7 @@ struct CtxImages {
   float* gbuf;
   uint8_t* out;
   cudaStream_t stream;
+  uint32_t samples;   // samples per pixel in the accumulation (0: unknown)
 };
 bool ctx_images(::wgpt_ctx* ctx, int view, CtxImages* out);   // view -1: the main image
 

@@ -266,32 +266,44 @@ def time_to_rmse(args) -> dict:
     """Time to display-space RMSE <= threshold against an FP64-accumulated reference of
     --ref-spp samples, on the flagship workload itself (1920x1080, 8 bounces, seed 1, the bench's
     scene and camera): plain accumulation plus the a-trous filter against accumulation plus the
-    learned denoiser.  The network is trained here, on the GPU, from pairs this tracer renders:
-    flagship-family scenes (seeds 1000.., their own cameras) as 256x256 windows of their 1080p
-    views, inputs at 1/2/4/8 spp, targets at --kpcn-target-spp with an independent stream; the
-    flagship scene and the held-out evaluation scenes (seeds 5000..) are not trained on."""
+    learned denoiser.  The network's weights were trained on the GPU by train_denoiser from pairs
+    this tracer renders (the package's flagship weights, whose recipe is stored with them), or
+    with --kpcn-train here: flagship-family scenes (seeds 1000.., their own cameras) as 256x256
+    windows of their 1080p views, inputs at --kpcn-spps, targets at --kpcn-target-spp with an
+    independent stream.  The flagship scene and the held-out evaluation scenes (seeds 5000..) are
+    not trained on."""
     import torch
-    from webgpuraytracer_b200 import kpcn
+    from webgpuraytracer_b200 import kpcn, train_denoiser
     from webgpuraytracer_b200 import renderer as rd
     from webgpuraytracer_b200 import scene as sc
     W, H, thr = WIDTH, HEIGHT, args.rmse_threshold
     out = {"threshold": thr, "space": "display (shader.wgsl tonemap, exposure 1); linear RMSE reported beside it",
            "scene": f"flagship workload, seed 1, {W}x{H}, {BOUNCES} bounces (held out of training)",
            "reference": f"{args.ref_spp} spp, FP64 Welford accumulation"}
-    t0 = time.perf_counter()
     k = kpcn.Kpcn(0, seed=1)
-    n_ex = kpcn.build_flagship_training_set(k, range(1000, 1000 + args.kpcn_scenes), crops=args.kpcn_crops,
-                                            target_spp=args.kpcn_target_spp, bounces=BOUNCES)
-    t_data = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    losses = k.train(args.kpcn_steps, batch=16, crop=128, lr=1e-3, seed=1)
-    t_train = time.perf_counter() - t0
-    out["training"] = {"family": "flagship (seeded instances, primitives, Disney materials, sun sky, seeded cameras)",
-                       "scenes": args.kpcn_scenes, "windows_per_scene": args.kpcn_crops, "window": "256x256 of 1920x1080",
-                       "examples": n_ex, "input_spp": [1, 2, 4, 8], "target_spp": args.kpcn_target_spp,
-                       "steps": args.kpcn_steps, "batch": "16 x 128^2 crops", "data_s": t_data, "train_s": t_train,
-                       "loss_first_50": float(np.mean(losses[:50])), "loss_last_50": float(np.mean(losses[-50:])),
-                       "params": k.n_params}
+    weights = Path(args.kpcn_weights) if args.kpcn_weights else kpcn.WEIGHTS_DIR / "kpcn_flagship.npz"
+    if weights.exists() and not args.kpcn_train:
+        # weights trained on the GPU by train_denoiser (the recipe travels inside the file)
+        meta = kpcn.load_weights(k, weights)
+        out["training"] = {"source": "pretrained", "file": str(weights.relative_to(ROOT))
+                           if weights.is_relative_to(ROOT) else str(weights), "params": k.n_params, **meta}
+    else:
+        t0 = time.perf_counter()
+        spps = tuple(int(v) for v in args.kpcn_spps.split(","))
+        n_ex = kpcn.build_flagship_training_set(k, range(1000, 1000 + args.kpcn_scenes), crops=args.kpcn_crops,
+                                                spps=spps, target_spp=args.kpcn_target_spp, bounces=BOUNCES)
+        t_data = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        losses = train_denoiser.train(k, args.kpcn_steps, 16, 128, 1e-3, args.kpcn_schedule)
+        t_train = time.perf_counter() - t0
+        out["training"] = {"source": "trained in this run",
+                           "family": "flagship (seeded instances, primitives, Disney materials, sun sky, seeded cameras)",
+                           "scenes": args.kpcn_scenes, "windows_per_scene": args.kpcn_crops,
+                           "window": "256x256 of 1920x1080", "examples": n_ex, "input_spp": list(spps),
+                           "target_spp": args.kpcn_target_spp, "steps": args.kpcn_steps, "schedule": args.kpcn_schedule,
+                           "batch": "16 x 128^2 crops", "data_s": t_data, "train_s": t_train,
+                           "loss_first_50": float(np.mean(losses[:50])), "loss_last_50": float(np.mean(losses[-50:])),
+                           "params": k.n_params}
     out["held_out"] = held_out_eval(k, args)
 
     scene, packed = build_workload()
@@ -1024,6 +1036,10 @@ def main():
     ap.add_argument("--kpcn-crops", type=int, default=2, help="256x256 training windows per scene")
     ap.add_argument("--kpcn-target-spp", type=int, default=1024)
     ap.add_argument("--kpcn-steps", type=int, default=3000)
+    ap.add_argument("--kpcn-spps", default="1,2,4,8,16,32,64", help="input samples per pixel of in-run training")
+    ap.add_argument("--kpcn-schedule", default="0.65:1,0.2:0.3,0.15:0.1", help="lr phases of in-run training")
+    ap.add_argument("--kpcn-weights", default="", help="trained weights (.npz; default: the package's flagship weights)")
+    ap.add_argument("--kpcn-train", action="store_true", help="train the network in this run even if weights exist")
     ap.add_argument("--max-nn-spp", type=int, default=256, help="largest sample count the network is evaluated at")
     ap.add_argument("--workload", choices=["flagship", "batch", "denoise"], default="flagship",
                     help="flagship: 1080p 64 spp; batch: 32 uneven views of the 5.24 M-triangle scene; "

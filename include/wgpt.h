@@ -236,7 +236,9 @@ int wgpt_gemm_bf16(int device, const uint16_t* a, const uint16_t* b, float* c, i
    filters per pixel, applied to the noisy colour as
    a cascade at dilations 1, 2 and 4 (29 x 29 footprint).  BF16
    weights and activations, FP32 accumulation on the tensor cores, FP32 master weights trained
-   by Adam on the relative L2 loss sum((f-t)^2/(t^2+0.01))/(3 pixels).  Parameters are one flat
+   by Adam on the relative L2 loss sum((f-t)^2/(t^2+0.01))/(3 pixels), each step's gradient
+   clipped to 4x the running mean of past gradient norms (a step with a non-finite gradient is
+   skipped; wgpt_kpcn_set_params resets the moments and the running mean).  Parameters are one flat
    FP32 array, per layer W[cout][taps][cin] then bias[cout] (layer table in kpcn.cu).
    Examples are (noisy rgba32f, 48-byte G-buffer, target rgba32f) images of one common size; the
    noisy image's fourth channel is its samples per pixel (values below 1 read as 1);

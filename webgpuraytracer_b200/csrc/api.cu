@@ -1039,7 +1039,8 @@ int wgpt_sample_env(wgpt_ctx* ctx, const float* u2, uint32_t n, uint32_t* texel_
   if (n > (1u << 24)) return fail(ctx, WGPT_E_INVALID, "at most 2^24 samples per call");
   CK(wgpt::select_device(ctx->device), "cudaSetDevice");
   void* d = nullptr;
-  CK(cudaMalloc(&d, (size_t)n * 16), "cudaMalloc env samples");
+  // per sample: u (2 floats), texel (2 uint32), pdf (1 float)
+  CK(cudaMalloc(&d, (size_t)n * 20), "cudaMalloc env samples");
   float* d_u = (float*)d;
   uint32_t* d_t = (uint32_t*)(d_u + (size_t)n * 2);
   float* d_p = (float*)(d_t + (size_t)n * 2);

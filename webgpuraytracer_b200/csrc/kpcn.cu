@@ -743,10 +743,43 @@ __global__ void k_bias_grad(const uint16_t* __restrict__ dz, int P, int C, float
 }
 
 // Adam (bias-corrected) over the flat FP32 parameters, with the gradient g * scale.
-__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
-                       size_t n, float lr, float b1, float b2, float eps, float c1, float c2, float scale) {
+// Gradient clipping by global norm: the squared norm of g * scale is summed into clip[0]; then
+// k_clip_factor turns it into the step's factor clip[2]: 1, or kClipRatio times the running mean
+// of past step norms (clip[1]) over this norm when the norm is above that (a batch whose noisy
+// input holds a firefly of the sun can carry a gradient thousands of times the usual one), or 0
+// for a non-finite norm (the step is skipped).  The first step sets the running mean.
+constexpr float kClipRatio = 4.0f;
+
+__global__ void k_grad_sqnorm(const float* __restrict__ g, size_t n, float scale, float* __restrict__ clip) {
+  float s = 0.0f;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    float gi = g[i] * scale;
+    const float v = g[i] * scale;
+    s += v * v;
+  }
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(clip, s);
+}
+
+__global__ void k_clip_factor(float* __restrict__ clip) {
+  const float norm = sqrtf(clip[0]);
+  clip[0] = 0.0f;
+  if (!isfinite(norm)) {
+    clip[2] = 0.0f;
+    return;
+  }
+  const float mean = clip[1] > 0.0f ? clip[1] : norm;
+  const float lim = kClipRatio * mean;
+  clip[2] = norm > lim ? lim / norm : 1.0f;
+  clip[1] = 0.98f * mean + 0.02f * fminf(norm, lim);
+}
+
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       size_t n, float lr, float b1, float b2, float eps, float c1, float c2, float scale,
+                       const float* __restrict__ clip) {
+  const float f = clip[2];
+  if (f == 0.0f) return;   // non-finite gradient: no step
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    float gi = g[i] * scale * f;
     float mi = b1 * m[i] + (1.0f - b1) * gi;
     float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
     m[i] = mi;
@@ -952,6 +985,7 @@ struct Net {
   uint16_t *dlog = nullptr, *dx = nullptr, *g_a = nullptr, *g_b = nullptr, *g_pool = nullptr, *g_skip = nullptr;
   std::vector<void*> bufs;
   float* loss = nullptr;
+  float* clip = nullptr;   // gradient clipping: squared norm, running mean of norms, step factor
   Crop* crops = nullptr;
   int crops_cap = 0;
   // dataset
@@ -1323,8 +1357,10 @@ cudaError_t adam_step(kp::Net& n, float lr, const float* g = nullptr, float scal
   n.adam_t += 1;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.0f - (float)std::pow(0.9, n.adam_t), c2 = 1.0f - (float)std::pow(0.999, n.adam_t);
+  kp::k_grad_sqnorm<<<kp::grid1(n.n_params), 256, 0, n.st>>>(g ? g : n.g, n.n_params, scale, n.clip);
+  kp::k_clip_factor<<<1, 1, 0, n.st>>>(n.clip);
   kp::k_adam<<<kp::grid1(n.n_params), 256, 0, n.st>>>(n.w, g ? g : n.g, n.m, n.v, n.n_params, lr, b1, b2, 1e-8f, c1,
-                                                      c2, scale);
+                                                      c2, scale, n.clip);
   return kp::refresh_bf16(n);
 }
 
@@ -1406,6 +1442,8 @@ int wgpt_kpcn_create(int device, uint64_t seed, wgpt_kpcn** out) {
   if (e == cudaSuccess) e = cudaMalloc(&n.v, n.n_params * 4);
   if (e == cudaSuccess) e = cudaMalloc(&n.err, 4);
   if (e == cudaSuccess) e = cudaMalloc(&n.loss, 4);
+  if (e == cudaSuccess) e = cudaMalloc(&n.clip, 16);
+  if (e == cudaSuccess) e = cudaMemset(n.clip, 0, 16);
   for (int i = 0; i < kp::NLAYERS && e == cudaSuccess; ++i) {
     e = cudaMalloc(&n.L[i].wb, n.L[i].nw() * 2);
     if (e == cudaSuccess) e = cudaMalloc(&n.L[i].wt, n.L[i].nw() * 2);
@@ -1443,7 +1481,7 @@ int wgpt_kpcn_destroy(wgpt_kpcn* k) {
   for (int i = 0; i < kp::NLAYERS; ++i) {
     cudaFree(n.L[i].wb); cudaFree(n.L[i].wt); cudaFree(n.L[i].wpk); cudaFree(n.L[i].wtpk);
   }
-  cudaFree(n.w); cudaFree(n.g); cudaFree(n.m); cudaFree(n.v); cudaFree(n.err); cudaFree(n.loss);
+  cudaFree(n.w); cudaFree(n.g); cudaFree(n.m); cudaFree(n.v); cudaFree(n.err); cudaFree(n.loss); cudaFree(n.clip);
   cudaFree(n.ds_col); cudaFree(n.ds_tgt); cudaFree(n.ds_gbuf);
   cudaFree(k->d_losses); cudaFree(k->d_crops);
   cudaFree(k->d_img_col); cudaFree(k->d_img_tgt); cudaFree(k->d_img_gbuf);
@@ -1484,6 +1522,7 @@ int wgpt_kpcn_set_params(wgpt_kpcn* k, const float* src) {
   KCK(cudaMemcpyAsync(n.w, src, n.n_params * 4, cudaMemcpyHostToDevice, n.st), "write params");
   KCK(cudaMemsetAsync(n.m, 0, n.n_params * 4, n.st), "reset moments");
   KCK(cudaMemsetAsync(n.v, 0, n.n_params * 4, n.st), "reset moments");
+  KCK(cudaMemsetAsync(n.clip, 0, 16, n.st), "reset clipping");
   n.adam_t = 0;
   KCK(kp::refresh_bf16(n), "bf16 weights");
   KCK(cudaStreamSynchronize(n.st), "synchronize");

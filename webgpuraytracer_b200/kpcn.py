@@ -8,7 +8,9 @@ image metrics used to compare it with the a-trous filter.
 from __future__ import annotations
 
 import ctypes as C
+import json
 from dataclasses import dataclass
+from pathlib import Path
 
 import numpy as np
 
@@ -163,6 +165,22 @@ class Kpcn:
         self._check(self.L.wgpt_kpcn_denoise_view(self.h, r.ctx, view, exposure, ptr(lin) if want_linear else None),
                     "denoise_view")
         return lin
+
+
+WEIGHTS_DIR = Path(__file__).resolve().parent / "weights"
+
+
+def save_weights(k: Kpcn, path, meta: dict) -> None:
+    """Writes the network's FP32 parameters and a JSON description of how they were trained
+    (an .npz with arrays `params` and `meta`)."""
+    np.savez_compressed(path, params=k.get_params(), meta=np.array(json.dumps(meta)))
+
+
+def load_weights(k: Kpcn, path) -> dict:
+    """Loads parameters written by save_weights into `k`; returns their training description."""
+    with np.load(path, allow_pickle=False) as f:
+        k.set_params(f["params"])
+        return json.loads(str(f["meta"]))
 
 
 def render_example(scene: sc.Scene, size: int, spp: int, target_spp: int, seed: int = 1, target_seed: int = 977):

@@ -50,11 +50,12 @@ BYTES_PER_UNIT = {
     11: 32,   # hit attributes of the winning primitive (normals)
 }
 PIXEL_BYTES = 16 + 16 + 4   # accumulation read + write, rgba8 store
-# DRAM bytes (read + write) per closest-hit ray of this workload: 502 MB per steady-state launch of
-# a 2,097,152-slot pool (every slot holds a live path while units remain, so 2,097,152 rays per
-# launch), from an ncu capture of this workload (bench.py cannot run ncu itself).
-# A launch's traffic is this times its rays.
-EXTEND_DRAM_BYTES_PER_RAY = 5.02e8 / 2_097_152
+# DRAM bytes (read + write) per closest-hit ray of this workload, from ncu captures of this
+# workload (bench.py cannot run ncu itself): 2,077 MB per steady-state launch of an
+# 8,388,608-slot pool (every slot holds a live path while units remain, so 8,388,608 rays per
+# launch; mean of launches 13-15: 248 B per ray); a 2,097,152-slot pool gives 250 B per ray, so
+# the traffic scales with the rays, not the pool.  A launch's traffic is this times its rays.
+EXTEND_DRAM_BYTES_PER_RAY = 2.0771e9 / 8_388_608
 KERNELS = ["k_wf_fill", "k_wf_extend", "k_wf_shade", "k_wf_shadow", "k_wf_resolve", "k_wf_shade_miss",
            "k_wf_accumulate", "k_wf_control"]
 
@@ -745,8 +746,8 @@ def run_ours(args):
                          / 1e9 / peaks["hbm_gbs"],
                          "traffic_source": None if mega else
                          "ncu dram__bytes_read.sum + dram__bytes_write.sum of steady-state k_wf_extend launches "
-                         "of a 2,097,152-slot pool (mean of launches 21-23 of this workload's stage-timing pass: "
-                         "239 B per ray), times this run's closest-hit rays per launch",
+                         "of an 8,388,608-slot pool (mean of launches 13-15: 248 B per ray; a 2,097,152-slot pool "
+                         "gives 250 B per ray), times this run's closest-hit rays per launch",
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",
                          "kernel": "k_render" if mega else KERNELS[dom],

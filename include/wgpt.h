@@ -231,25 +231,20 @@ int wgpt_gemm_bf16(int device, const uint16_t* a, const uint16_t* b, float* c, i
 
 /* Learned kernel-predicting denoiser (no counterpart in the reference, whose only denoiser is
    the a-trous filter, which stays the fallback).  A 5-level encoder-decoder (32/48/64/96/128
-   channels, ~0.73 M parameters) over 11 features of the accumulation and G-buffer (log colour,
-   albedo, normal, depth, and the noise level 1 / sqrt(samples per pixel)) predicts three 5x5
-   filters per pixel, applied to the noisy colour as
+   channels, ~0.73 M parameters) over 10 features of the accumulation and G-buffer (log colour,
+   albedo, normal, depth) predicts three 5x5 filters per pixel, applied to the noisy colour as
    a cascade at dilations 1, 2 and 4 (29 x 29 footprint).  BF16
    weights and activations, FP32 accumulation on the tensor cores, FP32 master weights trained
    by Adam on the relative L2 loss sum((f-t)^2/(t^2+0.01))/(3 pixels), each step's gradient
    clipped to 4x the running mean of past gradient norms (a step with a non-finite gradient is
    skipped; wgpt_kpcn_set_params resets the moments and the running mean).  Parameters are one flat
    FP32 array, per layer W[cout][taps][cin] then bias[cout] (layer table in kpcn.cu).
-   Examples are (noisy rgba32f, 48-byte G-buffer, target rgba32f) images of one common size; the
-   noisy image's fourth channel is its samples per pixel (values below 1 read as 1);
+   Examples are (noisy rgba32f, 48-byte G-buffer, target rgba32f) images of one common size;
    training samples `batch` random crops of crop x crop pixels per step (losses: steps floats).
    wgpt_kpcn_loss_and_grads evaluates one whole image (for gradient checks).  wgpt_kpcn_denoise
    filters a context's accumulation with its G-buffer into its rgba8 image (tonemapped with
    `exposure`), ordered after the context's queued work; filtered (nullable, host) receives the
-   linear result.  The samples per pixel of a context image are first_frame + reps of its last
-   wgpt_render (first_frames[i] + spp[i] of wgpt_render_views), zero after wgpt_resize, or what
-   wgpt_set_accum_samples declares (view -1: the main image; for images written with
-   wgpt_write_accum). */
+   linear result. */
 typedef struct wgpt_kpcn wgpt_kpcn;
 int wgpt_kpcn_create(int device, uint64_t seed, wgpt_kpcn** out);
 int wgpt_kpcn_destroy(wgpt_kpcn* k);
@@ -283,7 +278,6 @@ enum { WGPT_KPCN_CONV_PIPELINED = 0, WGPT_KPCN_CONV_PER_TILE = 1 };
 int wgpt_kpcn_set_conv_mode(wgpt_kpcn* k, int mode);
 int wgpt_kpcn_denoise(wgpt_kpcn* k, wgpt_ctx* ctx, float exposure, float* filtered_rgba32f);
 int wgpt_kpcn_denoise_view(wgpt_kpcn* k, wgpt_ctx* ctx, uint32_t view, float exposure, float* filtered_rgba32f);
-int wgpt_set_accum_samples(wgpt_ctx* ctx, int32_t view, uint32_t samples);
 
 /* Closest hit of caller rays (trace_scene, shader.wgsl:754-774) for parity tests: rays are n x
    (origin, direction) floats; outputs object index, material index, global triangle index

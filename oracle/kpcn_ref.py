@@ -2,8 +2,7 @@
 loss and gradients, used only by tests to check the tensor-core kernels.
 
 It follows kpcn.cu's definition layer by layer: features (log1p colour, albedo, normal,
-depth/(depth+3), 1/sqrt(samples per pixel), zero-padded to 16 channels), 3x3 convolutions
-with zero padding, 2x2 average pooling whose mean leaves out children beyond an odd edge,
+depth/(depth+3), zero-padded to 16 channels), 3x3 convolutions with zero padding, 2x2 average pooling whose mean leaves out children beyond an odd edge,
 nearest 2x upsampling cropped to the skip tensor's size, [upsampled, skip] concatenation, a 1x1 output convolution whose channels
 [25s, 25s + 25) are softmax-normalised into the 5x5 filter of stage s, the three stages applied
 in turn at dilations 1, 2, 4 with clamp-to-edge neighbours, starting from the noisy colour, and
@@ -68,8 +67,6 @@ def features(noisy: np.ndarray, gbuf: np.ndarray) -> np.ndarray:
     f[..., 6:9] = gbuf[..., 0:3]
     d = np.maximum(gbuf[..., 11], 0.0)
     f[..., 9] = d / (d + 3.0)
-    # the noise level: 1 / sqrt(samples per pixel), the count in the colour's fourth channel
-    f[..., 10] = np.float32(1.0) / np.sqrt(np.maximum(noisy[..., 3].astype(np.float32), np.float32(1.0)))
     return f
 
 

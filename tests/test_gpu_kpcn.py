@@ -59,7 +59,7 @@ def test_kpcn_layout_and_params_roundtrip():
     p = k.get_params()
     sl = kpcn.param_slices()
     w0 = p[sl["E0a"][0]].reshape(32, 9, 16)
-    assert np.all(w0[:, :, 11:] == 0.0), "padded input channels start at zero"
+    assert np.all(w0[:, :, 10:] == 0.0), "padded input channels start at zero"
     wo = p[sl["OUT"][0]].reshape(80, 32)
     assert np.all(wo[75:] == 0.0), "padded logits start at zero"
     q = p * 0.5
@@ -150,7 +150,7 @@ def test_kpcn_training_gains_over_atrous():
     s = synth.small_scene(1, size, size, 4)
     r = rd.Renderer(size, size)
     r.set_scene(s, isgbuf=True)
-    r.write_accum(noisy, samples=spp)
+    r.write_accum(noisy)
     r.write_gbuffer(gbuf)
     lin = k.denoise(r, exposure=1.0)
     dn = rd.Denoiser(r, passes=4)

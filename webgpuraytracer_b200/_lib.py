@@ -126,7 +126,6 @@ EXPORTS = {
     "wgpt_read_view": ([_P, C.c_uint32, _P, _P], C.c_int),
     "wgpt_render_views_gbuffer": ([_P, _P], C.c_int),
     "wgpt_kpcn_denoise_view": ([_P, _P, C.c_uint32, C.c_float, _P], C.c_int),
-    "wgpt_set_accum_samples": ([_P, C.c_int32, C.c_uint32], C.c_int),
     "wgpt_get_wavefront_config": ([_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)], C.c_int),
     "wgpt_denoise_noalloc": ([_P, _P, _P, _P, _U32, _P, _P, _P], C.c_int),
     "wgpt_set_counting": ([_P, C.c_int], C.c_int),

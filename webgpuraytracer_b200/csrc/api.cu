@@ -33,7 +33,6 @@ struct wgpt_ctx {
   float* accum = nullptr;
   uint8_t* out = nullptr;
   float* gbuf = nullptr;
-  uint32_t samples = 0;   // samples per pixel in accum: first_frame + reps of the last render
   // denoiser
   float* dn_a = nullptr;
   float* dn_b = nullptr;
@@ -60,7 +59,7 @@ struct wgpt_ctx {
   bool timing = false;
   wgpt::WfEngine* wf = nullptr;   // wavefront renderer: path pool, sample buffer, loop graph
   // batched views: size and images of each
-  struct View { uint32_t w, h; float* accum; uint8_t* out; float* gbuf; uint32_t samples; };
+  struct View { uint32_t w, h; float* accum; uint8_t* out; float* gbuf; };
   std::vector<View> views;
   double* acc64 = nullptr;        // optional FP64 Welford accumulation (8 doubles per pixel)
   // kept from the last full upload for the objects fast path: the (node, triangle) offset
@@ -523,7 +522,6 @@ bool wgpt::ctx_images(wgpt_ctx* ctx, int view, wgpt::CtxImages* out) {
     out->accum = ctx->accum;
     out->gbuf = ctx->gbuf;
     out->out = ctx->out;
-    out->samples = ctx->samples;
     return true;
   }
   if ((size_t)view >= ctx->views.size()) return false;
@@ -533,7 +531,6 @@ bool wgpt::ctx_images(wgpt_ctx* ctx, int view, wgpt::CtxImages* out) {
   out->accum = v.accum;
   out->gbuf = v.gbuf;
   out->out = v.out;
-  out->samples = v.samples;
   return true;
 }
 
@@ -786,7 +783,6 @@ int wgpt_resize(wgpt_ctx* ctx, uint32_t width, uint32_t height, int want_gbuf) {
   if (had_f64 && !ctx->acc64) CK(cudaMalloc(&ctx->acc64, npix * 64), "cudaMalloc FP64 accumulation");
   if (ctx->acc64) CK(cudaMemsetAsync(ctx->acc64, 0, npix * 64, ctx->stream), "clear FP64 accumulation");
   ctx->w = width; ctx->h = height;
-  ctx->samples = 0;
   CK(cudaStreamSynchronize(ctx->stream), "resize");
   return WGPT_OK;
 }
@@ -816,7 +812,6 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
                            ctx->d_status, cnt, ctx->stream),
        "render launch");
     if (tm) tm->end(0, ctx->stream);
-    ctx->samples = first_frame + reps;
     return WGPT_OK;
   }
   if (!ctx->wf) ctx->wf = wgpt::wf_engine_create();
@@ -832,18 +827,6 @@ int wgpt_render(wgpt_ctx* ctx, uint32_t first_frame, uint32_t reps, uint32_t sx,
   CK(wgpt::wf_render(ctx->wf, ctx->ds, ctx->d_pairs_tlas, ctx->d_pairs_bvh, &v, 1, ctx->d_status, cnt, ctx->stream,
                      tm),
      "wavefront render");
-  ctx->samples = first_frame + reps;
-  return WGPT_OK;
-}
-
-int wgpt_set_accum_samples(wgpt_ctx* ctx, int32_t view, uint32_t samples) {
-  if (!ctx) return WGPT_E_INVALID;
-  if (view < 0) {
-    ctx->samples = samples;
-    return WGPT_OK;
-  }
-  if ((size_t)view >= ctx->views.size()) return fail(ctx, WGPT_E_INVALID, "no such view");
-  ctx->views[(size_t)view].samples = samples;
   return WGPT_OK;
 }
 
@@ -1083,7 +1066,7 @@ int wgpt_set_views(wgpt_ctx* ctx, uint32_t n, const uint32_t* widths, const uint
   for (auto& v : ctx->views) { dfree_t(v.accum); dfree_t(v.out); dfree_t(v.gbuf); }
   ctx->views.clear();
   for (uint32_t i = 0; i < n; ++i) {
-    wgpt_ctx::View v{widths[i], heights[i], nullptr, nullptr, nullptr, 0u};
+    wgpt_ctx::View v{widths[i], heights[i], nullptr, nullptr, nullptr};
     size_t np = (size_t)v.w * v.h;
     ctx->views.push_back(v);
     CK(cudaMalloc(&ctx->views.back().accum, np * 16), "cudaMalloc view accumulation");
@@ -1138,7 +1121,6 @@ int wgpt_render_views(wgpt_ctx* ctx, const void* params_112n, const uint32_t* fi
   CK(wgpt::wf_render(ctx->wf, ctx->ds, ctx->d_pairs_tlas, ctx->d_pairs_bvh, jv.data(), n, ctx->d_status, cnt,
                      ctx->stream, tm, done_ms),
      "batched render");
-  for (uint32_t i = 0; i < n; ++i) ctx->views[i].samples = first_frames[i] + spp[i];
   return WGPT_OK;
 }
 

@@ -56,6 +56,18 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 __device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
+// Adds transaction bytes to the current phase without arriving.
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// 16-byte asynchronous global -> shared copy (cached in L1: the 2x-upsampled reads hit each
+// coarse value four times); src_bytes 0 writes zeros and reads nothing.
+__device__ __forceinline__ void cp_async_16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c, int x, int y, int b,
                                             uint32_t bar) {
   asm volatile(
@@ -134,6 +146,7 @@ k_conv3x3_ws(const __grid_constant__ CUtensorMap tmap, ConvGeom g, const uint16_
     int stage = 0;
     uint32_t phase = 0;
     int filled = 0;   // stages filled in total (to drain copies on abort)
+    int pend = -1;    // stage whose 16-byte copies are in flight, not yet arrived on
     bool ok = true;
     for (int tile = blockIdx.x; tile < g.n_tiles && ok; tile += gridDim.x) {
       const int nt = tile % g.ntn, rest = tile / g.ntn;
@@ -157,53 +170,42 @@ k_conv3x3_ws(const __grid_constant__ CUtensorMap tmap, ConvGeom g, const uint16_
             mbar_arrive(full_bar(stage));
           }
         } else {
-          // upsampled coarse channels: the tile's 18 x 18 halo is the 2x upsampling of 10 x 10
-          // coarse pixels (fine y = 2 cy + dy, cy from y0 / 2 - 1).  Each coarse value is loaded
-          // once, all of a thread's loads in flight together, and written to its (up to) four
-          // halo positions, zero where the fine position is outside the image.
+          // upsampled coarse channels: one 16-byte asynchronous copy per halo position and
+          // plane from its coarse pixel (zero outside the image); the stage is arrived on once
+          // the copies have landed, after the next stage has been issued (below), so the copies
+          // of consecutive stages overlap
           const int ci = kt * 16;
-          constexpr int CW = HW / 2 + 1, NV = 2 * CW * CW;
-          constexpr int PER = (NV + LOADER_THREADS - 1) / LOADER_THREADS;
-          const int cy0 = (y0 >> 1) - 1, cx0 = (x0 >> 1) - 1;
-          uint4 v[PER];
-#pragma unroll
-          for (int j = 0; j < PER; ++j) {
-            const int i = tid + j * LOADER_THREADS;
-            const int pl = i / (CW * CW), q = i - pl * (CW * CW), cy = cy0 + q / CW, cx = cx0 + q % CW;
-            v[j] = make_uint4(0u, 0u, 0u, 0u);
-            if (i < NV && cy >= 0 && cy < g.hc && cx >= 0 && cx < g.wc)
-              v[j] = __ldg(reinterpret_cast<const uint4*>(g.u + (((size_t)b * g.hc + cy) * g.wc + cx) * g.cu + ci + pl * 8));
+          for (int i = tid; i < 2 * HW * HW; i += LOADER_THREADS) {
+            const int pl = i / (HW * HW), q = i - pl * (HW * HW), hy = q / HW, hx = q - hy * HW;
+            const int y = y0 - 1 + hy, x = x0 - 1 + hx;
+            const bool in = y >= 0 && y < g.h && x >= 0 && x < g.w;
+            const uint16_t* src = in ? g.u + (((size_t)b * g.hc + (y >> 1)) * g.wc + (x >> 1)) * g.cu + ci + pl * 8 : g.u;
+            cp_async_16(st_addr + (uint32_t)(pl * PLANE_STRIDE + q * 16), src, in ? 16u : 0u);
           }
-#pragma unroll
-          for (int j = 0; j < PER; ++j) {
-            const int i = tid + j * LOADER_THREADS;
-            if (i >= NV) break;
-            const int pl = i / (CW * CW), q = i - pl * (CW * CW), qy = q / CW, qx = q % CW;
-#pragma unroll
-            for (int dy = 0; dy < 2; ++dy) {
-              const int hy = 2 * qy - 1 + dy, y = y0 - 1 + hy;
-              if (hy < 0 || hy >= HW) continue;
-#pragma unroll
-              for (int dx = 0; dx < 2; ++dx) {
-                const int hx = 2 * qx - 1 + dx, x = x0 - 1 + hx;
-                if (hx < 0 || hx >= HW) continue;
-                const bool in = y >= 0 && y < g.h && x >= 0 && x < g.w;
-                *reinterpret_cast<uint4*>(st + pl * PLANE_STRIDE + (hy * HW + hx) * 16) =
-                    in ? v[j] : make_uint4(0u, 0u, 0u, 0u);
-              }
-            }
-          }
-          tc::fence_async_smem();
+          cp_async_commit();
           if (tid == 0) {
-            mbar_arrive_tx(full_bar(stage), (uint32_t)wts_bytes(NT));
+            mbar_expect_tx(full_bar(stage), (uint32_t)wts_bytes(NT));
             bulk_load(st_addr + HALO_BYTES, wsrc, (uint32_t)wts_bytes(NT), full_bar(stage));
-          } else {
-            mbar_arrive(full_bar(stage));
           }
         }
+        // the previous stage filled by 16-byte copies: once this thread's copies have landed,
+        // make them visible to the tensor cores' proxy and arrive (stages older than the one
+        // just issued cannot wait on anything this thread still holds, so this never deadlocks)
+        if (pend >= 0) {
+          if (kt < KT_UP) cp_async_wait<1>(); else cp_async_wait<0>();
+          tc::fence_async_smem();
+          mbar_arrive(full_bar(pend));
+          pend = -1;
+        }
+        if (kt < KT_UP) pend = stage;
         ++filled;
         if (++stage == STAGES) { stage = 0; phase ^= 1u; }
       }
+    }
+    if (pend >= 0) {
+      cp_async_wait<0>();
+      tc::fence_async_smem();
+      mbar_arrive(full_bar(pend));
     }
     if (!ok && tid == 0) {
       // drain: every stage filled so far must have landed before the CTA can leave

@@ -534,11 +534,9 @@ struct Crop { int e, oy, ox, pad; };
 
 // Batch gather: features (log1p colour, albedo, normal, depth/(depth+3); 16 channels, BF16),
 // noisy colour and target of each crop pixel.  Dataset images are e x h_img x w_img.
-// Input features of a pixel: log1p colour, albedo, normal, depth / (depth + 3) and the noise
-// level 1 / sqrt(samples per pixel), with the sample count given (samples > 0) or read from the
-// colour's fourth channel (training examples); counts below 1 read as 1.
+// Input features of a pixel: log1p colour, albedo, normal, depth / (depth + 3), zero-padded to 16.
 __global__ void k_gather(const float4* __restrict__ col, const float* __restrict__ gbuf, const float4* __restrict__ tgt,
-                         int h_img, int w_img, const Crop* __restrict__ crops, int B, int h, int w, float samples,
+                         int h_img, int w_img, const Crop* __restrict__ crops, int B, int h, int w,
                          uint16_t* __restrict__ x0, float4* __restrict__ col_out, float4* __restrict__ tgt_out) {
   const int P = B * h * w;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
@@ -553,9 +551,8 @@ __global__ void k_gather(const float4* __restrict__ col, const float* __restrict
     f[6] = g[0]; f[7] = g[1]; f[8] = g[2];
     float d = fmaxf(g[11], 0.0f);
     f[9] = d / (d + 3.0f);
-    f[10] = 1.0f / sqrtf(fmaxf(samples > 0.0f ? samples : cl.w, 1.0f));
 #pragma unroll
-    for (int i = 11; i < 16; ++i) f[i] = 0.0f;
+    for (int i = 10; i < 16; ++i) f[i] = 0.0f;
     uint32_t wv[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) wv[i] = (uint32_t)f2bf(f[2 * i]) | ((uint32_t)f2bf(f[2 * i + 1]) << 16);
@@ -743,26 +740,38 @@ __global__ void k_bias_grad(const uint16_t* __restrict__ dz, int P, int C, float
 }
 
 // Adam (bias-corrected) over the flat FP32 parameters, with the gradient g * scale.
-// Gradient clipping by global norm: the squared norm of g * scale is summed into clip[0]; then
-// k_clip_factor turns it into the step's factor clip[2]: 1, or kClipRatio times the running mean
-// of past step norms (clip[1]) over this norm when the norm is above that (a batch whose noisy
-// input holds a firefly of the sun can carry a gradient thousands of times the usual one), or 0
-// for a non-finite norm (the step is skipped).  The first step sets the running mean.
+// Gradient clipping by global norm.  k_grad_sqnorm writes per-block partial sums of (g * scale)^2
+// into clip[4 ..], k_clip_factor adds them in a fixed order (the same bits on every data-parallel
+// rank that holds the same gradient) and sets the step's factor clip[2]: 1, or kClipRatio times
+// the running mean of past step norms (clip[1]) over this norm when the norm is above that (a
+// batch whose noisy input holds a firefly of the sun can carry a gradient thousands of times the
+// usual one), or 0 for a non-finite norm (the step is skipped).  The first step sets the mean.
 constexpr float kClipRatio = 4.0f;
+constexpr int kNormBlocks = 296;
 
-__global__ void k_grad_sqnorm(const float* __restrict__ g, size_t n, float scale, float* __restrict__ clip) {
+__global__ void __launch_bounds__(256) k_grad_sqnorm(const float* __restrict__ g, size_t n, float scale,
+                                                     float* __restrict__ clip) {
+  __shared__ float part[8];
   float s = 0.0f;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const float v = g[i] * scale;
     s += v * v;
   }
   for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-  if ((threadIdx.x & 31) == 0) atomicAdd(clip, s);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float b = 0.0f;
+    for (int w = 0; w < 8; ++w) b += part[w];
+    clip[4 + blockIdx.x] = b;
+  }
 }
 
 __global__ void k_clip_factor(float* __restrict__ clip) {
-  const float norm = sqrtf(clip[0]);
-  clip[0] = 0.0f;
+  if (threadIdx.x != 0) return;
+  float sq = 0.0f;
+  for (int b = 0; b < kNormBlocks; ++b) sq += clip[4 + b];
+  const float norm = sqrtf(sq);
   if (!isfinite(norm)) {
     clip[2] = 0.0f;
     return;
@@ -915,31 +924,46 @@ k_out_softmax(const uint16_t* __restrict__ d0, const uint16_t* __restrict__ wb, 
   if (warp == 0) tc::tmem_free(tmem, NCOLS);
 }
 
-// A filter stage with stored normalised kernels (planes off..off+24 of wk23); with rgba the
-// result is also tonemapped into the rgba8 image with the accumulation pass's display transform
-// (shader.wgsl:2487-2490).
-__global__ void k_filter_stored(const float* __restrict__ wk23, int off, int d, const float4* __restrict__ in,
-                                float4* __restrict__ out, uchar4* __restrict__ rgba, float exposure, int B, int h,
-                                int w) {
-  const int P = B * h * w;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-    const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
-    const float* wk = wk23 + (size_t)off * P + p;
-    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+// A filter stage with stored normalised kernels (planes off..off+24 of wk23) at dilation D over
+// a 32 x 8 pixel block: the block's colours and a 2D-pixel apron, clamped to the image like
+// tap_index, are staged in shared memory once, and the weights are read as planes (128
+// contiguous bytes a warp).  The taps are summed in tap_index order, so the result equals the
+// direct gather's.  With rgba the result is also tonemapped into the rgba8 image with the
+// accumulation pass's display transform (shader.wgsl:2487-2490).
+template <int D>
+__global__ void __launch_bounds__(256)
+k_filter_stored(const float* __restrict__ wk23, int off, const float4* __restrict__ in, float4* __restrict__ out,
+                uchar4* __restrict__ rgba, float exposure, int B, int h, int w) {
+  constexpr int BW = 32, BH = 8, SW = BW + 4 * D, SH = BH + 4 * D;
+  __shared__ float4 tile[SH * SW];
+  const int b = (int)blockIdx.z, x0 = (int)blockIdx.x * BW, y0 = (int)blockIdx.y * BH;
+  const float4* src = in + (size_t)b * h * w;
+  for (int i = threadIdx.x; i < SH * SW; i += blockDim.x) {
+    const int sy = i / SW, sx = i - (i / SW) * SW;
+    const int yy = min(max(y0 - 2 * D + sy, 0), h - 1), xx = min(max(x0 - 2 * D + sx, 0), w - 1);
+    tile[i] = src[(size_t)yy * w + xx];
+  }
+  __syncthreads();
+  const int tx = (int)(threadIdx.x & 31), ty = (int)(threadIdx.x >> 5);
+  const int x = x0 + tx, y = y0 + ty;
+  if (x >= w || y >= h) return;
+  const size_t P = (size_t)B * h * w;
+  const size_t p = ((size_t)b * h + y) * w + x;
+  const float* wk = wk23 + (size_t)off * P + p;
+  float fx = 0.0f, fy = 0.0f, fz = 0.0f;
 #pragma unroll
-    for (int k = 0; k < 25; ++k) {
-      const float wt = __ldcs(wk + (size_t)k * P);
-      float4 c = in[tap_index(b, y, x, k, d, h, w)];
-      fx += wt * c.x; fy += wt * c.y; fz += wt * c.z;
-    }
-    const float4 v = make_float4(fx, fy, fz, 1.0f);
-    out[p] = v;
-    if (rgba) {
-      float rr = v.x * exposure, gg = v.y * exposure, bb = v.z * exposure;
-      rr = powf(rr / (rr + 0.3f), 0.4545f); gg = powf(gg / (gg + 0.3f), 0.4545f); bb = powf(bb / (bb + 0.3f), 0.4545f);
-      auto u8 = [](float t) { return (unsigned char)floorf(fminf(fmaxf(t, 0.0f), 1.0f) * 255.0f + 0.5f); };
-      rgba[p] = make_uchar4(u8(rr), u8(gg), u8(bb), 255);
-    }
+  for (int k = 0; k < 25; ++k) {
+    const float wt = __ldcs(wk + (size_t)k * P);
+    const float4 c = tile[(ty + 2 * D + D * (k / 5 - 2)) * SW + tx + 2 * D + D * (k % 5 - 2)];
+    fx += wt * c.x; fy += wt * c.y; fz += wt * c.z;
+  }
+  const float4 v = make_float4(fx, fy, fz, 1.0f);
+  out[p] = v;
+  if (rgba) {
+    float rr = v.x * exposure, gg = v.y * exposure, bb = v.z * exposure;
+    rr = powf(rr / (rr + 0.3f), 0.4545f); gg = powf(gg / (gg + 0.3f), 0.4545f); bb = powf(bb / (bb + 0.3f), 0.4545f);
+    auto u8 = [](float t) { return (unsigned char)floorf(fminf(fmaxf(t, 0.0f), 1.0f) * 255.0f + 0.5f); };
+    rgba[p] = make_uchar4(u8(rr), u8(gg), u8(bb), 255);
   }
 }
 
@@ -985,7 +1009,7 @@ struct Net {
   uint16_t *dlog = nullptr, *dx = nullptr, *g_a = nullptr, *g_b = nullptr, *g_pool = nullptr, *g_skip = nullptr;
   std::vector<void*> bufs;
   float* loss = nullptr;
-  float* clip = nullptr;   // gradient clipping: squared norm, running mean of norms, step factor
+  float* clip = nullptr;   // gradient clipping: -, running mean of norms, step factor, -, block partial sums
   Crop* crops = nullptr;
   int crops_cap = 0;
   // dataset
@@ -1001,7 +1025,7 @@ static void set_layer(Layer& l, const char* name, int cu, int cs, int cout, int 
 }
 
 static void define_layers(Net& n) {
-  set_layer(n.L[L_E0A], "E0a", 0, 16, 32, 9, 1, 0, 11, 32);
+  set_layer(n.L[L_E0A], "E0a", 0, 16, 32, 9, 1, 0, 10, 32);
   set_layer(n.L[L_E0], "E0", 0, 32, 32, 9, 1, 0, 32, 32);
   set_layer(n.L[L_E1], "E1", 0, 32, 48, 9, 1, 1, 32, 48);
   set_layer(n.L[L_E2], "E2", 0, 48, 64, 9, 1, 2, 48, 64);
@@ -1178,8 +1202,9 @@ static cudaError_t forward(Net& n, uchar4* infer_rgba = nullptr, float exposure 
     const Layer& lo = n.L[L_OUT];
     k_out_softmax<<<(P0 + tc::BM - 1) / tc::BM, tc::THREADS, OutSmem::BYTES, n.st>>>(
         n.d0, lo.wb, n.w + lo.b_off, n.col, n.f1, n.logits, B, n.H, n.W, n.err);
-    k_filter_stored<<<grid1(P0), 256, 0, n.st>>>(n.logits, 0, 2, n.f1, n.f2, nullptr, exposure, B, n.H, n.W);
-    k_filter_stored<<<grid1(P0), 256, 0, n.st>>>(n.logits, 25, 4, n.f2, n.out, infer_rgba, exposure, B, n.H, n.W);
+    const dim3 fg((unsigned)((n.W + 31) / 32), (unsigned)((n.H + 7) / 8), (unsigned)B);
+    k_filter_stored<2><<<fg, 256, 0, n.st>>>(n.logits, 0, n.f1, n.f2, nullptr, exposure, B, n.H, n.W);
+    k_filter_stored<4><<<fg, 256, 0, n.st>>>(n.logits, 25, n.f2, n.out, infer_rgba, exposure, B, n.H, n.W);
     return cudaGetLastError();
   }
   if ((e = conv_fwd(n, n.L[L_OUT], nullptr, n.d0, n.logits, true))) return e;
@@ -1357,7 +1382,7 @@ cudaError_t adam_step(kp::Net& n, float lr, const float* g = nullptr, float scal
   n.adam_t += 1;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.0f - (float)std::pow(0.9, n.adam_t), c2 = 1.0f - (float)std::pow(0.999, n.adam_t);
-  kp::k_grad_sqnorm<<<kp::grid1(n.n_params), 256, 0, n.st>>>(g ? g : n.g, n.n_params, scale, n.clip);
+  kp::k_grad_sqnorm<<<kp::kNormBlocks, 256, 0, n.st>>>(g ? g : n.g, n.n_params, scale, n.clip);
   kp::k_clip_factor<<<1, 1, 0, n.st>>>(n.clip);
   kp::k_adam<<<kp::grid1(n.n_params), 256, 0, n.st>>>(n.w, g ? g : n.g, n.m, n.v, n.n_params, lr, b1, b2, 1e-8f, c1,
                                                       c2, scale, n.clip);
@@ -1442,8 +1467,8 @@ int wgpt_kpcn_create(int device, uint64_t seed, wgpt_kpcn** out) {
   if (e == cudaSuccess) e = cudaMalloc(&n.v, n.n_params * 4);
   if (e == cudaSuccess) e = cudaMalloc(&n.err, 4);
   if (e == cudaSuccess) e = cudaMalloc(&n.loss, 4);
-  if (e == cudaSuccess) e = cudaMalloc(&n.clip, 16);
-  if (e == cudaSuccess) e = cudaMemset(n.clip, 0, 16);
+  if (e == cudaSuccess) e = cudaMalloc(&n.clip, (4 + kp::kNormBlocks) * 4);
+  if (e == cudaSuccess) e = cudaMemset(n.clip, 0, (4 + kp::kNormBlocks) * 4);
   for (int i = 0; i < kp::NLAYERS && e == cudaSuccess; ++i) {
     e = cudaMalloc(&n.L[i].wb, n.L[i].nw() * 2);
     if (e == cudaSuccess) e = cudaMalloc(&n.L[i].wt, n.L[i].nw() * 2);
@@ -1522,7 +1547,7 @@ int wgpt_kpcn_set_params(wgpt_kpcn* k, const float* src) {
   KCK(cudaMemcpyAsync(n.w, src, n.n_params * 4, cudaMemcpyHostToDevice, n.st), "write params");
   KCK(cudaMemsetAsync(n.m, 0, n.n_params * 4, n.st), "reset moments");
   KCK(cudaMemsetAsync(n.v, 0, n.n_params * 4, n.st), "reset moments");
-  KCK(cudaMemsetAsync(n.clip, 0, 16, n.st), "reset clipping");
+  KCK(cudaMemsetAsync(n.clip, 0, 16, n.st), "reset clipping");   // the partial sums are rewritten each step
   n.adam_t = 0;
   KCK(kp::refresh_bf16(n), "bf16 weights");
   KCK(cudaStreamSynchronize(n.st), "synchronize");
@@ -1592,7 +1617,7 @@ int wgpt_kpcn_train(wgpt_kpcn* k, uint32_t steps, uint32_t batch, uint32_t crop,
   for (uint32_t it = 0; it < steps; ++it) {
     kp::k_gather<<<kp::grid1(P), 256, 0, n.st>>>(n.ds_col, n.ds_gbuf, n.ds_tgt, n.ds_h, n.ds_w,
                                                  k->d_crops + (size_t)it * batch, (int)batch, (int)crop, (int)crop,
-                                                 0.0f, n.x0, n.col, n.tgt);
+                                                 n.x0, n.col, n.tgt);
     KCK(kp::forward(n), "forward");
     KCK(kp::backward(n), "backward");
     KCK(cudaMemcpyAsync(k->d_losses + it, n.loss, 4, cudaMemcpyDeviceToDevice, n.st), "loss copy");
@@ -1620,7 +1645,7 @@ int wgpt_kpcn_grads(wgpt_kpcn* k, uint32_t batch, uint32_t crop, uint64_t seed, 
   if (rc) return rc;
   const size_t P = (size_t)batch * crop * crop;
   kp::k_gather<<<kp::grid1(P), 256, 0, n.st>>>(n.ds_col, n.ds_gbuf, n.ds_tgt, n.ds_h, n.ds_w, k->d_crops, (int)batch,
-                                               (int)crop, (int)crop, 0.0f, n.x0, n.col, n.tgt);
+                                               (int)crop, (int)crop, n.x0, n.col, n.tgt);
   KCK(kp::forward(n), "forward");
   KCK(kp::backward(n), "backward");
   KCK(cudaMemcpyAsync(dev_grads, n.g, n.n_params * 4, cudaMemcpyDeviceToDevice, n.st), "gradient copy");
@@ -1661,7 +1686,7 @@ int wgpt_kpcn_loss_and_grads(wgpt_kpcn* k, const float* noisy, const void* gbuf,
   KCK(cudaMemcpyAsync(k->d_img_tgt, target, npix * 16, cudaMemcpyHostToDevice, n.st), "upload image");
   KCK(cudaMemcpyAsync(k->d_img_gbuf, gbuf, npix * 48, cudaMemcpyHostToDevice, n.st), "upload image");
   kp::k_gather<<<kp::grid1(npix), 256, 0, n.st>>>(k->d_img_col, k->d_img_gbuf, k->d_img_tgt, (int)h, (int)w,
-                                                  k->d_crops, 1, (int)h, (int)w, 0.0f, n.x0, n.col, n.tgt);
+                                                  k->d_crops, 1, (int)h, (int)w, n.x0, n.col, n.tgt);
   KCK(kp::forward(n), "forward");
   KCK(kp::backward(n), "backward");
   if (loss) KCK(cudaMemcpyAsync(loss, n.loss, 4, cudaMemcpyDeviceToHost, n.st), "loss readback");
@@ -1689,8 +1714,7 @@ static int denoise_image(wgpt_kpcn* k, wgpt_ctx* ctx, int view, float exposure, 
   KCK(cudaEventRecord(k->ev_in, im.stream), "event");
   KCK(cudaStreamWaitEvent(n.st, k->ev_in, 0), "event wait");
   kp::k_gather<<<kp::grid1(npix), 256, 0, n.st>>>((const float4*)im.accum, im.gbuf, nullptr, (int)im.h, (int)im.w,
-                                                  k->d_crops, 1, (int)im.h, (int)im.w, (float)std::max(im.samples, 1u),
-                                                  n.x0, n.col, nullptr);
+                                                  k->d_crops, 1, (int)im.h, (int)im.w, n.x0, n.col, nullptr);
   KCK(kp::forward(n, (uchar4*)im.out, exposure), "forward");
   KCK(cudaGetLastError(), "denoise launch");
   KCK(cudaEventRecord(k->ev_out, n.st), "event");

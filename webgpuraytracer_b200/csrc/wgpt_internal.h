@@ -26,7 +26,6 @@ struct CtxImages {
   float* gbuf;
   uint8_t* out;
   cudaStream_t stream;
-  uint32_t samples;   // samples per pixel in the accumulation (0: unknown)
 };
 bool ctx_images(::wgpt_ctx* ctx, int view, CtxImages* out);   // view -1: the main image
 

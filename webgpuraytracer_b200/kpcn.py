@@ -109,13 +109,9 @@ class Kpcn:
         assert a.size == self.n_params
         self._check(self.L.wgpt_kpcn_set_params(self.h, ptr(a)), "set_params")
 
-    def add_example(self, noisy: np.ndarray, gbuf: np.ndarray, target: np.ndarray, samples: int | None = None):
-        """One training example; `samples` (the noisy image's samples per pixel, the network's
-        noise-level input) is written into the noisy image's fourth channel when given."""
+    def add_example(self, noisy: np.ndarray, gbuf: np.ndarray, target: np.ndarray):
         h, w = noisy.shape[:2]
-        noisy = np.array(noisy, np.float32, copy=samples is not None, order="C")
-        if samples is not None:
-            noisy[..., 3] = float(samples)
+        noisy = np.ascontiguousarray(noisy, np.float32)
         gbuf = np.ascontiguousarray(gbuf, np.float32)
         target = np.ascontiguousarray(target, np.float32)
         assert noisy.shape == (h, w, 4) and target.shape == (h, w, 4) and gbuf.shape == (h, w, 12)
@@ -184,9 +180,8 @@ def load_weights(k: Kpcn, path) -> dict:
 
 
 def render_example(scene: sc.Scene, size: int, spp: int, target_spp: int, seed: int = 1, target_seed: int = 977):
-    """(noisy accumulation at `spp` with the count in its fourth channel, G-buffer, target
-    accumulation at `target_spp`) of one view, rendered by the path tracer; the target uses an
-    independent sample stream."""
+    """(noisy accumulation at `spp`, G-buffer, target accumulation at `target_spp`) of one view,
+    rendered by the path tracer; the target uses an independent sample stream."""
     scene.camera.aspect = 1.0
     r = rd.Renderer(size, size, seed_fn=lambda: seed)
     r.set_scene(scene, isgbuf=True)
@@ -195,7 +190,6 @@ def render_example(scene: sc.Scene, size: int, spp: int, target_spp: int, seed: 
     r.reset()
     r.render(tsize=size, reps=spp)
     noisy = r.read_accum()
-    noisy[..., 3] = spp                  # samples per pixel: the network's noise-level input
     r.close()
     t = rd.Renderer(size, size, seed_fn=lambda: target_seed)
     t.set_scene(scene)
@@ -260,7 +254,7 @@ def build_training_set(k: Kpcn, seeds, size: int = 256, spps=(1, 2, 4, 8), targe
             for spp in spps:
                 r.render(tsize=size, reps=spp - done)
                 done = spp
-                k.add_example(r.read_accum(), gbuf, target, samples=spp)
+                k.add_example(r.read_accum(), gbuf, target)
                 n += 1
     finally:
         t.close()
@@ -329,7 +323,7 @@ def build_flagship_training_set(k: Kpcn, seeds, crops: int = 2, size: int = 256,
                 acc = in_r.read_accum()
                 for (cx, cy) in wins:
                     win = (slice(cy, cy + size), slice(cx, cx + size))
-                    k.add_example(acc[win], gbuf[win], target[win], samples=spp)
+                    k.add_example(acc[win], gbuf[win], target[win])
                     n += 1
     finally:
         tgt_r.close()

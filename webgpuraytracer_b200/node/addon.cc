@@ -579,13 +579,6 @@ EXPORT(SetDenoiseMode) {
   BODY(CtxBox* b = ctx_box(env, a.at(0)); check(wgpt_set_denoise_mode(b->ctx, a.i32(1)), b->ctx, "setDenoiseMode"); return undef(env);)
 }
 
-// setAccumSamples(ctx, view, samples): samples per pixel of an image written by writeAccum (view
-// -1: the main image), the learned denoiser's noise-level input
-EXPORT(SetAccumSamples) {
-  BODY(CtxBox* b = ctx_box(env, a.at(0));
-       check(wgpt_set_accum_samples(b->ctx, a.i32(1), a.u32(2)), b->ctx, "setAccumSamples"); return undef(env);)
-}
-
 // renderPreview blit (tracer.js:2365-2389): resample(ctx, dstW, dstH, ratioX, ratioY)
 EXPORT(Resample) {
   BODY(
@@ -1264,7 +1257,6 @@ napi_value Init(napi_env env, napi_value exports) {
       FN("getWavefrontTuning", GetWavefrontTuning), FN("denoise", Denoise), FN("setDenoiseMode", SetDenoiseMode), FN("resample", Resample),
       FN("synchronize", Synchronize), FN("synchronizeTimeout", SynchronizeTimeout),
       FN("synchronizeAsync", SynchronizeAsync), FN("readAccum", ReadAccum), FN("writeAccum", WriteAccum),
-      FN("setAccumSamples", SetAccumSamples),
       FN("readOutput", ReadOutput), FN("readGBuffer", ReadGBuffer), FN("writeGBuffer", WriteGBuffer),
       FN("readDenoised", ReadDenoised), FN("readCanvas", ReadCanvas), FN("setViews", SetViews),
       FN("renderViews", RenderViews), FN("renderViewsGBuffer", RenderViewsGBuffer), FN("readView", ReadView),

@@ -202,7 +202,7 @@ class Renderer:
             w, h = (int(v) for v in f["size"])
             if (w, h) != (self.width, self.height):
                 raise ValueError(f"checkpoint is {w}x{h}, renderer is {self.width}x{self.height}")
-            self.write_accum(np.ascontiguousarray(f["accum"], np.float32), samples=int(f["frame"]))
+            self.write_accum(np.ascontiguousarray(f["accum"], np.float32))
             if "accum64" in f.files:
                 self.set_accum_f64(True)
                 a = np.ascontiguousarray(f["accum64"], np.float64)
@@ -215,13 +215,9 @@ class Renderer:
         self._check(self.L.wgpt_read_accum(self.ctx, ptr(a)), "read_accum")
         return a
 
-    def write_accum(self, a: np.ndarray, samples: int | None = None):
-        """Writes the accumulation; `samples` declares its samples per pixel (what the learned
-        denoiser is told; a render sets it to first_frame + reps)."""
+    def write_accum(self, a: np.ndarray):
         a = np.ascontiguousarray(a, dtype=np.float32)
         self._check(self.L.wgpt_write_accum(self.ctx, ptr(a)), "write_accum")
-        if samples is not None:
-            self._check(self.L.wgpt_set_accum_samples(self.ctx, -1, int(samples)), "set_accum_samples")
 
     def read_output(self) -> np.ndarray:
         a = np.empty((self.height, self.width, 4), dtype=np.uint8)

@@ -7,10 +7,9 @@
         [--device 0] [--eval 16]
 
 The set: for each seeded scene of the chosen family, `crops` 256x256 windows of its view,
-progressive inputs at each sample count of --spps (one example each, the count stored as the
-network's noise-level input) and a target at --target-spp with an independent sample stream
-accumulated in FP64 (FP32 running mean with --target-f32), all path traced on the GPU by this
-renderer.  The defaults are the learned-denoiser configuration: 2,000 scenes of the
+progressive inputs at each sample count of --spps (one example each) and a target at
+--target-spp with an independent sample stream accumulated in FP64 (FP32 running mean with
+--target-f32), all path traced on the GPU by this renderer.  The defaults are the learned-denoiser configuration: 2,000 scenes of the
 small-configuration family, 256x256, 1/2/4/8-spp inputs, 4096-spp targets (the set is held in
 device memory: about 5 MB an example, 40 GB for the 8,000 examples).  The flagship family
 (seeded 8-bounce flagship scenes with their own cameras, windows of their 1920x1080 views)

@@ -194,6 +194,15 @@ def _learnable_image(h, w, seed):
     return noisy, gbuf, (noisy * 0.5).astype(np.float32)
 
 
+def _blurred_image(h, w, seed):
+    """A random noisy image, G-buffer, and as target its 3x3 box blur (clamped edges): a convex
+    combination of input pixels, which the softmax-normalised kernels can represent."""
+    noisy, gbuf, _ = _random_image(h, w, seed)
+    p = np.pad(noisy, ((1, 1), (1, 1), (0, 0)), mode="edge")
+    tgt = sum(p[dy:dy + h, dx:dx + w] for dy in range(3) for dx in range(3)) / 9.0
+    return noisy, gbuf, tgt.astype(np.float32)
+
+
 def test_kpcn_emulated_two_rank_steps_keep_weights_identical():
     """Two denoisers with different examples, one gradient sum per step (what all_reduce
     gives every rank), the mean applied on both: the weights stay bit-identical, the loss falls."""
@@ -201,18 +210,21 @@ def test_kpcn_emulated_two_rank_steps_keep_weights_identical():
     ks = [kpcn.Kpcn(0, seed=2) for _ in range(2)]
     for r, k in enumerate(ks):
         for e in range(3):
-            k.add_example(*_learnable_image(64, 64, 100 * r + e))
+            k.add_example(*_blurred_image(64, 64, 100 * r + e))
     gs = [torch.empty(ks[0].n_params, dtype=torch.float32, device="cuda:0") for _ in ks]
     first = last = None
-    for step in range(12):
+    seq = []
+    for step in range(16):
         # each rank keeps its batch (seed r), so the summed loss is of the same data every step
         losses = [k.grads(2, 32, r, g) for r, (k, g) in enumerate(zip(ks, gs))]
         total = gs[0] + gs[1]
         torch.cuda.synchronize()
         for k in ks:
-            k.apply(total, 0.5, 2e-3)
+            k.apply(total, 0.5, 1e-3)
+        seq.append(sum(losses))
         first = first if first is not None else sum(losses)
         last = sum(losses)
+    print("summed losses:", " ".join(f"{v:.4f}" for v in seq))
     assert np.array_equal(ks[0].get_params(), ks[1].get_params())
     assert last < first
     for k in ks:

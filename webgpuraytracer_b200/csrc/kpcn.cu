@@ -842,9 +842,12 @@ struct OutSmem {
   static constexpr int BYTES = A_BYTES + B_BYTES + 64;
 };
 
+// The output layer's bias as a kernel argument (read from the constant bank, no loads).
+struct OutBias { float v[LOGITS]; };
+
 // One CTA per 128 pixels.  d0: [P][32] BF16, wb: [80][32] BF16, bias: 80 floats.
 __global__ void __launch_bounds__(tc::THREADS)
-k_out_softmax(const uint16_t* __restrict__ d0, const uint16_t* __restrict__ wb, const float* __restrict__ bias,
+k_out_softmax(const uint16_t* __restrict__ d0, const uint16_t* __restrict__ wb, const OutBias bias,
               const float4* __restrict__ col, float4* __restrict__ f1, float* __restrict__ wk23, int B, int h,
               int w, uint32_t* err) {
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -896,27 +899,35 @@ k_out_softmax(const uint16_t* __restrict__ d0, const uint16_t* __restrict__ wb, 
       float v[16];
       tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) lg[c0 + i] = v[i] + bias[c0 + i];
+      for (int i = 0; i < 16; ++i) lg[c0 + i] = v[i] + bias.v[c0 + i];
     }
     const int p = p0 + warp * 32 + (tid & 31);
     if (p < P) {
       const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
       float wk[25];
       softmax_reg<25>(lg, 0, wk);
+      // the 5 clamped rows and columns of the taps (tap_index's clamping, computed once)
+      const float4* img = col + (size_t)b * h * w;
+      int rows[5], cols[5];
+#pragma unroll
+      for (int d = 0; d < 5; ++d) {
+        rows[d] = min(max(y + d - 2, 0), h - 1) * w;
+        cols[d] = min(max(x + d - 2, 0), w - 1);
+      }
       float fx = 0.0f, fy = 0.0f, fz = 0.0f;
 #pragma unroll
       for (int k = 0; k < 25; ++k) {
-        float4 c = col[tap_index(b, y, x, k, 1, h, w)];
+        float4 c = img[rows[k / 5] + cols[k % 5]];
         fx += wk[k] * c.x; fy += wk[k] * c.y; fz += wk[k] * c.z;
       }
       f1[p] = make_float4(fx, fy, fz, 1.0f);
       float* dst = wk23 + p;
       softmax_reg<25>(lg, 25, wk);
 #pragma unroll
-      for (int k = 0; k < 25; ++k) __stcs(dst + (size_t)k * P, wk[k]);
+      for (int k = 0; k < 25; ++k, dst += P) __stcs(dst, wk[k]);
       softmax_reg<25>(lg, 50, wk);
 #pragma unroll
-      for (int k = 0; k < 25; ++k) __stcs(dst + (size_t)(25 + k) * P, wk[k]);
+      for (int k = 0; k < 25; ++k, dst += P) __stcs(dst, wk[k]);
     }
   }
   tc::tc_fence_before();
@@ -1009,6 +1020,8 @@ struct Net {
   uint16_t *dlog = nullptr, *dx = nullptr, *g_a = nullptr, *g_b = nullptr, *g_pool = nullptr, *g_skip = nullptr;
   std::vector<void*> bufs;
   float* loss = nullptr;
+  OutBias out_bias;             // host copy of the output layer's bias for the inference tail
+  bool out_bias_valid = false;  // cleared whenever the weights change
   float* clip = nullptr;   // gradient clipping: -, running mean of norms, step factor, -, block partial sums
   Crop* crops = nullptr;
   int crops_cap = 0;
@@ -1050,6 +1063,7 @@ static void define_layers(Net& n) {
 static int grid1(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
 static cudaError_t refresh_bf16(Net& n) {
+  n.out_bias_valid = false;
   for (int i = 0; i < NLAYERS; ++i) {
     Layer& l = n.L[i];
     k_weights_bf16<<<grid1(l.nw()), 256, 0, n.st>>>(n.w + l.w_off, l.cout, l.taps, l.cin(), l.wb, l.wt);
@@ -1200,8 +1214,15 @@ static cudaError_t forward(Net& n, uchar4* infer_rgba = nullptr, float exposure 
     // (in the logits buffer, which inference does not otherwise use)
     const int P0 = B * n.H * n.W;
     const Layer& lo = n.L[L_OUT];
+    if (!n.out_bias_valid) {
+      // a host copy of the output bias, taken once after each weight change
+      if ((e = cudaMemcpyAsync(n.out_bias.v, n.w + lo.b_off, sizeof n.out_bias.v, cudaMemcpyDeviceToHost, n.st)))
+        return e;
+      if ((e = cudaStreamSynchronize(n.st))) return e;
+      n.out_bias_valid = true;
+    }
     k_out_softmax<<<(P0 + tc::BM - 1) / tc::BM, tc::THREADS, OutSmem::BYTES, n.st>>>(
-        n.d0, lo.wb, n.w + lo.b_off, n.col, n.f1, n.logits, B, n.H, n.W, n.err);
+        n.d0, lo.wb, n.out_bias, n.col, n.f1, n.logits, B, n.H, n.W, n.err);
     const dim3 fg((unsigned)((n.W + 31) / 32), (unsigned)((n.H + 7) / 8), (unsigned)B);
     k_filter_stored<2><<<fg, 256, 0, n.st>>>(n.logits, 0, n.f1, n.f2, nullptr, exposure, B, n.H, n.W);
     k_filter_stored<4><<<fg, 256, 0, n.st>>>(n.logits, 25, n.f2, n.out, infer_rgba, exposure, B, n.H, n.W);

@@ -214,13 +214,13 @@ def test_kpcn_emulated_two_rank_steps_keep_weights_identical():
     gs = [torch.empty(ks[0].n_params, dtype=torch.float32, device="cuda:0") for _ in ks]
     first = last = None
     seq = []
-    for step in range(16):
+    for step in range(12):
         # each rank keeps its batch (seed r), so the summed loss is of the same data every step
         losses = [k.grads(2, 32, r, g) for r, (k, g) in enumerate(zip(ks, gs))]
         total = gs[0] + gs[1]
         torch.cuda.synchronize()
         for k in ks:
-            k.apply(total, 0.5, 1e-3)
+            k.apply(total, 0.5, 2e-4)   # small steps: a fixed 2 x 32^2 batch overshoots at 1e-3
         seq.append(sum(losses))
         first = first if first is not None else sum(losses)
         last = sum(losses)

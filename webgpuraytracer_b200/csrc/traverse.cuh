@@ -36,11 +36,6 @@ enum : uint32_t {
   K_TLAS_REST = 5u     // remaining objects of a multi-object TLAS leaf (not a node visit)
 };
 constexpr int TRAV_STACK = 132;   // TLAS depth + BLAS depth (each <= 62, checked on upload) + 2
-// The top TRAV_SHORT entries of a thread's stack live in shared memory (a column of the block's
-// short-stack array); deeper entries move to local memory as the stack grows past the window and
-// come back as it shrinks, so traversals that stay within the window touch no local memory.
-constexpr int TRAV_SHORT = 16;
-static_assert((TRAV_SHORT & (TRAV_SHORT - 1)) == 0, "the window is indexed modulo its size");
 
 __device__ __forceinline__ uint2 ent(uint32_t kind, uint32_t count, uint32_t val) {
   return make_uint2((kind << 29) | count, val);
@@ -55,39 +50,11 @@ struct TravCommon {
   int32_t inst_mat;
   int32_t inst_oidx;
   int sp;
-  // shared-space address of this thread's 16-entry short-stack block (128-byte aligned), with the
-  // thread's index modulo 16 in its low bits: entry i sits in slot (i ^ thread) % 16, so the
-  // lanes of a half-warp reading the same depth hit 16 different bank pairs
-  uint32_t sh;
-  uint2 stack[TRAV_STACK - TRAV_SHORT];   // entries below the window
+  uint2 stack[TRAV_STACK];
 
-  __device__ __forceinline__ void bind_short(const uint2* block, uint32_t thread) {
-    sh = (uint32_t)__cvta_generic_to_shared(block) | (thread & (uint32_t)(TRAV_SHORT - 1));
-  }
-  __device__ __forceinline__ uint32_t slot_addr(int i) const {
-    return (sh & ~127u) + ((((uint32_t)i ^ sh) & (uint32_t)(TRAV_SHORT - 1)) << 3);
-  }
-  __device__ __forceinline__ uint2 ld_slot(int i) const {
-    uint2 v;
-    asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(slot_addr(i)) : "memory");
-    return v;
-  }
-  __device__ __forceinline__ void st_slot(int i, uint2 v) {
-    asm volatile("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(slot_addr(i)), "r"(v.x), "r"(v.y) : "memory");
-  }
   __device__ __forceinline__ void push(uint2 e, uint32_t& err) {
-    if (sp >= TRAV_STACK) { err |= ERR_STACK; return; }
-    if (sp >= TRAV_SHORT) stack[sp - TRAV_SHORT] = ld_slot(sp);   // the slot holds entry sp - TRAV_SHORT
-    st_slot(sp, e);
-    ++sp;
+    if (sp < TRAV_STACK) stack[sp++] = e; else err |= ERR_STACK;
   }
-  __device__ __forceinline__ uint2 pop() {
-    --sp;
-    const uint2 e = ld_slot(sp);
-    if (sp >= TRAV_SHORT) st_slot(sp, stack[sp - TRAV_SHORT]);   // the entry below the window moves up
-    return e;
-  }
-  __device__ __forceinline__ uint2 top() const { return ld_slot(sp - 1); }
   // Children of a pair record, pushed in the reference's order (the nearer one last).
   __device__ __forceinline__ void push_children(float lt, float rt, float limit, float4 lmin, float4 lmax, float4 rmin,
                                                 float4 rmax, bool blas, uint32_t& err) {
@@ -154,7 +121,7 @@ __device__ __forceinline__ void closest_init(const DScene& s, ClosestTrav& t, Co
     cn.add(C_CHILD_TESTS);
     float4 lo = ld4(s.tlas), hi = ld4(s.tlas + 1);
     float base_t = intersect_aabb(t.rw.origin, t.inv_w, lo, hi);
-    if (!(base_t < 0.0f || base_t >= hit.t)) { t.st_slot(0, t.root_entry(lo, hi, 0u, false)); t.sp = 1; }
+    if (!(base_t < 0.0f || base_t >= hit.t)) t.stack[t.sp++] = t.root_entry(lo, hi, 0u, false);
   }
 }
 
@@ -185,7 +152,7 @@ template <bool COUNT>
 __device__ __forceinline__ bool inner_run(const DPairs& P, TravCommon& t, float limit, uint32_t& err,
                                           Counters<COUNT>& cn, uint2& e) {
   while (t.sp > 0) {
-    e = t.pop();
+    e = t.stack[--t.sp];
     const uint32_t kind = e.x >> 29;
     if (kind != K_BLAS_INNER && kind != K_TLAS_INNER) return true;
     cn.add(C_NODES);
@@ -212,7 +179,7 @@ __device__ __forceinline__ bool inner_run(const DPairs& P, TravCommon& t, float 
 // reference's two-wide walk).
 __device__ __forceinline__ bool inner_run_wide(const DPairs& P, TravCommon& t, float limit, uint32_t& err, uint2& e) {
   while (t.sp > 0) {
-    e = t.pop();
+    e = t.stack[--t.sp];
     const uint32_t kind = e.x >> 29;
     if (kind != K_BLAS_INNER && kind != K_TLAS_INNER) return true;
     const bool blas = kind == K_BLAS_INNER;
@@ -275,8 +242,8 @@ __device__ __forceinline__ bool closest_step(const DScene& s, const DPairs& P, C
           }
         }
       }
-      if (t.sp == 0 || (t.top().x >> 29) != K_BLAS_LEAF) break;
-      e = t.pop();
+      if (t.sp == 0 || (t.stack[t.sp - 1].x >> 29) != K_BLAS_LEAF) break;
+      e = t.stack[--t.sp];
       cnt = e.x & 0x1fffffffu;
     }
   } else if (kind == K_TLAS_LEAF || kind == K_TLAS_REST) {
@@ -351,8 +318,7 @@ __device__ __forceinline__ void shadow_init(const DScene& s, ShadowTrav& t, Coun
   t.inv_w = 1.0f / t.rw.direction;
   if (HAS(s, WGPT_HAS_SPHERES | WGPT_HAS_CUBES | WGPT_HAS_CYLINDERS | WGPT_HAS_TORI | WGPT_HAS_MESHES)) {
     float4 lo = ld4(s.tlas), hi = ld4(s.tlas + 1);
-    t.st_slot(0, t.root_entry(lo, hi, 0u, false));
-    t.sp = 1;
+    t.stack[t.sp++] = t.root_entry(lo, hi, 0u, false);
   }
 }
 
@@ -382,8 +348,8 @@ __device__ __forceinline__ bool shadow_step(const DScene& s, const DPairs& P, Sh
           }
         }
       }
-      if (t.sp == 0 || (t.top().x >> 29) != K_BLAS_LEAF) break;
-      e = t.pop();
+      if (t.sp == 0 || (t.stack[t.sp - 1].x >> 29) != K_BLAS_LEAF) break;
+      e = t.stack[--t.sp];
       cnt = e.x & 0x1fffffffu;
     }
   } else if (kind == K_TLAS_LEAF || kind == K_TLAS_REST) {

@@ -323,8 +323,6 @@ __global__ void __launch_bounds__(trav_threads(SHAPE), trav_blocks(SHAPE)) k_wf_
   const uint32_t n = q.n;
   uint32_t* cursor = &a.ctl->counts[iter & 3u][K_EXT_CURSOR];
   ClosestTrav t;
-  __shared__ __align__(128) uint2 short_stack[TRAV_SHORT * trav_threads(SHAPE)];
-  t.bind_short(short_stack + threadIdx.x * TRAV_SHORT, threadIdx.x);
   bool have = false, exhausted = false;
   uint32_t slot = 0;
   while (true) {
@@ -787,8 +785,6 @@ k_wf_shadow(WfArgs a) {
   const uint32_t n = a.ctl->counts[iter & 3u][K_SHADOW];
   uint32_t* cursor = &a.ctl->counts[iter & 3u][K_SH_CURSOR];
   ShadowTrav t;
-  __shared__ __align__(128) uint2 short_stack[TRAV_SHORT * trav_threads(SHAPE)];
-  t.bind_short(short_stack + threadIdx.x * TRAV_SHORT, threadIdx.x);
   bool have = false, exhausted = false;
   uint32_t e = 0;
   while (true) {

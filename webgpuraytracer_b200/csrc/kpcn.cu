@@ -157,46 +157,43 @@ struct ConvA {
   }
 };
 
-__device__ __forceinline__ void scatter8(uint8_t* tile, int r0, int k, uint4 v) {
-  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    uint16_t h = (uint16_t)((w[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu);
-    *reinterpret_cast<uint16_t*>(tile + tc::elem_off(r0 + i, k)) = h;
-  }
-}
-
-// Weight gradient, A operand: row = output channel co, k = pixel; dZ is NHWC [P][cout].
+// Weight gradient, A operand: row = output channel co, k = pixel; dZ is NHWC [P][cout], so 8
+// consecutive channels of one pixel are one 16-byte vector: the tile is stored MN-major.  Each
+// group of 8 threads takes 8 consecutive pixels of one channel group (one 128-byte core matrix in
+// shared memory); consecutive groups take the next channel group of the same pixels.
 struct WgradA {
+  static constexpr bool kMnMajor = true;
   const uint16_t* dz;
   int cout, P;
   template <int ROWS>
   __device__ __forceinline__ void fill(uint8_t* tile, int row0, int k0, int tid) const {
     const int G = ROWS / 8;
     for (int i = tid; i < G * tc::BK; i += tc::THREADS) {
-      const int g = i % G, j = i / G, p = k0 + j, co0 = row0 + g * 8;
+      const int grp = i >> 3, g = grp % G, j = (grp / G) * 8 + (i & 7), p = k0 + j, co0 = row0 + g * 8;
       uint4 v = zero4();
       if (p < P && co0 < cout) v = *reinterpret_cast<const uint4*>(dz + (size_t)p * cout + co0);
-      scatter8(tile, g * 8, j, v);
+      tc::put_mn8(tile, g * 8, j, v);
     }
   }
 };
 
-// Weight gradient, B operand: row n = tap * cin + ci, k = pixel; the input gathered at the tap.
+// Weight gradient, B operand: row n = tap * cin + ci, k = pixel; the input gathered at the tap
+// (8 consecutive input channels of one pixel per vector; MN-major like WgradA).
 struct WgradB {
+  static constexpr bool kMnMajor = true;
   ConvSrc src;
   int cin, P, n_total;
   template <int ROWS>
   __device__ __forceinline__ void fill(uint8_t* tile, int row0, int k0, int tid) const {
     const int G = ROWS / 8;
     for (int i = tid; i < G * tc::BK; i += tc::THREADS) {
-      const int g = i % G, j = i / G, p = k0 + j, n = row0 + g * 8;
+      const int grp = i >> 3, g = grp % G, j = (grp / G) * 8 + (i & 7), p = k0 + j, n = row0 + g * 8;
       uint4 v = zero4();
       if (p < P && n < n_total) {
         const int tap = n / cin;
         v = src.vec(p, tap, n - tap * cin);
       }
-      scatter8(tile, g * 8, j, v);
+      tc::put_mn8(tile, g * 8, j, v);
     }
   }
 };

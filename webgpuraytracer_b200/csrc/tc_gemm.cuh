@@ -123,6 +123,21 @@ __device__ __forceinline__ void put_chunk(uint8_t* tile, int r, int c, uint4 v) 
 // Byte offset of element (r, k) of a tile in the core-matrix layout.
 __device__ __forceinline__ int elem_off(int r, int k) { return ((r >> 3) * (BK / 8) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2; }
 
+// MN-major tiles (operands whose 8 consecutive M or N elements of one K index are contiguous in
+// memory, e.g. the NHWC activations of a weight gradient, where K runs over pixels): each core
+// matrix holds 8 K indices x 16 bytes of 8 consecutive M (N) elements, at the same core
+// positions as the K-major layout ((row/8) * (BK/8) + k/8) * 128, so the descriptors keep
+// LBO = 128 B (next core along K) and SBO = 1024 B (next core along M/N, the no-swizzle
+// MN-major canonical form) and the instruction descriptor's transpose bit selects the layout.
+__device__ __forceinline__ void put_mn8(uint8_t* tile, int r0, int k, uint4 v) {
+  *reinterpret_cast<uint4*>(tile + ((r0 >> 3) * (BK / 8) + (k >> 3)) * 128 + (k & 7) * 16) = v;
+}
+// Loaders that store MN-major tiles declare `static constexpr bool kMnMajor = true`.
+template <class L, class = void>
+struct MnMajor { static constexpr bool value = false; };
+template <class L>
+struct MnMajor<L, decltype((void)L::kMnMajor)> { static constexpr bool value = L::kMnMajor; };
+
 // Fills a ROWS x BK tile from a chunk loader: `uint4 chunk(int row, int k8) const` returns
 // K-elements [8*k8, 8*k8 + 8) of operand row `row` as 8 BF16 values (zero outside the matrix).
 // Consecutive threads take consecutive rows of one K-chunk: conflict-free 16-byte smem stores.
@@ -163,7 +178,7 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(LA la, LB lb, EP ep, int M,
   const int KT_ALL = (K + BK - 1) / BK;
   const int kt_begin = blockIdx.z * kt_per;
   const int KT = max(0, min(KT_ALL - kt_begin, kt_per));   // k-tiles of this CTA
-  constexpr uint32_t IDESC = idesc_bf16(BN);
+  constexpr uint32_t IDESC = idesc_bf16(BN) | (MnMajor<LA>::value ? 1u << 15 : 0u) | (MnMajor<LB>::value ? 1u << 16 : 0u);
   bool ok = true;
   int committed = 0;   // k-tiles whose MMAs were committed
   for (int kt = 0; kt < KT; ++kt) {

@@ -131,6 +131,10 @@ struct ConvSrc {
       y += sign * (tap / 3 - 1);
       x += sign * (tap % 3 - 1);
     }
+    return vec_at(b, y, x, ci0);
+  }
+  // The vector at (image b, row y, column x) of the output grid (zero outside the image).
+  __device__ __forceinline__ uint4 vec_at(int b, int y, int x, int ci0) const {
     if (y < 0 || y >= h || x < 0 || x >= w) return zero4();
     if (ci0 < cu) {
       size_t q = ((size_t)b * hc + (y >> 1)) * wc + (x >> 1);
@@ -178,22 +182,36 @@ struct WgradA {
 };
 
 // Weight gradient, B operand: row n = tap * cin + ci, k = pixel; the input gathered at the tap
-// (8 consecutive input channels of one pixel per vector; MN-major like WgradA).
+// (8 consecutive input channels of one pixel per vector; MN-major like WgradA).  With 128 rows
+// and 128 threads, thread t always fills rows 8 * (t / 8) .. + 8 (one tap and channel group)
+// at pixels k0 + (t % 8) + 8 * i, i = 0..7: the tap and the first pixel's position are divided
+// out once, later pixels are stepped by 8.
 struct WgradB {
   static constexpr bool kMnMajor = true;
   ConvSrc src;
   int cin, P, n_total;
   template <int ROWS>
   __device__ __forceinline__ void fill(uint8_t* tile, int row0, int k0, int tid) const {
-    const int G = ROWS / 8;
-    for (int i = tid; i < G * tc::BK; i += tc::THREADS) {
-      const int grp = i >> 3, g = grp % G, j = (grp / G) * 8 + (i & 7), p = k0 + j, n = row0 + g * 8;
+    static_assert(ROWS == 128 && tc::THREADS == 128 && tc::BK == 64, "one channel group per thread");
+    const int g = tid >> 3, n = row0 + g * 8;
+    const bool n_ok = n < n_total;
+    const int tap = n_ok ? n / cin : 0, ci0 = n - tap * cin;
+    const int dy = src.taps == 9 ? src.sign * (tap / 3 - 1) : 0;
+    const int dx = src.taps == 9 ? src.sign * (tap % 3 - 1) : 0;
+    const int hw = src.h * src.w;
+    int p = k0 + (tid & 7);
+    int b = p / hw, r = p - b * hw, y = r / src.w, x = r - (r / src.w) * src.w;
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
       uint4 v = zero4();
-      if (p < P && n < n_total) {
-        const int tap = n / cin;
-        v = src.vec(p, tap, n - tap * cin);
+      if (n_ok && p < P) v = src.vec_at(b, y + dy, x + dx, ci0);
+      tc::put_mn8(tile, g * 8, it * 8 + (tid & 7), v);
+      p += 8;
+      x += 8;
+      while (x >= src.w) {
+        x -= src.w;
+        if (++y == src.h) { y = 0; ++b; }
       }
-      tc::put_mn8(tile, g * 8, j, v);
     }
   }
 };
@@ -1160,7 +1178,8 @@ static cudaError_t conv_bwd(Net& n, const Layer& l, const uint16_t* dz, const ui
   // weight gradient: M = cout, N = taps * cin, K = pixels, split over pixel ranges
   const int kt_all = (P + tc::BK - 1) / tc::BK;
   const int n_tiles = (K + 127) / 128;
-  int splits = std::max(1, std::min(kt_all, (148 * 2) / std::max(1, n_tiles)));
+  // three CTAs per SM fit (64 KB of shared memory each): split the pixels so they all have work
+  int splits = std::max(1, std::min(kt_all, (sm_count() * 3) / std::max(1, n_tiles)));
   cudaError_t e = gemm<128>(WgradA{dz, l.cout, P}, WgradB{src, cin, P, K}, EpiAtomic{n.g + l.w_off, K, K}, l.cout, K,
                             P, splits, n.err, n.st);
   if (e != cudaSuccess) return e;

@@ -182,8 +182,8 @@ int wgpt_denoise(wgpt_ctx* ctx, const void* uniforms_48, const uint32_t* steps, 
    evaluates every tap's four exponential edge stops and the normal stop with the pinned FP32
    built-ins in the reference's order, bit for bit like the CPU restatement; WGPT_DENOISE_FAST
    uses one hardware exponential of the summed stop arguments, the hardware power and fused
-   multiply-adds, within 1e-5 relative of the exact result per pixel (the tolerance the
-   reference's filter is judged by) but not bit-exact.  Applies to wgpt_denoise on this context. */
+   multiply-adds, within 1e-5 relative of the exact result per pixel (the tolerance stated for
+   the a-trous drop-in) but not bit-exact.  Applies to wgpt_denoise on this context. */
 enum { WGPT_DENOISE_EXACT = 0, WGPT_DENOISE_FAST = 1 };
 int wgpt_set_denoise_mode(wgpt_ctx* ctx, int mode);
 

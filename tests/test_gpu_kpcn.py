@@ -289,3 +289,27 @@ def test_kpcn_pipelined_denoise_equals_per_tile():
     np.testing.assert_array_equal(outs[0][1], outs[1][1])
     k.close()
     r.close()
+
+
+@pytest.mark.parametrize("h,w", [(40, 48), (67, 130)])
+def test_kpcn_inference_tail_equals_training_forward(h, w):
+    """Inference runs the output layer, the softmaxes and the first filter stage fused in one
+    kernel and the last two stages from stored kernels; training runs the output layer as a GEMM
+    into FP32 logits and the filter stages from those.  The arithmetic of every value is the
+    same, so the filtered image is identical bit for bit."""
+    noisy, gbuf, target = _random_image(h, w, h * 31 + w)
+    k = kpcn.Kpcn(0, seed=6)
+    p = k.get_params()
+    sl = kpcn.param_slices()
+    p[sl["OUT"][0]] *= 10.0          # sharper kernels than the initialisation's
+    k.set_params(p)
+    _, _, out_train = k.loss_and_grads(noisy, gbuf, target)
+    s = synth.small_scene(1, w, h, 4)
+    r = rd.Renderer(w, h)
+    r.set_scene(s, isgbuf=True)
+    r.write_accum(noisy)
+    r.write_gbuffer(gbuf)
+    out_infer = k.denoise(r, exposure=1.0)
+    np.testing.assert_array_equal(out_infer[..., :3], out_train[..., :3])
+    r.close()
+    k.close()

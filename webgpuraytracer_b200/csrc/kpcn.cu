@@ -851,98 +851,164 @@ __device__ __forceinline__ void softmax_reg(const float (&lg)[80], int off, floa
   for (int k = 0; k < N; ++k) wk[k] *= inv;
 }
 
-struct OutSmem {
-  static constexpr int A_BYTES = tc::BM * tc::BK * 2;    // 128 pixels x 64 K (32 used)
-  static constexpr int B_BYTES = LOGITS * tc::BK * 2;    // 80 logits x 64 K (32 used)
-  static constexpr int BYTES = A_BYTES + B_BYTES + 64;
-};
-
 // The output layer's bias as a kernel argument (read from the constant bank, no loads).
 struct OutBias { float v[LOGITS]; };
 
-// One CTA per 128 pixels.  d0: [P][32] BF16, wb: [80][32] BF16, bias: 80 floats.
-__global__ void __launch_bounds__(tc::THREADS)
+// Persistent output-layer kernel: warps 0-3 are the epilogue (thread t owns tensor-memory lane t,
+// pixel t of a 128-pixel tile), warp 4 loads each tile's D0 activations into one of two
+// shared-memory stages and issues its two MMAs (K = 32) into the CTA's one accumulator as soon as
+// the epilogue has read the previous tile out of it, so the next tile's loads and MMAs run while
+// the epilogue computes.  Operand tiles use a compact K-major layout: 4 core matrices (32 K) per
+// 8-row group, SBO 512 bytes.
+namespace outk {
+constexpr int THREADS = 160;
+constexpr int A_BYTES = tc::BM * 32 * 2;     // 128 pixels x 32 channels
+constexpr int B_BYTES = LOGITS * 32 * 2;     // 80 logits x 32 channels
+constexpr int SMEM = 2 * A_BYTES + B_BYTES + 128;
+constexpr int CTAS_PER_SM = 3;               // registers (136 a thread); 128 tensor-memory columns each
+__device__ __forceinline__ void put4(uint8_t* tile, int r, int c, uint4 v) {
+  *reinterpret_cast<uint4*>(tile + ((r >> 3) * 4 + c) * 128 + (r & 7) * 16) = v;
+}
+}  // namespace outk
+
+// d0: [P][32] BF16, wb: [80][32] BF16.  Writes stage 1's filtered colour (f1) and the
+// normalised kernels of stages 2 and 3 as 50 planes of P floats (wk23).
+__global__ void __launch_bounds__(outk::THREADS, 3)
 k_out_softmax(const uint16_t* __restrict__ d0, const uint16_t* __restrict__ wb, const OutBias bias,
               const float4* __restrict__ col, float4* __restrict__ f1, float* __restrict__ wk23, int B, int h,
               int w, uint32_t* err) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int P = B * h * w;
-  const int p0 = blockIdx.x * tc::BM;
-  uint8_t* ta = smem;
-  uint8_t* tb = smem + OutSmem::A_BYTES;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + OutSmem::A_BYTES + OutSmem::B_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + OutSmem::A_BYTES + OutSmem::B_BYTES + 16);
-  volatile uint32_t* flag = reinterpret_cast<volatile uint32_t*>(smem + OutSmem::A_BYTES + OutSmem::B_BYTES + 20);
+  const int n_tiles = (P + tc::BM - 1) / tc::BM;
+  uint8_t* ta0 = smem;
+  uint8_t* tb = smem + 2 * outk::A_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tb + outk::B_BYTES);
+  // bars: 0 accumulator full, 1 accumulator read out, 2-3 A stage free
+  const uint32_t bar_full = tc::smem_u32(&bars[0]), bar_tfree = tc::smem_u32(&bars[1]);
+  auto bar_afree = [&](int st) { return tc::smem_u32(&bars[2 + st]); };
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(&bars[4]);
+  volatile uint32_t* abort_flag = tmem_slot + 1;
   constexpr uint32_t NCOLS = tc::tmem_cols(LOGITS);
   if (warp == 0) tc::tmem_alloc(tc::smem_u32(tmem_slot), NCOLS);
-  if (tid == 0) tc::mbar_init(tc::smem_u32(bar), 1);
-  // operand tiles: K chunks 0..3 (32 channels) of every row
-  for (int i = tid; i < tc::BM * 4; i += tc::THREADS) {
-    const int r = i % tc::BM, c = i / tc::BM, p = p0 + r;
-    tc::put_chunk(ta, r, c, p < P ? *reinterpret_cast<const uint4*>(d0 + (size_t)p * 32 + c * 8) : zero4());
+  if (tid == 0) {
+    tc::mbar_init(bar_full, 1);
+    tc::mbar_init(bar_tfree, 128);
+    tc::mbar_init(bar_afree(0), 1);
+    tc::mbar_init(bar_afree(1), 1);
+    *abort_flag = 0u;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int i = tid; i < LOGITS * 4; i += tc::THREADS) {
+  // the weights, once: 80 rows x 4 chunks
+  for (int i = tid; i < LOGITS * 4; i += outk::THREADS) {
     const int r = i % LOGITS, c = i / LOGITS;
-    tc::put_chunk(tb, r, c, *reinterpret_cast<const uint4*>(wb + (size_t)r * 32 + c * 8));
+    outk::put4(tb, r, c, *reinterpret_cast<const uint4*>(wb + (size_t)r * 32 + c * 8));
   }
   tc::fence_async_smem();
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  if (tid == 0) {
-    constexpr uint32_t IDESC = tc::idesc_bf16(LOGITS);
-    const uint32_t a_addr = tc::smem_u32(ta), b_addr = tc::smem_u32(tb);
+  if (warp == 4) {
+    // ---------------------------------------------------------------- loader + MMA issuer
+    int last_j = -1;   // last tile whose MMAs were issued
+    for (int j = 0, tile = blockIdx.x; tile < n_tiles; ++j, tile += gridDim.x) {
+      const int st = j & 1;
+      uint8_t* ta = ta0 + st * outk::A_BYTES;
+      uint32_t go = 1u;
+      if (lane == 0) {
+        if (*abort_flag) go = 0u;
+        // the MMAs that read this stage two tiles ago are done
+        else if (j >= 2 && !tc::mbar_wait(bar_afree(st), (uint32_t)((j >> 1) - 1) & 1u)) go = 0u;
+      }
+      go = __shfl_sync(0xffffffffu, go, 0);
+      if (!go) break;
+      const int p0 = tile * tc::BM;
+      for (int i = lane; i < tc::BM * 4; i += 32) {
+        const int r = i % tc::BM, c = i / tc::BM, p = p0 + r;
+        outk::put4(ta, r, c, p < P ? *reinterpret_cast<const uint4*>(d0 + (size_t)p * 32 + c * 8) : zero4());
+      }
+      tc::fence_async_smem();
+      __syncwarp();
+      if (lane == 0) {
+        // the epilogue has read the previous tile out of the accumulator
+        if (j >= 1 && !tc::mbar_wait(bar_tfree, (uint32_t)(j - 1) & 1u)) go = 0u;
+        if (go) {
+          tc::tc_fence_after();
+          constexpr uint32_t IDESC = tc::idesc_bf16(LOGITS);
+          const uint32_t a_addr = tc::smem_u32(ta), b_addr = tc::smem_u32(tb);
 #pragma unroll
-    for (int kk = 0; kk < 2; ++kk) {
-      const uint64_t da = tc::smem_desc(a_addr + kk * 256, 128, (tc::BK / 8) * 128);
-      const uint64_t db = tc::smem_desc(b_addr + kk * 256, 128, (tc::BK / 8) * 128);
-      tc::mma_bf16(tmem, da, db, IDESC, kk > 0 ? 1u : 0u);
+          for (int kk = 0; kk < 2; ++kk) {
+            const uint64_t da = tc::smem_desc(a_addr + kk * 256, 128, 512);
+            const uint64_t db = tc::smem_desc(b_addr + kk * 256, 128, 512);
+            tc::mma_bf16(tmem, da, db, IDESC, kk > 0 ? 1u : 0u);
+          }
+          tc::mma_commit(bar_full);
+          tc::mma_commit(bar_afree(st));
+          last_j = j;
+        } else {
+          *abort_flag = 1u;
+          atomicOr(err, tc::ERR_TC_TIMEOUT);
+        }
+      }
+      go = __shfl_sync(0xffffffffu, go, 0);
+      if (!go) break;
     }
-    tc::mma_commit(tc::smem_u32(bar));
-    *flag = tc::mbar_wait(tc::smem_u32(bar), 0u) ? 1u : 0u;
-  }
-  __syncthreads();
-  if (*flag == 0u) {
-    if (tid == 0) atomicOr(err, tc::ERR_TC_TIMEOUT);
+    // the MMAs in flight finish before the tensor memory can be freed (the last commit covers all)
+    if (lane == 0 && last_j >= 0) tc::mbar_wait(bar_afree(last_j & 1), (uint32_t)(last_j >> 1) & 1u);
   } else {
-    tc::tc_fence_after();
-    float lg[80];
-#pragma unroll
-    for (int c0 = 0; c0 < 80; c0 += 16) {
-      float v[16];
-      tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) lg[c0 + i] = v[i] + bias.v[c0 + i];
-    }
-    const int p = p0 + warp * 32 + (tid & 31);
-    if (p < P) {
-      const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
-      float wk[25];
-      softmax_reg<25>(lg, 0, wk);
-      // the 5 clamped rows and columns of the taps (tap_index's clamping, computed once)
-      const float4* img = col + (size_t)b * h * w;
-      int rows[5], cols[5];
-#pragma unroll
-      for (int d = 0; d < 5; ++d) {
-        rows[d] = min(max(y + d - 2, 0), h - 1) * w;
-        cols[d] = min(max(x + d - 2, 0), w - 1);
+    // ---------------------------------------------------------------- epilogue
+    for (int j = 0, tile = blockIdx.x; tile < n_tiles; ++j, tile += gridDim.x) {
+      uint32_t go = 0u;
+      if (lane == 0) {
+        go = *abort_flag ? 0u : 1u;
+        if (go && !tc::mbar_wait(bar_full, (uint32_t)j & 1u)) {
+          go = 0u;
+          *abort_flag = 1u;
+          atomicOr(err, tc::ERR_TC_TIMEOUT);
+        }
       }
-      float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+      go = __shfl_sync(0xffffffffu, go, 0);
+      if (!go) break;
+      tc::tc_fence_after();
+      float lg[80];
 #pragma unroll
-      for (int k = 0; k < 25; ++k) {
-        float4 c = img[rows[k / 5] + cols[k % 5]];
-        fx += wk[k] * c.x; fy += wk[k] * c.y; fz += wk[k] * c.z;
+      for (int c0 = 0; c0 < 80; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) lg[c0 + i] = v[i] + bias.v[c0 + i];
       }
-      f1[p] = make_float4(fx, fy, fz, 1.0f);
-      float* dst = wk23 + p;
-      softmax_reg<25>(lg, 25, wk);
+      tc::tc_fence_before();
+      ws::mbar_arrive(bar_tfree);
+      const int p = tile * tc::BM + tid;
+      if (p < P) {
+        const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
+        float wk[25];
+        softmax_reg<25>(lg, 0, wk);
+        // the 5 clamped rows and columns of the taps (tap_index's clamping, computed once)
+        const float4* img = col + (size_t)b * h * w;
+        int rows[5], cols[5];
 #pragma unroll
-      for (int k = 0; k < 25; ++k, dst += P) __stcs(dst, wk[k]);
-      softmax_reg<25>(lg, 50, wk);
+        for (int d = 0; d < 5; ++d) {
+          rows[d] = min(max(y + d - 2, 0), h - 1) * w;
+          cols[d] = min(max(x + d - 2, 0), w - 1);
+        }
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
 #pragma unroll
-      for (int k = 0; k < 25; ++k, dst += P) __stcs(dst, wk[k]);
+        for (int k = 0; k < 25; ++k) {
+          float4 c = img[rows[k / 5] + cols[k % 5]];
+          fx += wk[k] * c.x; fy += wk[k] * c.y; fz += wk[k] * c.z;
+        }
+        f1[p] = make_float4(fx, fy, fz, 1.0f);
+        float* dst = wk23 + p;
+        softmax_reg<25>(lg, 25, wk);
+#pragma unroll
+        for (int k = 0; k < 25; ++k, dst += P) __stcs(dst, wk[k]);
+        softmax_reg<25>(lg, 50, wk);
+#pragma unroll
+        for (int k = 0; k < 25; ++k, dst += P) __stcs(dst, wk[k]);
+      }
     }
   }
   tc::tc_fence_before();
@@ -1237,7 +1303,8 @@ static cudaError_t forward(Net& n, uchar4* infer_rgba = nullptr, float exposure 
       if ((e = cudaStreamSynchronize(n.st))) return e;
       n.out_bias_valid = true;
     }
-    k_out_softmax<<<(P0 + tc::BM - 1) / tc::BM, tc::THREADS, OutSmem::BYTES, n.st>>>(
+    const int out_tiles = (P0 + tc::BM - 1) / tc::BM;
+    k_out_softmax<<<std::min(out_tiles, sm_count() * outk::CTAS_PER_SM), outk::THREADS, outk::SMEM, n.st>>>(
         n.d0, lo.wb, n.out_bias, n.col, n.f1, n.logits, B, n.H, n.W, n.err);
     const dim3 fg((unsigned)((n.W + 31) / 32), (unsigned)((n.H + 7) / 8), (unsigned)B);
     k_filter_stored<2><<<fg, 256, 0, n.st>>>(n.logits, 0, n.f1, n.f2, nullptr, exposure, B, n.H, n.W);

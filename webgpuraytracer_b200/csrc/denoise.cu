@@ -98,9 +98,10 @@ k_prepass(const float4* __restrict__ color, const float* __restrict__ gbuf, wgpt
 // direct gather.  The edge-stop weight of a tap pair is the same seen from either end, so the
 // exact passes evaluate each unordered pair of the tile once (3,570 pairs instead of 6,144
 // directed taps, 14.3 KB more shared memory) and each pixel then reads its 24 weights back in
-// the reference's tap order.  FAST (opt-in, not bit-exact) evaluates the four exponential edge stops as one
-// hardware exponential of their summed arguments and the normal stop with the hardware power,
-// with fused multiply-adds; its results stay within 1e-5 relative of the exact ones.
+// the reference's tap order.  FAST (opt-in, not bit-exact) evaluates the four exponential edge
+// stops as one hardware exponential of their summed arguments and the normal stop with the
+// hardware power, with fused multiply-adds; its results stay within 1e-5 relative of the exact
+// ones.
 // With COMPOSITE the last pass also remodulates and stores the rgba8 image
 // (composite_main, denoiser.wgsl:194-213), which then needs no pass of its own.
 constexpr int kTile = 16, kApron = 2, kPts = kTile + 2 * kApron;   // 20 x 20 lattice points
@@ -112,24 +113,38 @@ struct AtrousSmem {
 
 struct EdgeSigmas { float sc, sd, sa, sm, sn; };
 
+__device__ __forceinline__ bool same_normal(float4 a, float4 b) {
+  return __float_as_uint(a.x) == __float_as_uint(b.x) && __float_as_uint(a.y) == __float_as_uint(b.y) &&
+         __float_as_uint(a.z) == __float_as_uint(b.z);
+}
+
 // Edge-stop weight of the taps p (centre) and q, staged points, before the centre's attenuation:
 // denoiser.wgsl:140-170's factors and their order.  Each factor is symmetric in p and q bit for
 // bit (squared differences, products that commute, the normal test on either pixel), so the
-// weight of p's tap on q equals that of q's tap on p.
-__device__ __forceinline__ float pair_weight(const AtrousSmem& sm, int p, int q, float h, const EdgeSigmas& e) {
+// weight of p's tap on q equals that of q's tap on p.  npow[i] is the normal stop of staged point
+// i with itself, pow_(max(0, n.n), sigma_normal) (1 when its normal is too short), which every
+// pair of bitwise-equal normals (a flat face) shares; stops whose argument is exactly zero skip
+// the series, since exp_(-0 / s) is exactly 1 (s > 0).
+__device__ __forceinline__ float pair_weight(const AtrousSmem& sm, const float* npow, int p, int q, float h,
+                                             const EdgeSigmas& e) {
   const float4 cc = sm.col[p], ga = sm.ga[p], gb = sm.gb[p], gc = sm.gc[p];
   const float4 s = sm.col[q], sa4 = sm.ga[q], sb4 = sm.gb[q], sc4 = sm.gc[q];
   v3 c_diff = mk3(cc.x, cc.y, cc.z) - mk3(s.x, s.y, s.z);
-  float w_color = exp_(-dot(c_diff, c_diff) / e.sc);
+  const float c2 = dot(c_diff, c_diff);
+  float w_color = c2 == 0.0f ? 1.0f : exp_(-c2 / e.sc);
   float w_normal = 1.0f;
   if (ga.w > 0.1f || sa4.w > 0.1f) {
-    float n_dot = wmax(0.0f, dot(mk3(ga.x, ga.y, ga.z), mk3(sa4.x, sa4.y, sa4.z)));
-    w_normal = pow_(n_dot, e.sn);
+    if (same_normal(ga, sa4)) {
+      w_normal = npow[p];
+    } else {
+      float n_dot = wmax(0.0f, dot(mk3(ga.x, ga.y, ga.z), mk3(sa4.x, sa4.y, sa4.z)));
+      w_normal = pow_(n_dot, e.sn);
+    }
   }
   float d_diff = gb.x - sb4.x;
-  float w_depth = exp_(-(d_diff * d_diff) / e.sd);
-  // neighbours of the same material usually have identical albedo and material records:
-  // exp_(-0 / s) is exactly 1 (s > 0), so those stops skip the series (same value)
+  const float d2 = d_diff * d_diff;
+  float w_depth = d2 == 0.0f ? 1.0f : exp_(-d2 / e.sd);
+  // neighbours of the same material usually have identical albedo and material records
   v3 a_diff = mk3(gb.y, gb.z, gb.w) - mk3(sb4.y, sb4.z, sb4.w);
   const float a2 = dot(a_diff, a_diff);
   float w_albedo = a2 == 0.0f ? 1.0f : exp_(-a2 / e.sa);
@@ -160,6 +175,7 @@ k_atrous(const float4* __restrict__ in, const float4* __restrict__ guide, wgpt_d
          float4* __restrict__ out, float4* __restrict__ composited, uchar4* __restrict__ rgba) {
   __shared__ AtrousSmem sm;
   __shared__ float pw[FAST ? 1 : kPairSlots];
+  __shared__ float npow[FAST ? 1 : kPts * kPts];
   const int W = (int)u.width, H = (int)u.height;
   const int rx = (int)(blockIdx.x % (unsigned)step), tx = (int)(blockIdx.x / (unsigned)step);
   const int ry = (int)(blockIdx.y % (unsigned)step), ty = (int)(blockIdx.y / (unsigned)step);
@@ -173,6 +189,10 @@ k_atrous(const float4* __restrict__ in, const float4* __restrict__ guide, wgpt_d
     sm.ga[p] = __ldg(guide + si * 3);
     sm.gb[p] = __ldg(guide + si * 3 + 1);
     sm.gc[p] = __ldg(guide + si * 3 + 2);
+    if (!FAST) {
+      const float4 g = sm.ga[p];
+      npow[p] = g.w > 0.1f ? pow_(wmax(0.0f, dot(mk3(g.x, g.y, g.z), mk3(g.x, g.y, g.z))), u.sigma_normal) : 1.0f;
+    }
   }
   __syncthreads();
   EdgeSigmas es;
@@ -190,7 +210,7 @@ k_atrous(const float4* __restrict__ in, const float4* __restrict__ guide, wgpt_d
         if (t >= pair_base(k)) { odx = pair_dx(k); ody = pair_dy(k); ow = pair_w(k); ob = pair_base(k); }
       const int r = t - ob, ay = r / ow - ody, ax = r - (r / ow) * ow + min(0, -odx);
       const int pa = (ay + kApron) * kPts + (ax + kApron);
-      pw[t] = pair_weight(sm, pa, pa + ody * kPts + odx, kern_w(odx) * kern_w(ody), es);
+      pw[t] = pair_weight(sm, npow, pa, pa + ody * kPts + odx, kern_w(odx) * kern_w(ody), es);
     }
     __syncthreads();
   }
@@ -233,7 +253,7 @@ k_atrous(const float4* __restrict__ in, const float4* __restrict__ guide, wgpt_d
         }
         weight = h * __expf(-e) * w_normal;
       } else if (dx == 0 && dy == 0) {
-        weight = pair_weight(sm, cp, cp, kern[2] * kern[2], es);
+        weight = pair_weight(sm, npow, cp, cp, kern[2] * kern[2], es);
       } else if (dy > 0 || (dy == 0 && dx > 0)) {
         // the pair (this pixel, its neighbour): slot of a = this pixel
         const int k = pair_index(dx, dy);

@@ -151,13 +151,14 @@ int wgpt_get_wavefront_config(wgpt_ctx* ctx, uint32_t* pool_paths, uint64_t* uni
 
 /* Kernel variants and thresholds of the wavefront renderer, for the autotuner (no counterpart
    in the reference).  trav_shape: block shape of the closest-hit and shadow traversal kernels,
-   0 = 192 threads x 6 blocks per SM (default), 1 = 128 x 9, 2 = 256 x 4 (textured scenes keep 0
+   0 = 192 threads x 6 blocks per SM, 1 = 128 x 9, 2 = 256 x 4 (default; textured scenes keep 0
    for shadow rays); shade_block: surface-shading block of untextured scenes, 512 (default) or 256;
    refill_closest / refill_shadow: idle lanes (1..32) a traversal warp accumulates before it takes
-   new rays from the queue (defaults 24 and 8); shadow_wide: 1 (default) walks shadow rays of
+   new rays from the queue (defaults 24 and 8); shadow_wide: 1 walks shadow rays of
    scenes without alpha-textured occluders over a 4-wide view of the same BVHs (quad records
-   derived on upload: each visit tests the boxes two levels down), 0 over the reference's
-   2-wide trees.  Results do not depend on any of them. */
+   derived on upload: each visit tests the boxes two levels down), 0 (default) over the
+   reference's 2-wide trees.  Results do not depend on any of them.  The defaults are the
+   autotuner's choices on the flagship workload. */
 typedef struct wgpt_wavefront_tuning {
   uint32_t trav_shape;
   uint32_t shade_block;

@@ -1059,11 +1059,11 @@ struct WfEngine {
   int grids[8][8] = {{0}};                 // launch grid per stage, per (counting, textured, wide) variant
   int* grid = grids[0];
   // kernel variants and thresholds chosen by the wavefront tuning (wgpt_set_wavefront_tuning)
-  int trav_shape = 0;                      // traversal block shape (trav_threads / trav_blocks)
+  int trav_shape = 2;                      // traversal block shape (trav_threads / trav_blocks)
   int shade_block = 512;                   // surface-shading block of untextured scenes: 512 or 256
   uint32_t refill_closest = kRefillMinClosest;
   uint32_t refill_shadow = kRefillMinShadow;
-  int shadow_wide = 1;                     // 4-wide any-hit walk for untextured scenes
+  int shadow_wide = 0;                     // 4-wide any-hit walk for untextured scenes
   bool wide_now = false;                   // this call uses it (tuning, scene, not counting)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;

@@ -276,8 +276,8 @@ class Renderer:
         self._check(self.L.wgpt_set_wavefront_config(self.ctx, int(pool_paths), int(units_per_pass)),
                     "set_wavefront_config")
 
-    def set_wavefront_tuning(self, trav_shape: int = 0, shade_block: int = 512, refill_closest: int = 24,
-                             refill_shadow: int = 8, shadow_wide: int = 1):
+    def set_wavefront_tuning(self, trav_shape: int = 2, shade_block: int = 512, refill_closest: int = 24,
+                             refill_shadow: int = 8, shadow_wide: int = 0):
         """Kernel variants and thresholds of the wavefront renderer (results do not depend on
         them): traversal block shape 0 (192 x 6), 1 (128 x 9) or 2 (256 x 4); surface-shading
         block 512 or 256; idle lanes a traversal warp gathers before refilling (1..32); shadow

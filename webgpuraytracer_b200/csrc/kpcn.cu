@@ -133,6 +133,12 @@ struct ConvSrc {
     }
     return vec_at(b, y, x, ci0);
   }
+  // Address of the vector at (image b, row y, column x) of the output grid (null outside).
+  __device__ __forceinline__ const uint16_t* ptr_at(int b, int y, int x, int ci0) const {
+    if (y < 0 || y >= h || x < 0 || x >= w) return nullptr;
+    if (ci0 < cu) return u + (((size_t)b * hc + (y >> 1)) * wc + (x >> 1)) * cu + ci0;
+    return s + (((size_t)b * h + y) * w + x) * cs + (ci0 - cu);
+  }
   // The vector at (image b, row y, column x) of the output grid (zero outside the image).
   __device__ __forceinline__ uint4 vec_at(int b, int y, int x, int ci0) const {
     if (y < 0 || y >= h || x < 0 || x >= w) return zero4();
@@ -179,6 +185,18 @@ struct WgradA {
       tc::put_mn8(tile, g * 8, j, v);
     }
   }
+  static constexpr bool kAsync = true;
+  template <int ROWS>
+  __device__ __forceinline__ void fill_async(uint8_t* tile, int row0, int k0, int tid) const {
+    const int G = ROWS / 8;
+    const uint32_t base = tc::smem_u32(tile);
+    for (int i = tid; i < G * tc::BK; i += tc::THREADS) {
+      const int grp = i >> 3, g = grp % G, j = (grp / G) * 8 + (i & 7), p = k0 + j, co0 = row0 + g * 8;
+      const bool in = p < P && co0 < cout;
+      tc::cp_async_16(base + (uint32_t)(((g * (tc::BK / 8)) + (j >> 3)) * 128 + (j & 7) * 16),
+                      in ? dz + (size_t)p * cout + co0 : dz, in ? 16u : 0u);
+    }
+  }
 };
 
 // Weight gradient, B operand: row n = tap * cin + ci, k = pixel; the input gathered at the tap
@@ -206,6 +224,32 @@ struct WgradB {
       uint4 v = zero4();
       if (n_ok && p < P) v = src.vec_at(b, y + dy, x + dx, ci0);
       tc::put_mn8(tile, g * 8, it * 8 + (tid & 7), v);
+      p += 8;
+      x += 8;
+      while (x >= src.w) {
+        x -= src.w;
+        if (++y == src.h) { y = 0; ++b; }
+      }
+    }
+  }
+  static constexpr bool kAsync = true;
+  template <int ROWS>
+  __device__ __forceinline__ void fill_async(uint8_t* tile, int row0, int k0, int tid) const {
+    static_assert(ROWS == 128 && tc::THREADS == 128 && tc::BK == 64, "one channel group per thread");
+    const int g = tid >> 3, n = row0 + g * 8;
+    const bool n_ok = n < n_total;
+    const int tap = n_ok ? n / cin : 0, ci0 = n - tap * cin;
+    const int dy = src.taps == 9 ? src.sign * (tap / 3 - 1) : 0;
+    const int dx = src.taps == 9 ? src.sign * (tap % 3 - 1) : 0;
+    const int hw = src.h * src.w;
+    int p = k0 + (tid & 7);
+    int b = p / hw, r = p - b * hw, y = r / src.w, x = r - (r / src.w) * src.w;
+    const uint32_t base = tc::smem_u32(tile) + (uint32_t)(g * (tc::BK / 8) * 128);
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+      const uint16_t* q = (n_ok && p < P) ? src.ptr_at(b, y + dy, x + dx, ci0) : nullptr;
+      const int j = it * 8 + (tid & 7);
+      tc::cp_async_16(base + (uint32_t)((j >> 3) * 128 + (j & 7) * 16), q ? q : (src.s ? src.s : src.u), q ? 16u : 0u);
       p += 8;
       x += 8;
       while (x >= src.w) {

@@ -132,11 +132,26 @@ __device__ __forceinline__ int elem_off(int r, int k) { return ((r >> 3) * (BK /
 __device__ __forceinline__ void put_mn8(uint8_t* tile, int r0, int k, uint4 v) {
   *reinterpret_cast<uint4*>(tile + ((r0 >> 3) * (BK / 8) + (k >> 3)) * 128 + (k & 7) * 16) = v;
 }
+// 16-byte asynchronous global -> shared copy (cached in L1); src_bytes 0 writes zeros and reads
+// nothing.
+__device__ __forceinline__ void cp_async_16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // Loaders that store MN-major tiles declare `static constexpr bool kMnMajor = true`.
 template <class L, class = void>
 struct MnMajor { static constexpr bool value = false; };
 template <class L>
 struct MnMajor<L, decltype((void)L::kMnMajor)> { static constexpr bool value = L::kMnMajor; };
+// Loaders whose tiles are plain 16-byte copies also provide `fill_async`, which issues them as
+// cp.async (zero-filled where the operand has no element), and declare `kAsync = true`.
+template <class L, class = void>
+struct AsyncFill { static constexpr bool value = false; };
+template <class L>
+struct AsyncFill<L, decltype((void)L::kAsync)> { static constexpr bool value = L::kAsync; };
 
 // Fills a ROWS x BK tile from a chunk loader: `uint4 chunk(int row, int k8) const` returns
 // K-elements [8*k8, 8*k8 + 8) of operand row `row` as 8 BF16 values (zero outside the matrix).
@@ -181,20 +196,48 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(LA la, LB lb, EP ep, int M,
   constexpr uint32_t IDESC = idesc_bf16(BN) | (MnMajor<LA>::value ? 1u << 15 : 0u) | (MnMajor<LB>::value ? 1u << 16 : 0u);
   bool ok = true;
   int committed = 0;   // k-tiles whose MMAs were committed
+  // With asynchronous loaders the copies of k-tile kt + 1 are issued before k-tile kt's MMAs, so
+  // their latency overlaps the MMAs and the next iteration; otherwise each tile is filled in turn.
+  constexpr bool ASYNC = AsyncFill<LA>::value && AsyncFill<LB>::value;
+  if constexpr (ASYNC) {
+    if (KT > 0) {
+      la.template fill_async<BM>(smem, m0, kt_begin * BK, tid);
+      lb.template fill_async<BN>(smem + S::A_BYTES, n0, kt_begin * BK, tid);
+      cp_async_commit();
+    }
+  }
   for (int kt = 0; kt < KT; ++kt) {
     const int s = kt & 1;
     uint8_t* ta = smem + s * S::STAGE;
     uint8_t* tb = ta + S::A_BYTES;
-    if (kt >= 2) {
-      // the MMAs that read this stage two tiles ago must be done before it is overwritten; one
-      // thread waits and the block follows its verdict
-      if (tid == 0) *flag = mbar_wait(s ? bar1 : bar0, (uint32_t)((kt >> 1) - 1) & 1u) ? 1u : 0u;
-      __syncthreads();
-      if (*flag == 0u) { ok = false; break; }
+    if constexpr (ASYNC) {
+      if (kt + 1 < KT) {
+        if (kt >= 1) {
+          // the other stage was read by k-tile kt - 1's MMAs: done before it is overwritten
+          if (tid == 0) *flag = mbar_wait(s ? bar0 : bar1, (uint32_t)((kt - 1) >> 1) & 1u) ? 1u : 0u;
+          __syncthreads();
+          if (*flag == 0u) { ok = false; break; }
+        }
+        uint8_t* na = smem + (s ^ 1) * S::STAGE;
+        la.template fill_async<BM>(na, m0, (kt_begin + kt + 1) * BK, tid);
+        lb.template fill_async<BN>(na + S::A_BYTES, n0, (kt_begin + kt + 1) * BK, tid);
+        cp_async_commit();
+        cp_async_wait<1>();   // this thread's copies of k-tile kt have landed
+      } else {
+        cp_async_wait<0>();
+      }
+    } else {
+      if (kt >= 2) {
+        // the MMAs that read this stage two tiles ago must be done before it is overwritten; one
+        // thread waits and the block follows its verdict
+        if (tid == 0) *flag = mbar_wait(s ? bar1 : bar0, (uint32_t)((kt >> 1) - 1) & 1u) ? 1u : 0u;
+        __syncthreads();
+        if (*flag == 0u) { ok = false; break; }
+      }
+      const int k0 = (kt_begin + kt) * BK;
+      la.template fill<BM>(ta, m0, k0, tid);
+      lb.template fill<BN>(tb, n0, k0, tid);
     }
-    const int k0 = (kt_begin + kt) * BK;
-    la.template fill<BM>(ta, m0, k0, tid);
-    lb.template fill<BN>(tb, n0, k0, tid);
     fence_async_smem();
     __syncthreads();
     if (tid == 0) {
@@ -210,6 +253,7 @@ __global__ void __launch_bounds__(THREADS) k_tc_gemm(LA la, LB lb, EP ep, int M,
     }
     committed = kt + 1;
   }
+  if constexpr (ASYNC) cp_async_wait<0>();   // no copy outlives the loop (also after an abort)
   // all MMAs done: the last commit covers every earlier tcgen05 operation of the issuing thread
   // (after an expired wait this still waits, bounded, for the MMAs in flight before freeing)
   if (tid == 0) {

@@ -706,33 +706,65 @@ __global__ void k_filter_loss(const float4* __restrict__ f, const float4* __rest
   if ((threadIdx.x & 31) == 0) atomicAdd(loss, local * norm);
 }
 
-// Backward of one filter stage: logit gradients of its 25 kernel weights (softmax Jacobian) and,
-// when gin is given, the gradient of its input, scattered to the tap neighbours (atomics).
-__global__ void k_filter_bwd(const float* __restrict__ logits, int stage, int d, const float4* __restrict__ in,
-                             const float4* __restrict__ gout, uint16_t* __restrict__ dlogits, float* __restrict__ gin,
-                             int B, int h, int w) {
-  const int P = B * h * w;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-    const int b = p / (h * w), r = p - b * h * w, y = r / w, x = r - (r / w) * w;
+// Backward of one filter stage at dilation D over a 32 x 8 pixel block: logit gradients of its
+// 25 kernel weights (softmax Jacobian) and, when gin is given, the gradient of its input,
+// scattered to the tap neighbours.  The block's input colours and a 2D-pixel apron (clamped to
+// the image like tap_index) are staged in shared memory, and the input gradient is first summed
+// in a shared-memory copy of the same window, so each window point costs one global atomic per
+// channel instead of one per tap that reaches it (staged points that clamp onto the same pixel
+// each add their own share).
+template <int D>
+__global__ void __launch_bounds__(256)
+k_filter_bwd_tiled(const float* __restrict__ logits, int stage, const float4* __restrict__ in,
+                   const float4* __restrict__ gout, uint16_t* __restrict__ dlogits, float* __restrict__ gin,
+                   int B, int h, int w) {
+  constexpr int BW = 32, BH = 8, SW = BW + 4 * D, SH = BH + 4 * D, NP = SW * SH;
+  __shared__ float4 tile[NP];
+  __shared__ float acc[3][NP];
+  const int b = (int)blockIdx.z, x0 = (int)blockIdx.x * BW, y0 = (int)blockIdx.y * BH;
+  const float4* src = in + (size_t)b * h * w;
+  for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+    const int sy = i / SW, sx = i - (i / SW) * SW;
+    const int yy = min(max(y0 - 2 * D + sy, 0), h - 1), xx = min(max(x0 - 2 * D + sx, 0), w - 1);
+    tile[i] = src[(size_t)yy * w + xx];
+    acc[0][i] = 0.0f; acc[1][i] = 0.0f; acc[2][i] = 0.0f;
+  }
+  __syncthreads();
+  const int tx = (int)(threadIdx.x & 31), ty = (int)(threadIdx.x >> 5);
+  const int x = x0 + tx, y = y0 + ty;
+  if (x < w && y < h) {
+    const size_t p = ((size_t)b * h + y) * w + x;
     float wk[25], G[25];
-    softmax25(logits + (size_t)p * LOGITS + stage * 25, wk);
+    softmax25(logits + p * LOGITS + stage * 25, wk);
     const float4 g = gout[p];
     float gw = 0.0f;
+#pragma unroll
     for (int k = 0; k < 25; ++k) {
-      const size_t q = tap_index(b, y, x, k, d, h, w);
-      float4 c = in[q];
+      const int q = (ty + 2 * D + D * (k / 5 - 2)) * SW + tx + 2 * D + D * (k % 5 - 2);
+      const float4 c = tile[q];
       G[k] = g.x * c.x + g.y * c.y + g.z * c.z;
       gw += wk[k] * G[k];
       if (gin) {
-        atomicAdd(gin + q * 4 + 0, wk[k] * g.x);
-        atomicAdd(gin + q * 4 + 1, wk[k] * g.y);
-        atomicAdd(gin + q * 4 + 2, wk[k] * g.z);
+        atomicAdd(&acc[0][q], wk[k] * g.x);
+        atomicAdd(&acc[1][q], wk[k] * g.y);
+        atomicAdd(&acc[2][q], wk[k] * g.z);
       }
     }
-    uint16_t* dl = dlogits + (size_t)p * LOGITS + stage * 25;
+    uint16_t* dl = dlogits + p * LOGITS + stage * 25;
+#pragma unroll
     for (int k = 0; k < 25; ++k) dl[k] = f2bf(wk[k] * (G[k] - gw));
     if (stage == 2)
-      for (int k = 75; k < LOGITS; ++k) dlogits[(size_t)p * LOGITS + k] = 0;
+      for (int k = 75; k < LOGITS; ++k) dlogits[p * LOGITS + k] = 0;
+  }
+  if (!gin) return;
+  __syncthreads();
+  for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+    const int sy = i / SW, sx = i - (i / SW) * SW;
+    const int yy = min(max(y0 - 2 * D + sy, 0), h - 1), xx = min(max(x0 - 2 * D + sx, 0), w - 1);
+    float* dst = gin + (((size_t)b * h + yy) * w + xx) * 4;
+    if (acc[0][i] != 0.0f) atomicAdd(dst + 0, acc[0][i]);
+    if (acc[1][i] != 0.0f) atomicAdd(dst + 1, acc[1][i]);
+    if (acc[2][i] != 0.0f) atomicAdd(dst + 2, acc[2][i]);
   }
 }
 
@@ -1373,10 +1405,11 @@ static cudaError_t backward(Net& n) {
   const int P0 = (int)px(0);
   k_filter_loss<<<grid1(px(0)), 256, 0, n.st>>>(n.out, n.tgt, P0, n.gf_a, n.loss);
   if ((e = cudaMemsetAsync(n.gf_b, 0, px(0) * 16, n.st))) return e;
-  k_filter_bwd<<<grid1(px(0)), 256, 0, n.st>>>(n.logits, 2, 4, n.f2, n.gf_a, n.dlog, (float*)n.gf_b, B, n.H, n.W);
+  const dim3 fg((unsigned)((n.W + 31) / 32), (unsigned)((n.H + 7) / 8), (unsigned)B);
+  k_filter_bwd_tiled<4><<<fg, 256, 0, n.st>>>(n.logits, 2, n.f2, n.gf_a, n.dlog, (float*)n.gf_b, B, n.H, n.W);
   if ((e = cudaMemsetAsync(n.gf_a, 0, px(0) * 16, n.st))) return e;
-  k_filter_bwd<<<grid1(px(0)), 256, 0, n.st>>>(n.logits, 1, 2, n.f1, n.gf_b, n.dlog, (float*)n.gf_a, B, n.H, n.W);
-  k_filter_bwd<<<grid1(px(0)), 256, 0, n.st>>>(n.logits, 0, 1, n.col, n.gf_a, n.dlog, nullptr, B, n.H, n.W);
+  k_filter_bwd_tiled<2><<<fg, 256, 0, n.st>>>(n.logits, 1, n.f1, n.gf_b, n.dlog, (float*)n.gf_a, B, n.H, n.W);
+  k_filter_bwd_tiled<1><<<fg, 256, 0, n.st>>>(n.logits, 0, n.col, n.gf_a, n.dlog, nullptr, B, n.H, n.W);
   // OUT (1x1 over D0)
   if ((e = conv_bwd(n, n.L[L_OUT], n.dlog, nullptr, n.d0, true))) return e;
   uint16_t* gd0 = n.g_a;

@@ -463,9 +463,15 @@ cudaError_t conv3x3_nt(const HaloSrc& src, const uint16_t* wb, int cin, int N, i
 
 // Output-channel slice width per launch: the whole N when it fits one MMA pair (two
 // accumulators of N columns in 256 TMEM columns), else 128-wide slices.
+static int sm_count();
+
 template <class EP>
 cudaError_t conv3x3(const HaloSrc& src, const uint16_t* wb, int cin, int N, int B, const EP& ep, uint32_t* err,
                     cudaStream_t st) {
+  // small images (the coarse levels of training crops) have fewer 16 x 16 tiles than SMs: split
+  // the output channels into 32-wide slices so that more CTAs share the work
+  const int tiles = ((src.w + 15) / 16) * ((src.h + 15) / 16) * B;
+  if (N > 32 && tiles * ((N + 127) / 128) < sm_count()) return conv3x3_nt<32>(src, wb, cin, N, B, ep, err, st);
   switch (N) {
     case 32: return conv3x3_nt<32>(src, wb, cin, N, B, ep, err, st);
     case 48: return conv3x3_nt<48>(src, wb, cin, N, B, ep, err, st);
